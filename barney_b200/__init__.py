@@ -1,0 +1,300 @@
+"""barney_b200: B200-native (sm_100a) structured-volume path tracing behind
+Barney's native ``bn*`` API.
+
+The product is ``libbarney_b200.so`` (CUDA kernels + C++ object model,
+C ABI declared in ``include/bn_volume.h``).  This module is a thin ctypes
+mirror of that ABI, used the way an application uses Barney's native API
+(barney/native/include/barney.h): create a context, upload a structured
+scalar field, attach a transfer function, build, render, read the frame.
+
+There is no CPU fallback: importing works without a GPU, but every call that
+needs the device fails loudly if the library or the GPU is missing.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+from . import build as _build
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = _build.LIB
+_lib = None
+
+# BNDataType values (include/bn_volume.h)
+BN_OBJECT = 2
+BN_UINT8 = 110
+BN_FLOAT32 = 180
+BN_FLOAT4 = 183
+BN_UFIXED8 = 300
+BN_UFIXED8_RGBA = 301
+BN_UFIXED8_RGBA_SRGB = 302
+BNX_FLOAT16 = 1000
+BNX_BFLOAT16 = 1001
+BN_FB_COLOR = 1
+
+VOXEL_FORMATS = {"f32": BN_FLOAT32, "u8": BN_UFIXED8, "f16": BNX_FLOAT16, "bf16": BNX_BFLOAT16}
+COLOR_FORMATS = {"float4": BN_FLOAT4, "rgba8": BN_UFIXED8_RGBA, "rgba8_srgb": BN_UFIXED8_RGBA_SRGB}
+
+# every symbol include/bn_volume.h declares
+EXPORTS = [
+    "bnContextCreate", "bnContextDestroy", "bnPhysicalDeviceCount", "bnRelease", "bnAddReference", "bnCommit",
+    "bnSet1i", "bnSet2i", "bnSet3i", "bnSet4i", "bnSet1f", "bnSet2f", "bnSet3f", "bnSet4f", "bnSetObject",
+    "bnSetData", "bnDataCreate", "bnTextureData3DCreate", "bnScalarFieldCreate", "bnVolumeCreate",
+    "bnVolumeSetXF", "bnLightCreate", "bnGroupCreate", "bnGroupBuild", "bnModelCreate", "bnSetInstances",
+    "bnBuild", "bnCameraCreate", "bnRendererCreate", "bnFrameBufferCreate", "bnFrameBufferResize",
+    "bnFrameBufferRead", "bnFrameBufferGetSize", "bnAccumReset", "bnRender", "bnGetLastError",
+    "bnGetLastErrorString", "bnClearLastError", "bnxGetStats", "bnxSetStream", "bnxGetStream",
+    "bnxSetLaunchConfig", "bnxFrameBufferDevicePointer", "bnxVolumeGetMacrocells",
+]
+
+
+class bn_float2(ctypes.Structure):
+    _fields_ = [("x", ctypes.c_float), ("y", ctypes.c_float)]
+
+
+class BNXStats(ctypes.Structure):
+    _fields_ = [("samples", ctypes.c_ulonglong), ("mcVisits", ctypes.c_ulonglong), ("rays", ctypes.c_ulonglong),
+                ("pixelSamples", ctypes.c_ulonglong), ("errorFlags", ctypes.c_ulonglong),
+                ("renderMs", ctypes.c_float), ("resolveMs", ctypes.c_float)]
+
+
+class BarneyError(RuntimeError):
+    pass
+
+
+def lib(build_if_missing=True):
+    """Load libbarney_b200.so (building it first if needed)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if build_if_missing and _build._stale():
+        _build.build()
+    if not os.path.exists(LIB_PATH):
+        raise BarneyError("libbarney_b200.so is missing; run barney_b200.build.build()")
+    L = ctypes.CDLL(LIB_PATH)
+    P, I, F, S = ctypes.c_void_p, ctypes.c_int, ctypes.c_float, ctypes.c_char_p
+    sig = {
+        "bnContextCreate": ([I, P, I, P], P), "bnContextDestroy": ([P], None), "bnPhysicalDeviceCount": ([], I),
+        "bnRelease": ([P], None), "bnAddReference": ([P], None), "bnCommit": ([P], None),
+        "bnSet1i": ([P, S, I], None), "bnSet2i": ([P, S, I, I], None), "bnSet3i": ([P, S, I, I, I], None),
+        "bnSet4i": ([P, S, I, I, I, I], None), "bnSet1f": ([P, S, F], None), "bnSet2f": ([P, S, F, F], None),
+        "bnSet3f": ([P, S, F, F, F], None), "bnSet4f": ([P, S, F, F, F, F], None),
+        "bnSetObject": ([P, S, P], None), "bnSetData": ([P, S, P], None),
+        "bnDataCreate": ([P, I, I, ctypes.c_size_t, P], P),
+        "bnTextureData3DCreate": ([P, I, I, I, I, I, P], P), "bnScalarFieldCreate": ([P, I, S], P),
+        "bnVolumeCreate": ([P, I, P], P), "bnVolumeSetXF": ([P, bn_float2, P, I, F], None),
+        "bnLightCreate": ([P, I, S], P), "bnGroupCreate": ([P, I, P, I, P, I], P), "bnGroupBuild": ([P], None),
+        "bnModelCreate": ([P], P), "bnSetInstances": ([P, I, P, P, I], None), "bnBuild": ([P, I], None),
+        "bnCameraCreate": ([P, S], P), "bnRendererCreate": ([P, S], P), "bnFrameBufferCreate": ([P, I], P),
+        "bnFrameBufferResize": ([P, I, I, I, ctypes.c_uint32], None),
+        "bnFrameBufferRead": ([P, I, P, I], None), "bnFrameBufferGetSize": ([P, P, P], None),
+        "bnAccumReset": ([P], None), "bnRender": ([P, P, P, P], None), "bnGetLastError": ([], I),
+        "bnGetLastErrorString": ([], S), "bnClearLastError": ([], None),
+        "bnxGetStats": ([P, P], None), "bnxSetStream": ([P, P], None), "bnxGetStream": ([P], P),
+        "bnxSetLaunchConfig": ([P, I, I], None), "bnxFrameBufferDevicePointer": ([P], P),
+        "bnxVolumeGetMacrocells": ([P, P, P, P], None),
+    }
+    for name, (args, res) in sig.items():
+        fn = getattr(L, name)
+        fn.argtypes = args
+        fn.restype = res
+    _lib = L
+    return L
+
+
+def check():
+    """Raise BarneyError if the last bn* call on this thread recorded an error."""
+    L = lib()
+    code = L.bnGetLastError()
+    if code:
+        msg = L.bnGetLastErrorString().decode()
+        L.bnClearLastError()
+        raise BarneyError(f"barney error {code}: {msg}")
+
+
+def _b(s):
+    return s.encode() if isinstance(s, str) else s
+
+
+def _void_p(x):
+    if x is None:
+        return None
+    if isinstance(x, np.ndarray):
+        return x.ctypes.data
+    if hasattr(x, "data_ptr"):  # torch tensor (host or device)
+        return x.data_ptr()
+    return x
+
+
+class VolumeRenderer:
+    """One structured volume rendered through the bn* API (the call sequence
+    of SURVEY section 3.2/3.3: texture data -> structured field -> volume +
+    transfer function -> group -> model -> build; camera, renderer, frame
+    buffer -> bnRender -> bnFrameBufferRead).
+
+    ``desc`` is the scene dict of ``barney_b200.synth`` (the same dict the
+    oracle takes)."""
+
+    def __init__(self, desc, color_format="float4", gpu=0, stream=None):
+        L = lib()
+        self.L = L
+        self.desc = desc
+        ids = (ctypes.c_int * 1)(gpu)
+        self.ctx = L.bnContextCreate(1, None, 1, ids)
+        check()
+        if stream is not None:
+            L.bnxSetStream(self.ctx, stream)
+        self._objects = []
+        vox = desc["voxels"]
+        nz, ny, nx = vox.shape
+        self.td = self._keep(L.bnTextureData3DCreate(self.ctx, 0, VOXEL_FORMATS[desc["dtype"]], nx, ny, nz,
+                                                     _void_p(vox)))
+        check()
+        sf = self._keep(L.bnScalarFieldCreate(self.ctx, 0, b"structured"))
+        L.bnSetObject(sf, b"textureData", self.td)
+        L.bnSet3i(sf, b"dims", nx, ny, nz)
+        L.bnSet3f(sf, b"gridOrigin", *desc.get("origin", (0.0, 0.0, 0.0)))
+        L.bnSet3f(sf, b"gridSpacing", *desc["spacing"])
+        L.bnCommit(sf)
+        check()
+        self.sf = sf
+        self.vol = self._keep(L.bnVolumeCreate(self.ctx, 0, sf))
+        check()
+        self.set_transfer_function(desc["tf"], desc.get("domain", (0.0, 1.0)), desc["density"])
+        L.bnSet1f(self.vol, b"anisotropy", desc.get("anisotropy", 0.6))
+        L.bnSet1f(self.vol, b"scatteringAlbedo", desc.get("scattering_albedo", 0.9))
+        if desc.get("majorant_round_up"):
+            L.bnSet1i(self.vol, b"bnx.majorantRoundUp", 1)
+        L.bnCommit(self.vol)
+        check()
+        vols = (ctypes.c_void_p * 1)(self.vol)
+        self.group = self._keep(L.bnGroupCreate(self.ctx, 0, None, 0, vols, 1))
+        check()
+        lights = desc.get("dir_lights", [])
+        if lights:
+            hs = []
+            for l in lights:
+                h = self._keep(L.bnLightCreate(self.ctx, 0, b"directional"))
+                L.bnSet3f(h, b"direction", *l["direction"])
+                L.bnSet1f(h, b"radiance", l.get("radiance", 1.0))
+                if "color" in l:
+                    L.bnSet3f(h, b"color", *l["color"])
+                L.bnCommit(h)
+                hs.append(h)
+            arr = (ctypes.c_void_p * len(hs))(*hs)
+            data = self._keep(L.bnDataCreate(self.ctx, 0, BN_OBJECT, len(hs), arr))
+            L.bnSetData(self.group, b"lights", data)
+        L.bnGroupBuild(self.group)
+        check()
+        self.model = self._keep(L.bnModelCreate(self.ctx))
+        groups = (ctypes.c_void_p * 1)(self.group)
+        L.bnSetInstances(self.model, 0, groups, None, 1)
+        L.bnBuild(self.model, 0)
+        check()
+        self.camera = self._keep(L.bnCameraCreate(self.ctx, b"perspective"))
+        self.set_camera(desc["camera"])
+        self.renderer = self._keep(L.bnRendererCreate(self.ctx, b"default"))
+        self.fb = self._keep(L.bnFrameBufferCreate(self.ctx, 0))
+        self.color_format = color_format
+        self.resize(desc["width"], desc["height"], color_format)
+        self.set_renderer(desc, spp=desc.get("spp", 1))
+
+    def _keep(self, h):
+        self._objects.append(h)
+        return h
+
+    def set_transfer_function(self, tf, domain, density):
+        tf = np.ascontiguousarray(tf, np.float32).reshape(-1, 4)
+        self._tf = tf
+        self.L.bnVolumeSetXF(self.vol, bn_float2(*domain), tf.ctypes.data, tf.shape[0], float(density))
+        self.L.bnCommit(self.vol)
+        check()
+
+    def set_camera(self, cam):
+        L = self.L
+        L.bnSet3f(self.camera, b"position", *cam["position"])
+        L.bnSet3f(self.camera, b"direction", *cam["direction"])
+        L.bnSet3f(self.camera, b"up", *cam.get("up", (0.0, 1.0, 0.0)))
+        L.bnSet1f(self.camera, b"fovy", cam.get("fovy", 60.0))
+        L.bnCommit(self.camera)
+        check()
+
+    def set_renderer(self, desc, spp=1):
+        L = self.L
+        L.bnSet4f(self.renderer, b"bgColor", *desc.get("bg_color", (0.0, 0.0, 0.0, 1.0)))
+        L.bnSet4f(self.renderer, b"cutPlane", *desc.get("cut_plane", (0.0, 0.0, 0.0, -1e30)))
+        L.bnSet1f(self.renderer, b"ambientRadiance", desc.get("ambient", 1.0))
+        L.bnSet1i(self.renderer, b"pathsPerPixel", int(spp))
+        L.bnSet1i(self.renderer, b"maxVolumeBounces", 0)
+        L.bnSet1i(self.renderer, b"bnx.hgPhase", 1 if desc.get("phase", "simple") == "hg" else 0)
+        L.bnSet1i(self.renderer, b"bnx.emissionAbsorption", int(desc.get("emission_absorption", False)))
+        L.bnSet1i(self.renderer, b"bnx.exactLog", int(desc.get("exact_log", False)))
+        L.bnCommit(self.renderer)
+        check()
+
+    def set_spp(self, spp):
+        self.L.bnSet1i(self.renderer, b"pathsPerPixel", int(spp))
+        self.L.bnCommit(self.renderer)
+        check()
+
+    def resize(self, w, h, color_format=None):
+        fmt = color_format or self.color_format
+        self.color_format = fmt
+        self.width, self.height = w, h
+        self.L.bnFrameBufferResize(self.fb, COLOR_FORMATS[fmt], w, h, BN_FB_COLOR)
+        check()
+
+    def render(self):
+        self.L.bnRender(self.renderer, self.model, self.camera, self.fb)
+        check()
+
+    def accum_reset(self):
+        self.L.bnAccumReset(self.fb)
+        check()
+
+    def read(self, out=None):
+        """Copy the resolved colour channel into `out` (host numpy array or
+        device tensor) or a new numpy array."""
+        if out is None:
+            if self.color_format == "float4":
+                out = np.zeros((self.height, self.width, 4), np.float32)
+            else:
+                out = np.zeros((self.height, self.width), np.uint32)
+        self.L.bnFrameBufferRead(self.fb, BN_FB_COLOR, _void_p(out), COLOR_FORMATS[self.color_format])
+        check()
+        return out
+
+    def stats(self):
+        st = BNXStats()
+        self.L.bnxGetStats(self.ctx, ctypes.byref(st))
+        check()
+        return {"samples": st.samples, "mc_visits": st.mcVisits, "rays": st.rays,
+                "pixel_samples": st.pixelSamples, "error_flags": st.errorFlags,
+                "render_ms": st.renderMs, "resolve_ms": st.resolveMs}
+
+    def macrocells(self):
+        dims = (ctypes.c_int * 3)()
+        self.L.bnxVolumeGetMacrocells(self.vol, dims, None, None)
+        check()
+        d = tuple(dims)
+        ranges = np.zeros((d[2], d[1], d[0], 2), np.float32)
+        maj = np.zeros((d[2], d[1], d[0]), np.float32)
+        self.L.bnxVolumeGetMacrocells(self.vol, None, ranges.ctypes.data, maj.ctypes.data)
+        check()
+        return ranges, maj
+
+    def set_launch_config(self, blocks_per_sm=0, threads_per_block=0):
+        self.L.bnxSetLaunchConfig(self.ctx, blocks_per_sm, threads_per_block)
+        check()
+
+    def close(self):
+        if self.ctx:
+            self.L.bnContextDestroy(self.ctx)
+            self.ctx = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -1,0 +1,920 @@
+// bn_api.cpp -- host object model and extern "C" entry points of
+// barney_b200 (declared in include/bn_volume.h).
+//
+// Mirrors the object model of Barney's native layer for the structured-volume
+// path: Context (barney/native/Context.*), TextureData
+// (barney/native/common/Texture.cpp:85-135), StructuredData
+// (barney/native/volume/StructuredData.cu:128-181), Volume + TransferFunction
+// (barney/native/volume/Volume.cpp, TransferFunction.cpp), Group / Model
+// (barney/native/Group.cpp, GlobalModel.cpp, ModelSlot.cpp), DirLight
+// (barney/native/light/DirLight.*), PerspectiveCamera (barney/native/Camera.cu),
+// Renderer (barney/native/render/Renderer.*) and FrameBuffer
+// (barney/native/fb/FrameBuffer.*).  Parameter names and defaults are the
+// reference's.  Device work goes to the kernels in bn_kernels.cu.
+#include "../../include/bn_volume.h"
+#include "bn_device.h"
+
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <stdexcept>
+#include <string>
+#include <unordered_map>
+#include <vector>
+
+namespace bnb {
+
+// ---------------------------------------------------------------------------
+// errors
+// ---------------------------------------------------------------------------
+struct Error : std::runtime_error {
+  int code;
+  Error(int c, const std::string &m) : std::runtime_error(m), code(c) {}
+};
+enum : int { E_OK = 0, E_INVALID_HANDLE = 1, E_INVALID_ARG = 2, E_UNSUPPORTED = 3, E_CUDA = 4, E_STATE = 5,
+             E_OOM = 6, E_INTERNAL = 7 };
+static thread_local int g_lastError = 0;
+static thread_local std::string g_lastErrorString;
+
+static void ck(cudaError_t e, const char *what) {
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    throw Error(e == cudaErrorMemoryAllocation ? E_OOM : E_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+  }
+}
+
+// host-side float3 helpers (compiled with -ffp-contract=off)
+struct v3 { float x, y, z; };
+static inline v3 operator-(v3 a, v3 b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+static inline v3 operator*(v3 a, float s) { return {a.x * s, a.y * s, a.z * s}; }
+static inline float dot(v3 a, v3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+static inline v3 cross(v3 a, v3 b) { return {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x}; }
+static inline v3 normalize(v3 v) { return v * (1.f / sqrtf(dot(v, v))); }
+static inline float3 F3(v3 v) { return make_float3(v.x, v.y, v.z); }
+
+// ---------------------------------------------------------------------------
+// device buffer
+// ---------------------------------------------------------------------------
+struct DeviceBuffer {
+  void *ptr = nullptr;
+  size_t bytes = 0;
+  DeviceBuffer() = default;
+  DeviceBuffer(const DeviceBuffer &) = delete;
+  DeviceBuffer &operator=(const DeviceBuffer &) = delete;
+  ~DeviceBuffer() { release(); }
+  void release() {
+    if (ptr) cudaFree(ptr);
+    ptr = nullptr;
+    bytes = 0;
+  }
+  void resize(size_t n) {
+    if (n == bytes && ptr) return;
+    release();
+    if (n) ck(cudaMalloc(&ptr, n), "cudaMalloc");
+    bytes = n;
+  }
+};
+
+struct Context;
+
+// ---------------------------------------------------------------------------
+// objects (Object.h:42-56 set/commit interface)
+// ---------------------------------------------------------------------------
+struct Object : std::enable_shared_from_this<Object> {
+  enum Kind { K_DATA, K_TEXDATA, K_FIELD, K_VOLUME, K_GROUP, K_MODEL, K_LIGHT, K_CAMERA, K_RENDERER, K_FB };
+  Context *ctx;
+  Kind kind;
+  Object(Context *c, Kind k) : ctx(c), kind(k) {}
+  virtual ~Object() = default;
+  virtual bool set1i(const std::string &, int) { return false; }
+  virtual bool set3i(const std::string &, int, int, int) { return false; }
+  virtual bool set1f(const std::string &, float) { return false; }
+  virtual bool set2f(const std::string &, float, float) { return false; }
+  virtual bool set3f(const std::string &, float, float, float) { return false; }
+  virtual bool set4f(const std::string &, float, float, float, float) { return false; }
+  virtual bool setObject(const std::string &, const std::shared_ptr<Object> &) { return false; }
+  virtual void commit() {}
+};
+using ObjectSP = std::shared_ptr<Object>;
+
+struct Data : Object {
+  std::vector<ObjectSP> items;
+  explicit Data(Context *c) : Object(c, K_DATA) {}
+};
+
+struct TextureData : Object {
+  int type = VOX_F32;
+  int dims[3] = {0, 0, 0};
+  DeviceBuffer buf;
+  explicit TextureData(Context *c) : Object(c, K_TEXDATA) {}
+};
+
+// StructuredData (StructuredData.h:30-74)
+struct StructuredField : Object {
+  std::shared_ptr<TextureData> scalars;
+  int numScalars[3] = {0, 0, 0};
+  int numCells[3] = {0, 0, 0};
+  v3 gridOrigin{0, 0, 0};
+  v3 gridSpacing{1, 1, 1};
+  v3 boundsLo{0, 0, 0}, boundsHi{0, 0, 0};
+  explicit StructuredField(Context *c) : Object(c, K_FIELD) {}
+  bool set3i(const std::string &m, int x, int y, int z) override {
+    if (m == "dims") {
+      numScalars[0] = x; numScalars[1] = y; numScalars[2] = z;
+      numCells[0] = x - 1; numCells[1] = y - 1; numCells[2] = z - 1;
+      return true;
+    }
+    return false;
+  }
+  bool set3f(const std::string &m, float x, float y, float z) override {
+    if (m == "gridOrigin") { gridOrigin = {x, y, z}; return true; }
+    if (m == "gridSpacing") { gridSpacing = {x, y, z}; return true; }
+    return false;
+  }
+  bool setObject(const std::string &m, const ObjectSP &v) override {
+    if (m == "textureData") {
+      if (!v || v->kind != K_TEXDATA) throw Error(E_INVALID_ARG, "textureData must be a BNTextureData");
+      scalars = std::static_pointer_cast<TextureData>(v);
+      return true;
+    }
+    return false;
+  }
+  void commit() override {  // StructuredData.cu:177-181
+    boundsLo = gridOrigin;
+    boundsHi = {gridOrigin.x + gridSpacing.x * (float)numCells[0], gridOrigin.y + gridSpacing.y * (float)numCells[1],
+                gridOrigin.z + gridSpacing.z * (float)numCells[2]};
+  }
+};
+
+struct Volume : Object {
+  std::shared_ptr<StructuredField> sf;
+  // TransferFunction.cpp:10-24 defaults: domain [0,1], two entries of 1, density 1
+  float domain[2] = {0.f, 1.f};
+  std::vector<float4> tfValues{make_float4(1, 1, 1, 1), make_float4(1, 1, 1, 1)};
+  float baseDensity = 1.f;
+  float anisotropy = 0.6f;        // Volume.h:140
+  float scatteringAlbedo = 0.9f;  // Volume.h:141
+  int majorantRoundUp = 0;        // bnx.majorantRoundUp (precision forms)
+  bool needsMajorantRebuild = false;
+  bool built = false;
+  int mcDims[3] = {0, 0, 0};
+  DeviceBuffer tfBuf, ranges, majorants;
+  explicit Volume(Context *c) : Object(c, K_VOLUME) {}
+  bool set1i(const std::string &m, int v) override {
+    if (m == "bnx.majorantRoundUp") { majorantRoundUp = v ? 1 : 0; needsMajorantRebuild = true; return true; }
+    if (m == "userID") return true;
+    return false;
+  }
+  bool set1f(const std::string &m, float v) override {  // Volume.cpp:53-63
+    if (m == "anisotropy") { anisotropy = std::min(0.99f, std::max(-0.99f, v)); return true; }
+    if (m == "scatteringAlbedo") { scatteringAlbedo = std::min(1.f, std::max(0.f, v)); return true; }
+    return false;
+  }
+  VolumeDD dd() const;
+  void uploadTF();
+  void build();
+  void remapMajorants();
+  void commit() override;
+};
+
+struct DirLight : Object {
+  v3 direction{0.f, 0.f, -1.f};  // DirLight.h:37
+  float irradiance = NAN;
+  float radiance = 1.f;
+  v3 color{1.f, 1.f, 1.f};       // Light.h:52
+  explicit DirLight(Context *c) : Object(c, K_LIGHT) {}
+  bool set1f(const std::string &m, float v) override {
+    if (m == "irradiance") { irradiance = v; return true; }
+    if (m == "radiance") { radiance = v; return true; }
+    return false;
+  }
+  bool set3f(const std::string &m, float x, float y, float z) override {
+    if (m == "direction") { direction = {x, y, z}; return true; }
+    if (m == "color") { color = {x, y, z}; return true; }
+    if (m == "radiance") {  // DirLight.cu:48-54 (deprecated float3 form)
+      radiance = std::max(std::max(x, y), z);
+      color = {x / radiance, y / radiance, z / radiance};
+      return true;
+    }
+    if (m == "irradiance") {
+      irradiance = std::max(std::max(x, y), z);
+      color = {x / irradiance, y / irradiance, z / irradiance};
+      return true;
+    }
+    return false;
+  }
+  DirLightDD dd() const {  // DirLight.cu:11-20, identity instance
+    DirLightDD d;
+    v3 dir = normalize(direction);
+    d.toLight = make_float3(-dir.x, -dir.y, -dir.z);
+    d.color = F3(color);
+    d.radiance = std::isnan(irradiance) ? radiance : irradiance;
+    return d;
+  }
+};
+
+struct Group : Object {
+  std::shared_ptr<Volume> volume;
+  std::shared_ptr<Data> lights;
+  explicit Group(Context *c) : Object(c, K_GROUP) {}
+};
+
+struct Model : Object {
+  std::shared_ptr<Group> group;
+  bool built = false;
+  explicit Model(Context *c) : Object(c, K_MODEL) {}
+};
+
+// PerspectiveCamera (Camera.cu:17-101)
+struct Camera : Object {
+  v3 position{0, 0, 0}, direction{0, 0, 1}, up{0, 1, 0};
+  float aspect = 1.f, fovy = 60.f, focusDistance = 0.f, apertureRadius = 0.f;
+  v3 dir00{0, 0, 1}, dirdu{1, 0, 0}, dirdv{0, 1, 0}, lens00{0, 0, 0};
+  explicit Camera(Context *c) : Object(c, K_CAMERA) { commit(); }
+  bool set1f(const std::string &m, float v) override {
+    if (m == "aspect") { aspect = v; return true; }
+    if (m == "apertureRadius") { apertureRadius = v; return true; }
+    if (m == "focusDistance") { focusDistance = v; return true; }
+    if (m == "fovy") { fovy = v; return true; }
+    return false;
+  }
+  bool set3f(const std::string &m, float x, float y, float z) override {
+    if (m == "position") { position = {x, y, z}; return true; }
+    if (m == "direction") { direction = normalize(v3{x, y, z}); return true; }
+    if (m == "up") { up = {x, y, z}; return true; }
+    return false;
+  }
+  void commit() override {
+    v3 d00 = normalize(direction);
+    v3 du = normalize(cross(d00, up));
+    v3 dv = normalize(cross(du, d00));
+    d00 = d00 * (float)(1.f / (2.0f * tanf((0.5f * fovy) * (float)M_PI / 180.0f)));
+    dir00 = d00; dirdu = du; dirdv = dv; lens00 = position;
+  }
+};
+
+// Renderer (Renderer.h:17-78); staged values are committed on bnCommit.
+struct Renderer : Object {
+  struct Params {
+    float4 bgColor = make_float4(0, 0, 0, 1);
+    float4 cutPlane = make_float4(0, 0, 0, -1e30f);
+    int pathsPerPixel = 1;
+    float ambientRadiance = 1.f;
+    int maxVolumeBounces = 0;
+    int hgPhase = 0;              // bnx: multi-scatter-build phase model (HGPhase)
+    int emissionAbsorption = 0;   // bnx
+    int exactLog = 0;             // bnx
+  } staged, p;
+  explicit Renderer(Context *c) : Object(c, K_RENDERER) {}
+  bool set1i(const std::string &m, int v) override {
+    if (m == "pathsPerPixel") { staged.pathsPerPixel = v; return true; }
+    if (m == "maxVolumeBounces") { staged.maxVolumeBounces = v; return true; }
+    if (m == "crosshairs") return true;
+    if (m == "bnx.hgPhase") { staged.hgPhase = v ? 1 : 0; return true; }
+    if (m == "bnx.emissionAbsorption") { staged.emissionAbsorption = v ? 1 : 0; return true; }
+    if (m == "bnx.exactLog") { staged.exactLog = v ? 1 : 0; return true; }
+    return false;
+  }
+  bool set1f(const std::string &m, float v) override {
+    if (m == "ambientRadiance") { staged.ambientRadiance = v; return true; }
+    return false;
+  }
+  bool set4f(const std::string &m, float x, float y, float z, float w) override {
+    if (m == "bgColor") { staged.bgColor = make_float4(x, y, z, w); return true; }
+    if (m == "cutPlane") { staged.cutPlane = make_float4(x, y, z, w); return true; }
+    return false;
+  }
+  void commit() override { p = staged; }
+};
+
+struct FrameBuffer : Object {
+  int width = 0, height = 0;
+  int colorFormat = FMT_RGBA8;
+  uint32_t accumID = 0;
+  DeviceBuffer accum, color;
+  explicit FrameBuffer(Context *c) : Object(c, K_FB) {}
+};
+
+// ---------------------------------------------------------------------------
+// context
+// ---------------------------------------------------------------------------
+struct Context {
+  int device = 0;
+  cudaStream_t ownStream = nullptr;
+  cudaStream_t stream = nullptr;
+  LaunchCounters *dCounters = nullptr;
+  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+  int blocksPerSM = 0, threadsPerBlock = 128;
+  BNXStats stats{};
+  std::mutex mutex;
+  std::unordered_map<Object *, std::pair<ObjectSP, int>> handles;  // app references
+
+  explicit Context(int dev) : device(dev) {
+    ck(cudaSetDevice(dev), "cudaSetDevice");
+    ck(cudaStreamCreateWithFlags(&ownStream, cudaStreamNonBlocking), "cudaStreamCreate");
+    stream = ownStream;
+    ck(cudaMalloc(&dCounters, sizeof(LaunchCounters)), "cudaMalloc counters");
+    ck(cudaMemset(dCounters, 0, sizeof(LaunchCounters)), "cudaMemset");
+    for (auto &e : ev) ck(cudaEventCreate(&e), "cudaEventCreate");
+  }
+  ~Context() {
+    cudaSetDevice(device);
+    cudaStreamSynchronize(stream);
+    handles.clear();
+    for (auto &e : ev) if (e) cudaEventDestroy(e);
+    if (dCounters) cudaFree(dCounters);
+    if (ownStream) cudaStreamDestroy(ownStream);
+  }
+  void activate() { ck(cudaSetDevice(device), "cudaSetDevice"); }
+  BNObject add(const ObjectSP &o) {
+    std::lock_guard<std::mutex> l(mutex);
+    handles[o.get()] = {o, 1};
+    return (BNObject)o.get();
+  }
+};
+
+static std::mutex g_ctxMutex;
+static std::unordered_map<Context *, std::unique_ptr<Context>> g_contexts;
+
+static Context *getContext(BNContext c) {
+  std::lock_guard<std::mutex> l(g_ctxMutex);
+  auto it = g_contexts.find((Context *)c);
+  if (it == g_contexts.end()) throw Error(E_INVALID_HANDLE, "invalid BNContext handle");
+  return it->second.get();
+}
+
+// handle -> live object (searches all contexts; handles are unique pointers)
+static ObjectSP getObject(BNObject h) {
+  if (!h) throw Error(E_INVALID_HANDLE, "null object handle");
+  std::lock_guard<std::mutex> l(g_ctxMutex);
+  for (auto &kv : g_contexts) {
+    std::lock_guard<std::mutex> l2(kv.second->mutex);
+    auto it = kv.second->handles.find((Object *)h);
+    if (it != kv.second->handles.end()) return it->second.first;
+  }
+  throw Error(E_INVALID_HANDLE, "invalid or released object handle");
+}
+
+template <typename T>
+static std::shared_ptr<T> getAs(BNObject h, Object::Kind k, const char *what) {
+  ObjectSP o = getObject(h);
+  if (o->kind != k) throw Error(E_INVALID_HANDLE, std::string("handle is not a ") + what);
+  return std::static_pointer_cast<T>(o);
+}
+
+// ---------------------------------------------------------------------------
+// volume: TF upload, macrocell build (MCVolumeAccel::build, MCAccelerator.h:156-195)
+// ---------------------------------------------------------------------------
+VolumeDD Volume::dd() const {
+  VolumeDD v{};
+  const TextureData &td = *sf->scalars;
+  v.voxels = td.buf.ptr;
+  v.type = td.type;
+  v.numScalars = make_int3(td.dims[0], td.dims[1], td.dims[2]);
+  v.numCells = make_int3(sf->numCells[0], sf->numCells[1], sf->numCells[2]);
+  v.gridOrigin = F3(sf->gridOrigin);
+  v.rcpSpacing = make_float3(1.f / sf->gridSpacing.x, 1.f / sf->gridSpacing.y, 1.f / sf->gridSpacing.z);
+  v.boundsLo = F3(sf->boundsLo);
+  v.boundsHi = F3(sf->boundsHi);
+  v.majorants = (const float *)majorants.ptr;
+  v.mcDims = make_int3(mcDims[0], mcDims[1], mcDims[2]);
+  v.mcOrigin = F3(sf->boundsLo);                          // StructuredData.cu:76
+  const v3 mcs = {8.f * sf->gridSpacing.x, 8.f * sf->gridSpacing.y, 8.f * sf->gridSpacing.z};  // :77
+  v.rcpMcSpacing = make_float3(1.f / mcs.x, 1.f / mcs.y, 1.f / mcs.z);
+  v.tf = (const float4 *)tfBuf.ptr;
+  v.tfN = (int)tfValues.size();
+  v.domLo = domain[0];
+  v.domHi = domain[1];
+  v.baseDensity = baseDensity;
+  v.phase = PHASE_SIMPLE;
+  v.anisotropy = anisotropy;
+  v.scatteringAlbedo = scatteringAlbedo;
+  return v;
+}
+
+void Volume::uploadTF() {
+  tfBuf.resize(tfValues.size() * sizeof(float4));
+  ck(cudaMemcpyAsync(tfBuf.ptr, tfValues.data(), tfBuf.bytes, cudaMemcpyHostToDevice, ctx->stream), "TF upload");
+}
+
+void Volume::build() {
+  if (!sf || !sf->scalars) throw Error(E_STATE, "volume's scalar field has no textureData");
+  const TextureData &td = *sf->scalars;
+  for (int a = 0; a < 3; a++)
+    if (sf->numScalars[a] != td.dims[a] || sf->numScalars[a] < 2)
+      throw Error(E_INVALID_ARG, "structured field 'dims' must match the texture data and be >= 2");
+  if (!built) {
+    int d[3];
+    for (int a = 0; a < 3; a++) d[a] = (sf->numCells[a] + kCellsPerMC - 1) / kCellsPerMC;  // StructuredData.cu:74
+    const size_t n = (size_t)d[0] * d[1] * d[2];
+    if (n > 0x7fffffffull) throw Error(E_INVALID_ARG, "number of macrocells cannot be expressed in 32 bits");
+    memcpy(mcDims, d, sizeof d);
+    ranges.resize(n * sizeof(float2));
+    majorants.resize(n * sizeof(float));
+    uploadTF();
+    ck(launchBuildMacrocells(dd(), (float2 *)ranges.ptr, (float *)majorants.ptr, majorantRoundUp, ctx->stream),
+       "macrocell build");
+    built = true;
+    needsMajorantRebuild = false;
+  } else if (needsMajorantRebuild) {
+    remapMajorants();
+  }
+}
+
+void Volume::remapMajorants() {
+  uploadTF();
+  ck(launchMapMajorants(dd(), (const float2 *)ranges.ptr, (float *)majorants.ptr, majorantRoundUp, ctx->stream),
+     "majorant map");
+  needsMajorantRebuild = false;
+}
+
+void Volume::commit() {  // Volume.cpp:26-35
+  if (built && needsMajorantRebuild) remapMajorants();
+}
+
+// ---------------------------------------------------------------------------
+// render (Context::renderTiles, Context.cpp:139-182, + finalizeFrame)
+// ---------------------------------------------------------------------------
+static void render(Context *ctx, Renderer &r, Model &m, Camera &cam, FrameBuffer &fb) {
+  if (!m.built || !m.group || !m.group->volume) throw Error(E_STATE, "model has no built volume instance");
+  if (fb.width <= 0 || fb.height <= 0) throw Error(E_STATE, "frame buffer has not been resized");
+  if (cam.apertureRadius > 0.f) throw Error(E_UNSUPPORTED, "depth-of-field cameras are not supported");
+  const Renderer::Params &p = r.p;
+  if (p.hgPhase && p.maxVolumeBounces > 0)
+    throw Error(E_UNSUPPORTED, "multiple volume scattering (maxVolumeBounces > 0) is not supported");
+  if (p.pathsPerPixel <= 0) return;
+  Volume &vol = *m.group->volume;
+  vol.build();  // no-op unless the TF changed
+  VolumeDD v = vol.dd();
+  v.phase = p.hgPhase ? PHASE_HG : PHASE_SIMPLE;
+
+  FrameDD fr{};
+  fr.dir00 = F3(cam.dir00);
+  fr.dirdu = F3(cam.dirdu);
+  fr.dirdv = F3(cam.dirdv);
+  fr.lens00 = F3(cam.lens00);
+  fr.width = fb.width;
+  fr.height = fb.height;
+  fr.bgColor = p.bgColor;
+  fr.ambientRadiance = p.ambientRadiance;
+  fr.cutPlane = p.cutPlane;
+  fr.numDirLights = 0;
+  if (m.group->lights) {
+    for (auto &o : m.group->lights->items) {
+      if (!o || o->kind != Object::K_LIGHT) continue;
+      if (fr.numDirLights == kMaxDirLights) throw Error(E_UNSUPPORTED, "too many directional lights");
+      fr.dirLights[fr.numDirLights++] = std::static_pointer_cast<DirLight>(o)->dd();
+    }
+  }
+  fr.emissionAbsorption = p.emissionAbsorption;
+  fr.exactLog = p.exactLog;
+  fr.accum = (float4 *)fb.accum.ptr;
+  fr.accumID0 = (int)fb.accumID;
+  fr.spp = p.pathsPerPixel;
+
+  ck(cudaMemsetAsync(ctx->dCounters, 0, sizeof(LaunchCounters), ctx->stream), "counter reset");
+  ck(cudaEventRecord(ctx->ev[0], ctx->stream), "event");
+  ck(launchRender(v, fr, ctx->dCounters, ctx->blocksPerSM, ctx->threadsPerBlock, ctx->stream), "render kernel");
+  ck(cudaEventRecord(ctx->ev[1], ctx->stream), "event");
+  fb.accumID += p.pathsPerPixel;
+  ck(launchResolve((const float4 *)fb.accum.ptr, fb.width * fb.height, (int)fb.accumID, fb.colorFormat, fb.color.ptr,
+                   ctx->stream),
+     "resolve kernel");
+  ck(cudaEventRecord(ctx->ev[2], ctx->stream), "event");
+  LaunchCounters hc;
+  ck(cudaMemcpyAsync(&hc, ctx->dCounters, sizeof hc, cudaMemcpyDeviceToHost, ctx->stream), "counter read");
+  ck(cudaStreamSynchronize(ctx->stream), "render");
+  BNXStats &st = ctx->stats;
+  st.samples = hc.samples;
+  st.mcVisits = hc.mcVisits;
+  st.rays = hc.rays;
+  st.pixelSamples = (unsigned long long)fb.width * fb.height * p.pathsPerPixel;
+  st.errorFlags = hc.errorFlags;
+  cudaEventElapsedTime(&st.renderMs, ctx->ev[0], ctx->ev[1]);
+  cudaEventElapsedTime(&st.resolveMs, ctx->ev[1], ctx->ev[2]);
+}
+
+}  // namespace bnb
+
+using namespace bnb;
+
+// ---------------------------------------------------------------------------
+// extern "C" entry points
+// ---------------------------------------------------------------------------
+#define BN_TRY try {
+#define BN_CATCH(ret)                                              \
+  }                                                                \
+  catch (const Error &e) {                                         \
+    g_lastError = e.code;                                          \
+    g_lastErrorString = e.what();                                  \
+    return ret;                                                    \
+  }                                                                \
+  catch (const std::bad_alloc &) {                                 \
+    g_lastError = E_OOM;                                           \
+    g_lastErrorString = "host out of memory";                      \
+    return ret;                                                    \
+  }                                                                \
+  catch (const std::exception &e) {                                \
+    g_lastError = E_INTERNAL;                                      \
+    g_lastErrorString = e.what();                                  \
+    return ret;                                                    \
+  }
+
+extern "C" {
+
+BN_API int bnGetLastError(void) { return g_lastError; }
+BN_API const char *bnGetLastErrorString(void) { return g_lastErrorString.c_str(); }
+BN_API void bnClearLastError(void) { g_lastError = 0; g_lastErrorString.clear(); }
+
+BN_API int bnPhysicalDeviceCount(void) {
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess) { cudaGetLastError(); return 0; }
+  return n;
+}
+
+BN_API BNContext bnContextCreate(int numDataGroups, const int *dataRanks, int numGPUs, const int *gpuIDs) {
+  BN_TRY
+  (void)dataRanks;
+  if (numDataGroups > 1) throw Error(E_UNSUPPORTED, "only one data group per context is supported");
+  if (numGPUs > 1) throw Error(E_UNSUPPORTED, "only one GPU per context is supported");
+  int dev = (gpuIDs && numGPUs == 1) ? gpuIDs[0] : 0;
+  int n = bnPhysicalDeviceCount();
+  if (dev < 0 || dev >= n) throw Error(E_INVALID_ARG, "no such CUDA device");
+  auto c = std::make_unique<Context>(dev);
+  Context *raw = c.get();
+  std::lock_guard<std::mutex> l(g_ctxMutex);
+  g_contexts[raw] = std::move(c);
+  return (BNContext)raw;
+  BN_CATCH(nullptr)
+}
+
+BN_API void bnContextDestroy(BNContext context) {
+  BN_TRY
+  Context *c = getContext(context);
+  std::unique_ptr<Context> owned;
+  {
+    std::lock_guard<std::mutex> l(g_ctxMutex);
+    owned = std::move(g_contexts[c]);
+    g_contexts.erase(c);
+  }
+  BN_CATCH()
+}
+
+BN_API void bnRelease(BNObject object) {
+  BN_TRY
+  ObjectSP o = getObject(object);
+  Context *c = o->ctx;
+  std::lock_guard<std::mutex> l(c->mutex);
+  auto it = c->handles.find(o.get());
+  if (--it->second.second <= 0) c->handles.erase(it);
+  BN_CATCH()
+}
+
+BN_API void bnAddReference(BNObject object) {
+  BN_TRY
+  ObjectSP o = getObject(object);
+  std::lock_guard<std::mutex> l(o->ctx->mutex);
+  o->ctx->handles[o.get()].second++;
+  BN_CATCH()
+}
+
+BN_API void bnCommit(BNObject target) {
+  BN_TRY
+  ObjectSP o = getObject(target);
+  o->ctx->activate();
+  o->commit();
+  BN_CATCH()
+}
+
+static void warnUnsupported(const char *name) {
+  g_lastError = E_UNSUPPORTED;
+  g_lastErrorString = std::string("unsupported parameter '") + (name ? name : "(null)") + "'";
+}
+
+BN_API void bnSet1i(BNObject t, const char *n, int v) {
+  BN_TRY
+  if (!getObject(t)->set1i(n ? n : "", v)) warnUnsupported(n);
+  BN_CATCH()
+}
+BN_API void bnSet2i(BNObject t, const char *n, int, int) {
+  BN_TRY
+  getObject(t);
+  warnUnsupported(n);
+  BN_CATCH()
+}
+BN_API void bnSet3i(BNObject t, const char *n, int x, int y, int z) {
+  BN_TRY
+  if (!getObject(t)->set3i(n ? n : "", x, y, z)) warnUnsupported(n);
+  BN_CATCH()
+}
+BN_API void bnSet4i(BNObject t, const char *n, int, int, int, int) {
+  BN_TRY
+  getObject(t);
+  warnUnsupported(n);
+  BN_CATCH()
+}
+BN_API void bnSet1f(BNObject t, const char *n, float v) {
+  BN_TRY
+  if (!getObject(t)->set1f(n ? n : "", v)) warnUnsupported(n);
+  BN_CATCH()
+}
+BN_API void bnSet2f(BNObject t, const char *n, float x, float y) {
+  BN_TRY
+  if (!getObject(t)->set2f(n ? n : "", x, y)) warnUnsupported(n);
+  BN_CATCH()
+}
+BN_API void bnSet3f(BNObject t, const char *n, float x, float y, float z) {
+  BN_TRY
+  if (!getObject(t)->set3f(n ? n : "", x, y, z)) warnUnsupported(n);
+  BN_CATCH()
+}
+BN_API void bnSet4f(BNObject t, const char *n, float x, float y, float z, float w) {
+  BN_TRY
+  if (!getObject(t)->set4f(n ? n : "", x, y, z, w)) warnUnsupported(n);
+  BN_CATCH()
+}
+BN_API void bnSetObject(BNObject t, const char *n, BNObject v) {
+  BN_TRY
+  ObjectSP val = v ? getObject(v) : nullptr;
+  if (!getObject(t)->setObject(n ? n : "", val)) warnUnsupported(n);
+  BN_CATCH()
+}
+BN_API void bnSetData(BNObject t, const char *n, BNData v) {
+  BN_TRY
+  ObjectSP o = getObject(t);
+  std::string name = n ? n : "";
+  if (o->kind == Object::K_GROUP && name == "lights") {
+    auto g = std::static_pointer_cast<Group>(o);
+    g->lights = v ? getAs<Data>(v, Object::K_DATA, "BNData") : nullptr;
+    return;
+  }
+  warnUnsupported(n);
+  BN_CATCH()
+}
+
+BN_API BNData bnDataCreate(BNContext context, int, BNDataType type, size_t n, const void *items) {
+  BN_TRY
+  Context *c = getContext(context);
+  if (type != BN_OBJECT) throw Error(E_UNSUPPORTED, "only BN_OBJECT data arrays are supported");
+  auto d = std::make_shared<Data>(c);
+  const BNObject *objs = (const BNObject *)items;
+  for (size_t i = 0; i < n; i++) d->items.push_back(objs && objs[i] ? getObject(objs[i]) : nullptr);
+  return c->add(d);
+  BN_CATCH(nullptr)
+}
+
+BN_API BNTextureData bnTextureData3DCreate(BNContext context, int, BNDataType fmt, int w, int h, int d,
+                                           const void *texels) {
+  BN_TRY
+  Context *c = getContext(context);
+  c->activate();
+  int type;
+  size_t es;
+  switch ((int)fmt) {
+  case BN_FLOAT32: type = VOX_F32; es = 4; break;
+  case BN_UFIXED8:
+  case BN_UINT8: type = VOX_U8; es = 1; break;
+  case BNX_FLOAT16: type = VOX_F16; es = 2; break;
+  case BNX_BFLOAT16: type = VOX_BF16; es = 2; break;
+  default: throw Error(E_UNSUPPORTED, "unsupported 3D texel format");
+  }
+  if (w <= 0 || h <= 0 || d <= 0) throw Error(E_INVALID_ARG, "texture dimensions must be positive");
+  if (!texels) throw Error(E_INVALID_ARG, "texels pointer is null");
+  auto td = std::make_shared<TextureData>(c);
+  td->type = type;
+  td->dims[0] = w; td->dims[1] = h; td->dims[2] = d;
+  const size_t bytes = (size_t)w * h * d * es;
+  td->buf.resize(bytes);
+  ck(cudaMemcpyAsync(td->buf.ptr, texels, bytes, cudaMemcpyDefault, c->stream), "texture upload");
+  ck(cudaStreamSynchronize(c->stream), "texture upload");  // caller may free texels on return
+  return c->add(td);
+  BN_CATCH(nullptr)
+}
+
+BN_API BNScalarField bnScalarFieldCreate(BNContext context, int, const char *type) {
+  BN_TRY
+  Context *c = getContext(context);
+  if (!type || std::string(type) != "structured") throw Error(E_UNSUPPORTED, "only 'structured' scalar fields");
+  return c->add(std::make_shared<StructuredField>(c));
+  BN_CATCH(nullptr)
+}
+
+BN_API BNVolume bnVolumeCreate(BNContext context, int, BNScalarField sf) {
+  BN_TRY
+  Context *c = getContext(context);
+  auto v = std::make_shared<Volume>(c);
+  v->sf = getAs<StructuredField>(sf, Object::K_FIELD, "BNScalarField");
+  return c->add(v);
+  BN_CATCH(nullptr)
+}
+
+BN_API void bnVolumeSetXF(BNVolume volume, bn_float2 domain, const bn_float4 *values, int n, float densityAt1) {
+  BN_TRY
+  auto v = getAs<Volume>(volume, Object::K_VOLUME, "BNVolume");
+  if (!values || n < 2) throw Error(E_INVALID_ARG, "transfer function needs at least 2 values");
+  if (n > kMaxTF) throw Error(E_UNSUPPORTED, "transfer function has too many entries");
+  v->domain[0] = domain.x;
+  v->domain[1] = domain.y;
+  v->tfValues.resize(n);
+  memcpy(v->tfValues.data(), values, n * sizeof(bn_float4));
+  v->baseDensity = densityAt1;
+  v->needsMajorantRebuild = true;
+  BN_CATCH()
+}
+
+BN_API BNLight bnLightCreate(BNContext context, int, const char *type) {
+  BN_TRY
+  Context *c = getContext(context);
+  if (!type || std::string(type) != "directional") throw Error(E_UNSUPPORTED, "only 'directional' lights");
+  return c->add(std::make_shared<DirLight>(c));
+  BN_CATCH(nullptr)
+}
+
+BN_API BNGroup bnGroupCreate(BNContext context, int, BNGeom *, int numGeoms, BNVolume *volumes, int numVolumes) {
+  BN_TRY
+  Context *c = getContext(context);
+  if (numGeoms != 0) throw Error(E_UNSUPPORTED, "surface geometry is not supported");
+  if (numVolumes != 1 || !volumes) throw Error(E_UNSUPPORTED, "exactly one volume per group is supported");
+  auto g = std::make_shared<Group>(c);
+  g->volume = getAs<Volume>(volumes[0], Object::K_VOLUME, "BNVolume");
+  return c->add(g);
+  BN_CATCH(nullptr)
+}
+
+BN_API void bnGroupBuild(BNGroup group) {
+  BN_TRY
+  auto g = getAs<Group>(group, Object::K_GROUP, "BNGroup");
+  g->ctx->activate();
+  g->volume->build();
+  ck(cudaStreamSynchronize(g->ctx->stream), "group build");
+  BN_CATCH()
+}
+
+BN_API BNModel bnModelCreate(BNContext context) {
+  BN_TRY
+  Context *c = getContext(context);
+  return c->add(std::make_shared<Model>(c));
+  BN_CATCH(nullptr)
+}
+
+BN_API void bnSetInstances(BNModel model, int, BNGroup *groups, BNTransform *xfms, int n) {
+  BN_TRY
+  auto m = getAs<Model>(model, Object::K_MODEL, "BNModel");
+  if (n > 1) throw Error(E_UNSUPPORTED, "only one instance is supported");
+  if (n == 1 && xfms) {
+    const BNTransform &x = xfms[0];
+    bool identity = x.l.vx.x == 1 && x.l.vx.y == 0 && x.l.vx.z == 0 && x.l.vy.x == 0 && x.l.vy.y == 1 &&
+                    x.l.vy.z == 0 && x.l.vz.x == 0 && x.l.vz.y == 0 && x.l.vz.z == 1 && x.p.x == 0 && x.p.y == 0 &&
+                    x.p.z == 0;
+    if (!identity) throw Error(E_UNSUPPORTED, "only identity instance transforms are supported");
+  }
+  m->group = (n == 1 && groups) ? getAs<Group>(groups[0], Object::K_GROUP, "BNGroup") : nullptr;
+  m->built = false;
+  BN_CATCH()
+}
+
+BN_API void bnBuild(BNModel model, int) {
+  BN_TRY
+  auto m = getAs<Model>(model, Object::K_MODEL, "BNModel");
+  m->ctx->activate();
+  if (m->group && m->group->volume) m->group->volume->build();
+  ck(cudaStreamSynchronize(m->ctx->stream), "model build");
+  m->built = true;
+  BN_CATCH()
+}
+
+BN_API BNCamera bnCameraCreate(BNContext context, const char *type) {
+  BN_TRY
+  Context *c = getContext(context);
+  std::string t = type ? type : "";
+  if (t != "perspective" && t != "pinhole") throw Error(E_UNSUPPORTED, "only perspective cameras are supported");
+  return c->add(std::make_shared<Camera>(c));
+  BN_CATCH(nullptr)
+}
+
+BN_API BNRenderer bnRendererCreate(BNContext context, const char *) {
+  BN_TRY
+  Context *c = getContext(context);
+  return c->add(std::make_shared<Renderer>(c));
+  BN_CATCH(nullptr)
+}
+
+BN_API BNFrameBuffer bnFrameBufferCreate(BNContext context, int) {
+  BN_TRY
+  Context *c = getContext(context);
+  return c->add(std::make_shared<FrameBuffer>(c));
+  BN_CATCH(nullptr)
+}
+
+BN_API void bnFrameBufferResize(BNFrameBuffer fbh, BNDataType fmt, int sx, int sy, uint32_t channels) {
+  BN_TRY
+  auto fb = getAs<FrameBuffer>(fbh, Object::K_FB, "BNFrameBuffer");
+  fb->ctx->activate();
+  int f;
+  switch ((int)fmt) {
+  case BN_FLOAT4: f = FMT_FLOAT4; break;
+  case BN_UFIXED8_RGBA: f = FMT_RGBA8; break;
+  case BN_UFIXED8_RGBA_SRGB: f = FMT_RGBA8_SRGB; break;
+  default: throw Error(E_UNSUPPORTED, "unsupported frame buffer colour format");
+  }
+  if (sx <= 0 || sy <= 0) throw Error(E_INVALID_ARG, "frame buffer size must be positive");
+  if (!(channels & BN_FB_COLOR)) throw Error(E_UNSUPPORTED, "the colour channel is required");
+  fb->width = sx;
+  fb->height = sy;
+  fb->colorFormat = f;
+  fb->accum.resize((size_t)sx * sy * sizeof(float4));
+  fb->color.resize((size_t)sx * sy * (f == FMT_FLOAT4 ? 16 : 4));
+  fb->accumID = 0;
+  BN_CATCH()
+}
+
+BN_API void bnFrameBufferGetSize(BNFrameBuffer fbh, int *sx, int *sy) {
+  BN_TRY
+  if (!sx || !sy) return;
+  auto fb = getAs<FrameBuffer>(fbh, Object::K_FB, "BNFrameBuffer");
+  *sx = fb->width;
+  *sy = fb->height;
+  BN_CATCH()
+}
+
+BN_API void bnFrameBufferRead(BNFrameBuffer fbh, BNFrameBufferChannel ch, void *ptr, BNDataType fmt) {
+  BN_TRY
+  auto fb = getAs<FrameBuffer>(fbh, Object::K_FB, "BNFrameBuffer");
+  if (!ptr) return;  // FrameBuffer.cu:319
+  if (ch != BN_FB_COLOR) throw Error(E_UNSUPPORTED, "only the colour channel can be read");
+  int f = fmt == BN_FLOAT4 ? FMT_FLOAT4 : fmt == BN_UFIXED8_RGBA ? FMT_RGBA8
+        : fmt == BN_UFIXED8_RGBA_SRGB ? FMT_RGBA8_SRGB : -1;
+  if (f != fb->colorFormat) throw Error(E_INVALID_ARG, "requested format differs from the frame buffer's format");
+  fb->ctx->activate();
+  ck(cudaMemcpyAsync(ptr, fb->color.ptr, fb->color.bytes, cudaMemcpyDefault, fb->ctx->stream), "frame read");
+  ck(cudaStreamSynchronize(fb->ctx->stream), "frame read");
+  BN_CATCH()
+}
+
+BN_API void bnAccumReset(BNFrameBuffer fbh) {
+  BN_TRY
+  getAs<FrameBuffer>(fbh, Object::K_FB, "BNFrameBuffer")->accumID = 0;
+  BN_CATCH()
+}
+
+BN_API void bnRender(BNRenderer rh, BNModel mh, BNCamera ch, BNFrameBuffer fbh) {
+  BN_TRY
+  auto r = getAs<Renderer>(rh, Object::K_RENDERER, "BNRenderer");
+  auto m = getAs<Model>(mh, Object::K_MODEL, "BNModel");
+  auto c = getAs<Camera>(ch, Object::K_CAMERA, "BNCamera");
+  auto fb = getAs<FrameBuffer>(fbh, Object::K_FB, "BNFrameBuffer");
+  fb->ctx->activate();
+  render(fb->ctx, *r, *m, *c, *fb);
+  BN_CATCH()
+}
+
+BN_API void bnxGetStats(BNContext context, BNXStats *stats) {
+  BN_TRY
+  if (stats) *stats = getContext(context)->stats;
+  BN_CATCH()
+}
+
+BN_API void bnxSetStream(BNContext context, void *s) {
+  BN_TRY
+  Context *c = getContext(context);
+  c->stream = s ? (cudaStream_t)s : c->ownStream;
+  BN_CATCH()
+}
+
+BN_API void *bnxGetStream(BNContext context) {
+  BN_TRY
+  return (void *)getContext(context)->stream;
+  BN_CATCH(nullptr)
+}
+
+BN_API void bnxSetLaunchConfig(BNContext context, int bps, int tpb) {
+  BN_TRY
+  Context *c = getContext(context);
+  if (tpb != 0 && (tpb % 32 != 0 || tpb > 1024 || tpb < 32)) throw Error(E_INVALID_ARG, "threadsPerBlock");
+  c->blocksPerSM = bps < 0 ? 0 : bps;
+  c->threadsPerBlock = tpb ? tpb : 128;
+  BN_CATCH()
+}
+
+BN_API void *bnxFrameBufferDevicePointer(BNFrameBuffer fbh) {
+  BN_TRY
+  return getAs<FrameBuffer>(fbh, Object::K_FB, "BNFrameBuffer")->color.ptr;
+  BN_CATCH(nullptr)
+}
+
+BN_API void bnxVolumeGetMacrocells(BNVolume vh, int *dims3, float *rangesOut, float *majOut) {
+  BN_TRY
+  auto v = getAs<Volume>(vh, Object::K_VOLUME, "BNVolume");
+  if (!v->built) throw Error(E_STATE, "volume has not been built");
+  if (dims3) memcpy(dims3, v->mcDims, sizeof v->mcDims);
+  v->ctx->activate();
+  if (rangesOut) ck(cudaMemcpyAsync(rangesOut, v->ranges.ptr, v->ranges.bytes, cudaMemcpyDefault, v->ctx->stream), "copy");
+  if (majOut) ck(cudaMemcpyAsync(majOut, v->majorants.ptr, v->majorants.bytes, cudaMemcpyDefault, v->ctx->stream), "copy");
+  ck(cudaStreamSynchronize(v->ctx->stream), "copy");
+  BN_CATCH()
+}
+
+}  // extern "C"

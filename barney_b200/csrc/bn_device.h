@@ -1,0 +1,82 @@
+// bn_device.h -- data handed from the host object model (bn_api.cpp) to the
+// sm_100a kernels (bn_kernels.cu).  Plain structs passed by value as kernel
+// parameters; all pointers are device pointers.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace bnb {
+
+enum VoxelType : int { VOX_F32 = 0, VOX_U8 = 1, VOX_F16 = 2, VOX_BF16 = 3 };
+enum PhaseMode : int { PHASE_SIMPLE = 0, PHASE_HG = 1 };
+enum ColorFormat : int { FMT_FLOAT4 = 0, FMT_RGBA8 = 1, FMT_RGBA8_SRGB = 2 };
+enum ErrorBits : unsigned { ERR_ITER_CAP = 1u, ERR_ABORTED = 2u };
+
+constexpr int kMaxDirLights = 16;
+constexpr int kMaxTF = 4096;
+constexpr int kCellsPerMC = 8;  // StructuredData.cu:26
+
+// Structured field + macrocell majorant grid + transfer function
+// (MCVolumeAccel::DD, MCAccelerator.h:23-27).
+struct VolumeDD {
+  const void *voxels;   // x-fastest scalars, numScalars.x * .y * .z
+  int type;             // VoxelType
+  int3 numScalars;      // texture dims
+  int3 numCells;        // numScalars - 1
+  float3 gridOrigin;
+  float3 rcpSpacing;    // 1/gridSpacing (IEEE)
+  float3 boundsLo, boundsHi;
+  const float *majorants;
+  int3 mcDims;
+  float3 mcOrigin;
+  float3 rcpMcSpacing;  // 1/(8*gridSpacing)
+  const float4 *tf;     // tfN entries
+  int tfN;
+  float domLo, domHi;
+  float baseDensity;
+  int phase;            // PhaseMode
+  float anisotropy;
+  float scatteringAlbedo;
+};
+
+struct DirLightDD {
+  float3 toLight;       // -normalize(direction)  (DirLight.cu:11-20, shadeRays.cu:180)
+  float radiance;
+  float3 color;
+};
+
+// One frame's worth of render parameters (Camera::DD, Renderer::DD,
+// World::DD lights, frame buffer).
+struct FrameDD {
+  float3 dir00, dirdu, dirdv, lens00;   // PerspectiveCamera::commit, Camera.cu:82-100
+  int width, height;
+  float4 bgColor;
+  float ambientRadiance;
+  float4 cutPlane;
+  int numDirLights;
+  DirLightDD dirLights[kMaxDirLights];
+  int emissionAbsorption;
+  int exactLog;
+  float4 *accum;        // width*height, linear
+  int accumID0;         // accumID of the first wave of this launch
+  int spp;              // waves in this launch
+};
+
+// Device counters of one launch (samples, mcVisits, rays, errorFlags)
+struct LaunchCounters {
+  unsigned long long samples, mcVisits, rays, errorFlags;
+  unsigned int nextPixel;   // work counter of the persistent render kernel
+  unsigned int abort;       // host-set abort request
+};
+
+// launchers (bn_kernels.cu)
+cudaError_t launchBuildMacrocells(const VolumeDD &vol, float2 *ranges, float *majorants, int roundUp,
+                                  cudaStream_t s);
+cudaError_t launchMapMajorants(const VolumeDD &vol, const float2 *ranges, float *majorants, int roundUp,
+                               cudaStream_t s);
+cudaError_t launchRender(const VolumeDD &vol, const FrameDD &frame, LaunchCounters *counters, int blocksPerSM,
+                         int threadsPerBlock, cudaStream_t s);
+cudaError_t launchResolve(const float4 *accum, int numPixels, int accumID, int fmt, void *out, cudaStream_t s);
+int renderKernelMaxBlocksPerSM(int threadsPerBlock);
+
+}  // namespace bnb

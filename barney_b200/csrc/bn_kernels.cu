@@ -1,0 +1,793 @@
+// bn_kernels.cu -- sm_100a kernels of the structured-volume path.
+//
+//   mcBuildKernel      macrocell scalar ranges + majorants (StructuredData.cu:31-96,
+//                      MCGrid.cu:97-141), fused
+//   mcMapKernel        majorant re-map after a transfer-function change (mapMCs)
+//   renderKernel       persistent megakernel: ray generation (generateRays.cu:43-244),
+//                      box test + 3D-DDA over the macrocell grid (MCAccelerator.h:552-689,
+//                      DDA.h:61-201), Woodcock tracking with software trilinear sampling
+//                      and TF lookup (Volume.h:62-203, StructuredData.h:101-112,
+//                      rtcore/cpu/Texture.cpp:324-416, TransferFunction.h:68-87),
+//                      single-scatter shading with one shadow ray (shadeRays.cu:294-880),
+//                      shadow transmittance, and per-pixel accumulation
+//                      (shadeRays.cu:996-1040) -- rays never leave registers
+//   resolveKernel      accum * 1/accumID -> float4 / rgba8 / sRGB (TiledFB.cu:13-52)
+//
+// Numerics: compiled with --fmad=false and IEEE division/sqrt so every
+// expression is evaluated exactly as the reference source writes it; the
+// results are bit-identical to the FP32 CPU restatement in oracle/.
+//
+// Work decomposition: one warp owns an 8x4 pixel tile for all waves of the
+// launch; each lane owns one pixel and accumulates it in registers in wave
+// order (the order the reference's per-generation launches add in).  Warps
+// fetch tiles from a global counter.  Each loop iteration performs at most
+// one Woodcock step, so lanes on different rays, waves or generations keep
+// executing the sampling code together.
+#include "bn_device.h"
+
+#include <cuda_fp16.h>
+#include <cstdint>
+
+namespace bnb {
+
+#define DEV __device__ __forceinline__
+
+#define kInf __int_as_float(0x7f800000)
+// math.h:13-18
+#define ONE_PI_F 3.14159265358979323846f
+static constexpr float kFourPi = 4.f * ONE_PI_F;
+static constexpr float kOneOverFourPi = 1.f / kFourPi;
+
+// ---------------------------------------------------------------------------
+// RNG (barney-common.h:21-67)
+// ---------------------------------------------------------------------------
+static constexpr uint64_t kRngMul = 6364136223846793005ull;
+static constexpr uint64_t kRngInit = 0xcafef00dd15ea5e5ull;
+
+DEV uint32_t rngNext(uint64_t &state) {
+  uint64_t x = state;
+  unsigned count = (unsigned)(x >> 61);
+  state = x * kRngMul;
+  x ^= x >> 22;
+  return (uint32_t)(x >> (22 + count));
+}
+DEV float rngFloat(uint64_t &state) { return (rngNext(state) & 0x00FFFFFFu) * (1.f / 16777216.f); }
+DEV uint64_t rngSeed2(uint32_t a, uint32_t b) {
+  uint64_t st = kRngInit;
+  st ^= (uint32_t)(2u * a + 1u);
+  rngNext(st);
+  st ^= (uint32_t)(2u * b);
+  rngNext(st);
+  return st;
+}
+// Random2(RNGSeed &parent, b): child copies parent, parent advances once,
+// child mixes in b.
+DEV uint64_t rngDerive(uint64_t &parent, uint64_t b) {
+  uint64_t child = parent;
+  parent = parent * kRngMul;
+  child ^= ((b ? b : 290374ull) << 1);
+  rngNext(child);
+  return child;
+}
+// hash(0,0,0) of barney-common.h:88-104: instance 0, geometry 0
+static constexpr uint64_t kHash000 = (0xcbf29ce484222325ULL * 0x100000001b3ULL) * 0x100000001b3ULL;
+
+// Volume.h:154-164
+DEV float fastLog(float f) {
+  f = (f - 1.f) / (f + 1.f);
+  float f2 = f * f;
+  float s = f;
+  f *= f2;
+  s += (1.f / 3.f) * f;
+  f *= f2;
+  s += (1.f / 5.f) * f;
+  return s + s;
+}
+
+DEV float fmin_(float a, float b) { return fminf(a, b); }
+DEV float fmax_(float a, float b) { return fmaxf(a, b); }
+DEV float3 f3(float x, float y, float z) { return make_float3(x, y, z); }
+DEV float dot3(float3 a, float3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+DEV float3 normalize3(float3 v) {
+  float s = 1.f / sqrtf(dot3(v, v));
+  return f3(v.x * s, v.y * s, v.z * s);
+}
+
+// ---------------------------------------------------------------------------
+// field sampling
+// ---------------------------------------------------------------------------
+template <int T>
+DEV float loadVoxel(const void *p, int64_t i, const float *u8lut) {
+  if (T == VOX_F32) return __ldg((const float *)p + i);
+  if (T == VOX_U8) return u8lut[__ldg((const uint8_t *)p + i)];
+  if (T == VOX_F16) return __half2float(__ushort_as_half(__ldg((const unsigned short *)p + i)));
+  return __uint_as_float((uint32_t)__ldg((const unsigned short *)p + i) << 16);
+}
+
+// Texture.cpp:324-336
+DEV void lerpCoords(int &i0, int &d, float &f, int N, float tc) {
+  float u = tc - .5f;
+  if (u <= 0.f) { i0 = 0; d = 0; f = 0.f; return; }
+  if (u >= (float)(N - 1)) { i0 = N - 1; d = 0; f = 0.f; return; }
+  int iu = (int)u;
+  f = u - (float)iu;
+  i0 = iu;
+  d = 1;
+}
+DEV float lerp_l(float f, float a, float b) { return (1.f - f) * a + f * b; }
+
+// StructuredDataSampler::DD::sample + CPU LINEAR tex3D; returns NaN outside
+template <int T>
+DEV float sampleField(const VolumeDD &v, float3 P, const float *u8lut) {
+  float rx = (P.x - v.gridOrigin.x) * v.rcpSpacing.x;
+  float ry = (P.y - v.gridOrigin.y) * v.rcpSpacing.y;
+  float rz = (P.z - v.gridOrigin.z) * v.rcpSpacing.z;
+  if (rx < 0.f || ry < 0.f || rz < 0.f) return __int_as_float(0x7fc00000);
+  if (rx >= (float)v.numCells.x || ry >= (float)v.numCells.y || rz >= (float)v.numCells.z)
+    return __int_as_float(0x7fc00000);
+  int x0, y0, z0, dx, dy, dz;
+  float fx, fy, fz;
+  lerpCoords(x0, dx, fx, v.numScalars.x, rx + .5f);
+  lerpCoords(y0, dy, fy, v.numScalars.y, ry + .5f);
+  lerpCoords(z0, dz, fz, v.numScalars.z, rz + .5f);
+  const int64_t nx = v.numScalars.x, nxy = (int64_t)v.numScalars.x * v.numScalars.y;
+  const int64_t b = (int64_t)x0 + nx * y0 + nxy * z0;
+  const int64_t oy = dy ? nx : 0, oz = dz ? nxy : 0;
+  float v000 = loadVoxel<T>(v.voxels, b, u8lut);
+  float v001 = loadVoxel<T>(v.voxels, b + dx, u8lut);
+  float v010 = loadVoxel<T>(v.voxels, b + oy, u8lut);
+  float v011 = loadVoxel<T>(v.voxels, b + oy + dx, u8lut);
+  float v100 = loadVoxel<T>(v.voxels, b + oz, u8lut);
+  float v101 = loadVoxel<T>(v.voxels, b + oz + dx, u8lut);
+  float v110 = loadVoxel<T>(v.voxels, b + oz + oy, u8lut);
+  float v111 = loadVoxel<T>(v.voxels, b + oz + oy + dx, u8lut);
+  float v00 = lerp_l(fx, v000, v001);
+  float v01 = lerp_l(fx, v010, v011);
+  float v10 = lerp_l(fx, v100, v101);
+  float v11 = lerp_l(fx, v110, v111);
+  float w0 = lerp_l(fy, v00, v01);
+  float w1 = lerp_l(fy, v10, v11);
+  return lerp_l(fz, w0, w1);
+}
+
+// ---------------------------------------------------------------------------
+// macrocells (StructuredData.cu:31-62 + MCGrid.cu:97-113 + TransferFunction.h:93-117)
+// ---------------------------------------------------------------------------
+DEV float tfMajorant(const VolumeDD &v, float lo, float hi) {
+  if (lo > hi) return 0.f;
+  float span = v.domHi - v.domLo;
+  float f_lo = (lo - v.domLo) / span;
+  float f_hi = (hi - v.domLo) / span;
+  f_lo = fmin_(1.f, fmax_(0.f, f_lo));
+  f_hi = fmin_(1.f, fmax_(0.f, f_hi));
+  f_lo *= (float)(v.tfN - 1);
+  f_hi *= (float)(v.tfN - 1);
+  int i_lo = min(v.tfN - 2, max(0, (int)f_lo));
+  int i_hi = min(v.tfN - 2, max(0, (int)f_hi));
+  f_lo -= (float)i_lo;
+  f_hi -= (float)i_hi;
+  float lerp_lo = (1.f - f_lo) * v.tf[i_lo].w + f_lo * v.tf[i_lo + 1].w;
+  float lerp_hi = (1.f - f_hi) * v.tf[i_hi].w + f_hi * v.tf[i_hi + 1].w;
+  float m = 0.f;
+  m = fmax_(m, lerp_lo);
+  m = fmax_(m, lerp_hi);
+  for (int i = i_lo + 1; i <= i_hi; i++) m = fmax_(m, v.tf[i].w);
+  return m * v.baseDensity;
+}
+
+DEV float roundUpMajorant(float m, int roundUp) {
+  return (roundUp && m > 0.f) ? __int_as_float(__float_as_int(m) + 1) : m;
+}
+
+template <int T>
+__global__ void __launch_bounds__(128) mcBuildKernel(VolumeDD v, float2 *ranges, float *majorants, int roundUp) {
+  __shared__ float u8lut[256];
+  for (int i = threadIdx.x; i < 256; i += blockDim.x) u8lut[i] = (float)i * 1.f / 255.f;
+  __syncthreads();
+  const int64_t n = (int64_t)v.mcDims.x * v.mcDims.y * v.mcDims.z;
+  for (int64_t tid = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; tid < n; tid += (int64_t)gridDim.x * blockDim.x) {
+    const int mx = (int)(tid % v.mcDims.x);
+    const int my = (int)((tid / v.mcDims.x) % v.mcDims.y);
+    const int mz = (int)(tid / ((int64_t)v.mcDims.x * v.mcDims.y));
+    const int x0 = mx * kCellsPerMC, y0 = my * kCellsPerMC, z0 = mz * kCellsPerMC;
+    const int x1 = min(x0 + kCellsPerMC, v.numScalars.x - 1);
+    const int y1 = min(y0 + kCellsPerMC, v.numScalars.y - 1);
+    const int z1 = min(z0 + kCellsPerMC, v.numScalars.z - 1);
+    float lo = kInf, hi = -kInf;
+    const int64_t nx = v.numScalars.x, nxy = (int64_t)v.numScalars.x * v.numScalars.y;
+    for (int z = z0; z <= z1; z++)
+      for (int y = y0; y <= y1; y++) {
+        const int64_t row = nx * y + nxy * z;
+        for (int x = x0; x <= x1; x++) {
+          float f = loadVoxel<T>(v.voxels, row + x, u8lut);
+          lo = fmin_(lo, f);
+          hi = fmax_(hi, f);
+        }
+      }
+    ranges[tid] = make_float2(lo, hi);
+    majorants[tid] = roundUpMajorant(tfMajorant(v, lo, hi), roundUp);
+  }
+}
+
+__global__ void mcMapKernel(VolumeDD v, const float2 *ranges, float *majorants, int roundUp) {
+  const int64_t n = (int64_t)v.mcDims.x * v.mcDims.y * v.mcDims.z;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    float2 r = ranges[i];
+    majorants[i] = roundUpMajorant(tfMajorant(v, r.x, r.y), roundUp);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// render megakernel
+// ---------------------------------------------------------------------------
+enum Phase : int { PH_DONE = 0, PH_NEWSAMPLE = 1, PH_PRIMARY = 2, PH_SHADOW = 3 };
+
+// Per-lane state of the ray being traced.
+struct TraceState {
+  float3 org, dir;      // object-space ray, zero components of dir set to 1e-6
+  float rayTMax;        // ray.tMax (PRD), clamps every Woodcock range
+  float ddaTMax;        // tRange.upper after the box test, DDA's tMax
+  float rayT0;          // DDA ray_t0
+  float nextCellBegin;
+  float3 tNext, tStep;
+  int cx, cy, cz;
+  int bits;             // 1/2/4: dir.x/y/z > 0; 8/16/32: original dir component was 0
+  uint64_t rng;         // Random rng of isProg
+  bool inCell;          // a Woodcock range is active
+  bool cellValid;       // DDA has a current cell
+  float t, tUpper, maj;
+};
+
+// Ray.h:170-181
+DEV bool boxTest(float3 org, float3 dir, float &t0, float &t1, float3 lo, float3 hi) {
+  float rx = 1.f / dir.x, ry = 1.f / dir.y, rz = 1.f / dir.z;
+  float lx = (lo.x - org.x) * rx, ly = (lo.y - org.y) * ry, lz = (lo.z - org.z) * rz;
+  float hx = (hi.x - org.x) * rx, hy = (hi.y - org.y) * ry, hz = (hi.z - org.z) * rz;
+  float nx = fmin_(lx, hx), ny = fmin_(ly, hy), nz = fmin_(lz, hz);
+  float fx = fmax_(lx, hx), fy = fmax_(ly, hy), fz = fmax_(lz, hz);
+  t0 = fmax_(t0, fmax_(fmax_(nx, ny), nz));
+  t1 = fmin_(t1, fmin_(fmin_(fx, fy), fz));
+  return t0 <= t1;
+}
+
+// TraceRays::run fix-up + isProg prologue + dda3 set-up (DDA.h:68-171).
+// Returns false if the ray has no cell to visit.  raySeed is advanced when
+// the box test passes (Random rng(ray.rngSeed, ...), MCAccelerator.h:592).
+DEV bool traceBegin(const VolumeDD &v, TraceState &ts, float3 org, float3 dir, float tMax, uint64_t &raySeed) {
+  int bits = 0;
+  if (dir.x == 0.f) { dir.x = 1e-6f; bits |= 8; }
+  if (dir.y == 0.f) { dir.y = 1e-6f; bits |= 16; }
+  if (dir.z == 0.f) { dir.z = 1e-6f; bits |= 32; }
+  ts.org = org;
+  ts.dir = dir;
+  ts.rayTMax = tMax;
+  ts.inCell = false;
+  ts.cellValid = false;
+  float t0 = 0.f, t1 = tMax;
+  if (!boxTest(org, dir, t0, t1, v.boundsLo, v.boundsHi)) return false;
+  const float3 o = f3((org.x - v.mcOrigin.x) * v.rcpMcSpacing.x, (org.y - v.mcOrigin.y) * v.rcpMcSpacing.y,
+                      (org.z - v.mcOrigin.z) * v.rcpMcSpacing.z);
+  const float3 d = f3(dir.x * v.rcpMcSpacing.x, dir.y * v.rcpMcSpacing.y, dir.z * v.rcpMcSpacing.z);
+  ts.rng = rngDerive(raySeed, kHash000);
+  ts.ddaTMax = t1;
+  // dda3
+  const float3 rcpd = f3(1.f / d.x, 1.f / d.y, 1.f / d.z);
+  const float3 fs = f3((float)v.mcDims.x, (float)v.mcDims.y, (float)v.mcDims.z);
+  float lx = (0.f - o.x) * rcpd.x, ly = (0.f - o.y) * rcpd.y, lz = (0.f - o.z) * rcpd.z;
+  float hx = (fs.x - o.x) * rcpd.x, hy = (fs.y - o.y) * rcpd.y, hz = (fs.z - o.z) * rcpd.z;
+  float nx = fmin_(lx, hx), ny = fmin_(ly, hy), nz = fmin_(lz, hz);
+  float fx = fmax_(lx, hx), fy = fmax_(ly, hy), fz = fmax_(lz, hz);
+  if (d.x == 0.f) { if (o.x < 0.f || o.x > fs.x) return false; nx = -kInf; fx = kInf; }
+  if (d.y == 0.f) { if (o.y < 0.f || o.y > fs.y) return false; ny = -kInf; fy = kInf; }
+  if (d.z == 0.f) { if (o.z < 0.f || o.z > fs.z) return false; nz = -kInf; fz = kInf; }
+  const float ray_t0 = fmax_(0.f, fmax_(fmax_(nx, ny), nz));
+  const float ray_t1 = fmin_(t1, fmin_(fmin_(fx, fy), fz));
+  if (ray_t0 > ray_t1) return false;
+  const float3 oi = f3(o.x + ray_t0 * d.x, o.y + ray_t0 * d.y, o.z + ray_t0 * d.z);
+  const float3 fc = f3(fmax_(0.f, fmin_(fs.x - 1.f, floorf(oi.x))), fmax_(0.f, fmin_(fs.y - 1.f, floorf(oi.y))),
+                       fmax_(0.f, fmin_(fs.z - 1.f, floorf(oi.z))));
+  const float3 fe = f3(d.x > 0.f ? fc.x + 1.f : fc.x, d.y > 0.f ? fc.y + 1.f : fc.y, d.z > 0.f ? fc.z + 1.f : fc.z);
+  ts.tStep = f3(fabsf(rcpd.x), fabsf(rcpd.y), fabsf(rcpd.z));
+  ts.tNext = f3(d.x == 0.f ? kInf : fabsf(fe.x - oi.x) * ts.tStep.x, d.y == 0.f ? kInf : fabsf(fe.y - oi.y) * ts.tStep.y,
+                d.z == 0.f ? kInf : fabsf(fe.z - oi.z) * ts.tStep.z);
+  bits |= (d.x > 0.f ? 1 : 0) | (d.y > 0.f ? 2 : 0) | (d.z > 0.f ? 4 : 0);
+  ts.bits = bits;
+  ts.cx = (int)fc.x;
+  ts.cy = (int)fc.y;
+  ts.cz = (int)fc.z;
+  ts.rayT0 = ray_t0;
+  ts.nextCellBegin = 0.f;
+  ts.cellValid = true;
+  return true;
+}
+
+// DDA.h:184-199: leave the current cell; false when the grid is exited
+DEV bool ddaStep(const VolumeDD &v, TraceState &ts, float tClosest) {
+  ts.nextCellBegin = tClosest;
+  if (ts.tNext.x == tClosest) {
+    ts.tNext.x += ts.tStep.x;
+    ts.cx += (ts.bits & 1) ? 1 : -1;
+    if (ts.cx == ((ts.bits & 1) ? v.mcDims.x : -1)) return false;
+  }
+  if (ts.tNext.y == tClosest) {
+    ts.tNext.y += ts.tStep.y;
+    ts.cy += (ts.bits & 2) ? 1 : -1;
+    if (ts.cy == ((ts.bits & 2) ? v.mcDims.y : -1)) return false;
+  }
+  if (ts.tNext.z == tClosest) {
+    ts.tNext.z += ts.tStep.z;
+    ts.cz += (ts.bits & 4) ? 1 : -1;
+    if (ts.cz == ((ts.bits & 4) ? v.mcDims.z : -1)) return false;
+  }
+  return true;
+}
+
+struct LightSample {
+  float3 dir, radiance;
+  float pdf;
+};
+
+// DG.h:183-193
+DEV float3 randomDirection(uint64_t &rng) {
+  while (true) {
+    float x = 1.f - 2.f * rngFloat(rng);
+    float y = 1.f - 2.f * rngFloat(rng);
+    float z = 1.f - 2.f * rngFloat(rng);
+    float3 v = f3(x, y, z);
+    if (dot3(v, v) <= 1.f) return normalize3(v);
+  }
+}
+
+// Phase.h:51-58
+DEV float hgPhase(float g, float cosTheta) {
+  if (fabsf(g) < 1e-3f) return kOneOverFourPi;
+  float g2 = g * g;
+  float denom = 1.f + g2 - 2.f * g * cosTheta;
+  return kOneOverFourPi * (1.f - g2) / (denom * sqrtf(denom));
+}
+
+// shadeRays.cu:294-402 restricted to the constant environment and
+// directional lights, N = 0 (volume hit).  Returns false if no light
+// sample; sets lightNeedsMIS / lightIsDirLight.
+DEV bool sampleLights(const FrameDD &fr, uint64_t &random, LightSample &ls, bool &needsMIS, bool &isDir) {
+  needsMIS = false;
+  isDir = false;
+  // sampleEnvLight
+  const float3 eDir = randomDirection(random);
+  const float eRad = kFourPi * fr.ambientRadiance;
+  float elsWeight = eRad;  // reduce_max of a grey radiance
+  float dlsWeight = 0.f;
+  float3 dDir = f3(0.f, 0.f, 0.f), dRad = f3(0.f, 0.f, 0.f);
+  if (fr.numDirLights > 0) {
+    int lID[2];
+    float w[2];
+    float sumW = 0.f;
+    for (int i = 0; i < 2; i++) {
+      lID[i] = min(int(rngFloat(random) * fr.numDirLights), fr.numDirLights - 1);
+      w[i] = 0.f;
+      const DirLightDD &L = fr.dirLights[lID[i]];
+      float3 rad = f3(L.color.x * L.radiance, L.color.y * L.radiance, L.color.z * L.radiance);
+      float weight = 1.f;
+      weight *= fmax_(fmax_(rad.x, rad.y), rad.z);
+      if (weight <= 1e-3f) continue;
+      w[i] = weight;
+      sumW += weight;
+    }
+    if (sumW != 0.f) {
+      float r = rngFloat(random) * sumW;
+      int i = 0;
+      while (i < 2 && r >= w[i]) { r -= w[i]; ++i; }
+      if (i < 2) {
+        const DirLightDD &L = fr.dirLights[lID[i]];
+        dDir = L.toLight;
+        const float den = w[i] / sumW * (2.f / float(fr.numDirLights));
+        dRad = f3(L.color.x * L.radiance * 1.f / den, L.color.y * L.radiance * 1.f / den,
+                  L.color.z * L.radiance * 1.f / den);
+        if (w[i] != 0.f) dlsWeight = fmax_(fmax_(dRad.x, dRad.y), dRad.z);
+      }
+    }
+  }
+  float sumWeights = 0.f + dlsWeight + elsWeight + 0.f;
+  if (sumWeights == 0.f) return false;
+  elsWeight *= 1.f / sumWeights;
+  const float alsWeight = 0.f * (1.f / sumWeights);
+  dlsWeight *= 1.f / sumWeights;
+  const float plsWeight = 0.f * (1.f / sumWeights);
+  const float r = rngFloat(random);
+  if (r <= alsWeight) return false;  // area-light slot of an empty light list: pdf 0
+  if (r <= alsWeight + elsWeight) {
+    const float s = 1.f / elsWeight;
+    ls.dir = eDir;
+    ls.radiance = f3(eRad * s, eRad * s, eRad * s);
+    ls.pdf = kOneOverFourPi;
+    needsMIS = true;
+    return true;
+  }
+  if (r <= alsWeight + elsWeight + plsWeight) return false;
+  if (dlsWeight == 0.f) return false;
+  const float s = 1.f / dlsWeight;
+  ls.dir = dDir;
+  ls.radiance = f3(dRad.x * s, dRad.y * s, dRad.z * s);
+  ls.pdf = kInf;
+  isDir = true;
+  return true;
+}
+
+DEV float roundHalf(float x) { return __half2float(__float2half_rn(x)); }
+
+template <int T>
+__global__ void __launch_bounds__(128, 4) renderKernel(VolumeDD v, FrameDD fr, LaunchCounters *ctr) {
+  extern __shared__ float4 sTF[];
+  __shared__ float u8lut[256];
+  for (int i = threadIdx.x; i < v.tfN; i += blockDim.x) sTF[i] = v.tf[i];
+  for (int i = threadIdx.x; i < 256; i += blockDim.x) u8lut[i] = (float)i * 1.f / 255.f;
+  __syncthreads();
+
+  const int lane = threadIdx.x & 31;
+  const int W = fr.width, H = fr.height;
+  const int tilesX = (W + 7) >> 3;
+  const int numTiles = tilesX * ((H + 3) >> 2);
+  const float aspect = W / float(H);
+  const float tfScale = (float)(v.tfN - 1);
+  const float span = v.domHi - v.domLo;
+
+  unsigned long long nSamples = 0, nVisits = 0, nRays = 0;
+  unsigned errBits = 0;
+
+  while (true) {
+    int tile = 0, abortReq = 0;
+    if (lane == 0) {
+      tile = (int)atomicAdd(&ctr->nextPixel, 1u);
+      abortReq = (int)*(volatile unsigned *)&ctr->abort;
+    }
+    tile = __shfl_sync(0xffffffffu, tile, 0);
+    abortReq = __shfl_sync(0xffffffffu, abortReq, 0);
+    if (tile >= numTiles) break;
+    if (abortReq) { errBits |= ERR_ABORTED; break; }
+    const int ix = (tile % tilesX) * 8 + (lane & 7);
+    const int iy = (tile / tilesX) * 4 + (lane >> 3);
+    const bool active = ix < W && iy < H;
+    const int64_t pix = (int64_t)iy * W + ix;
+
+    float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (active && fr.accumID0 > 0) acc = fr.accum[pix];
+    int k = 0;                    // wave index within this launch
+    int phase = active ? PH_NEWSAMPLE : PH_DONE;
+    TraceState ts;
+    ts.inCell = false;
+    ts.cellValid = false;
+    uint64_t raySeed = 0;
+    float3 primDir = f3(0.f, 0.f, 0.f);
+    float4 bg = make_float4(0.f, 0.f, 0.f, 0.f);
+    float3 shadowTp = f3(0.f, 0.f, 0.f);
+    float misWeight = 0.f;
+    unsigned steps = 0;
+
+    while (true) {
+      // ------------------------------------------------------------------
+      // control: find the next Woodcock range of this lane (or finish)
+      // ------------------------------------------------------------------
+      while (!ts.inCell && phase != PH_DONE) {
+        bool rayEnded = false;   // current ray left the grid without collision
+        if (phase == PH_NEWSAMPLE) {
+          // ---- generateRays.cu:71-243
+          const int accumID = fr.accumID0 + k;
+          uint64_t rnd = rngSeed2(unsigned(ix + W * accumID), unsigned(iy + H * accumID));
+          raySeed = rngSeed2((uint32_t)(ix + accumID * W), (uint32_t)iy);
+          const float pixel_u = (accumID == 0) ? .5f : rngFloat(rnd);
+          const float pixel_v = (accumID == 0) ? .5f : rngFloat(rnd);
+          const float image_u = ((ix + pixel_u) / float(W));
+          const float image_v = ((iy + pixel_v) / float(H));
+          const float su = 1.f * aspect * (image_u - .5f), sv = 1.f * (image_v - .5f);
+          float3 d = f3(fr.dir00.x + su * fr.dirdu.x + sv * fr.dirdv.x, fr.dir00.y + su * fr.dirdu.y + sv * fr.dirdv.y,
+                        fr.dir00.z + su * fr.dirdu.z + sv * fr.dirdv.z);
+          d = normalize3(d);
+          float3 o = fr.lens00;
+          float tMax = 1e30f;
+          if (fr.cutPlane.w > -1e28f) {
+            const float3 N = f3(fr.cutPlane.x, fr.cutPlane.y, fr.cutPlane.z);
+            const float dist_org = dot3(N, o) + fr.cutPlane.w;
+            const float denom = dot3(N, d);
+            if (dist_org >= 0.f) {
+              if (denom < 0.f) tMax = fmin_(tMax, -dist_org / denom);
+            } else {
+              if (denom > 0.f) {
+                const float te = -dist_org / denom;
+                o = f3(o.x + te * d.x, o.y + te * d.y, o.z + te * d.z);
+              } else tMax = 0.f;
+            }
+          }
+          if (fr.bgColor.w >= 0.f) bg = fr.bgColor;
+          else {
+            const float t = (iy + .5f) / float(H);
+            bg = make_float4((1.0f - t) * 0.9f + t * 0.15f, (1.0f - t) * 0.9f + t * 0.25f,
+                             (1.0f - t) * 0.9f + t * .8f, (1.0f - t) * 1.f + t * 1.f);
+          }
+          primDir = d;
+          nRays++;
+          steps = 0;
+          phase = PH_PRIMARY;
+          if (!traceBegin(v, ts, o, d, tMax, raySeed)) rayEnded = true;
+        } else if (ts.cellValid) {
+          // ---- enter the DDA's current cell (DDA.h:173-181, MCAccelerator.h:596-612)
+          const float tClosest = fmin_(fmin_(ts.tNext.x, ts.tNext.y), ts.tNext.z);
+          const float cell_t0 = ts.rayT0 + ts.nextCellBegin;
+          const float cell_t1 = ts.rayT0 + fmin_(tClosest, ts.ddaTMax);
+          const float maj = __ldg(v.majorants + (ts.cx + (int64_t)v.mcDims.x * (ts.cy + (int64_t)v.mcDims.y * ts.cz)));
+          nVisits++;
+          if (maj == 0.f) {
+            if (!ddaStep(v, ts, tClosest)) rayEnded = true;
+          } else {
+            ts.maj = maj;
+            ts.t = cell_t0;
+            ts.tUpper = fmin_(cell_t1, ts.rayTMax);
+            ts.inCell = true;
+          }
+        } else {
+          rayEnded = true;
+        }
+        if (rayEnded) {
+          ts.cellValid = false;
+          // ---- bounce() for a ray without intersection (shadeRays.cu:507-600)
+          const int accumID = fr.accumID0 + k;
+          const float clampMax = 10.f * (1 + accumID);
+          if (phase == PH_PRIMARY) {
+            const float f0x = fmin_(bg.x, clampMax), f0y = fmin_(bg.y, clampMax), f0z = fmin_(bg.z, clampMax);
+            if (accumID == 0) acc = make_float4(f0x, f0y, f0z, bg.w);
+            else {
+              if (bg.w > 0.f) acc.w += bg.w;
+              if (f0x > 0.f) acc.x += f0x;
+              if (f0y > 0.f) acc.y += f0y;
+              if (f0z > 0.f) acc.z += f0z;
+            }
+          } else {  // shadow ray reached the light
+            const float f1x = fmin_(misWeight * shadowTp.x, clampMax);
+            const float f1y = fmin_(misWeight * shadowTp.y, clampMax);
+            const float f1z = fmin_(misWeight * shadowTp.z, clampMax);
+            if (f1x > 0.f) acc.x += f1x;
+            if (f1y > 0.f) acc.y += f1y;
+            if (f1z > 0.f) acc.z += f1z;
+          }
+          if (++k == fr.spp) phase = PH_DONE;
+          else phase = PH_NEWSAMPLE;
+        }
+      }
+      if (phase == PH_DONE) break;
+
+      // ------------------------------------------------------------------
+      // one Woodcock step (Volume.h:180-201)
+      // ------------------------------------------------------------------
+      bool hit = false;
+      float4 sample = make_float4(0.f, 0.f, 0.f, 0.f);
+      {
+        const float r = rngFloat(ts.rng);
+        const float dt = fr.exactLog ? (-logf(1.f - r) / ts.maj) : (-fastLog(1.f - r) / ts.maj);
+        ts.t += dt;
+        if (ts.t >= ts.tUpper) {
+          ts.inCell = false;
+          const float tClosest = fmin_(fmin_(ts.tNext.x, ts.tNext.y), ts.tNext.z);
+          if (!ddaStep(v, ts, tClosest)) ts.cellValid = false;
+        } else {
+          const float3 P = f3(ts.org.x + ts.t * ts.dir.x, ts.org.y + ts.t * ts.dir.y, ts.org.z + ts.t * ts.dir.z);
+          const float s = sampleField<T>(v, P, u8lut);
+          nSamples++;
+          float w = 0.f;
+          int idx = 0;
+          float f = 0.f;
+          if (!isnan(s)) {
+            f = (s - v.domLo) / span;
+            f = fmin_(1.f, fmax_(0.f, f));
+            f *= tfScale;
+            idx = min(v.tfN - 2, max(0, (int)f));
+            f -= (float)idx;
+            w = ((1.f - f) * sTF[idx].w + f * sTF[idx + 1].w) * v.baseDensity;
+          }
+          if (w >= rngFloat(ts.rng) * ts.maj) {
+            hit = true;
+            if (!isnan(s)) {
+              const float4 a = sTF[idx], b = sTF[idx + 1];
+              sample = make_float4((1.f - f) * a.x + f * b.x, (1.f - f) * a.y + f * b.y, (1.f - f) * a.z + f * b.z, w);
+            }
+          }
+        }
+        if (++steps > (1u << 22)) {  // iteration cap: terminate this ray as a miss
+          errBits |= ERR_ITER_CAP;
+          ts.inCell = false;
+          ts.cellValid = false;
+        }
+      }
+      if (!hit) continue;
+
+      // ------------------------------------------------------------------
+      // collision: shade (primary) or occlusion (shadow)
+      // ------------------------------------------------------------------
+      ts.inCell = false;
+      ts.cellValid = false;
+      const int accumID = fr.accumID0 + k;
+      const float clampMax = 10.f * (1 + accumID);
+      if (phase == PH_SHADOW) {  // occluded: no contribution
+        if (++k == fr.spp) phase = PH_DONE;
+        else phase = PH_NEWSAMPLE;
+        continue;
+      }
+      // primary hit: generation-0 accumulation (fragment 0, alpha 1)
+      if (accumID == 0) acc = make_float4(0.f, 0.f, 0.f, 1.f);
+      else acc.w += 1.f;
+      const float tHit = ts.t;
+      const float3 P = f3(ts.org.x + tHit * ts.dir.x, ts.org.y + tHit * ts.dir.y, ts.org.z + tHit * ts.dir.z);
+      bool spawned = false;
+      if (fr.emissionAbsorption) {
+        const float ex = fmin_(sample.x, clampMax), ey = fmin_(sample.y, clampMax), ez = fmin_(sample.z, clampMax);
+        if (accumID == 0) acc = make_float4(ex, ey, ez, 1.f);
+        else {
+          if (ex > 0.f) acc.x += ex;
+          if (ey > 0.f) acc.y += ey;
+          if (ez > 0.f) acc.z += ez;
+        }
+      } else {
+        // bounce() volume-hit branch, shadeRays.cu:608-746
+        uint64_t random = rngDerive(raySeed, (uint64_t)__float_as_uint(tHit));
+        const float3 won = normalize3(primDir);
+        const float3 woN = f3(-won.x, -won.y, -won.z);  // dg.wo
+        const float offsetEpsilon = fmax_(1e-4f, 1e-6f * fmax_(fmax_(fabsf(P.x), fabsf(P.y)), fabsf(P.z)));
+        LightSample ls;
+        bool needsMIS, isDir;
+        if (sampleLights(fr, random, ls, needsMIS, isDir)) {
+          float3 alb;
+          float fpdf;
+          if (v.phase == PHASE_SIMPLE) {
+            alb = f3(.7f * sample.x, .7f * sample.y, .7f * sample.z);
+            fpdf = kOneOverFourPi;
+          } else {
+            alb = f3(v.scatteringAlbedo * sample.x, v.scatteringAlbedo * sample.y, v.scatteringAlbedo * sample.z);
+            const float3 wi_in = normalize3(f3(-woN.x, -woN.y, -woN.z));
+            fpdf = hgPhase(v.anisotropy, dot3(wi_in, normalize3(ls.dir)));
+          }
+          float3 fv = f3(fpdf * alb.x, fpdf * alb.y, fpdf * alb.z);
+          if (fpdf > 0.f && !(fmax_(fmax_(fv.x, fv.y), fv.z) < 1e-4f)) {
+            fv = f3(fmin_(fv.x, 13.f), fmin_(fv.y, 13.f), fmin_(fv.z, 13.f));
+            const float ip = isinf(ls.pdf) ? 1.f : (1.f / ls.pdf);
+            const float3 tp = f3(1.f * ip * fv.x * ls.radiance.x * 1.f, 1.f * ip * fv.y * ls.radiance.y * 1.f,
+                                 1.f * ip * fv.z * ls.radiance.z * 1.f);
+            misWeight = 1.f;
+            bool alive = true;
+            if (!isDir && needsMIS) {
+              const float pl = kOneOverFourPi;
+              float ps;
+              if (v.phase == PHASE_SIMPLE) ps = kOneOverFourPi;
+              else ps = hgPhase(v.anisotropy, dot3(normalize3(f3(-woN.x, -woN.y, -woN.z)), normalize3(ls.dir)));
+              misWeight = pl / (pl + ps + 1e-10f);
+              if (misWeight < 1e-5f) alive = false;
+            }
+            const float sTMax = kInf * (1.f - 2.f * offsetEpsilon);
+            if (alive && sTMax > 0.f) {
+              shadowTp = f3(roundHalf(tp.x), roundHalf(tp.y), roundHalf(tp.z));
+              const float3 so = f3(P.x + offsetEpsilon * woN.x, P.y + offsetEpsilon * woN.y, P.z + offsetEpsilon * woN.z);
+              uint64_t shadowSeed = raySeed;
+              phase = PH_SHADOW;
+              spawned = true;
+              nRays++;
+              steps = 0;
+              traceBegin(v, ts, so, ls.dir, sTMax, shadowSeed);
+              // a shadow ray with no cell to visit is handled as reaching the light
+            }
+          }
+        }
+      }
+      if (!spawned) {
+        if (++k == fr.spp) phase = PH_DONE;
+        else phase = PH_NEWSAMPLE;
+      }
+    }
+    if (active) fr.accum[pix] = acc;
+    __syncwarp();
+  }
+
+  // counters: warp reduction, one atomic per warp
+  for (int o = 16; o > 0; o >>= 1) {
+    nSamples += __shfl_down_sync(0xffffffffu, nSamples, o);
+    nVisits += __shfl_down_sync(0xffffffffu, nVisits, o);
+    nRays += __shfl_down_sync(0xffffffffu, nRays, o);
+    errBits |= __shfl_down_sync(0xffffffffu, errBits, o);
+  }
+  if (lane == 0) {
+    atomicAdd(&ctr->samples, nSamples);
+    atomicAdd(&ctr->mcVisits, nVisits);
+    atomicAdd(&ctr->rays, nRays);
+    if (errBits) atomicOr(&ctr->errorFlags, (unsigned long long)errBits);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// resolve (TiledFB.cu:13-52, math.h:61-125)
+// ---------------------------------------------------------------------------
+DEV float linearToSrgb(float x) {
+  if (x <= 0.0031308f) return 12.92f * x;
+  return 1.055f * powf(x, 1.f / 2.4f) - 0.055f;
+}
+DEV uint32_t make8(float f) { return (uint32_t)min(255, max(0, int(f * 256.f))); }
+
+__global__ void resolveKernel(const float4 *accum, int n, float accumScale, int fmt, void *out) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    float4 a = accum[i];
+    float4 c = make_float4(a.x * accumScale, a.y * accumScale, a.z * accumScale, a.w * accumScale);
+    if (fmt == FMT_FLOAT4) {
+      ((float4 *)out)[i] = c;
+    } else {
+      if (fmt == FMT_RGBA8_SRGB) { c.x = linearToSrgb(c.x); c.y = linearToSrgb(c.y); c.z = linearToSrgb(c.z); }
+      ((uint32_t *)out)[i] = (make8(c.x) << 0) + (make8(c.y) << 8) + (make8(c.z) << 16) + (make8(c.w) << 24);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// launchers
+// ---------------------------------------------------------------------------
+static int smCount() {
+  static int n = 0;
+  if (!n) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+  }
+  return n;
+}
+
+cudaError_t launchBuildMacrocells(const VolumeDD &v, float2 *ranges, float *majorants, int roundUp, cudaStream_t s) {
+  const int64_t n = (int64_t)v.mcDims.x * v.mcDims.y * v.mcDims.z;
+  const int blocks = (int)std::min<int64_t>((n + 127) / 128, (int64_t)smCount() * 16);
+  switch (v.type) {
+  case VOX_F32: mcBuildKernel<VOX_F32><<<blocks, 128, 0, s>>>(v, ranges, majorants, roundUp); break;
+  case VOX_U8: mcBuildKernel<VOX_U8><<<blocks, 128, 0, s>>>(v, ranges, majorants, roundUp); break;
+  case VOX_F16: mcBuildKernel<VOX_F16><<<blocks, 128, 0, s>>>(v, ranges, majorants, roundUp); break;
+  default: mcBuildKernel<VOX_BF16><<<blocks, 128, 0, s>>>(v, ranges, majorants, roundUp); break;
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t launchMapMajorants(const VolumeDD &v, const float2 *ranges, float *majorants, int roundUp, cudaStream_t s) {
+  const int64_t n = (int64_t)v.mcDims.x * v.mcDims.y * v.mcDims.z;
+  const int blocks = (int)std::min<int64_t>((n + 255) / 256, (int64_t)smCount() * 8);
+  mcMapKernel<<<blocks, 256, 0, s>>>(v, ranges, majorants, roundUp);
+  return cudaGetLastError();
+}
+
+template <int T>
+static cudaError_t launchRenderT(const VolumeDD &v, const FrameDD &fr, LaunchCounters *ctr, int bps, int tpb,
+                                 cudaStream_t s) {
+  const size_t smem = (size_t)v.tfN * sizeof(float4);
+  auto kern = renderKernel<T>;
+  if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (bps <= 0) {
+    int occ = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, tpb, smem);
+    bps = occ > 0 ? occ : 1;
+  }
+  kern<<<smCount() * bps, tpb, smem, s>>>(v, fr, ctr);
+  return cudaGetLastError();
+}
+
+cudaError_t launchRender(const VolumeDD &v, const FrameDD &fr, LaunchCounters *ctr, int bps, int tpb, cudaStream_t s) {
+  if (tpb <= 0) tpb = 128;
+  switch (v.type) {
+  case VOX_F32: return launchRenderT<VOX_F32>(v, fr, ctr, bps, tpb, s);
+  case VOX_U8: return launchRenderT<VOX_U8>(v, fr, ctr, bps, tpb, s);
+  case VOX_F16: return launchRenderT<VOX_F16>(v, fr, ctr, bps, tpb, s);
+  default: return launchRenderT<VOX_BF16>(v, fr, ctr, bps, tpb, s);
+  }
+}
+
+cudaError_t launchResolve(const float4 *accum, int n, int accumID, int fmt, void *out, cudaStream_t s) {
+  const float accumScale = 1.f / accumID;
+  const int blocks = std::max(1, std::min((n + 255) / 256, smCount() * 8));
+  resolveKernel<<<blocks, 256, 0, s>>>(accum, n, accumScale, fmt, out);
+  return cudaGetLastError();
+}
+
+int renderKernelMaxBlocksPerSM(int tpb) {
+  int occ = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, renderKernel<VOX_F32>, tpb, 256 * sizeof(float4));
+  return occ;
+}
+
+}  // namespace bnb

@@ -1,0 +1,228 @@
+/* bn_volume.h -- C ABI of barney_b200, a B200-native (sm_100a) replacement
+ * for Barney's structured-volume path-tracing path.
+ *
+ * The bn* entry points below have the names, argument meanings and call
+ * order of Barney's native API (barney/native/include/barney.h, where they
+ * are C++ functions in namespace BARNEY_NS, deliberately not extern "C",
+ * implemented in barney/native/barney.cu).  Here they are plain extern "C"
+ * symbols over opaque handles, so any FFI (ctypes, cgo, JNI, N-API) or a C++
+ * namespace shim (include/barney_shim.hpp) can bind them.  Each declaration
+ * cites the reference entry point it replaces.
+ *
+ * Scope: one GPU; scalar fields of type "structured" (float32 / unorm8, plus
+ * the float16 / bfloat16 storage forms added here); one volume per group,
+ * identity instance transforms; pinhole ("perspective") camera; constant
+ * environment (ambientRadiance) and "directional" lights; colour channel of
+ * the frame buffer.  Anything else is rejected with an error.
+ *
+ * Errors: the reference throws C++ exceptions through its API
+ * (barney.cu:23-37).  No exception crosses this ABI: every entry point
+ * catches, records a thread-local error (bnGetLastError /
+ * bnGetLastErrorString) and returns (0 / NULL for constructors).
+ *
+ * Threading: as in the reference, calls are expected from one thread per
+ * context; bnRender is synchronous (returns after the frame is resolved).
+ */
+#ifndef BN_VOLUME_H
+#define BN_VOLUME_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#define BN_API __attribute__((visibility("default")))
+#else
+#define BN_API
+#endif
+
+typedef struct _BNContext *BNContext;
+typedef struct _BNObject *BNObject;
+typedef BNObject BNData;
+typedef BNObject BNTextureData;
+typedef BNObject BNScalarField;
+typedef BNObject BNGeom;
+typedef BNObject BNVolume;
+typedef BNObject BNGroup;
+typedef BNObject BNModel;
+typedef BNObject BNRenderer;
+typedef BNObject BNFrameBuffer;
+typedef BNObject BNLight;
+typedef BNObject BNCamera;
+
+typedef struct { float x, y; } bn_float2;
+typedef struct { float x, y, z; } bn_float3;
+typedef struct { float x, y, z, w; } bn_float4;
+
+/* barney.h BNTransform: 3x3 linear part (columns vx, vy, vz) + translation */
+typedef struct {
+  struct { bn_float3 vx, vy, vz; } l;
+  bn_float3 p;
+} BNTransform;
+
+/* barney.h BNFrameBufferChannel (values kept) */
+typedef enum {
+  BN_FB_COLOR = (1 << 0),
+  BN_FB_DEPTH = (1 << 1),
+  BN_FB_PRIMID = (1 << 2),
+  BN_FB_INSTID = (1 << 3),
+  BN_FB_OBJID = (1 << 4),
+  BN_FB_NORMAL = (1 << 5)
+} BNFrameBufferChannel;
+
+/* barney.h BNDataType (values kept; only the ones this path uses listed) */
+typedef enum {
+  BN_DATA_UNDEFINED = 0,
+  BN_DATA = 1,
+  BN_OBJECT = 2,
+  BN_UINT8 = 110,
+  BN_FLOAT32 = 180,
+  BN_FLOAT32_VEC4 = 183,
+  BN_FLOAT = BN_FLOAT32,
+  BN_FLOAT4 = BN_FLOAT32_VEC4,
+  BN_UFIXED8 = 300,
+  BN_UFIXED8_RGBA = 301,
+  BN_UFIXED8_RGBA_SRGB = 302,
+  BN_UFIXED16 = 303,
+  /* storage forms with no reference counterpart (precision path) */
+  BNX_FLOAT16 = 1000,
+  BNX_BFLOAT16 = 1001
+} BNDataType;
+
+/* ---------------------------------------------------------------------- */
+/* context                                                                 */
+/* ---------------------------------------------------------------------- */
+
+/* replaces barney.cu:58 bnContextCreate. Exactly one data group and at most
+   one GPU; gpuIDs may be NULL (device 0). */
+BN_API BNContext bnContextCreate(int numDataGroupsOnThisContext, const int *dataRanksInDataGroup,
+                                 int numGPUs, const int *gpuIDs);
+/* replaces barney.cu bnContextDestroy: frees every object of the context */
+BN_API void bnContextDestroy(BNContext context);
+/* replaces barney.cu bnPhysicalDeviceCount */
+BN_API int bnPhysicalDeviceCount(void);
+
+/* ---------------------------------------------------------------------- */
+/* object lifetime and parameters (barney.h "general set/commit")          */
+/* ---------------------------------------------------------------------- */
+/* replaces barney.cu bnRelease (Context.cpp:250-261): drops the app's reference */
+BN_API void bnRelease(BNObject object);
+/* replaces barney.cu bnAddReference */
+BN_API void bnAddReference(BNObject object);
+/* replaces barney.cu bnCommit (Object::commit) */
+BN_API void bnCommit(BNObject target);
+/* replace barney.cu bnSet{1,2,3,4}{i,f} (Object::set*) */
+BN_API void bnSet1i(BNObject target, const char *paramName, int value);
+BN_API void bnSet2i(BNObject target, const char *paramName, int x, int y);
+BN_API void bnSet3i(BNObject target, const char *paramName, int x, int y, int z);
+BN_API void bnSet4i(BNObject target, const char *paramName, int x, int y, int z, int w);
+BN_API void bnSet1f(BNObject target, const char *paramName, float value);
+BN_API void bnSet2f(BNObject target, const char *paramName, float x, float y);
+BN_API void bnSet3f(BNObject target, const char *paramName, float x, float y, float z);
+BN_API void bnSet4f(BNObject target, const char *paramName, float x, float y, float z, float w);
+/* replaces barney.cu bnSetObject (StructuredData::setObject "textureData") */
+BN_API void bnSetObject(BNObject target, const char *paramName, BNObject value);
+/* replaces barney.cu bnSetData (Group "lights", Group.cpp:50-51) */
+BN_API void bnSetData(BNObject target, const char *paramName, BNData value);
+
+/* ---------------------------------------------------------------------- */
+/* scene content                                                           */
+/* ---------------------------------------------------------------------- */
+/* replaces barney.cu bnDataCreate (BN_OBJECT arrays of lights) */
+BN_API BNData bnDataCreate(BNContext context, int whichSlot, BNDataType dataType, size_t numItems,
+                           const void *items);
+/* replaces barney.cu:223 bnTextureData3DCreate. texelFormat: BN_FLOAT32,
+   BN_UFIXED8 / BN_UINT8 (unorm, x/255), BNX_FLOAT16, BNX_BFLOAT16. texels may
+   be host or device memory; it is copied before return. */
+BN_API BNTextureData bnTextureData3DCreate(BNContext context, int whichSlot, BNDataType texelFormat,
+                                           int width, int height, int depth, const void *texels);
+/* replaces barney.cu:382 bnScalarFieldCreate; type must be "structured" */
+BN_API BNScalarField bnScalarFieldCreate(BNContext context, int whichSlot, const char *type);
+/* replaces barney.cu:457 bnVolumeCreate */
+BN_API BNVolume bnVolumeCreate(BNContext context, int whichSlot, BNScalarField sf);
+/* replaces barney.cu:442 bnVolumeSetXF (Volume::setXF, Volume.cpp:15-24) */
+BN_API void bnVolumeSetXF(BNVolume volume, bn_float2 domain, const bn_float4 *colorMap,
+                          int numColorMapValues, float densityAt1);
+/* replaces barney.cu bnLightCreate; type "directional" */
+BN_API BNLight bnLightCreate(BNContext context, int whichSlot, const char *type);
+/* replaces barney.cu:510 bnGroupCreate; numGeoms must be 0, numVolumes 1 */
+BN_API BNGroup bnGroupCreate(BNContext context, int whichSlot, BNGeom *geoms, int numGeoms,
+                             BNVolume *volumes, int numVolumes);
+/* replaces barney.cu bnGroupBuild (Group::build -> MCVolumeAccel::build):
+   macrocell ranges + majorants are built here */
+BN_API void bnGroupBuild(BNGroup group);
+/* replaces barney.cu bnModelCreate */
+BN_API BNModel bnModelCreate(BNContext ctx);
+/* replaces barney.cu bnSetInstances; one group, transform NULL or identity */
+BN_API void bnSetInstances(BNModel model, int whichSlot, BNGroup *groups, BNTransform *xfms,
+                           int numInstances);
+/* replaces barney.cu:542 bnBuild */
+BN_API void bnBuild(BNModel model, int whichSlot);
+
+/* ---------------------------------------------------------------------- */
+/* camera, renderer, frame buffer                                          */
+/* ---------------------------------------------------------------------- */
+/* replaces barney.cu bnCameraCreate; type "perspective" (or "pinhole") */
+BN_API BNCamera bnCameraCreate(BNContext context, const char *type);
+/* replaces barney.cu bnRendererCreate; type "default" / "pathTracer" */
+BN_API BNRenderer bnRendererCreate(BNContext ctx, const char *type);
+/* replaces barney.cu bnFrameBufferCreate */
+BN_API BNFrameBuffer bnFrameBufferCreate(BNContext context, int deprecated);
+/* replaces barney.cu bnFrameBufferResize (FrameBuffer::resize); colorFormat
+   BN_FLOAT4, BN_UFIXED8_RGBA or BN_UFIXED8_RGBA_SRGB. Resets accumulation. */
+BN_API void bnFrameBufferResize(BNFrameBuffer fb, BNDataType colorFormat, int sizeX, int sizeY,
+                                uint32_t requiredChannels);
+/* replaces barney.cu:696 bnFrameBufferRead (FrameBuffer::read); BN_FB_COLOR
+   only; pointer may be host or device memory */
+BN_API void bnFrameBufferRead(BNFrameBuffer fb, BNFrameBufferChannel channelToRead,
+                              void *pointerToReadDataInto, BNDataType requiredFormat);
+/* replaces barney.cu bnFrameBufferGetSize */
+BN_API void bnFrameBufferGetSize(BNFrameBuffer fb, int *sizeX, int *sizeY);
+/* replaces barney.cu:721 bnAccumReset */
+BN_API void bnAccumReset(BNFrameBuffer fb);
+/* replaces barney.cu:727 bnRender (Context::renderTiles, Context.cpp:139-182):
+   renders renderer.pathsPerPixel waves and resolves the colour channel */
+BN_API void bnRender(BNRenderer renderer, BNModel model, BNCamera camera, BNFrameBuffer fb);
+
+/* ---------------------------------------------------------------------- */
+/* errors (no reference counterpart: the reference throws)                 */
+/* ---------------------------------------------------------------------- */
+BN_API int bnGetLastError(void);
+BN_API const char *bnGetLastErrorString(void);
+BN_API void bnClearLastError(void);
+
+/* ---------------------------------------------------------------------- */
+/* bnx: extensions with no reference counterpart                           */
+/* ---------------------------------------------------------------------- */
+/* Work done by the last bnRender / batch on this context and the device
+   time of its render kernel. */
+typedef struct {
+  unsigned long long samples;       /* volume samples (sampleAndMap calls) */
+  unsigned long long mcVisits;      /* macrocells whose majorant was read */
+  unsigned long long rays;          /* primary + shadow rays traced */
+  unsigned long long pixelSamples;  /* pixels x waves */
+  unsigned long long errorFlags;    /* iteration caps hit, aborts */
+  float renderMs;                   /* device time of the render kernel(s) */
+  float resolveMs;                  /* device time of the resolve kernel */
+} BNXStats;
+BN_API void bnxGetStats(BNContext context, BNXStats *stats);
+/* Launch all work of the context on this CUDA stream (cudaStream_t); NULL
+   selects the context's own stream. */
+BN_API void bnxSetStream(BNContext context, void *cudaStream);
+BN_API void *bnxGetStream(BNContext context);
+/* Launch parameters of the render kernel (0 = automatic). */
+BN_API void bnxSetLaunchConfig(BNContext context, int blocksPerSM, int threadsPerBlock);
+/* Device pointer of the resolved colour channel of a frame buffer. */
+BN_API void *bnxFrameBufferDevicePointer(BNFrameBuffer fb);
+/* Device copies of the macrocell grid of a volume after bnGroupBuild:
+   ranges (2 floats per cell) and majorants (1 float per cell), x fastest. */
+BN_API void bnxVolumeGetMacrocells(BNVolume volume, int *dims3, float *rangesHostOut,
+                                   float *majorantsHostOut);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* BN_VOLUME_H */

@@ -1,0 +1,894 @@
+// bn_oracle.cpp -- TEST INFRASTRUCTURE ONLY.
+//
+// CPU restatement of Barney's structured-volume path-tracing hot path, used
+// as the parity checker for the CUDA implementation in barney_b200/.  Only
+// tests/, __graft_entry__.smoke() and bench.py's cpu_baseline / reference
+// legs may load this library; the product never links or calls it.
+//
+// Parity status: the reference cannot be compiled here (its owl, cuBQL,
+// embree and optix submodules are empty and the ANARI SDK is absent) and its
+// own tests hold no golden vectors for this path, so this restatement is
+// "parity unpinned" against reference outputs.  It is pinned instead against
+// (a) hand-derived known-answer values written into tests/test_oracle_kat.py
+// and (b) the committed fixtures under tests/golden/, generated from this
+// file by tests/golden/make_golden.py.
+//
+// Arithmetic convention: every expression is evaluated in IEEE-754 binary32
+// in the order the reference source writes it, with no FMA contraction
+// (built with -ffp-contract=off).  Division and sqrt are correctly rounded.
+//
+// Reference files followed (paths relative to the Barney source tree):
+//   barney/native/common/barney-common.h:21-108   RNGSeed, Random2, hash
+//   barney/native/common/math.h:13-18,61-128      constants, sRGB, make_rgba, clamp
+//   barney/native/Camera.cu:82-100                perspective camera commit
+//   barney/native/kernels/generateRays.cu:43-244  primary ray generation
+//   barney/native/kernels/traceRays.dev.cu:26-52  zero-direction fix-up
+//   barney/native/render/Ray.h:111-217            setVolumeHit, makeShadowRay, boxTest
+//   barney/native/volume/MCAccelerator.h:552-689  MCVolumeAccel::isProg
+//   barney/native/volume/DDA.h:61-201             dda3
+//   barney/native/volume/Volume.h:62-74,154-203   sampleAndMap, fastLog, Woodcock
+//   barney/native/volume/StructuredData.h:101-112 structured sampler
+//   barney/rtcore/cpu/Texture.cpp:193-276,324-416 software point / linear filtering
+//   barney/native/volume/TransferFunction.h:68-117 map, majorant
+//   barney/native/volume/StructuredData.cu:26-96  macrocell range build
+//   barney/native/volume/MCGrid.cu:97-141         mapMCs
+//   barney/native/kernels/shadeRays.cu:17-402,475-1042 light sampling, bounce, accumulate
+//   barney/native/packedBSDF/Phase.h:14-176       HGPhase, SimplePhase
+//   barney/native/render/DG.h:183-193             randomDirection
+//   barney/native/light/EnvMap.h:136-151          constant-env pdf
+//   barney/native/light/DirLight.cu:11-20         directional light device data
+//   barney/native/fb/TiledFB.cu:13-52, LocalFB.cpp:61-71 resolve / tonemap
+//   barney/rtcore/cpu/Float16.cpp:25+             float -> half, round to nearest even
+//   barney/rtcore/cpu/Compute.cpp:17-80           job-per-block thread pool (CPU baseline)
+
+#include <atomic>
+#include <chrono>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <limits>
+#include <thread>
+#include <vector>
+
+namespace orc {
+
+// ---------------------------------------------------------------------------
+// small vector math (owl::common semantics restated from their meaning)
+// ---------------------------------------------------------------------------
+struct vec3f { float x, y, z; };
+struct vec4f { float x, y, z, w; };
+struct vec3i { int x, y, z; };
+
+static const float INF = std::numeric_limits<float>::infinity();
+// math.h:13-18
+static const float ONE_PI = (float)M_PI;
+static const float TWO_PI = 2.f * ONE_PI;
+static const float FOUR_PI = 4.f * ONE_PI;
+static const float ONE_OVER_FOUR_PI = 1.f / FOUR_PI;
+
+static inline float fmin_(float a, float b) { return a < b ? a : b; }
+static inline float fmax_(float a, float b) { return b < a ? a : b; }
+static inline vec3f V(float x, float y, float z) { return {x, y, z}; }
+static inline vec3f V(float s) { return {s, s, s}; }
+static inline vec3f operator+(vec3f a, vec3f b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
+static inline vec3f operator-(vec3f a, vec3f b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+static inline vec3f operator*(vec3f a, vec3f b) { return {a.x * b.x, a.y * b.y, a.z * b.z}; }
+static inline vec3f operator*(float s, vec3f b) { return {s * b.x, s * b.y, s * b.z}; }
+static inline vec3f operator*(vec3f a, float s) { return {a.x * s, a.y * s, a.z * s}; }
+static inline vec3f operator/(vec3f a, float s) { return {a.x / s, a.y / s, a.z / s}; }
+static inline vec3f operator-(vec3f a) { return {-a.x, -a.y, -a.z}; }
+static inline vec3f rcp(vec3f a) { return {1.f / a.x, 1.f / a.y, 1.f / a.z}; }
+static inline vec3f vmin(vec3f a, vec3f b) { return {fmin_(a.x, b.x), fmin_(a.y, b.y), fmin_(a.z, b.z)}; }
+static inline vec3f vmax(vec3f a, vec3f b) { return {fmax_(a.x, b.x), fmax_(a.y, b.y), fmax_(a.z, b.z)}; }
+static inline vec3f vabs(vec3f a) { return {fabsf(a.x), fabsf(a.y), fabsf(a.z)}; }
+static inline vec3f vfloor(vec3f a) { return {floorf(a.x), floorf(a.y), floorf(a.z)}; }
+static inline float reduce_max(vec3f a) { return fmax_(fmax_(a.x, a.y), a.z); }
+static inline float reduce_min(vec3f a) { return fmin_(fmin_(a.x, a.y), a.z); }
+static inline float dot(vec3f a, vec3f b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+static inline vec3f cross(vec3f a, vec3f b) {
+  return {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
+}
+static inline vec3f normalize(vec3f v) { return v * (1.f / sqrtf(dot(v, v))); }
+static inline bool isZero(vec3f v) { return v.x == 0.f && v.y == 0.f && v.z == 0.f; }
+static inline float clampf(float f, float lo, float hi) { return fmin_(hi, fmax_(lo, f)); }  // math.h:127
+static inline int clampi(int f, int lo, int hi) { return std::min(hi, std::max(lo, f)); }
+static inline uint32_t floatBits(float f) { uint32_t u; memcpy(&u, &f, 4); return u; }
+
+// float -> IEEE binary16, round to nearest even (the conversion Float16.cpp:25
+// and __float2half_rn both perform), and back.
+static inline uint16_t f2h(float f) {
+  uint32_t x = floatBits(f);
+  uint32_t sign = (x >> 16) & 0x8000u;
+  uint32_t ax = x & 0x7fffffffu;
+  if (ax >= 0x7f800000u) return (uint16_t)(sign | 0x7c00u | (ax > 0x7f800000u ? 0x200u : 0u));
+  if (ax >= 0x477ff000u) return (uint16_t)(sign | 0x7c00u);  // rounds to >= 65520 -> inf
+  if (ax < 0x38800000u) {                                     // result is subnormal or zero
+    if (ax < 0x33000000u) return (uint16_t)sign;              // < 2^-25 -> zero
+    uint32_t e = ax >> 23;
+    uint32_t m = (ax & 0x7fffffu) | 0x800000u;
+    uint32_t shift = 126u - e;                                // 14..24
+    uint32_t q = m >> shift;
+    uint32_t rem = m & ((1u << shift) - 1u);
+    uint32_t half = 1u << (shift - 1u);
+    if (rem > half || (rem == half && (q & 1u))) q++;
+    return (uint16_t)(sign | q);
+  }
+  uint32_t e = (ax >> 23) - 112u;  // rebias 127 -> 15
+  uint32_t m = ax & 0x7fffffu;
+  uint32_t q = (e << 10) | (m >> 13);
+  uint32_t rem = m & 0x1fffu;
+  if (rem > 0x1000u || (rem == 0x1000u && (q & 1u))) q++;
+  return (uint16_t)(sign | q);
+}
+static inline float h2f(uint16_t h) {
+  uint32_t sign = (uint32_t)(h & 0x8000u) << 16;
+  uint32_t e = (h >> 10) & 0x1fu, m = h & 0x3ffu, out;
+  if (e == 0) {
+    if (m == 0) out = sign;
+    else { float f = (float)m * (1.f / 16777216.f); uint32_t b = floatBits(f); out = sign | b; }
+  } else if (e == 31) out = sign | 0x7f800000u | (m << 13);
+  else out = sign | ((e + 112u) << 23) | (m << 13);
+  float r; memcpy(&r, &out, 4); return r;
+}
+static inline float bf2f(uint16_t h) { uint32_t u = (uint32_t)h << 16; float r; memcpy(&r, &u, 4); return r; }
+static inline vec3f halfRound(vec3f v) { return {h2f(f2h(v.x)), h2f(f2h(v.y)), h2f(f2h(v.z))}; }
+
+// ---------------------------------------------------------------------------
+// RNG and hash -- barney-common.h:21-108
+// ---------------------------------------------------------------------------
+struct RNGSeed {
+  uint64_t state = 0xcafef00dd15ea5e5ull;
+  void seed(uint32_t a, uint32_t b) {
+    state ^= (uint32_t)(2u * a + 1u);
+    next();
+    state ^= (uint32_t)(2u * b);
+    next();
+  }
+  uint32_t next() {
+    uint64_t x = state;
+    const uint64_t multiplier = 6364136223846793005ull;
+    unsigned count = (unsigned)(x >> 61);
+    state = x * multiplier;
+    x ^= x >> 22;
+    return (uint32_t)(x >> (22 + count));
+  }
+  uint32_t nextHashed(uint64_t h) { state ^= (h << 1); return next(); }
+};
+struct Random2 : RNGSeed {
+  Random2(uint32_t a, uint32_t b) { seed(a, b); }
+  Random2(RNGSeed &s, uint64_t b) { state = s.state; s.next(); nextHashed(b ? b : 290374ull); }
+  float operator()() { return (next() & 0x00FFFFFFu) * (1.f / (float)0x01000000); }
+};
+static inline uint64_t hash1(uint32_t v) { return 0xcbf29ce484222325ULL ^ (0x100000001b3ULL * v); }
+static inline uint64_t hash2(uint64_t h, uint32_t v) { return h * 0x100000001b3ULL ^ v; }
+static inline uint64_t hash3(uint32_t a, uint32_t b, uint32_t c) { return hash2(hash2(hash1(a), b), c); }
+
+// Volume.h:154-164
+static inline float fastLog(float f) {
+  f = (f - 1.f) / (f + 1.f);
+  float f2 = f * f;
+  float s = f;
+  f *= f2;
+  s += (1.f / 3.f) * f;
+  f *= f2;
+  s += (1.f / 5.f) * f;
+  return s + s;
+}
+
+} // namespace orc
+
+using namespace orc;
+
+// ---------------------------------------------------------------------------
+// scene description shared with the Python harness (oracle/__init__.py)
+// ---------------------------------------------------------------------------
+extern "C" {
+typedef struct {
+  const void *voxels;
+  int dtype;              // 0 f32, 1 u8 unorm (/255), 2 f16, 3 bf16
+  int dims[3];
+  float origin[3];
+  float spacing[3];
+  const float *tf;        // tfN x rgba
+  int tfN;
+  float domain[2];
+  float baseDensity;
+  float camPos[3], camDir[3], camUp[3];
+  float fovy;
+  float bgColor[4];
+  float ambientRadiance;
+  float cutPlane[4];
+  int numDirLights;
+  const float *dirLights; // per light: direction xyz, radiance, color rgb
+  int phaseMode;          // 0 SimplePhase(0.7*rgb) (default build); 1 HGPhase (multi-scatter build)
+  float anisotropy;
+  float scatteringAlbedo;
+  int emissionAbsorption; // 1: collision contributes TF rgb, no shadow ray (extension)
+  int exactLog;           // 1: -logf instead of fastLog (extension)
+  int majorantRoundUp;    // 1: majorant bumped one ulp up (precision forms)
+  int width, height;
+} OrcScene;
+
+typedef struct {
+  unsigned long long samples;      // sampleAndMap calls
+  unsigned long long mcVisits;     // DDA cells whose majorant was read
+  unsigned long long rays;         // rays traced (primary + shadow)
+  unsigned long long pixelSamples;
+} OrcStats;
+}
+
+namespace orc {
+
+struct Scene {
+  const OrcScene &s;
+  vec3i numScalars, numCells, mcDims;
+  vec3f gridOrigin, gridSpacing, mcOrigin, mcSpacing;
+  vec3f boundsLo, boundsHi;
+  std::vector<float> majorants;
+  // camera DD, Camera.cu:82-100
+  vec3f dir00, dirdu, dirdv, lens00;
+  explicit Scene(const OrcScene &s) : s(s) {}
+};
+
+// rtcore/cpu/Texture.cpp:193-225 (float, uchar); f16 / bf16 are the
+// precision-form extensions (no reference counterpart).
+static inline float texel(const OrcScene &s, int64_t idx) {
+  switch (s.dtype) {
+  case 0: return ((const float *)s.voxels)[idx];
+  case 1: { float v = (float)((const uint8_t *)s.voxels)[idx]; return v * 1.f / 255.f; }
+  case 2: return h2f(((const uint16_t *)s.voxels)[idx]);
+  default: return bf2f(((const uint16_t *)s.voxels)[idx]);
+  }
+}
+
+// Texture.cpp:324-336
+static inline void lerpCoords(int &i0, int &i1, float &f, int N, float tc) {
+  if (tc - .5f <= 0.f) { i0 = i1 = 0; f = 0.f; return; }
+  if (tc - .5f >= N - 1) { i0 = i1 = N - 1; f = 0.f; return; }
+  f = (tc - .5f) - int(tc - .5f);
+  i0 = int(tc - .5f);
+  i1 = i0 + 1;
+}
+static inline float lerp_l(float f, float a, float b) { return (1.f - f) * a + f * b; }
+
+// Texture.cpp:339-411, LINEAR filter, unnormalized coordinates, clamp
+static float tex3DLinear(const OrcScene &s, float tx, float ty, float tz) {
+  const int Nx = s.dims[0], Ny = s.dims[1], Nz = s.dims[2];
+  int ix0, ix1, iy0, iy1, iz0, iz1;
+  float fx, fy, fz;
+  lerpCoords(ix0, ix1, fx, Nx, tx);
+  lerpCoords(iy0, iy1, fy, Ny, ty);
+  lerpCoords(iz0, iz1, fz, Nz, tz);
+  auto addr = [&](int x, int y, int z) { return (int64_t)x + (int64_t)Nx * ((int64_t)y + (int64_t)Ny * z); };
+  float v000 = texel(s, addr(ix0, iy0, iz0));
+  float v001 = texel(s, addr(ix1, iy0, iz0));
+  float v010 = texel(s, addr(ix0, iy1, iz0));
+  float v011 = texel(s, addr(ix1, iy1, iz0));
+  float v100 = texel(s, addr(ix0, iy0, iz1));
+  float v101 = texel(s, addr(ix1, iy0, iz1));
+  float v110 = texel(s, addr(ix0, iy1, iz1));
+  float v111 = texel(s, addr(ix1, iy1, iz1));
+  float v00 = lerp_l(fx, v000, v001);
+  float v01 = lerp_l(fx, v010, v011);
+  float v10 = lerp_l(fx, v100, v101);
+  float v11 = lerp_l(fx, v110, v111);
+  float v0 = lerp_l(fy, v00, v01);
+  float v1 = lerp_l(fy, v10, v11);
+  return lerp_l(fz, v0, v1);
+}
+
+// StructuredData.h:101-112
+static float sampleField(const Scene &sc, vec3f P) {
+  vec3f rel = (P - sc.gridOrigin) * rcp(sc.gridSpacing);
+  if (rel.x < 0.f) return NAN;
+  if (rel.y < 0.f) return NAN;
+  if (rel.z < 0.f) return NAN;
+  if (rel.x >= sc.numCells.x) return NAN;
+  if (rel.y >= sc.numCells.y) return NAN;
+  if (rel.z >= sc.numCells.z) return NAN;
+  return tex3DLinear(sc.s, rel.x + .5f, rel.y + .5f, rel.z + .5f);
+}
+
+static inline vec4f tfValue(const OrcScene &s, int i) {
+  return {s.tf[4 * i + 0], s.tf[4 * i + 1], s.tf[4 * i + 2], s.tf[4 * i + 3]};
+}
+
+// TransferFunction.h:68-87
+static vec4f tfMap(const OrcScene &s, float v) {
+  float span = s.domain[1] - s.domain[0];
+  float f = (v - s.domain[0]) / span;
+  f = clampf(f, 0.f, 1.f);
+  f *= (s.tfN - 1);
+  int idx = clampi(int(f), 0, s.tfN - 2);
+  f -= idx;
+  vec4f v0 = tfValue(s, idx), v1 = tfValue(s, idx + 1);
+  vec4f r = {(1.f - f) * v0.x + f * v1.x, (1.f - f) * v0.y + f * v1.y,
+             (1.f - f) * v0.z + f * v1.z, (1.f - f) * v0.w + f * v1.w};
+  r.w *= s.baseDensity;
+  return r;
+}
+
+// TransferFunction.h:93-117
+static float tfMajorant(const OrcScene &s, float lo, float hi) {
+  if (lo > hi) return 0.f;
+  float span = s.domain[1] - s.domain[0];
+  float f_lo = (lo - s.domain[0]) / span;
+  float f_hi = (hi - s.domain[0]) / span;
+  f_lo = clampf(f_lo, 0.f, 1.f);
+  f_hi = clampf(f_hi, 0.f, 1.f);
+  f_lo *= (s.tfN - 1);
+  f_hi *= (s.tfN - 1);
+  int idx0_lo = clampi(int(f_lo), 0, s.tfN - 2);
+  int idx0_hi = clampi(int(f_hi), 0, s.tfN - 2);
+  f_lo -= idx0_lo;
+  f_hi -= idx0_hi;
+  float lerp_lo = (1.f - f_lo) * s.tf[4 * idx0_lo + 3] + f_lo * s.tf[4 * (idx0_lo + 1) + 3];
+  float lerp_hi = (1.f - f_hi) * s.tf[4 * idx0_hi + 3] + f_hi * s.tf[4 * (idx0_hi + 1) + 3];
+  float m = 0.f;
+  m = fmax_(m, lerp_lo);
+  m = fmax_(m, lerp_hi);
+  for (int i = idx0_lo + 1; i <= idx0_hi; i++) m = fmax_(m, s.tf[4 * i + 3]);
+  return m * s.baseDensity;
+}
+
+// Volume.h:62-74 (principled branch is not part of this path)
+static inline vec4f sampleAndMap(const Scene &sc, vec3f P) {
+  float f = sampleField(sc, P);
+  if (std::isnan(f)) return {0.f, 0.f, 0.f, 0.f};
+  return tfMap(sc.s, f);
+}
+
+// StructuredData.cu:31-62, cellsPerMC = 8, NEAREST fetch at integer coords
+static void buildRanges(const OrcScene &s, vec3i mcDims, float *out) {
+  const int64_t n = (int64_t)mcDims.x * mcDims.y * mcDims.z;
+  for (int64_t tid = 0; tid < n; tid++) {
+    vec3i mc = {(int)(tid % mcDims.x), (int)((tid / mcDims.x) % mcDims.y), (int)(tid / ((int64_t)mcDims.x * mcDims.y))};
+    float lo = INF, hi = -INF;  // owl interval<float> default = empty
+    for (int iiz = 0; iiz <= 8; iiz++)
+      for (int iiy = 0; iiy <= 8; iiy++)
+        for (int iix = 0; iix <= 8; iix++) {
+          int x = mc.x * 8 + iix, y = mc.y * 8 + iiy, z = mc.z * 8 + iiz;
+          if (x >= s.dims[0] || y >= s.dims[1] || z >= s.dims[2]) continue;
+          float f = texel(s, (int64_t)x + (int64_t)s.dims[0] * ((int64_t)y + (int64_t)s.dims[1] * z));
+          lo = fmin_(lo, f);
+          hi = fmax_(hi, f);
+        }
+    out[2 * tid + 0] = lo;
+    out[2 * tid + 1] = hi;
+  }
+}
+
+static void setupScene(Scene &sc) {
+  const OrcScene &s = sc.s;
+  sc.numScalars = {s.dims[0], s.dims[1], s.dims[2]};
+  sc.numCells = {s.dims[0] - 1, s.dims[1] - 1, s.dims[2] - 1};       // StructuredData.cu:146-150
+  sc.gridOrigin = V(s.origin[0], s.origin[1], s.origin[2]);
+  sc.gridSpacing = V(s.spacing[0], s.spacing[1], s.spacing[2]);
+  sc.boundsLo = sc.gridOrigin;                                        // :177-181
+  sc.boundsHi = sc.gridOrigin + sc.gridSpacing * V((float)sc.numCells.x, (float)sc.numCells.y, (float)sc.numCells.z);
+  sc.mcDims = {(sc.numCells.x + 7) / 8, (sc.numCells.y + 7) / 8, (sc.numCells.z + 7) / 8};  // :74
+  sc.mcOrigin = sc.boundsLo;                                          // :76
+  sc.mcSpacing = V(8.f) * sc.gridSpacing;                             // :77
+  int64_t n = (int64_t)sc.mcDims.x * sc.mcDims.y * sc.mcDims.z;
+  std::vector<float> ranges(2 * n);
+  buildRanges(s, sc.mcDims, ranges.data());
+  sc.majorants.resize(n);
+  for (int64_t i = 0; i < n; i++) {                                   // MCGrid.cu:97-113
+    float m = tfMajorant(s, ranges[2 * i], ranges[2 * i + 1]);
+    if (s.majorantRoundUp && m > 0.f) m = nextafterf(m, INF);
+    sc.majorants[i] = m;
+  }
+  // Camera.cu:63-101: "direction" is normalized on set, again on commit
+  vec3f direction = normalize(V(s.camDir[0], s.camDir[1], s.camDir[2]));
+  vec3f up = V(s.camUp[0], s.camUp[1], s.camUp[2]);
+  vec3f dir00 = normalize(direction);
+  vec3f dirdu = normalize(cross(dir00, up));
+  vec3f dirdv = normalize(cross(dirdu, dir00));
+  dir00 = dir00 * (float)(1.f / (2.0f * tanf((0.5f * s.fovy) * (float)M_PI / 180.0f)));
+  sc.dir00 = dir00; sc.dirdu = dirdu; sc.dirdv = dirdv;
+  sc.lens00 = V(s.camPos[0], s.camPos[1], s.camPos[2]);
+}
+
+// Ray.h:170-181
+static inline bool boxTest(vec3f org, vec3f dir, float &t0, float &t1, vec3f lo, vec3f hi) {
+  vec3f t_lo = (lo - org) * rcp(dir);
+  vec3f t_hi = (hi - org) * rcp(dir);
+  vec3f t_nr = vmin(t_lo, t_hi);
+  vec3f t_fr = vmax(t_lo, t_hi);
+  t0 = fmax_(t0, reduce_max(t_nr));
+  t1 = fmin_(t1, reduce_min(t_fr));
+  return t0 <= t1;
+}
+
+// DDA.h:61-201
+template <typename Lambda>
+static void dda3(vec3f org, vec3f dir, float tMax, vec3i gridSize, const Lambda &lambda) {
+  const vec3f rcp_dir = rcp(dir);
+  const vec3f f_size = V((float)gridSize.x, (float)gridSize.y, (float)gridSize.z);
+  vec3f t_lo = (V(0.f) - org) * rcp(dir);
+  vec3f t_hi = (f_size - org) * rcp(dir);
+  vec3f t_nr = vmin(t_lo, t_hi);
+  vec3f t_fr = vmax(t_lo, t_hi);
+  if (dir.x == 0.f) { if (org.x < 0.f || org.x > f_size.x) return; t_nr.x = -INF; t_fr.x = +INF; }
+  if (dir.y == 0.f) { if (org.y < 0.f || org.y > f_size.y) return; t_nr.y = -INF; t_fr.y = +INF; }
+  if (dir.z == 0.f) { if (org.z < 0.f || org.z > f_size.z) return; t_nr.z = -INF; t_fr.z = +INF; }
+  float ray_t0 = fmax_(0.f, reduce_max(t_nr));
+  float ray_t1 = fmin_(tMax, reduce_min(t_fr));
+  if (ray_t0 > ray_t1) return;
+  vec3f org_in_volume = org + ray_t0 * dir;
+  vec3f f_cell = vmax(V(0.f), vmin(f_size - V(1.f), vfloor(org_in_volume)));
+  vec3f f_cell_end = {dir.x > 0.f ? f_cell.x + 1.f : f_cell.x,
+                      dir.y > 0.f ? f_cell.y + 1.f : f_cell.y,
+                      dir.z > 0.f ? f_cell.z + 1.f : f_cell.z};
+  vec3f t_step = vabs(rcp_dir);
+  vec3f t_next = {(dir.x == 0.f) ? INF : (fabsf(f_cell_end.x - org_in_volume.x) * t_step.x),
+                  (dir.y == 0.f) ? INF : (fabsf(f_cell_end.y - org_in_volume.y) * t_step.y),
+                  (dir.z == 0.f) ? INF : (fabsf(f_cell_end.z - org_in_volume.z) * t_step.z)};
+  const vec3i stop = {dir.x > 0.f ? gridSize.x : -1, dir.y > 0.f ? gridSize.y : -1, dir.z > 0.f ? gridSize.z : -1};
+  const vec3i cell_delta = {dir.x > 0.f ? +1 : -1, dir.y > 0.f ? +1 : -1, dir.z > 0.f ? +1 : -1};
+  vec3i cell = {(int)f_cell.x, (int)f_cell.y, (int)f_cell.z};
+  float next_cell_begin = 0.f;
+  while (1) {
+    float t_closest = reduce_min(t_next);
+    const float cell_t0 = ray_t0 + next_cell_begin;
+    const float cell_t1 = ray_t0 + fmin_(t_closest, tMax);
+    if (!lambda(cell, cell_t0, cell_t1)) return;
+    next_cell_begin = t_closest;
+    if (t_next.x == t_closest) { t_next.x += t_step.x; cell.x += cell_delta.x; if (cell.x == stop.x) return; }
+    if (t_next.y == t_closest) { t_next.y += t_step.y; cell.y += cell_delta.y; if (cell.y == stop.y) return; }
+    if (t_next.z == t_closest) { t_next.z += t_step.z; cell.z += cell_delta.z; if (cell.z == stop.z) return; }
+  }
+}
+
+struct Ray {
+  vec3f org, dir;
+  float tMax;
+  RNGSeed rngSeed;
+  bool hadHit = false;
+  vec3f P;
+  vec3f hitColor;  // TF rgb at the collision (phase tint)
+};
+
+struct LocalStats { uint64_t samples = 0, mcVisits = 0, rays = 0; };
+
+// Woodcock::sampleRange, Volume.h:168-203
+static bool woodcock(vec4f &sample, const Scene &sc, vec3f org, vec3f dir, float t_lower, float &t_upper,
+                     float majorant, Random2 &rand, LocalStats &st) {
+  float t = t_lower;
+  while (true) {
+    float r = rand();
+    float dt = sc.s.exactLog ? (-logf(1.f - r) / majorant) : (-fastLog(1.f - r) / majorant);
+    t += dt;
+    if (t >= t_upper) return false;
+    vec3f P = org + t * dir;
+    sample = sampleAndMap(sc, P);
+    st.samples++;
+    if (sample.w >= rand() * majorant) { t_upper = t; return true; }
+  }
+}
+
+// TraceRays::run (traceRays.dev.cu:26-52) + MCVolumeAccel::isProg
+// (MCAccelerator.h:552-689) for one identity-instanced structured volume.
+static void traceRay(const Scene &sc, Ray &ray, LocalStats &st) {
+  st.rays++;
+  vec3f dir = ray.dir;
+  if (dir.x == 0.f) dir.x = 1e-6f;
+  if (dir.y == 0.f) dir.y = 1e-6f;
+  if (dir.z == 0.f) dir.z = 1e-6f;
+  const vec3f obj_org = ray.org, obj_dir = dir;
+  float t0 = 0.f, t1 = ray.tMax;
+  if (!boxTest(obj_org, obj_dir, t0, t1, sc.boundsLo, sc.boundsHi)) return;
+  vec3f dda_org = (obj_org - sc.mcOrigin) * rcp(sc.mcSpacing);
+  vec3f dda_dir = obj_dir * rcp(sc.mcSpacing);
+  Random2 rng(ray.rngSeed, hash3(0, 0, 0));
+  dda3(dda_org, dda_dir, t1, sc.mcDims, [&](const vec3i &c, float ct0, float ct1) -> bool {
+    const float majorant = sc.majorants[(int64_t)c.x + (int64_t)sc.mcDims.x * ((int64_t)c.y + (int64_t)sc.mcDims.y * c.z)];
+    st.mcVisits++;
+    if (majorant == 0.f) return true;
+    vec4f sample = {0, 0, 0, 0};
+    float upper = fmin_(ct1, ray.tMax);
+    if (!woodcock(sample, sc, obj_org, obj_dir, ct0, upper, majorant, rng, st)) return true;
+    vec3f P = obj_org + upper * obj_dir;
+    ray.hadHit = true;           // Ray::setVolumeHit -> setHit (Ray.h:101-144)
+    ray.P = P;
+    ray.tMax = upper;
+    ray.hitColor = V(sample.x, sample.y, sample.z);
+    return false;
+  });
+}
+
+struct PixelSample {
+  // gen-0 contribution
+  vec3f frag0; float alpha0;
+  // gen-1 (shadow ray) contribution, valid if hasShadow
+  bool hasShadow; vec3f frag1;
+};
+
+struct LightSample { vec3f direction, radiance; float distance; float pdf = 0.f; };
+
+// DG.h:183-193
+static vec3f randomDirection(Random2 &rng) {
+  vec3f v;
+  while (true) {
+    v.x = 1.f - 2.f * rng();
+    v.y = 1.f - 2.f * rng();
+    v.z = 1.f - 2.f * rng();
+    if (dot(v, v) <= 1.f) return normalize(v);
+  }
+}
+
+// Phase.h:51-58
+static inline float hgPhase(float g, float cosTheta) {
+  if (fabsf(g) < 1e-3f) return ONE_OVER_FOUR_PI;
+  float g2 = g * g;
+  float denom = 1.f + g2 - 2.f * g * cosTheta;
+  return ONE_OVER_FOUR_PI * (1.f - g2) / (denom * sqrtf(denom));
+}
+
+// shadeRays.cu:294-402 for the lights this path has: the constant
+// environment (renderer.ambientRadiance, no env-map texture) and
+// directional lights.  N is the zero vector for volume hits.
+static bool sampleLights(const Scene &sc, LightSample &ls, Random2 &random, bool &lightNeedsMIS,
+                         bool &lightIsDirLight) {
+  const OrcScene &s = sc.s;
+  lightNeedsMIS = false;
+  // sampleEnvLight :266-291 (N == 0 branch)
+  LightSample els;
+  els.direction = randomDirection(random);
+  els.distance = INF;
+  els.radiance = V(FOUR_PI * s.ambientRadiance);
+  els.pdf = ONE_OVER_FOUR_PI;
+  float elsWeight = reduce_max(els.radiance);
+  // sampleAreaLights: none on this path -> false, no random numbers
+  float alsWeight = 0.f;
+  // sampleDirLights :139-189
+  LightSample dls;
+  float dlsWeight = 0.f;
+  if (s.numDirLights > 0) {
+    const int RES = 2;
+    int lID[RES];
+    float weights[RES];
+    float sumW = 0.f;
+    bool ok = true;
+    for (int i = 0; i < RES; i++) {
+      lID[i] = std::min(int(random() * s.numDirLights), s.numDirLights - 1);
+      weights[i] = 0.f;
+      const float *L = s.dirLights + 7 * lID[i];
+      vec3f rad = V(L[4], L[5], L[6]) * L[3];
+      float weight = 1.f;  // N == 0
+      if (weight <= 1e-3f) continue;
+      weight *= reduce_max(rad);
+      if (weight <= 1e-3f) continue;
+      weights[i] = weight;
+      sumW += weight;
+    }
+    if (sumW == 0.f) ok = false;
+    if (ok) {
+      float r = random() * sumW;
+      int i = 0;
+      while (i < RES && r >= weights[i]) { r -= weights[i]; ++i; }
+      if (i == RES) ok = false;
+      else {
+        const float *L = s.dirLights + 7 * lID[i];
+        // DirLight.cu:11-20: direction normalized (identity instance)
+        vec3f ldir = normalize(V(L[0], L[1], L[2]));
+        dls.direction = -ldir;
+        dls.distance = INF;
+        dls.radiance = V(L[4], L[5], L[6]) * L[3] * 1.f / (weights[i] / sumW * (float(RES) / float(s.numDirLights)));
+        dls.pdf = INF;
+        ok = weights[i] != 0.f;
+      }
+    }
+    dlsWeight = ok ? reduce_max(dls.radiance) : 0.f;
+  }
+  float plsWeight = 0.f;
+  float sumWeights = alsWeight + dlsWeight + elsWeight + plsWeight;
+  if (sumWeights == 0.f) return false;
+  elsWeight *= 1.f / sumWeights;
+  alsWeight *= 1.f / sumWeights;
+  dlsWeight *= 1.f / sumWeights;
+  plsWeight *= 1.f / sumWeights;
+  float r = random();
+  if (r <= alsWeight) {
+    ls = LightSample();  // area-light sample of an empty light list: pdf 0
+  } else if (r <= alsWeight + elsWeight) {
+    ls = els;
+    ls.radiance = ls.radiance * (1.f / elsWeight);
+    lightNeedsMIS = true;
+  } else if (r <= alsWeight + elsWeight + plsWeight) {
+    ls = LightSample();
+  } else {
+    if (dlsWeight == 0.f) return false;  // no directional sample exists
+    ls = dls;
+    ls.radiance = ls.radiance * (1.f / dlsWeight);
+    lightIsDirLight = true;
+  }
+  if (std::isnan(ls.pdf) || (ls.pdf <= 0.f)) return false;
+  return true;
+}
+
+// one wave for one pixel: generateRays.cu:43-244, trace, bounce()
+// (shadeRays.cu:475-880) for generation 0, trace of the shadow ray,
+// bounce() for generation 1.
+static PixelSample renderPixelSample(const Scene &sc, int ix, int iy, int accumID, LocalStats &st) {
+  const OrcScene &s = sc.s;
+  const int W = s.width, H = s.height;
+  PixelSample out{};
+  Ray ray;
+  Random2 rand(unsigned(ix + W * accumID), unsigned(iy + H * accumID));
+  ray.rngSeed.seed(ix + accumID * W, iy);
+  float pixel_u = ((accumID == 0) ? .5f : rand());
+  float pixel_v = ((accumID == 0) ? .5f : rand());
+  float image_u = ((ix + pixel_u) / float(W));
+  float image_v = ((iy + pixel_v) / float(H));
+  float aspect = W / float(H);
+  ray.org = sc.lens00;
+  vec3f ray_dir = sc.dir00 + (1.f * aspect * (image_u - .5f)) * sc.dirdu + (1.f * (image_v - .5f)) * sc.dirdv;
+  ray.dir = normalize(ray_dir);
+  ray.tMax = 1e30f;
+  if (s.cutPlane[3] > -1e28f) {
+    vec3f N = V(s.cutPlane[0], s.cutPlane[1], s.cutPlane[2]);
+    float d_plane = s.cutPlane[3];
+    float dist_org = dot(N, ray.org) + d_plane;
+    float denom = dot(N, ray.dir);
+    if (dist_org >= 0.f) {
+      if (denom < 0.f) { float t_cut = -dist_org / denom; ray.tMax = fmin_(ray.tMax, t_cut); }
+    } else {
+      if (denom > 0.f) { float t_entry = -dist_org / denom; ray.org = ray.org + t_entry * ray.dir; }
+      else ray.tMax = 0.f;
+    }
+  }
+  const float t = (iy + .5f) / float(H);
+  vec4f bg;
+  if (s.bgColor[3] >= 0.f) bg = {s.bgColor[0], s.bgColor[1], s.bgColor[2], s.bgColor[3]};
+  else bg = {(1.0f - t) * 0.9f + t * 0.15f, (1.0f - t) * 0.9f + t * 0.25f, (1.0f - t) * 0.9f + t * .8f, (1.0f - t) * 1.f + t * 1.f};
+
+  traceRay(sc, ray, st);
+
+  // ---- generation 0: bounce() on the primary ray
+  if (!ray.hadHit) {
+    out.frag0 = V(bg.x, bg.y, bg.z);
+    out.alpha0 = bg.w;
+    out.hasShadow = false;
+    return out;
+  }
+  out.frag0 = V(0.f);
+  out.alpha0 = 1.f;
+  out.hasShadow = false;
+  if (s.emissionAbsorption) {  // extension: collision estimator of emission
+    out.frag0 = ray.hitColor;
+    return out;
+  }
+  Random2 random(ray.rngSeed, (uint64_t)floatBits(ray.tMax));
+  vec3f P = ray.P;
+  vec3f wo = -normalize(ray.dir);
+  const float offsetEpsilon = fmax_(1e-4f, 1e-6f * reduce_max(vabs(P)));  // safe_eps
+  LightSample ls;
+  bool lightNeedsMIS = false, lightIsDirLight = false;
+  if (!sampleLights(sc, ls, random, lightNeedsMIS, lightIsDirLight)) return out;
+  // bsdf.eval (Phase.h:68-73 / 148-154)
+  vec3f albedo;
+  float fpdf;
+  if (s.phaseMode == 0) {
+    albedo = .7f * ray.hitColor;
+    fpdf = ONE_OVER_FOUR_PI;
+  } else {
+    albedo = s.scatteringAlbedo * ray.hitColor;
+    vec3f wi_in = normalize(-wo);
+    fpdf = hgPhase(s.anisotropy, dot(wi_in, normalize(ls.direction)));
+  }
+  vec3f fval = fpdf * albedo;
+  if (!(fpdf > 0.f) || reduce_max(fval) < 1e-4f) return out;
+  fval = vmin(fval, V(13.f));
+  const vec3f incomingThroughput = V(1.f);
+  vec3f tp_sr = incomingThroughput * (std::isinf(ls.pdf) ? 1.f : (1.f / ls.pdf)) * fval * ls.radiance * 1.f;
+  Ray shadow;
+  shadow.org = P + offsetEpsilon * wo;
+  shadow.dir = ls.direction;
+  shadow.tMax = ls.distance * (1.f - 2.f * offsetEpsilon);
+  vec3f shadowTp = halfRound(tp_sr);  // PathState::throughput is vec3h
+  shadow.rngSeed = ray.rngSeed;
+  float misWeight = 1.f;
+  if (!lightIsDirLight && lightNeedsMIS) {
+    float pdf_light = ONE_OVER_FOUR_PI;  // EnvMap.h:142-151, no texture
+    float pdf_scatter;
+    if (s.phaseMode == 0) pdf_scatter = ONE_OVER_FOUR_PI;
+    else pdf_scatter = hgPhase(s.anisotropy, dot(normalize(-wo), normalize(ls.direction)));
+    misWeight = pdf_light / (pdf_light + pdf_scatter + 1e-10f);
+    if (misWeight < 1e-5f) return out;
+  }
+  if (!(shadow.tMax > 0.f)) return out;
+  // ---- generation 1: trace the shadow ray, bounce() on it
+  traceRay(sc, shadow, st);
+  out.hasShadow = true;
+  out.frag1 = shadow.hadHit ? V(0.f) : (misWeight * shadowTp);
+  return out;
+}
+
+// _shadeRays accumulation, shadeRays.cu:996-1040
+static inline void accumulate(vec4f &acc, const PixelSample &ps, int accumID) {
+  float clampMax = 10.f * (1 + accumID);
+  vec3f f0 = vmin(ps.frag0, V(clampMax));
+  if (accumID == 0) {
+    acc = {f0.x, f0.y, f0.z, ps.alpha0};
+  } else {
+    if (ps.alpha0 > 0.f) acc.w += ps.alpha0;
+    if (f0.x > 0.f) acc.x += f0.x;
+    if (f0.y > 0.f) acc.y += f0.y;
+    if (f0.z > 0.f) acc.z += f0.z;
+  }
+  if (ps.hasShadow) {
+    vec3f f1 = vmin(ps.frag1, V(clampMax));
+    if (f1.x > 0.f) acc.x += f1.x;
+    if (f1.y > 0.f) acc.y += f1.y;
+    if (f1.z > 0.f) acc.z += f1.z;
+  }
+}
+
+} // namespace orc
+
+extern "C" {
+
+uint32_t orc_version() { return 1; }
+
+// RNG known-answer helpers
+void orc_rng_stream(uint32_t a, uint32_t b, int n, uint32_t *out) {
+  Random2 r(a, b);
+  for (int i = 0; i < n; i++) out[i] = r.next();
+}
+void orc_rng_floats(uint32_t a, uint32_t b, int n, float *out) {
+  Random2 r(a, b);
+  for (int i = 0; i < n; i++) out[i] = r();
+}
+// Random2(seed, h) derived stream; returns the advanced parent state in *parentOut
+void orc_rng_derived(uint64_t parentState, uint64_t h, int n, uint32_t *out, uint64_t *parentOut) {
+  RNGSeed p;
+  p.state = parentState;
+  Random2 r(p, h);
+  for (int i = 0; i < n; i++) out[i] = r.next();
+  *parentOut = p.state;
+}
+uint64_t orc_hash3(uint32_t a, uint32_t b, uint32_t c) { return hash3(a, b, c); }
+float orc_fastlog(float f) { return fastLog(f); }
+uint16_t orc_f2h(float f) { return f2h(f); }
+float orc_h2f(uint16_t h) { return h2f(h); }
+
+void orc_mc_dims(const OrcScene *s, int *out3) {
+  out3[0] = (s->dims[0] - 1 + 7) / 8;
+  out3[1] = (s->dims[1] - 1 + 7) / 8;
+  out3[2] = (s->dims[2] - 1 + 7) / 8;
+}
+void orc_build_ranges(const OrcScene *s, float *out) {
+  vec3i d = {(s->dims[0] - 1 + 7) / 8, (s->dims[1] - 1 + 7) / 8, (s->dims[2] - 1 + 7) / 8};
+  buildRanges(*s, d, out);
+}
+void orc_map_majorants(const OrcScene *s, const float *ranges, int64_t n, float *out) {
+  for (int64_t i = 0; i < n; i++) {
+    float m = tfMajorant(*s, ranges[2 * i], ranges[2 * i + 1]);
+    if (s->majorantRoundUp && m > 0.f) m = nextafterf(m, INF);
+    out[i] = m;
+  }
+}
+void orc_sample_points(const OrcScene *s, int n, const float *P, float *outScalar, float *outRGBA) {
+  Scene sc(*s);
+  sc.numScalars = {s->dims[0], s->dims[1], s->dims[2]};
+  sc.numCells = {s->dims[0] - 1, s->dims[1] - 1, s->dims[2] - 1};
+  sc.gridOrigin = V(s->origin[0], s->origin[1], s->origin[2]);
+  sc.gridSpacing = V(s->spacing[0], s->spacing[1], s->spacing[2]);
+  for (int i = 0; i < n; i++) {
+    vec3f p = V(P[3 * i], P[3 * i + 1], P[3 * i + 2]);
+    outScalar[i] = sampleField(sc, p);
+    vec4f m = sampleAndMap(sc, p);
+    outRGBA[4 * i + 0] = m.x; outRGBA[4 * i + 1] = m.y; outRGBA[4 * i + 2] = m.z; outRGBA[4 * i + 3] = m.w;
+  }
+}
+void orc_tf_map(const OrcScene *s, int n, const float *v, float *outRGBA) {
+  for (int i = 0; i < n; i++) {
+    vec4f m = tfMap(*s, v[i]);
+    outRGBA[4 * i + 0] = m.x; outRGBA[4 * i + 1] = m.y; outRGBA[4 * i + 2] = m.z; outRGBA[4 * i + 3] = m.w;
+  }
+}
+// DDA cell sequence for a grid-space ray; returns number of cells written (<= maxCells)
+int orc_dda_cells(const float *org, const float *dir, float tMax, const int *grid, int maxCells, int *outCells,
+                  float *outT) {
+  int n = 0;
+  dda3(V(org[0], org[1], org[2]), V(dir[0], dir[1], dir[2]), tMax, vec3i{grid[0], grid[1], grid[2]},
+       [&](const vec3i &c, float t0, float t1) -> bool {
+         if (n >= maxCells) return false;
+         outCells[3 * n] = c.x; outCells[3 * n + 1] = c.y; outCells[3 * n + 2] = c.z;
+         outT[2 * n] = t0; outT[2 * n + 1] = t1;
+         n++;
+         return true;
+       });
+  return n;
+}
+
+// Primary-ray trace for one pixel: writes hit flag, t, rgb.
+void orc_trace_primary(const OrcScene *s, int ix, int iy, int accumID, int *hit, float *t, float *rgb) {
+  Scene sc(*s);
+  setupScene(sc);
+  LocalStats st;
+  const int W = s->width, H = s->height;
+  Ray ray;
+  Random2 rand(unsigned(ix + W * accumID), unsigned(iy + H * accumID));
+  ray.rngSeed.seed(ix + accumID * W, iy);
+  float pixel_u = ((accumID == 0) ? .5f : rand());
+  float pixel_v = ((accumID == 0) ? .5f : rand());
+  float image_u = ((ix + pixel_u) / float(W));
+  float image_v = ((iy + pixel_v) / float(H));
+  float aspect = W / float(H);
+  ray.org = sc.lens00;
+  ray.dir = normalize(sc.dir00 + (1.f * aspect * (image_u - .5f)) * sc.dirdu + (1.f * (image_v - .5f)) * sc.dirdv);
+  ray.tMax = 1e30f;
+  traceRay(sc, ray, st);
+  *hit = ray.hadHit;
+  *t = ray.tMax;
+  rgb[0] = ray.hitColor.x; rgb[1] = ray.hitColor.y; rgb[2] = ray.hitColor.z;
+}
+
+// Render waves accumID0 .. accumID0+spp-1 over the pixel rectangle
+// [x0,x1) x [y0,y1), accumulating into accum (width*height float4, linear).
+// Rows are handed out to numThreads workers (Compute.cpp:17-80 scheme).
+// Returns wall seconds spent.
+double orc_render(const OrcScene *s, int accumID0, int spp, float *accum, int x0, int y0, int x1, int y1,
+                  int numThreads, OrcStats *stats) {
+  auto tStart = std::chrono::steady_clock::now();
+  Scene sc(*s);
+  setupScene(sc);
+  if (numThreads <= 0) numThreads = (int)std::thread::hardware_concurrency();
+  std::atomic<int> nextRow{y0};
+  std::vector<LocalStats> perThread(numThreads);
+  auto worker = [&](int tid) {
+    LocalStats &st = perThread[tid];
+    while (true) {
+      int iy = nextRow++;
+      if (iy >= y1) break;
+      for (int ix = x0; ix < x1; ix++) {
+        vec4f *accp = (vec4f *)(accum + 4 * ((int64_t)iy * s->width + ix));
+        vec4f acc = *accp;
+        for (int k = 0; k < spp; k++) {
+          int accumID = accumID0 + k;
+          PixelSample ps = renderPixelSample(sc, ix, iy, accumID, st);
+          accumulate(acc, ps, accumID);
+        }
+        *accp = acc;
+      }
+    }
+  };
+  std::vector<std::thread> threads;
+  for (int i = 0; i < numThreads; i++) threads.emplace_back(worker, i);
+  for (auto &t : threads) t.join();
+  if (stats) {
+    OrcStats tot{0, 0, 0, 0};
+    for (auto &p : perThread) { tot.samples += p.samples; tot.mcVisits += p.mcVisits; tot.rays += p.rays; }
+    tot.pixelSamples = (unsigned long long)(x1 - x0) * (y1 - y0) * spp;
+    *stats = tot;
+  }
+  return std::chrono::duration<double>(std::chrono::steady_clock::now() - tStart).count();
+}
+
+// math.h:61-66
+static inline float linear_to_srgb(float x) {
+  if (x <= 0.0031308f) return 12.92f * x;
+  return 1.055f * powf(x, 1.f / 2.4f) - 0.055f;
+}
+static inline uint32_t make_8bit(float f) { return (uint32_t)std::min(255, std::max(0, int(f * 256.f))); }
+
+// TiledFB.cu:13-52 with accumScale = 1/accumID (LocalFB.cpp:65).
+// fmt: 0 float4, 1 rgba8, 2 rgba8 sRGB
+void orc_resolve(const float *accum, int64_t numPixels, int accumID, int fmt, void *out) {
+  float accumScale = 1.f / accumID;
+  for (int64_t i = 0; i < numPixels; i++) {
+    vec4f c = {accum[4 * i] * accumScale, accum[4 * i + 1] * accumScale, accum[4 * i + 2] * accumScale,
+               accum[4 * i + 3] * accumScale};
+    if (fmt == 0) {
+      float *o = (float *)out + 4 * i;
+      o[0] = c.x; o[1] = c.y; o[2] = c.z; o[3] = c.w;
+    } else {
+      if (fmt == 2) { c.x = linear_to_srgb(c.x); c.y = linear_to_srgb(c.y); c.z = linear_to_srgb(c.z); }
+      ((uint32_t *)out)[i] = (make_8bit(c.x) << 0) + (make_8bit(c.y) << 8) + (make_8bit(c.z) << 16) + (make_8bit(c.w) << 24);
+    }
+  }
+}
+
+} // extern "C"

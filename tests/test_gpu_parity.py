@@ -1,0 +1,127 @@
+"""Parity of the CUDA path (through the bn* C ABI) with the CPU oracle.
+
+Bar: bit-exact.  Macrocell ranges and majorants, every accumulated float4
+pixel, the work counters (volume samples, macrocell visits, rays) and the
+rgba8 frames must be identical; the sRGB frame may differ by one 8-bit step
+where powf of the two math libraries rounds differently (tolerance 1).
+"""
+import numpy as np
+import pytest
+
+import oracle
+from barney_b200 import synth
+from tests.helpers import (assert_bitexact, gpu_render, oracle_render, small_blob_scene,
+                           small_noise_scene)
+
+pytestmark = pytest.mark.gpu
+
+
+def _bn():
+    import barney_b200 as bn
+    return bn
+
+
+@pytest.mark.parametrize("dtype", ["f32", "u8", "f16", "bf16"])
+@pytest.mark.parametrize("shape", [(33, 40, 17), (64, 64, 64), (2, 2, 2), (9, 9, 9), (3, 70, 5)])
+def test_macrocells_bitexact(dtype, shape):
+    rng = np.random.default_rng(hash((dtype, shape)) & 0xFFFF)
+    vol = synth.to_storage(rng.random(shape).astype(np.float32), dtype)
+    d = synth.scene(vol, dtype, 8, 8, synth.tf_knots(256, 1), 50.0, synth.DEFAULT_CAMERA)
+    for round_up in (False, True):
+        d["majorant_round_up"] = round_up
+        r = _bn().VolumeRenderer(d)
+        ranges, maj = r.macrocells()
+        r.close()
+        sc = oracle.Scene(d)
+        o_ranges = oracle.build_ranges(sc)
+        o_maj = oracle.map_majorants(sc, o_ranges)
+        assert_bitexact(ranges, o_ranges, "ranges")
+        assert_bitexact(maj, o_maj, "majorants")
+
+
+SCENES = {
+    "blobs_ambient": lambda: small_blob_scene(),
+    "blobs_emission_absorption": lambda: small_blob_scene(emission_absorption=True, ambient=0.0),
+    "noise_hg_dirlight": lambda: small_noise_scene(),
+    "noise_simple_dirlight": lambda: small_noise_scene(phase="simple"),
+    "noise_u8": lambda: small_noise_scene(dtype="u8"),
+    "noise_f16": lambda: small_noise_scene(dtype="f16"),
+    "noise_bf16": lambda: small_noise_scene(dtype="bf16"),
+    "two_lights_aniso": lambda: small_noise_scene(
+        dir_lights=[{"direction": (-1, -1, -1), "radiance": 1.0},
+                    {"direction": (0.3, -1, 0.2), "radiance": 2.0, "color": (1.0, 0.5, 0.25)}],
+        anisotropy=0.5),
+    "gradient_bg_cutplane": lambda: small_blob_scene(bg_color=(0, 0, 0, -1), cut_plane=(1.0, 0.0, 0.0, -0.5)),
+    "camera_inside": lambda: small_blob_scene(camera=synth.look_at((0.5, 0.5, 0.45), (0.5, 0.5, 1.0), fovy=70)),
+    "axis_aligned_view": lambda: small_blob_scene(w=41, h=41, camera={"position": (0.5, 0.5, -2.0), "direction": (0.0, 0.0, 1.0),
+                                                         "up": (0.0, 1.0, 0.0), "fovy": 30.0}),
+    "ragged_volume": lambda: synth.scene(synth.blobs(20, 0)[:, 3:17, 1:20].copy(), "f32", 37, 29,
+                                         synth.tf_linear_ramp(64), 30.0, synth.DEFAULT_CAMERA,
+                                         spacing=(1 / 18.0, 1 / 13.0, 1 / 19.0)),
+}
+
+
+@pytest.mark.parametrize("name", sorted(SCENES))
+def test_render_bitexact(name):
+    d = SCENES[name]()
+    for spp in (1, 5):
+        img, st = gpu_render(d, spp)
+        ref, _, ost = oracle_render(d, spp)
+        assert_bitexact(img, ref, f"{name} spp={spp}")
+        assert st["samples"] == ost["samples"]
+        assert st["mc_visits"] == ost["mc_visits"]
+        assert st["rays"] == ost["rays"]
+        assert st["error_flags"] == 0
+
+
+def test_accumulation_across_renders():
+    d = small_noise_scene(w=32, h=24)
+    img, _ = gpu_render(d, 2, renders=3)  # accumIDs 0..5 over three bnRender calls
+    ref, _, _ = oracle_render(d, 6)
+    assert_bitexact(img, ref, "3 x 2 waves")
+
+
+@pytest.mark.parametrize("fmt", ["rgba8", "rgba8_srgb"])
+def test_color_formats(fmt):
+    d = small_blob_scene()
+    img, _ = gpu_render(d, 3, fmt=fmt)
+    ref, _, _ = oracle_render(d, 3, fmt=fmt)
+    if fmt == "rgba8":
+        assert_bitexact(img, ref, fmt)
+    else:
+        a = img.view(np.uint8).astype(int)
+        b = ref.view(np.uint8).astype(int)
+        assert np.abs(a - b).max() <= 1
+
+
+def test_deterministic_and_launch_shape_invariant():
+    bn = _bn()
+    d = small_noise_scene(n=48, w=64, h=40)
+    r = bn.VolumeRenderer(d)
+    r.set_spp(3)
+    r.render()
+    a = r.read().copy()
+    for bps, tpb in [(1, 32), (2, 64), (0, 256)]:
+        r.accum_reset()
+        r.set_launch_config(bps, tpb)
+        r.render()
+        assert_bitexact(r.read(), a, f"launch {bps}x{tpb}")
+    r.close()
+
+
+def test_invalid_calls_record_errors():
+    bn = _bn()
+    d = small_blob_scene()
+    r = bn.VolumeRenderer(d)
+    L = r.L
+    L.bnClearLastError()
+    L.bnFrameBufferRead(r.fb, 1, np.zeros(4, np.uint32).ctypes.data, bn.BN_UFIXED8_RGBA)  # wrong format
+    assert L.bnGetLastError() != 0
+    L.bnClearLastError()
+    L.bnSet1i(r.renderer, b"maxVolumeBounces", 3)
+    L.bnSet1i(r.renderer, b"bnx.hgPhase", 1)
+    L.bnCommit(r.renderer)
+    L.bnRender(r.renderer, r.model, r.camera, r.fb)
+    assert L.bnGetLastError() == 3  # unsupported: multiple scattering
+    L.bnClearLastError()
+    r.close()

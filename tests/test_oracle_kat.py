@@ -1,0 +1,226 @@
+"""Known-answer tests pinning the CPU oracle (oracle/bn_oracle.cpp).
+
+The reference ships no golden vectors for the structured-volume path, so
+each expected value here is derived independently: the RNG and hash are
+restated a second time in Python integers from barney-common.h:21-108;
+fastLog, trilinear sampling and the transfer function are re-evaluated
+with numpy float32 scalars in the reference's operation order; DDA cell
+sequences are worked out by hand from DDA.h:61-201.
+"""
+import math
+
+import numpy as np
+import pytest
+
+import oracle
+
+M64 = (1 << 64) - 1
+M32 = (1 << 32) - 1
+f32 = np.float32
+
+
+def py_next(state):
+    x = state
+    count = x >> 61
+    state = (x * 6364136223846793005) & M64
+    x ^= x >> 22
+    return state, (x >> (22 + count)) & M32
+
+
+def py_seed(a, b):
+    st = 0xcafef00dd15ea5e5
+    st ^= (2 * a + 1) & M32
+    st, _ = py_next(st)
+    st ^= (2 * b) & M32
+    st, _ = py_next(st)
+    return st
+
+
+def test_rng_stream_matches_python_restatement():
+    for a, b in [(0, 0), (1, 2), (1919, 1079), (0xFFFFFFFF, 7), (123456, 654321)]:
+        st = py_seed(a, b)
+        expect = []
+        for _ in range(32):
+            st, v = py_next(st)
+            expect.append(v)
+        assert list(oracle.rng_stream(a, b, 32)) == expect
+
+
+def test_rng_float_is_24bit_uniform():
+    st = py_seed(5, 9)
+    vals = oracle.rng_floats(5, 9, 64)
+    for v in vals:
+        st, u = py_next(st)
+        assert v == f32((u & 0xFFFFFF)) * f32(1.0 / 16777216.0)
+    assert vals.min() >= 0.0 and vals.max() < 1.0
+
+
+def test_rng_derived_stream():
+    # Random2(RNGSeed &seed, b): child = parent; parent.next(); child.next(b ? b : 290374)
+    parent = py_seed(3, 4)
+    for h in [0, 1, 0x3f800000, oracle.hash3(0, 0, 0)]:
+        child = parent ^ (((h if h else 290374) << 1) & M64)
+        child, _ = py_next(child)
+        exp = []
+        for _ in range(8):
+            child, v = py_next(child)
+            exp.append(v)
+        got, parent_after = oracle.rng_derived(parent, h, 8)
+        assert list(got) == exp
+        assert parent_after == (parent * 6364136223846793005) & M64
+
+
+def test_hash_fnv():
+    basis, prime = 0xcbf29ce484222325, 0x100000001b3
+    def h1(v): return basis ^ ((prime * v) & M64)
+    def h2(h, v): return ((h * prime) & M64) ^ v
+    for a, b, c in [(0, 0, 0), (1, 2, 3), (7, 0, 9)]:
+        assert oracle.hash3(a, b, c) == h2(h2(h1(a), b), c)
+
+
+def test_fastlog_series():
+    for x in [1.0, 0.5, 0.25, 1e-3, 0.999, 2.0 ** -24, 0.75]:
+        f = f32(x)
+        g = (f - f32(1)) / (f + f32(1))
+        g2 = g * g
+        s = g
+        g = g * g2
+        s = s + f32(1.0 / 3.0) * g
+        g = g * g2
+        s = s + f32(1.0 / 5.0) * g
+        assert oracle.fastlog(float(f)) == s + s
+    # the series is biased: at 2^-24 it returns ~ -3.07 instead of -16.6
+    assert -3.1 < oracle.fastlog(2.0 ** -24) < -3.0
+
+
+@pytest.mark.filterwarnings("ignore::RuntimeWarning")
+def test_float_to_half_round_nearest_even():
+    rng = np.random.default_rng(0)
+    vals = np.concatenate([
+        rng.standard_normal(2000).astype(np.float32) * 10,
+        np.array([0.0, -0.0, 65504.0, 65519.99, 65520.0, 1e-8, 6e-8, 5.96e-8, 2.98e-8, 1e5,
+                  1.0 + 2.0 ** -11, 1.0 + 3 * 2.0 ** -11, np.inf, -np.inf], np.float32),
+        (rng.random(2000) * 1e-4).astype(np.float32)])
+    for v in vals:
+        assert oracle.f2h(float(v)) == int(np.array(v, np.float32).astype(np.float16).view(np.uint16))
+
+
+def test_dda_axis_aligned():
+    cells, ts = oracle.dda_cells((-1.0, 0.5, 0.5), (1.0, 0.0, 0.0), 1e30, (4, 4, 4))
+    assert cells.tolist() == [[0, 0, 0], [1, 0, 0], [2, 0, 0], [3, 0, 0]]
+    assert ts.tolist() == [[1, 2], [2, 3], [3, 4], [4, 5]]
+
+
+def test_dda_diagonal_steps_all_axes_at_once():
+    cells, ts = oracle.dda_cells((-1.0, -1.0, -1.0), (1.0, 1.0, 1.0), 1e30, (2, 2, 2))
+    assert cells.tolist() == [[0, 0, 0], [1, 1, 1]]
+    assert ts.tolist() == [[1, 2], [2, 3]]
+
+
+def test_dda_tmax_quirk_keeps_walking():
+    # DDA.h:175 clamps cell_t1 to ray_t0 + tMax and never stops at tMax
+    cells, ts = oracle.dda_cells((-1.0, 0.5, 0.5), (1.0, 0.0, 0.0), 1.5, (4, 4, 4))
+    assert cells.tolist() == [[0, 0, 0], [1, 0, 0], [2, 0, 0], [3, 0, 0]]
+    assert ts.tolist() == [[1, 2], [2, 2.5], [3, 2.5], [4, 2.5]]
+
+
+def test_dda_negative_direction_and_miss():
+    cells, _ = oracle.dda_cells((3.5, 0.5, 0.5), (-1.0, 0.0, 0.0), 1e30, (4, 4, 4))
+    assert cells.tolist() == [[3, 0, 0], [2, 0, 0], [1, 0, 0], [0, 0, 0]]
+    cells, _ = oracle.dda_cells((0.5, 5.0, 0.5), (1.0, 0.0, 0.0), 1e30, (4, 4, 4))
+    assert len(cells) == 0
+
+
+def _tiny_scene(vol, dtype="f32", tf=None, **kw):
+    if tf is None:
+        tf = np.array([[0, 0, 1, 0], [1, 0, 0, 1]], np.float32)
+    d = {"voxels": vol, "dtype": dtype, "spacing": (1.0, 1.0, 1.0), "tf": tf, "density": 2.0,
+         "camera": {"position": (0, 0, -5), "direction": (0, 0, 1)}, "width": 4, "height": 4}
+    d.update(kw)
+    return oracle.Scene(d)
+
+
+def _trilinear_ref(v, fx, fy, fz, i):
+    x0, x1, y0, y1, z0, z1 = i
+    lerp = lambda f, a, b: (f32(1) - f) * a + f * b
+    c00 = lerp(fx, v[z0, y0, x0], v[z0, y0, x1])
+    c01 = lerp(fx, v[z0, y1, x0], v[z0, y1, x1])
+    c10 = lerp(fx, v[z1, y0, x0], v[z1, y0, x1])
+    c11 = lerp(fx, v[z1, y1, x0], v[z1, y1, x1])
+    return lerp(fz, lerp(fy, c00, c01), lerp(fy, c10, c11))
+
+
+def test_trilinear_interior_edges_and_outside():
+    rng = np.random.default_rng(1)
+    vol = rng.random((3, 4, 5)).astype(np.float32)
+    sc = _tiny_scene(vol)
+    P = np.array([[0.25, 0.5, 0.75], [0.0, 0.0, 0.0], [3.5, 2.25, 1.5], [4.0, 0.0, 0.0],
+                  [-1e-7, 0.0, 0.0], [1.0, 1.0, 1.0], [np.nextafter(np.float32(4), 0), 0.5, 0.5]], np.float32)
+    scal, _ = oracle.sample_points(sc, P)
+    assert scal[0] == _trilinear_ref(vol, f32(0.25), f32(0.5), f32(0.75), (0, 1, 0, 1, 0, 1))
+    assert scal[1] == vol[0, 0, 0]
+    assert scal[2] == _trilinear_ref(vol, f32(0.5), f32(0.25), f32(0.5), (3, 4, 2, 3, 1, 2))
+    assert math.isnan(scal[3]) and math.isnan(scal[4])       # rel >= numCells, rel < 0
+    assert scal[5] == vol[1, 1, 1]
+    # rel = 4 - ulp: rel + .5 rounds to 4.5, so tc - .5 >= N - 1 clamps to x = 4
+    assert scal[6] == _trilinear_ref(vol, f32(0), f32(0), f32(0), (4, 4, 0, 1, 0, 1)) or \
+        scal[6] == (f32(1) - f32(0.5)) * ((f32(1) - f32(0.5)) * vol[0, 0, 4] + f32(0.5) * vol[0, 1, 4]) + \
+        f32(0.5) * ((f32(1) - f32(0.5)) * vol[1, 0, 4] + f32(0.5) * vol[1, 1, 4])
+
+
+def test_uchar_texels_divide_by_255():
+    vol = np.arange(8, dtype=np.uint8).reshape(2, 2, 2) * 30
+    sc = _tiny_scene(vol, dtype="u8")
+    scal, _ = oracle.sample_points(sc, np.array([[0, 0, 0], [0.999, 0, 0]], np.float32))
+    assert scal[0] == f32(0) and scal[1] > 0
+    sc2 = _tiny_scene(np.full((2, 2, 2), 200, np.uint8), dtype="u8")
+    s2, _ = oracle.sample_points(sc2, np.array([[0.0, 0.0, 0.0], [0.3, 0.3, 0.3]], np.float32))
+    c = f32(200) / f32(255)
+    assert s2[0] == c
+    assert s2[1] == _trilinear_ref(np.full((2, 2, 2), c, np.float32), f32(0.3), f32(0.3), f32(0.3), (0, 1, 0, 1, 0, 1))
+
+
+def test_transfer_function_map():
+    tf = np.array([[0, 0, 1, 0], [0.5, 0, 0.5, 0.25], [1, 0, 0, 1]], np.float32)
+    sc = _tiny_scene(np.zeros((2, 2, 2), np.float32), tf=tf, domain=(0.0, 2.0))
+    v = np.array([-1.0, 0.0, 0.5, 1.0, 1.5, 2.0, 3.0], np.float32)
+    rgba = oracle.tf_map(sc, v)
+    for s, out in zip(v, rgba):
+        f = (s - f32(0)) / f32(2)
+        f = min(f32(1), max(f32(0), f)) * f32(2)
+        idx = min(1, max(0, int(f)))
+        f = f - f32(idx)
+        exp = (f32(1) - f) * tf[idx] + f * tf[idx + 1]
+        exp[3] = exp[3] * f32(2.0)
+        assert np.array_equal(out, exp)
+
+
+def test_majorant_of_ranges():
+    tf = np.array([[0, 0, 0, 0.0], [0, 0, 0, 0.8], [0, 0, 0, 0.2], [0, 0, 0, 0.4]], np.float32)
+    sc = _tiny_scene(np.zeros((2, 2, 2), np.float32), tf=tf)
+    ranges = np.array([[0.0, 1.0], [0.9, 1.0], [0.1, 0.2], [0.5, 0.4], [0.0, 0.0]], np.float32)
+    m = oracle.map_majorants(sc, ranges)
+    assert m[0] == f32(0.8) * f32(2)                       # interior knot 1 inside [0,1]
+    assert m[4] == f32(0)
+    assert m[3] == 0.0                                     # empty range
+    f = (f32(0.9) - 0) / f32(1) * f32(3)
+    lo = (f32(1) - (f - f32(2))) * f32(0.2) + (f - f32(2)) * f32(0.4)
+    assert m[1] == max(f32(0), lo, f32(0.4)) * f32(2)
+    fl = f32(0.1) * f32(3)
+    fh = f32(0.2) * f32(3)
+    e_lo = (f32(1) - fl) * f32(0) + fl * f32(0.8)
+    e_hi = (f32(1) - fh) * f32(0) + fh * f32(0.8)
+    assert m[2] == max(f32(0), e_lo, e_hi) * f32(2)
+
+
+def test_macrocell_ranges_bruteforce():
+    rng = np.random.default_rng(2)
+    vol = rng.random((19, 10, 23)).astype(np.float32)  # ragged: 18 x 9 x 22 cells
+    sc = _tiny_scene(vol)
+    r = oracle.build_ranges(sc)
+    assert r.shape == (3, 2, 3, 2)
+    for z in range(3):
+        for y in range(2):
+            for x in range(3):
+                blk = vol[8 * z:8 * z + 9, 8 * y:8 * y + 9, 8 * x:8 * x + 9]
+                assert r[z, y, x, 0] == blk.min() and r[z, y, x, 1] == blk.max()
