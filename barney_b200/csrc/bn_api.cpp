@@ -893,7 +893,8 @@ BN_API void *bnxGetStream(BNContext context) {
 BN_API void bnxSetLaunchConfig(BNContext context, int bps, int tpb) {
   BN_TRY
   Context *c = getContext(context);
-  if (tpb != 0 && (tpb % 32 != 0 || tpb > 1024 || tpb < 32)) throw Error(E_INVALID_ARG, "threadsPerBlock");
+  if (tpb != 0 && (tpb % 32 != 0 || tpb > kRenderMaxThreads || tpb < 32))
+    throw Error(E_INVALID_ARG, "threadsPerBlock must be a multiple of 32 in [32, 128]");
   c->blocksPerSM = bps < 0 ? 0 : bps;
   c->threadsPerBlock = tpb ? tpb : 128;
   BN_CATCH()

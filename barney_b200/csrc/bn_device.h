@@ -15,6 +15,7 @@ enum ErrorBits : unsigned { ERR_ITER_CAP = 1u, ERR_ABORTED = 2u };
 constexpr int kMaxDirLights = 16;
 constexpr int kMaxTF = 4096;
 constexpr int kCellsPerMC = 8;  // StructuredData.cu:26
+constexpr int kRenderMaxThreads = 128;  // __launch_bounds__ of the render kernel
 
 // Structured field + macrocell majorant grid + transfer function
 // (MCVolumeAccel::DD, MCAccelerator.h:23-27).

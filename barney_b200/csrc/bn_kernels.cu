@@ -416,7 +416,7 @@ DEV bool sampleLights(const FrameDD &fr, uint64_t &random, LightSample &ls, bool
 DEV float roundHalf(float x) { return __half2float(__float2half_rn(x)); }
 
 template <int T>
-__global__ void __launch_bounds__(128, 4) renderKernel(VolumeDD v, FrameDD fr, LaunchCounters *ctr) {
+__global__ void __launch_bounds__(kRenderMaxThreads, 4) renderKernel(VolumeDD v, FrameDD fr, LaunchCounters *ctr) {
   extern __shared__ float4 sTF[];
   __shared__ float u8lut[256];
   for (int i = threadIdx.x; i < v.tfN; i += blockDim.x) sTF[i] = v.tf[i];

@@ -74,3 +74,20 @@ def test_kernels_compiled_for_sm100a():
     assert render
     for b in render:
         assert "0 bytes spill stores" in b.splitlines()[1]
+
+
+def test_header_compiles_as_c_and_shim_as_cpp(tmp_path):
+    c_src = tmp_path / "client.c"
+    c_src.write_text('#include "bn_volume.h"\nint main(void){ BNXStats s; (void)s; '
+                     'return bnPhysicalDeviceCount() < 0; }\n')
+    subprocess.run(["gcc", "-std=c99", "-Wall", "-Werror", "-I", os.path.join(ROOT, "include"), "-c",
+                    str(c_src), "-o", str(tmp_path / "client.o")], check=True)
+    cpp_src = tmp_path / "client.cpp"
+    cpp_src.write_text('#include "barney_shim.hpp"\nint main(){ using namespace barney_cuda;\n'
+                       ' BNContext c = bnContextCreate(1, nullptr, 0, nullptr);\n'
+                       ' BNFrameBuffer fb = bnFrameBufferCreate(c); bnFrameBufferResize(fb, BN_UFIXED8_RGBA, 4, 4);\n'
+                       ' bn_float3 v{1,2,3}; bnSet(fb, "x", v); return 0; }\n')
+    lib_dir = os.path.dirname(bn.LIB_PATH)
+    subprocess.run(["g++", "-std=c++17", "-I", os.path.join(ROOT, "include"), str(cpp_src), "-L", lib_dir,
+                    "-lbarney_b200", "-Wl,-rpath," + lib_dir, "-o", str(tmp_path / "client")], check=True)
+    subprocess.run([str(tmp_path / "client")], check=True)

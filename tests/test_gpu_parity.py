@@ -101,7 +101,7 @@ def test_deterministic_and_launch_shape_invariant():
     r.set_spp(3)
     r.render()
     a = r.read().copy()
-    for bps, tpb in [(1, 32), (2, 64), (0, 256)]:
+    for bps, tpb in [(1, 32), (2, 64), (0, 128), (3, 96)]:
         r.accum_reset()
         r.set_launch_config(bps, tpb)
         r.render()
@@ -123,5 +123,8 @@ def test_invalid_calls_record_errors():
     L.bnCommit(r.renderer)
     L.bnRender(r.renderer, r.model, r.camera, r.fb)
     assert L.bnGetLastError() == 3  # unsupported: multiple scattering
+    L.bnClearLastError()
+    L.bnxSetLaunchConfig(r.ctx, 1, 256)  # beyond the kernel's launch bounds
+    assert L.bnGetLastError() == 2
     L.bnClearLastError()
     r.close()
