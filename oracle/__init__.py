@@ -49,6 +49,7 @@ class OrcScene(ctypes.Structure):
         ("emissionAbsorption", ctypes.c_int),
         ("exactLog", ctypes.c_int),
         ("majorantRoundUp", ctypes.c_int),
+        ("compensatedAccum", ctypes.c_int),
         ("width", ctypes.c_int),
         ("height", ctypes.c_int),
     ]
@@ -91,9 +92,9 @@ def lib():
         L.orc_dda_cells.argtypes = [P, P, F, P, I, P, P]
         L.orc_dda_cells.restype = I
         L.orc_trace_primary.argtypes = [P, I, I, I, P, P, P]
-        L.orc_render.argtypes = [P, I, I, P, I, I, I, I, I, P]
+        L.orc_render.argtypes = [P, I, I, P, P, I, I, I, I, I, P]
         L.orc_render.restype = D
-        L.orc_resolve.argtypes = [P, ctypes.c_int64, I, I, P]
+        L.orc_resolve.argtypes = [P, P, ctypes.c_int64, I, I, P]
         L.orc64_render_expected.argtypes = [P, I, I, I, I, D, I, I, I, P]
         _lib = L
     return _lib
@@ -141,6 +142,7 @@ class Scene:
         s.emissionAbsorption = int(desc.get("emission_absorption", False))
         s.exactLog = int(desc.get("exact_log", False))
         s.majorantRoundUp = int(desc.get("majorant_round_up", False))
+        s.compensatedAccum = int(desc.get("compensated_accum", False))
         s.width, s.height = desc["width"], desc["height"]
         self.s = s
 
@@ -225,26 +227,29 @@ def dda_cells(org, dir, tmax, grid, max_cells=4096):
     return cells[:n], ts[:n]
 
 
-def render(sc, accum_id0, spp, accum=None, rect=None, threads=0):
-    """Accumulate spp waves into a (H, W, 4) float32 buffer; returns (accum, seconds, stats)."""
+def render(sc, accum_id0, spp, accum=None, rect=None, threads=0, comp=None):
+    """Accumulate spp waves into a (H, W, 4) float32 buffer; returns (accum, seconds, stats).
+    comp: (H, W, 4) compensation buffer of the compensated-accumulation form."""
     W, H = sc.s.width, sc.s.height
     if accum is None:
         accum = np.zeros((H, W, 4), np.float32)
     x0, y0, x1, y1 = rect if rect is not None else (0, 0, W, H)
     st = OrcStats()
-    secs = lib().orc_render(sc.ref, accum_id0, spp, _ptr(accum), x0, y0, x1, y1, threads, ctypes.byref(st))
+    secs = lib().orc_render(sc.ref, accum_id0, spp, _ptr(accum), _ptr(comp) if comp is not None else None,
+                            x0, y0, x1, y1, threads, ctypes.byref(st))
     return accum, secs, {"samples": st.samples, "mc_visits": st.mcVisits, "rays": st.rays,
                          "pixel_samples": st.pixelSamples}
 
 
-def resolve(accum, accum_id, fmt="float4"):
+def resolve(accum, accum_id, fmt="float4", comp=None):
     code = {"float4": 0, "rgba8": 1, "rgba8_srgb": 2}[fmt]
     n = accum.shape[0] * accum.shape[1]
     if code == 0:
         out = np.zeros(accum.shape, np.float32)
     else:
         out = np.zeros(accum.shape[:2], np.uint32)
-    lib().orc_resolve(_ptr(np.ascontiguousarray(accum)), n, accum_id, code, _ptr(out))
+    cp = _ptr(np.ascontiguousarray(comp)) if comp is not None else None
+    lib().orc_resolve(_ptr(np.ascontiguousarray(accum)), cp, n, accum_id, code, _ptr(out))
     return out
 
 

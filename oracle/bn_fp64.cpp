@@ -33,33 +33,7 @@
 #include <thread>
 #include <vector>
 
-extern "C" {
-typedef struct {
-  const void *voxels;
-  int dtype;
-  int dims[3];
-  float origin[3];
-  float spacing[3];
-  const float *tf;
-  int tfN;
-  float domain[2];
-  float baseDensity;
-  float camPos[3], camDir[3], camUp[3];
-  float fovy;
-  float bgColor[4];
-  float ambientRadiance;
-  float cutPlane[4];
-  int numDirLights;
-  const float *dirLights;
-  int phaseMode;
-  float anisotropy;
-  float scatteringAlbedo;
-  int emissionAbsorption;
-  int exactLog;
-  int majorantRoundUp;
-  int width, height;
-} OrcScene;
-}
+#include "bn_oracle.h"
 
 namespace {
 

@@ -182,32 +182,9 @@ using namespace orc;
 // ---------------------------------------------------------------------------
 // scene description shared with the Python harness (oracle/__init__.py)
 // ---------------------------------------------------------------------------
+#include "bn_oracle.h"
+
 extern "C" {
-typedef struct {
-  const void *voxels;
-  int dtype;              // 0 f32, 1 u8 unorm (/255), 2 f16, 3 bf16
-  int dims[3];
-  float origin[3];
-  float spacing[3];
-  const float *tf;        // tfN x rgba
-  int tfN;
-  float domain[2];
-  float baseDensity;
-  float camPos[3], camDir[3], camUp[3];
-  float fovy;
-  float bgColor[4];
-  float ambientRadiance;
-  float cutPlane[4];
-  int numDirLights;
-  const float *dirLights; // per light: direction xyz, radiance, color rgb
-  int phaseMode;          // 0 SimplePhase(0.7*rgb) (default build); 1 HGPhase (multi-scatter build)
-  float anisotropy;
-  float scatteringAlbedo;
-  int emissionAbsorption; // 1: collision contributes TF rgb, no shadow ray (extension)
-  int exactLog;           // 1: -logf instead of fastLog (extension)
-  int majorantRoundUp;    // 1: majorant bumped one ulp up (precision forms)
-  int width, height;
-} OrcScene;
 
 typedef struct {
   unsigned long long samples;      // sampleAndMap calls
@@ -705,23 +682,37 @@ static PixelSample renderPixelSample(const Scene &sc, int ix, int iy, int accumI
   return out;
 }
 
-// _shadeRays accumulation, shadeRays.cu:996-1040
-static inline void accumulate(vec4f &acc, const PixelSample &ps, int accumID) {
+// Neumaier-compensated sum (precision forms): sum += x, error kept in c.
+static inline void neumaier(float &sum, float &c, float x) {
+  float t = sum + x;
+  if (fabsf(sum) >= fabsf(x)) c += (sum - t) + x;
+  else c += (x - t) + sum;
+  sum = t;
+}
+static inline void addTo(float &sum, float &c, float x, bool comp) {
+  if (comp) neumaier(sum, c, x);
+  else sum += x;
+}
+
+// _shadeRays accumulation, shadeRays.cu:996-1040.  With compensation the
+// positive adds go through neumaier() and comp holds the running error.
+static inline void accumulate(vec4f &acc, vec4f &comp, const PixelSample &ps, int accumID, bool compensated) {
   float clampMax = 10.f * (1 + accumID);
   vec3f f0 = vmin(ps.frag0, V(clampMax));
   if (accumID == 0) {
     acc = {f0.x, f0.y, f0.z, ps.alpha0};
+    comp = {0.f, 0.f, 0.f, 0.f};
   } else {
-    if (ps.alpha0 > 0.f) acc.w += ps.alpha0;
-    if (f0.x > 0.f) acc.x += f0.x;
-    if (f0.y > 0.f) acc.y += f0.y;
-    if (f0.z > 0.f) acc.z += f0.z;
+    if (ps.alpha0 > 0.f) addTo(acc.w, comp.w, ps.alpha0, compensated);
+    if (f0.x > 0.f) addTo(acc.x, comp.x, f0.x, compensated);
+    if (f0.y > 0.f) addTo(acc.y, comp.y, f0.y, compensated);
+    if (f0.z > 0.f) addTo(acc.z, comp.z, f0.z, compensated);
   }
   if (ps.hasShadow) {
     vec3f f1 = vmin(ps.frag1, V(clampMax));
-    if (f1.x > 0.f) acc.x += f1.x;
-    if (f1.y > 0.f) acc.y += f1.y;
-    if (f1.z > 0.f) acc.z += f1.z;
+    if (f1.x > 0.f) addTo(acc.x, comp.x, f1.x, compensated);
+    if (f1.y > 0.f) addTo(acc.y, comp.y, f1.y, compensated);
+    if (f1.z > 0.f) addTo(acc.z, comp.z, f1.z, compensated);
   }
 }
 
@@ -830,8 +821,8 @@ void orc_trace_primary(const OrcScene *s, int ix, int iy, int accumID, int *hit,
 // [x0,x1) x [y0,y1), accumulating into accum (width*height float4, linear).
 // Rows are handed out to numThreads workers (Compute.cpp:17-80 scheme).
 // Returns wall seconds spent.
-double orc_render(const OrcScene *s, int accumID0, int spp, float *accum, int x0, int y0, int x1, int y1,
-                  int numThreads, OrcStats *stats) {
+double orc_render(const OrcScene *s, int accumID0, int spp, float *accum, float *compBuf, int x0, int y0, int x1,
+                  int y1, int numThreads, OrcStats *stats) {
   auto tStart = std::chrono::steady_clock::now();
   Scene sc(*s);
   setupScene(sc);
@@ -844,14 +835,17 @@ double orc_render(const OrcScene *s, int accumID0, int spp, float *accum, int x0
       int iy = nextRow++;
       if (iy >= y1) break;
       for (int ix = x0; ix < x1; ix++) {
-        vec4f *accp = (vec4f *)(accum + 4 * ((int64_t)iy * s->width + ix));
+        const int64_t p = (int64_t)iy * s->width + ix;
+        vec4f *accp = (vec4f *)(accum + 4 * p);
         vec4f acc = *accp;
+        vec4f comp = compBuf ? *(vec4f *)(compBuf + 4 * p) : vec4f{0.f, 0.f, 0.f, 0.f};
         for (int k = 0; k < spp; k++) {
           int accumID = accumID0 + k;
           PixelSample ps = renderPixelSample(sc, ix, iy, accumID, st);
-          accumulate(acc, ps, accumID);
+          accumulate(acc, comp, ps, accumID, s->compensatedAccum != 0);
         }
         *accp = acc;
+        if (compBuf) *(vec4f *)(compBuf + 4 * p) = comp;
       }
     }
   };
@@ -876,11 +870,14 @@ static inline uint32_t make_8bit(float f) { return (uint32_t)std::min(255, std::
 
 // TiledFB.cu:13-52 with accumScale = 1/accumID (LocalFB.cpp:65).
 // fmt: 0 float4, 1 rgba8, 2 rgba8 sRGB
-void orc_resolve(const float *accum, int64_t numPixels, int accumID, int fmt, void *out) {
+// comp (may be NULL): compensation terms of the precision forms, added
+// before scaling.
+void orc_resolve(const float *accum, const float *comp, int64_t numPixels, int accumID, int fmt, void *out) {
   float accumScale = 1.f / accumID;
   for (int64_t i = 0; i < numPixels; i++) {
-    vec4f c = {accum[4 * i] * accumScale, accum[4 * i + 1] * accumScale, accum[4 * i + 2] * accumScale,
-               accum[4 * i + 3] * accumScale};
+    float a[4];
+    for (int c = 0; c < 4; c++) a[c] = comp ? accum[4 * i + c] + comp[4 * i + c] : accum[4 * i + c];
+    vec4f c = {a[0] * accumScale, a[1] * accumScale, a[2] * accumScale, a[3] * accumScale};
     if (fmt == 0) {
       float *o = (float *)out + 4 * i;
       o[0] = c.x; o[1] = c.y; o[2] = c.z; o[3] = c.w;

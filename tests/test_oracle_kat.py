@@ -224,3 +224,27 @@ def test_macrocell_ranges_bruteforce():
             for x in range(3):
                 blk = vol[8 * z:8 * z + 9, 8 * y:8 * y + 9, 8 * x:8 * x + 9]
                 assert r[z, y, x, 0] == blk.min() and r[z, y, x, 1] == blk.max()
+
+
+def test_compensated_accumulation_tracks_double_sum():
+    """Precision form: Neumaier-compensated accumulation across waves stays at
+    the double-precision sum of the same per-wave fragments, where the plain
+    float sum drifts."""
+    from barney_b200 import synth
+    vol = synth.blobs(12, 0)
+    base = synth.scene(vol, "f32", 6, 4, synth.tf_linear_ramp(32), 20.0, synth.DEFAULT_CAMERA, ambient=1.0)
+    plain = oracle.Scene(dict(base))
+    comp_sc = oracle.Scene(dict(base, compensated_accum=True))
+    spp = 600
+    acc_p, _, _ = oracle.render(plain, 0, spp, threads=1)
+    acc_c = np.zeros_like(acc_p)
+    cbuf = np.zeros_like(acc_p)
+    oracle.render(comp_sc, 0, spp, accum=acc_c, comp=cbuf, threads=1)
+    exact = np.zeros(acc_p.shape, np.float64)
+    for k in range(spp):  # each wave alone onto a zero buffer = that wave's fragments
+        one, _, _ = oracle.render(plain, k, 1, accum=np.zeros_like(acc_p), threads=1)
+        exact += one
+    err_plain = np.abs(acc_p - exact).sum()
+    err_comp = np.abs(acc_c.astype(np.float64) + cbuf - exact).sum()
+    assert err_comp <= err_plain
+    assert err_comp < 1e-3 * max(err_plain, 1e-30) or err_comp < 1e-5
