@@ -46,6 +46,7 @@ EXPORTS = [
     "bnFrameBufferRead", "bnFrameBufferGetSize", "bnAccumReset", "bnRender", "bnGetLastError",
     "bnGetLastErrorString", "bnClearLastError", "bnxGetStats", "bnxSetStream", "bnxGetStream",
     "bnxSetLaunchConfig", "bnxFrameBufferDevicePointer", "bnxVolumeGetMacrocells",
+    "bnxRenderStructuredNoAlloc",
 ]
 
 
@@ -94,6 +95,7 @@ def lib(build_if_missing=True):
         "bnxGetStats": ([P, P], None), "bnxSetStream": ([P, P], None), "bnxGetStream": ([P], P),
         "bnxSetLaunchConfig": ([P, I, I], None), "bnxFrameBufferDevicePointer": ([P], P),
         "bnxVolumeGetMacrocells": ([P, P, P, P], None),
+        "bnxRenderStructuredNoAlloc": ([P, P], I),
     }
     for name, (args, res) in sig.items():
         fn = getattr(L, name)

@@ -918,4 +918,92 @@ BN_API void bnxVolumeGetMacrocells(BNVolume vh, int *dims3, float *rangesOut, fl
   BN_CATCH()
 }
 
+BN_API int bnxRenderStructuredNoAlloc(const BNXNoAllocFrame *f, void *stream) {
+  BN_TRY
+  if (!f) throw Error(E_INVALID_ARG, "frame description is null");
+  int type;
+  switch ((int)f->voxelType) {
+  case BN_FLOAT32: type = VOX_F32; break;
+  case BN_UFIXED8:
+  case BN_UINT8: type = VOX_U8; break;
+  case BNX_FLOAT16: type = VOX_F16; break;
+  case BNX_BFLOAT16: type = VOX_BF16; break;
+  default: throw Error(E_UNSUPPORTED, "unsupported voxel type");
+  }
+  int fmt = f->colorFormat == BN_FLOAT4 ? FMT_FLOAT4 : f->colorFormat == BN_UFIXED8_RGBA ? FMT_RGBA8
+          : f->colorFormat == BN_UFIXED8_RGBA_SRGB ? FMT_RGBA8_SRGB : -1;
+  if (fmt < 0) throw Error(E_UNSUPPORTED, "unsupported colour format");
+  if (!f->voxels || !f->transferFunction || !f->accum || !f->color)
+    throw Error(E_INVALID_ARG, "voxels, transferFunction, accum and color must be device pointers");
+  for (int a = 0; a < 3; a++)
+    if (f->dims[a] < 2) throw Error(E_INVALID_ARG, "every grid dimension must be >= 2");
+  if (f->numTFValues < 2 || f->numTFValues > kMaxTF) throw Error(E_INVALID_ARG, "numTFValues must be in [2, 4096]");
+  if (f->width <= 0 || f->height <= 0 || f->pathsPerPixel <= 0 || f->accumID < 0)
+    throw Error(E_INVALID_ARG, "width, height and pathsPerPixel must be positive, accumID >= 0");
+  if (f->numDirLights < 0 || f->numDirLights > kMaxDirLights || (f->numDirLights && !f->dirLights))
+    throw Error(E_INVALID_ARG, "numDirLights must be in [0, 16] with a host array of lights");
+  int mc[3];
+  for (int a = 0; a < 3; a++) mc[a] = (f->dims[a] - 1 + kCellsPerMC - 1) / kCellsPerMC;
+  const long long nMC = (long long)mc[0] * mc[1] * mc[2];
+  if (nMC > kNoAllocMaxMacrocells)
+    throw Error(E_INVALID_ARG, "volume needs " + std::to_string(nMC) +
+                                   " macrocells; the no-allocation entry point holds at most " +
+                                   std::to_string((long long)kNoAllocMaxMacrocells) + " (a 513^3 grid)");
+  VolumeDD v{};
+  const v3 org = {f->gridOrigin.x, f->gridOrigin.y, f->gridOrigin.z};
+  const v3 spc = {f->gridSpacing.x, f->gridSpacing.y, f->gridSpacing.z};
+  v.voxels = f->voxels;
+  v.type = type;
+  v.numScalars = make_int3(f->dims[0], f->dims[1], f->dims[2]);
+  v.numCells = make_int3(f->dims[0] - 1, f->dims[1] - 1, f->dims[2] - 1);
+  v.gridOrigin = F3(org);
+  v.rcpSpacing = make_float3(1.f / spc.x, 1.f / spc.y, 1.f / spc.z);
+  v.boundsLo = F3(org);
+  v.boundsHi = make_float3(org.x + spc.x * (float)v.numCells.x, org.y + spc.y * (float)v.numCells.y,
+                           org.z + spc.z * (float)v.numCells.z);
+  v.majorants = nullptr;  // set to the static scratch by the launcher
+  v.mcDims = make_int3(mc[0], mc[1], mc[2]);
+  v.mcOrigin = F3(org);
+  v.rcpMcSpacing = make_float3(1.f / (8.f * spc.x), 1.f / (8.f * spc.y), 1.f / (8.f * spc.z));
+  v.tf = (const float4 *)f->transferFunction;
+  v.tfN = f->numTFValues;
+  v.domLo = f->domain.x;
+  v.domHi = f->domain.y;
+  v.baseDensity = f->densityAt1;
+  v.phase = f->hgPhase ? PHASE_HG : PHASE_SIMPLE;
+  v.anisotropy = std::min(0.99f, std::max(-0.99f, f->anisotropy));
+  v.scatteringAlbedo = std::min(1.f, std::max(0.f, f->scatteringAlbedo));
+  Camera cam(nullptr);
+  cam.set3f("position", f->cameraPosition.x, f->cameraPosition.y, f->cameraPosition.z);
+  cam.set3f("direction", f->cameraDirection.x, f->cameraDirection.y, f->cameraDirection.z);
+  cam.set3f("up", f->cameraUp.x, f->cameraUp.y, f->cameraUp.z);
+  cam.set1f("fovy", f->fovy);
+  cam.commit();
+  FrameDD fr{};
+  fr.dir00 = F3(cam.dir00);
+  fr.dirdu = F3(cam.dirdu);
+  fr.dirdv = F3(cam.dirdv);
+  fr.lens00 = F3(cam.lens00);
+  fr.width = f->width;
+  fr.height = f->height;
+  fr.bgColor = make_float4(f->bgColor.x, f->bgColor.y, f->bgColor.z, f->bgColor.w);
+  fr.ambientRadiance = f->ambientRadiance;
+  fr.cutPlane = make_float4(0.f, 0.f, 0.f, -1e30f);
+  fr.numDirLights = f->numDirLights;
+  for (int i = 0; i < f->numDirLights; i++) {
+    const float *L = f->dirLights + 7 * i;
+    DirLight l(nullptr);
+    l.set3f("direction", L[0], L[1], L[2]);
+    l.set1f("radiance", L[3]);
+    l.set3f("color", L[4], L[5], L[6]);
+    fr.dirLights[i] = l.dd();
+  }
+  fr.accum = (float4 *)f->accum;
+  fr.accumID0 = f->accumID;
+  fr.spp = f->pathsPerPixel;
+  ck(launchRenderNoAlloc(v, fr, fmt, f->color, 0, (cudaStream_t)stream), "no-allocation render");
+  return 0;
+  BN_CATCH(g_lastError)
+}
+
 }  // extern "C"

@@ -80,4 +80,9 @@ cudaError_t launchRender(const VolumeDD &vol, const FrameDD &frame, LaunchCounte
 cudaError_t launchResolve(const float4 *accum, int numPixels, int accumID, int fmt, void *out, cudaStream_t s);
 int renderKernelMaxBlocksPerSM(int threadsPerBlock);
 
+// No-allocation render: majorant grid and counters in a static device array
+// sized for kNoAllocMaxMacrocells macrocells (see bn_kernels.cu).
+constexpr int64_t kNoAllocMaxMacrocells = 64 * 64 * 64;
+cudaError_t launchRenderNoAlloc(VolumeDD v, FrameDD fr, int fmt, void *color, int roundUp, cudaStream_t s);
+
 }  // namespace bnb

@@ -27,6 +27,7 @@
 
 #include <cuda_fp16.h>
 #include <cstdint>
+#include <mutex>
 
 namespace bnb {
 
@@ -788,6 +789,97 @@ int renderKernelMaxBlocksPerSM(int tpb) {
   int occ = 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, renderKernel<VOX_F32>, tpb, 256 * sizeof(float4));
   return occ;
+}
+
+// ---------------------------------------------------------------------------
+// No-allocation render (bnxRenderStructuredNoAlloc)
+//
+// Scratch of this path -- the macrocell majorant grid and the launch
+// counters -- lives in the file-scope array below instead of in memory the
+// context allocates.  It is sized for kNoAllocMaxMacrocells macrocells
+// (64^3, i.e. grids up to 513^3 scalars) and is held by every GPU that loads
+// the library until the process exits: 1 MiB of majorants + 256 bytes of
+// counters.  All calls share it, so calls whose work overlaps on the GPU
+// race; each call overwrites the majorants it needs and clears the counters.
+// ---------------------------------------------------------------------------
+constexpr size_t kNoAllocCountersBytes = 256;
+static __device__ __align__(256) unsigned char
+    g_noAllocScratch[kNoAllocCountersBytes + kNoAllocMaxMacrocells * sizeof(float)];
+
+// Majorant grid straight from the voxels: the fused build of mcBuildKernel
+// without storing the scalar ranges.
+template <int T>
+__global__ void __launch_bounds__(128) mcMajorantScratchKernel(VolumeDD v, int roundUp) {
+  __shared__ float u8lut[256];
+  for (int i = threadIdx.x; i < 256; i += blockDim.x) u8lut[i] = (float)i * 1.f / 255.f;
+  __syncthreads();
+  float *majorants = (float *)(g_noAllocScratch + kNoAllocCountersBytes);
+  const int64_t n = (int64_t)v.mcDims.x * v.mcDims.y * v.mcDims.z;
+  for (int64_t tid = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; tid < n; tid += (int64_t)gridDim.x * blockDim.x) {
+    const int mx = (int)(tid % v.mcDims.x);
+    const int my = (int)((tid / v.mcDims.x) % v.mcDims.y);
+    const int mz = (int)(tid / ((int64_t)v.mcDims.x * v.mcDims.y));
+    const int x0 = mx * kCellsPerMC, y0 = my * kCellsPerMC, z0 = mz * kCellsPerMC;
+    const int x1 = min(x0 + kCellsPerMC, v.numScalars.x - 1);
+    const int y1 = min(y0 + kCellsPerMC, v.numScalars.y - 1);
+    const int z1 = min(z0 + kCellsPerMC, v.numScalars.z - 1);
+    float lo = kInf, hi = -kInf;
+    const int64_t nx = v.numScalars.x, nxy = (int64_t)v.numScalars.x * v.numScalars.y;
+    for (int z = z0; z <= z1; z++)
+      for (int y = y0; y <= y1; y++) {
+        const int64_t row = nx * y + nxy * z;
+        for (int x = x0; x <= x1; x++) {
+          float f = loadVoxel<T>(v.voxels, row + x, u8lut);
+          lo = fmin_(lo, f);
+          hi = fmax_(hi, f);
+        }
+      }
+    majorants[tid] = roundUpMajorant(tfMajorant(v, lo, hi), roundUp);
+  }
+}
+
+// Device address of g_noAllocScratch on the current device, looked up once
+// per device with cudaGetSymbolAddress (the host-side name of the array is
+// only a stand-in, never a device address).
+static void *noAllocScratchAddress(cudaError_t *err) {
+  static std::mutex m;
+  static void *addr[64] = {nullptr};
+  int dev = 0;
+  *err = cudaGetDevice(&dev);
+  if (*err != cudaSuccess) return nullptr;
+  if (dev < 0 || dev >= 64) { *err = cudaErrorInvalidDevice; return nullptr; }
+  std::lock_guard<std::mutex> l(m);
+  if (!addr[dev]) {
+    void *p = nullptr;
+    *err = cudaGetSymbolAddress(&p, g_noAllocScratch);
+    if (*err != cudaSuccess) return nullptr;
+    addr[dev] = p;
+  }
+  return addr[dev];
+}
+
+cudaError_t launchRenderNoAlloc(VolumeDD v, FrameDD fr, int fmt, void *color, int roundUp, cudaStream_t s) {
+  const int64_t n = (int64_t)v.mcDims.x * v.mcDims.y * v.mcDims.z;
+  if (n <= 0 || n > kNoAllocMaxMacrocells) return cudaErrorInvalidValue;
+  cudaError_t e = cudaSuccess;
+  unsigned char *base = (unsigned char *)noAllocScratchAddress(&e);
+  if (!base) return e;
+  LaunchCounters *ctr = (LaunchCounters *)base;
+  v.majorants = (const float *)(base + kNoAllocCountersBytes);
+  e = cudaMemsetAsync(ctr, 0, sizeof(LaunchCounters), s);
+  if (e != cudaSuccess) return e;
+  const int blocks = (int)std::min<int64_t>((n + 127) / 128, (int64_t)smCount() * 16);
+  switch (v.type) {
+  case VOX_F32: mcMajorantScratchKernel<VOX_F32><<<blocks, 128, 0, s>>>(v, roundUp); break;
+  case VOX_U8: mcMajorantScratchKernel<VOX_U8><<<blocks, 128, 0, s>>>(v, roundUp); break;
+  case VOX_F16: mcMajorantScratchKernel<VOX_F16><<<blocks, 128, 0, s>>>(v, roundUp); break;
+  default: mcMajorantScratchKernel<VOX_BF16><<<blocks, 128, 0, s>>>(v, roundUp); break;
+  }
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  e = launchRender(v, fr, ctr, 0, 0, s);
+  if (e != cudaSuccess) return e;
+  return launchResolve(fr.accum, fr.width * fr.height, fr.accumID0 + fr.spp, fmt, color, s);
 }
 
 }  // namespace bnb

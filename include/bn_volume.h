@@ -222,6 +222,50 @@ BN_API void *bnxFrameBufferDevicePointer(BNFrameBuffer fb);
 BN_API void bnxVolumeGetMacrocells(BNVolume volume, int *dims3, float *rangesHostOut,
                                    float *majorantsHostOut);
 
+/* No-allocation render (no reference counterpart).  For callers that cannot
+   allocate device memory while rendering -- an application that reserves
+   all of its GPU memory up front and hands this library only buffers it
+   owns, or a real-time loop that must not stall a frame on cudaMalloc's
+   implicit device synchronisation.  Renders pathsPerPixel waves of one
+   structured volume into the caller's accumulation buffer and resolves the
+   colour into the caller's output, launching asynchronously on cudaStream
+   (NULL: the legacy default stream) and allocating nothing: the macrocell
+   majorant grid and the launch counters live in a static device array sized
+   for BNX_NOALLOC_MAX_MACROCELLS macrocells (64^3, i.e. grids up to 513^3
+   scalars; 1 MiB held by every GPU that loads the library until exit).
+   Larger volumes are rejected with error 2 and a message.  All calls share
+   that array, so calls whose work overlaps on the GPU (other streams, other
+   host threads) race; serialise them.  The first call on each device looks
+   up the array's device address (cudaGetSymbolAddress); make that first call
+   outside any stream capture.  Returns 0 or the error code also recorded for
+   bnGetLastError. */
+#define BNX_NOALLOC_MAX_MACROCELLS (64 * 64 * 64)
+typedef struct {
+  const void *voxels;              /* device: x-fastest scalars, dims[0]*dims[1]*dims[2] */
+  BNDataType voxelType;            /* BN_FLOAT32, BN_UFIXED8, BNX_FLOAT16, BNX_BFLOAT16 */
+  int dims[3];
+  bn_float3 gridOrigin, gridSpacing;
+  const bn_float4 *transferFunction; /* device: numTFValues RGBA entries */
+  int numTFValues;
+  bn_float2 domain;
+  float densityAt1;
+  bn_float3 cameraPosition, cameraDirection, cameraUp;
+  float fovy;
+  bn_float4 bgColor;
+  float ambientRadiance;
+  int numDirLights;                /* at most 16 */
+  const float *dirLights;          /* host: per light direction xyz, radiance, colour rgb */
+  int hgPhase;                     /* as renderer parameter bnx.hgPhase */
+  float anisotropy, scatteringAlbedo;
+  int width, height;
+  int accumID;                     /* accumulation index of the first wave; 0 starts a frame */
+  int pathsPerPixel;
+  bn_float4 *accum;                /* device: width*height accumulation buffer, in/out */
+  void *color;                     /* device: width*height pixels of colorFormat */
+  BNDataType colorFormat;          /* BN_FLOAT4, BN_UFIXED8_RGBA, BN_UFIXED8_RGBA_SRGB */
+} BNXNoAllocFrame;
+BN_API int bnxRenderStructuredNoAlloc(const BNXNoAllocFrame *frame, void *cudaStream);
+
 #ifdef __cplusplus
 }
 #endif
