@@ -46,7 +46,7 @@ EXPORTS = [
     "bnFrameBufferRead", "bnFrameBufferGetSize", "bnAccumReset", "bnRender", "bnGetLastError",
     "bnGetLastErrorString", "bnClearLastError", "bnxGetStats", "bnxSetStream", "bnxGetStream",
     "bnxSetLaunchConfig", "bnxFrameBufferDevicePointer", "bnxVolumeGetMacrocells",
-    "bnxRenderStructuredNoAlloc",
+    "bnxRenderStructuredNoAlloc", "bnxSetScheduling", "bnxRenderBatch", "bnxSetBatchGraphs", "bnxAutotuneBatch",
 ]
 
 
@@ -58,6 +58,16 @@ class BNXStats(ctypes.Structure):
     _fields_ = [("samples", ctypes.c_ulonglong), ("mcVisits", ctypes.c_ulonglong), ("rays", ctypes.c_ulonglong),
                 ("pixelSamples", ctypes.c_ulonglong), ("errorFlags", ctypes.c_ulonglong),
                 ("renderMs", ctypes.c_float), ("resolveMs", ctypes.c_float)]
+
+
+class BNXRenderJob(ctypes.Structure):
+    _fields_ = [("renderer", ctypes.c_void_p), ("model", ctypes.c_void_p), ("camera", ctypes.c_void_p),
+                ("frameBuffer", ctypes.c_void_p)]
+
+
+class BNXLaunchConfig(ctypes.Structure):
+    _fields_ = [("threadsPerBlock", ctypes.c_int), ("blocksPerSM", ctypes.c_int), ("genBatch", ctypes.c_int),
+                ("shadeBatch", ctypes.c_int), ("minBusy", ctypes.c_int), ("renderMs", ctypes.c_float)]
 
 
 class BarneyError(RuntimeError):
@@ -96,6 +106,8 @@ def lib(build_if_missing=True):
         "bnxSetLaunchConfig": ([P, I, I], None), "bnxFrameBufferDevicePointer": ([P], P),
         "bnxVolumeGetMacrocells": ([P, P, P, P], None),
         "bnxRenderStructuredNoAlloc": ([P, P], I),
+        "bnxSetScheduling": ([P, I, I, I], None), "bnxRenderBatch": ([P, P, I], None),
+        "bnxSetBatchGraphs": ([P, I], None), "bnxAutotuneBatch": ([P, P, I, P], None),
     }
     for name, (args, res) in sig.items():
         fn = getattr(L, name)
@@ -129,6 +141,59 @@ def _void_p(x):
     return x
 
 
+class Context:
+    """A bn* context shared by several VolumeRenderers (batch rendering)."""
+
+    def __init__(self, gpu=0, stream=None):
+        L = lib()
+        self.L = L
+        ids = (ctypes.c_int * 1)(gpu)
+        self.ctx = L.bnContextCreate(1, None, 1, ids)
+        check()
+        if stream is not None:
+            L.bnxSetStream(self.ctx, stream)
+
+    def render_batch(self, renderers):
+        """One persistent launch for all renderers' frames (bnxRenderBatch)."""
+        jobs = (BNXRenderJob * len(renderers))()
+        for j, r in zip(jobs, renderers):
+            j.renderer, j.model, j.camera, j.frameBuffer = r.renderer, r.model, r.camera, r.fb
+        self.L.bnxRenderBatch(self.ctx, jobs, len(renderers))
+        check()
+
+    def autotune_batch(self, renderers):
+        jobs = (BNXRenderJob * len(renderers))()
+        for j, r in zip(jobs, renderers):
+            j.renderer, j.model, j.camera, j.frameBuffer = r.renderer, r.model, r.camera, r.fb
+        best = BNXLaunchConfig()
+        self.L.bnxAutotuneBatch(self.ctx, jobs, len(renderers), ctypes.byref(best))
+        check()
+        return {f: getattr(best, f) for f, _ in BNXLaunchConfig._fields_}
+
+    def set_graphs(self, enable):
+        self.L.bnxSetBatchGraphs(self.ctx, int(enable))
+        check()
+
+    def stats(self):
+        st = BNXStats()
+        self.L.bnxGetStats(self.ctx, ctypes.byref(st))
+        check()
+        return {"samples": st.samples, "mc_visits": st.mcVisits, "rays": st.rays,
+                "pixel_samples": st.pixelSamples, "error_flags": st.errorFlags,
+                "render_ms": st.renderMs, "resolve_ms": st.resolveMs}
+
+    def close(self):
+        if self.ctx:
+            self.L.bnContextDestroy(self.ctx)
+            self.ctx = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 class VolumeRenderer:
     """One structured volume rendered through the bn* API (the call sequence
     of SURVEY section 3.2/3.3: texture data -> structured field -> volume +
@@ -138,15 +203,19 @@ class VolumeRenderer:
     ``desc`` is the scene dict of ``barney_b200.synth`` (the same dict the
     oracle takes)."""
 
-    def __init__(self, desc, color_format="float4", gpu=0, stream=None):
+    def __init__(self, desc, color_format="float4", gpu=0, stream=None, context=None):
         L = lib()
         self.L = L
         self.desc = desc
-        ids = (ctypes.c_int * 1)(gpu)
-        self.ctx = L.bnContextCreate(1, None, 1, ids)
-        check()
-        if stream is not None:
-            L.bnxSetStream(self.ctx, stream)
+        self.shared = context
+        if context is not None:
+            self.ctx = context.ctx
+        else:
+            ids = (ctypes.c_int * 1)(gpu)
+            self.ctx = L.bnContextCreate(1, None, 1, ids)
+            check()
+            if stream is not None:
+                L.bnxSetStream(self.ctx, stream)
         self._objects = []
         vox = desc["voxels"]
         nz, ny, nx = vox.shape
@@ -232,6 +301,7 @@ class VolumeRenderer:
         L.bnSet1i(self.renderer, b"bnx.hgPhase", 1 if desc.get("phase", "simple") == "hg" else 0)
         L.bnSet1i(self.renderer, b"bnx.emissionAbsorption", int(desc.get("emission_absorption", False)))
         L.bnSet1i(self.renderer, b"bnx.exactLog", int(desc.get("exact_log", False)))
+        L.bnSet1i(self.renderer, b"bnx.compensatedAccum", int(desc.get("compensated_accum", False)))
         L.bnCommit(self.renderer)
         check()
 
@@ -286,14 +356,22 @@ class VolumeRenderer:
         check()
         return ranges, maj
 
+    def set_scheduling(self, gen_batch=16, shade_batch=8, min_busy=8):
+        self.L.bnxSetScheduling(self.ctx, gen_batch, shade_batch, min_busy)
+        check()
+
     def set_launch_config(self, blocks_per_sm=0, threads_per_block=0):
         self.L.bnxSetLaunchConfig(self.ctx, blocks_per_sm, threads_per_block)
         check()
 
     def close(self):
-        if self.ctx:
+        if self.ctx and self.shared is None:
             self.L.bnContextDestroy(self.ctx)
-            self.ctx = None
+        elif self.ctx:
+            for h in self._objects:
+                self.L.bnRelease(h)
+            self._objects = []
+        self.ctx = None
 
     def __del__(self):
         try:

@@ -267,6 +267,7 @@ struct Renderer : Object {
     int hgPhase = 0;              // bnx: multi-scatter-build phase model (HGPhase)
     int emissionAbsorption = 0;   // bnx
     int exactLog = 0;             // bnx
+    int compensatedAccum = 0;     // bnx: Neumaier-compensated accumulation (precision forms)
   } staged, p;
   explicit Renderer(Context *c) : Object(c, K_RENDERER) {}
   bool set1i(const std::string &m, int v) override {
@@ -276,6 +277,7 @@ struct Renderer : Object {
     if (m == "bnx.hgPhase") { staged.hgPhase = v ? 1 : 0; return true; }
     if (m == "bnx.emissionAbsorption") { staged.emissionAbsorption = v ? 1 : 0; return true; }
     if (m == "bnx.exactLog") { staged.exactLog = v ? 1 : 0; return true; }
+    if (m == "bnx.compensatedAccum") { staged.compensatedAccum = v ? 1 : 0; return true; }
     return false;
   }
   bool set1f(const std::string &m, float v) override {
@@ -294,7 +296,7 @@ struct FrameBuffer : Object {
   int width = 0, height = 0;
   int colorFormat = FMT_RGBA8;
   uint32_t accumID = 0;
-  DeviceBuffer accum, color;
+  DeviceBuffer accum, color, comp;
   explicit FrameBuffer(Context *c) : Object(c, K_FB) {}
 };
 
@@ -308,7 +310,18 @@ struct Context {
   LaunchCounters *dCounters = nullptr;
   cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
   int blocksPerSM = 0, threadsPerBlock = 128;
+  SchedDD sched;
   BNXStats stats{};
+  // batch path: job table + chunk prefix (device, and pinned host mirrors a
+  // captured graph copies from), and the cached graph of the last batch shape
+  DeviceBuffer batchJobs, batchChunks;
+  JobDD *hostJobs = nullptr;
+  int *hostChunks = nullptr;
+  LaunchCounters *hostCounters = nullptr;
+  int hostCapacity = 0;
+  bool useGraphs = true;
+  cudaGraphExec_t graphExec = nullptr;
+  std::vector<const void *> graphKey;
   std::mutex mutex;
   std::unordered_map<Object *, std::pair<ObjectSP, int>> handles;  // app references
 
@@ -323,6 +336,10 @@ struct Context {
   ~Context() {
     cudaSetDevice(device);
     cudaStreamSynchronize(stream);
+    if (graphExec) cudaGraphExecDestroy(graphExec);
+    if (hostJobs) cudaFreeHost(hostJobs);
+    if (hostChunks) cudaFreeHost(hostChunks);
+    if (hostCounters) cudaFreeHost(hostCounters);
     handles.clear();
     for (auto &e : ev) if (e) cudaEventDestroy(e);
     if (dCounters) cudaFree(dCounters);
@@ -438,20 +455,22 @@ void Volume::commit() {  // Volume.cpp:26-35
 // ---------------------------------------------------------------------------
 // render (Context::renderTiles, Context.cpp:139-182, + finalizeFrame)
 // ---------------------------------------------------------------------------
-static void render(Context *ctx, Renderer &r, Model &m, Camera &cam, FrameBuffer &fb) {
+// The device job of one (renderer, model, camera, frame buffer) tuple,
+// validated; fr.spp waves starting at the frame buffer's accumID.
+static JobDD buildJob(Context *ctx, Renderer &r, Model &m, Camera &cam, FrameBuffer &fb) {
   if (!m.built || !m.group || !m.group->volume) throw Error(E_STATE, "model has no built volume instance");
   if (fb.width <= 0 || fb.height <= 0) throw Error(E_STATE, "frame buffer has not been resized");
   if (cam.apertureRadius > 0.f) throw Error(E_UNSUPPORTED, "depth-of-field cameras are not supported");
   const Renderer::Params &p = r.p;
   if (p.hgPhase && p.maxVolumeBounces > 0)
     throw Error(E_UNSUPPORTED, "multiple volume scattering (maxVolumeBounces > 0) is not supported");
-  if (p.pathsPerPixel <= 0) return;
   Volume &vol = *m.group->volume;
   vol.build();  // no-op unless the TF changed
-  VolumeDD v = vol.dd();
+  JobDD job{};
+  VolumeDD &v = job.v;
+  v = vol.dd();
   v.phase = p.hgPhase ? PHASE_HG : PHASE_SIMPLE;
-
-  FrameDD fr{};
+  FrameDD &fr = job.fr;
   fr.dir00 = F3(cam.dir00);
   fr.dirdu = F3(cam.dirdu);
   fr.dirdv = F3(cam.dirdv);
@@ -472,29 +491,139 @@ static void render(Context *ctx, Renderer &r, Model &m, Camera &cam, FrameBuffer
   fr.emissionAbsorption = p.emissionAbsorption;
   fr.exactLog = p.exactLog;
   fr.accum = (float4 *)fb.accum.ptr;
+  fr.comp = nullptr;
+  if (p.compensatedAccum) {
+    if (!fb.comp.ptr) {
+      fb.comp.resize((size_t)fb.width * fb.height * sizeof(float4));
+      ck(cudaMemsetAsync(fb.comp.ptr, 0, fb.comp.bytes, ctx->stream), "compensation clear");
+    }
+    fr.comp = (float4 *)fb.comp.ptr;
+  }
   fr.accumID0 = (int)fb.accumID;
   fr.spp = p.pathsPerPixel;
+  fr.color = fb.color.ptr;
+  fr.colorFormat = fb.colorFormat;
+  return job;
+}
 
+static void readStats(Context *ctx, const LaunchCounters &hc, unsigned long long pixelSamples) {
+  BNXStats &st = ctx->stats;
+  st.samples = hc.samples;
+  st.mcVisits = hc.mcVisits;
+  st.rays = hc.rays;
+  st.pixelSamples = pixelSamples;
+  st.errorFlags = hc.errorFlags;
+  cudaEventElapsedTime(&st.renderMs, ctx->ev[0], ctx->ev[1]);
+  cudaEventElapsedTime(&st.resolveMs, ctx->ev[1], ctx->ev[2]);
+}
+
+static void render(Context *ctx, Renderer &r, Model &m, Camera &cam, FrameBuffer &fb) {
+  JobDD job = buildJob(ctx, r, m, cam, fb);
+  if (job.fr.spp <= 0) return;
   ck(cudaMemsetAsync(ctx->dCounters, 0, sizeof(LaunchCounters), ctx->stream), "counter reset");
   ck(cudaEventRecord(ctx->ev[0], ctx->stream), "event");
-  ck(launchRender(v, fr, ctx->dCounters, ctx->blocksPerSM, ctx->threadsPerBlock, ctx->stream), "render kernel");
+  ck(launchRender(job.v, job.fr, ctx->dCounters, ctx->blocksPerSM, ctx->threadsPerBlock, ctx->stream, ctx->sched),
+     "render kernel");
   ck(cudaEventRecord(ctx->ev[1], ctx->stream), "event");
-  fb.accumID += p.pathsPerPixel;
+  fb.accumID += job.fr.spp;
   ck(launchResolve((const float4 *)fb.accum.ptr, fb.width * fb.height, (int)fb.accumID, fb.colorFormat, fb.color.ptr,
-                   ctx->stream),
+                   ctx->stream, job.fr.comp),
      "resolve kernel");
   ck(cudaEventRecord(ctx->ev[2], ctx->stream), "event");
   LaunchCounters hc;
   ck(cudaMemcpyAsync(&hc, ctx->dCounters, sizeof hc, cudaMemcpyDeviceToHost, ctx->stream), "counter read");
   ck(cudaStreamSynchronize(ctx->stream), "render");
-  BNXStats &st = ctx->stats;
-  st.samples = hc.samples;
-  st.mcVisits = hc.mcVisits;
-  st.rays = hc.rays;
-  st.pixelSamples = (unsigned long long)fb.width * fb.height * p.pathsPerPixel;
-  st.errorFlags = hc.errorFlags;
-  cudaEventElapsedTime(&st.renderMs, ctx->ev[0], ctx->ev[1]);
-  cudaEventElapsedTime(&st.resolveMs, ctx->ev[1], ctx->ev[2]);
+  readStats(ctx, hc, (unsigned long long)fb.width * fb.height * job.fr.spp);
+}
+
+// Every job's waves in one persistent launch of the batch kernel, then one
+// batch resolve.  The copy-in of the job table, the counter reset, both
+// kernels and the counter read-back are captured once into a CUDA graph per
+// batch shape (same frame buffers, sizes and launch configuration) and
+// replayed; per-frame values (cameras, accumIDs) travel in the pinned job
+// table the graph copies from.  Results equal one bnRender per job.
+struct BatchEntry { Renderer *r; Model *m; Camera *c; FrameBuffer *fb; };
+
+static void renderBatch(Context *ctx, const std::vector<BatchEntry> &entries) {
+  const int n = (int)entries.size();
+  if (n == 0) return;
+  if (n > ctx->hostCapacity) {
+    if (ctx->graphExec) { cudaGraphExecDestroy(ctx->graphExec); ctx->graphExec = nullptr; ctx->graphKey.clear(); }
+    if (ctx->hostJobs) cudaFreeHost(ctx->hostJobs);
+    if (ctx->hostChunks) cudaFreeHost(ctx->hostChunks);
+    ctx->hostJobs = nullptr;
+    ctx->hostChunks = nullptr;
+    const int cap = std::max(n, 2 * ctx->hostCapacity);
+    ck(cudaHostAlloc((void **)&ctx->hostJobs, cap * sizeof(JobDD), cudaHostAllocDefault), "pinned job table");
+    ck(cudaHostAlloc((void **)&ctx->hostChunks, (cap + 1) * sizeof(int), cudaHostAllocDefault), "pinned chunks");
+    if (!ctx->hostCounters)
+      ck(cudaHostAlloc((void **)&ctx->hostCounters, sizeof(LaunchCounters), cudaHostAllocDefault), "pinned counters");
+    ctx->batchJobs.resize(cap * sizeof(JobDD));
+    ctx->batchChunks.resize((cap + 1) * sizeof(int));
+    ctx->hostCapacity = cap;
+  }
+  std::vector<const void *> key;
+  long long chunks = 0;
+  unsigned long long pixelSamples = 0;
+  ctx->hostChunks[0] = 0;
+  for (int i = 0; i < n; i++) {
+    const BatchEntry &e = entries[i];
+    JobDD job = buildJob(ctx, *e.r, *e.m, *e.c, *e.fb);
+    if (job.fr.spp <= 0) throw Error(E_INVALID_ARG, "every batch job needs pathsPerPixel >= 1");
+    ctx->hostJobs[i] = job;
+    chunks += ((long long)job.fr.width * job.fr.height + 31) / 32;
+    if (chunks > 0x7fffffffLL) throw Error(E_INVALID_ARG, "batch too large");
+    ctx->hostChunks[i + 1] = (int)chunks;
+    pixelSamples += (unsigned long long)job.fr.width * job.fr.height * job.fr.spp;
+    key.push_back(e.fb);
+    key.push_back(e.fb->accum.ptr);
+    key.push_back(e.fb->comp.ptr);
+    key.push_back((const void *)(intptr_t)(e.fb->width * 65536 + e.fb->height));
+  }
+  key.push_back((const void *)(intptr_t)(ctx->blocksPerSM * 4096 + ctx->threadsPerBlock));
+  key.push_back((const void *)(intptr_t)(ctx->sched.genBatch * 65536 + ctx->sched.shadeBatch * 256 + ctx->sched.minBusy));
+  key.push_back((const void *)(intptr_t)n);
+  auto enqueue = [&](cudaStream_t s) {
+    ck(cudaMemcpyAsync(ctx->batchJobs.ptr, ctx->hostJobs, n * sizeof(JobDD), cudaMemcpyHostToDevice, s), "job table");
+    ck(cudaMemcpyAsync(ctx->batchChunks.ptr, ctx->hostChunks, (n + 1) * sizeof(int), cudaMemcpyHostToDevice, s),
+       "chunk table");
+    ck(cudaMemsetAsync(ctx->dCounters, 0, sizeof(LaunchCounters), s), "counter reset");
+    ck(cudaEventRecord(ctx->ev[0], s), "event");
+    ck(launchRenderBatch((const JobDD *)ctx->batchJobs.ptr, (const int *)ctx->batchChunks.ptr, n, ctx->dCounters,
+                         ctx->blocksPerSM, ctx->threadsPerBlock, s, ctx->sched),
+       "batch render kernel");
+    ck(cudaEventRecord(ctx->ev[1], s), "event");
+    ck(launchResolveBatch((const JobDD *)ctx->batchJobs.ptr, (const int *)ctx->batchChunks.ptr, n, (int)chunks, s),
+       "batch resolve kernel");
+    ck(cudaEventRecord(ctx->ev[2], s), "event");
+    ck(cudaMemcpyAsync(ctx->hostCounters, ctx->dCounters, sizeof(LaunchCounters), cudaMemcpyDeviceToHost, s),
+       "counter read");
+  };
+  if (ctx->useGraphs) {
+    if (!ctx->graphExec || key != ctx->graphKey) {
+      if (ctx->graphExec) { cudaGraphExecDestroy(ctx->graphExec); ctx->graphExec = nullptr; }
+      cudaGraph_t g = nullptr;
+      ck(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal), "graph capture");
+      try {
+        enqueue(ctx->stream);
+      } catch (...) {
+        cudaStreamEndCapture(ctx->stream, &g);
+        if (g) cudaGraphDestroy(g);
+        throw;
+      }
+      ck(cudaStreamEndCapture(ctx->stream, &g), "graph capture");
+      cudaError_t e = cudaGraphInstantiate(&ctx->graphExec, g, 0);
+      cudaGraphDestroy(g);
+      ck(e, "graph instantiate");
+      ctx->graphKey = key;
+    }
+    ck(cudaGraphLaunch(ctx->graphExec, ctx->stream), "graph launch");
+  } else {
+    enqueue(ctx->stream);
+  }
+  ck(cudaStreamSynchronize(ctx->stream), "batch render");
+  for (int i = 0; i < n; i++) entries[i].fb->accumID += ctx->hostJobs[i].fr.spp;
+  readStats(ctx, *ctx->hostCounters, pixelSamples);
 }
 
 }  // namespace bnb
@@ -827,6 +956,7 @@ BN_API void bnFrameBufferResize(BNFrameBuffer fbh, BNDataType fmt, int sx, int s
   fb->colorFormat = f;
   fb->accum.resize((size_t)sx * sy * sizeof(float4));
   fb->color.resize((size_t)sx * sy * (f == FMT_FLOAT4 ? 16 : 4));
+  fb->comp.release();
   fb->accumID = 0;
   BN_CATCH()
 }
@@ -1004,6 +1134,85 @@ BN_API int bnxRenderStructuredNoAlloc(const BNXNoAllocFrame *f, void *stream) {
   ck(launchRenderNoAlloc(v, fr, fmt, f->color, 0, (cudaStream_t)stream), "no-allocation render");
   return 0;
   BN_CATCH(g_lastError)
+}
+
+BN_API void bnxSetScheduling(BNContext context, int genBatch, int shadeBatch, int minBusy) {
+  BN_TRY
+  Context *c = getContext(context);
+  if (genBatch < 1 || genBatch > 32 || shadeBatch < 1 || shadeBatch > 32 || minBusy < 0 || minBusy > 32)
+    throw Error(E_INVALID_ARG, "scheduling thresholds must lie in [1, 32] (minBusy in [0, 32])");
+  c->sched.genBatch = genBatch;
+  c->sched.shadeBatch = shadeBatch;
+  c->sched.minBusy = minBusy;
+  BN_CATCH()
+}
+
+static std::vector<BatchEntry> batchEntries(const BNXRenderJob *jobs, int n) {
+  if (n < 0 || (n && !jobs)) throw Error(E_INVALID_ARG, "invalid job array");
+  std::vector<BatchEntry> e;
+  std::vector<ObjectSP> keep;
+  for (int i = 0; i < n; i++) {
+    auto r = getAs<Renderer>(jobs[i].renderer, Object::K_RENDERER, "BNRenderer");
+    auto m = getAs<Model>(jobs[i].model, Object::K_MODEL, "BNModel");
+    auto c = getAs<Camera>(jobs[i].camera, Object::K_CAMERA, "BNCamera");
+    auto fb = getAs<FrameBuffer>(jobs[i].frameBuffer, Object::K_FB, "BNFrameBuffer");
+    for (auto &p : e)
+      if (p.fb == fb.get()) throw Error(E_INVALID_ARG, "a frame buffer appears twice in one batch");
+    e.push_back({r.get(), m.get(), c.get(), fb.get()});
+  }
+  return e;
+}
+
+BN_API void bnxRenderBatch(BNContext context, const BNXRenderJob *jobs, int numJobs) {
+  BN_TRY
+  Context *c = getContext(context);
+  c->activate();
+  renderBatch(c, batchEntries(jobs, numJobs));
+  BN_CATCH()
+}
+
+BN_API void bnxSetBatchGraphs(BNContext context, int enable) {
+  BN_TRY
+  getContext(context)->useGraphs = enable != 0;
+  BN_CATCH()
+}
+
+BN_API void bnxAutotuneBatch(BNContext context, const BNXRenderJob *jobs, int numJobs, BNXLaunchConfig *best) {
+  BN_TRY
+  Context *c = getContext(context);
+  c->activate();
+  std::vector<BatchEntry> e = batchEntries(jobs, numJobs);
+  std::vector<uint32_t> saved;
+  for (auto &x : e) saved.push_back(x.fb->accumID);
+  const int maxBps = std::max(1, renderKernelMaxBlocksPerSM(128));
+  struct Cand { int tpb, bps, gen, shade, busy; };
+  std::vector<Cand> cands;
+  for (int tpb : {64, 128})
+    for (int gen : {8, 16, 24})
+      for (int shade : {4, 8, 16})
+        cands.push_back({tpb, tpb == 64 ? 2 * maxBps : maxBps, gen, shade, 8});
+  const int oldTpb = c->threadsPerBlock, oldBps = c->blocksPerSM;
+  const SchedDD oldSched = c->sched;
+  Cand bestC{oldTpb, oldBps, oldSched.genBatch, oldSched.shadeBatch, oldSched.minBusy};
+  float bestMs = 1e30f;
+  for (const Cand &k : cands) {
+    c->threadsPerBlock = k.tpb;
+    c->blocksPerSM = k.bps;
+    c->sched.genBatch = k.gen;
+    c->sched.shadeBatch = k.shade;
+    c->sched.minBusy = k.busy;
+    for (size_t i = 0; i < e.size(); i++) e[i].fb->accumID = saved[i];
+    renderBatch(c, e);
+    if (c->stats.renderMs < bestMs) { bestMs = c->stats.renderMs; bestC = k; }
+  }
+  c->threadsPerBlock = bestC.tpb;
+  c->blocksPerSM = bestC.bps;
+  c->sched.genBatch = bestC.gen;
+  c->sched.shadeBatch = bestC.shade;
+  c->sched.minBusy = bestC.busy;
+  for (auto &x : e) x.fb->accumID = 0;  // tuning frames are discarded
+  if (best) *best = {bestC.tpb, bestC.bps, bestC.gen, bestC.shade, bestC.busy, bestMs};
+  BN_CATCH()
 }
 
 }  // extern "C"

@@ -59,8 +59,28 @@ struct FrameDD {
   int emissionAbsorption;
   int exactLog;
   float4 *accum;        // width*height, linear
+  float4 *comp;         // width*height Neumaier compensation terms, or null (plain sums)
   int accumID0;         // accumID of the first wave of this launch
   int spp;              // waves in this launch
+  void *color;          // resolved output (batch resolve only)
+  int colorFormat;      // ColorFormat of color
+};
+
+// One render job: a volume and a frame.  The single-frame kernel takes it
+// as a parameter; the batch kernel reads a table of them from HBM.
+struct JobDD {
+  VolumeDD v;
+  FrameDD fr;
+};
+
+// Warp scheduling of the render loop: primary rays are generated once at
+// least genBatch lanes of a warp need one, collisions shaded once at least
+// shadeBatch lanes have one -- or as soon as fewer than minBusy lanes are
+// inside a Woodcock range.
+struct SchedDD {
+  int genBatch = 16;
+  int shadeBatch = 8;
+  int minBusy = 8;
 };
 
 // Device counters of one launch (samples, mcVisits, rays, errorFlags)
@@ -76,8 +96,15 @@ cudaError_t launchBuildMacrocells(const VolumeDD &vol, float2 *ranges, float *ma
 cudaError_t launchMapMajorants(const VolumeDD &vol, const float2 *ranges, float *majorants, int roundUp,
                                cudaStream_t s);
 cudaError_t launchRender(const VolumeDD &vol, const FrameDD &frame, LaunchCounters *counters, int blocksPerSM,
-                         int threadsPerBlock, cudaStream_t s);
-cudaError_t launchResolve(const float4 *accum, int numPixels, int accumID, int fmt, void *out, cudaStream_t s);
+                         int threadsPerBlock, cudaStream_t s, const SchedDD &sd = SchedDD());
+// jobs / chunkStart: device arrays; chunkStart has numJobs+1 entries, the
+// prefix sum of each job's ceil(width*height/32) pixel chunks.
+cudaError_t launchRenderBatch(const JobDD *jobs, const int *chunkStart, int numJobs, LaunchCounters *counters,
+                              int blocksPerSM, int threadsPerBlock, cudaStream_t s, const SchedDD &sd = SchedDD());
+cudaError_t launchResolve(const float4 *accum, int numPixels, int accumID, int fmt, void *out, cudaStream_t s,
+                          const float4 *comp = nullptr);
+// resolves every job of a batch table into its fr.color after its waves
+cudaError_t launchResolveBatch(const JobDD *jobs, const int *chunkStart, int numJobs, int numChunks, cudaStream_t s);
 int renderKernelMaxBlocksPerSM(int threadsPerBlock);
 
 // No-allocation render: majorant grid and counters in a static device array

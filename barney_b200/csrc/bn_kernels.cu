@@ -221,7 +221,6 @@ __global__ void mcMapKernel(VolumeDD v, const float2 *ranges, float *majorants, 
 // ---------------------------------------------------------------------------
 // render megakernel
 // ---------------------------------------------------------------------------
-enum Phase : int { PH_DONE = 0, PH_NEWSAMPLE = 1, PH_PRIMARY = 2, PH_SHADOW = 3 };
 
 // Per-lane state of the ray being traced.
 struct TraceState {
@@ -232,11 +231,9 @@ struct TraceState {
   float nextCellBegin;
   float3 tNext, tStep;
   int cx, cy, cz;
-  int bits;             // 1/2/4: dir.x/y/z > 0; 8/16/32: original dir component was 0
+  int bits;             // 1/2/4: DDA direction > 0 on x/y/z
   uint64_t rng;         // Random rng of isProg
-  bool inCell;          // a Woodcock range is active
-  bool cellValid;       // DDA has a current cell
-  float t, tUpper, maj;
+  float t, tUpper, maj; // current Woodcock range
 };
 
 // Ray.h:170-181
@@ -255,15 +252,12 @@ DEV bool boxTest(float3 org, float3 dir, float &t0, float &t1, float3 lo, float3
 // Returns false if the ray has no cell to visit.  raySeed is advanced when
 // the box test passes (Random rng(ray.rngSeed, ...), MCAccelerator.h:592).
 DEV bool traceBegin(const VolumeDD &v, TraceState &ts, float3 org, float3 dir, float tMax, uint64_t &raySeed) {
-  int bits = 0;
-  if (dir.x == 0.f) { dir.x = 1e-6f; bits |= 8; }
-  if (dir.y == 0.f) { dir.y = 1e-6f; bits |= 16; }
-  if (dir.z == 0.f) { dir.z = 1e-6f; bits |= 32; }
+  if (dir.x == 0.f) dir.x = 1e-6f;
+  if (dir.y == 0.f) dir.y = 1e-6f;
+  if (dir.z == 0.f) dir.z = 1e-6f;
   ts.org = org;
   ts.dir = dir;
   ts.rayTMax = tMax;
-  ts.inCell = false;
-  ts.cellValid = false;
   float t0 = 0.f, t1 = tMax;
   if (!boxTest(org, dir, t0, t1, v.boundsLo, v.boundsHi)) return false;
   const float3 o = f3((org.x - v.mcOrigin.x) * v.rcpMcSpacing.x, (org.y - v.mcOrigin.y) * v.rcpMcSpacing.y,
@@ -291,14 +285,12 @@ DEV bool traceBegin(const VolumeDD &v, TraceState &ts, float3 org, float3 dir, f
   ts.tStep = f3(fabsf(rcpd.x), fabsf(rcpd.y), fabsf(rcpd.z));
   ts.tNext = f3(d.x == 0.f ? kInf : fabsf(fe.x - oi.x) * ts.tStep.x, d.y == 0.f ? kInf : fabsf(fe.y - oi.y) * ts.tStep.y,
                 d.z == 0.f ? kInf : fabsf(fe.z - oi.z) * ts.tStep.z);
-  bits |= (d.x > 0.f ? 1 : 0) | (d.y > 0.f ? 2 : 0) | (d.z > 0.f ? 4 : 0);
-  ts.bits = bits;
+  ts.bits = (d.x > 0.f ? 1 : 0) | (d.y > 0.f ? 2 : 0) | (d.z > 0.f ? 4 : 0);
   ts.cx = (int)fc.x;
   ts.cy = (int)fc.y;
   ts.cz = (int)fc.z;
   ts.rayT0 = ray_t0;
   ts.nextCellBegin = 0.f;
-  ts.cellValid = true;
   return true;
 }
 
@@ -416,280 +408,381 @@ DEV bool sampleLights(const FrameDD &fr, uint64_t &random, LightSample &ls, bool
 
 DEV float roundHalf(float x) { return __half2float(__float2half_rn(x)); }
 
-template <int T>
-__global__ void __launch_bounds__(kRenderMaxThreads, 4) renderKernel(VolumeDD v, FrameDD fr, LaunchCounters *ctr) {
-  extern __shared__ float4 sTF[];
-  __shared__ float u8lut[256];
-  for (int i = threadIdx.x; i < v.tfN; i += blockDim.x) sTF[i] = v.tf[i];
-  for (int i = threadIdx.x; i < 256; i += blockDim.x) u8lut[i] = (float)i * 1.f / 255.f;
-  __syncthreads();
+// Neumaier-compensated sum (precision forms): sum += x, error kept in c.
+DEV void neumaier(float &sum, float &c, float x) {
+  const float t = sum + x;
+  if (fabsf(sum) >= fabsf(x)) c += (sum - t) + x;
+  else c += (x - t) + sum;
+  sum = t;
+}
+DEV void accAdd(float &sum, float &c, float x, bool comp) {
+  if (comp) neumaier(sum, c, x);
+  else sum += x;
+}
 
+// Field sample of a job: compile-time voxel type, or (T < 0) the job's type.
+template <int T>
+DEV float sampleJob(const VolumeDD &v, float3 P, const float *u8lut) {
+  if (T >= 0) return sampleField<(T < 0 ? 0 : T)>(v, P, u8lut);
+  switch (v.type) {
+  case VOX_F32: return sampleField<VOX_F32>(v, P, u8lut);
+  case VOX_U8: return sampleField<VOX_U8>(v, P, u8lut);
+  case VOX_F16: return sampleField<VOX_F16>(v, P, u8lut);
+  default: return sampleField<VOX_BF16>(v, P, u8lut);
+  }
+}
+
+// Lane phases of the render loop.
+enum LanePhase : int {
+  LP_IDLE = 0,      // no pixel
+  LP_NEWSAMPLE = 1, // the next wave of its pixel needs a primary ray
+  LP_CELL = 2,      // a ray needs its next macrocell with a non-zero majorant
+  LP_WOODCOCK = 3,  // inside a Woodcock range
+  LP_HIT = 4,       // collision found, waiting to be shaded
+  LP_ENDED = 5      // ray left the grid (primary: background; shadow: reached the light)
+};
+
+constexpr int kChunk = 32;  // pixels a warp takes at a time (one 8x4 tile)
+
+// The render loop shared by the single-frame kernel (one job, read from a
+// __grid_constant__ parameter, TF staged in shared memory) and the batch
+// kernel (a job table in global memory, chunks of all jobs in one counter).
+template <int T, bool BATCH>
+DEV void renderLoop(const JobDD *jobs, const int *chunkStart, int numJobs, int numChunks, const SchedDD &sd,
+                    LaunchCounters *ctr, const float4 *sTF, const float *u8lut) {
+  const unsigned FULL = 0xffffffffu;
   const int lane = threadIdx.x & 31;
-  const int W = fr.width, H = fr.height;
-  const int tilesX = (W + 7) >> 3;
-  const int numTiles = tilesX * ((H + 3) >> 2);
-  const float aspect = W / float(H);
-  const float tfScale = (float)(v.tfN - 1);
-  const float span = v.domHi - v.domLo;
 
   unsigned long long nSamples = 0, nVisits = 0, nRays = 0;
   unsigned errBits = 0;
 
+  // warp-uniform work chunk
+  int chunkJob = 0, chunkBase = 0, chunkLeft = 0;
+  bool exhausted = false;
+
+  // lane state
+  int phase = LP_IDLE;
+  int job = 0, ix = 0, iy = 0, k = 0;
+  int64_t pix = 0;
+  float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
+  float4 comp = make_float4(0.f, 0.f, 0.f, 0.f);
+  TraceState ts;
+  uint64_t raySeed = 0;
+  float3 primDir = f3(0.f, 0.f, 0.f);
+  float4 bg = make_float4(0.f, 0.f, 0.f, 0.f);
+  float3 shadowTp = f3(0.f, 0.f, 0.f);
+  float3 hitRGB = f3(0.f, 0.f, 0.f);
+  float misWeight = 0.f;
+  bool shadowRay = false;
+  unsigned steps = 0;
+
   while (true) {
-    int tile = 0, abortReq = 0;
-    if (lane == 0) {
-      tile = (int)atomicAdd(&ctr->nextPixel, 1u);
-      abortReq = (int)*(volatile unsigned *)&ctr->abort;
+    // ------------------------------------------------------------------
+    // 1. lanes without a pixel take the next ones of the warp's chunk
+    // ------------------------------------------------------------------
+    unsigned need = __ballot_sync(FULL, phase == LP_IDLE);
+    while (need && !exhausted) {
+      if (chunkLeft == 0) {
+        int c = 0, ab = 0;
+        if (lane == 0) {
+          c = (int)atomicAdd(&ctr->nextPixel, 1u);
+          ab = (int)*(volatile unsigned *)&ctr->abort;
+        }
+        c = __shfl_sync(FULL, c, 0);
+        ab = __shfl_sync(FULL, ab, 0);
+        if (ab) { errBits |= ERR_ABORTED; exhausted = true; break; }
+        if (c >= numChunks) { exhausted = true; break; }
+        int j = 0;
+        if (BATCH) {  // last job whose first chunk is <= c
+          int lo = 0, hi = numJobs - 1;
+          while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (__ldg(chunkStart + mid) <= c) lo = mid; else hi = mid - 1;
+          }
+          j = lo;
+        }
+        const int first = BATCH ? __ldg(chunkStart + j) : 0;
+        const int npix = jobs[j].fr.width * jobs[j].fr.height;
+        chunkJob = j;
+        chunkBase = (c - first) * kChunk;
+        chunkLeft = min(kChunk, npix - chunkBase);
+      }
+      const int n = __popc(need);
+      const int take = min(n, chunkLeft);
+      const int rank = __popc(need & ((1u << lane) - 1u));
+      if (((need >> lane) & 1u) && rank < take) {
+        const FrameDD &fr = jobs[chunkJob].fr;
+        const int W = fr.width, H = fr.height;
+        // pixel order: 4-row bands, column-major inside a band (8x4 tiles per 32 pixels)
+        const int w = chunkBase + rank;
+        const int band = w / (4 * W);
+        const int rows = min(4, H - 4 * band);
+        const int within = w - band * 4 * W;
+        job = chunkJob;
+        ix = within / rows;
+        iy = 4 * band + within % rows;
+        pix = (int64_t)iy * W + ix;
+        k = 0;
+        acc = fr.accumID0 > 0 ? fr.accum[pix] : make_float4(0.f, 0.f, 0.f, 0.f);
+        comp = (fr.accumID0 > 0 && fr.comp) ? fr.comp[pix] : make_float4(0.f, 0.f, 0.f, 0.f);
+        phase = LP_NEWSAMPLE;
+      }
+      for (int i = 0; i < take; i++) need &= need - 1u;
+      chunkBase += take;
+      chunkLeft -= take;
     }
-    tile = __shfl_sync(0xffffffffu, tile, 0);
-    abortReq = __shfl_sync(0xffffffffu, abortReq, 0);
-    if (tile >= numTiles) break;
-    if (abortReq) { errBits |= ERR_ABORTED; break; }
-    const int ix = (tile % tilesX) * 8 + (lane & 7);
-    const int iy = (tile / tilesX) * 4 + (lane >> 3);
-    const bool active = ix < W && iy < H;
-    const int64_t pix = (int64_t)iy * W + ix;
+    if (!__ballot_sync(FULL, phase != LP_IDLE)) break;  // no work left for this warp
+    const int nWood = __popc(__ballot_sync(FULL, phase == LP_WOODCOCK));
+    const int nHit = __popc(__ballot_sync(FULL, phase == LP_HIT));
+    const int nNew = __popc(__ballot_sync(FULL, phase == LP_NEWSAMPLE));
+    const JobDD &J = jobs[BATCH ? job : 0];
+    const VolumeDD &v = J.v;
+    const FrameDD &fr = J.fr;
 
-    float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
-    if (active && fr.accumID0 > 0) acc = fr.accum[pix];
-    int k = 0;                    // wave index within this launch
-    int phase = active ? PH_NEWSAMPLE : PH_DONE;
-    TraceState ts;
-    ts.inCell = false;
-    ts.cellValid = false;
-    uint64_t raySeed = 0;
-    float3 primDir = f3(0.f, 0.f, 0.f);
-    float4 bg = make_float4(0.f, 0.f, 0.f, 0.f);
-    float3 shadowTp = f3(0.f, 0.f, 0.f);
-    float misWeight = 0.f;
-    unsigned steps = 0;
-
-    while (true) {
-      // ------------------------------------------------------------------
-      // control: find the next Woodcock range of this lane (or finish)
-      // ------------------------------------------------------------------
-      while (!ts.inCell && phase != PH_DONE) {
-        bool rayEnded = false;   // current ray left the grid without collision
-        if (phase == PH_NEWSAMPLE) {
-          // ---- generateRays.cu:71-243
-          const int accumID = fr.accumID0 + k;
-          uint64_t rnd = rngSeed2(unsigned(ix + W * accumID), unsigned(iy + H * accumID));
-          raySeed = rngSeed2((uint32_t)(ix + accumID * W), (uint32_t)iy);
-          const float pixel_u = (accumID == 0) ? .5f : rngFloat(rnd);
-          const float pixel_v = (accumID == 0) ? .5f : rngFloat(rnd);
-          const float image_u = ((ix + pixel_u) / float(W));
-          const float image_v = ((iy + pixel_v) / float(H));
-          const float su = 1.f * aspect * (image_u - .5f), sv = 1.f * (image_v - .5f);
-          float3 d = f3(fr.dir00.x + su * fr.dirdu.x + sv * fr.dirdv.x, fr.dir00.y + su * fr.dirdu.y + sv * fr.dirdv.y,
-                        fr.dir00.z + su * fr.dirdu.z + sv * fr.dirdv.z);
-          d = normalize3(d);
-          float3 o = fr.lens00;
-          float tMax = 1e30f;
-          if (fr.cutPlane.w > -1e28f) {
-            const float3 N = f3(fr.cutPlane.x, fr.cutPlane.y, fr.cutPlane.z);
-            const float dist_org = dot3(N, o) + fr.cutPlane.w;
-            const float denom = dot3(N, d);
-            if (dist_org >= 0.f) {
-              if (denom < 0.f) tMax = fmin_(tMax, -dist_org / denom);
-            } else {
-              if (denom > 0.f) {
-                const float te = -dist_org / denom;
-                o = f3(o.x + te * d.x, o.y + te * d.y, o.z + te * d.z);
-              } else tMax = 0.f;
-            }
-          }
-          if (fr.bgColor.w >= 0.f) bg = fr.bgColor;
-          else {
-            const float t = (iy + .5f) / float(H);
-            bg = make_float4((1.0f - t) * 0.9f + t * 0.15f, (1.0f - t) * 0.9f + t * 0.25f,
-                             (1.0f - t) * 0.9f + t * .8f, (1.0f - t) * 1.f + t * 1.f);
-          }
-          primDir = d;
-          nRays++;
-          steps = 0;
-          phase = PH_PRIMARY;
-          if (!traceBegin(v, ts, o, d, tMax, raySeed)) rayEnded = true;
-        } else if (ts.cellValid) {
-          // ---- enter the DDA's current cell (DDA.h:173-181, MCAccelerator.h:596-612)
-          const float tClosest = fmin_(fmin_(ts.tNext.x, ts.tNext.y), ts.tNext.z);
-          const float cell_t0 = ts.rayT0 + ts.nextCellBegin;
-          const float cell_t1 = ts.rayT0 + fmin_(tClosest, ts.ddaTMax);
-          const float maj = __ldg(v.majorants + (ts.cx + (int64_t)v.mcDims.x * (ts.cy + (int64_t)v.mcDims.y * ts.cz)));
-          nVisits++;
-          if (maj == 0.f) {
-            if (!ddaStep(v, ts, tClosest)) rayEnded = true;
-          } else {
-            ts.maj = maj;
-            ts.t = cell_t0;
-            ts.tUpper = fmin_(cell_t1, ts.rayTMax);
-            ts.inCell = true;
-          }
-        } else {
-          rayEnded = true;
+    // ------------------------------------------------------------------
+    // 2. one Woodcock step (Volume.h:180-201)
+    // ------------------------------------------------------------------
+    if (phase == LP_WOODCOCK) {
+      const float r = rngFloat(ts.rng);
+      const float dt = fr.exactLog ? (-logf(1.f - r) / ts.maj) : (-fastLog(1.f - r) / ts.maj);
+      ts.t += dt;
+      if (ts.t >= ts.tUpper) {
+        const float tClosest = fmin_(fmin_(ts.tNext.x, ts.tNext.y), ts.tNext.z);
+        phase = ddaStep(v, ts, tClosest) ? LP_CELL : LP_ENDED;
+      } else {
+        const float3 P = f3(ts.org.x + ts.t * ts.dir.x, ts.org.y + ts.t * ts.dir.y, ts.org.z + ts.t * ts.dir.z);
+        const float s = sampleJob<T>(v, P, u8lut);
+        nSamples++;
+        float w = 0.f, f = 0.f;
+        int idx = 0;
+        if (!isnan(s)) {
+          const float span = v.domHi - v.domLo;
+          f = (s - v.domLo) / span;
+          f = fmin_(1.f, fmax_(0.f, f));
+          f *= (float)(v.tfN - 1);
+          idx = min(v.tfN - 2, max(0, (int)f));
+          f -= (float)idx;
+          const float w0 = BATCH ? __ldg(&v.tf[idx].w) : sTF[idx].w;
+          const float w1 = BATCH ? __ldg(&v.tf[idx + 1].w) : sTF[idx + 1].w;
+          w = ((1.f - f) * w0 + f * w1) * v.baseDensity;
         }
-        if (rayEnded) {
-          ts.cellValid = false;
-          // ---- bounce() for a ray without intersection (shadeRays.cu:507-600)
-          const int accumID = fr.accumID0 + k;
-          const float clampMax = 10.f * (1 + accumID);
-          if (phase == PH_PRIMARY) {
-            const float f0x = fmin_(bg.x, clampMax), f0y = fmin_(bg.y, clampMax), f0z = fmin_(bg.z, clampMax);
-            if (accumID == 0) acc = make_float4(f0x, f0y, f0z, bg.w);
-            else {
-              if (bg.w > 0.f) acc.w += bg.w;
-              if (f0x > 0.f) acc.x += f0x;
-              if (f0y > 0.f) acc.y += f0y;
-              if (f0z > 0.f) acc.z += f0z;
-            }
-          } else {  // shadow ray reached the light
-            const float f1x = fmin_(misWeight * shadowTp.x, clampMax);
-            const float f1y = fmin_(misWeight * shadowTp.y, clampMax);
-            const float f1z = fmin_(misWeight * shadowTp.z, clampMax);
-            if (f1x > 0.f) acc.x += f1x;
-            if (f1y > 0.f) acc.y += f1y;
-            if (f1z > 0.f) acc.z += f1z;
-          }
-          if (++k == fr.spp) phase = PH_DONE;
-          else phase = PH_NEWSAMPLE;
-        }
-      }
-      if (phase == PH_DONE) break;
-
-      // ------------------------------------------------------------------
-      // one Woodcock step (Volume.h:180-201)
-      // ------------------------------------------------------------------
-      bool hit = false;
-      float4 sample = make_float4(0.f, 0.f, 0.f, 0.f);
-      {
-        const float r = rngFloat(ts.rng);
-        const float dt = fr.exactLog ? (-logf(1.f - r) / ts.maj) : (-fastLog(1.f - r) / ts.maj);
-        ts.t += dt;
-        if (ts.t >= ts.tUpper) {
-          ts.inCell = false;
-          const float tClosest = fmin_(fmin_(ts.tNext.x, ts.tNext.y), ts.tNext.z);
-          if (!ddaStep(v, ts, tClosest)) ts.cellValid = false;
-        } else {
-          const float3 P = f3(ts.org.x + ts.t * ts.dir.x, ts.org.y + ts.t * ts.dir.y, ts.org.z + ts.t * ts.dir.z);
-          const float s = sampleField<T>(v, P, u8lut);
-          nSamples++;
-          float w = 0.f;
-          int idx = 0;
-          float f = 0.f;
+        if (w >= rngFloat(ts.rng) * ts.maj) {
+          hitRGB = f3(0.f, 0.f, 0.f);
           if (!isnan(s)) {
-            f = (s - v.domLo) / span;
-            f = fmin_(1.f, fmax_(0.f, f));
-            f *= tfScale;
-            idx = min(v.tfN - 2, max(0, (int)f));
-            f -= (float)idx;
-            w = ((1.f - f) * sTF[idx].w + f * sTF[idx + 1].w) * v.baseDensity;
+            const float4 a = BATCH ? __ldg(&v.tf[idx]) : sTF[idx];
+            const float4 b = BATCH ? __ldg(&v.tf[idx + 1]) : sTF[idx + 1];
+            hitRGB = f3((1.f - f) * a.x + f * b.x, (1.f - f) * a.y + f * b.y, (1.f - f) * a.z + f * b.z);
           }
-          if (w >= rngFloat(ts.rng) * ts.maj) {
-            hit = true;
-            if (!isnan(s)) {
-              const float4 a = sTF[idx], b = sTF[idx + 1];
-              sample = make_float4((1.f - f) * a.x + f * b.x, (1.f - f) * a.y + f * b.y, (1.f - f) * a.z + f * b.z, w);
-            }
-          }
-        }
-        if (++steps > (1u << 22)) {  // iteration cap: terminate this ray as a miss
-          errBits |= ERR_ITER_CAP;
-          ts.inCell = false;
-          ts.cellValid = false;
+          phase = LP_HIT;
         }
       }
-      if (!hit) continue;
+      if (++steps > (1u << 22)) {  // iteration cap: end this ray as if it left the grid
+        errBits |= ERR_ITER_CAP;
+        phase = LP_ENDED;
+      }
+    }
 
-      // ------------------------------------------------------------------
-      // collision: shade (primary) or occlusion (shadow)
-      // ------------------------------------------------------------------
-      ts.inCell = false;
-      ts.cellValid = false;
+    // ------------------------------------------------------------------
+    // 3. rays that left the grid: bounce() without intersection
+    //    (shadeRays.cu:507-600) and accumulation (:996-1040)
+    // ------------------------------------------------------------------
+    if (phase == LP_ENDED) {
       const int accumID = fr.accumID0 + k;
       const float clampMax = 10.f * (1 + accumID);
-      if (phase == PH_SHADOW) {  // occluded: no contribution
-        if (++k == fr.spp) phase = PH_DONE;
-        else phase = PH_NEWSAMPLE;
-        continue;
-      }
-      // primary hit: generation-0 accumulation (fragment 0, alpha 1)
-      if (accumID == 0) acc = make_float4(0.f, 0.f, 0.f, 1.f);
-      else acc.w += 1.f;
-      const float tHit = ts.t;
-      const float3 P = f3(ts.org.x + tHit * ts.dir.x, ts.org.y + tHit * ts.dir.y, ts.org.z + tHit * ts.dir.z);
-      bool spawned = false;
-      if (fr.emissionAbsorption) {
-        const float ex = fmin_(sample.x, clampMax), ey = fmin_(sample.y, clampMax), ez = fmin_(sample.z, clampMax);
-        if (accumID == 0) acc = make_float4(ex, ey, ez, 1.f);
-        else {
-          if (ex > 0.f) acc.x += ex;
-          if (ey > 0.f) acc.y += ey;
-          if (ez > 0.f) acc.z += ez;
+      const bool cmp = fr.comp != nullptr;
+      if (!shadowRay) {
+        const float f0x = fmin_(bg.x, clampMax), f0y = fmin_(bg.y, clampMax), f0z = fmin_(bg.z, clampMax);
+        if (accumID == 0) {
+          acc = make_float4(f0x, f0y, f0z, bg.w);
+          comp = make_float4(0.f, 0.f, 0.f, 0.f);
+        } else {
+          if (bg.w > 0.f) accAdd(acc.w, comp.w, bg.w, cmp);
+          if (f0x > 0.f) accAdd(acc.x, comp.x, f0x, cmp);
+          if (f0y > 0.f) accAdd(acc.y, comp.y, f0y, cmp);
+          if (f0z > 0.f) accAdd(acc.z, comp.z, f0z, cmp);
         }
+      } else {  // the shadow ray reached the light
+        const float f1x = fmin_(misWeight * shadowTp.x, clampMax);
+        const float f1y = fmin_(misWeight * shadowTp.y, clampMax);
+        const float f1z = fmin_(misWeight * shadowTp.z, clampMax);
+        if (f1x > 0.f) accAdd(acc.x, comp.x, f1x, cmp);
+        if (f1y > 0.f) accAdd(acc.y, comp.y, f1y, cmp);
+        if (f1z > 0.f) accAdd(acc.z, comp.z, f1z, cmp);
+      }
+      if (++k == fr.spp) {
+        fr.accum[pix] = acc;
+        if (cmp) fr.comp[pix] = comp;
+        phase = LP_IDLE;
       } else {
-        // bounce() volume-hit branch, shadeRays.cu:608-746
-        uint64_t random = rngDerive(raySeed, (uint64_t)__float_as_uint(tHit));
-        const float3 won = normalize3(primDir);
-        const float3 woN = f3(-won.x, -won.y, -won.z);  // dg.wo
-        const float offsetEpsilon = fmax_(1e-4f, 1e-6f * fmax_(fmax_(fabsf(P.x), fabsf(P.y)), fabsf(P.z)));
-        LightSample ls;
-        bool needsMIS, isDir;
-        if (sampleLights(fr, random, ls, needsMIS, isDir)) {
-          float3 alb;
-          float fpdf;
-          if (v.phase == PHASE_SIMPLE) {
-            alb = f3(.7f * sample.x, .7f * sample.y, .7f * sample.z);
-            fpdf = kOneOverFourPi;
-          } else {
-            alb = f3(v.scatteringAlbedo * sample.x, v.scatteringAlbedo * sample.y, v.scatteringAlbedo * sample.z);
-            const float3 wi_in = normalize3(f3(-woN.x, -woN.y, -woN.z));
-            fpdf = hgPhase(v.anisotropy, dot3(wi_in, normalize3(ls.dir)));
-          }
-          float3 fv = f3(fpdf * alb.x, fpdf * alb.y, fpdf * alb.z);
-          if (fpdf > 0.f && !(fmax_(fmax_(fv.x, fv.y), fv.z) < 1e-4f)) {
-            fv = f3(fmin_(fv.x, 13.f), fmin_(fv.y, 13.f), fmin_(fv.z, 13.f));
-            const float ip = isinf(ls.pdf) ? 1.f : (1.f / ls.pdf);
-            const float3 tp = f3(1.f * ip * fv.x * ls.radiance.x * 1.f, 1.f * ip * fv.y * ls.radiance.y * 1.f,
-                                 1.f * ip * fv.z * ls.radiance.z * 1.f);
-            misWeight = 1.f;
-            bool alive = true;
-            if (!isDir && needsMIS) {
-              const float pl = kOneOverFourPi;
-              float ps;
-              if (v.phase == PHASE_SIMPLE) ps = kOneOverFourPi;
-              else ps = hgPhase(v.anisotropy, dot3(normalize3(f3(-woN.x, -woN.y, -woN.z)), normalize3(ls.dir)));
-              misWeight = pl / (pl + ps + 1e-10f);
-              if (misWeight < 1e-5f) alive = false;
-            }
-            const float sTMax = kInf * (1.f - 2.f * offsetEpsilon);
-            if (alive && sTMax > 0.f) {
-              shadowTp = f3(roundHalf(tp.x), roundHalf(tp.y), roundHalf(tp.z));
-              const float3 so = f3(P.x + offsetEpsilon * woN.x, P.y + offsetEpsilon * woN.y, P.z + offsetEpsilon * woN.z);
-              uint64_t shadowSeed = raySeed;
-              phase = PH_SHADOW;
-              spawned = true;
-              nRays++;
-              steps = 0;
-              traceBegin(v, ts, so, ls.dir, sTMax, shadowSeed);
-              // a shadow ray with no cell to visit is handled as reaching the light
-            }
-          }
-        }
-      }
-      if (!spawned) {
-        if (++k == fr.spp) phase = PH_DONE;
-        else phase = PH_NEWSAMPLE;
+        phase = LP_NEWSAMPLE;
       }
     }
-    if (active) fr.accum[pix] = acc;
-    __syncwarp();
+
+    // ------------------------------------------------------------------
+    // 4. collisions, shaded together once enough lanes have one
+    // ------------------------------------------------------------------
+    const bool doShade = nHit > 0 && (nHit >= sd.shadeBatch || nWood < sd.minBusy);
+    if (doShade && phase == LP_HIT) {
+      const int accumID = fr.accumID0 + k;
+      const float clampMax = 10.f * (1 + accumID);
+      const bool cmp = fr.comp != nullptr;
+      bool spawned = false;
+      if (!shadowRay) {
+        // primary hit: generation-0 accumulation (fragment 0, alpha 1)
+        if (accumID == 0) {
+          acc = make_float4(0.f, 0.f, 0.f, 1.f);
+          comp = make_float4(0.f, 0.f, 0.f, 0.f);
+        } else {
+          accAdd(acc.w, comp.w, 1.f, cmp);
+        }
+        const float tHit = ts.t;
+        const float3 P = f3(ts.org.x + tHit * ts.dir.x, ts.org.y + tHit * ts.dir.y, ts.org.z + tHit * ts.dir.z);
+        if (fr.emissionAbsorption) {
+          const float ex = fmin_(hitRGB.x, clampMax), ey = fmin_(hitRGB.y, clampMax), ez = fmin_(hitRGB.z, clampMax);
+          if (accumID == 0) acc = make_float4(ex, ey, ez, 1.f);
+          else {
+            if (ex > 0.f) accAdd(acc.x, comp.x, ex, cmp);
+            if (ey > 0.f) accAdd(acc.y, comp.y, ey, cmp);
+            if (ez > 0.f) accAdd(acc.z, comp.z, ez, cmp);
+          }
+        } else {
+          // bounce() volume-hit branch, shadeRays.cu:608-746
+          uint64_t random = rngDerive(raySeed, (uint64_t)__float_as_uint(tHit));
+          const float3 won = normalize3(primDir);
+          const float3 woN = f3(-won.x, -won.y, -won.z);  // dg.wo
+          const float offsetEpsilon = fmax_(1e-4f, 1e-6f * fmax_(fmax_(fabsf(P.x), fabsf(P.y)), fabsf(P.z)));
+          LightSample ls;
+          bool needsMIS, isDir;
+          if (sampleLights(fr, random, ls, needsMIS, isDir)) {
+            float3 alb;
+            float fpdf;
+            if (v.phase == PHASE_SIMPLE) {
+              alb = f3(.7f * hitRGB.x, .7f * hitRGB.y, .7f * hitRGB.z);
+              fpdf = kOneOverFourPi;
+            } else {
+              alb = f3(v.scatteringAlbedo * hitRGB.x, v.scatteringAlbedo * hitRGB.y, v.scatteringAlbedo * hitRGB.z);
+              const float3 wi_in = normalize3(f3(-woN.x, -woN.y, -woN.z));
+              fpdf = hgPhase(v.anisotropy, dot3(wi_in, normalize3(ls.dir)));
+            }
+            float3 fv = f3(fpdf * alb.x, fpdf * alb.y, fpdf * alb.z);
+            if (fpdf > 0.f && !(fmax_(fmax_(fv.x, fv.y), fv.z) < 1e-4f)) {
+              fv = f3(fmin_(fv.x, 13.f), fmin_(fv.y, 13.f), fmin_(fv.z, 13.f));
+              const float ip = isinf(ls.pdf) ? 1.f : (1.f / ls.pdf);
+              const float3 tp = f3(1.f * ip * fv.x * ls.radiance.x * 1.f, 1.f * ip * fv.y * ls.radiance.y * 1.f,
+                                   1.f * ip * fv.z * ls.radiance.z * 1.f);
+              misWeight = 1.f;
+              bool alive = true;
+              if (!isDir && needsMIS) {
+                const float pl = kOneOverFourPi;
+                float ps;
+                if (v.phase == PHASE_SIMPLE) ps = kOneOverFourPi;
+                else ps = hgPhase(v.anisotropy, dot3(normalize3(f3(-woN.x, -woN.y, -woN.z)), normalize3(ls.dir)));
+                misWeight = pl / (pl + ps + 1e-10f);
+                if (misWeight < 1e-5f) alive = false;
+              }
+              const float sTMax = kInf * (1.f - 2.f * offsetEpsilon);
+              if (alive && sTMax > 0.f) {
+                shadowTp = f3(roundHalf(tp.x), roundHalf(tp.y), roundHalf(tp.z));
+                const float3 so =
+                    f3(P.x + offsetEpsilon * woN.x, P.y + offsetEpsilon * woN.y, P.z + offsetEpsilon * woN.z);
+                uint64_t shadowSeed = raySeed;
+                shadowRay = true;
+                spawned = true;
+                nRays++;
+                steps = 0;
+                phase = traceBegin(v, ts, so, ls.dir, sTMax, shadowSeed) ? LP_CELL : LP_ENDED;
+              }
+            }
+          }
+        }
+      }
+      if (!spawned) {  // shadow ray occluded, or no shadow ray: the wave is done
+        if (++k == fr.spp) {
+          fr.accum[pix] = acc;
+          if (cmp) fr.comp[pix] = comp;
+          phase = LP_IDLE;
+        } else {
+          phase = LP_NEWSAMPLE;
+        }
+      }
+    }
+
+    // ------------------------------------------------------------------
+    // 5. primary rays, generated together once enough lanes need one
+    //    (generateRays.cu:71-243)
+    // ------------------------------------------------------------------
+    const bool doGen = nNew > 0 && (nNew >= sd.genBatch || nWood < sd.minBusy);
+    if (doGen && phase == LP_NEWSAMPLE) {
+      const int W = fr.width, H = fr.height;
+      const int accumID = fr.accumID0 + k;
+      uint64_t rnd = rngSeed2(unsigned(ix + W * accumID), unsigned(iy + H * accumID));
+      raySeed = rngSeed2((uint32_t)(ix + accumID * W), (uint32_t)iy);
+      const float pixel_u = (accumID == 0) ? .5f : rngFloat(rnd);
+      const float pixel_v = (accumID == 0) ? .5f : rngFloat(rnd);
+      const float image_u = ((ix + pixel_u) / float(W));
+      const float image_v = ((iy + pixel_v) / float(H));
+      const float aspect = W / float(H);
+      const float su = 1.f * aspect * (image_u - .5f), sv = 1.f * (image_v - .5f);
+      float3 d = f3(fr.dir00.x + su * fr.dirdu.x + sv * fr.dirdv.x, fr.dir00.y + su * fr.dirdu.y + sv * fr.dirdv.y,
+                    fr.dir00.z + su * fr.dirdu.z + sv * fr.dirdv.z);
+      d = normalize3(d);
+      float3 o = fr.lens00;
+      float tMax = 1e30f;
+      if (fr.cutPlane.w > -1e28f) {
+        const float3 N = f3(fr.cutPlane.x, fr.cutPlane.y, fr.cutPlane.z);
+        const float dist_org = dot3(N, o) + fr.cutPlane.w;
+        const float denom = dot3(N, d);
+        if (dist_org >= 0.f) {
+          if (denom < 0.f) tMax = fmin_(tMax, -dist_org / denom);
+        } else {
+          if (denom > 0.f) {
+            const float te = -dist_org / denom;
+            o = f3(o.x + te * d.x, o.y + te * d.y, o.z + te * d.z);
+          } else tMax = 0.f;
+        }
+      }
+      if (fr.bgColor.w >= 0.f) bg = fr.bgColor;
+      else {
+        const float t = (iy + .5f) / float(H);
+        bg = make_float4((1.0f - t) * 0.9f + t * 0.15f, (1.0f - t) * 0.9f + t * 0.25f, (1.0f - t) * 0.9f + t * .8f,
+                         (1.0f - t) * 1.f + t * 1.f);
+      }
+      primDir = d;
+      shadowRay = false;
+      nRays++;
+      steps = 0;
+      phase = traceBegin(v, ts, o, d, tMax, raySeed) ? LP_CELL : LP_ENDED;
+    }
+
+    // ------------------------------------------------------------------
+    // 6. next macrocell with a non-zero majorant (DDA.h:172-200,
+    //    MCAccelerator.h:596-612)
+    // ------------------------------------------------------------------
+    if (phase == LP_CELL) {
+      while (true) {
+        const float tClosest = fmin_(fmin_(ts.tNext.x, ts.tNext.y), ts.tNext.z);
+        const float maj = __ldg(v.majorants + (ts.cx + (int64_t)v.mcDims.x * (ts.cy + (int64_t)v.mcDims.y * ts.cz)));
+        nVisits++;
+        if (maj == 0.f) {
+          if (!ddaStep(v, ts, tClosest)) { phase = LP_ENDED; break; }
+          if (++steps > (1u << 22)) { errBits |= ERR_ITER_CAP; phase = LP_ENDED; break; }
+        } else {
+          ts.maj = maj;
+          ts.t = ts.rayT0 + ts.nextCellBegin;
+          ts.tUpper = fmin_(ts.rayT0 + fmin_(tClosest, ts.ddaTMax), ts.rayTMax);
+          phase = LP_WOODCOCK;
+          break;
+        }
+      }
+    }
   }
 
   // counters: warp reduction, one atomic per warp
   for (int o = 16; o > 0; o >>= 1) {
-    nSamples += __shfl_down_sync(0xffffffffu, nSamples, o);
-    nVisits += __shfl_down_sync(0xffffffffu, nVisits, o);
-    nRays += __shfl_down_sync(0xffffffffu, nRays, o);
-    errBits |= __shfl_down_sync(0xffffffffu, errBits, o);
+    nSamples += __shfl_down_sync(FULL, nSamples, o);
+    nVisits += __shfl_down_sync(FULL, nVisits, o);
+    nRays += __shfl_down_sync(FULL, nRays, o);
+    errBits |= __shfl_down_sync(FULL, errBits, o);
   }
   if (lane == 0) {
     atomicAdd(&ctr->samples, nSamples);
@@ -697,6 +790,27 @@ __global__ void __launch_bounds__(kRenderMaxThreads, 4) renderKernel(VolumeDD v,
     atomicAdd(&ctr->rays, nRays);
     if (errBits) atomicOr(&ctr->errorFlags, (unsigned long long)errBits);
   }
+}
+
+template <int T>
+__global__ void __launch_bounds__(kRenderMaxThreads, 4)
+    renderKernel(const __grid_constant__ JobDD job, const __grid_constant__ SchedDD sd, LaunchCounters *ctr) {
+  extern __shared__ float4 sTF[];
+  __shared__ float u8lut[256];
+  for (int i = threadIdx.x; i < job.v.tfN; i += blockDim.x) sTF[i] = job.v.tf[i];
+  for (int i = threadIdx.x; i < 256; i += blockDim.x) u8lut[i] = (float)i * 1.f / 255.f;
+  __syncthreads();
+  const int numChunks = (job.fr.width * job.fr.height + kChunk - 1) / kChunk;
+  renderLoop<T, false>(&job, nullptr, 1, numChunks, sd, ctr, sTF, u8lut);
+}
+
+__global__ void __launch_bounds__(kRenderMaxThreads, 4)
+    renderBatchKernel(const JobDD *jobs, const int *chunkStart, int numJobs, const __grid_constant__ SchedDD sd,
+                      LaunchCounters *ctr) {
+  __shared__ float u8lut[256];
+  for (int i = threadIdx.x; i < 256; i += blockDim.x) u8lut[i] = (float)i * 1.f / 255.f;
+  __syncthreads();
+  renderLoop<-1, true>(jobs, chunkStart, numJobs, __ldg(chunkStart + numJobs), sd, ctr, nullptr, u8lut);
 }
 
 // ---------------------------------------------------------------------------
@@ -708,15 +822,54 @@ DEV float linearToSrgb(float x) {
 }
 DEV uint32_t make8(float f) { return (uint32_t)min(255, max(0, int(f * 256.f))); }
 
-__global__ void resolveKernel(const float4 *accum, int n, float accumScale, int fmt, void *out) {
+__global__ void resolveKernel(const float4 *accum, const float4 *comp, int n, float accumScale, int fmt, void *out) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     float4 a = accum[i];
+    if (comp) {  // compensated accumulation: add the running error back before scaling
+      const float4 c = comp[i];
+      a = make_float4(a.x + c.x, a.y + c.y, a.z + c.z, a.w + c.w);
+    }
     float4 c = make_float4(a.x * accumScale, a.y * accumScale, a.z * accumScale, a.w * accumScale);
     if (fmt == FMT_FLOAT4) {
       ((float4 *)out)[i] = c;
     } else {
       if (fmt == FMT_RGBA8_SRGB) { c.x = linearToSrgb(c.x); c.y = linearToSrgb(c.y); c.z = linearToSrgb(c.z); }
       ((uint32_t *)out)[i] = (make8(c.x) << 0) + (make8(c.y) << 8) + (make8(c.z) << 16) + (make8(c.w) << 24);
+    }
+  }
+}
+
+// batch resolve: one 32-thread group per pixel chunk of any job
+__global__ void resolveBatchKernel(const JobDD *jobs, const int *chunkStart, int numJobs, int numChunks) {
+  const int groupsPerBlock = blockDim.x / 32;
+  const int sub = threadIdx.x & 31;
+  for (int c = blockIdx.x * groupsPerBlock + threadIdx.x / 32; c < numChunks; c += gridDim.x * groupsPerBlock) {
+    int lo = 0, hi = numJobs - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (__ldg(chunkStart + mid) <= c) lo = mid; else hi = mid - 1;
+    }
+    const FrameDD &fr = jobs[lo].fr;
+    const int i = (c - __ldg(chunkStart + lo)) * 32 + sub;
+    if (i >= fr.width * fr.height) continue;
+    // pixel i of the chunk order maps to the same pixel as in the render loop
+    const int W = fr.width, H = fr.height;
+    const int band = i / (4 * W);
+    const int rows = min(4, H - 4 * band);
+    const int within = i - band * 4 * W;
+    const int64_t p = (int64_t)(4 * band + within % rows) * W + within / rows;
+    float4 a = fr.accum[p];
+    if (fr.comp) {
+      const float4 cc = fr.comp[p];
+      a = make_float4(a.x + cc.x, a.y + cc.y, a.z + cc.z, a.w + cc.w);
+    }
+    const float accumScale = 1.f / (fr.accumID0 + fr.spp);
+    float4 col = make_float4(a.x * accumScale, a.y * accumScale, a.z * accumScale, a.w * accumScale);
+    if (fr.colorFormat == FMT_FLOAT4) {
+      ((float4 *)fr.color)[p] = col;
+    } else {
+      if (fr.colorFormat == FMT_RGBA8_SRGB) { col.x = linearToSrgb(col.x); col.y = linearToSrgb(col.y); col.z = linearToSrgb(col.z); }
+      ((uint32_t *)fr.color)[p] = (make8(col.x) << 0) + (make8(col.y) << 8) + (make8(col.z) << 16) + (make8(col.w) << 24);
     }
   }
 }
@@ -754,8 +907,8 @@ cudaError_t launchMapMajorants(const VolumeDD &v, const float2 *ranges, float *m
 }
 
 template <int T>
-static cudaError_t launchRenderT(const VolumeDD &v, const FrameDD &fr, LaunchCounters *ctr, int bps, int tpb,
-                                 cudaStream_t s) {
+static cudaError_t launchRenderT(const VolumeDD &v, const FrameDD &fr, const SchedDD &sd, LaunchCounters *ctr,
+                                 int bps, int tpb, cudaStream_t s) {
   const size_t smem = (size_t)v.tfN * sizeof(float4);
   auto kern = renderKernel<T>;
   if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -764,24 +917,47 @@ static cudaError_t launchRenderT(const VolumeDD &v, const FrameDD &fr, LaunchCou
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, tpb, smem);
     bps = occ > 0 ? occ : 1;
   }
-  kern<<<smCount() * bps, tpb, smem, s>>>(v, fr, ctr);
+  JobDD job;
+  job.v = v;
+  job.fr = fr;
+  kern<<<smCount() * bps, tpb, smem, s>>>(job, sd, ctr);
   return cudaGetLastError();
 }
 
-cudaError_t launchRender(const VolumeDD &v, const FrameDD &fr, LaunchCounters *ctr, int bps, int tpb, cudaStream_t s) {
+cudaError_t launchRender(const VolumeDD &v, const FrameDD &fr, LaunchCounters *ctr, int bps, int tpb, cudaStream_t s,
+                         const SchedDD &sd) {
   if (tpb <= 0) tpb = 128;
   switch (v.type) {
-  case VOX_F32: return launchRenderT<VOX_F32>(v, fr, ctr, bps, tpb, s);
-  case VOX_U8: return launchRenderT<VOX_U8>(v, fr, ctr, bps, tpb, s);
-  case VOX_F16: return launchRenderT<VOX_F16>(v, fr, ctr, bps, tpb, s);
-  default: return launchRenderT<VOX_BF16>(v, fr, ctr, bps, tpb, s);
+  case VOX_F32: return launchRenderT<VOX_F32>(v, fr, sd, ctr, bps, tpb, s);
+  case VOX_U8: return launchRenderT<VOX_U8>(v, fr, sd, ctr, bps, tpb, s);
+  case VOX_F16: return launchRenderT<VOX_F16>(v, fr, sd, ctr, bps, tpb, s);
+  default: return launchRenderT<VOX_BF16>(v, fr, sd, ctr, bps, tpb, s);
   }
 }
 
-cudaError_t launchResolve(const float4 *accum, int n, int accumID, int fmt, void *out, cudaStream_t s) {
+cudaError_t launchRenderBatch(const JobDD *jobs, const int *chunkStart, int numJobs, LaunchCounters *ctr, int bps,
+                              int tpb, cudaStream_t s, const SchedDD &sd) {
+  if (tpb <= 0) tpb = 128;
+  if (bps <= 0) {
+    int occ = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, renderBatchKernel, tpb, 0);
+    bps = occ > 0 ? occ : 1;
+  }
+  renderBatchKernel<<<smCount() * bps, tpb, 0, s>>>(jobs, chunkStart, numJobs, sd, ctr);
+  return cudaGetLastError();
+}
+
+cudaError_t launchResolveBatch(const JobDD *jobs, const int *chunkStart, int numJobs, int numChunks, cudaStream_t s) {
+  const int blocks = std::max(1, std::min((numChunks + 7) / 8, smCount() * 8));
+  resolveBatchKernel<<<blocks, 256, 0, s>>>(jobs, chunkStart, numJobs, numChunks);
+  return cudaGetLastError();
+}
+
+cudaError_t launchResolve(const float4 *accum, int n, int accumID, int fmt, void *out, cudaStream_t s,
+                          const float4 *comp) {
   const float accumScale = 1.f / accumID;
   const int blocks = std::max(1, std::min((n + 255) / 256, smCount() * 8));
-  resolveKernel<<<blocks, 256, 0, s>>>(accum, n, accumScale, fmt, out);
+  resolveKernel<<<blocks, 256, 0, s>>>(accum, comp, n, accumScale, fmt, out);
   return cudaGetLastError();
 }
 

@@ -229,3 +229,34 @@ def config2(n=512, width=1920, height=1080, spp=64, dtype="f32", vol=None, xp=np
               scattering_albedo=0.8)
     d["spp"] = spp
     return d
+
+
+def config4_jobs(n_jobs=64, xp=np, device=None):
+    """The batching workload: job i draws from default_rng(i) a volume edge
+    log-uniform in [32, 256], a field (Gaussian blobs or value noise, seeded
+    by i), a storage type from {u8, f16, f32}, an image side log-uniform in
+    [128, 1024], spp from {1, 4, 16, 32} and an orbit camera (azimuth
+    U[0, 2pi), elevation U[-30, 60] degrees, radius 2.5 about the cube
+    centre).  Blob jobs use the config-1 look (linear TF, ambient 1, default
+    single scatter); noise jobs the config-2 look (knot TF, HG albedo 0.8,
+    directional light + ambient 0.25)."""
+    jobs = []
+    for i in range(n_jobs):
+        rng = np.random.default_rng(i)
+        edge = int(round(math.exp(rng.uniform(math.log(32), math.log(256)))))
+        field = "blobs" if rng.integers(2) == 0 else "noise"
+        dtype = ["u8", "f16", "f32"][int(rng.integers(3))]
+        side = int(round(math.exp(rng.uniform(math.log(128), math.log(1024)))))
+        spp = [1, 4, 16, 32][int(rng.integers(4))]
+        cam = orbit_camera(rng)
+        if field == "blobs":
+            vol = to_storage(blobs(edge, i, xp=xp, device=device), dtype)
+            d = scene(vol, dtype, side, side, tf_linear_ramp(128), 50.0, cam, ambient=1.0)
+        else:
+            vol = to_storage(value_noise(edge, i, xp=xp, device=device), dtype)
+            d = config2(vol=vol, dtype=dtype, width=side, height=side, spp=spp)
+            d["camera"] = cam
+        d["spp"] = spp
+        d["field"] = field
+        jobs.append(d)
+    return jobs

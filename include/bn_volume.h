@@ -215,6 +215,32 @@ BN_API void bnxSetStream(BNContext context, void *cudaStream);
 BN_API void *bnxGetStream(BNContext context);
 /* Launch parameters of the render kernel (0 = automatic). */
 BN_API void bnxSetLaunchConfig(BNContext context, int blocksPerSM, int threadsPerBlock);
+/* Warp scheduling of the render kernel: a warp generates primary rays once
+   genBatch of its lanes need one and shades collisions once shadeBatch lanes
+   have one, or as soon as fewer than minBusy lanes are inside a Woodcock
+   range (defaults 16, 8, 8). */
+BN_API void bnxSetScheduling(BNContext context, int genBatch, int shadeBatch, int minBusy);
+/* Render several jobs in one persistent launch (each job: renderer, model,
+   camera, frame buffer of this context; distinct frame buffers).  Same
+   result as one bnRender per job, bit for bit.  The launch sequence is
+   captured into a CUDA graph per batch shape and replayed (see
+   bnxSetBatchGraphs). */
+typedef struct {
+  BNRenderer renderer;
+  BNModel model;
+  BNCamera camera;
+  BNFrameBuffer frameBuffer;
+} BNXRenderJob;
+BN_API void bnxRenderBatch(BNContext context, const BNXRenderJob *jobs, int numJobs);
+BN_API void bnxSetBatchGraphs(BNContext context, int enable);
+/* Times candidate launch shapes and scheduling thresholds on this batch,
+   keeps the fastest for the context and reports it.  The tuning frames are
+   rendered into the jobs' frame buffers and discarded (accumulation reset). */
+typedef struct {
+  int threadsPerBlock, blocksPerSM, genBatch, shadeBatch, minBusy;
+  float renderMs;
+} BNXLaunchConfig;
+BN_API void bnxAutotuneBatch(BNContext context, const BNXRenderJob *jobs, int numJobs, BNXLaunchConfig *best);
 /* Device pointer of the resolved colour channel of a frame buffer. */
 BN_API void *bnxFrameBufferDevicePointer(BNFrameBuffer fb);
 /* Device copies of the macrocell grid of a volume after bnGroupBuild:

@@ -128,3 +128,86 @@ def test_invalid_calls_record_errors():
     assert L.bnGetLastError() == 2
     L.bnClearLastError()
     r.close()
+
+
+def test_scheduling_thresholds_do_not_change_results():
+    bn = _bn()
+    d = small_noise_scene(n=40, w=48, h=40)
+    r = bn.VolumeRenderer(d)
+    r.set_spp(3)
+    r.render()
+    a = r.read().copy()
+    for gen, shade, busy in [(1, 1, 0), (32, 32, 32), (8, 16, 4)]:
+        r.accum_reset()
+        r.set_scheduling(gen, shade, busy)
+        r.render()
+        assert_bitexact(r.read(), a, f"sched {gen}/{shade}/{busy}")
+    r.close()
+
+
+BATCH = [
+    (lambda: small_noise_scene(n=40, w=48, h=32), 3),
+    (lambda: small_blob_scene(n=24, w=40, h=36), 2),
+    (lambda: small_noise_scene(n=33, w=37, h=29, dtype="u8", phase="simple"), 4),
+    (lambda: small_blob_scene(n=20, w=20, h=52, emission_absorption=True, ambient=0.0), 1),
+    (lambda: small_noise_scene(n=24, w=16, h=16, dtype="f16", compensated_accum=True), 5),
+]
+
+
+@pytest.mark.parametrize("graphs", [True, False])
+def test_batch_equals_one_render_per_job(graphs):
+    bn = _bn()
+    descs = [f() for f, _ in BATCH]
+    spps = [s for _, s in BATCH]
+    ctx = bn.Context()
+    rs = [bn.VolumeRenderer(d, context=ctx) for d in descs]
+    try:
+        ctx.set_graphs(graphs)
+        for r, spp in zip(rs, spps):
+            r.set_spp(spp)
+        ctx.render_batch(rs)
+        ctx.render_batch(rs)  # the second frame continues every job's accumulation
+        total = 0
+        for r, d, spp in zip(rs, descs, spps):
+            sc = oracle.Scene(d)
+            acc = np.zeros((d["height"], d["width"], 4), np.float32)
+            comp = np.zeros_like(acc) if d.get("compensated_accum") else None
+            _, _, st = oracle.render(sc, 0, 2 * spp, accum=acc, comp=comp)
+            ref = oracle.resolve(acc, 2 * spp, comp=comp)
+            assert_bitexact(r.read(), ref, f"batch job {d['width']}x{d['height']}")
+            total += st["samples"]
+        assert ctx.stats()["error_flags"] == 0
+    finally:
+        for r in rs:
+            r.close()
+        ctx.close()
+
+
+def test_autotuned_batch_is_still_exact():
+    bn = _bn()
+    descs = [f() for f, _ in BATCH[:3]]
+    ctx = bn.Context()
+    rs = [bn.VolumeRenderer(d, context=ctx) for d in descs]
+    try:
+        for r in rs:
+            r.set_spp(2)
+        best = ctx.autotune_batch(rs)
+        assert best["threadsPerBlock"] in (64, 128) and best["renderMs"] > 0
+        ctx.render_batch(rs)
+        for r, d in zip(rs, descs):
+            ref, _, _ = oracle_render(d, 2)
+            assert_bitexact(r.read(), ref, "after autotune")
+    finally:
+        for r in rs:
+            r.close()
+        ctx.close()
+
+
+def test_compensated_accumulation_bitexact():
+    d = small_noise_scene(w=32, h=24, compensated_accum=True)
+    img, _ = gpu_render(d, 7, renders=2)
+    sc = oracle.Scene(d)
+    acc = np.zeros((24, 32, 4), np.float32)
+    comp = np.zeros_like(acc)
+    oracle.render(sc, 0, 14, accum=acc, comp=comp)
+    assert_bitexact(img, oracle.resolve(acc, 14, comp=comp), "compensated")
