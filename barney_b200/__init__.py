@@ -47,6 +47,8 @@ EXPORTS = [
     "bnGetLastErrorString", "bnClearLastError", "bnxGetStats", "bnxSetStream", "bnxGetStream",
     "bnxSetLaunchConfig", "bnxFrameBufferDevicePointer", "bnxVolumeGetMacrocells",
     "bnxRenderStructuredNoAlloc", "bnxSetScheduling", "bnxRenderBatch", "bnxSetBatchGraphs", "bnxAutotuneBatch",
+    "bnxServerCreate", "bnxServerDestroy", "bnxServerSubmit", "bnxServerWait", "bnxServerGetStats",
+    "bnxServerResetStats",
 ]
 
 
@@ -68,6 +70,27 @@ class BNXRenderJob(ctypes.Structure):
 class BNXLaunchConfig(ctypes.Structure):
     _fields_ = [("threadsPerBlock", ctypes.c_int), ("blocksPerSM", ctypes.c_int), ("genBatch", ctypes.c_int),
                 ("shadeBatch", ctypes.c_int), ("minBusy", ctypes.c_int), ("renderMs", ctypes.c_float)]
+
+
+class BNXServerConfig(ctypes.Structure):
+    _fields_ = [("hbmBudgetBytes", ctypes.c_size_t), ("maxSlots", ctypes.c_int), ("sliceWaves", ctypes.c_int)]
+
+
+_F3 = ctypes.c_float * 3
+
+
+class BNXRequest(ctypes.Structure):
+    _fields_ = [("model", ctypes.c_void_p), ("renderer", ctypes.c_void_p), ("position", _F3), ("direction", _F3),
+                ("up", _F3), ("fovy", ctypes.c_float), ("width", ctypes.c_int), ("height", ctypes.c_int),
+                ("spp", ctypes.c_int), ("colorFormat", ctypes.c_int)]
+
+
+class BNXServerStats(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_ulonglong) for n in ("submitted", "completed", "rejected", "launches", "queued",
+                                                  "active", "samples")] + \
+               [("peakBytes", ctypes.c_size_t)] + \
+               [(n, ctypes.c_double) for n in ("busySeconds", "wallSeconds", "framesPerSecond", "p50Ms", "p99Ms",
+                                               "meanMs", "maxMs")]
 
 
 class BarneyError(RuntimeError):
@@ -108,6 +131,9 @@ def lib(build_if_missing=True):
         "bnxRenderStructuredNoAlloc": ([P, P], I),
         "bnxSetScheduling": ([P, I, I, I], None), "bnxRenderBatch": ([P, P, I], None),
         "bnxSetBatchGraphs": ([P, I], None), "bnxAutotuneBatch": ([P, P, I, P], None),
+        "bnxServerCreate": ([P, P], P), "bnxServerDestroy": ([P], None),
+        "bnxServerSubmit": ([P, P], ctypes.c_longlong), "bnxServerWait": ([P, ctypes.c_longlong, I, P], I),
+        "bnxServerGetStats": ([P, P], None), "bnxServerResetStats": ([P], None),
     }
     for name, (args, res) in sig.items():
         fn = getattr(L, name)
@@ -372,6 +398,59 @@ class VolumeRenderer:
                 self.L.bnRelease(h)
             self._objects = []
         self.ctx = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Server:
+    """Continuous-batching render server over resident volumes (bnxServer*)."""
+
+    def __init__(self, context, hbm_budget_bytes=150 << 30, max_slots=256, slice_waves=4):
+        self.L = lib()
+        self.context = context
+        cfg = BNXServerConfig(hbm_budget_bytes, max_slots, slice_waves)
+        self.h = self.L.bnxServerCreate(context.ctx, ctypes.byref(cfg))
+        check()
+
+    def submit(self, renderer, camera, width, height, spp, color_format="rgba8"):
+        """renderer: a VolumeRenderer of the server's context (its model and
+        renderer parameters are used); camera: dict as in synth.look_at."""
+        q = BNXRequest()
+        q.model, q.renderer = renderer.model, renderer.renderer
+        q.position[:] = camera["position"]
+        q.direction[:] = camera["direction"]
+        q.up[:] = camera.get("up", (0.0, 1.0, 0.0))
+        q.fovy = camera.get("fovy", 60.0)
+        q.width, q.height, q.spp = width, height, spp
+        q.colorFormat = COLOR_FORMATS[color_format]
+        rid = self.L.bnxServerSubmit(self.h, ctypes.byref(q))
+        if rid < 0:
+            check()
+        return rid
+
+    def wait(self, rid, out=None, timeout_ms=-1):
+        rc = self.L.bnxServerWait(self.h, rid, timeout_ms, _void_p(out))
+        if rc < 0:
+            check()
+        return rc == 1
+
+    def stats(self):
+        st = BNXServerStats()
+        self.L.bnxServerGetStats(self.h, ctypes.byref(st))
+        check()
+        return {f: getattr(st, f) for f, _ in BNXServerStats._fields_}
+
+    def reset_stats(self):
+        self.L.bnxServerResetStats(self.h)
+
+    def close(self):
+        if self.h:
+            self.L.bnxServerDestroy(self.h)
+            self.h = None
 
     def __del__(self):
         try:

@@ -14,8 +14,8 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libbarney_b200.so")
-SOURCES = ["bn_kernels.cu", "bn_api.cpp"]
-HEADERS = ["bn_device.h", os.path.join("..", "..", "include", "bn_volume.h")]
+SOURCES = ["bn_kernels.cu", "bn_api.cpp", "bn_server.cpp"]
+HEADERS = ["bn_device.h", "bn_objects.h", os.path.join("..", "..", "include", "bn_volume.h")]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

@@ -1,362 +1,17 @@
-// bn_api.cpp -- host object model and extern "C" entry points of
-// barney_b200 (declared in include/bn_volume.h).
-//
-// Mirrors the object model of Barney's native layer for the structured-volume
-// path: Context (barney/native/Context.*), TextureData
-// (barney/native/common/Texture.cpp:85-135), StructuredData
-// (barney/native/volume/StructuredData.cu:128-181), Volume + TransferFunction
-// (barney/native/volume/Volume.cpp, TransferFunction.cpp), Group / Model
-// (barney/native/Group.cpp, GlobalModel.cpp, ModelSlot.cpp), DirLight
-// (barney/native/light/DirLight.*), PerspectiveCamera (barney/native/Camera.cu),
-// Renderer (barney/native/render/Renderer.*) and FrameBuffer
-// (barney/native/fb/FrameBuffer.*).  Parameter names and defaults are the
-// reference's.  Device work goes to the kernels in bn_kernels.cu.
-#include "../../include/bn_volume.h"
-#include "bn_device.h"
-
-#include <cuda_runtime.h>
-
-#include <cmath>
-#include <cstring>
-#include <memory>
-#include <mutex>
-#include <stdexcept>
-#include <string>
-#include <unordered_map>
-#include <vector>
+// bn_api.cpp -- extern "C" entry points of barney_b200 (declared in
+// include/bn_volume.h) over the host object model of bn_objects.h, and the
+// host side of rendering: macrocell builds, job set-up, single and batched
+// launches.  Device work goes to the kernels in bn_kernels.cu.
+#include "bn_objects.h"
 
 namespace bnb {
 
-// ---------------------------------------------------------------------------
-// errors
-// ---------------------------------------------------------------------------
-struct Error : std::runtime_error {
-  int code;
-  Error(int c, const std::string &m) : std::runtime_error(m), code(c) {}
-};
-enum : int { E_OK = 0, E_INVALID_HANDLE = 1, E_INVALID_ARG = 2, E_UNSUPPORTED = 3, E_CUDA = 4, E_STATE = 5,
-             E_OOM = 6, E_INTERNAL = 7 };
-static thread_local int g_lastError = 0;
-static thread_local std::string g_lastErrorString;
+thread_local int g_lastError = 0;
+thread_local std::string g_lastErrorString;
+std::mutex g_ctxMutex;
+std::unordered_map<Context *, std::unique_ptr<Context>> g_contexts;
 
-static void ck(cudaError_t e, const char *what) {
-  if (e != cudaSuccess) {
-    cudaGetLastError();
-    throw Error(e == cudaErrorMemoryAllocation ? E_OOM : E_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
-  }
-}
-
-// host-side float3 helpers (compiled with -ffp-contract=off)
-struct v3 { float x, y, z; };
-static inline v3 operator-(v3 a, v3 b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
-static inline v3 operator*(v3 a, float s) { return {a.x * s, a.y * s, a.z * s}; }
-static inline float dot(v3 a, v3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
-static inline v3 cross(v3 a, v3 b) { return {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x}; }
-static inline v3 normalize(v3 v) { return v * (1.f / sqrtf(dot(v, v))); }
-static inline float3 F3(v3 v) { return make_float3(v.x, v.y, v.z); }
-
-// ---------------------------------------------------------------------------
-// device buffer
-// ---------------------------------------------------------------------------
-struct DeviceBuffer {
-  void *ptr = nullptr;
-  size_t bytes = 0;
-  DeviceBuffer() = default;
-  DeviceBuffer(const DeviceBuffer &) = delete;
-  DeviceBuffer &operator=(const DeviceBuffer &) = delete;
-  ~DeviceBuffer() { release(); }
-  void release() {
-    if (ptr) cudaFree(ptr);
-    ptr = nullptr;
-    bytes = 0;
-  }
-  void resize(size_t n) {
-    if (n == bytes && ptr) return;
-    release();
-    if (n) ck(cudaMalloc(&ptr, n), "cudaMalloc");
-    bytes = n;
-  }
-};
-
-struct Context;
-
-// ---------------------------------------------------------------------------
-// objects (Object.h:42-56 set/commit interface)
-// ---------------------------------------------------------------------------
-struct Object : std::enable_shared_from_this<Object> {
-  enum Kind { K_DATA, K_TEXDATA, K_FIELD, K_VOLUME, K_GROUP, K_MODEL, K_LIGHT, K_CAMERA, K_RENDERER, K_FB };
-  Context *ctx;
-  Kind kind;
-  Object(Context *c, Kind k) : ctx(c), kind(k) {}
-  virtual ~Object() = default;
-  virtual bool set1i(const std::string &, int) { return false; }
-  virtual bool set3i(const std::string &, int, int, int) { return false; }
-  virtual bool set1f(const std::string &, float) { return false; }
-  virtual bool set2f(const std::string &, float, float) { return false; }
-  virtual bool set3f(const std::string &, float, float, float) { return false; }
-  virtual bool set4f(const std::string &, float, float, float, float) { return false; }
-  virtual bool setObject(const std::string &, const std::shared_ptr<Object> &) { return false; }
-  virtual void commit() {}
-};
-using ObjectSP = std::shared_ptr<Object>;
-
-struct Data : Object {
-  std::vector<ObjectSP> items;
-  explicit Data(Context *c) : Object(c, K_DATA) {}
-};
-
-struct TextureData : Object {
-  int type = VOX_F32;
-  int dims[3] = {0, 0, 0};
-  DeviceBuffer buf;
-  explicit TextureData(Context *c) : Object(c, K_TEXDATA) {}
-};
-
-// StructuredData (StructuredData.h:30-74)
-struct StructuredField : Object {
-  std::shared_ptr<TextureData> scalars;
-  int numScalars[3] = {0, 0, 0};
-  int numCells[3] = {0, 0, 0};
-  v3 gridOrigin{0, 0, 0};
-  v3 gridSpacing{1, 1, 1};
-  v3 boundsLo{0, 0, 0}, boundsHi{0, 0, 0};
-  explicit StructuredField(Context *c) : Object(c, K_FIELD) {}
-  bool set3i(const std::string &m, int x, int y, int z) override {
-    if (m == "dims") {
-      numScalars[0] = x; numScalars[1] = y; numScalars[2] = z;
-      numCells[0] = x - 1; numCells[1] = y - 1; numCells[2] = z - 1;
-      return true;
-    }
-    return false;
-  }
-  bool set3f(const std::string &m, float x, float y, float z) override {
-    if (m == "gridOrigin") { gridOrigin = {x, y, z}; return true; }
-    if (m == "gridSpacing") { gridSpacing = {x, y, z}; return true; }
-    return false;
-  }
-  bool setObject(const std::string &m, const ObjectSP &v) override {
-    if (m == "textureData") {
-      if (!v || v->kind != K_TEXDATA) throw Error(E_INVALID_ARG, "textureData must be a BNTextureData");
-      scalars = std::static_pointer_cast<TextureData>(v);
-      return true;
-    }
-    return false;
-  }
-  void commit() override {  // StructuredData.cu:177-181
-    boundsLo = gridOrigin;
-    boundsHi = {gridOrigin.x + gridSpacing.x * (float)numCells[0], gridOrigin.y + gridSpacing.y * (float)numCells[1],
-                gridOrigin.z + gridSpacing.z * (float)numCells[2]};
-  }
-};
-
-struct Volume : Object {
-  std::shared_ptr<StructuredField> sf;
-  // TransferFunction.cpp:10-24 defaults: domain [0,1], two entries of 1, density 1
-  float domain[2] = {0.f, 1.f};
-  std::vector<float4> tfValues{make_float4(1, 1, 1, 1), make_float4(1, 1, 1, 1)};
-  float baseDensity = 1.f;
-  float anisotropy = 0.6f;        // Volume.h:140
-  float scatteringAlbedo = 0.9f;  // Volume.h:141
-  int majorantRoundUp = 0;        // bnx.majorantRoundUp (precision forms)
-  bool needsMajorantRebuild = false;
-  bool built = false;
-  int mcDims[3] = {0, 0, 0};
-  DeviceBuffer tfBuf, ranges, majorants;
-  explicit Volume(Context *c) : Object(c, K_VOLUME) {}
-  bool set1i(const std::string &m, int v) override {
-    if (m == "bnx.majorantRoundUp") { majorantRoundUp = v ? 1 : 0; needsMajorantRebuild = true; return true; }
-    if (m == "userID") return true;
-    return false;
-  }
-  bool set1f(const std::string &m, float v) override {  // Volume.cpp:53-63
-    if (m == "anisotropy") { anisotropy = std::min(0.99f, std::max(-0.99f, v)); return true; }
-    if (m == "scatteringAlbedo") { scatteringAlbedo = std::min(1.f, std::max(0.f, v)); return true; }
-    return false;
-  }
-  VolumeDD dd() const;
-  void uploadTF();
-  void build();
-  void remapMajorants();
-  void commit() override;
-};
-
-struct DirLight : Object {
-  v3 direction{0.f, 0.f, -1.f};  // DirLight.h:37
-  float irradiance = NAN;
-  float radiance = 1.f;
-  v3 color{1.f, 1.f, 1.f};       // Light.h:52
-  explicit DirLight(Context *c) : Object(c, K_LIGHT) {}
-  bool set1f(const std::string &m, float v) override {
-    if (m == "irradiance") { irradiance = v; return true; }
-    if (m == "radiance") { radiance = v; return true; }
-    return false;
-  }
-  bool set3f(const std::string &m, float x, float y, float z) override {
-    if (m == "direction") { direction = {x, y, z}; return true; }
-    if (m == "color") { color = {x, y, z}; return true; }
-    if (m == "radiance") {  // DirLight.cu:48-54 (deprecated float3 form)
-      radiance = std::max(std::max(x, y), z);
-      color = {x / radiance, y / radiance, z / radiance};
-      return true;
-    }
-    if (m == "irradiance") {
-      irradiance = std::max(std::max(x, y), z);
-      color = {x / irradiance, y / irradiance, z / irradiance};
-      return true;
-    }
-    return false;
-  }
-  DirLightDD dd() const {  // DirLight.cu:11-20, identity instance
-    DirLightDD d;
-    v3 dir = normalize(direction);
-    d.toLight = make_float3(-dir.x, -dir.y, -dir.z);
-    d.color = F3(color);
-    d.radiance = std::isnan(irradiance) ? radiance : irradiance;
-    return d;
-  }
-};
-
-struct Group : Object {
-  std::shared_ptr<Volume> volume;
-  std::shared_ptr<Data> lights;
-  explicit Group(Context *c) : Object(c, K_GROUP) {}
-};
-
-struct Model : Object {
-  std::shared_ptr<Group> group;
-  bool built = false;
-  explicit Model(Context *c) : Object(c, K_MODEL) {}
-};
-
-// PerspectiveCamera (Camera.cu:17-101)
-struct Camera : Object {
-  v3 position{0, 0, 0}, direction{0, 0, 1}, up{0, 1, 0};
-  float aspect = 1.f, fovy = 60.f, focusDistance = 0.f, apertureRadius = 0.f;
-  v3 dir00{0, 0, 1}, dirdu{1, 0, 0}, dirdv{0, 1, 0}, lens00{0, 0, 0};
-  explicit Camera(Context *c) : Object(c, K_CAMERA) { commit(); }
-  bool set1f(const std::string &m, float v) override {
-    if (m == "aspect") { aspect = v; return true; }
-    if (m == "apertureRadius") { apertureRadius = v; return true; }
-    if (m == "focusDistance") { focusDistance = v; return true; }
-    if (m == "fovy") { fovy = v; return true; }
-    return false;
-  }
-  bool set3f(const std::string &m, float x, float y, float z) override {
-    if (m == "position") { position = {x, y, z}; return true; }
-    if (m == "direction") { direction = normalize(v3{x, y, z}); return true; }
-    if (m == "up") { up = {x, y, z}; return true; }
-    return false;
-  }
-  void commit() override {
-    v3 d00 = normalize(direction);
-    v3 du = normalize(cross(d00, up));
-    v3 dv = normalize(cross(du, d00));
-    d00 = d00 * (float)(1.f / (2.0f * tanf((0.5f * fovy) * (float)M_PI / 180.0f)));
-    dir00 = d00; dirdu = du; dirdv = dv; lens00 = position;
-  }
-};
-
-// Renderer (Renderer.h:17-78); staged values are committed on bnCommit.
-struct Renderer : Object {
-  struct Params {
-    float4 bgColor = make_float4(0, 0, 0, 1);
-    float4 cutPlane = make_float4(0, 0, 0, -1e30f);
-    int pathsPerPixel = 1;
-    float ambientRadiance = 1.f;
-    int maxVolumeBounces = 0;
-    int hgPhase = 0;              // bnx: multi-scatter-build phase model (HGPhase)
-    int emissionAbsorption = 0;   // bnx
-    int exactLog = 0;             // bnx
-    int compensatedAccum = 0;     // bnx: Neumaier-compensated accumulation (precision forms)
-  } staged, p;
-  explicit Renderer(Context *c) : Object(c, K_RENDERER) {}
-  bool set1i(const std::string &m, int v) override {
-    if (m == "pathsPerPixel") { staged.pathsPerPixel = v; return true; }
-    if (m == "maxVolumeBounces") { staged.maxVolumeBounces = v; return true; }
-    if (m == "crosshairs") return true;
-    if (m == "bnx.hgPhase") { staged.hgPhase = v ? 1 : 0; return true; }
-    if (m == "bnx.emissionAbsorption") { staged.emissionAbsorption = v ? 1 : 0; return true; }
-    if (m == "bnx.exactLog") { staged.exactLog = v ? 1 : 0; return true; }
-    if (m == "bnx.compensatedAccum") { staged.compensatedAccum = v ? 1 : 0; return true; }
-    return false;
-  }
-  bool set1f(const std::string &m, float v) override {
-    if (m == "ambientRadiance") { staged.ambientRadiance = v; return true; }
-    return false;
-  }
-  bool set4f(const std::string &m, float x, float y, float z, float w) override {
-    if (m == "bgColor") { staged.bgColor = make_float4(x, y, z, w); return true; }
-    if (m == "cutPlane") { staged.cutPlane = make_float4(x, y, z, w); return true; }
-    return false;
-  }
-  void commit() override { p = staged; }
-};
-
-struct FrameBuffer : Object {
-  int width = 0, height = 0;
-  int colorFormat = FMT_RGBA8;
-  uint32_t accumID = 0;
-  DeviceBuffer accum, color, comp;
-  explicit FrameBuffer(Context *c) : Object(c, K_FB) {}
-};
-
-// ---------------------------------------------------------------------------
-// context
-// ---------------------------------------------------------------------------
-struct Context {
-  int device = 0;
-  cudaStream_t ownStream = nullptr;
-  cudaStream_t stream = nullptr;
-  LaunchCounters *dCounters = nullptr;
-  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
-  int blocksPerSM = 0, threadsPerBlock = 128;
-  SchedDD sched;
-  BNXStats stats{};
-  // batch path: job table + chunk prefix (device, and pinned host mirrors a
-  // captured graph copies from), and the cached graph of the last batch shape
-  DeviceBuffer batchJobs, batchChunks;
-  JobDD *hostJobs = nullptr;
-  int *hostChunks = nullptr;
-  LaunchCounters *hostCounters = nullptr;
-  int hostCapacity = 0;
-  bool useGraphs = true;
-  cudaGraphExec_t graphExec = nullptr;
-  std::vector<const void *> graphKey;
-  std::mutex mutex;
-  std::unordered_map<Object *, std::pair<ObjectSP, int>> handles;  // app references
-
-  explicit Context(int dev) : device(dev) {
-    ck(cudaSetDevice(dev), "cudaSetDevice");
-    ck(cudaStreamCreateWithFlags(&ownStream, cudaStreamNonBlocking), "cudaStreamCreate");
-    stream = ownStream;
-    ck(cudaMalloc(&dCounters, sizeof(LaunchCounters)), "cudaMalloc counters");
-    ck(cudaMemset(dCounters, 0, sizeof(LaunchCounters)), "cudaMemset");
-    for (auto &e : ev) ck(cudaEventCreate(&e), "cudaEventCreate");
-  }
-  ~Context() {
-    cudaSetDevice(device);
-    cudaStreamSynchronize(stream);
-    if (graphExec) cudaGraphExecDestroy(graphExec);
-    if (hostJobs) cudaFreeHost(hostJobs);
-    if (hostChunks) cudaFreeHost(hostChunks);
-    if (hostCounters) cudaFreeHost(hostCounters);
-    handles.clear();
-    for (auto &e : ev) if (e) cudaEventDestroy(e);
-    if (dCounters) cudaFree(dCounters);
-    if (ownStream) cudaStreamDestroy(ownStream);
-  }
-  void activate() { ck(cudaSetDevice(device), "cudaSetDevice"); }
-  BNObject add(const ObjectSP &o) {
-    std::lock_guard<std::mutex> l(mutex);
-    handles[o.get()] = {o, 1};
-    return (BNObject)o.get();
-  }
-};
-
-static std::mutex g_ctxMutex;
-static std::unordered_map<Context *, std::unique_ptr<Context>> g_contexts;
-
-static Context *getContext(BNContext c) {
+Context *getContext(BNContext c) {
   std::lock_guard<std::mutex> l(g_ctxMutex);
   auto it = g_contexts.find((Context *)c);
   if (it == g_contexts.end()) throw Error(E_INVALID_HANDLE, "invalid BNContext handle");
@@ -364,7 +19,7 @@ static Context *getContext(BNContext c) {
 }
 
 // handle -> live object (searches all contexts; handles are unique pointers)
-static ObjectSP getObject(BNObject h) {
+ObjectSP getObject(BNObject h) {
   if (!h) throw Error(E_INVALID_HANDLE, "null object handle");
   std::lock_guard<std::mutex> l(g_ctxMutex);
   for (auto &kv : g_contexts) {
@@ -373,13 +28,6 @@ static ObjectSP getObject(BNObject h) {
     if (it != kv.second->handles.end()) return it->second.first;
   }
   throw Error(E_INVALID_HANDLE, "invalid or released object handle");
-}
-
-template <typename T>
-static std::shared_ptr<T> getAs(BNObject h, Object::Kind k, const char *what) {
-  ObjectSP o = getObject(h);
-  if (o->kind != k) throw Error(E_INVALID_HANDLE, std::string("handle is not a ") + what);
-  return std::static_pointer_cast<T>(o);
 }
 
 // ---------------------------------------------------------------------------
@@ -457,7 +105,7 @@ void Volume::commit() {  // Volume.cpp:26-35
 // ---------------------------------------------------------------------------
 // The device job of one (renderer, model, camera, frame buffer) tuple,
 // validated; fr.spp waves starting at the frame buffer's accumID.
-static JobDD buildJob(Context *ctx, Renderer &r, Model &m, Camera &cam, FrameBuffer &fb) {
+JobDD buildJob(Context *ctx, Renderer &r, Model &m, Camera &cam, FrameBuffer &fb) {
   if (!m.built || !m.group || !m.group->volume) throw Error(E_STATE, "model has no built volume instance");
   if (fb.width <= 0 || fb.height <= 0) throw Error(E_STATE, "frame buffer has not been resized");
   if (cam.apertureRadius > 0.f) throw Error(E_UNSUPPORTED, "depth-of-field cameras are not supported");
@@ -506,15 +154,22 @@ static JobDD buildJob(Context *ctx, Renderer &r, Model &m, Camera &cam, FrameBuf
   return job;
 }
 
-static void readStats(Context *ctx, const LaunchCounters &hc, unsigned long long pixelSamples) {
+// ev[0..1] bracket the render kernel, ev[1..2] the resolve; a replayed
+// graph records only ev[0] and ev[2] around the whole launch (ev[1] = -1).
+static void readStats(Context *ctx, const LaunchCounters &hc, unsigned long long pixelSamples, bool whole = false) {
   BNXStats &st = ctx->stats;
   st.samples = hc.samples;
   st.mcVisits = hc.mcVisits;
   st.rays = hc.rays;
   st.pixelSamples = pixelSamples;
   st.errorFlags = hc.errorFlags;
-  cudaEventElapsedTime(&st.renderMs, ctx->ev[0], ctx->ev[1]);
-  cudaEventElapsedTime(&st.resolveMs, ctx->ev[1], ctx->ev[2]);
+  st.renderMs = st.resolveMs = 0.f;
+  if (whole) {
+    if (cudaEventElapsedTime(&st.renderMs, ctx->ev[0], ctx->ev[2]) != cudaSuccess) cudaGetLastError();
+  } else {
+    if (cudaEventElapsedTime(&st.renderMs, ctx->ev[0], ctx->ev[1]) != cudaSuccess) cudaGetLastError();
+    if (cudaEventElapsedTime(&st.resolveMs, ctx->ev[1], ctx->ev[2]) != cudaSuccess) cudaGetLastError();
+  }
 }
 
 static void render(Context *ctx, Renderer &r, Model &m, Camera &cam, FrameBuffer &fb) {
@@ -542,9 +197,7 @@ static void render(Context *ctx, Renderer &r, Model &m, Camera &cam, FrameBuffer
 // batch shape (same frame buffers, sizes and launch configuration) and
 // replayed; per-frame values (cameras, accumIDs) travel in the pinned job
 // table the graph copies from.  Results equal one bnRender per job.
-struct BatchEntry { Renderer *r; Model *m; Camera *c; FrameBuffer *fb; };
-
-static void renderBatch(Context *ctx, const std::vector<BatchEntry> &entries) {
+void renderBatch(Context *ctx, const std::vector<BatchEntry> &entries) {
   const int n = (int)entries.size();
   if (n == 0) return;
   if (n > ctx->hostCapacity) {
@@ -583,19 +236,19 @@ static void renderBatch(Context *ctx, const std::vector<BatchEntry> &entries) {
   key.push_back((const void *)(intptr_t)(ctx->blocksPerSM * 4096 + ctx->threadsPerBlock));
   key.push_back((const void *)(intptr_t)(ctx->sched.genBatch * 65536 + ctx->sched.shadeBatch * 256 + ctx->sched.minBusy));
   key.push_back((const void *)(intptr_t)n);
-  auto enqueue = [&](cudaStream_t s) {
+  auto enqueue = [&](cudaStream_t s, bool timed) {
     ck(cudaMemcpyAsync(ctx->batchJobs.ptr, ctx->hostJobs, n * sizeof(JobDD), cudaMemcpyHostToDevice, s), "job table");
     ck(cudaMemcpyAsync(ctx->batchChunks.ptr, ctx->hostChunks, (n + 1) * sizeof(int), cudaMemcpyHostToDevice, s),
        "chunk table");
     ck(cudaMemsetAsync(ctx->dCounters, 0, sizeof(LaunchCounters), s), "counter reset");
-    ck(cudaEventRecord(ctx->ev[0], s), "event");
+    if (timed) ck(cudaEventRecord(ctx->ev[0], s), "event");
     ck(launchRenderBatch((const JobDD *)ctx->batchJobs.ptr, (const int *)ctx->batchChunks.ptr, n, ctx->dCounters,
                          ctx->blocksPerSM, ctx->threadsPerBlock, s, ctx->sched),
        "batch render kernel");
-    ck(cudaEventRecord(ctx->ev[1], s), "event");
+    if (timed) ck(cudaEventRecord(ctx->ev[1], s), "event");
     ck(launchResolveBatch((const JobDD *)ctx->batchJobs.ptr, (const int *)ctx->batchChunks.ptr, n, (int)chunks, s),
        "batch resolve kernel");
-    ck(cudaEventRecord(ctx->ev[2], s), "event");
+    if (timed) ck(cudaEventRecord(ctx->ev[2], s), "event");
     ck(cudaMemcpyAsync(ctx->hostCounters, ctx->dCounters, sizeof(LaunchCounters), cudaMemcpyDeviceToHost, s),
        "counter read");
   };
@@ -605,7 +258,7 @@ static void renderBatch(Context *ctx, const std::vector<BatchEntry> &entries) {
       cudaGraph_t g = nullptr;
       ck(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal), "graph capture");
       try {
-        enqueue(ctx->stream);
+        enqueue(ctx->stream, false);
       } catch (...) {
         cudaStreamEndCapture(ctx->stream, &g);
         if (g) cudaGraphDestroy(g);
@@ -617,13 +270,15 @@ static void renderBatch(Context *ctx, const std::vector<BatchEntry> &entries) {
       ck(e, "graph instantiate");
       ctx->graphKey = key;
     }
+    ck(cudaEventRecord(ctx->ev[0], ctx->stream), "event");
     ck(cudaGraphLaunch(ctx->graphExec, ctx->stream), "graph launch");
+    ck(cudaEventRecord(ctx->ev[2], ctx->stream), "event");
   } else {
-    enqueue(ctx->stream);
+    enqueue(ctx->stream, true);
   }
   ck(cudaStreamSynchronize(ctx->stream), "batch render");
   for (int i = 0; i < n; i++) entries[i].fb->accumID += ctx->hostJobs[i].fr.spp;
-  readStats(ctx, *ctx->hostCounters, pixelSamples);
+  readStats(ctx, *ctx->hostCounters, pixelSamples, ctx->useGraphs);
 }
 
 }  // namespace bnb
@@ -633,25 +288,6 @@ using namespace bnb;
 // ---------------------------------------------------------------------------
 // extern "C" entry points
 // ---------------------------------------------------------------------------
-#define BN_TRY try {
-#define BN_CATCH(ret)                                              \
-  }                                                                \
-  catch (const Error &e) {                                         \
-    g_lastError = e.code;                                          \
-    g_lastErrorString = e.what();                                  \
-    return ret;                                                    \
-  }                                                                \
-  catch (const std::bad_alloc &) {                                 \
-    g_lastError = E_OOM;                                           \
-    g_lastErrorString = "host out of memory";                      \
-    return ret;                                                    \
-  }                                                                \
-  catch (const std::exception &e) {                                \
-    g_lastError = E_INTERNAL;                                      \
-    g_lastErrorString = e.what();                                  \
-    return ret;                                                    \
-  }
-
 extern "C" {
 
 BN_API int bnGetLastError(void) { return g_lastError; }

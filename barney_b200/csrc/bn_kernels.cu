@@ -439,7 +439,8 @@ enum LanePhase : int {
   LP_CELL = 2,      // a ray needs its next macrocell with a non-zero majorant
   LP_WOODCOCK = 3,  // inside a Woodcock range
   LP_HIT = 4,       // collision found, waiting to be shaded
-  LP_ENDED = 5      // ray left the grid (primary: background; shadow: reached the light)
+  LP_ENDED = 5,     // ray left the grid (primary: background; shadow: reached the light)
+  LP_BEGIN = 6      // a new primary or shadow ray (ts.org, ts.dir, ts.rayTMax) needs its set-up
 };
 
 constexpr int kChunk = 32;  // pixels a warp takes at a time (one 8x4 tile)
@@ -447,7 +448,8 @@ constexpr int kChunk = 32;  // pixels a warp takes at a time (one 8x4 tile)
 // The render loop shared by the single-frame kernel (one job, read from a
 // __grid_constant__ parameter, TF staged in shared memory) and the batch
 // kernel (a job table in global memory, chunks of all jobs in one counter).
-template <int T, bool BATCH>
+// LOG: 0 fastLog (Volume.h:154-164), 1 -logf (bnx.exactLog), 2 per job (batch)
+template <int T, bool BATCH, int LOG>
 DEV void renderLoop(const JobDD *jobs, const int *chunkStart, int numJobs, int numChunks, const SchedDD &sd,
                     LaunchCounters *ctr, const float4 *sTF, const float *u8lut) {
   const unsigned FULL = 0xffffffffu;
@@ -544,7 +546,8 @@ DEV void renderLoop(const JobDD *jobs, const int *chunkStart, int numJobs, int n
     // ------------------------------------------------------------------
     if (phase == LP_WOODCOCK) {
       const float r = rngFloat(ts.rng);
-      const float dt = fr.exactLog ? (-logf(1.f - r) / ts.maj) : (-fastLog(1.f - r) / ts.maj);
+      const bool exact = LOG == 1 || (LOG == 2 && fr.exactLog);
+      const float dt = exact ? (-logf(1.f - r) / ts.maj) : (-fastLog(1.f - r) / ts.maj);
       ts.t += dt;
       if (ts.t >= ts.tUpper) {
         const float tClosest = fmin_(fmin_(ts.tNext.x, ts.tNext.y), ts.tNext.z);
@@ -557,7 +560,7 @@ DEV void renderLoop(const JobDD *jobs, const int *chunkStart, int numJobs, int n
         int idx = 0;
         if (!isnan(s)) {
           const float span = v.domHi - v.domLo;
-          f = (s - v.domLo) / span;
+          f = span == 1.f ? (s - v.domLo) : (s - v.domLo) / span;  // x/1 == x exactly
           f = fmin_(1.f, fmax_(0.f, f));
           f *= (float)(v.tfN - 1);
           idx = min(v.tfN - 2, max(0, (int)f));
@@ -683,14 +686,16 @@ DEV void renderLoop(const JobDD *jobs, const int *chunkStart, int numJobs, int n
               const float sTMax = kInf * (1.f - 2.f * offsetEpsilon);
               if (alive && sTMax > 0.f) {
                 shadowTp = f3(roundHalf(tp.x), roundHalf(tp.y), roundHalf(tp.z));
-                const float3 so =
-                    f3(P.x + offsetEpsilon * woN.x, P.y + offsetEpsilon * woN.y, P.z + offsetEpsilon * woN.z);
-                uint64_t shadowSeed = raySeed;
+                // makeShadowRay (Ray.h:147-157); its RNG seed is the primary's,
+                // which is not used again by this wave
+                ts.org = f3(P.x + offsetEpsilon * woN.x, P.y + offsetEpsilon * woN.y, P.z + offsetEpsilon * woN.z);
+                ts.dir = ls.dir;
+                ts.rayTMax = sTMax;
                 shadowRay = true;
                 spawned = true;
                 nRays++;
                 steps = 0;
-                phase = traceBegin(v, ts, so, ls.dir, sTMax, shadowSeed) ? LP_CELL : LP_ENDED;
+                phase = LP_BEGIN;
               }
             }
           }
@@ -751,11 +756,19 @@ DEV void renderLoop(const JobDD *jobs, const int *chunkStart, int numJobs, int n
       shadowRay = false;
       nRays++;
       steps = 0;
-      phase = traceBegin(v, ts, o, d, tMax, raySeed) ? LP_CELL : LP_ENDED;
+      ts.org = o;
+      ts.dir = d;
+      ts.rayTMax = tMax;
+      phase = LP_BEGIN;
     }
 
     // ------------------------------------------------------------------
-    // 6. next macrocell with a non-zero majorant (DDA.h:172-200,
+    // 6. ray set-up, primary and shadow rays together
+    // ------------------------------------------------------------------
+    if (phase == LP_BEGIN) phase = traceBegin(v, ts, ts.org, ts.dir, ts.rayTMax, raySeed) ? LP_CELL : LP_ENDED;
+
+    // ------------------------------------------------------------------
+    // 7. next macrocell with a non-zero majorant (DDA.h:172-200,
     //    MCAccelerator.h:596-612)
     // ------------------------------------------------------------------
     if (phase == LP_CELL) {
@@ -792,7 +805,7 @@ DEV void renderLoop(const JobDD *jobs, const int *chunkStart, int numJobs, int n
   }
 }
 
-template <int T>
+template <int T, int LOG>
 __global__ void __launch_bounds__(kRenderMaxThreads, 4)
     renderKernel(const __grid_constant__ JobDD job, const __grid_constant__ SchedDD sd, LaunchCounters *ctr) {
   extern __shared__ float4 sTF[];
@@ -801,7 +814,7 @@ __global__ void __launch_bounds__(kRenderMaxThreads, 4)
   for (int i = threadIdx.x; i < 256; i += blockDim.x) u8lut[i] = (float)i * 1.f / 255.f;
   __syncthreads();
   const int numChunks = (job.fr.width * job.fr.height + kChunk - 1) / kChunk;
-  renderLoop<T, false>(&job, nullptr, 1, numChunks, sd, ctr, sTF, u8lut);
+  renderLoop<T, false, LOG>(&job, nullptr, 1, numChunks, sd, ctr, sTF, u8lut);
 }
 
 __global__ void __launch_bounds__(kRenderMaxThreads, 4)
@@ -810,7 +823,7 @@ __global__ void __launch_bounds__(kRenderMaxThreads, 4)
   __shared__ float u8lut[256];
   for (int i = threadIdx.x; i < 256; i += blockDim.x) u8lut[i] = (float)i * 1.f / 255.f;
   __syncthreads();
-  renderLoop<-1, true>(jobs, chunkStart, numJobs, __ldg(chunkStart + numJobs), sd, ctr, nullptr, u8lut);
+  renderLoop<-1, true, 2>(jobs, chunkStart, numJobs, __ldg(chunkStart + numJobs), sd, ctr, nullptr, u8lut);
 }
 
 // ---------------------------------------------------------------------------
@@ -880,9 +893,12 @@ __global__ void resolveBatchKernel(const JobDD *jobs, const int *chunkStart, int
 static int smCount() {
   static int n = 0;
   if (!n) {
-    int dev = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+    int dev = 0, c = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&c, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) {
+      cudaGetLastError();
+      return 1;
+    }
+    n = c;
   }
   return n;
 }
@@ -910,11 +926,13 @@ template <int T>
 static cudaError_t launchRenderT(const VolumeDD &v, const FrameDD &fr, const SchedDD &sd, LaunchCounters *ctr,
                                  int bps, int tpb, cudaStream_t s) {
   const size_t smem = (size_t)v.tfN * sizeof(float4);
-  auto kern = renderKernel<T>;
-  if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  auto kern = fr.exactLog ? renderKernel<T, 1> : renderKernel<T, 0>;
+  if (smem > 48 * 1024 &&
+      cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+    return cudaGetLastError();
   if (bps <= 0) {
     int occ = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, tpb, smem);
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, tpb, smem) != cudaSuccess) return cudaGetLastError();
     bps = occ > 0 ? occ : 1;
   }
   JobDD job;
@@ -940,7 +958,8 @@ cudaError_t launchRenderBatch(const JobDD *jobs, const int *chunkStart, int numJ
   if (tpb <= 0) tpb = 128;
   if (bps <= 0) {
     int occ = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, renderBatchKernel, tpb, 0);
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, renderBatchKernel, tpb, 0) != cudaSuccess)
+      return cudaGetLastError();
     bps = occ > 0 ? occ : 1;
   }
   renderBatchKernel<<<smCount() * bps, tpb, 0, s>>>(jobs, chunkStart, numJobs, sd, ctr);
@@ -963,7 +982,11 @@ cudaError_t launchResolve(const float4 *accum, int n, int accumID, int fmt, void
 
 int renderKernelMaxBlocksPerSM(int tpb) {
   int occ = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, renderKernel<VOX_F32>, tpb, 256 * sizeof(float4));
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, renderKernel<VOX_F32, 0>, tpb, 256 * sizeof(float4)) !=
+      cudaSuccess) {
+    cudaGetLastError();
+    return 1;
+  }
   return occ;
 }
 

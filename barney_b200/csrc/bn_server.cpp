@@ -1,0 +1,394 @@
+// bn_server.cpp -- continuous-batching render server (bnxServer*, no
+// reference counterpart).
+//
+// Requests name a resident volume (a built BNModel), a renderer (its
+// parameters are copied at submission), a camera, an image size and a wave
+// count.  One worker thread owns the context's stream and loops:
+//
+//   1. admit queued requests, in arrival order, while their per-request
+//      device buffers (accumulation, compensation, colour) fit the HBM budget
+//      and a batch slot is free;
+//   2. render one slice -- at most sliceWaves waves of every admitted request
+//      -- in one persistent launch of the batch kernel (renderBatch);
+//   3. requests whose waves are all done are resolved; their colour is copied
+//      to a pinned staging buffer, their device buffers return to the pool,
+//      and waiters are woken.
+//
+// Requests that arrive while a slice is on the GPU join the next slice, so
+// their work overlaps with every other admitted request's on the device.
+// A request's result does not depend on what it was batched with: its pixels
+// are accumulated in wave order by one lane each, with per-pixel RNG streams
+// keyed by (pixel, accumID), never by queue position.
+#include "bn_objects.h"
+
+#include <chrono>
+#include <condition_variable>
+#include <deque>
+#include <map>
+#include <thread>
+
+namespace bnb {
+
+using Clock = std::chrono::steady_clock;
+
+struct ServerRequest {
+  long long id = 0;
+  std::shared_ptr<Model> model;
+  std::shared_ptr<Renderer> renderer;  // private copy of the submitted renderer's parameters
+  std::shared_ptr<Camera> camera;
+  std::shared_ptr<FrameBuffer> fb;     // device buffers while admitted
+  int spp = 1, wavesDone = 0;
+  size_t deviceBytes = 0;
+  Clock::time_point submitted, admitted, finished;
+  bool done = false, failed = false;
+  std::string error;
+  void *staging = nullptr;  // pinned host copy of the colour channel
+  size_t stagingBytes = 0;
+};
+
+// Pool of equally sized device / pinned buffers, so steady-state serving
+// performs no cudaMalloc / cudaFree (either would synchronise the device).
+struct BufferPool {
+  std::multimap<size_t, void *> freeDevice, freeHost;
+  size_t deviceBytesHeld = 0;
+  ~BufferPool() {
+    for (auto &kv : freeDevice) cudaFree(kv.second);
+    for (auto &kv : freeHost) cudaFreeHost(kv.second);
+  }
+  void *getDevice(size_t n) {
+    auto it = freeDevice.find(n);
+    if (it != freeDevice.end()) { void *p = it->second; freeDevice.erase(it); return p; }
+    void *p = nullptr;
+    ck(cudaMalloc(&p, n), "server buffer");
+    deviceBytesHeld += n;
+    return p;
+  }
+  void putDevice(void *p, size_t n) { if (p) freeDevice.emplace(n, p); }
+  void *getHost(size_t n) {
+    auto it = freeHost.find(n);
+    if (it != freeHost.end()) { void *p = it->second; freeHost.erase(it); return p; }
+    void *p = nullptr;
+    ck(cudaHostAlloc(&p, n, cudaHostAllocDefault), "server staging buffer");
+    return p;
+  }
+  void putHost(void *p, size_t n) { if (p) freeHost.emplace(n, p); }
+};
+
+struct Server {
+  Context *ctx;
+  BNXServerConfig cfg;
+  std::mutex m;
+  std::condition_variable cvWork, cvDone;
+  std::deque<std::shared_ptr<ServerRequest>> queue;
+  std::vector<std::shared_ptr<ServerRequest>> active;
+  std::unordered_map<long long, std::shared_ptr<ServerRequest>> finished;
+  long long nextId = 0;
+  size_t bytesInUse = 0, peakBytes = 0;
+  bool stop = false;
+  BufferPool pool;
+  std::thread worker;
+  // statistics
+  std::vector<double> latenciesMs;
+  unsigned long long submittedCount = 0, completedCount = 0, rejectedCount = 0, launches = 0;
+  double busySeconds = 0.0;
+  Clock::time_point statsStart = Clock::now();
+  unsigned long long samples = 0;
+
+  Server(Context *c, const BNXServerConfig &config) : ctx(c), cfg(config) { worker = std::thread([this] { loop(); }); }
+  ~Server() {
+    {
+      std::lock_guard<std::mutex> l(m);
+      stop = true;
+    }
+    cvWork.notify_all();
+    if (worker.joinable()) worker.join();
+    for (auto &r : active) releaseDevice(*r);
+    for (auto &kv : finished) pool.putHost(kv.second->staging, kv.second->stagingBytes);
+  }
+
+  static size_t bytesFor(int w, int h, int fmt, bool comp) {
+    const size_t px = (size_t)w * h;
+    return px * 16 + (comp ? px * 16 : 0) + px * (fmt == FMT_FLOAT4 ? 16 : 4);
+  }
+
+  void releaseDevice(ServerRequest &r) {
+    if (!r.fb) return;
+    const size_t px = (size_t)r.fb->width * r.fb->height;
+    pool.putDevice(r.fb->accum.ptr, px * 16);
+    if (r.fb->comp.ptr) pool.putDevice(r.fb->comp.ptr, px * 16);
+    pool.putDevice(r.fb->color.ptr, r.fb->color.bytes);
+    r.fb->accum.ptr = r.fb->comp.ptr = r.fb->color.ptr = nullptr;  // owned by the pool now
+    r.fb->accum.bytes = r.fb->comp.bytes = r.fb->color.bytes = 0;
+    r.fb.reset();
+    bytesInUse -= r.deviceBytes;
+  }
+
+  // device buffers of an admitted request (from the pool)
+  void acquireDevice(ServerRequest &r) {
+    auto fb = std::make_shared<FrameBuffer>(ctx);
+    const int w = r.fb ? r.fb->width : 0, h = r.fb ? r.fb->height : 0;
+    const int fmt = r.fb ? r.fb->colorFormat : FMT_RGBA8;
+    fb->width = w;
+    fb->height = h;
+    fb->colorFormat = fmt;
+    const size_t px = (size_t)w * h;
+    fb->accum.ptr = pool.getDevice(px * 16);
+    fb->accum.bytes = px * 16;
+    if (r.renderer->p.compensatedAccum) {
+      fb->comp.ptr = pool.getDevice(px * 16);
+      fb->comp.bytes = px * 16;
+      ck(cudaMemsetAsync(fb->comp.ptr, 0, px * 16, ctx->stream), "compensation clear");
+    }
+    const size_t cb = px * (fmt == FMT_FLOAT4 ? 16 : 4);
+    fb->color.ptr = pool.getDevice(cb);
+    fb->color.bytes = cb;
+    fb->accumID = 0;
+    r.fb = fb;
+    bytesInUse += r.deviceBytes;
+    peakBytes = std::max(peakBytes, bytesInUse);
+  }
+
+  void loop() {
+    cudaSetDevice(ctx->device);
+    while (true) {
+      std::vector<std::shared_ptr<ServerRequest>> slice;
+      {
+        std::unique_lock<std::mutex> l(m);
+        cvWork.wait(l, [&] { return stop || !queue.empty() || !active.empty(); });
+        if (stop) return;
+        // 1. admission, in arrival order, by HBM budget and slots
+        while (!queue.empty() && (int)active.size() < cfg.maxSlots) {
+          auto r = queue.front();
+          if (r->deviceBytes > cfg.hbmBudgetBytes) {  // can never fit: reject
+            queue.pop_front();
+            r->failed = true;
+            r->error = "request needs more device memory than the server's budget";
+            r->done = true;
+            rejectedCount++;
+            finished[r->id] = r;
+            cvDone.notify_all();
+            continue;
+          }
+          if (bytesInUse + r->deviceBytes > cfg.hbmBudgetBytes) break;
+          queue.pop_front();
+          try {
+            acquireDevice(*r);
+          } catch (const Error &) {  // out of device memory: retry once others finish
+            queue.push_front(r);
+            break;
+          }
+          r->admitted = Clock::now();
+          active.push_back(r);
+        }
+        slice = active;
+      }
+      if (slice.empty()) {
+        std::this_thread::sleep_for(std::chrono::microseconds(200));
+        continue;
+      }
+      // 2. one slice of waves for every admitted request, one launch
+      std::vector<BatchEntry> entries;
+      std::vector<int> waves;
+      for (auto &r : slice) {
+        const int n = std::min(cfg.sliceWaves, r->spp - r->wavesDone);
+        r->renderer->p.pathsPerPixel = n;
+        waves.push_back(n);
+        entries.push_back({r->renderer.get(), r->model.get(), r->camera.get(), r->fb.get()});
+      }
+      const auto t0 = Clock::now();
+      std::string err;
+      const bool graphs = ctx->useGraphs;
+      ctx->useGraphs = false;  // the batch changes every slice: plain launches
+      try {
+        renderBatch(ctx, entries);
+      } catch (const std::exception &e) {
+        err = e.what();
+      }
+      ctx->useGraphs = graphs;
+      const auto t1 = Clock::now();
+      // 3. completions
+      std::lock_guard<std::mutex> l(m);
+      busySeconds += std::chrono::duration<double>(t1 - t0).count();
+      launches++;
+      samples += ctx->stats.samples;
+      std::vector<std::shared_ptr<ServerRequest>> still;
+      for (size_t i = 0; i < slice.size(); i++) {
+        auto &r = slice[i];
+        r->wavesDone += waves[i];
+        if (err.empty() && r->wavesDone < r->spp) { still.push_back(r); continue; }
+        if (err.empty()) {
+          try {
+            r->stagingBytes = r->fb->color.bytes;
+            r->staging = pool.getHost(r->stagingBytes);
+            ck(cudaMemcpyAsync(r->staging, r->fb->color.ptr, r->stagingBytes, cudaMemcpyDeviceToHost, ctx->stream),
+               "result copy");
+            ck(cudaStreamSynchronize(ctx->stream), "result copy");
+          } catch (const std::exception &e) {
+            r->failed = true;
+            r->error = e.what();
+          }
+        } else {
+          r->failed = true;
+          r->error = err;
+        }
+        r->finished = Clock::now();
+        r->done = true;
+        releaseDevice(*r);
+        if (!r->failed) {
+          latenciesMs.push_back(std::chrono::duration<double, std::milli>(r->finished - r->submitted).count());
+          completedCount++;
+        }
+        finished[r->id] = r;
+      }
+      active.swap(still);
+      cvDone.notify_all();
+    }
+  }
+};
+
+static std::mutex g_serverMutex;
+static std::unordered_map<Server *, std::unique_ptr<Server>> g_servers;
+
+static Server *getServer(BNXServer h) {
+  std::lock_guard<std::mutex> l(g_serverMutex);
+  auto it = g_servers.find((Server *)h);
+  if (it == g_servers.end()) throw Error(E_INVALID_HANDLE, "invalid BNXServer handle");
+  return it->second.get();
+}
+
+}  // namespace bnb
+
+using namespace bnb;
+
+extern "C" {
+
+BN_API BNXServer bnxServerCreate(BNContext context, const BNXServerConfig *config) {
+  BN_TRY
+  Context *c = getContext(context);
+  BNXServerConfig cfg{(size_t)150 << 30, 256, 4};
+  if (config) cfg = *config;
+  if (cfg.maxSlots < 1 || cfg.sliceWaves < 1) throw Error(E_INVALID_ARG, "maxSlots and sliceWaves must be >= 1");
+  c->activate();
+  auto s = std::make_unique<Server>(c, cfg);
+  Server *raw = s.get();
+  std::lock_guard<std::mutex> l(g_serverMutex);
+  g_servers[raw] = std::move(s);
+  return (BNXServer)raw;
+  BN_CATCH(nullptr)
+}
+
+BN_API void bnxServerDestroy(BNXServer server) {
+  BN_TRY
+  Server *s = getServer(server);
+  std::unique_ptr<Server> owned;
+  {
+    std::lock_guard<std::mutex> l(g_serverMutex);
+    owned = std::move(g_servers[s]);
+    g_servers.erase(s);
+  }
+  BN_CATCH()
+}
+
+BN_API long long bnxServerSubmit(BNXServer server, const BNXRequest *q) {
+  BN_TRY
+  Server *s = getServer(server);
+  if (!q) throw Error(E_INVALID_ARG, "request is null");
+  auto r = std::make_shared<ServerRequest>();
+  r->submitted = Clock::now();
+  r->model = getAs<Model>(q->model, Object::K_MODEL, "BNModel");
+  if (!r->model->built) throw Error(E_STATE, "the request's model has not been built");
+  auto tmpl = getAs<Renderer>(q->renderer, Object::K_RENDERER, "BNRenderer");
+  r->renderer = std::make_shared<Renderer>(s->ctx);
+  r->renderer->p = tmpl->p;
+  auto cam = std::make_shared<Camera>(s->ctx);
+  cam->set3f("position", q->position.x, q->position.y, q->position.z);
+  cam->set3f("direction", q->direction.x, q->direction.y, q->direction.z);
+  cam->set3f("up", q->up.x, q->up.y, q->up.z);
+  cam->set1f("fovy", q->fovy);
+  cam->commit();
+  r->camera = cam;
+  if (q->width <= 0 || q->height <= 0 || q->spp <= 0) throw Error(E_INVALID_ARG, "width, height, spp must be > 0");
+  const int fmt = q->colorFormat == BN_FLOAT4 ? FMT_FLOAT4 : q->colorFormat == BN_UFIXED8_RGBA ? FMT_RGBA8
+                : q->colorFormat == BN_UFIXED8_RGBA_SRGB ? FMT_RGBA8_SRGB : -1;
+  if (fmt < 0) throw Error(E_UNSUPPORTED, "unsupported colour format");
+  auto fb = std::make_shared<FrameBuffer>(s->ctx);  // size holder until admission
+  fb->width = q->width;
+  fb->height = q->height;
+  fb->colorFormat = fmt;
+  r->fb = fb;
+  r->spp = q->spp;
+  r->deviceBytes = Server::bytesFor(q->width, q->height, fmt, r->renderer->p.compensatedAccum != 0);
+  {
+    std::lock_guard<std::mutex> l(s->m);
+    r->id = s->nextId++;
+    s->submittedCount++;
+    s->queue.push_back(r);
+  }
+  s->cvWork.notify_one();
+  return r->id;
+  BN_CATCH(-1)
+}
+
+BN_API int bnxServerWait(BNXServer server, long long id, int timeoutMs, void *hostPixels) {
+  BN_TRY
+  Server *s = getServer(server);
+  std::unique_lock<std::mutex> l(s->m);
+  auto ready = [&] { return s->finished.count(id) > 0; };
+  if (timeoutMs < 0) s->cvDone.wait(l, ready);
+  else if (!s->cvDone.wait_for(l, std::chrono::milliseconds(timeoutMs), ready)) return 0;
+  auto r = s->finished[id];
+  s->finished.erase(id);
+  if (r->failed) throw Error(E_CUDA, "request failed: " + r->error);
+  if (hostPixels) memcpy(hostPixels, r->staging, r->stagingBytes);
+  s->pool.putHost(r->staging, r->stagingBytes);
+  r->staging = nullptr;
+  return 1;
+  BN_CATCH(-g_lastError)
+}
+
+BN_API void bnxServerGetStats(BNXServer server, BNXServerStats *out) {
+  BN_TRY
+  Server *s = getServer(server);
+  if (!out) return;
+  std::lock_guard<std::mutex> l(s->m);
+  BNXServerStats st{};
+  st.submitted = s->submittedCount;
+  st.completed = s->completedCount;
+  st.rejected = s->rejectedCount;
+  st.launches = s->launches;
+  st.busySeconds = s->busySeconds;
+  st.samples = s->samples;
+  st.peakBytes = s->peakBytes;
+  st.queued = (unsigned long long)s->queue.size();
+  st.active = (unsigned long long)s->active.size();
+  const double wall = std::chrono::duration<double>(Clock::now() - s->statsStart).count();
+  st.wallSeconds = wall;
+  st.framesPerSecond = wall > 0 ? s->completedCount / wall : 0.0;
+  if (!s->latenciesMs.empty()) {
+    std::vector<double> v = s->latenciesMs;
+    std::sort(v.begin(), v.end());
+    auto pct = [&](double q) { return v[std::min(v.size() - 1, (size_t)(q * (v.size() - 1) + 0.5))]; };
+    st.p50Ms = pct(0.50);
+    st.p99Ms = pct(0.99);
+    double sum = 0;
+    for (double x : v) sum += x;
+    st.meanMs = sum / v.size();
+    st.maxMs = v.back();
+  }
+  *out = st;
+  BN_CATCH()
+}
+
+BN_API void bnxServerResetStats(BNXServer server) {
+  BN_TRY
+  Server *s = getServer(server);
+  std::lock_guard<std::mutex> l(s->m);
+  s->latenciesMs.clear();
+  s->submittedCount = s->completedCount = s->rejectedCount = s->launches = 0;
+  s->busySeconds = 0;
+  s->samples = 0;
+  s->statsStart = Clock::now();
+  BN_CATCH()
+}
+
+}  // extern "C"

@@ -292,6 +292,47 @@ typedef struct {
 } BNXNoAllocFrame;
 BN_API int bnxRenderStructuredNoAlloc(const BNXNoAllocFrame *frame, void *cudaStream);
 
+/* ---------------------------------------------------------------------- */
+/* render server: continuous batching (no reference counterpart)           */
+/* ---------------------------------------------------------------------- */
+/* A worker thread renders submitted requests in slices of at most
+   sliceWaves waves per request, one persistent batch launch per slice.
+   Requests are admitted in arrival order while their per-request device
+   buffers (accumulation, compensation, colour) fit hbmBudgetBytes and fewer
+   than maxSlots requests are admitted; later arrivals join the next slice.
+   Volumes (built BNModels) stay resident and are shared by requests.  While
+   a server runs, it alone launches work on its context. */
+typedef struct _BNXServer *BNXServer;
+typedef struct {
+  size_t hbmBudgetBytes;  /* device memory for admitted requests' buffers */
+  int maxSlots;           /* requests rendered together in one launch */
+  int sliceWaves;         /* waves per request per launch */
+} BNXServerConfig;
+typedef struct {
+  BNModel model;          /* a built model of the server's context */
+  BNRenderer renderer;    /* parameters copied at submission (pathsPerPixel ignored) */
+  bn_float3 position, direction, up;
+  float fovy;
+  int width, height, spp;
+  BNDataType colorFormat; /* BN_FLOAT4, BN_UFIXED8_RGBA, BN_UFIXED8_RGBA_SRGB */
+} BNXRequest;
+typedef struct {
+  unsigned long long submitted, completed, rejected, launches, queued, active, samples;
+  size_t peakBytes;
+  double busySeconds, wallSeconds, framesPerSecond;
+  double p50Ms, p99Ms, meanMs, maxMs;  /* submission to completion */
+} BNXServerStats;
+BN_API BNXServer bnxServerCreate(BNContext context, const BNXServerConfig *config);
+BN_API void bnxServerDestroy(BNXServer server);
+/* returns the request id (>= 0), or -1 on error; callable from any thread */
+BN_API long long bnxServerSubmit(BNXServer server, const BNXRequest *request);
+/* waits up to timeoutMs (< 0: forever) for a request; copies its colour
+   channel into hostPixels (may be NULL) and forgets it.  Returns 1 when
+   done, 0 on timeout, a negative error code on failure. */
+BN_API int bnxServerWait(BNXServer server, long long id, int timeoutMs, void *hostPixels);
+BN_API void bnxServerGetStats(BNXServer server, BNXServerStats *stats);
+BN_API void bnxServerResetStats(BNXServer server);
+
 #ifdef __cplusplus
 }
 #endif

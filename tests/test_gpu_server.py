@@ -1,0 +1,88 @@
+"""Continuous-batching server: every request's frame is identical whether it
+is rendered alone or in the mix with other requests (bit-exact, against the
+oracle and against a solo bnRender), requests are admitted by HBM budget, and
+a request that can never fit is rejected with an error."""
+import time
+
+import numpy as np
+import pytest
+
+from barney_b200 import synth
+from tests.helpers import assert_bitexact, oracle_render, small_blob_scene, small_noise_scene
+
+pytestmark = pytest.mark.gpu
+
+
+def _setup(budget, slots, slice_waves):
+    import barney_b200 as bn
+    ctx = bn.Context()
+    scenes = [small_noise_scene(n=40, w=48, h=32), small_blob_scene(n=24, w=40, h=36),
+              small_noise_scene(n=33, w=37, h=29, dtype="u8", phase="simple"),
+              small_noise_scene(n=24, w=16, h=16, dtype="f16", compensated_accum=True)]
+    rs = [bn.VolumeRenderer(d, context=ctx, color_format="float4") for d in scenes]
+    server = bn.Server(ctx, hbm_budget_bytes=budget, max_slots=slots, slice_waves=slice_waves)
+    return bn, ctx, scenes, rs, server
+
+
+def _expected(scene, cam, w, h, spp):
+    d = dict(scene, camera=cam, width=w, height=h)
+    if not d.get("compensated_accum"):
+        ref, _, _ = oracle_render(d, spp)
+        return ref
+    import oracle
+    sc = oracle.Scene(d)
+    acc = np.zeros((h, w, 4), np.float32)
+    comp = np.zeros_like(acc)
+    oracle.render(sc, 0, spp, accum=acc, comp=comp)
+    return oracle.resolve(acc, spp, comp=comp)
+
+
+@pytest.mark.parametrize("budget,slots,slice_waves", [(1 << 30, 8, 2), (60000, 4, 1), (1 << 30, 64, 16)])
+def test_mixed_requests_equal_solo_renders(budget, slots, slice_waves):
+    bn, ctx, scenes, rs, server = _setup(budget, slots, slice_waves)
+    try:
+        rng = np.random.default_rng(5)
+        reqs = []
+        for i in range(20):
+            k = i % len(scenes)
+            spp = int(rng.integers(1, 7))
+            w, h = 24 + 8 * (i % 4), 16 + 4 * (i % 3)
+            cam = synth.orbit_camera(rng)
+            reqs.append((server.submit(rs[k], cam, w, h, spp, "float4"), k, cam, w, h, spp))
+            time.sleep(float(rng.exponential(0.001)))
+        for rid, k, cam, w, h, spp in reqs:
+            out = np.zeros((h, w, 4), np.float32)
+            assert server.wait(rid, out, timeout_ms=60000)
+            assert_bitexact(out, _expected(scenes[k], cam, w, h, spp), f"request {rid}")
+        st = server.stats()
+        assert st["completed"] == 20 and st["rejected"] == 0
+        assert st["p50Ms"] > 0 and st["p99Ms"] >= st["p50Ms"]
+        assert st["peakBytes"] <= budget
+    finally:
+        server.close()
+        for r in rs:
+            r.close()
+        ctx.close()
+
+
+def test_request_beyond_budget_is_rejected_and_solo_render_matches():
+    bn, ctx, scenes, rs, server = _setup(50000, 4, 4)
+    try:
+        cam = synth.DEFAULT_CAMERA
+        big = server.submit(rs[0], cam, 200, 200, 2, "float4")  # 200*200*20 B > 50 kB budget
+        small = server.submit(rs[0], cam, 24, 16, 3, "float4")
+        with pytest.raises(bn.BarneyError):
+            server.wait(big, np.zeros((200, 200, 4), np.float32), timeout_ms=60000)
+        out = np.zeros((16, 24, 4), np.float32)
+        assert server.wait(small, out, timeout_ms=60000)
+        solo = bn.VolumeRenderer(dict(scenes[0], camera=cam, width=24, height=16), color_format="float4")
+        solo.set_spp(3)
+        solo.render()
+        assert_bitexact(out, solo.read(), "server vs bnRender")
+        solo.close()
+        assert server.stats()["rejected"] == 1
+    finally:
+        server.close()
+        for r in rs:
+            r.close()
+        ctx.close()
