@@ -68,8 +68,8 @@ class BNXRenderJob(ctypes.Structure):
 
 
 class BNXLaunchConfig(ctypes.Structure):
-    _fields_ = [("threadsPerBlock", ctypes.c_int), ("blocksPerSM", ctypes.c_int), ("genBatch", ctypes.c_int),
-                ("shadeBatch", ctypes.c_int), ("minBusy", ctypes.c_int), ("renderMs", ctypes.c_float)]
+    _fields_ = [("threadsPerBlock", ctypes.c_int), ("blocksPerSM", ctypes.c_int), ("serviceBatch", ctypes.c_int),
+                ("renderMs", ctypes.c_float)]
 
 
 class BNXServerConfig(ctypes.Structure):
@@ -129,7 +129,7 @@ def lib(build_if_missing=True):
         "bnxSetLaunchConfig": ([P, I, I], None), "bnxFrameBufferDevicePointer": ([P], P),
         "bnxVolumeGetMacrocells": ([P, P, P, P], None),
         "bnxRenderStructuredNoAlloc": ([P, P], I),
-        "bnxSetScheduling": ([P, I, I, I], None), "bnxRenderBatch": ([P, P, I], None),
+        "bnxSetScheduling": ([P, I], None), "bnxRenderBatch": ([P, P, I], None),
         "bnxSetBatchGraphs": ([P, I], None), "bnxAutotuneBatch": ([P, P, I, P], None),
         "bnxServerCreate": ([P, P], P), "bnxServerDestroy": ([P], None),
         "bnxServerSubmit": ([P, P], ctypes.c_longlong), "bnxServerWait": ([P, ctypes.c_longlong, I, P], I),
@@ -382,8 +382,8 @@ class VolumeRenderer:
         check()
         return ranges, maj
 
-    def set_scheduling(self, gen_batch=16, shade_batch=8, min_busy=8):
-        self.L.bnxSetScheduling(self.ctx, gen_batch, shade_batch, min_busy)
+    def set_scheduling(self, service_batch=16):
+        self.L.bnxSetScheduling(self.ctx, service_batch)
         check()
 
     def set_launch_config(self, blocks_per_sm=0, threads_per_block=0):

@@ -234,7 +234,7 @@ void renderBatch(Context *ctx, const std::vector<BatchEntry> &entries) {
     key.push_back((const void *)(intptr_t)(e.fb->width * 65536 + e.fb->height));
   }
   key.push_back((const void *)(intptr_t)(ctx->blocksPerSM * 4096 + ctx->threadsPerBlock));
-  key.push_back((const void *)(intptr_t)(ctx->sched.genBatch * 65536 + ctx->sched.shadeBatch * 256 + ctx->sched.minBusy));
+  key.push_back((const void *)(intptr_t)ctx->sched.serviceBatch);
   key.push_back((const void *)(intptr_t)n);
   auto enqueue = [&](cudaStream_t s, bool timed) {
     ck(cudaMemcpyAsync(ctx->batchJobs.ptr, ctx->hostJobs, n * sizeof(JobDD), cudaMemcpyHostToDevice, s), "job table");
@@ -772,14 +772,11 @@ BN_API int bnxRenderStructuredNoAlloc(const BNXNoAllocFrame *f, void *stream) {
   BN_CATCH(g_lastError)
 }
 
-BN_API void bnxSetScheduling(BNContext context, int genBatch, int shadeBatch, int minBusy) {
+BN_API void bnxSetScheduling(BNContext context, int serviceBatch) {
   BN_TRY
   Context *c = getContext(context);
-  if (genBatch < 1 || genBatch > 32 || shadeBatch < 1 || shadeBatch > 32 || minBusy < 0 || minBusy > 32)
-    throw Error(E_INVALID_ARG, "scheduling thresholds must lie in [1, 32] (minBusy in [0, 32])");
-  c->sched.genBatch = genBatch;
-  c->sched.shadeBatch = shadeBatch;
-  c->sched.minBusy = minBusy;
+  if (serviceBatch < 1 || serviceBatch > 32) throw Error(E_INVALID_ARG, "serviceBatch must lie in [1, 32]");
+  c->sched.serviceBatch = serviceBatch;
   BN_CATCH()
 }
 
@@ -821,33 +818,26 @@ BN_API void bnxAutotuneBatch(BNContext context, const BNXRenderJob *jobs, int nu
   std::vector<uint32_t> saved;
   for (auto &x : e) saved.push_back(x.fb->accumID);
   const int maxBps = std::max(1, renderKernelMaxBlocksPerSM(128));
-  struct Cand { int tpb, bps, gen, shade, busy; };
+  struct Cand { int tpb, bps, service; };
   std::vector<Cand> cands;
   for (int tpb : {64, 128})
-    for (int gen : {8, 16, 24})
-      for (int shade : {4, 8, 16})
-        cands.push_back({tpb, tpb == 64 ? 2 * maxBps : maxBps, gen, shade, 8});
-  const int oldTpb = c->threadsPerBlock, oldBps = c->blocksPerSM;
-  const SchedDD oldSched = c->sched;
-  Cand bestC{oldTpb, oldBps, oldSched.genBatch, oldSched.shadeBatch, oldSched.minBusy};
+    for (int service : {4, 8, 12, 16, 20, 24, 28})
+      cands.push_back({tpb, tpb == 64 ? 2 * maxBps : maxBps, service});
+  Cand bestC{c->threadsPerBlock, c->blocksPerSM, c->sched.serviceBatch};
   float bestMs = 1e30f;
   for (const Cand &k : cands) {
     c->threadsPerBlock = k.tpb;
     c->blocksPerSM = k.bps;
-    c->sched.genBatch = k.gen;
-    c->sched.shadeBatch = k.shade;
-    c->sched.minBusy = k.busy;
+    c->sched.serviceBatch = k.service;
     for (size_t i = 0; i < e.size(); i++) e[i].fb->accumID = saved[i];
     renderBatch(c, e);
     if (c->stats.renderMs < bestMs) { bestMs = c->stats.renderMs; bestC = k; }
   }
   c->threadsPerBlock = bestC.tpb;
   c->blocksPerSM = bestC.bps;
-  c->sched.genBatch = bestC.gen;
-  c->sched.shadeBatch = bestC.shade;
-  c->sched.minBusy = bestC.busy;
+  c->sched.serviceBatch = bestC.service;
   for (auto &x : e) x.fb->accumID = 0;  // tuning frames are discarded
-  if (best) *best = {bestC.tpb, bestC.bps, bestC.gen, bestC.shade, bestC.busy, bestMs};
+  if (best) *best = {bestC.tpb, bestC.bps, bestC.service, bestMs};
   BN_CATCH()
 }
 

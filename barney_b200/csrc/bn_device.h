@@ -73,14 +73,12 @@ struct JobDD {
   FrameDD fr;
 };
 
-// Warp scheduling of the render loop: primary rays are generated once at
-// least genBatch lanes of a warp need one, collisions shaded once at least
-// shadeBatch lanes have one -- or as soon as fewer than minBusy lanes are
-// inside a Woodcock range.
+// Warp scheduling of the render loop: a warp keeps stepping macrocells and
+// Woodcock ranges until at least serviceBatch of its lanes (or all of its
+// busy lanes) need service -- shading, accumulation, a new ray -- and then
+// serves them together.
 struct SchedDD {
-  int genBatch = 16;
-  int shadeBatch = 8;
-  int minBusy = 8;
+  int serviceBatch = 16;
 };
 
 // Device counters of one launch (samples, mcVisits, rays, errorFlags)

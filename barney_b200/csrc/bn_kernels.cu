@@ -478,9 +478,144 @@ DEV void renderLoop(const JobDD *jobs, const int *chunkStart, int numJobs, int n
   bool shadowRay = false;
   unsigned steps = 0;
 
+  // Each round: (A) one service pass over the lanes whose ray needs host
+  // work -- shading, accumulation, a new pixel, ray generation, ray set-up --
+  // then (B) a tight loop that only steps macrocells and Woodcock ranges
+  // until at least sd.serviceBatch lanes (or every busy lane) need service.
   while (true) {
+    {
+      const JobDD &J = jobs[BATCH ? job : 0];
+      const VolumeDD &v = J.v;
+      const FrameDD &fr = J.fr;
+      // ------------------------------------------------------------------
+      // A1. collisions: shading and shadow-ray spawn (shadeRays.cu:608-746)
+      // ------------------------------------------------------------------
+      if (phase == LP_HIT) {
+        const int accumID = fr.accumID0 + k;
+        const float clampMax = 10.f * (1 + accumID);
+        const bool cmp = fr.comp != nullptr;
+        bool spawned = false;
+        if (!shadowRay) {
+          // primary hit: generation-0 accumulation (fragment 0, alpha 1)
+          if (accumID == 0) {
+            acc = make_float4(0.f, 0.f, 0.f, 1.f);
+            comp = make_float4(0.f, 0.f, 0.f, 0.f);
+          } else {
+            accAdd(acc.w, comp.w, 1.f, cmp);
+          }
+          const float tHit = ts.t;
+          const float3 P = f3(ts.org.x + tHit * ts.dir.x, ts.org.y + tHit * ts.dir.y, ts.org.z + tHit * ts.dir.z);
+          if (fr.emissionAbsorption) {
+            const float ex = fmin_(hitRGB.x, clampMax), ey = fmin_(hitRGB.y, clampMax), ez = fmin_(hitRGB.z, clampMax);
+            if (accumID == 0) acc = make_float4(ex, ey, ez, 1.f);
+            else {
+              if (ex > 0.f) accAdd(acc.x, comp.x, ex, cmp);
+              if (ey > 0.f) accAdd(acc.y, comp.y, ey, cmp);
+              if (ez > 0.f) accAdd(acc.z, comp.z, ez, cmp);
+            }
+          } else {
+            // bounce() volume-hit branch, shadeRays.cu:608-746
+            uint64_t random = rngDerive(raySeed, (uint64_t)__float_as_uint(tHit));
+            const float3 won = normalize3(primDir);
+            const float3 woN = f3(-won.x, -won.y, -won.z);  // dg.wo
+            const float offsetEpsilon = fmax_(1e-4f, 1e-6f * fmax_(fmax_(fabsf(P.x), fabsf(P.y)), fabsf(P.z)));
+            LightSample ls;
+            bool needsMIS, isDir;
+            if (sampleLights(fr, random, ls, needsMIS, isDir)) {
+              float3 alb;
+              float fpdf;
+              if (v.phase == PHASE_SIMPLE) {
+                alb = f3(.7f * hitRGB.x, .7f * hitRGB.y, .7f * hitRGB.z);
+                fpdf = kOneOverFourPi;
+              } else {
+                alb = f3(v.scatteringAlbedo * hitRGB.x, v.scatteringAlbedo * hitRGB.y, v.scatteringAlbedo * hitRGB.z);
+                const float3 wi_in = normalize3(f3(-woN.x, -woN.y, -woN.z));
+                fpdf = hgPhase(v.anisotropy, dot3(wi_in, normalize3(ls.dir)));
+              }
+              float3 fv = f3(fpdf * alb.x, fpdf * alb.y, fpdf * alb.z);
+              if (fpdf > 0.f && !(fmax_(fmax_(fv.x, fv.y), fv.z) < 1e-4f)) {
+                fv = f3(fmin_(fv.x, 13.f), fmin_(fv.y, 13.f), fmin_(fv.z, 13.f));
+                const float ip = isinf(ls.pdf) ? 1.f : (1.f / ls.pdf);
+                const float3 tp = f3(1.f * ip * fv.x * ls.radiance.x * 1.f, 1.f * ip * fv.y * ls.radiance.y * 1.f,
+                                     1.f * ip * fv.z * ls.radiance.z * 1.f);
+                misWeight = 1.f;
+                bool alive = true;
+                if (!isDir && needsMIS) {
+                  const float pl = kOneOverFourPi;
+                  float ps;
+                  if (v.phase == PHASE_SIMPLE) ps = kOneOverFourPi;
+                  else ps = hgPhase(v.anisotropy, dot3(normalize3(f3(-woN.x, -woN.y, -woN.z)), normalize3(ls.dir)));
+                  misWeight = pl / (pl + ps + 1e-10f);
+                  if (misWeight < 1e-5f) alive = false;
+                }
+                const float sTMax = kInf * (1.f - 2.f * offsetEpsilon);
+                if (alive && sTMax > 0.f) {
+                  shadowTp = f3(roundHalf(tp.x), roundHalf(tp.y), roundHalf(tp.z));
+                  // makeShadowRay (Ray.h:147-157); its RNG seed is the primary's,
+                  // which is not used again by this wave
+                  ts.org = f3(P.x + offsetEpsilon * woN.x, P.y + offsetEpsilon * woN.y, P.z + offsetEpsilon * woN.z);
+                  ts.dir = ls.dir;
+                  ts.rayTMax = sTMax;
+                  shadowRay = true;
+                  spawned = true;
+                  nRays++;
+                  steps = 0;
+                  phase = LP_BEGIN;
+                }
+              }
+            }
+          }
+        }
+        if (!spawned) {  // shadow ray occluded, or no shadow ray: the wave is done
+          if (++k == fr.spp) {
+            fr.accum[pix] = acc;
+            if (cmp) fr.comp[pix] = comp;
+            phase = LP_IDLE;
+          } else {
+            phase = LP_NEWSAMPLE;
+          }
+        }
+      }
+
+      // ------------------------------------------------------------------
+      // A2. rays that left the grid: bounce() without intersection
+      //    (shadeRays.cu:507-600) and accumulation (:996-1040)
+      // ------------------------------------------------------------------
+      if (phase == LP_ENDED) {
+        const int accumID = fr.accumID0 + k;
+        const float clampMax = 10.f * (1 + accumID);
+        const bool cmp = fr.comp != nullptr;
+        if (!shadowRay) {
+          const float f0x = fmin_(bg.x, clampMax), f0y = fmin_(bg.y, clampMax), f0z = fmin_(bg.z, clampMax);
+          if (accumID == 0) {
+            acc = make_float4(f0x, f0y, f0z, bg.w);
+            comp = make_float4(0.f, 0.f, 0.f, 0.f);
+          } else {
+            if (bg.w > 0.f) accAdd(acc.w, comp.w, bg.w, cmp);
+            if (f0x > 0.f) accAdd(acc.x, comp.x, f0x, cmp);
+            if (f0y > 0.f) accAdd(acc.y, comp.y, f0y, cmp);
+            if (f0z > 0.f) accAdd(acc.z, comp.z, f0z, cmp);
+          }
+        } else {  // the shadow ray reached the light
+          const float f1x = fmin_(misWeight * shadowTp.x, clampMax);
+          const float f1y = fmin_(misWeight * shadowTp.y, clampMax);
+          const float f1z = fmin_(misWeight * shadowTp.z, clampMax);
+          if (f1x > 0.f) accAdd(acc.x, comp.x, f1x, cmp);
+          if (f1y > 0.f) accAdd(acc.y, comp.y, f1y, cmp);
+          if (f1z > 0.f) accAdd(acc.z, comp.z, f1z, cmp);
+        }
+        if (++k == fr.spp) {
+          fr.accum[pix] = acc;
+          if (cmp) fr.comp[pix] = comp;
+          phase = LP_IDLE;
+        } else {
+          phase = LP_NEWSAMPLE;
+        }
+      }
+
+    }
     // ------------------------------------------------------------------
-    // 1. lanes without a pixel take the next ones of the warp's chunk
+    // A3. lanes without a pixel take the next ones of the warp's chunk
     // ------------------------------------------------------------------
     unsigned need = __ballot_sync(FULL, phase == LP_IDLE);
     while (need && !exhausted) {
@@ -534,258 +669,139 @@ DEV void renderLoop(const JobDD *jobs, const int *chunkStart, int numJobs, int n
       chunkLeft -= take;
     }
     if (!__ballot_sync(FULL, phase != LP_IDLE)) break;  // no work left for this warp
-    const int nWood = __popc(__ballot_sync(FULL, phase == LP_WOODCOCK));
-    const int nHit = __popc(__ballot_sync(FULL, phase == LP_HIT));
-    const int nNew = __popc(__ballot_sync(FULL, phase == LP_NEWSAMPLE));
-    const JobDD &J = jobs[BATCH ? job : 0];
-    const VolumeDD &v = J.v;
-    const FrameDD &fr = J.fr;
-
-    // ------------------------------------------------------------------
-    // 2. one Woodcock step (Volume.h:180-201)
-    // ------------------------------------------------------------------
-    if (phase == LP_WOODCOCK) {
-      const float r = rngFloat(ts.rng);
-      const bool exact = LOG == 1 || (LOG == 2 && fr.exactLog);
-      const float dt = exact ? (-logf(1.f - r) / ts.maj) : (-fastLog(1.f - r) / ts.maj);
-      ts.t += dt;
-      if (ts.t >= ts.tUpper) {
-        const float tClosest = fmin_(fmin_(ts.tNext.x, ts.tNext.y), ts.tNext.z);
-        phase = ddaStep(v, ts, tClosest) ? LP_CELL : LP_ENDED;
-      } else {
-        const float3 P = f3(ts.org.x + ts.t * ts.dir.x, ts.org.y + ts.t * ts.dir.y, ts.org.z + ts.t * ts.dir.z);
-        const float s = sampleJob<T>(v, P, u8lut);
-        nSamples++;
-        float w = 0.f, f = 0.f;
-        int idx = 0;
-        if (!isnan(s)) {
-          const float span = v.domHi - v.domLo;
-          f = span == 1.f ? (s - v.domLo) : (s - v.domLo) / span;  // x/1 == x exactly
-          f = fmin_(1.f, fmax_(0.f, f));
-          f *= (float)(v.tfN - 1);
-          idx = min(v.tfN - 2, max(0, (int)f));
-          f -= (float)idx;
-          const float w0 = BATCH ? __ldg(&v.tf[idx].w) : sTF[idx].w;
-          const float w1 = BATCH ? __ldg(&v.tf[idx + 1].w) : sTF[idx + 1].w;
-          w = ((1.f - f) * w0 + f * w1) * v.baseDensity;
-        }
-        if (w >= rngFloat(ts.rng) * ts.maj) {
-          hitRGB = f3(0.f, 0.f, 0.f);
-          if (!isnan(s)) {
-            const float4 a = BATCH ? __ldg(&v.tf[idx]) : sTF[idx];
-            const float4 b = BATCH ? __ldg(&v.tf[idx + 1]) : sTF[idx + 1];
-            hitRGB = f3((1.f - f) * a.x + f * b.x, (1.f - f) * a.y + f * b.y, (1.f - f) * a.z + f * b.z);
-          }
-          phase = LP_HIT;
-        }
-      }
-      if (++steps > (1u << 22)) {  // iteration cap: end this ray as if it left the grid
-        errBits |= ERR_ITER_CAP;
-        phase = LP_ENDED;
-      }
-    }
-
-    // ------------------------------------------------------------------
-    // 3. rays that left the grid: bounce() without intersection
-    //    (shadeRays.cu:507-600) and accumulation (:996-1040)
-    // ------------------------------------------------------------------
-    if (phase == LP_ENDED) {
-      const int accumID = fr.accumID0 + k;
-      const float clampMax = 10.f * (1 + accumID);
-      const bool cmp = fr.comp != nullptr;
-      if (!shadowRay) {
-        const float f0x = fmin_(bg.x, clampMax), f0y = fmin_(bg.y, clampMax), f0z = fmin_(bg.z, clampMax);
-        if (accumID == 0) {
-          acc = make_float4(f0x, f0y, f0z, bg.w);
-          comp = make_float4(0.f, 0.f, 0.f, 0.f);
-        } else {
-          if (bg.w > 0.f) accAdd(acc.w, comp.w, bg.w, cmp);
-          if (f0x > 0.f) accAdd(acc.x, comp.x, f0x, cmp);
-          if (f0y > 0.f) accAdd(acc.y, comp.y, f0y, cmp);
-          if (f0z > 0.f) accAdd(acc.z, comp.z, f0z, cmp);
-        }
-      } else {  // the shadow ray reached the light
-        const float f1x = fmin_(misWeight * shadowTp.x, clampMax);
-        const float f1y = fmin_(misWeight * shadowTp.y, clampMax);
-        const float f1z = fmin_(misWeight * shadowTp.z, clampMax);
-        if (f1x > 0.f) accAdd(acc.x, comp.x, f1x, cmp);
-        if (f1y > 0.f) accAdd(acc.y, comp.y, f1y, cmp);
-        if (f1z > 0.f) accAdd(acc.z, comp.z, f1z, cmp);
-      }
-      if (++k == fr.spp) {
-        fr.accum[pix] = acc;
-        if (cmp) fr.comp[pix] = comp;
-        phase = LP_IDLE;
-      } else {
-        phase = LP_NEWSAMPLE;
-      }
-    }
-
-    // ------------------------------------------------------------------
-    // 4. collisions, shaded together once enough lanes have one
-    // ------------------------------------------------------------------
-    const bool doShade = nHit > 0 && (nHit >= sd.shadeBatch || nWood < sd.minBusy);
-    if (doShade && phase == LP_HIT) {
-      const int accumID = fr.accumID0 + k;
-      const float clampMax = 10.f * (1 + accumID);
-      const bool cmp = fr.comp != nullptr;
-      bool spawned = false;
-      if (!shadowRay) {
-        // primary hit: generation-0 accumulation (fragment 0, alpha 1)
-        if (accumID == 0) {
-          acc = make_float4(0.f, 0.f, 0.f, 1.f);
-          comp = make_float4(0.f, 0.f, 0.f, 0.f);
-        } else {
-          accAdd(acc.w, comp.w, 1.f, cmp);
-        }
-        const float tHit = ts.t;
-        const float3 P = f3(ts.org.x + tHit * ts.dir.x, ts.org.y + tHit * ts.dir.y, ts.org.z + tHit * ts.dir.z);
-        if (fr.emissionAbsorption) {
-          const float ex = fmin_(hitRGB.x, clampMax), ey = fmin_(hitRGB.y, clampMax), ez = fmin_(hitRGB.z, clampMax);
-          if (accumID == 0) acc = make_float4(ex, ey, ez, 1.f);
-          else {
-            if (ex > 0.f) accAdd(acc.x, comp.x, ex, cmp);
-            if (ey > 0.f) accAdd(acc.y, comp.y, ey, cmp);
-            if (ez > 0.f) accAdd(acc.z, comp.z, ez, cmp);
-          }
-        } else {
-          // bounce() volume-hit branch, shadeRays.cu:608-746
-          uint64_t random = rngDerive(raySeed, (uint64_t)__float_as_uint(tHit));
-          const float3 won = normalize3(primDir);
-          const float3 woN = f3(-won.x, -won.y, -won.z);  // dg.wo
-          const float offsetEpsilon = fmax_(1e-4f, 1e-6f * fmax_(fmax_(fabsf(P.x), fabsf(P.y)), fabsf(P.z)));
-          LightSample ls;
-          bool needsMIS, isDir;
-          if (sampleLights(fr, random, ls, needsMIS, isDir)) {
-            float3 alb;
-            float fpdf;
-            if (v.phase == PHASE_SIMPLE) {
-              alb = f3(.7f * hitRGB.x, .7f * hitRGB.y, .7f * hitRGB.z);
-              fpdf = kOneOverFourPi;
-            } else {
-              alb = f3(v.scatteringAlbedo * hitRGB.x, v.scatteringAlbedo * hitRGB.y, v.scatteringAlbedo * hitRGB.z);
-              const float3 wi_in = normalize3(f3(-woN.x, -woN.y, -woN.z));
-              fpdf = hgPhase(v.anisotropy, dot3(wi_in, normalize3(ls.dir)));
-            }
-            float3 fv = f3(fpdf * alb.x, fpdf * alb.y, fpdf * alb.z);
-            if (fpdf > 0.f && !(fmax_(fmax_(fv.x, fv.y), fv.z) < 1e-4f)) {
-              fv = f3(fmin_(fv.x, 13.f), fmin_(fv.y, 13.f), fmin_(fv.z, 13.f));
-              const float ip = isinf(ls.pdf) ? 1.f : (1.f / ls.pdf);
-              const float3 tp = f3(1.f * ip * fv.x * ls.radiance.x * 1.f, 1.f * ip * fv.y * ls.radiance.y * 1.f,
-                                   1.f * ip * fv.z * ls.radiance.z * 1.f);
-              misWeight = 1.f;
-              bool alive = true;
-              if (!isDir && needsMIS) {
-                const float pl = kOneOverFourPi;
-                float ps;
-                if (v.phase == PHASE_SIMPLE) ps = kOneOverFourPi;
-                else ps = hgPhase(v.anisotropy, dot3(normalize3(f3(-woN.x, -woN.y, -woN.z)), normalize3(ls.dir)));
-                misWeight = pl / (pl + ps + 1e-10f);
-                if (misWeight < 1e-5f) alive = false;
-              }
-              const float sTMax = kInf * (1.f - 2.f * offsetEpsilon);
-              if (alive && sTMax > 0.f) {
-                shadowTp = f3(roundHalf(tp.x), roundHalf(tp.y), roundHalf(tp.z));
-                // makeShadowRay (Ray.h:147-157); its RNG seed is the primary's,
-                // which is not used again by this wave
-                ts.org = f3(P.x + offsetEpsilon * woN.x, P.y + offsetEpsilon * woN.y, P.z + offsetEpsilon * woN.z);
-                ts.dir = ls.dir;
-                ts.rayTMax = sTMax;
-                shadowRay = true;
-                spawned = true;
-                nRays++;
-                steps = 0;
-                phase = LP_BEGIN;
-              }
-            }
+    {
+      const JobDD &J = jobs[BATCH ? job : 0];
+      const VolumeDD &v = J.v;
+      const FrameDD &fr = J.fr;
+      // ------------------------------------------------------------------
+      // A4. primary rays
+      //    (generateRays.cu:71-243)
+      // ------------------------------------------------------------------
+      if (phase == LP_NEWSAMPLE) {
+        const int W = fr.width, H = fr.height;
+        const int accumID = fr.accumID0 + k;
+        uint64_t rnd = rngSeed2(unsigned(ix + W * accumID), unsigned(iy + H * accumID));
+        raySeed = rngSeed2((uint32_t)(ix + accumID * W), (uint32_t)iy);
+        const float pixel_u = (accumID == 0) ? .5f : rngFloat(rnd);
+        const float pixel_v = (accumID == 0) ? .5f : rngFloat(rnd);
+        const float image_u = ((ix + pixel_u) / float(W));
+        const float image_v = ((iy + pixel_v) / float(H));
+        const float aspect = W / float(H);
+        const float su = 1.f * aspect * (image_u - .5f), sv = 1.f * (image_v - .5f);
+        float3 d = f3(fr.dir00.x + su * fr.dirdu.x + sv * fr.dirdv.x, fr.dir00.y + su * fr.dirdu.y + sv * fr.dirdv.y,
+                      fr.dir00.z + su * fr.dirdu.z + sv * fr.dirdv.z);
+        d = normalize3(d);
+        float3 o = fr.lens00;
+        float tMax = 1e30f;
+        if (fr.cutPlane.w > -1e28f) {
+          const float3 N = f3(fr.cutPlane.x, fr.cutPlane.y, fr.cutPlane.z);
+          const float dist_org = dot3(N, o) + fr.cutPlane.w;
+          const float denom = dot3(N, d);
+          if (dist_org >= 0.f) {
+            if (denom < 0.f) tMax = fmin_(tMax, -dist_org / denom);
+          } else {
+            if (denom > 0.f) {
+              const float te = -dist_org / denom;
+              o = f3(o.x + te * d.x, o.y + te * d.y, o.z + te * d.z);
+            } else tMax = 0.f;
           }
         }
-      }
-      if (!spawned) {  // shadow ray occluded, or no shadow ray: the wave is done
-        if (++k == fr.spp) {
-          fr.accum[pix] = acc;
-          if (cmp) fr.comp[pix] = comp;
-          phase = LP_IDLE;
-        } else {
-          phase = LP_NEWSAMPLE;
+        if (fr.bgColor.w >= 0.f) bg = fr.bgColor;
+        else {
+          const float t = (iy + .5f) / float(H);
+          bg = make_float4((1.0f - t) * 0.9f + t * 0.15f, (1.0f - t) * 0.9f + t * 0.25f, (1.0f - t) * 0.9f + t * .8f,
+                           (1.0f - t) * 1.f + t * 1.f);
         }
+        primDir = d;
+        shadowRay = false;
+        nRays++;
+        steps = 0;
+        ts.org = o;
+        ts.dir = d;
+        ts.rayTMax = tMax;
+        phase = LP_BEGIN;
       }
+
+      // ------------------------------------------------------------------
+      // A5. ray set-up, primary and shadow rays together
+      // ------------------------------------------------------------------
+      if (phase == LP_BEGIN) phase = traceBegin(v, ts, ts.org, ts.dir, ts.rayTMax, raySeed) ? LP_CELL : LP_ENDED;
+
     }
-
-    // ------------------------------------------------------------------
-    // 5. primary rays, generated together once enough lanes need one
-    //    (generateRays.cu:71-243)
-    // ------------------------------------------------------------------
-    const bool doGen = nNew > 0 && (nNew >= sd.genBatch || nWood < sd.minBusy);
-    if (doGen && phase == LP_NEWSAMPLE) {
-      const int W = fr.width, H = fr.height;
-      const int accumID = fr.accumID0 + k;
-      uint64_t rnd = rngSeed2(unsigned(ix + W * accumID), unsigned(iy + H * accumID));
-      raySeed = rngSeed2((uint32_t)(ix + accumID * W), (uint32_t)iy);
-      const float pixel_u = (accumID == 0) ? .5f : rngFloat(rnd);
-      const float pixel_v = (accumID == 0) ? .5f : rngFloat(rnd);
-      const float image_u = ((ix + pixel_u) / float(W));
-      const float image_v = ((iy + pixel_v) / float(H));
-      const float aspect = W / float(H);
-      const float su = 1.f * aspect * (image_u - .5f), sv = 1.f * (image_v - .5f);
-      float3 d = f3(fr.dir00.x + su * fr.dirdu.x + sv * fr.dirdv.x, fr.dir00.y + su * fr.dirdu.y + sv * fr.dirdv.y,
-                    fr.dir00.z + su * fr.dirdu.z + sv * fr.dirdv.z);
-      d = normalize3(d);
-      float3 o = fr.lens00;
-      float tMax = 1e30f;
-      if (fr.cutPlane.w > -1e28f) {
-        const float3 N = f3(fr.cutPlane.x, fr.cutPlane.y, fr.cutPlane.z);
-        const float dist_org = dot3(N, o) + fr.cutPlane.w;
-        const float denom = dot3(N, d);
-        if (dist_org >= 0.f) {
-          if (denom < 0.f) tMax = fmin_(tMax, -dist_org / denom);
-        } else {
-          if (denom > 0.f) {
-            const float te = -dist_org / denom;
-            o = f3(o.x + te * d.x, o.y + te * d.y, o.z + te * d.z);
-          } else tMax = 0.f;
-        }
-      }
-      if (fr.bgColor.w >= 0.f) bg = fr.bgColor;
-      else {
-        const float t = (iy + .5f) / float(H);
-        bg = make_float4((1.0f - t) * 0.9f + t * 0.15f, (1.0f - t) * 0.9f + t * 0.25f, (1.0f - t) * 0.9f + t * .8f,
-                         (1.0f - t) * 1.f + t * 1.f);
-      }
-      primDir = d;
-      shadowRay = false;
-      nRays++;
-      steps = 0;
-      ts.org = o;
-      ts.dir = d;
-      ts.rayTMax = tMax;
-      phase = LP_BEGIN;
-    }
-
-    // ------------------------------------------------------------------
-    // 6. ray set-up, primary and shadow rays together
-    // ------------------------------------------------------------------
-    if (phase == LP_BEGIN) phase = traceBegin(v, ts, ts.org, ts.dir, ts.rayTMax, raySeed) ? LP_CELL : LP_ENDED;
-
-    // ------------------------------------------------------------------
-    // 7. next macrocell with a non-zero majorant (DDA.h:172-200,
-    //    MCAccelerator.h:596-612)
-    // ------------------------------------------------------------------
-    if (phase == LP_CELL) {
+    {
+      const JobDD &J = jobs[BATCH ? job : 0];
+      const VolumeDD &v = J.v;
+      const FrameDD &fr = J.fr;
       while (true) {
-        const float tClosest = fmin_(fmin_(ts.tNext.x, ts.tNext.y), ts.tNext.z);
-        const float maj = __ldg(v.majorants + (ts.cx + (int64_t)v.mcDims.x * (ts.cy + (int64_t)v.mcDims.y * ts.cz)));
-        nVisits++;
-        if (maj == 0.f) {
-          if (!ddaStep(v, ts, tClosest)) { phase = LP_ENDED; break; }
-          if (++steps > (1u << 22)) { errBits |= ERR_ITER_CAP; phase = LP_ENDED; break; }
-        } else {
-          ts.maj = maj;
-          ts.t = ts.rayT0 + ts.nextCellBegin;
-          ts.tUpper = fmin_(ts.rayT0 + fmin_(tClosest, ts.ddaTMax), ts.rayTMax);
-          phase = LP_WOODCOCK;
-          break;
+        // ------------------------------------------------------------------
+        // B1. next macrocell with a non-zero majorant (DDA.h:172-200,
+        //    MCAccelerator.h:596-612)
+        // ------------------------------------------------------------------
+        if (phase == LP_CELL) {
+          while (true) {
+            const float tClosest = fmin_(fmin_(ts.tNext.x, ts.tNext.y), ts.tNext.z);
+            const float maj = __ldg(v.majorants + (ts.cx + (int64_t)v.mcDims.x * (ts.cy + (int64_t)v.mcDims.y * ts.cz)));
+            nVisits++;
+            if (maj == 0.f) {
+              if (!ddaStep(v, ts, tClosest)) { phase = LP_ENDED; break; }
+              if (++steps > (1u << 22)) { errBits |= ERR_ITER_CAP; phase = LP_ENDED; break; }
+            } else {
+              ts.maj = maj;
+              ts.t = ts.rayT0 + ts.nextCellBegin;
+              ts.tUpper = fmin_(ts.rayT0 + fmin_(tClosest, ts.ddaTMax), ts.rayTMax);
+              phase = LP_WOODCOCK;
+              break;
+            }
+          }
         }
+        // ------------------------------------------------------------------
+        // B2. one Woodcock step (Volume.h:180-201)
+        // ------------------------------------------------------------------
+        if (phase == LP_WOODCOCK) {
+          const float r = rngFloat(ts.rng);
+          const bool exact = LOG == 1 || (LOG == 2 && fr.exactLog);
+          const float dt = exact ? (-logf(1.f - r) / ts.maj) : (-fastLog(1.f - r) / ts.maj);
+          ts.t += dt;
+          if (ts.t >= ts.tUpper) {
+            const float tClosest = fmin_(fmin_(ts.tNext.x, ts.tNext.y), ts.tNext.z);
+            phase = ddaStep(v, ts, tClosest) ? LP_CELL : LP_ENDED;
+          } else {
+            const float3 P = f3(ts.org.x + ts.t * ts.dir.x, ts.org.y + ts.t * ts.dir.y, ts.org.z + ts.t * ts.dir.z);
+            const float s = sampleJob<T>(v, P, u8lut);
+            nSamples++;
+            float w = 0.f, f = 0.f;
+            int idx = 0;
+            if (!isnan(s)) {
+              const float span = v.domHi - v.domLo;
+              f = span == 1.f ? (s - v.domLo) : (s - v.domLo) / span;  // x/1 == x exactly
+              f = fmin_(1.f, fmax_(0.f, f));
+              f *= (float)(v.tfN - 1);
+              idx = min(v.tfN - 2, max(0, (int)f));
+              f -= (float)idx;
+              const float w0 = BATCH ? __ldg(&v.tf[idx].w) : sTF[idx].w;
+              const float w1 = BATCH ? __ldg(&v.tf[idx + 1].w) : sTF[idx + 1].w;
+              w = ((1.f - f) * w0 + f * w1) * v.baseDensity;
+            }
+            if (w >= rngFloat(ts.rng) * ts.maj) {
+              hitRGB = f3(0.f, 0.f, 0.f);
+              if (!isnan(s)) {
+                const float4 a = BATCH ? __ldg(&v.tf[idx]) : sTF[idx];
+                const float4 b = BATCH ? __ldg(&v.tf[idx + 1]) : sTF[idx + 1];
+                hitRGB = f3((1.f - f) * a.x + f * b.x, (1.f - f) * a.y + f * b.y, (1.f - f) * a.z + f * b.z);
+              }
+              phase = LP_HIT;
+            }
+          }
+          if (++steps > (1u << 22)) {  // iteration cap: end this ray as if it left the grid
+            errBits |= ERR_ITER_CAP;
+            phase = LP_ENDED;
+          }
+        }
+
+        const bool moving = phase == LP_WOODCOCK || phase == LP_CELL;
+        const int nMoving = __popc(__ballot_sync(FULL, moving));
+        const int nWaiting = __popc(__ballot_sync(FULL, !moving && (phase != LP_IDLE || !exhausted)));
+        if (nMoving == 0 || nWaiting >= sd.serviceBatch) break;
       }
     }
   }

@@ -10,9 +10,9 @@
 //      and a batch slot is free;
 //   2. render one slice -- at most sliceWaves waves of every admitted request
 //      -- in one persistent launch of the batch kernel (renderBatch);
-//   3. requests whose waves are all done are resolved; their colour is copied
-//      to a pinned staging buffer, their device buffers return to the pool,
-//      and waiters are woken.
+//   3. requests whose waves are all done keep only their resolved colour
+//      buffer (counted against the budget until the client reads it); their
+//      other device buffers return to the pool and waiters are woken.
 //
 // Requests that arrive while a slice is on the GPU join the next slice, so
 // their work overlaps with every other admitted request's on the device.
@@ -42,18 +42,17 @@ struct ServerRequest {
   Clock::time_point submitted, admitted, finished;
   bool done = false, failed = false;
   std::string error;
-  void *staging = nullptr;  // pinned host copy of the colour channel
-  size_t stagingBytes = 0;
+  void *result = nullptr;   // device colour channel, held until the client reads it
+  size_t resultBytes = 0;
 };
 
-// Pool of equally sized device / pinned buffers, so steady-state serving
-// performs no cudaMalloc / cudaFree (either would synchronise the device).
+// Pool of equally sized device buffers, so steady-state serving performs
+// no cudaMalloc / cudaFree (either would synchronise the device).
 struct BufferPool {
-  std::multimap<size_t, void *> freeDevice, freeHost;
+  std::multimap<size_t, void *> freeDevice;
   size_t deviceBytesHeld = 0;
   ~BufferPool() {
     for (auto &kv : freeDevice) cudaFree(kv.second);
-    for (auto &kv : freeHost) cudaFreeHost(kv.second);
   }
   void *getDevice(size_t n) {
     auto it = freeDevice.find(n);
@@ -64,14 +63,6 @@ struct BufferPool {
     return p;
   }
   void putDevice(void *p, size_t n) { if (p) freeDevice.emplace(n, p); }
-  void *getHost(size_t n) {
-    auto it = freeHost.find(n);
-    if (it != freeHost.end()) { void *p = it->second; freeHost.erase(it); return p; }
-    void *p = nullptr;
-    ck(cudaHostAlloc(&p, n, cudaHostAllocDefault), "server staging buffer");
-    return p;
-  }
-  void putHost(void *p, size_t n) { if (p) freeHost.emplace(n, p); }
 };
 
 struct Server {
@@ -94,7 +85,12 @@ struct Server {
   Clock::time_point statsStart = Clock::now();
   unsigned long long samples = 0;
 
-  Server(Context *c, const BNXServerConfig &config) : ctx(c), cfg(config) { worker = std::thread([this] { loop(); }); }
+  cudaStream_t copyStream = nullptr;  // client read-back, off the render stream
+
+  Server(Context *c, const BNXServerConfig &config) : ctx(c), cfg(config) {
+    ck(cudaStreamCreateWithFlags(&copyStream, cudaStreamNonBlocking), "server copy stream");
+    worker = std::thread([this] { loop(); });
+  }
   ~Server() {
     {
       std::lock_guard<std::mutex> l(m);
@@ -103,7 +99,16 @@ struct Server {
     cvWork.notify_all();
     if (worker.joinable()) worker.join();
     for (auto &r : active) releaseDevice(*r);
-    for (auto &kv : finished) pool.putHost(kv.second->staging, kv.second->stagingBytes);
+    for (auto &kv : finished) releaseResult(*kv.second);
+    if (copyStream) cudaStreamDestroy(copyStream);
+    cudaGetLastError();
+  }
+
+  void releaseResult(ServerRequest &r) {
+    if (!r.result) return;
+    pool.putDevice(r.result, r.resultBytes);
+    bytesInUse -= r.resultBytes;
+    r.result = nullptr;
   }
 
   static size_t bytesFor(int w, int h, int fmt, bool comp) {
@@ -111,16 +116,23 @@ struct Server {
     return px * 16 + (comp ? px * 16 : 0) + px * (fmt == FMT_FLOAT4 ? 16 : 4);
   }
 
-  void releaseDevice(ServerRequest &r) {
+  // Returns the request's accumulation buffers to the pool; the colour buffer
+  // moves to r.result when keepColor (completed requests), else it is freed too.
+  void releaseDevice(ServerRequest &r, bool keepColor = false) {
     if (!r.fb) return;
     const size_t px = (size_t)r.fb->width * r.fb->height;
     pool.putDevice(r.fb->accum.ptr, px * 16);
     if (r.fb->comp.ptr) pool.putDevice(r.fb->comp.ptr, px * 16);
-    pool.putDevice(r.fb->color.ptr, r.fb->color.bytes);
-    r.fb->accum.ptr = r.fb->comp.ptr = r.fb->color.ptr = nullptr;  // owned by the pool now
+    if (keepColor) {
+      r.result = r.fb->color.ptr;
+      r.resultBytes = r.fb->color.bytes;
+    } else {
+      pool.putDevice(r.fb->color.ptr, r.fb->color.bytes);
+    }
+    bytesInUse -= r.deviceBytes - (keepColor ? r.fb->color.bytes : 0);
+    r.fb->accum.ptr = r.fb->comp.ptr = r.fb->color.ptr = nullptr;  // owned by the pool / result now
     r.fb->accum.bytes = r.fb->comp.bytes = r.fb->color.bytes = 0;
     r.fb.reset();
-    bytesInUse -= r.deviceBytes;
   }
 
   // device buffers of an admitted request (from the pool)
@@ -216,24 +228,13 @@ struct Server {
         auto &r = slice[i];
         r->wavesDone += waves[i];
         if (err.empty() && r->wavesDone < r->spp) { still.push_back(r); continue; }
-        if (err.empty()) {
-          try {
-            r->stagingBytes = r->fb->color.bytes;
-            r->staging = pool.getHost(r->stagingBytes);
-            ck(cudaMemcpyAsync(r->staging, r->fb->color.ptr, r->stagingBytes, cudaMemcpyDeviceToHost, ctx->stream),
-               "result copy");
-            ck(cudaStreamSynchronize(ctx->stream), "result copy");
-          } catch (const std::exception &e) {
-            r->failed = true;
-            r->error = e.what();
-          }
-        } else {
+        if (!err.empty()) {
           r->failed = true;
           r->error = err;
         }
         r->finished = Clock::now();
         r->done = true;
-        releaseDevice(*r);
+        releaseDevice(*r, !r->failed);
         if (!r->failed) {
           latenciesMs.push_back(std::chrono::duration<double, std::milli>(r->finished - r->submitted).count());
           completedCount++;
@@ -339,9 +340,20 @@ BN_API int bnxServerWait(BNXServer server, long long id, int timeoutMs, void *ho
   auto r = s->finished[id];
   s->finished.erase(id);
   if (r->failed) throw Error(E_CUDA, "request failed: " + r->error);
-  if (hostPixels) memcpy(hostPixels, r->staging, r->stagingBytes);
-  s->pool.putHost(r->staging, r->stagingBytes);
-  r->staging = nullptr;
+  void *src = r->result;
+  const size_t n = r->resultBytes;
+  l.unlock();
+  cudaError_t e = cudaSuccess;
+  if (hostPixels && src) {
+    cudaSetDevice(s->ctx->device);
+    e = cudaMemcpyAsync(hostPixels, src, n, cudaMemcpyDefault, s->copyStream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s->copyStream);
+  }
+  l.lock();
+  s->releaseResult(*r);
+  l.unlock();
+  s->cvWork.notify_one();  // freed budget may admit queued requests
+  ck(e, "result copy");
   return 1;
   BN_CATCH(-g_lastError)
 }

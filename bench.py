@@ -52,6 +52,9 @@ def parse():
     p.add_argument("--e2e-steps", type=int, default=None)
     p.add_argument("--cpu-seconds", type=float, default=12.0)
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--rmse", action="store_true", help="image RMSE of every storage form vs the FP64 oracle")
+    p.add_argument("--rmse-size", default="96x54", help="image size of the RMSE frames")
+    p.add_argument("--rmse-spp", type=int, default=4096)
     return p.parse_args()
 
 
@@ -523,8 +526,63 @@ def run_serving(args):
     return 0
 
 
+def run_rmse(args):
+    """Image RMSE against the FP64 expectation (oracle/bn_fp64.cpp, exact
+    -log, off the hot path) for the plain FP32 path and every storage /
+    precision form, on a reduced frame of the configured workload at high
+    spp.  The FP64 reference is computed from the float32 field, so storage
+    error shows up in the forms' RMSE."""
+    import numpy as np
+    import torch
+    import barney_b200 as bn
+    import oracle
+    from barney_b200 import synth
+    torch.cuda.set_device(0)
+    w, h = (int(x) for x in args.rmse_size.split("x"))
+    if args.config == "1":
+        base = synth.config1(reference_semantics=True)
+        f32 = base["voxels"]
+        n = 64
+    else:
+        n = 512 if args.config == "2" else 1024
+        f32d = synth.value_noise(n, 0, xp=torch, device="cuda")
+        f32 = f32d.cpu().numpy()
+        base = synth.config2(vol=f32, dtype="f32")
+    base = dict(base, width=w, height=h)
+    t0 = time.time()
+    step = 1.0 / (n - 1)
+    truth = oracle.render_expected_fp64(oracle.Scene(base), step=step, subpix=2, env_dirs=64)
+    fp64_s = time.time() - t0
+    forms = [("plain f32 (fastLog)", "f32", {}), ("f32 exact -log", "f32", {"exact_log": True}),
+             ("f16 storage", "f16", {"majorant_round_up": True, "compensated_accum": True}),
+             ("bf16 storage", "bf16", {"majorant_round_up": True, "compensated_accum": True}),
+             ("u8 storage", "u8", {"majorant_round_up": True, "compensated_accum": True})]
+    out = []
+    for name, dtype, kw in forms:
+        d = dict(base, voxels=synth.to_storage(f32, dtype), dtype=dtype, **kw)
+        r = bn.VolumeRenderer(d, color_format="float4")
+        r.set_spp(args.rmse_spp)
+        r.render()
+        img = r.read().astype(np.float64)
+        st = r.stats()
+        r.close()
+        err = img[..., :3] - truth[..., :3]
+        out.append({"form": name, "rmse": float(np.sqrt((err ** 2).mean())),
+                    "mean_abs": float(np.abs(err).mean()), "render_ms": st["render_ms"],
+                    "Msamples_per_s": st["samples"] / st["render_ms"] / 1e3})
+    plain = out[0]["rmse"]
+    for o in out:
+        o["rmse_over_plain"] = o["rmse"] / plain
+    line = {"rmse_vs_fp64": out, "config": args.config, "image": [w, h], "spp": args.rmse_spp,
+            "fp64_oracle": {"step": step, "subpix": 2, "env_dirs": 64, "seconds": fp64_s, "threads": os.cpu_count()}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     args = parse()
+    if args.rmse:
+        return run_rmse(args)
     if args.impl == "reference":
         return run_reference(args)
     if args.config == "4":

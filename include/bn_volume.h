@@ -215,11 +215,11 @@ BN_API void bnxSetStream(BNContext context, void *cudaStream);
 BN_API void *bnxGetStream(BNContext context);
 /* Launch parameters of the render kernel (0 = automatic). */
 BN_API void bnxSetLaunchConfig(BNContext context, int blocksPerSM, int threadsPerBlock);
-/* Warp scheduling of the render kernel: a warp generates primary rays once
-   genBatch of its lanes need one and shades collisions once shadeBatch lanes
-   have one, or as soon as fewer than minBusy lanes are inside a Woodcock
-   range (defaults 16, 8, 8). */
-BN_API void bnxSetScheduling(BNContext context, int genBatch, int shadeBatch, int minBusy);
+/* Warp scheduling of the render kernel: a warp keeps stepping macrocells and
+   Woodcock ranges until at least serviceBatch of its lanes (or all of its
+   busy lanes) need service -- shading, accumulation, a new ray -- and then
+   serves them together (1..32, default 16). */
+BN_API void bnxSetScheduling(BNContext context, int serviceBatch);
 /* Render several jobs in one persistent launch (each job: renderer, model,
    camera, frame buffer of this context; distinct frame buffers).  Same
    result as one bnRender per job, bit for bit.  The launch sequence is
@@ -237,7 +237,7 @@ BN_API void bnxSetBatchGraphs(BNContext context, int enable);
    keeps the fastest for the context and reports it.  The tuning frames are
    rendered into the jobs' frame buffers and discarded (accumulation reset). */
 typedef struct {
-  int threadsPerBlock, blocksPerSM, genBatch, shadeBatch, minBusy;
+  int threadsPerBlock, blocksPerSM, serviceBatch;
   float renderMs;
 } BNXLaunchConfig;
 BN_API void bnxAutotuneBatch(BNContext context, const BNXRenderJob *jobs, int numJobs, BNXLaunchConfig *best);
