@@ -29,11 +29,12 @@ BN_FLOAT4 = 183
 BN_UFIXED8 = 300
 BN_UFIXED8_RGBA = 301
 BN_UFIXED8_RGBA_SRGB = 302
+BN_UFIXED16 = 303
 BNX_FLOAT16 = 1000
 BNX_BFLOAT16 = 1001
 BN_FB_COLOR = 1
 
-VOXEL_FORMATS = {"f32": BN_FLOAT32, "u8": BN_UFIXED8, "f16": BNX_FLOAT16, "bf16": BNX_BFLOAT16}
+VOXEL_FORMATS = {"f32": BN_FLOAT32, "u8": BN_UFIXED8, "u16": BN_UFIXED16, "f16": BNX_FLOAT16, "bf16": BNX_BFLOAT16}
 COLOR_FORMATS = {"float4": BN_FLOAT4, "rgba8": BN_UFIXED8_RGBA, "rgba8_srgb": BN_UFIXED8_RGBA_SRGB}
 
 # every symbol include/bn_volume.h declares
@@ -48,12 +49,38 @@ EXPORTS = [
     "bnxSetLaunchConfig", "bnxFrameBufferDevicePointer", "bnxVolumeGetMacrocells",
     "bnxRenderStructuredNoAlloc", "bnxSetScheduling", "bnxRenderBatch", "bnxSetBatchGraphs", "bnxAutotuneBatch",
     "bnxServerCreate", "bnxServerDestroy", "bnxServerSubmit", "bnxServerWait", "bnxServerGetStats",
-    "bnxServerResetStats",
+    "bnxServerResetStats", "bnxSetRenderTimeout", "bnxAnariTransferFunction1D", "bnxAnariDensityScale",
+    "bnxAnariStructuredRegular",
 ]
 
 
 class bn_float2(ctypes.Structure):
     _fields_ = [("x", ctypes.c_float), ("y", ctypes.c_float)]
+
+
+class bn_float3(ctypes.Structure):
+    _fields_ = [("x", ctypes.c_float), ("y", ctypes.c_float), ("z", ctypes.c_float)]
+
+
+class bn_float4(ctypes.Structure):
+    _fields_ = [("x", ctypes.c_float), ("y", ctypes.c_float), ("z", ctypes.c_float), ("w", ctypes.c_float)]
+
+
+def anari_transfer_function_1d(colors=None, opacities=None, uniform_color=(1.0, 1.0, 1.0, 1.0),
+                               uniform_opacity=1.0):
+    """ANARI transferFunction1D arrays -> the RGBA table for bnVolumeSetXF."""
+    L = lib()
+    c = None if colors is None else np.ascontiguousarray(colors, np.float32)
+    o = None if opacities is None else np.ascontiguousarray(opacities, np.float32).reshape(-1)
+    nc, ch = (0, 4) if c is None else (c.shape[0], c.shape[1])
+    no = 0 if o is None else o.shape[0]
+    uc = bn_float4(*uniform_color)
+    n = L.bnxAnariTransferFunction1D(_void_p(c), nc, ch, _void_p(o), no, uc, uniform_opacity, None)
+    check()
+    out = np.zeros((n, 4), np.float32)
+    L.bnxAnariTransferFunction1D(_void_p(c), nc, ch, _void_p(o), no, uc, uniform_opacity, out.ctypes.data)
+    check()
+    return out
 
 
 class BNXStats(ctypes.Structure):
@@ -134,6 +161,10 @@ def lib(build_if_missing=True):
         "bnxServerCreate": ([P, P], P), "bnxServerDestroy": ([P], None),
         "bnxServerSubmit": ([P, P], ctypes.c_longlong), "bnxServerWait": ([P, ctypes.c_longlong, I, P], I),
         "bnxServerGetStats": ([P, P], None), "bnxServerResetStats": ([P], None),
+        "bnxSetRenderTimeout": ([P, I], None),
+        "bnxAnariTransferFunction1D": ([P, I, I, P, I, bn_float4, F, P], I),
+        "bnxAnariDensityScale": ([F], F),
+        "bnxAnariStructuredRegular": ([P, I, I, P, I, I, I, bn_float3, bn_float3], P),
     }
     for name, (args, res) in sig.items():
         fn = getattr(L, name)
@@ -384,6 +415,10 @@ class VolumeRenderer:
 
     def set_scheduling(self, service_batch=16):
         self.L.bnxSetScheduling(self.ctx, service_batch)
+        check()
+
+    def set_timeout(self, milliseconds):
+        self.L.bnxSetRenderTimeout(self.ctx, int(milliseconds))
         check()
 
     def set_launch_config(self, blocks_per_sm=0, threads_per_block=0):

@@ -4,6 +4,9 @@
 // launches.  Device work goes to the kernels in bn_kernels.cu.
 #include "bn_objects.h"
 
+#include <chrono>
+#include <thread>
+
 namespace bnb {
 
 thread_local int g_lastError = 0;
@@ -172,6 +175,27 @@ static void readStats(Context *ctx, const LaunchCounters &hc, unsigned long long
   }
 }
 
+// Waits for `done` with the context's render deadline.  On expiry the abort
+// word of the launch counters is raised from a side stream; every warp of the
+// render kernel stops at its next pixel-chunk fetch, so the stream drains
+// promptly and the context stays usable.  Returns true if aborted.
+static bool waitWithDeadline(Context *ctx, cudaEvent_t done) {
+  if (ctx->timeoutMs <= 0) return false;
+  const auto deadline = std::chrono::steady_clock::now() + std::chrono::milliseconds(ctx->timeoutMs);
+  while (true) {
+    cudaError_t q = cudaEventQuery(done);
+    if (q == cudaSuccess) return false;
+    if (q != cudaErrorNotReady) ck(q, "render");
+    if (std::chrono::steady_clock::now() >= deadline) break;
+    std::this_thread::sleep_for(std::chrono::microseconds(100));
+  }
+  if (!ctx->abortStream) ck(cudaStreamCreateWithFlags(&ctx->abortStream, cudaStreamNonBlocking), "abort stream");
+  static const unsigned one = 1;
+  ck(cudaMemcpyAsync(&ctx->dCounters->abort, &one, sizeof one, cudaMemcpyHostToDevice, ctx->abortStream), "abort");
+  ck(cudaStreamSynchronize(ctx->abortStream), "abort");
+  return true;
+}
+
 static void render(Context *ctx, Renderer &r, Model &m, Camera &cam, FrameBuffer &fb) {
   JobDD job = buildJob(ctx, r, m, cam, fb);
   if (job.fr.spp <= 0) return;
@@ -187,8 +211,13 @@ static void render(Context *ctx, Renderer &r, Model &m, Camera &cam, FrameBuffer
   ck(cudaEventRecord(ctx->ev[2], ctx->stream), "event");
   LaunchCounters hc;
   ck(cudaMemcpyAsync(&hc, ctx->dCounters, sizeof hc, cudaMemcpyDeviceToHost, ctx->stream), "counter read");
+  waitWithDeadline(ctx, ctx->ev[1]);
   ck(cudaStreamSynchronize(ctx->stream), "render");
   readStats(ctx, hc, (unsigned long long)fb.width * fb.height * job.fr.spp);
+  if (hc.errorFlags & ERR_ABORTED) {
+    fb.accumID = 0;  // the frame is incomplete
+    throw Error(E_TIMEOUT, "render aborted: exceeded the " + std::to_string(ctx->timeoutMs) + " ms deadline");
+  }
 }
 
 // Every job's waves in one persistent launch of the batch kernel, then one
@@ -444,6 +473,7 @@ BN_API BNTextureData bnTextureData3DCreate(BNContext context, int, BNDataType fm
   case BN_UINT8: type = VOX_U8; es = 1; break;
   case BNX_FLOAT16: type = VOX_F16; es = 2; break;
   case BNX_BFLOAT16: type = VOX_BF16; es = 2; break;
+  case BN_UFIXED16: type = VOX_U16; es = 2; break;
   default: throw Error(E_UNSUPPORTED, "unsupported 3D texel format");
   }
   if (w <= 0 || h <= 0 || d <= 0) throw Error(E_INVALID_ARG, "texture dimensions must be positive");
@@ -694,6 +724,7 @@ BN_API int bnxRenderStructuredNoAlloc(const BNXNoAllocFrame *f, void *stream) {
   case BN_UINT8: type = VOX_U8; break;
   case BNX_FLOAT16: type = VOX_F16; break;
   case BNX_BFLOAT16: type = VOX_BF16; break;
+  case BN_UFIXED16: type = VOX_U16; break;
   default: throw Error(E_UNSUPPORTED, "unsupported voxel type");
   }
   int fmt = f->colorFormat == BN_FLOAT4 ? FMT_FLOAT4 : f->colorFormat == BN_UFIXED8_RGBA ? FMT_RGBA8
@@ -804,6 +835,13 @@ BN_API void bnxRenderBatch(BNContext context, const BNXRenderJob *jobs, int numJ
   BN_CATCH()
 }
 
+BN_API void bnxSetRenderTimeout(BNContext context, int milliseconds) {
+  BN_TRY
+  if (milliseconds < 0) throw Error(E_INVALID_ARG, "timeout must be >= 0");
+  getContext(context)->timeoutMs = milliseconds;
+  BN_CATCH()
+}
+
 BN_API void bnxSetBatchGraphs(BNContext context, int enable) {
   BN_TRY
   getContext(context)->useGraphs = enable != 0;
@@ -839,6 +877,84 @@ BN_API void bnxAutotuneBatch(BNContext context, const BNXRenderJob *jobs, int nu
   for (auto &x : e) x.fb->accumID = 0;  // tuning frames are discarded
   if (best) *best = {bestC.tpb, bestC.bps, bestC.service, bestMs};
   BN_CATCH()
+}
+
+// ---------------------------------------------------------------------------
+// ANARI parameter mapping (barney/anari/SpatialField.cpp:70-157,
+// barney/anari/Volume.cpp:82-234): what the ANARI device does before it
+// calls the native API, restated so an ANARI front-end can be layered on
+// these entry points.
+// ---------------------------------------------------------------------------
+BN_API int bnxAnariTransferFunction1D(const float *colors, int numColorsIn, int colorChannels,
+                                      const float *opacities, int numOpacitiesIn, bn_float4 uniformColor,
+                                      float uniformOpacity, bn_float4 *out) {
+  BN_TRY
+  if (colors && colorChannels != 3 && colorChannels != 4) throw Error(E_INVALID_ARG, "colorChannels must be 3 or 4");
+  if ((colors && numColorsIn < 1) || (opacities && numOpacitiesIn < 1)) throw Error(E_INVALID_ARG, "empty array");
+  const int numColors = colors ? numColorsIn : 1;
+  const int numOpacities = opacities ? numOpacitiesIn : 1;
+  const int tfSize = std::max(numColors, numOpacities);
+  if (!out) return tfSize;
+  // Volume.cpp:166-167: m_uniformOpacity = opacity * color.w
+  const float uOpacity = uniformOpacity * uniformColor.w;
+  for (int i = 0; i < tfSize; ++i) {
+    const float colorPos = tfSize > 1 ? (float(i) / (tfSize - 1)) * (numColors - 1) : 0.f;
+    const float colorFrac = colorPos - floorf(colorPos);
+    float c0[4] = {uniformColor.x, uniformColor.y, uniformColor.z, uOpacity};
+    float c1[4] = {uniformColor.x, uniformColor.y, uniformColor.z, uOpacity};
+    if (colors) {
+      const int i0 = int(floorf(colorPos)), i1 = int(ceilf(colorPos));
+      for (int c = 0; c < 3; c++) {
+        c0[c] = colors[colorChannels * i0 + c];
+        c1[c] = colors[colorChannels * i1 + c];
+      }
+      if (colorChannels == 4) {
+        c0[3] = colors[4 * i0 + 3];
+        c1[3] = colors[4 * i1 + 3];
+      }
+    }
+    float color[4];
+    for (int c = 0; c < 4; c++) color[c] = (1.f - colorFrac) * c0[c] + colorFrac * c1[c];
+    if (opacities) {
+      const float alphaPos = tfSize > 1 ? (float(i) / (tfSize - 1)) * (numOpacities - 1) : 0.f;
+      const float alphaFrac = alphaPos - floorf(alphaPos);
+      const float a0 = opacities[int(floorf(alphaPos))];
+      const float a1 = opacities[int(ceilf(alphaPos))];
+      color[3] *= (1.f - alphaFrac) * a0 + alphaFrac * a1;
+    }
+    out[i] = {color[0], color[1], color[2], color[3]};
+  }
+  return tfSize;
+  BN_CATCH(-1)
+}
+
+BN_API float bnxAnariDensityScale(float unitDistance) {
+  return unitDistance <= 0.f ? 1.f : 1.f / unitDistance;  // Volume.cpp:99-107
+}
+
+BN_API BNScalarField bnxAnariStructuredRegular(BNContext context, int slot, BNDataType elementType, const void *data,
+                                               int nx, int ny, int nz, bn_float3 origin, bn_float3 spacing) {
+  BN_TRY
+  BNDataType bt;
+  switch ((int)elementType) {  // SpatialField.cpp:106-116: float32, or ufixed8 / uint8
+  case BN_FLOAT32: bt = BN_FLOAT32; break;
+  case BN_UFIXED8:
+  case BN_UINT8: bt = BN_UFIXED8; break;
+  default: throw Error(E_UNSUPPORTED, "structuredRegular supports float32 and uint8 / ufixed8 data");
+  }
+  BNScalarField sf = bnScalarFieldCreate(context, slot, "structured");
+  if (!sf) return nullptr;
+  BNTextureData td = bnTextureData3DCreate(context, slot, bt, nx, ny, nz, data);
+  if (!td) { bnRelease(sf); return nullptr; }
+  bnSetObject(sf, "textureData", td);
+  bnRelease(td);  // the field keeps its own reference (SpatialField.cpp:122)
+  bnSet3i(sf, "dims", nx, ny, nz);
+  bnSet3f(sf, "gridOrigin", origin.x, origin.y, origin.z);
+  bnSet3f(sf, "gridSpacing", spacing.x, spacing.y, spacing.z);
+  bnCommit(sf);
+  if (g_lastError) return nullptr;
+  return sf;
+  BN_CATCH(nullptr)
 }
 
 }  // extern "C"

@@ -7,7 +7,7 @@
 
 namespace bnb {
 
-enum VoxelType : int { VOX_F32 = 0, VOX_U8 = 1, VOX_F16 = 2, VOX_BF16 = 3 };
+enum VoxelType : int { VOX_F32 = 0, VOX_U8 = 1, VOX_F16 = 2, VOX_BF16 = 3, VOX_U16 = 4 };
 enum PhaseMode : int { PHASE_SIMPLE = 0, PHASE_HG = 1 };
 enum ColorFormat : int { FMT_FLOAT4 = 0, FMT_RGBA8 = 1, FMT_RGBA8_SRGB = 2 };
 enum ErrorBits : unsigned { ERR_ITER_CAP = 1u, ERR_ABORTED = 2u };
@@ -78,7 +78,7 @@ struct JobDD {
 // busy lanes) need service -- shading, accumulation, a new ray -- and then
 // serves them together.
 struct SchedDD {
-  int serviceBatch = 16;
+  int serviceBatch = 24;
 };
 
 // Device counters of one launch (samples, mcVisits, rays, errorFlags)

@@ -102,6 +102,15 @@ DEV float loadVoxel(const void *p, int64_t i, const float *u8lut) {
   if (T == VOX_F32) return __ldg((const float *)p + i);
   if (T == VOX_U8) return u8lut[__ldg((const uint8_t *)p + i)];
   if (T == VOX_F16) return __half2float(__ushort_as_half(__ldg((const unsigned short *)p + i)));
+  if (T == VOX_U16) {
+    // x / 65535 (unorm16) without a division: q + (x - 65535 q) / 65535,
+    // evaluated unfused, equals the correctly rounded quotient for every
+    // 16-bit x (checked exhaustively in tests/test_oracle_kat.py)
+    const float x = (float)__ldg((const unsigned short *)p + i);
+    const float r = 1.f / 65535.f;
+    const float q = x * r;
+    return q + (x - q * 65535.f) * r;
+  }
   return __uint_as_float((uint32_t)__ldg((const unsigned short *)p + i) << 16);
 }
 
@@ -428,6 +437,7 @@ DEV float sampleJob(const VolumeDD &v, float3 P, const float *u8lut) {
   case VOX_F32: return sampleField<VOX_F32>(v, P, u8lut);
   case VOX_U8: return sampleField<VOX_U8>(v, P, u8lut);
   case VOX_F16: return sampleField<VOX_F16>(v, P, u8lut);
+  case VOX_U16: return sampleField<VOX_U16>(v, P, u8lut);
   default: return sampleField<VOX_BF16>(v, P, u8lut);
   }
 }
@@ -926,6 +936,7 @@ cudaError_t launchBuildMacrocells(const VolumeDD &v, float2 *ranges, float *majo
   case VOX_F32: mcBuildKernel<VOX_F32><<<blocks, 128, 0, s>>>(v, ranges, majorants, roundUp); break;
   case VOX_U8: mcBuildKernel<VOX_U8><<<blocks, 128, 0, s>>>(v, ranges, majorants, roundUp); break;
   case VOX_F16: mcBuildKernel<VOX_F16><<<blocks, 128, 0, s>>>(v, ranges, majorants, roundUp); break;
+  case VOX_U16: mcBuildKernel<VOX_U16><<<blocks, 128, 0, s>>>(v, ranges, majorants, roundUp); break;
   default: mcBuildKernel<VOX_BF16><<<blocks, 128, 0, s>>>(v, ranges, majorants, roundUp); break;
   }
   return cudaGetLastError();
@@ -965,6 +976,7 @@ cudaError_t launchRender(const VolumeDD &v, const FrameDD &fr, LaunchCounters *c
   case VOX_F32: return launchRenderT<VOX_F32>(v, fr, sd, ctr, bps, tpb, s);
   case VOX_U8: return launchRenderT<VOX_U8>(v, fr, sd, ctr, bps, tpb, s);
   case VOX_F16: return launchRenderT<VOX_F16>(v, fr, sd, ctr, bps, tpb, s);
+  case VOX_U16: return launchRenderT<VOX_U16>(v, fr, sd, ctr, bps, tpb, s);
   default: return launchRenderT<VOX_BF16>(v, fr, sd, ctr, bps, tpb, s);
   }
 }
@@ -1088,6 +1100,7 @@ cudaError_t launchRenderNoAlloc(VolumeDD v, FrameDD fr, int fmt, void *color, in
   case VOX_F32: mcMajorantScratchKernel<VOX_F32><<<blocks, 128, 0, s>>>(v, roundUp); break;
   case VOX_U8: mcMajorantScratchKernel<VOX_U8><<<blocks, 128, 0, s>>>(v, roundUp); break;
   case VOX_F16: mcMajorantScratchKernel<VOX_F16><<<blocks, 128, 0, s>>>(v, roundUp); break;
+  case VOX_U16: mcMajorantScratchKernel<VOX_U16><<<blocks, 128, 0, s>>>(v, roundUp); break;
   default: mcMajorantScratchKernel<VOX_BF16><<<blocks, 128, 0, s>>>(v, roundUp); break;
   }
   e = cudaGetLastError();

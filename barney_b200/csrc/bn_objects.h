@@ -37,7 +37,7 @@ struct Error : std::runtime_error {
   Error(int c, const std::string &m) : std::runtime_error(m), code(c) {}
 };
 enum : int { E_OK = 0, E_INVALID_HANDLE = 1, E_INVALID_ARG = 2, E_UNSUPPORTED = 3, E_CUDA = 4, E_STATE = 5,
-             E_OOM = 6, E_INTERNAL = 7 };
+             E_OOM = 6, E_INTERNAL = 7, E_TIMEOUT = 8 };
 extern thread_local int g_lastError;
 extern thread_local std::string g_lastErrorString;
 
@@ -322,6 +322,8 @@ struct Context {
   LaunchCounters *hostCounters = nullptr;
   int hostCapacity = 0;
   bool useGraphs = true;
+  int timeoutMs = 0;                 // render deadline (0: none)
+  cudaStream_t abortStream = nullptr;
   cudaGraphExec_t graphExec = nullptr;
   std::vector<const void *> graphKey;
   std::mutex mutex;
@@ -339,6 +341,7 @@ struct Context {
     cudaSetDevice(device);
     cudaStreamSynchronize(stream);
     if (graphExec) cudaGraphExecDestroy(graphExec);
+    if (abortStream) cudaStreamDestroy(abortStream);
     if (hostJobs) cudaFreeHost(hostJobs);
     if (hostChunks) cudaFreeHost(hostChunks);
     if (hostCounters) cudaFreeHost(hostCounters);

@@ -130,12 +130,15 @@ def blobs(n, seed=0, xp=np, device=None):
 
 def to_storage(vol_f32, dtype):
     """Stored form of a [0,1] float32 field: f32 as is, u8 = round(255 v),
-    f16 / bf16 by round-to-nearest-even (returned as uint16 bit patterns)."""
+    u16 = round(65535 v), f16 / bf16 by round-to-nearest-even (returned as
+    16-bit patterns)."""
     if dtype == "f32":
         return vol_f32
     if isinstance(vol_f32, np.ndarray):
         if dtype == "u8":
             return np.clip(np.rint(vol_f32.astype(np.float64) * 255.0), 0, 255).astype(np.uint8)
+        if dtype == "u16":
+            return np.clip(np.rint(vol_f32.astype(np.float64) * 65535.0), 0, 65535).astype(np.uint16)
         if dtype == "f16":
             return vol_f32.astype(np.float16).view(np.uint16)
         if dtype == "bf16":
@@ -145,6 +148,8 @@ def to_storage(vol_f32, dtype):
     import torch
     if dtype == "u8":
         return torch.clamp(torch.round(vol_f32.double() * 255.0), 0, 255).to(torch.uint8)
+    if dtype == "u16":
+        return torch.clamp(torch.round(vol_f32.double() * 65535.0), 0, 65535).to(torch.int32).to(torch.int16)
     if dtype == "f16":
         return vol_f32.half().view(torch.int16)
     if dtype == "bf16":

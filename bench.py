@@ -479,8 +479,9 @@ def run_serving(args):
         th = threading.Thread(target=producer)
         th.start()
         th.join()
+        host = np.zeros((1024 * 1024,), np.uint32)
         for rid in ids:
-            server.wait(rid, None)
+            server.wait(rid, host)
         st = server.stats()
         results.append({"rate_req_s": rate, "requests": n, "frames_per_s": st["completed"] / st["wallSeconds"],
                         "p50_ms": st["p50Ms"], "p99_ms": st["p99Ms"], "mean_ms": st["meanMs"],
@@ -493,21 +494,33 @@ def run_serving(args):
         r.close()
     ctx.close()
     torch.cuda.empty_cache()
-    # plain FP32 path: the same kind of stream, one bnRender per request
+    # plain FP32 path: the same kind of stream, one bnRender per request into a
+    # frame buffer of the request's size (allocated once per size and volume,
+    # as a plain-API client would), read back to host memory
+    import ctypes
     ctx2 = bn.Context()
     plain = [bn.VolumeRenderer(d, context=ctx2, color_format="rgba8") for d in serving_volumes(torch, "cuda", "f32")]
+    L = bn.lib()
+    fbs = {}
+    for i, r in enumerate(plain):
+        for side in (256, 512, 1024):
+            fb = L.bnFrameBufferCreate(ctx2.ctx, 0)
+            L.bnFrameBufferResize(fb, bn.BN_UFIXED8_RGBA, side, side, bn.BN_FB_COLOR)
+            fbs[i, side] = fb
+    bn.check()
     reqs = request_stream(args.requests or 300, seed=99)
     host = np.zeros((1024 * 1024,), np.uint32)
+    torch.cuda.synchronize()
     t0 = time.perf_counter()
     for v, side, spp, cam in reqs:
         r = plain[v]
         r.set_camera(cam)
-        if r.width != side:
-            r.resize(side, side)
         r.set_spp(spp)
-        r.accum_reset()
-        r.render()
-        r.read(host[:side * side].reshape(side, side))
+        fb = fbs[v, side]
+        L.bnAccumReset(fb)
+        L.bnRender(r.renderer, r.model, r.camera, fb)
+        L.bnFrameBufferRead(fb, bn.BN_FB_COLOR, host.ctypes.data, bn.BN_UFIXED8_RGBA)
+    bn.check()
     plain_fps = len(reqs) / (time.perf_counter() - t0)
     for r in plain:
         r.close()

@@ -135,8 +135,9 @@ BN_API void bnSetData(BNObject target, const char *paramName, BNData value);
 BN_API BNData bnDataCreate(BNContext context, int whichSlot, BNDataType dataType, size_t numItems,
                            const void *items);
 /* replaces barney.cu:223 bnTextureData3DCreate. texelFormat: BN_FLOAT32,
-   BN_UFIXED8 / BN_UINT8 (unorm, x/255), BNX_FLOAT16, BNX_BFLOAT16. texels may
-   be host or device memory; it is copied before return. */
+   BN_UFIXED8 / BN_UINT8 (unorm, x/255), BN_UFIXED16 (unorm, x/65535),
+   BNX_FLOAT16, BNX_BFLOAT16. texels may be host or device memory; it is
+   copied before return. */
 BN_API BNTextureData bnTextureData3DCreate(BNContext context, int whichSlot, BNDataType texelFormat,
                                            int width, int height, int depth, const void *texels);
 /* replaces barney.cu:382 bnScalarFieldCreate; type must be "structured" */
@@ -213,12 +214,17 @@ BN_API void bnxGetStats(BNContext context, BNXStats *stats);
    selects the context's own stream. */
 BN_API void bnxSetStream(BNContext context, void *cudaStream);
 BN_API void *bnxGetStream(BNContext context);
+/* Deadline of bnRender (0: none).  When a frame exceeds it, the render
+   kernel is told to stop (every warp quits at its next pixel chunk), the
+   frame buffer's accumulation is reset and bnRender records error 8
+   (timeout); the context stays usable. */
+BN_API void bnxSetRenderTimeout(BNContext context, int milliseconds);
 /* Launch parameters of the render kernel (0 = automatic). */
 BN_API void bnxSetLaunchConfig(BNContext context, int blocksPerSM, int threadsPerBlock);
 /* Warp scheduling of the render kernel: a warp keeps stepping macrocells and
    Woodcock ranges until at least serviceBatch of its lanes (or all of its
    busy lanes) need service -- shading, accumulation, a new ray -- and then
-   serves them together (1..32, default 16). */
+   serves them together (1..32, default 24). */
 BN_API void bnxSetScheduling(BNContext context, int serviceBatch);
 /* Render several jobs in one persistent launch (each job: renderer, model,
    camera, frame buffer of this context; distinct frame buffers).  Same
@@ -268,7 +274,7 @@ BN_API void bnxVolumeGetMacrocells(BNVolume volume, int *dims3, float *rangesHos
 #define BNX_NOALLOC_MAX_MACROCELLS (64 * 64 * 64)
 typedef struct {
   const void *voxels;              /* device: x-fastest scalars, dims[0]*dims[1]*dims[2] */
-  BNDataType voxelType;            /* BN_FLOAT32, BN_UFIXED8, BNX_FLOAT16, BNX_BFLOAT16 */
+  BNDataType voxelType;            /* BN_FLOAT32, BN_UFIXED8, BN_UFIXED16, BNX_FLOAT16, BNX_BFLOAT16 */
   int dims[3];
   bn_float3 gridOrigin, gridSpacing;
   const bn_float4 *transferFunction; /* device: numTFValues RGBA entries */
@@ -332,6 +338,28 @@ BN_API long long bnxServerSubmit(BNXServer server, const BNXRequest *request);
 BN_API int bnxServerWait(BNXServer server, long long id, int timeoutMs, void *hostPixels);
 BN_API void bnxServerGetStats(BNXServer server, BNXServerStats *stats);
 BN_API void bnxServerResetStats(BNXServer server);
+
+/* ---------------------------------------------------------------------- */
+/* ANARI parameter mapping (no native-API counterpart: the ANARI device      */
+/* does this before calling bn*; restated from barney/anari)                */
+/* ---------------------------------------------------------------------- */
+/* "transferFunction1D" colour / opacity arrays -> the RGBA table passed to
+   bnVolumeSetXF (Volume.cpp:178-234).  colors: numColors x colorChannels (3
+   or 4) floats or NULL (uniformColor); opacities: numOpacities floats or NULL
+   (uniformOpacity, multiplied by uniformColor.w as Volume.cpp:166-167 does).
+   Returns the table size max(numColors, numOpacities) and, if out is not
+   NULL, writes the table. */
+BN_API int bnxAnariTransferFunction1D(const float *colors, int numColors, int colorChannels,
+                                      const float *opacities, int numOpacities, bn_float4 uniformColor,
+                                      float uniformOpacity, bn_float4 *out);
+/* volume "unitDistance" -> densityAt1 of bnVolumeSetXF (Volume.cpp:99-107) */
+BN_API float bnxAnariDensityScale(float unitDistance);
+/* "structuredRegular" spatial field (SpatialField.cpp:74-140): texture data
+   of float32 or uint8 / ufixed8 scalars + a "structured" field with dims,
+   gridOrigin, gridSpacing, committed */
+BN_API BNScalarField bnxAnariStructuredRegular(BNContext context, int slot, BNDataType elementType,
+                                               const void *data, int nx, int ny, int nz, bn_float3 origin,
+                                               bn_float3 spacing);
 
 #ifdef __cplusplus
 }

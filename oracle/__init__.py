@@ -20,7 +20,7 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 _LIB_PATH = os.path.join(_HERE, "liboracle.so")
 _lib = None
 
-DTYPE_CODES = {"f32": 0, "u8": 1, "f16": 2, "bf16": 3}
+DTYPE_CODES = {"f32": 0, "u8": 1, "f16": 2, "bf16": 3, "u16": 4}
 
 
 class OrcScene(ctypes.Structure):

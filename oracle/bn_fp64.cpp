@@ -69,7 +69,8 @@ struct Field {
     case 0: return ((const float *)s.voxels)[i];
     case 1: return ((const uint8_t *)s.voxels)[i] / 255.0;
     case 2: return h2f(((const uint16_t *)s.voxels)[i]);
-    default: { uint32_t u = (uint32_t)((const uint16_t *)s.voxels)[i] << 16; float f; memcpy(&f, &u, 4); return f; }
+    case 3: { uint32_t u = (uint32_t)((const uint16_t *)s.voxels)[i] << 16; float f; memcpy(&f, &u, 4); return f; }
+    default: return ((const uint16_t *)s.voxels)[i] / 65535.0;
     }
   }
   static void coord(double u, int N, int &i0, int &i1, double &f) {

@@ -207,14 +207,17 @@ struct Scene {
   explicit Scene(const OrcScene &s) : s(s) {}
 };
 
-// rtcore/cpu/Texture.cpp:193-225 (float, uchar); f16 / bf16 are the
+// rtcore/cpu/Texture.cpp:193-225 (float, uchar); unorm16 follows the
+// GPU backend's normalised read of BN_UFIXED16 (cudaCommon/TextureData.cu:46-51,
+// x/65535; the CPU backend has no sampler for it); f16 / bf16 are the
 // precision-form extensions (no reference counterpart).
 static inline float texel(const OrcScene &s, int64_t idx) {
   switch (s.dtype) {
   case 0: return ((const float *)s.voxels)[idx];
   case 1: { float v = (float)((const uint8_t *)s.voxels)[idx]; return v * 1.f / 255.f; }
   case 2: return h2f(((const uint16_t *)s.voxels)[idx]);
-  default: return bf2f(((const uint16_t *)s.voxels)[idx]);
+  case 3: return bf2f(((const uint16_t *)s.voxels)[idx]);
+  default: { float v = (float)((const uint16_t *)s.voxels)[idx]; return v * 1.f / 65535.f; }  // unorm16
   }
 }
 

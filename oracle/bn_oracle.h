@@ -7,7 +7,7 @@
 extern "C" {
 typedef struct {
   const void *voxels;
-  int dtype;              // 0 f32, 1 u8 unorm (/255), 2 f16, 3 bf16
+  int dtype;              // 0 f32, 1 u8 unorm (/255), 2 f16, 3 bf16, 4 u16 unorm (/65535)
   int dims[3];
   float origin[3];
   float spacing[3];

@@ -248,3 +248,22 @@ def test_compensated_accumulation_tracks_double_sum():
     err_comp = np.abs(acc_c.astype(np.float64) + cbuf - exact).sum()
     assert err_comp <= err_plain
     assert err_comp < 1e-3 * max(err_plain, 1e-30) or err_comp < 1e-5
+
+
+def test_unorm16_reciprocal_form_is_exact():
+    """The kernels normalise unorm16 voxels as q + (x - 65535 q) / 65535 with
+    q = x * (1/65535), unfused; that equals x / 65535 for every 16-bit x."""
+    x = np.arange(65536, dtype=np.float32)
+    r = f32(1) / f32(65535)
+    q = x * r
+    assert np.array_equal(q + (x - q * f32(65535)) * r, x / f32(65535))
+
+
+def test_u16_texels_divide_by_65535():
+    vol = (np.arange(8, dtype=np.uint16).reshape(2, 2, 2) * 9000).astype(np.uint16)
+    sc = _tiny_scene(vol, dtype="u16")
+    scal, _ = oracle.sample_points(sc, np.array([[0, 0, 0]], np.float32))
+    assert scal[0] == f32(0)
+    sc2 = _tiny_scene(np.full((2, 2, 2), 40000, np.uint16), dtype="u16")
+    s2, _ = oracle.sample_points(sc2, np.array([[0.0, 0.0, 0.0]], np.float32))
+    assert s2[0] == f32(40000) / f32(65535)
