@@ -179,6 +179,12 @@ static void readStats(Context *ctx, const LaunchCounters &hc, unsigned long long
 // word of the launch counters is raised from a side stream; every warp of the
 // render kernel stops at its next pixel-chunk fetch, so the stream drains
 // promptly and the context stays usable.  Returns true if aborted.
+static LaunchCounters *pinnedCounters(Context *ctx) {
+  if (!ctx->hostCounters)
+    ck(cudaHostAlloc((void **)&ctx->hostCounters, sizeof(LaunchCounters), cudaHostAllocDefault), "pinned counters");
+  return ctx->hostCounters;
+}
+
 static bool waitWithDeadline(Context *ctx, cudaEvent_t done) {
   if (ctx->timeoutMs <= 0) return false;
   const auto deadline = std::chrono::steady_clock::now() + std::chrono::milliseconds(ctx->timeoutMs);
@@ -209,10 +215,13 @@ static void render(Context *ctx, Renderer &r, Model &m, Camera &cam, FrameBuffer
                    ctx->stream, job.fr.comp),
      "resolve kernel");
   ck(cudaEventRecord(ctx->ev[2], ctx->stream), "event");
-  LaunchCounters hc;
-  ck(cudaMemcpyAsync(&hc, ctx->dCounters, sizeof hc, cudaMemcpyDeviceToHost, ctx->stream), "counter read");
+  // Pinned destination: a copy into pageable memory would block this thread
+  // until the render finished, before the deadline could be checked.
+  ck(cudaMemcpyAsync(pinnedCounters(ctx), ctx->dCounters, sizeof(LaunchCounters), cudaMemcpyDeviceToHost, ctx->stream),
+     "counter read");
   waitWithDeadline(ctx, ctx->ev[1]);
   ck(cudaStreamSynchronize(ctx->stream), "render");
+  const LaunchCounters hc = *ctx->hostCounters;
   readStats(ctx, hc, (unsigned long long)fb.width * fb.height * job.fr.spp);
   if (hc.errorFlags & ERR_ABORTED) {
     fb.accumID = 0;  // the frame is incomplete
@@ -238,8 +247,7 @@ void renderBatch(Context *ctx, const std::vector<BatchEntry> &entries) {
     const int cap = std::max(n, 2 * ctx->hostCapacity);
     ck(cudaHostAlloc((void **)&ctx->hostJobs, cap * sizeof(JobDD), cudaHostAllocDefault), "pinned job table");
     ck(cudaHostAlloc((void **)&ctx->hostChunks, (cap + 1) * sizeof(int), cudaHostAllocDefault), "pinned chunks");
-    if (!ctx->hostCounters)
-      ck(cudaHostAlloc((void **)&ctx->hostCounters, sizeof(LaunchCounters), cudaHostAllocDefault), "pinned counters");
+    pinnedCounters(ctx);
     ctx->batchJobs.resize(cap * sizeof(JobDD));
     ctx->batchChunks.resize((cap + 1) * sizeof(int));
     ctx->hostCapacity = cap;
@@ -305,9 +313,13 @@ void renderBatch(Context *ctx, const std::vector<BatchEntry> &entries) {
   } else {
     enqueue(ctx->stream, true);
   }
+  waitWithDeadline(ctx, ctx->ev[2]);
   ck(cudaStreamSynchronize(ctx->stream), "batch render");
-  for (int i = 0; i < n; i++) entries[i].fb->accumID += ctx->hostJobs[i].fr.spp;
+  const bool aborted = ctx->hostCounters->errorFlags & ERR_ABORTED;
+  for (int i = 0; i < n; i++) entries[i].fb->accumID = aborted ? 0 : entries[i].fb->accumID + ctx->hostJobs[i].fr.spp;
   readStats(ctx, *ctx->hostCounters, pixelSamples, ctx->useGraphs);
+  if (aborted)
+    throw Error(E_TIMEOUT, "batch render aborted: exceeded the " + std::to_string(ctx->timeoutMs) + " ms deadline");
 }
 
 }  // namespace bnb

@@ -209,6 +209,22 @@ def run_reference(args):
     return 0
 
 
+def reduce_over_ranks(ms, samples, rays, device=None):
+    """Whole-job figures of a replicated run: the slowest rank's device time
+    (MAX) and the work of all ranks (SUM).  Every rank calls this, in the same
+    order, with its own figures; single-process runs return them unchanged."""
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([ms, float(samples), float(rays)], dtype=torch.float64, device=device)
+    if dist.is_available() and dist.is_initialized() and dist.get_world_size() > 1:
+        tmax = t[:1].clone()
+        dist.all_reduce(tmax, op=dist.ReduceOp.MAX)
+        tsum = t[1:].clone()
+        dist.all_reduce(tsum, op=dist.ReduceOp.SUM)
+        t = torch.cat([tmax, tsum])
+    return float(t[0]), float(t[1]), float(t[2])
+
+
 def run_ours(args):
     import torch
     import torch.distributed as dist
@@ -255,13 +271,7 @@ def run_ours(args):
     ms = e0.elapsed_time(e1)
     samples = sum(s["samples"] for s in stats)
     rays = sum(s["rays"] for s in stats)
-    t = torch.tensor([ms, float(samples), float(rays)], dtype=torch.float64, device="cuda")
-    if world > 1:
-        tmax = t.clone()
-        dist.all_reduce(tmax[:1], op=dist.ReduceOp.MAX)
-        dist.all_reduce(t[1:], op=dist.ReduceOp.SUM)
-        t[0] = tmax[0]
-    ms_max, samples_all, rays_all = float(t[0]), float(t[1]), float(t[2])
+    ms_max, samples_all, rays_all = reduce_over_ranks(ms, samples, rays, device="cuda")
     secs = ms_max / 1e3
 
     # roofline of the render kernel: algorithmic bytes per launch / its mean duration
@@ -292,13 +302,8 @@ def run_ours(args):
     e1.record(stream)
     torch.cuda.synchronize()
     e2e_ms = e0.elapsed_time(e1)
-    t2 = torch.tensor([e2e_ms, float(e2e_samples)], dtype=torch.float64, device="cuda")
-    if world > 1:
-        m = t2.clone()
-        dist.all_reduce(m[:1], op=dist.ReduceOp.MAX)
-        dist.all_reduce(t2[1:], op=dist.ReduceOp.SUM)
-        t2[0] = m[0]
-    e2e_value = float(t2[1]) / (float(t2[0]) / 1e3) / 1e6
+    e2e_ms_max, e2e_samples_all, _ = reduce_over_ranks(e2e_ms, e2e_samples, 0, device="cuda")
+    e2e_value = e2e_samples_all / (e2e_ms_max / 1e3) / 1e6
     h2d = 3 * 3 * 4 + 4 + 8  # position, direction, up, fovy, accumID/spp words
     d2h = d["width"] * d["height"] * 4
 
@@ -328,7 +333,7 @@ def run_ours(args):
                          "algorithmic_bytes_per_launch": statistics.mean(alg),
                          "kernel_ms": statistics.mean(kms)},
             "e2e": {"value": e2e_value, "unit": "Msamples/s", "h2d_bytes_per_step": h2d,
-                    "d2h_bytes_per_step": d2h, "frames_per_s": world * e2e_steps / (float(t2[0]) / 1e3)},
+                    "d2h_bytes_per_step": d2h, "frames_per_s": world * e2e_steps / (e2e_ms_max / 1e3)},
             "cpu_baseline": cpu,
         }
         print(json.dumps(line), flush=True)

@@ -30,3 +30,28 @@ def test_render_deadline_aborts_and_context_recovers():
     img, st = gpu_render(d, 2)
     ref, _, _ = oracle_render(d, 2)
     assert_bitexact(img, ref, "after an aborted frame")
+
+
+def test_batch_deadline_aborts_and_context_recovers():
+    import barney_b200 as bn
+    from barney_b200 import synth
+    ctx = bn.Context()
+    big = [bn.VolumeRenderer(synth.config2(n=96, width=1920, height=1080, spp=128), context=ctx,
+                             color_format="rgba8") for _ in range(2)]
+    small = bn.VolumeRenderer(small_noise_scene(w=24, h=16), context=ctx, color_format="float4")
+    try:
+        big[0].set_timeout(1)  # the deadline belongs to the shared context
+        with pytest.raises(bn.BarneyError) as e:
+            ctx.render_batch(big)
+        assert "error 8" in str(e.value)
+        assert ctx.stats()["error_flags"] & 2
+        big[0].set_timeout(0)
+        small.set_spp(2)
+        ctx.render_batch([small])
+        assert ctx.stats()["error_flags"] == 0
+        ref, _, _ = oracle_render(small_noise_scene(w=24, h=16), 2)
+        assert_bitexact(small.read(), ref, "batch after an aborted batch")
+    finally:
+        for r in big + [small]:
+            r.close()
+        ctx.close()
