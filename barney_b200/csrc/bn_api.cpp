@@ -48,6 +48,7 @@ VolumeDD Volume::dd() const {
   v.boundsLo = F3(sf->boundsLo);
   v.boundsHi = F3(sf->boundsHi);
   v.majorants = (const float *)majorants.ptr;
+  v.mcOccupied = (const unsigned *)occupied.ptr;
   v.mcDims = make_int3(mcDims[0], mcDims[1], mcDims[2]);
   v.mcOrigin = F3(sf->boundsLo);                          // StructuredData.cu:76
   const v3 mcs = {8.f * sf->gridSpacing.x, 8.f * sf->gridSpacing.y, 8.f * sf->gridSpacing.z};  // :77
@@ -82,8 +83,10 @@ void Volume::build() {
     memcpy(mcDims, d, sizeof d);
     ranges.resize(n * sizeof(float2));
     majorants.resize(n * sizeof(float));
+    occupied.resize((n + 31) / 32 * sizeof(unsigned));
     uploadTF();
-    ck(launchBuildMacrocells(dd(), (float2 *)ranges.ptr, (float *)majorants.ptr, majorantRoundUp, ctx->stream),
+    ck(launchBuildMacrocells(dd(), (float2 *)ranges.ptr, (float *)majorants.ptr, (unsigned *)occupied.ptr,
+                             majorantRoundUp, ctx->stream),
        "macrocell build");
     built = true;
     needsMajorantRebuild = false;
@@ -94,7 +97,8 @@ void Volume::build() {
 
 void Volume::remapMajorants() {
   uploadTF();
-  ck(launchMapMajorants(dd(), (const float2 *)ranges.ptr, (float *)majorants.ptr, majorantRoundUp, ctx->stream),
+  ck(launchMapMajorants(dd(), (const float2 *)ranges.ptr, (float *)majorants.ptr, (unsigned *)occupied.ptr,
+                        majorantRoundUp, ctx->stream),
      "majorant map");
   needsMajorantRebuild = false;
 }

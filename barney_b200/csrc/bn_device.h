@@ -15,7 +15,8 @@ enum ErrorBits : unsigned { ERR_ITER_CAP = 1u, ERR_ABORTED = 2u };
 constexpr int kMaxDirLights = 16;
 constexpr int kMaxTF = 4096;
 constexpr int kCellsPerMC = 8;  // StructuredData.cu:26
-constexpr int kRenderMaxThreads = 128;  // __launch_bounds__ of the render kernel
+constexpr int kRenderMaxThreads = 128;  // __launch_bounds__ of the render kernel:
+constexpr int kRenderMinBlocks = 5;     // 5 x 128 threads per SM (at most 102 registers)
 
 // Structured field + macrocell majorant grid + transfer function
 // (MCVolumeAccel::DD, MCAccelerator.h:23-27).
@@ -28,6 +29,7 @@ struct VolumeDD {
   float3 rcpSpacing;    // 1/gridSpacing (IEEE)
   float3 boundsLo, boundsHi;
   const float *majorants;
+  const unsigned *mcOccupied;  // bit (i & 31) of word i >> 5 set iff majorants[i] != 0
   int3 mcDims;
   float3 mcOrigin;
   float3 rcpMcSpacing;  // 1/(8*gridSpacing)
@@ -88,11 +90,12 @@ struct LaunchCounters {
   unsigned int abort;       // host-set abort request
 };
 
-// launchers (bn_kernels.cu)
-cudaError_t launchBuildMacrocells(const VolumeDD &vol, float2 *ranges, float *majorants, int roundUp,
-                                  cudaStream_t s);
-cudaError_t launchMapMajorants(const VolumeDD &vol, const float2 *ranges, float *majorants, int roundUp,
-                               cudaStream_t s);
+// launchers (bn_kernels.cu).  Both majorant launchers also write the
+// occupancy bitmap of the new majorants, ceil(n/32) words.
+cudaError_t launchBuildMacrocells(const VolumeDD &vol, float2 *ranges, float *majorants, unsigned *occupied,
+                                  int roundUp, cudaStream_t s);
+cudaError_t launchMapMajorants(const VolumeDD &vol, const float2 *ranges, float *majorants, unsigned *occupied,
+                               int roundUp, cudaStream_t s);
 cudaError_t launchRender(const VolumeDD &vol, const FrameDD &frame, LaunchCounters *counters, int blocksPerSM,
                          int threadsPerBlock, cudaStream_t s, const SchedDD &sd = SchedDD());
 // jobs / chunkStart: device arrays; chunkStart has numJobs+1 entries, the
@@ -105,8 +108,9 @@ cudaError_t launchResolve(const float4 *accum, int numPixels, int accumID, int f
 cudaError_t launchResolveBatch(const JobDD *jobs, const int *chunkStart, int numJobs, int numChunks, cudaStream_t s);
 int renderKernelMaxBlocksPerSM(int threadsPerBlock);
 
-// No-allocation render: majorant grid and counters in a static device array
-// sized for kNoAllocMaxMacrocells macrocells (see bn_kernels.cu).
+// No-allocation render: majorant grid, occupancy bitmap and counters in a
+// static device array sized for kNoAllocMaxMacrocells macrocells (see
+// bn_kernels.cu).
 constexpr int64_t kNoAllocMaxMacrocells = 64 * 64 * 64;
 cudaError_t launchRenderNoAlloc(VolumeDD v, FrameDD fr, int fmt, void *color, int roundUp, cudaStream_t s);
 

@@ -750,13 +750,15 @@ DEV void renderLoop(const JobDD *jobs, const int *chunkStart, int numJobs, int n
         if (phase == LP_CELL) {
           while (true) {
             const float tClosest = fmin_(fmin_(ts.tNext.x, ts.tNext.y), ts.tNext.z);
-            const float maj = __ldg(v.majorants + (ts.cx + (int64_t)v.mcDims.x * (ts.cy + (int64_t)v.mcDims.y * ts.cz)));
+            // cell indices are inside the grid here and the grid has < 2^31 cells
+            const int ci = ts.cx + v.mcDims.x * (ts.cy + v.mcDims.y * ts.cz);
+            const bool occupied = (__ldg(v.mcOccupied + (ci >> 5)) >> (ci & 31)) & 1u;
             nVisits++;
-            if (maj == 0.f) {
+            if (!occupied) {  // majorant == 0
               if (!ddaStep(v, ts, tClosest)) { phase = LP_ENDED; break; }
               if (++steps > (1u << 22)) { errBits |= ERR_ITER_CAP; phase = LP_ENDED; break; }
             } else {
-              ts.maj = maj;
+              ts.maj = __ldg(v.majorants + ci);
               ts.t = ts.rayT0 + ts.nextCellBegin;
               ts.tUpper = fmin_(ts.rayT0 + fmin_(tClosest, ts.ddaTMax), ts.rayTMax);
               phase = LP_WOODCOCK;
@@ -832,7 +834,7 @@ DEV void renderLoop(const JobDD *jobs, const int *chunkStart, int numJobs, int n
 }
 
 template <int T, int LOG>
-__global__ void __launch_bounds__(kRenderMaxThreads, 4)
+__global__ void __launch_bounds__(kRenderMaxThreads, kRenderMinBlocks)
     renderKernel(const __grid_constant__ JobDD job, const __grid_constant__ SchedDD sd, LaunchCounters *ctr) {
   extern __shared__ float4 sTF[];
   __shared__ float u8lut[256];
@@ -843,7 +845,7 @@ __global__ void __launch_bounds__(kRenderMaxThreads, 4)
   renderLoop<T, false, LOG>(&job, nullptr, 1, numChunks, sd, ctr, sTF, u8lut);
 }
 
-__global__ void __launch_bounds__(kRenderMaxThreads, 4)
+__global__ void __launch_bounds__(kRenderMaxThreads, kRenderMinBlocks)
     renderBatchKernel(const JobDD *jobs, const int *chunkStart, int numJobs, const __grid_constant__ SchedDD sd,
                       LaunchCounters *ctr) {
   __shared__ float u8lut[256];
@@ -929,7 +931,31 @@ static int smCount() {
   return n;
 }
 
-cudaError_t launchBuildMacrocells(const VolumeDD &v, float2 *ranges, float *majorants, int roundUp, cudaStream_t s) {
+// Occupancy bitmap of a majorant grid: one ballot per warp packs the
+// "majorant != 0" flags of 32 consecutive macrocells into one word.  The
+// render loop tests these bits (32 KB for a 64^3 grid, resident in L1)
+// instead of loading a majorant for every macrocell it crosses.
+__global__ void __launch_bounds__(256) mcOccupancyKernel(const float *majorants, int64_t n, unsigned *occupied) {
+  const int lane = threadIdx.x & 31;
+  const int64_t words = (n + 31) >> 5;
+  const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+  for (int64_t w = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; w < words; w += warps) {
+    const int64_t i = (w << 5) + lane;
+    const bool occ = i < n && majorants[i] != 0.f;
+    const unsigned bits = __ballot_sync(0xffffffffu, occ);
+    if (lane == 0) occupied[w] = bits;
+  }
+}
+
+static cudaError_t launchOccupancy(const float *majorants, int64_t n, unsigned *occupied, cudaStream_t s) {
+  const int64_t words = (n + 31) >> 5;
+  const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>((words + 7) / 8, (int64_t)smCount() * 8));
+  mcOccupancyKernel<<<blocks, 256, 0, s>>>(majorants, n, occupied);
+  return cudaGetLastError();
+}
+
+cudaError_t launchBuildMacrocells(const VolumeDD &v, float2 *ranges, float *majorants, unsigned *occupied, int roundUp,
+                                  cudaStream_t s) {
   const int64_t n = (int64_t)v.mcDims.x * v.mcDims.y * v.mcDims.z;
   const int blocks = (int)std::min<int64_t>((n + 127) / 128, (int64_t)smCount() * 16);
   switch (v.type) {
@@ -939,14 +965,17 @@ cudaError_t launchBuildMacrocells(const VolumeDD &v, float2 *ranges, float *majo
   case VOX_U16: mcBuildKernel<VOX_U16><<<blocks, 128, 0, s>>>(v, ranges, majorants, roundUp); break;
   default: mcBuildKernel<VOX_BF16><<<blocks, 128, 0, s>>>(v, ranges, majorants, roundUp); break;
   }
-  return cudaGetLastError();
+  cudaError_t e = cudaGetLastError();
+  return e != cudaSuccess ? e : launchOccupancy(majorants, n, occupied, s);
 }
 
-cudaError_t launchMapMajorants(const VolumeDD &v, const float2 *ranges, float *majorants, int roundUp, cudaStream_t s) {
+cudaError_t launchMapMajorants(const VolumeDD &v, const float2 *ranges, float *majorants, unsigned *occupied,
+                               int roundUp, cudaStream_t s) {
   const int64_t n = (int64_t)v.mcDims.x * v.mcDims.y * v.mcDims.z;
   const int blocks = (int)std::min<int64_t>((n + 255) / 256, (int64_t)smCount() * 8);
   mcMapKernel<<<blocks, 256, 0, s>>>(v, ranges, majorants, roundUp);
-  return cudaGetLastError();
+  cudaError_t e = cudaGetLastError();
+  return e != cudaSuccess ? e : launchOccupancy(majorants, n, occupied, s);
 }
 
 template <int T>
@@ -1021,17 +1050,18 @@ int renderKernelMaxBlocksPerSM(int tpb) {
 // ---------------------------------------------------------------------------
 // No-allocation render (bnxRenderStructuredNoAlloc)
 //
-// Scratch of this path -- the macrocell majorant grid and the launch
-// counters -- lives in the file-scope array below instead of in memory the
-// context allocates.  It is sized for kNoAllocMaxMacrocells macrocells
-// (64^3, i.e. grids up to 513^3 scalars) and is held by every GPU that loads
-// the library until the process exits: 1 MiB of majorants + 256 bytes of
-// counters.  All calls share it, so calls whose work overlaps on the GPU
+// Scratch of this path -- the macrocell majorant grid, its occupancy bitmap
+// and the launch counters -- lives in the file-scope array below instead of
+// in memory the context allocates.  It is sized for kNoAllocMaxMacrocells
+// macrocells (64^3, i.e. grids up to 513^3 scalars) and is held by every GPU
+// that loads the library until the process exits: 1 MiB of majorants +
+// 32 KiB of bitmap + 256 bytes of counters.  All calls share it, so calls whose work overlaps on the GPU
 // race; each call overwrites the majorants it needs and clears the counters.
 // ---------------------------------------------------------------------------
 constexpr size_t kNoAllocCountersBytes = 256;
+constexpr size_t kNoAllocMajorantBytes = kNoAllocMaxMacrocells * sizeof(float);
 static __device__ __align__(256) unsigned char
-    g_noAllocScratch[kNoAllocCountersBytes + kNoAllocMaxMacrocells * sizeof(float)];
+    g_noAllocScratch[kNoAllocCountersBytes + kNoAllocMajorantBytes + kNoAllocMaxMacrocells / 8];
 
 // Majorant grid straight from the voxels: the fused build of mcBuildKernel
 // without storing the scalar ranges.
@@ -1092,7 +1122,10 @@ cudaError_t launchRenderNoAlloc(VolumeDD v, FrameDD fr, int fmt, void *color, in
   unsigned char *base = (unsigned char *)noAllocScratchAddress(&e);
   if (!base) return e;
   LaunchCounters *ctr = (LaunchCounters *)base;
-  v.majorants = (const float *)(base + kNoAllocCountersBytes);
+  float *majorants = (float *)(base + kNoAllocCountersBytes);
+  unsigned *occupied = (unsigned *)(base + kNoAllocCountersBytes + kNoAllocMajorantBytes);
+  v.majorants = majorants;
+  v.mcOccupied = occupied;
   e = cudaMemsetAsync(ctr, 0, sizeof(LaunchCounters), s);
   if (e != cudaSuccess) return e;
   const int blocks = (int)std::min<int64_t>((n + 127) / 128, (int64_t)smCount() * 16);
@@ -1104,6 +1137,8 @@ cudaError_t launchRenderNoAlloc(VolumeDD v, FrameDD fr, int fmt, void *color, in
   default: mcMajorantScratchKernel<VOX_BF16><<<blocks, 128, 0, s>>>(v, roundUp); break;
   }
   e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  e = launchOccupancy(majorants, n, occupied, s);
   if (e != cudaSuccess) return e;
   e = launchRender(v, fr, ctr, 0, 0, s);
   if (e != cudaSuccess) return e;

@@ -163,7 +163,7 @@ struct Volume : Object {
   bool needsMajorantRebuild = false;
   bool built = false;
   int mcDims[3] = {0, 0, 0};
-  DeviceBuffer tfBuf, ranges, majorants;
+  DeviceBuffer tfBuf, ranges, majorants, occupied;
   explicit Volume(Context *c) : Object(c, K_VOLUME) {}
   bool set1i(const std::string &m, int v) override {
     if (m == "bnx.majorantRoundUp") { majorantRoundUp = v ? 1 : 0; needsMajorantRebuild = true; return true; }

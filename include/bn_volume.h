@@ -262,9 +262,10 @@ BN_API void bnxVolumeGetMacrocells(BNVolume volume, int *dims3, float *rangesHos
    structured volume into the caller's accumulation buffer and resolves the
    colour into the caller's output, launching asynchronously on cudaStream
    (NULL: the legacy default stream) and allocating nothing: the macrocell
-   majorant grid and the launch counters live in a static device array sized
-   for BNX_NOALLOC_MAX_MACROCELLS macrocells (64^3, i.e. grids up to 513^3
-   scalars; 1 MiB held by every GPU that loads the library until exit).
+   majorant grid, its occupancy bitmap and the launch counters live in a
+   static device array sized for BNX_NOALLOC_MAX_MACROCELLS macrocells (64^3,
+   i.e. grids up to 513^3 scalars; 1.03 MiB held by every GPU that loads the
+   library until exit).
    Larger volumes are rejected with error 2 and a message.  All calls share
    that array, so calls whose work overlaps on the GPU (other streams, other
    host threads) race; serialise them.  The first call on each device looks
