@@ -49,7 +49,7 @@ EXPORTS = [
     "bnxSetLaunchConfig", "bnxFrameBufferDevicePointer", "bnxVolumeGetMacrocells",
     "bnxRenderStructuredNoAlloc", "bnxSetScheduling", "bnxRenderBatch", "bnxSetBatchGraphs", "bnxAutotuneBatch",
     "bnxServerCreate", "bnxServerDestroy", "bnxServerSubmit", "bnxServerWait", "bnxServerGetStats",
-    "bnxServerResetStats", "bnxSetRenderTimeout", "bnxAnariTransferFunction1D", "bnxAnariDensityScale",
+    "bnxServerResetStats", "bnxServerReserve", "bnxSetRenderTimeout", "bnxAnariTransferFunction1D", "bnxAnariDensityScale",
     "bnxAnariStructuredRegular",
 ]
 
@@ -117,7 +117,7 @@ class BNXServerStats(ctypes.Structure):
                                                   "active", "samples")] + \
                [("peakBytes", ctypes.c_size_t)] + \
                [(n, ctypes.c_double) for n in ("busySeconds", "wallSeconds", "framesPerSecond", "p50Ms", "p99Ms",
-                                               "meanMs", "maxMs")]
+                                               "meanMs", "maxMs", "queueP99Ms", "maxSliceMs")]
 
 
 class BarneyError(RuntimeError):
@@ -161,6 +161,7 @@ def lib(build_if_missing=True):
         "bnxServerCreate": ([P, P], P), "bnxServerDestroy": ([P], None),
         "bnxServerSubmit": ([P, P], ctypes.c_longlong), "bnxServerWait": ([P, ctypes.c_longlong, I, P], I),
         "bnxServerGetStats": ([P, P], None), "bnxServerResetStats": ([P], None),
+        "bnxServerReserve": ([P, ctypes.c_size_t], None),
         "bnxSetRenderTimeout": ([P, I], None),
         "bnxAnariTransferFunction1D": ([P, I, I, P, I, bn_float4, F, P], I),
         "bnxAnariDensityScale": ([F], F),
@@ -449,6 +450,11 @@ class Server:
         self.context = context
         cfg = BNXServerConfig(hbm_budget_bytes, max_slots, slice_waves)
         self.h = self.L.bnxServerCreate(context.ctx, ctypes.byref(cfg))
+        check()
+
+    def reserve(self, nbytes):
+        """Take device memory for request buffers now (bnxServerReserve)."""
+        self.L.bnxServerReserve(self.h, ctypes.c_size_t(nbytes))
         check()
 
     def submit(self, renderer, camera, width, height, spp, color_format="rgba8"):

@@ -233,15 +233,8 @@ static void render(Context *ctx, Renderer &r, Model &m, Camera &cam, FrameBuffer
   }
 }
 
-// Every job's waves in one persistent launch of the batch kernel, then one
-// batch resolve.  The copy-in of the job table, the counter reset, both
-// kernels and the counter read-back are captured once into a CUDA graph per
-// batch shape (same frame buffers, sizes and launch configuration) and
-// replayed; per-frame values (cameras, accumIDs) travel in the pinned job
-// table the graph copies from.  Results equal one bnRender per job.
-void renderBatch(Context *ctx, const std::vector<BatchEntry> &entries) {
-  const int n = (int)entries.size();
-  if (n == 0) return;
+// Pinned and device job tables for batches of up to n jobs.
+void reserveBatch(Context *ctx, int n) {
   if (n > ctx->hostCapacity) {
     if (ctx->graphExec) { cudaGraphExecDestroy(ctx->graphExec); ctx->graphExec = nullptr; ctx->graphKey.clear(); }
     if (ctx->hostJobs) cudaFreeHost(ctx->hostJobs);
@@ -256,6 +249,18 @@ void renderBatch(Context *ctx, const std::vector<BatchEntry> &entries) {
     ctx->batchChunks.resize((cap + 1) * sizeof(int));
     ctx->hostCapacity = cap;
   }
+}
+
+// Every job's waves in one persistent launch of the batch kernel, then one
+// batch resolve.  The copy-in of the job table, the counter reset, both
+// kernels and the counter read-back are captured once into a CUDA graph per
+// batch shape (same frame buffers, sizes and launch configuration) and
+// replayed; per-frame values (cameras, accumIDs) travel in the pinned job
+// table the graph copies from.  Results equal one bnRender per job.
+void renderBatch(Context *ctx, const std::vector<BatchEntry> &entries) {
+  const int n = (int)entries.size();
+  if (n == 0) return;
+  reserveBatch(ctx, n);
   std::vector<const void *> key;
   long long chunks = 0;
   unsigned long long pixelSamples = 0;

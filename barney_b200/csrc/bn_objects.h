@@ -377,6 +377,7 @@ inline std::shared_ptr<T> getAs(BNObject h, Object::Kind k, const char *what) {
 struct BatchEntry { Renderer *r; Model *m; Camera *c; FrameBuffer *fb; };
 JobDD buildJob(Context *ctx, Renderer &r, Model &m, Camera &cam, FrameBuffer &fb);
 void renderBatch(Context *ctx, const std::vector<BatchEntry> &entries);
+void reserveBatch(Context *ctx, int numJobs);  // job tables for batches up to numJobs
 
 }  // namespace bnb
 

@@ -21,8 +21,11 @@
 // keyed by (pixel, accumID), never by queue position.
 #include "bn_objects.h"
 
+#include <algorithm>
 #include <chrono>
 #include <condition_variable>
+#include <cstdio>
+#include <cstdlib>
 #include <deque>
 #include <map>
 #include <thread>
@@ -46,23 +49,67 @@ struct ServerRequest {
   size_t resultBytes = 0;
 };
 
-// Pool of equally sized device buffers, so steady-state serving performs
-// no cudaMalloc / cudaFree (either would synchronise the device).
+// Device buffers of admitted requests.  Buffers are carved out of large
+// chunks (one cudaMalloc per kChunkBytes, 256-byte aligned) and, once
+// released, kept on a free list keyed by size for the next request of that
+// size: a cudaMalloc per request measured several milliseconds each inside a
+// serving process, and admitting a burst of requests stalled the GPU for
+// hundreds of milliseconds.  The worker takes buffers; client threads return
+// colour buffers after reading them.  Chunks are freed with the server.
 struct BufferPool {
+  static constexpr size_t kChunkBytes = (size_t)256 << 20;
+  struct Chunk {
+    unsigned char *base;
+    size_t size, used;
+  };
+  std::mutex m;
   std::multimap<size_t, void *> freeDevice;
+  std::vector<Chunk> chunks;
   size_t deviceBytesHeld = 0;
   ~BufferPool() {
-    for (auto &kv : freeDevice) cudaFree(kv.second);
+    for (auto &c : chunks) cudaFree(c.base);
   }
   void *getDevice(size_t n) {
-    auto it = freeDevice.find(n);
-    if (it != freeDevice.end()) { void *p = it->second; freeDevice.erase(it); return p; }
-    void *p = nullptr;
-    ck(cudaMalloc(&p, n), "server buffer");
-    deviceBytesHeld += n;
-    return p;
+    const size_t need = (n + 255) & ~(size_t)255;
+    {
+      std::lock_guard<std::mutex> l(m);
+      auto it = freeDevice.find(n);
+      if (it != freeDevice.end()) { void *p = it->second; freeDevice.erase(it); return p; }
+      for (auto &c : chunks)  // first chunk with room at its end
+        if (c.size - c.used >= need) {
+          void *p = c.base + c.used;
+          c.used += need;
+          return p;
+        }
+    }
+    // a new chunk, not under the lock: cudaMalloc can take milliseconds
+    const size_t size = std::max(kChunkBytes, need);
+    void *base = nullptr;
+    ck(cudaMalloc(&base, size), "server buffer chunk");
+    std::lock_guard<std::mutex> l(m);
+    chunks.push_back({(unsigned char *)base, size, need});
+    deviceBytesHeld += size;
+    return base;
   }
-  void putDevice(void *p, size_t n) { if (p) freeDevice.emplace(n, p); }
+  void putDevice(void *p, size_t n) {
+    if (!p) return;
+    std::lock_guard<std::mutex> l(m);
+    freeDevice.emplace(n, p);
+  }
+  // chunks until at least `bytes` are held, so that serving allocates nothing
+  void reserve(size_t bytes) {
+    while (true) {
+      {
+        std::lock_guard<std::mutex> l(m);
+        if (deviceBytesHeld >= bytes) return;
+      }
+      void *base = nullptr;
+      ck(cudaMalloc(&base, kChunkBytes), "server buffer chunk");
+      std::lock_guard<std::mutex> l(m);
+      chunks.push_back({(unsigned char *)base, kChunkBytes, 0});
+      deviceBytesHeld += kChunkBytes;
+    }
+  }
 };
 
 struct Server {
@@ -79,7 +126,10 @@ struct Server {
   BufferPool pool;
   std::thread worker;
   // statistics
-  std::vector<double> latenciesMs;
+  std::vector<double> latenciesMs, queueWaitsMs;
+  double maxSliceMs = 0.0;
+  FILE *trace = nullptr;  // BNX_SERVER_TRACE: one line per launch
+  Clock::time_point created = Clock::now(), lastSliceEnd = Clock::now();
   unsigned long long submittedCount = 0, completedCount = 0, rejectedCount = 0, launches = 0;
   double busySeconds = 0.0;
   Clock::time_point statsStart = Clock::now();
@@ -89,6 +139,13 @@ struct Server {
 
   Server(Context *c, const BNXServerConfig &config) : ctx(c), cfg(config) {
     ck(cudaStreamCreateWithFlags(&copyStream, cudaStreamNonBlocking), "server copy stream");
+    reserveBatch(ctx, cfg.maxSlots);  // no pinned-table growth while serving
+    if (const char *path = std::getenv("BNX_SERVER_TRACE")) {
+      trace = std::fopen(path, "a");
+      if (trace)
+        std::fprintf(trace,
+                     "# start_ms gap_ms admit_ms dur_ms requests admitted retired queued waves pixel_waves\n");
+    }
     worker = std::thread([this] { loop(); });
   }
   ~Server() {
@@ -101,6 +158,7 @@ struct Server {
     for (auto &r : active) releaseDevice(*r);
     for (auto &kv : finished) releaseResult(*kv.second);
     if (copyStream) cudaStreamDestroy(copyStream);
+    if (trace) std::fclose(trace);
     cudaGetLastError();
   }
 
@@ -135,7 +193,8 @@ struct Server {
     r.fb.reset();
   }
 
-  // device buffers of an admitted request (from the pool)
+  // device buffers of an admitted request (from the pool); its bytes were
+  // reserved against the budget when it was picked for admission
   void acquireDevice(ServerRequest &r) {
     auto fb = std::make_shared<FrameBuffer>(ctx);
     const int w = r.fb ? r.fb->width : 0, h = r.fb ? r.fb->height : 0;
@@ -144,32 +203,41 @@ struct Server {
     fb->height = h;
     fb->colorFormat = fmt;
     const size_t px = (size_t)w * h;
-    fb->accum.ptr = pool.getDevice(px * 16);
-    fb->accum.bytes = px * 16;
-    if (r.renderer->p.compensatedAccum) {
-      fb->comp.ptr = pool.getDevice(px * 16);
-      fb->comp.bytes = px * 16;
-      ck(cudaMemsetAsync(fb->comp.ptr, 0, px * 16, ctx->stream), "compensation clear");
-    }
     const size_t cb = px * (fmt == FMT_FLOAT4 ? 16 : 4);
-    fb->color.ptr = pool.getDevice(cb);
-    fb->color.bytes = cb;
+    try {
+      fb->accum.ptr = pool.getDevice(px * 16);
+      fb->accum.bytes = px * 16;
+      if (r.renderer->p.compensatedAccum) {
+        fb->comp.ptr = pool.getDevice(px * 16);
+        fb->comp.bytes = px * 16;
+        ck(cudaMemsetAsync(fb->comp.ptr, 0, px * 16, ctx->stream), "compensation clear");
+      }
+      fb->color.ptr = pool.getDevice(cb);
+      fb->color.bytes = cb;
+    } catch (...) {  // give back what was taken; the pool owns the buffers
+      pool.putDevice(fb->accum.ptr, fb->accum.bytes);
+      pool.putDevice(fb->comp.ptr, fb->comp.bytes);
+      fb->accum.ptr = fb->comp.ptr = nullptr;
+      throw;
+    }
     fb->accumID = 0;
     r.fb = fb;
-    bytesInUse += r.deviceBytes;
-    peakBytes = std::max(peakBytes, bytesInUse);
   }
 
   void loop() {
     cudaSetDevice(ctx->device);
     while (true) {
-      std::vector<std::shared_ptr<ServerRequest>> slice;
+      std::vector<std::shared_ptr<ServerRequest>> slice, admit;
+      int admittedNow = 0;
+      size_t queuedNow = 0;
+      double admitMs = 0.0;
       {
         std::unique_lock<std::mutex> l(m);
         cvWork.wait(l, [&] { return stop || !queue.empty() || !active.empty(); });
         if (stop) return;
-        // 1. admission, in arrival order, by HBM budget and slots
-        while (!queue.empty() && (int)active.size() < cfg.maxSlots) {
+        // 1. admission, in arrival order, by HBM budget and slots: the
+        //    bytes are reserved here, the buffers taken below without the lock
+        while (!queue.empty() && (int)(active.size() + admit.size()) < cfg.maxSlots) {
           auto r = queue.front();
           if (r->deviceBytes > cfg.hbmBudgetBytes) {  // can never fit: reject
             queue.pop_front();
@@ -183,16 +251,46 @@ struct Server {
           }
           if (bytesInUse + r->deviceBytes > cfg.hbmBudgetBytes) break;
           queue.pop_front();
-          try {
-            acquireDevice(*r);
-          } catch (const Error &) {  // out of device memory: retry once others finish
-            queue.push_front(r);
-            break;
-          }
+          bytesInUse += r->deviceBytes;
+          peakBytes = std::max(peakBytes, bytesInUse);
+          admit.push_back(r);
+        }
+      }
+      const auto ta = Clock::now();
+      std::vector<std::shared_ptr<ServerRequest>> noMemory;
+      for (auto &r : admit) {
+        try {
+          acquireDevice(*r);
+        } catch (const Error &) {  // out of device memory: retry once others finish
+          noMemory.push_back(r);
+        }
+      }
+      admitMs = std::chrono::duration<double, std::milli>(Clock::now() - ta).count();
+      {
+        std::lock_guard<std::mutex> l(m);
+        for (auto &r : admit) {
+          if (std::find(noMemory.begin(), noMemory.end(), r) != noMemory.end()) continue;
           r->admitted = Clock::now();
+          queueWaitsMs.push_back(std::chrono::duration<double, std::milli>(r->admitted - r->submitted).count());
           active.push_back(r);
+          admittedNow++;
+        }
+        for (auto it = noMemory.rbegin(); it != noMemory.rend(); ++it) {
+          bytesInUse -= (*it)->deviceBytes;
+          if (active.empty()) {  // nothing will free memory: the request cannot run
+            auto &r = *it;
+            r->failed = true;
+            r->error = "out of device memory for the request's buffers";
+            r->done = true;
+            rejectedCount++;
+            finished[r->id] = r;
+            cvDone.notify_all();
+          } else {
+            queue.push_front(*it);
+          }
         }
         slice = active;
+        queuedNow = queue.size();
       }
       if (slice.empty()) {
         std::this_thread::sleep_for(std::chrono::microseconds(200));
@@ -201,8 +299,11 @@ struct Server {
       // 2. one slice of waves for every admitted request, one launch
       std::vector<BatchEntry> entries;
       std::vector<int> waves;
+      long long sliceWaves = 0, pixelWaves = 0;
       for (auto &r : slice) {
         const int n = std::min(cfg.sliceWaves, r->spp - r->wavesDone);
+        sliceWaves += n;
+        pixelWaves += (long long)n * r->fb->width * r->fb->height;
         r->renderer->p.pathsPerPixel = n;
         waves.push_back(n);
         entries.push_back({r->renderer.get(), r->model.get(), r->camera.get(), r->fb.get()});
@@ -220,9 +321,12 @@ struct Server {
       const auto t1 = Clock::now();
       // 3. completions
       std::lock_guard<std::mutex> l(m);
-      busySeconds += std::chrono::duration<double>(t1 - t0).count();
+      const double durMs = std::chrono::duration<double, std::milli>(t1 - t0).count();
+      busySeconds += durMs * 1e-3;
+      maxSliceMs = std::max(maxSliceMs, durMs);
       launches++;
       samples += ctx->stats.samples;
+      int retiredNow = 0;
       std::vector<std::shared_ptr<ServerRequest>> still;
       for (size_t i = 0; i < slice.size(); i++) {
         auto &r = slice[i];
@@ -234,6 +338,7 @@ struct Server {
         }
         r->finished = Clock::now();
         r->done = true;
+        retiredNow++;
         releaseDevice(*r, !r->failed);
         if (!r->failed) {
           latenciesMs.push_back(std::chrono::duration<double, std::milli>(r->finished - r->submitted).count());
@@ -242,6 +347,15 @@ struct Server {
         finished[r->id] = r;
       }
       active.swap(still);
+      if (trace) {
+        std::fprintf(trace, "%.3f %.3f %.3f %.3f %zu %d %d %zu %lld %lld\n",
+                     std::chrono::duration<double, std::milli>(t0 - created).count(),
+                     std::chrono::duration<double, std::milli>(t0 - lastSliceEnd).count(), admitMs, durMs,
+                     slice.size(),
+                     admittedNow, retiredNow, queuedNow, sliceWaves, pixelWaves);
+        std::fflush(trace);
+      }
+      lastSliceEnd = t1;
       cvDone.notify_all();
     }
   }
@@ -287,6 +401,15 @@ BN_API void bnxServerDestroy(BNXServer server) {
     owned = std::move(g_servers[s]);
     g_servers.erase(s);
   }
+  BN_CATCH()
+}
+
+BN_API void bnxServerReserve(BNXServer server, size_t bytes) {
+  BN_TRY
+  Server *s = getServer(server);
+  if (bytes > s->cfg.hbmBudgetBytes) throw Error(E_INVALID_ARG, "reservation exceeds the server's HBM budget");
+  s->ctx->activate();
+  s->pool.reserve(bytes);
   BN_CATCH()
 }
 
@@ -387,6 +510,12 @@ BN_API void bnxServerGetStats(BNXServer server, BNXServerStats *out) {
     st.meanMs = sum / v.size();
     st.maxMs = v.back();
   }
+  if (!s->queueWaitsMs.empty()) {
+    std::vector<double> q = s->queueWaitsMs;
+    std::sort(q.begin(), q.end());
+    st.queueP99Ms = q[std::min(q.size() - 1, (size_t)(0.99 * (q.size() - 1) + 0.5))];
+  }
+  st.maxSliceMs = s->maxSliceMs;
   *out = st;
   BN_CATCH()
 }
@@ -396,6 +525,8 @@ BN_API void bnxServerResetStats(BNXServer server) {
   Server *s = getServer(server);
   std::lock_guard<std::mutex> l(s->m);
   s->latenciesMs.clear();
+  s->queueWaitsMs.clear();
+  s->maxSliceMs = 0;
   s->submittedCount = s->completedCount = s->rejectedCount = s->launches = 0;
   s->busySeconds = 0;
   s->samples = 0;

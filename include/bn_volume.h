@@ -328,15 +328,28 @@ typedef struct {
   size_t peakBytes;
   double busySeconds, wallSeconds, framesPerSecond;
   double p50Ms, p99Ms, meanMs, maxMs;  /* submission to completion */
+  double queueP99Ms;                   /* submission to admission */
+  double maxSliceMs;                   /* longest launch (host time around it) */
 } BNXServerStats;
 BN_API BNXServer bnxServerCreate(BNContext context, const BNXServerConfig *config);
 BN_API void bnxServerDestroy(BNXServer server);
+/* Takes `bytes` (at most the HBM budget) of device memory for request
+   buffers now, in 256 MiB chunks, so that admissions find buffers without a
+   cudaMalloc, which inside a busy process took up to tens of milliseconds per
+   chunk.  Without a reservation the chunks are taken as requests need them. */
+BN_API void bnxServerReserve(BNXServer server, size_t bytes);
 /* returns the request id (>= 0), or -1 on error; callable from any thread */
 BN_API long long bnxServerSubmit(BNXServer server, const BNXRequest *request);
 /* waits up to timeoutMs (< 0: forever) for a request; copies its colour
    channel into hostPixels (may be NULL) and forgets it.  Returns 1 when
    done, 0 on timeout, a negative error code on failure. */
 BN_API int bnxServerWait(BNXServer server, long long id, int timeoutMs, void *hostPixels);
+/* Setting the environment variable BNX_SERVER_TRACE to a file path makes
+   every server created afterwards append one line per launch to that file:
+   start and gap since the previous launch (ms from the server's creation),
+   time spent taking device buffers for newly admitted requests, duration,
+   requests in the launch, admitted and retired by it, queue length, waves and
+   pixel-waves rendered. */
 BN_API void bnxServerGetStats(BNXServer server, BNXServerStats *stats);
 BN_API void bnxServerResetStats(BNXServer server);
 

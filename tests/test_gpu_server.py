@@ -86,3 +86,28 @@ def test_request_beyond_budget_is_rejected_and_solo_render_matches():
         for r in rs:
             r.close()
         ctx.close()
+
+
+def test_reserved_buffers_serve_identical_frames():
+    bn, ctx, scenes, rs, server = _setup(1 << 30, 8, 2)
+    try:
+        with pytest.raises(bn.BarneyError):
+            server.reserve(2 << 30)  # beyond the budget
+        server.reserve(300 << 20)  # two 256 MiB chunks
+        rng = np.random.default_rng(11)
+        reqs = []
+        for i in range(8):
+            k = i % len(scenes)
+            cam = synth.orbit_camera(rng)
+            w, h, spp = 20 + 4 * i, 18, 1 + i % 3
+            reqs.append((server.submit(rs[k], cam, w, h, spp, "float4"), k, cam, w, h, spp))
+        for rid, k, cam, w, h, spp in reqs:
+            out = np.zeros((h, w, 4), np.float32)
+            assert server.wait(rid, out, timeout_ms=60000)
+            assert_bitexact(out, _expected(scenes[k], cam, w, h, spp), f"request {rid}")
+        assert server.stats()["completed"] == 8
+    finally:
+        server.close()
+        for r in rs:
+            r.close()
+        ctx.close()
