@@ -355,7 +355,7 @@ class VolumeRenderer:
         L.bnSet4f(self.renderer, b"cutPlane", *desc.get("cut_plane", (0.0, 0.0, 0.0, -1e30)))
         L.bnSet1f(self.renderer, b"ambientRadiance", desc.get("ambient", 1.0))
         L.bnSet1i(self.renderer, b"pathsPerPixel", int(spp))
-        L.bnSet1i(self.renderer, b"maxVolumeBounces", 0)
+        L.bnSet1i(self.renderer, b"maxVolumeBounces", int(desc.get("max_volume_bounces", 0)))
         L.bnSet1i(self.renderer, b"bnx.hgPhase", 1 if desc.get("phase", "simple") == "hg" else 0)
         L.bnSet1i(self.renderer, b"bnx.emissionAbsorption", int(desc.get("emission_absorption", False)))
         L.bnSet1i(self.renderer, b"bnx.exactLog", int(desc.get("exact_log", False)))

@@ -117,8 +117,6 @@ JobDD buildJob(Context *ctx, Renderer &r, Model &m, Camera &cam, FrameBuffer &fb
   if (fb.width <= 0 || fb.height <= 0) throw Error(E_STATE, "frame buffer has not been resized");
   if (cam.apertureRadius > 0.f) throw Error(E_UNSUPPORTED, "depth-of-field cameras are not supported");
   const Renderer::Params &p = r.p;
-  if (p.hgPhase && p.maxVolumeBounces > 0)
-    throw Error(E_UNSUPPORTED, "multiple volume scattering (maxVolumeBounces > 0) is not supported");
   Volume &vol = *m.group->volume;
   vol.build();  // no-op unless the TF changed
   JobDD job{};
@@ -145,6 +143,10 @@ JobDD buildJob(Context *ctx, Renderer &r, Model &m, Camera &cam, FrameBuffer &fb
   }
   fr.emissionAbsorption = p.emissionAbsorption;
   fr.exactLog = p.exactLog;
+  // maxVolumeBounces acts in the multi-scatter build only (bnx.hgPhase); the
+  // default build treats a volume scatter as the end of the path
+  // (shadeRays.cu:23-25,774-796), so there it has no effect, as in Barney
+  fr.maxVolumeBounces = (p.hgPhase && p.maxVolumeBounces > 0) ? p.maxVolumeBounces : 0;
   fr.accum = (float4 *)fb.accum.ptr;
   fr.comp = nullptr;
   if (p.compensatedAccum) {
@@ -264,11 +266,13 @@ void renderBatch(Context *ctx, const std::vector<BatchEntry> &entries) {
   std::vector<const void *> key;
   long long chunks = 0;
   unsigned long long pixelSamples = 0;
+  bool multiScatter = false;
   ctx->hostChunks[0] = 0;
   for (int i = 0; i < n; i++) {
     const BatchEntry &e = entries[i];
     JobDD job = buildJob(ctx, *e.r, *e.m, *e.c, *e.fb);
     if (job.fr.spp <= 0) throw Error(E_INVALID_ARG, "every batch job needs pathsPerPixel >= 1");
+    multiScatter = multiScatter || job.fr.maxVolumeBounces > 0;
     ctx->hostJobs[i] = job;
     chunks += ((long long)job.fr.width * job.fr.height + 31) / 32;
     if (chunks > 0x7fffffffLL) throw Error(E_INVALID_ARG, "batch too large");
@@ -282,6 +286,7 @@ void renderBatch(Context *ctx, const std::vector<BatchEntry> &entries) {
   key.push_back((const void *)(intptr_t)(ctx->blocksPerSM * 4096 + ctx->threadsPerBlock));
   key.push_back((const void *)(intptr_t)ctx->sched.serviceBatch);
   key.push_back((const void *)(intptr_t)n);
+  key.push_back((const void *)(intptr_t)(multiScatter ? 1 : 0));
   auto enqueue = [&](cudaStream_t s, bool timed) {
     ck(cudaMemcpyAsync(ctx->batchJobs.ptr, ctx->hostJobs, n * sizeof(JobDD), cudaMemcpyHostToDevice, s), "job table");
     ck(cudaMemcpyAsync(ctx->batchChunks.ptr, ctx->hostChunks, (n + 1) * sizeof(int), cudaMemcpyHostToDevice, s),
@@ -289,7 +294,7 @@ void renderBatch(Context *ctx, const std::vector<BatchEntry> &entries) {
     ck(cudaMemsetAsync(ctx->dCounters, 0, sizeof(LaunchCounters), s), "counter reset");
     if (timed) ck(cudaEventRecord(ctx->ev[0], s), "event");
     ck(launchRenderBatch((const JobDD *)ctx->batchJobs.ptr, (const int *)ctx->batchChunks.ptr, n, ctx->dCounters,
-                         ctx->blocksPerSM, ctx->threadsPerBlock, s, ctx->sched),
+                         ctx->blocksPerSM, ctx->threadsPerBlock, s, ctx->sched, multiScatter),
        "batch render kernel");
     if (timed) ck(cudaEventRecord(ctx->ev[1], s), "event");
     ck(launchResolveBatch((const JobDD *)ctx->batchJobs.ptr, (const int *)ctx->batchChunks.ptr, n, (int)chunks, s),

@@ -60,6 +60,7 @@ struct FrameDD {
   DirLightDD dirLights[kMaxDirLights];
   int emissionAbsorption;
   int exactLog;
+  int maxVolumeBounces;  // > 0: multi-scatter build (HG phase), scattered rays up to this many volume bounces
   float4 *accum;        // width*height, linear
   float4 *comp;         // width*height Neumaier compensation terms, or null (plain sums)
   int accumID0;         // accumID of the first wave of this launch
@@ -100,8 +101,10 @@ cudaError_t launchRender(const VolumeDD &vol, const FrameDD &frame, LaunchCounte
                          int threadsPerBlock, cudaStream_t s, const SchedDD &sd = SchedDD());
 // jobs / chunkStart: device arrays; chunkStart has numJobs+1 entries, the
 // prefix sum of each job's ceil(width*height/32) pixel chunks.
+// multiScatter: some job has fr.maxVolumeBounces > 0 (selects the kernel that can continue paths)
 cudaError_t launchRenderBatch(const JobDD *jobs, const int *chunkStart, int numJobs, LaunchCounters *counters,
-                              int blocksPerSM, int threadsPerBlock, cudaStream_t s, const SchedDD &sd = SchedDD());
+                              int blocksPerSM, int threadsPerBlock, cudaStream_t s, const SchedDD &sd = SchedDD(),
+                              bool multiScatter = false);
 cudaError_t launchResolve(const float4 *accum, int numPixels, int accumID, int fmt, void *out, cudaStream_t s,
                           const float4 *comp = nullptr);
 // resolves every job of a batch table into its fr.color after its waves

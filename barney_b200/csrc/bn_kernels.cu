@@ -348,6 +348,77 @@ DEV float hgPhase(float g, float cosTheta) {
   return kOneOverFourPi * (1.f - g2) / (denom * sqrtf(denom));
 }
 
+// Natural logarithm of a normal binary32 x > 0, for the exact-log free-flight
+// step (bnx.exactLog).  logf differs in its last bits between CUDA and host
+// libm, so the oracle and the CUDA kernels share this one evaluation:
+// x = m 2^e with m in [sqrt(1/2), sqrt(2)), log m = 2 atanh(s) with
+// s = (m-1)/(m+1) (|s| <= 0.1716) as an odd series to s^11, plus e ln2 with
+// ln2 split as 0.693145751953125 (16 significant bits, so e times it is
+// exact) + 1.42860682e-6.  Within 1.7 ulp of log over (0, 1].
+DEV float logPortable(float x) {
+  const uint32_t b = __float_as_uint(x);
+  int e = (int)((b >> 23) & 0xffu) - 127;
+  float m = __uint_as_float((b & 0x7fffffu) | 0x3f800000u);
+  if (m > 1.41421356f) {
+    m = m * 0.5f;
+    e += 1;
+  }
+  const float s = (m - 1.f) / (m + 1.f);
+  const float z = s * s;
+  const float p = 0.666666667f + z * (0.4f + z * (0.285714286f + z * (0.222222222f + z * 0.181818182f)));
+  const float lm = 2.f * s + s * (z * p);
+  const float fe = (float)e;
+  return fe * 0.693145751953125f + (fe * 1.42860682e-6f + lm);
+}
+
+// sin and cos of x in [0, 2pi] (the HG sampler's azimuth).  The reference
+// calls cosf/sinf, whose last bits differ between CUDA and host libm; the
+// oracle and these kernels share one binary32 evaluation instead:
+// Cody-Waite reduction by pi/2 = P1 + P2 + P3 (P1 has 8 significant bits, so
+// j*P1 is exact) to |r| <= pi/4, then the Taylor series of sin to r^11 and
+// of cos to r^12 (truncation error below 1e-10) in Horner form.
+DEV void sincosPortable(float x, float &sn, float &cs) {
+  const float j = rintf(x * 0.636619772f);
+  const float r = ((x - j * 1.5703125f) - j * 4.83751296997070312e-4f) - j * 7.54978995e-8f;
+  const float r2 = r * r;
+  const float sp = r + r * (r2 * (-1.66666667e-1f + r2 * (8.33333333e-3f + r2 * (-1.98412698e-4f +
+                   r2 * (2.75573192e-6f + r2 * -2.50521084e-8f)))));
+  const float cp = 1.f + r2 * (-0.5f + r2 * (4.16666667e-2f + r2 * (-1.38888889e-3f + r2 * (2.48015873e-5f +
+                   r2 * (-2.75573192e-7f + r2 * 2.08767570e-9f)))));
+  switch ((int)j & 3) {
+  case 0: sn = sp; cs = cp; break;
+  case 1: sn = cp; cs = -sp; break;
+  case 2: sn = -sp; cs = -cp; break;
+  default: sn = -cp; cs = sp; break;
+  }
+}
+
+DEV float3 cross3(float3 a, float3 b) {
+  return f3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
+}
+
+// HGPhase::sampleDirection, Phase.h:76-101 (cosf/sinf via sincosPortable)
+DEV float3 hgSampleDirection(float3 wi_in, float g, uint64_t &random) {
+  const float u0 = rngFloat(random);
+  const float u1 = rngFloat(random);
+  float cosTheta;
+  if (fabsf(g) < 1e-3f) cosTheta = 1.f - 2.f * u0;
+  else {
+    const float sqrTerm = (1.f - g * g) / (1.f + g - 2.f * g * u0);
+    cosTheta = (1.f + g * g - sqrTerm * sqrTerm) / (2.f * g);
+  }
+  const float sinTheta = sqrtf(fmax_(0.f, 1.f - cosTheta * cosTheta));
+  const float phi = (2.f * ONE_PI_F) * u1;
+  float sinPhi, cosPhi;
+  sincosPortable(phi, sinPhi, cosPhi);
+  const float3 local = f3(cosPhi * sinTheta, sinPhi * sinTheta, cosTheta);
+  const float3 w = normalize3(wi_in);
+  const float3 u = fabsf(w.x) > 0.1f ? normalize3(cross3(f3(0.f, 1.f, 0.f), w)) : normalize3(cross3(f3(1.f, 0.f, 0.f), w));
+  const float3 vv = cross3(w, u);
+  return normalize3(f3(local.x * u.x + local.y * vv.x + local.z * w.x, local.x * u.y + local.y * vv.y + local.z * w.y,
+                       local.x * u.z + local.y * vv.z + local.z * w.z));
+}
+
 // shadeRays.cu:294-402 restricted to the constant environment and
 // directional lights, N = 0 (volume hit).  Returns false if no light
 // sample; sets lightNeedsMIS / lightIsDirLight.
@@ -459,7 +530,10 @@ constexpr int kChunk = 32;  // pixels a warp takes at a time (one 8x4 tile)
 // __grid_constant__ parameter, TF staged in shared memory) and the batch
 // kernel (a job table in global memory, chunks of all jobs in one counter).
 // LOG: 0 fastLog (Volume.h:154-164), 1 -logf (bnx.exactLog), 2 per job (batch)
-template <int T, bool BATCH, int LOG>
+// shadeRays.cu:17-41 (MAX_PATH_DEPTH)
+constexpr int kMaxPathDepth = 10;
+
+template <int T, bool BATCH, int LOG, bool MS>
 DEV void renderLoop(const JobDD *jobs, const int *chunkStart, int numJobs, int numChunks, const SchedDD &sd,
                     LaunchCounters *ctr, const float4 *sTF, const float *u8lut) {
   const unsigned FULL = 0xffffffffu;
@@ -487,6 +561,16 @@ DEV void renderLoop(const JobDD *jobs, const int *chunkStart, int numJobs, int n
   float misWeight = 0.f;
   bool shadowRay = false;
   unsigned steps = 0;
+  // MS (multi-scatter build): the path's throughput, rounded to binary16 like
+  // PathState::throughput (Ray.h:17-23); the MIS weight of the path ray; its
+  // generation; the volume bounces taken; and a scattered ray that waits
+  // while its generation's shadow ray is traced (it starts where the shadow
+  // ray starts, in direction primDir, with RNG seed pendSeed)
+  float3 pathTp = f3(1.f, 1.f, 1.f);
+  float pathMis = 1.f;
+  int depth = 0, nVolB = 0;
+  bool pend = false;
+  uint64_t pendSeed = 0;
 
   // Each round: (A) one service pass over the lanes whose ray needs host
   // work -- shading, accumulation, a new pixel, ray generation, ray set-up --
@@ -506,12 +590,15 @@ DEV void renderLoop(const JobDD *jobs, const int *chunkStart, int numJobs, int n
         const bool cmp = fr.comp != nullptr;
         bool spawned = false;
         if (!shadowRay) {
-          // primary hit: generation-0 accumulation (fragment 0, alpha 1)
-          if (accumID == 0) {
-            acc = make_float4(0.f, 0.f, 0.f, 1.f);
-            comp = make_float4(0.f, 0.f, 0.f, 0.f);
-          } else {
-            accAdd(acc.w, comp.w, 1.f, cmp);
+          // primary hit: generation-0 accumulation (fragment 0, alpha 1); a
+          // later generation's volume hit has fragment 0 and adds nothing
+          if (!MS || depth == 0) {
+            if (accumID == 0) {
+              acc = make_float4(0.f, 0.f, 0.f, 1.f);
+              comp = make_float4(0.f, 0.f, 0.f, 0.f);
+            } else {
+              accAdd(acc.w, comp.w, 1.f, cmp);
+            }
           }
           const float tHit = ts.t;
           const float3 P = f3(ts.org.x + tHit * ts.dir.x, ts.org.y + tHit * ts.dir.y, ts.org.z + tHit * ts.dir.z);
@@ -531,6 +618,7 @@ DEV void renderLoop(const JobDD *jobs, const int *chunkStart, int numJobs, int n
             const float offsetEpsilon = fmax_(1e-4f, 1e-6f * fmax_(fmax_(fabsf(P.x), fabsf(P.y)), fabsf(P.z)));
             LightSample ls;
             bool needsMIS, isDir;
+            uint64_t scatSeed = raySeed;  // the path ray's seed after the shadow ray took its copy
             if (sampleLights(fr, random, ls, needsMIS, isDir)) {
               float3 alb;
               float fpdf;
@@ -546,8 +634,11 @@ DEV void renderLoop(const JobDD *jobs, const int *chunkStart, int numJobs, int n
               if (fpdf > 0.f && !(fmax_(fmax_(fv.x, fv.y), fv.z) < 1e-4f)) {
                 fv = f3(fmin_(fv.x, 13.f), fmin_(fv.y, 13.f), fmin_(fv.z, 13.f));
                 const float ip = isinf(ls.pdf) ? 1.f : (1.f / ls.pdf);
-                const float3 tp = f3(1.f * ip * fv.x * ls.radiance.x * 1.f, 1.f * ip * fv.y * ls.radiance.y * 1.f,
-                                     1.f * ip * fv.z * ls.radiance.z * 1.f);
+                const float3 tin = MS ? pathTp : f3(1.f, 1.f, 1.f);  // incomingThroughput
+                const float3 tp = f3(tin.x * ip * fv.x * ls.radiance.x * 1.f, tin.y * ip * fv.y * ls.radiance.y * 1.f,
+                                     tin.z * ip * fv.z * ls.radiance.z * 1.f);
+                // shadowRay.rngSeed = ray.rngSeed; ray.rngSeed.next(tMax)
+                if (MS) scatSeed = (raySeed ^ ((uint64_t)__float_as_uint(tHit) << 1)) * kRngMul;
                 misWeight = 1.f;
                 bool alive = true;
                 if (!isDir && needsMIS) {
@@ -574,10 +665,62 @@ DEV void renderLoop(const JobDD *jobs, const int *chunkStart, int numJobs, int n
                 }
               }
             }
+            // multi-scatter build: HGPhase::scatter and the volume-bounce
+            // budget (shadeRays.cu:749-878).  A sample with pdf <= 1e-6 would
+            // end the path here (the reference re-traces the old ray); with
+            // anisotropy clamped to [-0.99, 0.99] (Volume.cpp:55-57) the HG
+            // pdf stays above 2e-4, so neither can happen.
+            if (MS && fr.maxVolumeBounces > 0 && depth < kMaxPathDepth) {
+              const float3 wi_in = normalize3(f3(-woN.x, -woN.y, -woN.z));
+              const float3 sdir = hgSampleDirection(wi_in, v.anisotropy, random);
+              const float pdf = hgPhase(v.anisotropy, dot3(wi_in, sdir));
+              const float3 alb = f3(v.scatteringAlbedo * hitRGB.x, v.scatteringAlbedo * hitRGB.y,
+                                    v.scatteringAlbedo * hitRGB.z);
+              const float3 f_r = f3(alb.x * pdf, alb.y * pdf, alb.z * pdf);
+              if (pdf > 0.f && !(pdf <= 1e-6f) && nVolB < fr.maxVolumeBounces) {
+                nVolB++;
+                depth++;
+                primDir = normalize3(sdir);
+                const float denom = isinf(pdf) ? 1.f : (pdf + 1e-10f);
+                pathTp = f3(roundHalf(pathTp.x * fmin_((f_r.x * 1.f) / denom, 2.5f)),
+                            roundHalf(pathTp.y * fmin_((f_r.y * 1.f) / denom, 2.5f)),
+                            roundHalf(pathTp.z * fmin_((f_r.z * 1.f) / denom, 2.5f)));
+                if (needsMIS && !isinf(pdf)) {
+                  const float ps = hgPhase(v.anisotropy, dot3(normalize3(f3(-woN.x, -woN.y, -woN.z)), normalize3(primDir)));
+                  pathMis = ps / (ps + kOneOverFourPi);
+                } else {
+                  pathMis = 1.f;
+                }
+                if (spawned) {  // after the shadow ray, from the shadow ray's origin
+                  pend = true;
+                  pendSeed = scatSeed;
+                } else {
+                  ts.org = f3(P.x + (1.f * offsetEpsilon) * woN.x, P.y + (1.f * offsetEpsilon) * woN.y,
+                              P.z + (1.f * offsetEpsilon) * woN.z);
+                  ts.dir = primDir;
+                  ts.rayTMax = kInf;
+                  raySeed = scatSeed;
+                  shadowRay = false;
+                  spawned = true;
+                  nRays++;
+                  steps = 0;
+                  phase = LP_BEGIN;
+                }
+              }
+            }
           }
         }
-        if (!spawned) {  // shadow ray occluded, or no shadow ray: the wave is done
-          if (++k == fr.spp) {
+        if (!spawned) {
+          if (MS && pend) {  // the shadow ray was occluded: the scattered ray goes next
+            ts.dir = primDir;
+            ts.rayTMax = kInf;
+            raySeed = pendSeed;
+            pend = false;
+            shadowRay = false;
+            nRays++;
+            steps = 0;
+            phase = LP_BEGIN;
+          } else if (++k == fr.spp) {  // no ray left: the wave is done
             fr.accum[pix] = acc;
             if (cmp) fr.comp[pix] = comp;
             phase = LP_IDLE;
@@ -595,7 +738,7 @@ DEV void renderLoop(const JobDD *jobs, const int *chunkStart, int numJobs, int n
         const int accumID = fr.accumID0 + k;
         const float clampMax = 10.f * (1 + accumID);
         const bool cmp = fr.comp != nullptr;
-        if (!shadowRay) {
+        if (!shadowRay && (!MS || depth == 0)) {
           const float f0x = fmin_(bg.x, clampMax), f0y = fmin_(bg.y, clampMax), f0z = fmin_(bg.z, clampMax);
           if (accumID == 0) {
             acc = make_float4(f0x, f0y, f0z, bg.w);
@@ -606,6 +749,13 @@ DEV void renderLoop(const JobDD *jobs, const int *chunkStart, int numJobs, int n
             if (f0y > 0.f) accAdd(acc.y, comp.y, f0y, cmp);
             if (f0z > 0.f) accAdd(acc.z, comp.z, f0z, cmp);
           }
+        } else if (!shadowRay) {  // a scattered ray left into the environment (shadeRays.cu:529-557)
+          const float fx = fmin_(pathTp.x * fr.ambientRadiance * pathMis, clampMax);
+          const float fy = fmin_(pathTp.y * fr.ambientRadiance * pathMis, clampMax);
+          const float fz = fmin_(pathTp.z * fr.ambientRadiance * pathMis, clampMax);
+          if (fx > 0.f) accAdd(acc.x, comp.x, fx, cmp);
+          if (fy > 0.f) accAdd(acc.y, comp.y, fy, cmp);
+          if (fz > 0.f) accAdd(acc.z, comp.z, fz, cmp);
         } else {  // the shadow ray reached the light
           const float f1x = fmin_(misWeight * shadowTp.x, clampMax);
           const float f1y = fmin_(misWeight * shadowTp.y, clampMax);
@@ -614,7 +764,16 @@ DEV void renderLoop(const JobDD *jobs, const int *chunkStart, int numJobs, int n
           if (f1y > 0.f) accAdd(acc.y, comp.y, f1y, cmp);
           if (f1z > 0.f) accAdd(acc.z, comp.z, f1z, cmp);
         }
-        if (++k == fr.spp) {
+        if (MS && shadowRay && pend) {  // the scattered ray goes next, from the shadow ray's origin
+          ts.dir = primDir;
+          ts.rayTMax = kInf;
+          raySeed = pendSeed;
+          pend = false;
+          shadowRay = false;
+          nRays++;
+          steps = 0;
+          phase = LP_BEGIN;
+        } else if (++k == fr.spp) {
           fr.accum[pix] = acc;
           if (cmp) fr.comp[pix] = comp;
           phase = LP_IDLE;
@@ -724,6 +883,13 @@ DEV void renderLoop(const JobDD *jobs, const int *chunkStart, int numJobs, int n
         }
         primDir = d;
         shadowRay = false;
+        if (MS) {
+          pathTp = f3(1.f, 1.f, 1.f);
+          pathMis = 1.f;
+          depth = 0;
+          nVolB = 0;
+          pend = false;
+        }
         nRays++;
         steps = 0;
         ts.org = o;
@@ -772,7 +938,7 @@ DEV void renderLoop(const JobDD *jobs, const int *chunkStart, int numJobs, int n
         if (phase == LP_WOODCOCK) {
           const float r = rngFloat(ts.rng);
           const bool exact = LOG == 1 || (LOG == 2 && fr.exactLog);
-          const float dt = exact ? (-logf(1.f - r) / ts.maj) : (-fastLog(1.f - r) / ts.maj);
+          const float dt = exact ? (-logPortable(1.f - r) / ts.maj) : (-fastLog(1.f - r) / ts.maj);
           ts.t += dt;
           if (ts.t >= ts.tUpper) {
             const float tClosest = fmin_(fmin_(ts.tNext.x, ts.tNext.y), ts.tNext.z);
@@ -833,7 +999,7 @@ DEV void renderLoop(const JobDD *jobs, const int *chunkStart, int numJobs, int n
   }
 }
 
-template <int T, int LOG>
+template <int T, int LOG, bool MS>
 __global__ void __launch_bounds__(kRenderMaxThreads, kRenderMinBlocks)
     renderKernel(const __grid_constant__ JobDD job, const __grid_constant__ SchedDD sd, LaunchCounters *ctr) {
   extern __shared__ float4 sTF[];
@@ -842,16 +1008,17 @@ __global__ void __launch_bounds__(kRenderMaxThreads, kRenderMinBlocks)
   for (int i = threadIdx.x; i < 256; i += blockDim.x) u8lut[i] = (float)i * 1.f / 255.f;
   __syncthreads();
   const int numChunks = (job.fr.width * job.fr.height + kChunk - 1) / kChunk;
-  renderLoop<T, false, LOG>(&job, nullptr, 1, numChunks, sd, ctr, sTF, u8lut);
+  renderLoop<T, false, LOG, MS>(&job, nullptr, 1, numChunks, sd, ctr, sTF, u8lut);
 }
 
+template <bool MS>
 __global__ void __launch_bounds__(kRenderMaxThreads, kRenderMinBlocks)
     renderBatchKernel(const JobDD *jobs, const int *chunkStart, int numJobs, const __grid_constant__ SchedDD sd,
                       LaunchCounters *ctr) {
   __shared__ float u8lut[256];
   for (int i = threadIdx.x; i < 256; i += blockDim.x) u8lut[i] = (float)i * 1.f / 255.f;
   __syncthreads();
-  renderLoop<-1, true, 2>(jobs, chunkStart, numJobs, __ldg(chunkStart + numJobs), sd, ctr, nullptr, u8lut);
+  renderLoop<-1, true, 2, MS>(jobs, chunkStart, numJobs, __ldg(chunkStart + numJobs), sd, ctr, nullptr, u8lut);
 }
 
 // ---------------------------------------------------------------------------
@@ -982,7 +1149,8 @@ template <int T>
 static cudaError_t launchRenderT(const VolumeDD &v, const FrameDD &fr, const SchedDD &sd, LaunchCounters *ctr,
                                  int bps, int tpb, cudaStream_t s) {
   const size_t smem = (size_t)v.tfN * sizeof(float4);
-  auto kern = fr.exactLog ? renderKernel<T, 1> : renderKernel<T, 0>;
+  auto kern = fr.maxVolumeBounces > 0 ? (fr.exactLog ? renderKernel<T, 1, true> : renderKernel<T, 0, true>)
+                                      : (fr.exactLog ? renderKernel<T, 1, false> : renderKernel<T, 0, false>);
   if (smem > 48 * 1024 &&
       cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
     return cudaGetLastError();
@@ -1011,15 +1179,16 @@ cudaError_t launchRender(const VolumeDD &v, const FrameDD &fr, LaunchCounters *c
 }
 
 cudaError_t launchRenderBatch(const JobDD *jobs, const int *chunkStart, int numJobs, LaunchCounters *ctr, int bps,
-                              int tpb, cudaStream_t s, const SchedDD &sd) {
+                              int tpb, cudaStream_t s, const SchedDD &sd, bool multiScatter) {
   if (tpb <= 0) tpb = 128;
+  auto kern = multiScatter ? renderBatchKernel<true> : renderBatchKernel<false>;
   if (bps <= 0) {
     int occ = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, renderBatchKernel, tpb, 0) != cudaSuccess)
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, tpb, 0) != cudaSuccess)
       return cudaGetLastError();
     bps = occ > 0 ? occ : 1;
   }
-  renderBatchKernel<<<smCount() * bps, tpb, 0, s>>>(jobs, chunkStart, numJobs, sd, ctr);
+  kern<<<smCount() * bps, tpb, 0, s>>>(jobs, chunkStart, numJobs, sd, ctr);
   return cudaGetLastError();
 }
 
@@ -1039,7 +1208,7 @@ cudaError_t launchResolve(const float4 *accum, int n, int accumID, int fmt, void
 
 int renderKernelMaxBlocksPerSM(int tpb) {
   int occ = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, renderKernel<VOX_F32, 0>, tpb, 256 * sizeof(float4)) !=
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, renderKernel<VOX_F32, 0, false>, tpb, 256 * sizeof(float4)) !=
       cudaSuccess) {
     cudaGetLastError();
     return 1;

@@ -168,7 +168,14 @@ BN_API void bnBuild(BNModel model, int whichSlot);
 /* ---------------------------------------------------------------------- */
 /* replaces barney.cu bnCameraCreate; type "perspective" (or "pinhole") */
 BN_API BNCamera bnCameraCreate(BNContext context, const char *type);
-/* replaces barney.cu bnRendererCreate; type "default" / "pathTracer" */
+/* replaces barney.cu bnRendererCreate; type "default" / "pathTracer".
+   Parameters (Renderer.cpp:42-95): bgColor, ambientRadiance, pathsPerPixel,
+   cutPlane, maxVolumeBounces; extensions bnx.hgPhase, bnx.emissionAbsorption,
+   bnx.exactLog, bnx.compensatedAccum.  maxVolumeBounces acts only together
+   with bnx.hgPhase, which selects Barney's multi-scatter build: scattered
+   rays continue for up to that many volume bounces (path depth at most 10,
+   shadeRays.cu:749-878).  Without it, a volume scatter ends the path, as in
+   Barney's default build. */
 BN_API BNRenderer bnRendererCreate(BNContext ctx, const char *type);
 /* replaces barney.cu bnFrameBufferCreate */
 BN_API BNFrameBuffer bnFrameBufferCreate(BNContext context, int deprecated);

@@ -50,6 +50,7 @@ class OrcScene(ctypes.Structure):
         ("exactLog", ctypes.c_int),
         ("majorantRoundUp", ctypes.c_int),
         ("compensatedAccum", ctypes.c_int),
+        ("maxVolumeBounces", ctypes.c_int),
         ("width", ctypes.c_int),
         ("height", ctypes.c_int),
     ]
@@ -96,6 +97,9 @@ def lib():
         L.orc_render.restype = D
         L.orc_resolve.argtypes = [P, P, ctypes.c_int64, I, I, P]
         L.orc64_render_expected.argtypes = [P, I, I, I, I, D, I, I, I, P]
+        L.orc_sincos.argtypes = [I, P, P, P]
+        L.orc_logp.argtypes = [I, P, P]
+        L.orc_hg_sample.argtypes = [P, F, U64, I, P]
         _lib = L
     return _lib
 
@@ -143,6 +147,7 @@ class Scene:
         s.exactLog = int(desc.get("exact_log", False))
         s.majorantRoundUp = int(desc.get("majorant_round_up", False))
         s.compensatedAccum = int(desc.get("compensated_accum", False))
+        s.maxVolumeBounces = int(desc.get("max_volume_bounces", 0))
         s.width, s.height = desc["width"], desc["height"]
         self.s = s
 
@@ -180,6 +185,30 @@ def fastlog(f):
 
 def f2h(f):
     return lib().orc_f2h(f)
+
+
+def sincos(x):
+    """The portable binary32 sin/cos shared by the oracle and the kernels."""
+    x = np.ascontiguousarray(x, np.float32)
+    sn, cs = np.empty_like(x), np.empty_like(x)
+    lib().orc_sincos(x.size, _ptr(x), _ptr(sn), _ptr(cs))
+    return sn, cs
+
+
+def logp(x):
+    """The portable binary32 natural log shared by the oracle and the kernels."""
+    x = np.ascontiguousarray(x, np.float32)
+    out = np.empty_like(x)
+    lib().orc_logp(x.size, _ptr(x), _ptr(out))
+    return out
+
+
+def hg_sample(wi, g, seed_state, n):
+    """n directions of HGPhase::sampleDirection from one RNG state."""
+    wi = np.ascontiguousarray(wi, np.float32)
+    out = np.empty((n, 3), np.float32)
+    lib().orc_hg_sample(_ptr(wi), g, seed_state, n, _ptr(out))
+    return out
 
 
 def mc_dims(sc):
@@ -254,6 +283,8 @@ def resolve(accum, accum_id, fmt="float4", comp=None):
 
 
 def render_expected_fp64(sc, rect=None, step=None, subpix=2, env_dirs=64, threads=0):
+    if sc.s.maxVolumeBounces > 0:
+        raise ValueError("the FP64 expectation covers single scattering only")
     W, H = sc.s.width, sc.s.height
     x0, y0, x1, y1 = rect if rect is not None else (0, 0, W, H)
     if step is None:

@@ -130,6 +130,7 @@ static inline float h2f(uint16_t h) {
   else out = sign | ((e + 112u) << 23) | (m << 13);
   float r; memcpy(&r, &out, 4); return r;
 }
+static inline float bitsFloat(uint32_t u) { float f; memcpy(&f, &u, 4); return f; }
 static inline float bf2f(uint16_t h) { uint32_t u = (uint32_t)h << 16; float r; memcpy(&r, &u, 4); return r; }
 static inline vec3f halfRound(vec3f v) { return {h2f(f2h(v.x)), h2f(f2h(v.y)), h2f(f2h(v.z))}; }
 
@@ -174,6 +175,30 @@ static inline float fastLog(float f) {
   s += (1.f / 5.f) * f;
   return s + s;
 }
+
+// Natural logarithm of a normal binary32 x > 0, for the exact-log free-flight
+// step (bnx.exactLog).  logf differs in its last bits between CUDA and host
+// libm, so the oracle and the CUDA kernels share this one evaluation:
+// x = m 2^e with m in [sqrt(1/2), sqrt(2)), log m = 2 atanh(s) with
+// s = (m-1)/(m+1) (|s| <= 0.1716) as an odd series to s^11, plus e ln2 with
+// ln2 split as 0.693145751953125 (16 significant bits, so e times it is
+// exact) + 1.42860682e-6.  Within 1.7 ulp of log over (0, 1].
+static inline float logPortable(float x) {
+  const uint32_t b = floatBits(x);
+  int e = (int)((b >> 23) & 0xffu) - 127;
+  float m = bitsFloat((b & 0x7fffffu) | 0x3f800000u);
+  if (m > 1.41421356f) {
+    m = m * 0.5f;
+    e += 1;
+  }
+  const float s = (m - 1.f) / (m + 1.f);
+  const float z = s * s;
+  const float p = 0.666666667f + z * (0.4f + z * (0.285714286f + z * (0.222222222f + z * 0.181818182f)));
+  const float lm = 2.f * s + s * (z * p);
+  const float fe = (float)e;
+  return fe * 0.693145751953125f + (fe * 1.42860682e-6f + lm);
+}
+
 
 } // namespace orc
 
@@ -437,7 +462,7 @@ static bool woodcock(vec4f &sample, const Scene &sc, vec3f org, vec3f dir, float
   float t = t_lower;
   while (true) {
     float r = rand();
-    float dt = sc.s.exactLog ? (-logf(1.f - r) / majorant) : (-fastLog(1.f - r) / majorant);
+    float dt = sc.s.exactLog ? (-logPortable(1.f - r) / majorant) : (-fastLog(1.f - r) / majorant);
     t += dt;
     if (t >= t_upper) return false;
     vec3f P = org + t * dir;
@@ -477,11 +502,18 @@ static void traceRay(const Scene &sc, Ray &ray, LocalStats &st) {
   });
 }
 
+// shadeRays.cu:17-41: MAX_PATH_DEPTH; PathState::throughput is vec3h
+// (Ray.h:17-23), so every stored throughput is rounded to binary16.
+static const int MAX_PATH_DEPTH = 10;
+
 struct PixelSample {
-  // gen-0 contribution
+  // generation-0 contribution
   vec3f frag0; float alpha0;
-  // gen-1 (shadow ray) contribution, valid if hasShadow
-  bool hasShadow; vec3f frag1;
+  // later generations' contributions in accumulation order: per generation
+  // the shadow ray's, then the scattered ray's
+  int n = 0;
+  vec3f frags[2 * (MAX_PATH_DEPTH + 2)];
+  void add(vec3f f) { frags[n++] = f; }
 };
 
 struct LightSample { vec3f direction, radiance; float distance; float pdf = 0.f; };
@@ -503,6 +535,52 @@ static inline float hgPhase(float g, float cosTheta) {
   float g2 = g * g;
   float denom = 1.f + g2 - 2.f * g * cosTheta;
   return ONE_OVER_FOUR_PI * (1.f - g2) / (denom * sqrtf(denom));
+}
+
+// sin and cos of x in [0, 2pi] (the phase-function samplers' azimuth).  The
+// reference calls cosf/sinf, whose last bits differ between CUDA and host
+// libm; this restatement and the CUDA kernels share one binary32
+// evaluation instead: Cody-Waite reduction by pi/2 = P1 + P2 + P3 (P1 has 8
+// significant bits, so j*P1 is exact) to |r| <= pi/4, then the Taylor series
+// of sin to r^11 and of cos to r^12 (truncation error below 1e-10) in
+// Horner form.
+static inline void sincosPortable(float x, float &sn, float &cs) {
+  const float j = rintf(x * 0.636619772f);
+  const float r = ((x - j * 1.5703125f) - j * 4.83751296997070312e-4f) - j * 7.54978995e-8f;
+  const float r2 = r * r;
+  const float sp = r + r * (r2 * (-1.66666667e-1f + r2 * (8.33333333e-3f + r2 * (-1.98412698e-4f +
+                   r2 * (2.75573192e-6f + r2 * -2.50521084e-8f)))));
+  const float cp = 1.f + r2 * (-0.5f + r2 * (4.16666667e-2f + r2 * (-1.38888889e-3f + r2 * (2.48015873e-5f +
+                   r2 * (-2.75573192e-7f + r2 * 2.08767570e-9f)))));
+  switch ((int)j & 3) {
+  case 0: sn = sp; cs = cp; break;
+  case 1: sn = cp; cs = -sp; break;
+  case 2: sn = -sp; cs = -cp; break;
+  default: sn = -cp; cs = sp; break;
+  }
+}
+
+// HGPhase::sampleDirection, Phase.h:76-101 (cosf/sinf via sincosPortable)
+static vec3f hgSampleDirection(vec3f wi_in, float g, Random2 &random) {
+  float u0 = random();
+  float u1 = random();
+  float cosTheta;
+  if (fabsf(g) < 1e-3f) cosTheta = 1.f - 2.f * u0;
+  else {
+    float sqrTerm = (1.f - g * g) / (1.f + g - 2.f * g * u0);
+    cosTheta = (1.f + g * g - sqrTerm * sqrTerm) / (2.f * g);
+  }
+  float sinTheta = sqrtf(fmax_(0.f, 1.f - cosTheta * cosTheta));
+  float phi = TWO_PI * u1;
+  float sinPhi, cosPhi;
+  sincosPortable(phi, sinPhi, cosPhi);
+  vec3f local = V(cosPhi * sinTheta, sinPhi * sinTheta, cosTheta);
+  vec3f w = normalize(wi_in);
+  vec3f u, v;
+  if (fabsf(w.x) > 0.1f) u = normalize(cross(V(0.f, 1.f, 0.f), w));
+  else u = normalize(cross(V(1.f, 0.f, 0.f), w));
+  v = cross(w, u);
+  return normalize(local.x * u + local.y * v + local.z * w);
 }
 
 // shadeRays.cu:294-402 for the lights this path has: the constant
@@ -629,60 +707,105 @@ static PixelSample renderPixelSample(const Scene &sc, int ix, int iy, int accumI
   if (!ray.hadHit) {
     out.frag0 = V(bg.x, bg.y, bg.z);
     out.alpha0 = bg.w;
-    out.hasShadow = false;
     return out;
   }
   out.frag0 = V(0.f);
   out.alpha0 = 1.f;
-  out.hasShadow = false;
   if (s.emissionAbsorption) {  // extension: collision estimator of emission
     out.frag0 = ray.hitColor;
     return out;
   }
-  Random2 random(ray.rngSeed, (uint64_t)floatBits(ray.tMax));
-  vec3f P = ray.P;
-  vec3f wo = -normalize(ray.dir);
-  const float offsetEpsilon = fmax_(1e-4f, 1e-6f * reduce_max(vabs(P)));  // safe_eps
-  LightSample ls;
-  bool lightNeedsMIS = false, lightIsDirLight = false;
-  if (!sampleLights(sc, ls, random, lightNeedsMIS, lightIsDirLight)) return out;
-  // bsdf.eval (Phase.h:68-73 / 148-154)
-  vec3f albedo;
-  float fpdf;
-  if (s.phaseMode == 0) {
-    albedo = .7f * ray.hitColor;
-    fpdf = ONE_OVER_FOUR_PI;
-  } else {
-    albedo = s.scatteringAlbedo * ray.hitColor;
-    vec3f wi_in = normalize(-wo);
-    fpdf = hgPhase(s.anisotropy, dot(wi_in, normalize(ls.direction)));
+  // path state: throughput (vec3h), MIS weight of the path ray, bounces
+  vec3f tp = V(1.f);
+  float pathMis = 1.f;
+  int numVolumeBounces = 0;
+  for (int depth = 0;; depth++) {
+    // ---- bounce() on a volume hit of generation `depth` (shadeRays.cu:608-878)
+    Random2 random(ray.rngSeed, (uint64_t)floatBits(ray.tMax));
+    const vec3f P = ray.P;
+    const vec3f wo = -normalize(ray.dir);
+    const float offsetEpsilon = fmax_(1e-4f, 1e-6f * reduce_max(vabs(P)));  // safe_eps
+    // bsdf at the collision (Phase.h): SimplePhase(0.7) or HGPhase
+    vec3f albedo;
+    if (s.phaseMode == 0) albedo = .7f * ray.hitColor;
+    else albedo = s.scatteringAlbedo * ray.hitColor;
+    // shadow ray (:640-746)
+    Ray shadow;
+    vec3f shadowTp = V(0.f);
+    float shadowMis = 1.f;
+    bool haveShadow = false;
+    LightSample ls;
+    bool lightNeedsMIS = false, lightIsDirLight = false;
+    if (sampleLights(sc, ls, random, lightNeedsMIS, lightIsDirLight)) {
+      float fpdf;
+      if (s.phaseMode == 0) fpdf = ONE_OVER_FOUR_PI;
+      else fpdf = hgPhase(s.anisotropy, dot(normalize(-wo), normalize(ls.direction)));
+      vec3f fval = fpdf * albedo;
+      if ((fpdf > 0.f) && !(reduce_max(fval) < 1e-4f)) {
+        fval = vmin(fval, V(13.f));
+        const vec3f incomingThroughput = tp;
+        vec3f tp_sr = incomingThroughput * (std::isinf(ls.pdf) ? 1.f : (1.f / ls.pdf)) * fval * ls.radiance * 1.f;
+        shadow.org = P + offsetEpsilon * wo;
+        shadow.dir = ls.direction;
+        shadow.tMax = ls.distance * (1.f - 2.f * offsetEpsilon);
+        shadowTp = halfRound(tp_sr);
+        shadow.rngSeed = ray.rngSeed;
+        ray.rngSeed.nextHashed((uint64_t)floatBits(ray.tMax));
+        haveShadow = true;
+        if (!lightIsDirLight && lightNeedsMIS) {
+          float pdf_light = ONE_OVER_FOUR_PI;  // EnvMap.h:142-151, no texture
+          float pdf_scatter;
+          if (s.phaseMode == 0) pdf_scatter = ONE_OVER_FOUR_PI;
+          else pdf_scatter = hgPhase(s.anisotropy, dot(normalize(-wo), normalize(ls.direction)));
+          shadowMis = pdf_light / (pdf_light + pdf_scatter + 1e-10f);
+          if (shadowMis < 1e-5f) haveShadow = false;
+        }
+        if (!(shadow.tMax > 0.f)) haveShadow = false;
+      }
+    }
+    // scattered ray (:749-878), multi-scatter build: HGPhase::scatter, then
+    // the volume-bounce budget.  A sample with pdf <= 1e-6 would end the path
+    // here (the reference re-traces the old ray); with anisotropy clamped to
+    // [-0.99, 0.99] (Volume.cpp:55-57) the HG pdf stays above 2e-4.
+    bool haveScatter = false;
+    if (s.phaseMode == 1 && s.maxVolumeBounces > 0 && depth < MAX_PATH_DEPTH) {
+      const vec3f wi_in = normalize(-wo);
+      const vec3f sdir = hgSampleDirection(wi_in, s.anisotropy, random);
+      const float pdf = hgPhase(s.anisotropy, dot(wi_in, sdir));
+      const vec3f f_r = albedo * pdf;
+      if (pdf > 0.f && !(pdf <= 1e-6f) && numVolumeBounces < s.maxVolumeBounces) {
+        numVolumeBounces++;
+        ray.org = P + (1.f * offsetEpsilon) * wo;
+        ray.dir = normalize(sdir);
+        const float denom = std::isinf(pdf) ? 1.f : (pdf + 1e-10f);
+        vec3f scatterFactor = V((f_r.x * 1.f) / denom, (f_r.y * 1.f) / denom, (f_r.z * 1.f) / denom);
+        scatterFactor = vmin(scatterFactor, V(2.5f));
+        tp = halfRound(tp * scatterFactor);
+        if (lightNeedsMIS && !std::isinf(pdf)) {
+          const float ps = hgPhase(s.anisotropy, dot(normalize(-wo), normalize(ray.dir)));
+          const float pl = ONE_OVER_FOUR_PI;
+          pathMis = ps / (ps + pl);
+        } else {
+          pathMis = 1.f;
+        }
+        ray.tMax = INF;
+        ray.hadHit = false;
+        haveScatter = true;
+      }
+    }
+    // ---- generation depth+1: the shadow ray, then the scattered ray
+    if (haveShadow) {
+      traceRay(sc, shadow, st);
+      out.add(shadow.hadHit ? V(0.f) : (shadowMis * shadowTp));
+    }
+    if (!haveScatter) return out;
+    traceRay(sc, ray, st);
+    if (!ray.hadHit) {  // secondary ray into the environment (:529-557)
+      out.add(tp * V(s.ambientRadiance) * pathMis);
+      return out;
+    }
+    // a secondary volume hit: no emission without principled volumes
   }
-  vec3f fval = fpdf * albedo;
-  if (!(fpdf > 0.f) || reduce_max(fval) < 1e-4f) return out;
-  fval = vmin(fval, V(13.f));
-  const vec3f incomingThroughput = V(1.f);
-  vec3f tp_sr = incomingThroughput * (std::isinf(ls.pdf) ? 1.f : (1.f / ls.pdf)) * fval * ls.radiance * 1.f;
-  Ray shadow;
-  shadow.org = P + offsetEpsilon * wo;
-  shadow.dir = ls.direction;
-  shadow.tMax = ls.distance * (1.f - 2.f * offsetEpsilon);
-  vec3f shadowTp = halfRound(tp_sr);  // PathState::throughput is vec3h
-  shadow.rngSeed = ray.rngSeed;
-  float misWeight = 1.f;
-  if (!lightIsDirLight && lightNeedsMIS) {
-    float pdf_light = ONE_OVER_FOUR_PI;  // EnvMap.h:142-151, no texture
-    float pdf_scatter;
-    if (s.phaseMode == 0) pdf_scatter = ONE_OVER_FOUR_PI;
-    else pdf_scatter = hgPhase(s.anisotropy, dot(normalize(-wo), normalize(ls.direction)));
-    misWeight = pdf_light / (pdf_light + pdf_scatter + 1e-10f);
-    if (misWeight < 1e-5f) return out;
-  }
-  if (!(shadow.tMax > 0.f)) return out;
-  // ---- generation 1: trace the shadow ray, bounce() on it
-  traceRay(sc, shadow, st);
-  out.hasShadow = true;
-  out.frag1 = shadow.hadHit ? V(0.f) : (misWeight * shadowTp);
-  return out;
 }
 
 // Neumaier-compensated sum (precision forms): sum += x, error kept in c.
@@ -711,8 +834,8 @@ static inline void accumulate(vec4f &acc, vec4f &comp, const PixelSample &ps, in
     if (f0.y > 0.f) addTo(acc.y, comp.y, f0.y, compensated);
     if (f0.z > 0.f) addTo(acc.z, comp.z, f0.z, compensated);
   }
-  if (ps.hasShadow) {
-    vec3f f1 = vmin(ps.frag1, V(clampMax));
+  for (int i = 0; i < ps.n; i++) {
+    vec3f f1 = vmin(ps.frags[i], V(clampMax));
     if (f1.x > 0.f) addTo(acc.x, comp.x, f1.x, compensated);
     if (f1.y > 0.f) addTo(acc.y, comp.y, f1.y, compensated);
     if (f1.z > 0.f) addTo(acc.z, comp.z, f1.z, compensated);
@@ -745,6 +868,20 @@ void orc_rng_derived(uint64_t parentState, uint64_t h, int n, uint32_t *out, uin
 uint64_t orc_hash3(uint32_t a, uint32_t b, uint32_t c) { return hash3(a, b, c); }
 float orc_fastlog(float f) { return fastLog(f); }
 uint16_t orc_f2h(float f) { return f2h(f); }
+void orc_logp(int n, const float *x, float *out) {
+  for (int i = 0; i < n; i++) out[i] = logPortable(x[i]);
+}
+void orc_sincos(int n, const float *x, float *sn, float *cs) {
+  for (int i = 0; i < n; i++) sincosPortable(x[i], sn[i], cs[i]);
+}
+void orc_hg_sample(const float *wi, float g, uint64_t seedState, int n, float *outDirs) {
+  Random2 rng(1u, 1u);
+  rng.state = seedState;
+  for (int i = 0; i < n; i++) {
+    vec3f d = hgSampleDirection(V(wi[0], wi[1], wi[2]), g, rng);
+    outDirs[3 * i] = d.x; outDirs[3 * i + 1] = d.y; outDirs[3 * i + 2] = d.z;
+  }
+}
 float orc_h2f(uint16_t h) { return h2f(h); }
 
 void orc_mc_dims(const OrcScene *s, int *out3) {

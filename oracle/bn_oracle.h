@@ -29,6 +29,7 @@ typedef struct {
   int exactLog;           // 1: -logf instead of fastLog (extension)
   int majorantRoundUp;    // 1: majorant bumped one ulp up (precision forms)
   int compensatedAccum;   // 1: Neumaier-compensated accumulation across waves (precision forms)
+  int maxVolumeBounces;   // with phaseMode 1: up to this many volume bounces (multi-scatter build)
   int width, height;
 } OrcScene;
 }

@@ -48,6 +48,7 @@ SCENES = {
     "noise_f16": lambda: small_noise_scene(dtype="f16"),
     "noise_bf16": lambda: small_noise_scene(dtype="bf16"),
     "noise_u16": lambda: small_noise_scene(dtype="u16"),
+    "noise_exact_log": lambda: small_noise_scene(exact_log=True),
     "two_lights_aniso": lambda: small_noise_scene(
         dir_lights=[{"direction": (-1, -1, -1), "radiance": 1.0},
                     {"direction": (0.3, -1, 0.2), "radiance": 2.0, "color": (1.0, 0.5, 0.25)}],
@@ -123,7 +124,11 @@ def test_invalid_calls_record_errors():
     L.bnSet1i(r.renderer, b"bnx.hgPhase", 1)
     L.bnCommit(r.renderer)
     L.bnRender(r.renderer, r.model, r.camera, r.fb)
-    assert L.bnGetLastError() == 3  # unsupported: multiple scattering
+    assert L.bnGetLastError() == 0  # multiple scattering renders
+    L.bnSet1f(r.camera, b"apertureRadius", 0.1)
+    L.bnCommit(r.camera)
+    L.bnRender(r.renderer, r.model, r.camera, r.fb)
+    assert L.bnGetLastError() == 3  # unsupported: depth of field
     L.bnClearLastError()
     L.bnxSetLaunchConfig(r.ctx, 1, 256)  # beyond the kernel's launch bounds
     assert L.bnGetLastError() == 2

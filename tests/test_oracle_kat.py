@@ -267,3 +267,80 @@ def test_u16_texels_divide_by_65535():
     sc2 = _tiny_scene(np.full((2, 2, 2), 40000, np.uint16), dtype="u16")
     s2, _ = oracle.sample_points(sc2, np.array([[0.0, 0.0, 0.0]], np.float32))
     assert s2[0] == f32(40000) / f32(65535)
+
+
+def test_portable_sincos_matches_float64_within_two_ulp():
+    # one binary32 sin/cos shared by the oracle and the kernels (the HG
+    # sampler's azimuth runs over [0, 2pi])
+    x = np.linspace(0, 2 * np.pi, 100001, dtype=np.float32)
+    sn, cs = oracle.sincos(x)
+    x64 = x.astype(np.float64)
+    assert np.abs(sn - np.sin(x64)).max() < 2.4e-7
+    assert np.abs(cs - np.cos(x64)).max() < 2.4e-7
+    big = np.abs(np.sin(x64)) > 0.25
+    assert (np.abs(sn[big] - np.sin(x64[big])) <= 2 * np.spacing(np.abs(sn[big]))).all()
+    # quadrant boundaries reduce to exact values
+    s0, c0 = oracle.sincos(np.array([0.0], np.float32))
+    assert s0[0] == 0.0 and c0[0] == 1.0
+
+
+@pytest.mark.parametrize("g", [0.0, 0.6, -0.5, 0.9])
+def test_hg_direction_sampler_has_mean_cosine_g(g):
+    # Phase.h:76-101: the mean cosine of Henyey-Greenstein is g
+    d = oracle.hg_sample([0.0, 0.0, 1.0], g, 0x1234567, 100000)
+    assert np.abs(np.linalg.norm(d, axis=1) - 1).max() < 3e-7
+    assert abs(d[:, 2].mean() - g) < 0.01
+    # the sampler is symmetric about the incoming direction
+    assert abs(d[:, 0].mean()) < 0.01 and abs(d[:, 1].mean()) < 0.01
+
+
+def test_multi_scatter_adds_energy_and_rays():
+    from tests.helpers import small_noise_scene
+    d = small_noise_scene(w=24, h=16, phase="hg", anisotropy=0.6)
+    means, rays = [], []
+    for mvb in (0, 1, 4):
+        sc = oracle.Scene(dict(d, max_volume_bounces=mvb))
+        acc = np.zeros((16, 24, 4), np.float32)
+        _, _, st = oracle.render(sc, 0, 32, accum=acc)
+        means.append(float(oracle.resolve(acc, 32)[..., :3].mean()))
+        rays.append(st["rays"])
+    assert means[0] < means[1] < means[2]
+    assert rays[0] < rays[1] < rays[2]
+    with pytest.raises(ValueError):
+        oracle.render_expected_fp64(oracle.Scene(dict(d, max_volume_bounces=1)))
+    # the default build (SimplePhase) ignores maxVolumeBounces, as the reference's does
+    simple = small_noise_scene(w=24, h=16, phase="simple")
+    imgs = []
+    for mvb in (0, 3):
+        acc = np.zeros((16, 24, 4), np.float32)
+        oracle.render(oracle.Scene(dict(simple, max_volume_bounces=mvb)), 0, 4, accum=acc)
+        imgs.append(acc)
+    assert np.array_equal(imgs[0], imgs[1])
+
+
+def test_path_depth_cap_binds_before_the_bounce_budget():
+    # MAX_PATH_DEPTH = 10 (shadeRays.cu:31): a hit of generation 10 does not
+    # scatter, so budgets of 10 and 14 bounces give the same sums, 9 does not
+    from tests.helpers import small_noise_scene
+    accs = {}
+    for mvb in (9, 10, 14):
+        d = small_noise_scene(phase="hg", anisotropy=0.3, max_volume_bounces=mvb)
+        acc = np.zeros((d["height"], d["width"], 4), np.float32)
+        oracle.render(oracle.Scene(d), 0, 8, accum=acc)
+        accs[mvb] = acc
+    assert np.array_equal(accs[10], accs[14])
+    assert not np.array_equal(accs[9], accs[10])
+
+
+def test_portable_log_within_two_ulp_on_free_flight_inputs():
+    # bnx.exactLog draws dt = -log(1 - r) / majorant, r a multiple of 2^-24 in [0, 1)
+    r = np.arange(0, 2 ** 24, 37, dtype=np.float64) * 2.0 ** -24
+    x = (1.0 - r).astype(np.float32)
+    v = oracle.logp(x).astype(np.float64)
+    t = np.log(x.astype(np.float64))
+    ulp = np.spacing(np.abs(t).astype(np.float32)).astype(np.float64)
+    nz = t != 0
+    assert (np.abs(v - t)[nz] <= 2 * ulp[nz]).all()
+    assert oracle.logp(np.array([1.0], np.float32))[0] == 0.0
+    p2 = np.float32(2.0) ** -np.arange(1, 24, dtype=np.float32)
+    assert np.allclose(oracle.logp(p2), np.log(p2.astype(np.float64)), rtol=2 ** -23, atol=0)
