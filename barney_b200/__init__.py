@@ -295,6 +295,24 @@ class VolumeRenderer:
         L.bnSet1f(self.vol, b"scatteringAlbedo", desc.get("scattering_albedo", 0.9))
         if desc.get("majorant_round_up"):
             L.bnSet1i(self.vol, b"bnx.majorantRoundUp", 1)
+        pv = desc.get("principled")
+        if pv:  # principled volume coefficients (Volume.cpp:36-126 parameter names)
+            L.bnSet1i(self.vol, b"principledVolume", 1 if pv.get("enabled", True) else 0)
+            for key, name in (("density", b"principledDensity"), ("density_threshold", b"principledDensityThreshold"),
+                              ("density_scale", b"principledDensityScale"),
+                              ("emission_strength", b"principledEmissionStrength"),
+                              ("blackbody_intensity", b"principledBlackbodyIntensity"),
+                              ("temperature", b"principledTemperature")):
+                if key in pv:
+                    L.bnSet1f(self.vol, name, float(pv[key]))
+            if "value_range" in pv:
+                L.bnSet2f(self.vol, b"principledValueRange", *map(float, pv["value_range"]))
+            for key, name in (("scatter_color", b"principledScatterColor"),
+                              ("absorption_color", b"principledAbsorptionColor"),
+                              ("emission_color", b"principledEmissionColor"),
+                              ("blackbody_tint", b"principledBlackbodyTint")):
+                if key in pv:
+                    L.bnSet3f(self.vol, name, *map(float, pv[key]))
         L.bnCommit(self.vol)
         check()
         vols = (ctypes.c_void_p * 1)(self.vol)

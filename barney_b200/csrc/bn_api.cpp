@@ -61,6 +61,7 @@ VolumeDD Volume::dd() const {
   v.phase = PHASE_SIMPLE;
   v.anisotropy = anisotropy;
   v.scatteringAlbedo = scatteringAlbedo;
+  v.pv = pv;
   return v;
 }
 
@@ -266,13 +267,13 @@ void renderBatch(Context *ctx, const std::vector<BatchEntry> &entries) {
   std::vector<const void *> key;
   long long chunks = 0;
   unsigned long long pixelSamples = 0;
-  bool multiScatter = false;
+  bool extended = false;  // multi-scatter or principled: the extended kernel
   ctx->hostChunks[0] = 0;
   for (int i = 0; i < n; i++) {
     const BatchEntry &e = entries[i];
     JobDD job = buildJob(ctx, *e.r, *e.m, *e.c, *e.fb);
     if (job.fr.spp <= 0) throw Error(E_INVALID_ARG, "every batch job needs pathsPerPixel >= 1");
-    multiScatter = multiScatter || job.fr.maxVolumeBounces > 0;
+    extended = extended || job.fr.maxVolumeBounces > 0 || job.v.pv.enabled;
     ctx->hostJobs[i] = job;
     chunks += ((long long)job.fr.width * job.fr.height + 31) / 32;
     if (chunks > 0x7fffffffLL) throw Error(E_INVALID_ARG, "batch too large");
@@ -286,7 +287,7 @@ void renderBatch(Context *ctx, const std::vector<BatchEntry> &entries) {
   key.push_back((const void *)(intptr_t)(ctx->blocksPerSM * 4096 + ctx->threadsPerBlock));
   key.push_back((const void *)(intptr_t)ctx->sched.serviceBatch);
   key.push_back((const void *)(intptr_t)n);
-  key.push_back((const void *)(intptr_t)(multiScatter ? 1 : 0));
+  key.push_back((const void *)(intptr_t)(extended ? 1 : 0));
   auto enqueue = [&](cudaStream_t s, bool timed) {
     ck(cudaMemcpyAsync(ctx->batchJobs.ptr, ctx->hostJobs, n * sizeof(JobDD), cudaMemcpyHostToDevice, s), "job table");
     ck(cudaMemcpyAsync(ctx->batchChunks.ptr, ctx->hostChunks, (n + 1) * sizeof(int), cudaMemcpyHostToDevice, s),
@@ -294,7 +295,7 @@ void renderBatch(Context *ctx, const std::vector<BatchEntry> &entries) {
     ck(cudaMemsetAsync(ctx->dCounters, 0, sizeof(LaunchCounters), s), "counter reset");
     if (timed) ck(cudaEventRecord(ctx->ev[0], s), "event");
     ck(launchRenderBatch((const JobDD *)ctx->batchJobs.ptr, (const int *)ctx->batchChunks.ptr, n, ctx->dCounters,
-                         ctx->blocksPerSM, ctx->threadsPerBlock, s, ctx->sched, multiScatter),
+                         ctx->blocksPerSM, ctx->threadsPerBlock, s, ctx->sched, extended),
        "batch render kernel");
     if (timed) ck(cudaEventRecord(ctx->ev[1], s), "event");
     ck(launchResolveBatch((const JobDD *)ctx->batchJobs.ptr, (const int *)ctx->batchChunks.ptr, n, (int)chunks, s),

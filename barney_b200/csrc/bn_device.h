@@ -18,6 +18,15 @@ constexpr int kCellsPerMC = 8;  // StructuredData.cu:26
 constexpr int kRenderMaxThreads = 128;  // __launch_bounds__ of the render kernel:
 constexpr int kRenderMinBlocks = 5;     // 5 x 128 threads per SM (at most 102 registers)
 
+// Principled volume coefficients evaluated from the field value
+// (PrincipledVolumeParams::DD, PrincipledVolume.h:33-46).
+struct PrincipledDD {
+  int enabled;
+  float density, densityThreshold, densityScale, valueLo, valueHi;
+  float emissionStrength, blackbodyIntensity, temperature;
+  float3 scatterColor, absorptionColor, emissionColor, blackbodyTint;
+};
+
 // Structured field + macrocell majorant grid + transfer function
 // (MCVolumeAccel::DD, MCAccelerator.h:23-27).
 struct VolumeDD {
@@ -40,6 +49,7 @@ struct VolumeDD {
   int phase;            // PhaseMode
   float anisotropy;
   float scatteringAlbedo;
+  PrincipledDD pv;
 };
 
 struct DirLightDD {
@@ -101,10 +111,11 @@ cudaError_t launchRender(const VolumeDD &vol, const FrameDD &frame, LaunchCounte
                          int threadsPerBlock, cudaStream_t s, const SchedDD &sd = SchedDD());
 // jobs / chunkStart: device arrays; chunkStart has numJobs+1 entries, the
 // prefix sum of each job's ceil(width*height/32) pixel chunks.
-// multiScatter: some job has fr.maxVolumeBounces > 0 (selects the kernel that can continue paths)
+// extended: some job has fr.maxVolumeBounces > 0 or a principled volume
+// (selects the kernel instantiation that implements them)
 cudaError_t launchRenderBatch(const JobDD *jobs, const int *chunkStart, int numJobs, LaunchCounters *counters,
                               int blocksPerSM, int threadsPerBlock, cudaStream_t s, const SchedDD &sd = SchedDD(),
-                              bool multiScatter = false);
+                              bool extended = false);
 cudaError_t launchResolve(const float4 *accum, int numPixels, int accumID, int fmt, void *out, cudaStream_t s,
                           const float4 *comp = nullptr);
 // resolves every job of a batch table into its fr.color after its waves

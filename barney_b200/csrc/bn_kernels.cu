@@ -85,6 +85,44 @@ DEV float fastLog(float f) {
   return s + s;
 }
 
+// Natural logarithm of a normal binary32 x > 0, for the exact-log free-flight
+// step (bnx.exactLog).  logf differs in its last bits between CUDA and host
+// libm, so the oracle and the CUDA kernels share this one evaluation:
+// x = m 2^e with m in [sqrt(1/2), sqrt(2)), log m = 2 atanh(s) with
+// s = (m-1)/(m+1) (|s| <= 0.1716) as an odd series to s^11, plus e ln2 with
+// ln2 split as 0.693145751953125 (16 significant bits, so e times it is
+// exact) + 1.42860682e-6.  Within 1.7 ulp of log over (0, 1].
+DEV float logPortable(float x) {
+  const uint32_t b = __float_as_uint(x);
+  int e = (int)((b >> 23) & 0xffu) - 127;
+  float m = __uint_as_float((b & 0x7fffffu) | 0x3f800000u);
+  if (m > 1.41421356f) {
+    m = m * 0.5f;
+    e += 1;
+  }
+  const float s = (m - 1.f) / (m + 1.f);
+  const float z = s * s;
+  const float p = 0.666666667f + z * (0.4f + z * (0.285714286f + z * (0.222222222f + z * 0.181818182f)));
+  const float lm = 2.f * s + s * (z * p);
+  const float fe = (float)e;
+  return fe * 0.693145751953125f + (fe * 1.42860682e-6f + lm);
+}
+
+// e^x for |x| < 87 (the blackbody colour's powf), shared with the oracle like
+// logPortable: k = rint(x / ln2), r = x - k ln2 (split ln2, |r| <= 0.347),
+// e^r as the Taylor series to r^8 (truncation below 3e-9), times 2^k by
+// exponent arithmetic.
+DEV float expPortable(float x) {
+  const float k = rintf(x * 1.44269504f);
+  const float r = (x - k * 0.693145751953125f) - k * 1.42860682e-6f;
+  const float p = 1.f + r * (1.f + r * (0.5f + r * (1.66666667e-1f + r * (4.16666667e-2f + r * (8.33333333e-3f +
+                  r * (1.38888889e-3f + r * (1.98412698e-4f + r * 2.48015873e-5f)))))));
+  return p * __uint_as_float((uint32_t)((int)k + 127) << 23);
+}
+// x^y for x > 0 (PrincipledVolume.h's powf), as e^(y log x)
+DEV float powPortable(float x, float y) { return expPortable(y * logPortable(x)); }
+
+
 DEV float fmin_(float a, float b) { return fminf(a, b); }
 DEV float fmax_(float a, float b) { return fmaxf(a, b); }
 DEV float3 f3(float x, float y, float z) { return make_float3(x, y, z); }
@@ -185,6 +223,76 @@ DEV float tfMajorant(const VolumeDD &v, float lo, float hi) {
   return m * v.baseDensity;
 }
 
+// ---- principled volumes (PrincipledVolume.h:55-175) ----
+DEV float clampF(float f, float lo, float hi) { return fmin_(hi, fmax_(lo, f)); }  // math.h:127
+DEV float rmax3(float3 a) { return fmax_(fmax_(a.x, a.y), a.z); }
+DEV float principledDensityFactor(const PrincipledDD &p, float scalar) {
+  const float x = clampF(scalar, p.valueLo, p.valueHi);
+  if (p.densityThreshold > 0.f && x < p.densityThreshold) return 0.f;
+  return p.density * fmax_(x, 0.f) * p.densityScale;
+}
+DEV float3 principledSigma(float d, float3 color) { return f3(d * color.x, d * color.y, d * color.z); }
+DEV float principledSigmaT(const PrincipledDD &p, float scalar) {
+  const float d = principledDensityFactor(p, scalar);
+  const float3 s = principledSigma(d, p.scatterColor), a = principledSigma(d, p.absorptionColor);
+  return rmax3(f3(s.x + a.x, s.y + a.y, s.z + a.z));
+}
+// principledSampleMap's tint (its w is principledSigmaT), times rgb; not
+// inlined, so that the Woodcock loop keeps its registers
+__device__ __noinline__ float3 principledTintTimes(const PrincipledDD &p, float scalar, float3 rgb) {
+  const float d = principledDensityFactor(p, scalar);
+  const float3 s = principledSigma(d, p.scatterColor), a = principledSigma(d, p.absorptionColor);
+  float3 tint = f3(1.f, 1.f, 1.f);
+  if (rmax3(f3(s.x + a.x, s.y + a.y, s.z + a.z)) > 0.f) {
+    const float ms = rmax3(s);
+    if (ms > 0.f) tint = f3(s.x / ms, s.y / ms, s.z / ms);
+  }
+  return f3(tint.x * rgb.x, tint.y * rgb.y, tint.z * rgb.z);
+}
+DEV float3 principledBlackbodyColor(float kelvin) {
+  kelvin = clampF(kelvin, 1000.f, 40000.f);
+  const float t = kelvin / 100.f;
+  float r, g, b;
+  if (t <= 66.f) {
+    r = 1.f;
+    g = clampF(0.390081578f * logPortable(t) - 0.631841444f, 0.f, 1.f);
+  } else {
+    r = clampF(1.292936186f * powPortable(t - 60.f, -0.1332047592f), 0.f, 1.f);
+    g = clampF(1.129890860f * powPortable(t - 60.f, -0.0755148492f), 0.f, 1.f);
+  }
+  if (t >= 66.f) b = 1.f;
+  else if (t <= 19.f) b = 0.f;
+  else b = clampF(0.543206789f * logPortable(t - 10.f) - 1.196254089f, 0.f, 1.f);
+  return f3(r, g, b);
+}
+DEV float3 principledEmission(const PrincipledDD &p, float scalar) {
+  const float d = principledDensityFactor(p, scalar);
+  float3 Le = f3(p.emissionStrength * p.emissionColor.x * d, p.emissionStrength * p.emissionColor.y * d,
+                 p.emissionStrength * p.emissionColor.z * d);
+  if (p.blackbodyIntensity > 0.f && p.temperature > 0.f) {
+    const float3 bb = principledBlackbodyColor(p.temperature);
+    Le = f3(Le.x + p.blackbodyIntensity * p.blackbodyTint.x * bb.x * d,
+            Le.y + p.blackbodyIntensity * p.blackbodyTint.y * bb.y * d,
+            Le.z + p.blackbodyIntensity * p.blackbodyTint.z * bb.z * d);
+  }
+  return Le;
+}
+// sampled, not a guaranteed bound, as in the reference
+DEV float principledMajorant(const PrincipledDD &p, float lo, float hi) {
+  if (lo > hi) return 0.f;
+  float m = 0.f;
+  for (int i = 0; i <= 8; ++i) {
+    const float t = float(i) / float(8);
+    m = fmax_(m, principledSigmaT(p, lo + t * (hi - lo)));
+  }
+  return m;
+}
+// mapMCs (MCGrid.cu:97-113)
+DEV float mapMajorant(const VolumeDD &v, float lo, float hi) {
+  const float tfMaj = tfMajorant(v, lo, hi);
+  return v.pv.enabled ? principledMajorant(v.pv, lo, hi) * tfMaj : tfMaj;
+}
+
 DEV float roundUpMajorant(float m, int roundUp) {
   return (roundUp && m > 0.f) ? __int_as_float(__float_as_int(m) + 1) : m;
 }
@@ -215,7 +323,7 @@ __global__ void __launch_bounds__(128) mcBuildKernel(VolumeDD v, float2 *ranges,
         }
       }
     ranges[tid] = make_float2(lo, hi);
-    majorants[tid] = roundUpMajorant(tfMajorant(v, lo, hi), roundUp);
+    majorants[tid] = roundUpMajorant(mapMajorant(v, lo, hi), roundUp);
   }
 }
 
@@ -223,7 +331,7 @@ __global__ void mcMapKernel(VolumeDD v, const float2 *ranges, float *majorants, 
   const int64_t n = (int64_t)v.mcDims.x * v.mcDims.y * v.mcDims.z;
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
     float2 r = ranges[i];
-    majorants[i] = roundUpMajorant(tfMajorant(v, r.x, r.y), roundUp);
+    majorants[i] = roundUpMajorant(mapMajorant(v, r.x, r.y), roundUp);
   }
 }
 
@@ -346,29 +454,6 @@ DEV float hgPhase(float g, float cosTheta) {
   float g2 = g * g;
   float denom = 1.f + g2 - 2.f * g * cosTheta;
   return kOneOverFourPi * (1.f - g2) / (denom * sqrtf(denom));
-}
-
-// Natural logarithm of a normal binary32 x > 0, for the exact-log free-flight
-// step (bnx.exactLog).  logf differs in its last bits between CUDA and host
-// libm, so the oracle and the CUDA kernels share this one evaluation:
-// x = m 2^e with m in [sqrt(1/2), sqrt(2)), log m = 2 atanh(s) with
-// s = (m-1)/(m+1) (|s| <= 0.1716) as an odd series to s^11, plus e ln2 with
-// ln2 split as 0.693145751953125 (16 significant bits, so e times it is
-// exact) + 1.42860682e-6.  Within 1.7 ulp of log over (0, 1].
-DEV float logPortable(float x) {
-  const uint32_t b = __float_as_uint(x);
-  int e = (int)((b >> 23) & 0xffu) - 127;
-  float m = __uint_as_float((b & 0x7fffffu) | 0x3f800000u);
-  if (m > 1.41421356f) {
-    m = m * 0.5f;
-    e += 1;
-  }
-  const float s = (m - 1.f) / (m + 1.f);
-  const float z = s * s;
-  const float p = 0.666666667f + z * (0.4f + z * (0.285714286f + z * (0.222222222f + z * 0.181818182f)));
-  const float lm = 2.f * s + s * (z * p);
-  const float fe = (float)e;
-  return fe * 0.693145751953125f + (fe * 1.42860682e-6f + lm);
 }
 
 // sin and cos of x in [0, 2pi] (the HG sampler's azimuth).  The reference
@@ -530,10 +615,47 @@ constexpr int kChunk = 32;  // pixels a warp takes at a time (one 8x4 tile)
 // __grid_constant__ parameter, TF staged in shared memory) and the batch
 // kernel (a job table in global memory, chunks of all jobs in one counter).
 // LOG: 0 fastLog (Volume.h:154-164), 1 -logf (bnx.exactLog), 2 per job (batch)
+// A principled volume's hit in the multi-scatter build (MCAccelerator.h:621-659):
+// tint, scattering albedo and emission from the field value at P (sampled
+// again: it is the collision's value).  Not inlined, so that the render loop
+// keeps its registers when principled volumes are off.
+template <int T>
+__device__ __noinline__ void principledAtHit(const VolumeDD &v, float3 P, const float4 *tfTab, const float *u8lut,
+                                             float3 &tint, float &hitAlb, float3 &emission) {
+  const float scalar = sampleJob<T>(v, P, u8lut);
+  const float d = principledDensityFactor(v.pv, scalar);
+  float3 ss = principledSigma(d, v.pv.scatterColor), sa = principledSigma(d, v.pv.absorptionColor);
+  // the TF at the hit (TransferFunction::map)
+  const float span = v.domHi - v.domLo;
+  float tf = span == 1.f ? (scalar - v.domLo) : (scalar - v.domLo) / span;
+  tf = fmin_(1.f, fmax_(0.f, tf));
+  tf *= (float)(v.tfN - 1);
+  const int ti = min(v.tfN - 2, max(0, (int)tf));
+  tf -= (float)ti;
+  const float4 ta = tfTab[ti], tb = tfTab[ti + 1];
+  const float tw = ((1.f - tf) * ta.w + tf * tb.w) * v.baseDensity;
+  if (tw > 0.f) {
+    ss = f3(ss.x * tw, ss.y * tw, ss.z * tw);
+    sa = f3(sa.x * tw, sa.y * tw, sa.z * tw);
+    tint = f3(tint.x * ((1.f - tf) * ta.x + tf * tb.x), tint.y * ((1.f - tf) * ta.y + tf * tb.y),
+              tint.z * ((1.f - tf) * ta.z + tf * tb.z));
+  } else {
+    ss = f3(0.f, 0.f, 0.f);
+    sa = f3(0.f, 0.f, 0.f);
+  }
+  const float st = rmax3(f3(ss.x + sa.x, ss.y + sa.y, ss.z + sa.z));
+  if (st > 0.f) {
+    const float ms = rmax3(ss);
+    if (ms > 0.f) tint = f3(ss.x / ms, ss.y / ms, ss.z / ms);
+    hitAlb = rmax3(ss) / st;
+  }
+  emission = principledEmission(v.pv, scalar);
+}
+
 // shadeRays.cu:17-41 (MAX_PATH_DEPTH)
 constexpr int kMaxPathDepth = 10;
 
-template <int T, bool BATCH, int LOG, bool MS>
+template <int T, bool BATCH, int LOG, bool EXT>
 DEV void renderLoop(const JobDD *jobs, const int *chunkStart, int numJobs, int numChunks, const SchedDD &sd,
                     LaunchCounters *ctr, const float4 *sTF, const float *u8lut) {
   const unsigned FULL = 0xffffffffu;
@@ -561,7 +683,8 @@ DEV void renderLoop(const JobDD *jobs, const int *chunkStart, int numJobs, int n
   float misWeight = 0.f;
   bool shadowRay = false;
   unsigned steps = 0;
-  // MS (multi-scatter build): the path's throughput, rounded to binary16 like
+  // EXT (the instantiation for multi-scatter paths and principled volumes;
+  // the plain kernels compile neither): the path's throughput, rounded to binary16 like
   // PathState::throughput (Ray.h:17-23); the MIS weight of the path ray; its
   // generation; the volume bounces taken; and a scattered ray that waits
   // while its generation's shadow ray is traced (it starts where the shadow
@@ -590,9 +713,7 @@ DEV void renderLoop(const JobDD *jobs, const int *chunkStart, int numJobs, int n
         const bool cmp = fr.comp != nullptr;
         bool spawned = false;
         if (!shadowRay) {
-          // primary hit: generation-0 accumulation (fragment 0, alpha 1); a
-          // later generation's volume hit has fragment 0 and adds nothing
-          if (!MS || depth == 0) {
+          if (!EXT) {  // primary hit: generation-0 accumulation (fragment 0, alpha 1)
             if (accumID == 0) {
               acc = make_float4(0.f, 0.f, 0.f, 1.f);
               comp = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -602,6 +723,37 @@ DEV void renderLoop(const JobDD *jobs, const int *chunkStart, int numJobs, int n
           }
           const float tHit = ts.t;
           const float3 P = f3(ts.org.x + tHit * ts.dir.x, ts.org.y + tHit * ts.dir.y, ts.org.z + tHit * ts.dir.z);
+          // the multi-scatter build re-derives a principled volume's tint,
+          // albedo and emission from the field value at the hit
+          // (MCAccelerator.h:621-659); the field is sampled again at the same
+          // point instead of keeping the value in a register
+          float3 tint = hitRGB;
+          float hitAlb = v.scatteringAlbedo;
+          if (EXT) {
+            float3 frag = f3(0.f, 0.f, 0.f);
+            if (v.phase == PHASE_HG && v.pv.enabled && !fr.emissionAbsorption) {
+              float3 e;
+              principledAtHit<T>(v, P, BATCH ? v.tf : sTF, u8lut, tint, hitAlb, e);
+              // emission of the HGPhase hit: incomingThroughput * emission (shadeRays.cu:613-617)
+              if (rmax3(e) > 0.f) frag = f3(pathTp.x * e.x, pathTp.y * e.y, pathTp.z * e.z);
+            }
+            const float fx = fmin_(frag.x, clampMax), fy = fmin_(frag.y, clampMax), fz = fmin_(frag.z, clampMax);
+            if (depth == 0) {  // generation 0: the fragment and alpha 1
+              if (accumID == 0) {
+                acc = make_float4(fx, fy, fz, 1.f);
+                comp = make_float4(0.f, 0.f, 0.f, 0.f);
+              } else {
+                accAdd(acc.w, comp.w, 1.f, cmp);
+                if (fx > 0.f) accAdd(acc.x, comp.x, fx, cmp);
+                if (fy > 0.f) accAdd(acc.y, comp.y, fy, cmp);
+                if (fz > 0.f) accAdd(acc.z, comp.z, fz, cmp);
+              }
+            } else {  // a scattered ray's hit: its emission, if any
+              if (fx > 0.f) accAdd(acc.x, comp.x, fx, cmp);
+              if (fy > 0.f) accAdd(acc.y, comp.y, fy, cmp);
+              if (fz > 0.f) accAdd(acc.z, comp.z, fz, cmp);
+            }
+          }
           if (fr.emissionAbsorption) {
             const float ex = fmin_(hitRGB.x, clampMax), ey = fmin_(hitRGB.y, clampMax), ez = fmin_(hitRGB.z, clampMax);
             if (accumID == 0) acc = make_float4(ex, ey, ez, 1.f);
@@ -623,10 +775,11 @@ DEV void renderLoop(const JobDD *jobs, const int *chunkStart, int numJobs, int n
               float3 alb;
               float fpdf;
               if (v.phase == PHASE_SIMPLE) {
-                alb = f3(.7f * hitRGB.x, .7f * hitRGB.y, .7f * hitRGB.z);
+                alb = f3(.7f * tint.x, .7f * tint.y, .7f * tint.z);
                 fpdf = kOneOverFourPi;
               } else {
-                alb = f3(v.scatteringAlbedo * hitRGB.x, v.scatteringAlbedo * hitRGB.y, v.scatteringAlbedo * hitRGB.z);
+                const float a = EXT ? hitAlb : v.scatteringAlbedo;  // plain kernels read it here, not earlier
+                alb = f3(a * tint.x, a * tint.y, a * tint.z);
                 const float3 wi_in = normalize3(f3(-woN.x, -woN.y, -woN.z));
                 fpdf = hgPhase(v.anisotropy, dot3(wi_in, normalize3(ls.dir)));
               }
@@ -634,11 +787,11 @@ DEV void renderLoop(const JobDD *jobs, const int *chunkStart, int numJobs, int n
               if (fpdf > 0.f && !(fmax_(fmax_(fv.x, fv.y), fv.z) < 1e-4f)) {
                 fv = f3(fmin_(fv.x, 13.f), fmin_(fv.y, 13.f), fmin_(fv.z, 13.f));
                 const float ip = isinf(ls.pdf) ? 1.f : (1.f / ls.pdf);
-                const float3 tin = MS ? pathTp : f3(1.f, 1.f, 1.f);  // incomingThroughput
+                const float3 tin = EXT ? pathTp : f3(1.f, 1.f, 1.f);  // incomingThroughput
                 const float3 tp = f3(tin.x * ip * fv.x * ls.radiance.x * 1.f, tin.y * ip * fv.y * ls.radiance.y * 1.f,
                                      tin.z * ip * fv.z * ls.radiance.z * 1.f);
                 // shadowRay.rngSeed = ray.rngSeed; ray.rngSeed.next(tMax)
-                if (MS) scatSeed = (raySeed ^ ((uint64_t)__float_as_uint(tHit) << 1)) * kRngMul;
+                if (EXT) scatSeed = (raySeed ^ ((uint64_t)__float_as_uint(tHit) << 1)) * kRngMul;
                 misWeight = 1.f;
                 bool alive = true;
                 if (!isDir && needsMIS) {
@@ -670,12 +823,11 @@ DEV void renderLoop(const JobDD *jobs, const int *chunkStart, int numJobs, int n
             // end the path here (the reference re-traces the old ray); with
             // anisotropy clamped to [-0.99, 0.99] (Volume.cpp:55-57) the HG
             // pdf stays above 2e-4, so neither can happen.
-            if (MS && fr.maxVolumeBounces > 0 && depth < kMaxPathDepth) {
+            if (EXT && fr.maxVolumeBounces > 0 && depth < kMaxPathDepth) {
               const float3 wi_in = normalize3(f3(-woN.x, -woN.y, -woN.z));
               const float3 sdir = hgSampleDirection(wi_in, v.anisotropy, random);
               const float pdf = hgPhase(v.anisotropy, dot3(wi_in, sdir));
-              const float3 alb = f3(v.scatteringAlbedo * hitRGB.x, v.scatteringAlbedo * hitRGB.y,
-                                    v.scatteringAlbedo * hitRGB.z);
+              const float3 alb = f3(hitAlb * tint.x, hitAlb * tint.y, hitAlb * tint.z);
               const float3 f_r = f3(alb.x * pdf, alb.y * pdf, alb.z * pdf);
               if (pdf > 0.f && !(pdf <= 1e-6f) && nVolB < fr.maxVolumeBounces) {
                 nVolB++;
@@ -711,7 +863,7 @@ DEV void renderLoop(const JobDD *jobs, const int *chunkStart, int numJobs, int n
           }
         }
         if (!spawned) {
-          if (MS && pend) {  // the shadow ray was occluded: the scattered ray goes next
+          if (EXT && pend) {  // the shadow ray was occluded: the scattered ray goes next
             ts.dir = primDir;
             ts.rayTMax = kInf;
             raySeed = pendSeed;
@@ -738,7 +890,7 @@ DEV void renderLoop(const JobDD *jobs, const int *chunkStart, int numJobs, int n
         const int accumID = fr.accumID0 + k;
         const float clampMax = 10.f * (1 + accumID);
         const bool cmp = fr.comp != nullptr;
-        if (!shadowRay && (!MS || depth == 0)) {
+        if (!shadowRay && (!EXT || depth == 0)) {
           const float f0x = fmin_(bg.x, clampMax), f0y = fmin_(bg.y, clampMax), f0z = fmin_(bg.z, clampMax);
           if (accumID == 0) {
             acc = make_float4(f0x, f0y, f0z, bg.w);
@@ -764,7 +916,7 @@ DEV void renderLoop(const JobDD *jobs, const int *chunkStart, int numJobs, int n
           if (f1y > 0.f) accAdd(acc.y, comp.y, f1y, cmp);
           if (f1z > 0.f) accAdd(acc.z, comp.z, f1z, cmp);
         }
-        if (MS && shadowRay && pend) {  // the scattered ray goes next, from the shadow ray's origin
+        if (EXT && shadowRay && pend) {  // the scattered ray goes next, from the shadow ray's origin
           ts.dir = primDir;
           ts.rayTMax = kInf;
           raySeed = pendSeed;
@@ -883,7 +1035,7 @@ DEV void renderLoop(const JobDD *jobs, const int *chunkStart, int numJobs, int n
         }
         primDir = d;
         shadowRay = false;
-        if (MS) {
+        if (EXT) {
           pathTp = f3(1.f, 1.f, 1.f);
           pathMis = 1.f;
           depth = 0;
@@ -947,7 +1099,7 @@ DEV void renderLoop(const JobDD *jobs, const int *chunkStart, int numJobs, int n
             const float3 P = f3(ts.org.x + ts.t * ts.dir.x, ts.org.y + ts.t * ts.dir.y, ts.org.z + ts.t * ts.dir.z);
             const float s = sampleJob<T>(v, P, u8lut);
             nSamples++;
-            float w = 0.f, f = 0.f;
+            float w = 0.f, f = 0.f, tfw = 0.f;
             int idx = 0;
             if (!isnan(s)) {
               const float span = v.domHi - v.domLo;
@@ -959,13 +1111,18 @@ DEV void renderLoop(const JobDD *jobs, const int *chunkStart, int numJobs, int n
               const float w0 = BATCH ? __ldg(&v.tf[idx].w) : sTF[idx].w;
               const float w1 = BATCH ? __ldg(&v.tf[idx + 1].w) : sTF[idx + 1].w;
               w = ((1.f - f) * w0 + f * w1) * v.baseDensity;
+              if (EXT) {  // principled volume (Volume.h:66-72): density sigma_t times the TF's
+                tfw = w;
+                if (v.pv.enabled) w = tfw <= 0.f ? 0.f : principledSigmaT(v.pv, s) * tfw;
+              }
             }
             if (w >= rngFloat(ts.rng) * ts.maj) {
               hitRGB = f3(0.f, 0.f, 0.f);
-              if (!isnan(s)) {
+              if (!isnan(s) && !((EXT && v.pv.enabled) && tfw <= 0.f)) {
                 const float4 a = BATCH ? __ldg(&v.tf[idx]) : sTF[idx];
                 const float4 b = BATCH ? __ldg(&v.tf[idx + 1]) : sTF[idx + 1];
                 hitRGB = f3((1.f - f) * a.x + f * b.x, (1.f - f) * a.y + f * b.y, (1.f - f) * a.z + f * b.z);
+                if ((EXT && v.pv.enabled)) hitRGB = principledTintTimes(v.pv, s, hitRGB);
               }
               phase = LP_HIT;
             }
@@ -999,7 +1156,7 @@ DEV void renderLoop(const JobDD *jobs, const int *chunkStart, int numJobs, int n
   }
 }
 
-template <int T, int LOG, bool MS>
+template <int T, int LOG, bool EXT>
 __global__ void __launch_bounds__(kRenderMaxThreads, kRenderMinBlocks)
     renderKernel(const __grid_constant__ JobDD job, const __grid_constant__ SchedDD sd, LaunchCounters *ctr) {
   extern __shared__ float4 sTF[];
@@ -1008,17 +1165,17 @@ __global__ void __launch_bounds__(kRenderMaxThreads, kRenderMinBlocks)
   for (int i = threadIdx.x; i < 256; i += blockDim.x) u8lut[i] = (float)i * 1.f / 255.f;
   __syncthreads();
   const int numChunks = (job.fr.width * job.fr.height + kChunk - 1) / kChunk;
-  renderLoop<T, false, LOG, MS>(&job, nullptr, 1, numChunks, sd, ctr, sTF, u8lut);
+  renderLoop<T, false, LOG, EXT>(&job, nullptr, 1, numChunks, sd, ctr, sTF, u8lut);
 }
 
-template <bool MS>
+template <bool EXT>
 __global__ void __launch_bounds__(kRenderMaxThreads, kRenderMinBlocks)
     renderBatchKernel(const JobDD *jobs, const int *chunkStart, int numJobs, const __grid_constant__ SchedDD sd,
                       LaunchCounters *ctr) {
   __shared__ float u8lut[256];
   for (int i = threadIdx.x; i < 256; i += blockDim.x) u8lut[i] = (float)i * 1.f / 255.f;
   __syncthreads();
-  renderLoop<-1, true, 2, MS>(jobs, chunkStart, numJobs, __ldg(chunkStart + numJobs), sd, ctr, nullptr, u8lut);
+  renderLoop<-1, true, 2, EXT>(jobs, chunkStart, numJobs, __ldg(chunkStart + numJobs), sd, ctr, nullptr, u8lut);
 }
 
 // ---------------------------------------------------------------------------
@@ -1149,8 +1306,9 @@ template <int T>
 static cudaError_t launchRenderT(const VolumeDD &v, const FrameDD &fr, const SchedDD &sd, LaunchCounters *ctr,
                                  int bps, int tpb, cudaStream_t s) {
   const size_t smem = (size_t)v.tfN * sizeof(float4);
-  auto kern = fr.maxVolumeBounces > 0 ? (fr.exactLog ? renderKernel<T, 1, true> : renderKernel<T, 0, true>)
-                                      : (fr.exactLog ? renderKernel<T, 1, false> : renderKernel<T, 0, false>);
+  const bool ext = fr.maxVolumeBounces > 0 || v.pv.enabled;
+  auto kern = ext ? (fr.exactLog ? renderKernel<T, 1, true> : renderKernel<T, 0, true>)
+                  : (fr.exactLog ? renderKernel<T, 1, false> : renderKernel<T, 0, false>);
   if (smem > 48 * 1024 &&
       cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
     return cudaGetLastError();
@@ -1179,9 +1337,9 @@ cudaError_t launchRender(const VolumeDD &v, const FrameDD &fr, LaunchCounters *c
 }
 
 cudaError_t launchRenderBatch(const JobDD *jobs, const int *chunkStart, int numJobs, LaunchCounters *ctr, int bps,
-                              int tpb, cudaStream_t s, const SchedDD &sd, bool multiScatter) {
+                              int tpb, cudaStream_t s, const SchedDD &sd, bool extended) {
   if (tpb <= 0) tpb = 128;
-  auto kern = multiScatter ? renderBatchKernel<true> : renderBatchKernel<false>;
+  auto kern = extended ? renderBatchKernel<true> : renderBatchKernel<false>;
   if (bps <= 0) {
     int occ = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, tpb, 0) != cudaSuccess)
@@ -1260,7 +1418,7 @@ __global__ void __launch_bounds__(128) mcMajorantScratchKernel(VolumeDD v, int r
           hi = fmax_(hi, f);
         }
       }
-    majorants[tid] = roundUpMajorant(tfMajorant(v, lo, hi), roundUp);
+    majorants[tid] = roundUpMajorant(mapMajorant(v, lo, hi), roundUp);
   }
 }
 

@@ -160,19 +160,41 @@ struct Volume : Object {
   float anisotropy = 0.6f;        // Volume.h:140
   float scatteringAlbedo = 0.9f;  // Volume.h:141
   int majorantRoundUp = 0;        // bnx.majorantRoundUp (precision forms)
+  // PrincipledVolumeParams defaults (PrincipledVolume.h:17-30)
+  PrincipledDD pv{0, 1.f, 0.f, 1.f, 0.f, 1.f, 0.f, 0.f, 0.f, {0.8f, 0.8f, 0.8f}, {0.f, 0.f, 0.f},
+                  {1.f, 1.f, 1.f}, {1.f, 1.f, 1.f}};
   bool needsMajorantRebuild = false;
   bool built = false;
   int mcDims[3] = {0, 0, 0};
   DeviceBuffer tfBuf, ranges, majorants, occupied;
   explicit Volume(Context *c) : Object(c, K_VOLUME) {}
-  bool set1i(const std::string &m, int v) override {
+  bool set1i(const std::string &m, int v) override {  // Volume.cpp:36-50
     if (m == "bnx.majorantRoundUp") { majorantRoundUp = v ? 1 : 0; needsMajorantRebuild = true; return true; }
+    if (m == "principledVolume") { pv.enabled = v ? 1 : 0; needsMajorantRebuild = true; return true; }
     if (m == "userID") return true;
     return false;
   }
-  bool set1f(const std::string &m, float v) override {  // Volume.cpp:53-63
+  bool set1f(const std::string &m, float v) override {  // Volume.cpp:53-91
     if (m == "anisotropy") { anisotropy = std::min(0.99f, std::max(-0.99f, v)); return true; }
     if (m == "scatteringAlbedo") { scatteringAlbedo = std::min(1.f, std::max(0.f, v)); return true; }
+    if (m == "principledDensity") { pv.density = v; needsMajorantRebuild = true; return true; }
+    if (m == "principledDensityThreshold") { pv.densityThreshold = std::max(v, 0.f); needsMajorantRebuild = true; return true; }
+    if (m == "principledDensityScale") { pv.densityScale = v > 0.f ? v : 1.f; needsMajorantRebuild = true; return true; }
+    if (m == "principledEmissionStrength") { pv.emissionStrength = std::max(v, 0.f); return true; }
+    if (m == "principledBlackbodyIntensity") { pv.blackbodyIntensity = std::max(v, 0.f); return true; }
+    if (m == "principledTemperature") { pv.temperature = std::max(v, 0.f); return true; }
+    return false;
+  }
+  bool set2f(const std::string &m, float x, float y) override {  // Volume.cpp:94-103
+    if (m == "principledValueRange") { pv.valueLo = x; pv.valueHi = y; needsMajorantRebuild = true; return true; }
+    return false;
+  }
+  bool set3f(const std::string &m, float x, float y, float z) override {  // Volume.cpp:105-126
+    const float3 c = make_float3(std::max(x, 0.f), std::max(y, 0.f), std::max(z, 0.f));
+    if (m == "principledScatterColor") { pv.scatterColor = c; needsMajorantRebuild = true; return true; }
+    if (m == "principledAbsorptionColor") { pv.absorptionColor = c; needsMajorantRebuild = true; return true; }
+    if (m == "principledEmissionColor") { pv.emissionColor = c; return true; }
+    if (m == "principledBlackbodyTint") { pv.blackbodyTint = c; return true; }
     return false;
   }
   VolumeDD dd() const;

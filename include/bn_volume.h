@@ -142,7 +142,14 @@ BN_API BNTextureData bnTextureData3DCreate(BNContext context, int whichSlot, BND
                                            int width, int height, int depth, const void *texels);
 /* replaces barney.cu:382 bnScalarFieldCreate; type must be "structured" */
 BN_API BNScalarField bnScalarFieldCreate(BNContext context, int whichSlot, const char *type);
-/* replaces barney.cu:457 bnVolumeCreate */
+/* replaces barney.cu:457 bnVolumeCreate.  Parameters (Volume.cpp:36-126):
+   anisotropy (clamped to +-0.99), scatteringAlbedo, and the principled
+   volume set -- principledVolume (int), principledDensity,
+   principledDensityThreshold, principledDensityScale,
+   principledEmissionStrength, principledBlackbodyIntensity,
+   principledTemperature, principledValueRange (float2),
+   principledScatterColor, principledAbsorptionColor, principledEmissionColor,
+   principledBlackbodyTint (float3); extension bnx.majorantRoundUp. */
 BN_API BNVolume bnVolumeCreate(BNContext context, int whichSlot, BNScalarField sf);
 /* replaces barney.cu:442 bnVolumeSetXF (Volume::setXF, Volume.cpp:15-24) */
 BN_API void bnVolumeSetXF(BNVolume volume, bn_float2 domain, const bn_float4 *colorMap,

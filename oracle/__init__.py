@@ -51,6 +51,13 @@ class OrcScene(ctypes.Structure):
         ("majorantRoundUp", ctypes.c_int),
         ("compensatedAccum", ctypes.c_int),
         ("maxVolumeBounces", ctypes.c_int),
+        ("principled", ctypes.c_int),
+        ("pDensity", ctypes.c_float), ("pDensityThreshold", ctypes.c_float), ("pDensityScale", ctypes.c_float),
+        ("pValueRange", ctypes.c_float * 2),
+        ("pEmissionStrength", ctypes.c_float), ("pBlackbodyIntensity", ctypes.c_float),
+        ("pTemperature", ctypes.c_float),
+        ("pScatterColor", ctypes.c_float * 3), ("pAbsorptionColor", ctypes.c_float * 3),
+        ("pEmissionColor", ctypes.c_float * 3), ("pBlackbodyTint", ctypes.c_float * 3),
         ("width", ctypes.c_int),
         ("height", ctypes.c_int),
     ]
@@ -99,9 +106,31 @@ def lib():
         L.orc64_render_expected.argtypes = [P, I, I, I, I, D, I, I, I, P]
         L.orc_sincos.argtypes = [I, P, P, P]
         L.orc_logp.argtypes = [I, P, P]
+        L.orc_expp.argtypes = [I, P, P]
+        L.orc_blackbody.argtypes = [F, P]
         L.orc_hg_sample.argtypes = [P, F, U64, I, P]
         _lib = L
     return _lib
+
+
+def principled_params(p):
+    """Principled volume parameters with the reference's defaults and the
+    clamps of its setters (PrincipledVolume.h:17-30, Volume.cpp:36-126)."""
+    p = dict(p or {})
+    out = {"enabled": 1 if p.get("enabled", bool(p)) else 0,
+           "density": float(p.get("density", 1.0)),
+           "density_threshold": max(float(p.get("density_threshold", 0.0)), 0.0),
+           "density_scale": float(p.get("density_scale", 1.0)),
+           "value_range": tuple(float(x) for x in p.get("value_range", (0.0, 1.0))),
+           "emission_strength": max(float(p.get("emission_strength", 0.0)), 0.0),
+           "blackbody_intensity": max(float(p.get("blackbody_intensity", 0.0)), 0.0),
+           "temperature": max(float(p.get("temperature", 0.0)), 0.0)}
+    if not out["density_scale"] > 0.0:
+        out["density_scale"] = 1.0
+    for k, dflt in (("scatter_color", (0.8, 0.8, 0.8)), ("absorption_color", (0.0, 0.0, 0.0)),
+                    ("emission_color", (1.0, 1.0, 1.0)), ("blackbody_tint", (1.0, 1.0, 1.0))):
+        out[k] = tuple(max(float(x), 0.0) for x in p.get(k, dflt))
+    return out
 
 
 def _ptr(a):
@@ -148,6 +177,14 @@ class Scene:
         s.majorantRoundUp = int(desc.get("majorant_round_up", False))
         s.compensatedAccum = int(desc.get("compensated_accum", False))
         s.maxVolumeBounces = int(desc.get("max_volume_bounces", 0))
+        pv = principled_params(desc.get("principled"))
+        s.principled = pv["enabled"]
+        s.pDensity, s.pDensityThreshold, s.pDensityScale = pv["density"], pv["density_threshold"], pv["density_scale"]
+        s.pValueRange[:] = pv["value_range"]
+        s.pEmissionStrength, s.pBlackbodyIntensity = pv["emission_strength"], pv["blackbody_intensity"]
+        s.pTemperature = pv["temperature"]
+        s.pScatterColor[:], s.pAbsorptionColor[:] = pv["scatter_color"], pv["absorption_color"]
+        s.pEmissionColor[:], s.pBlackbodyTint[:] = pv["emission_color"], pv["blackbody_tint"]
         s.width, s.height = desc["width"], desc["height"]
         self.s = s
 
@@ -200,6 +237,20 @@ def logp(x):
     x = np.ascontiguousarray(x, np.float32)
     out = np.empty_like(x)
     lib().orc_logp(x.size, _ptr(x), _ptr(out))
+    return out
+
+
+def expp(x):
+    """The portable binary32 exponential shared by the oracle and the kernels."""
+    x = np.ascontiguousarray(x, np.float32)
+    out = np.empty_like(x)
+    lib().orc_expp(x.size, _ptr(x), _ptr(out))
+    return out
+
+
+def blackbody(kelvin):
+    out = np.empty(3, np.float32)
+    lib().orc_blackbody(kelvin, _ptr(out))
     return out
 
 

@@ -199,6 +199,20 @@ static inline float logPortable(float x) {
   return fe * 0.693145751953125f + (fe * 1.42860682e-6f + lm);
 }
 
+// e^x for |x| < 87 (the blackbody colour's powf), shared with the CUDA kernels
+// like logPortable: k = rint(x / ln2), r = x - k ln2 (split ln2, |r| <=
+// 0.347), e^r as the Taylor series to r^8 (truncation below 3e-9), times 2^k
+// by exponent arithmetic.
+static inline float expPortable(float x) {
+  const float k = rintf(x * 1.44269504f);
+  const float r = (x - k * 0.693145751953125f) - k * 1.42860682e-6f;
+  const float p = 1.f + r * (1.f + r * (0.5f + r * (1.66666667e-1f + r * (4.16666667e-2f + r * (8.33333333e-3f +
+                  r * (1.38888889e-3f + r * (1.98412698e-4f + r * 2.48015873e-5f)))))));
+  return p * bitsFloat((uint32_t)((int)k + 127) << 23);
+}
+// x^y for x > 0 (PrincipledVolume.h's powf), as e^(y log x)
+static inline float powPortable(float x, float y) { return expPortable(y * logPortable(x)); }
+
 
 } // namespace orc
 
@@ -336,10 +350,85 @@ static float tfMajorant(const OrcScene &s, float lo, float hi) {
   return m * s.baseDensity;
 }
 
-// Volume.h:62-74 (principled branch is not part of this path)
-static inline vec4f sampleAndMap(const Scene &sc, vec3f P) {
+// ---- principled volumes (PrincipledVolume.h:55-175) ----
+static inline vec3f pv3(const float *c) { return V(c[0], c[1], c[2]); }
+static inline float principledDensityFactor(const OrcScene &s, float scalar) {
+  float x = clampf(scalar, s.pValueRange[0], s.pValueRange[1]);
+  if (s.pDensityThreshold > 0.f && x < s.pDensityThreshold) return 0.f;
+  return s.pDensity * fmax_(x, 0.f) * s.pDensityScale;
+}
+static inline vec3f principledSigmaS(const OrcScene &s, float scalar) {
+  return principledDensityFactor(s, scalar) * pv3(s.pScatterColor);
+}
+static inline vec3f principledSigmaA(const OrcScene &s, float scalar) {
+  return principledDensityFactor(s, scalar) * pv3(s.pAbsorptionColor);
+}
+static inline float principledSigmaT(const OrcScene &s, float scalar) {
+  return reduce_max(principledSigmaS(s, scalar) + principledSigmaA(s, scalar));
+}
+static inline vec4f principledSampleMap(const OrcScene &s, float scalar) {
+  vec3f sigma_s = principledSigmaS(s, scalar);
+  vec3f sigma_a = principledSigmaA(s, scalar);
+  vec3f sigma_t = sigma_s + sigma_a;
+  float sigma_t_scalar = reduce_max(sigma_t);
+  vec3f tint = V(1.f);
+  if (sigma_t_scalar > 0.f) {
+    float ms = reduce_max(sigma_s);
+    tint = ms > 0.f ? V(sigma_s.x / ms, sigma_s.y / ms, sigma_s.z / ms) : V(1.f);
+  }
+  return {tint.x, tint.y, tint.z, sigma_t_scalar};
+}
+static inline vec3f principledBlackbodyColor(float kelvin) {
+  kelvin = clampf(kelvin, 1000.f, 40000.f);
+  float t = kelvin / 100.f;
+  float r, g, b;
+  if (t <= 66.f) {
+    r = 1.f;
+    g = clampf(0.390081578f * logPortable(t) - 0.631841444f, 0.f, 1.f);
+  } else {
+    r = clampf(1.292936186f * powPortable(t - 60.f, -0.1332047592f), 0.f, 1.f);
+    g = clampf(1.129890860f * powPortable(t - 60.f, -0.0755148492f), 0.f, 1.f);
+  }
+  if (t >= 66.f) b = 1.f;
+  else if (t <= 19.f) b = 0.f;
+  else b = clampf(0.543206789f * logPortable(t - 10.f) - 1.196254089f, 0.f, 1.f);
+  return V(r, g, b);
+}
+static inline vec3f principledEmission(const OrcScene &s, float scalar) {
+  float d = principledDensityFactor(s, scalar);
+  vec3f Le = s.pEmissionStrength * pv3(s.pEmissionColor) * d;
+  if (s.pBlackbodyIntensity > 0.f && s.pTemperature > 0.f)
+    Le = Le + s.pBlackbodyIntensity * pv3(s.pBlackbodyTint) * principledBlackbodyColor(s.pTemperature) * d;
+  return Le;
+}
+static inline float principledMajorant(const OrcScene &s, float lo, float hi) {
+  if (lo > hi) return 0.f;
+  float m = 0.f;
+  const int steps = 8;
+  for (int i = 0; i <= steps; ++i) {
+    float t = float(i) / float(steps);
+    float x = lo + t * (hi - lo);
+    m = fmax_(m, principledSigmaT(s, x));
+  }
+  return m;
+}
+// MCGrid.cu:97-113 mapMCs, with the principled scale
+static inline float mapMajorant(const OrcScene &s, float lo, float hi) {
+  const float tfMaj = tfMajorant(s, lo, hi);
+  return s.principled ? principledMajorant(s, lo, hi) * tfMaj : tfMaj;
+}
+
+// Volume.h:60-74
+static inline vec4f sampleAndMap(const Scene &sc, vec3f P, float &scalar) {
   float f = sampleField(sc, P);
+  scalar = f;
   if (std::isnan(f)) return {0.f, 0.f, 0.f, 0.f};
+  if (sc.s.principled) {
+    vec4f tf = tfMap(sc.s, f);
+    if (tf.w <= 0.f) return {0.f, 0.f, 0.f, 0.f};
+    vec4f p = principledSampleMap(sc.s, f);
+    return {p.x * tf.x, p.y * tf.y, p.z * tf.z, p.w * tf.w};
+  }
   return tfMap(sc.s, f);
 }
 
@@ -379,7 +468,7 @@ static void setupScene(Scene &sc) {
   buildRanges(s, sc.mcDims, ranges.data());
   sc.majorants.resize(n);
   for (int64_t i = 0; i < n; i++) {                                   // MCGrid.cu:97-113
-    float m = tfMajorant(s, ranges[2 * i], ranges[2 * i + 1]);
+    float m = mapMajorant(s, ranges[2 * i], ranges[2 * i + 1]);
     if (s.majorantRoundUp && m > 0.f) m = nextafterf(m, INF);
     sc.majorants[i] = m;
   }
@@ -451,14 +540,15 @@ struct Ray {
   RNGSeed rngSeed;
   bool hadHit = false;
   vec3f P;
-  vec3f hitColor;  // TF rgb at the collision (phase tint)
+  vec3f hitColor;  // mapped rgb at the collision (phase tint)
+  float hitScalar; // field value at the collision (principled volumes)
 };
 
 struct LocalStats { uint64_t samples = 0, mcVisits = 0, rays = 0; };
 
 // Woodcock::sampleRange, Volume.h:168-203
-static bool woodcock(vec4f &sample, const Scene &sc, vec3f org, vec3f dir, float t_lower, float &t_upper,
-                     float majorant, Random2 &rand, LocalStats &st) {
+static bool woodcock(vec4f &sample, float &scalar, const Scene &sc, vec3f org, vec3f dir, float t_lower,
+                     float &t_upper, float majorant, Random2 &rand, LocalStats &st) {
   float t = t_lower;
   while (true) {
     float r = rand();
@@ -466,7 +556,7 @@ static bool woodcock(vec4f &sample, const Scene &sc, vec3f org, vec3f dir, float
     t += dt;
     if (t >= t_upper) return false;
     vec3f P = org + t * dir;
-    sample = sampleAndMap(sc, P);
+    sample = sampleAndMap(sc, P, scalar);
     st.samples++;
     if (sample.w >= rand() * majorant) { t_upper = t; return true; }
   }
@@ -491,13 +581,15 @@ static void traceRay(const Scene &sc, Ray &ray, LocalStats &st) {
     st.mcVisits++;
     if (majorant == 0.f) return true;
     vec4f sample = {0, 0, 0, 0};
+    float scalar = 0.f;
     float upper = fmin_(ct1, ray.tMax);
-    if (!woodcock(sample, sc, obj_org, obj_dir, ct0, upper, majorant, rng, st)) return true;
+    if (!woodcock(sample, scalar, sc, obj_org, obj_dir, ct0, upper, majorant, rng, st)) return true;
     vec3f P = obj_org + upper * obj_dir;
     ray.hadHit = true;           // Ray::setVolumeHit -> setHit (Ray.h:101-144)
     ray.P = P;
     ray.tMax = upper;
     ray.hitColor = V(sample.x, sample.y, sample.z);
+    ray.hitScalar = scalar;
     return false;
   });
 }
@@ -725,10 +817,41 @@ static PixelSample renderPixelSample(const Scene &sc, int ix, int iy, int accumI
     const vec3f P = ray.P;
     const vec3f wo = -normalize(ray.dir);
     const float offsetEpsilon = fmax_(1e-4f, 1e-6f * reduce_max(vabs(P)));  // safe_eps
-    // bsdf at the collision (Phase.h): SimplePhase(0.7) or HGPhase
+    // bsdf at the collision (Phase.h): SimplePhase(0.7) or HGPhase.  The
+    // multi-scatter build re-derives a principled volume's tint, albedo and
+    // emission from the field value at the hit (MCAccelerator.h:621-659).
+    vec3f tint = ray.hitColor;
+    float hitAlbedo = s.scatteringAlbedo;
+    vec3f emission = V(0.f);
+    if (s.phaseMode == 1 && s.principled) {
+      const float scalar = ray.hitScalar;
+      vec3f sigma_s = principledSigmaS(s, scalar);
+      vec3f sigma_a = principledSigmaA(s, scalar);
+      vec4f tf = tfMap(s, scalar);
+      if (tf.w > 0.f) {
+        sigma_s = sigma_s * tf.w;
+        sigma_a = sigma_a * tf.w;
+        tint = tint * V(tf.x, tf.y, tf.z);
+      } else {
+        sigma_s = V(0.f);
+        sigma_a = V(0.f);
+      }
+      float sigma_t = reduce_max(sigma_s + sigma_a);
+      if (sigma_t > 0.f) {
+        float ms = reduce_max(sigma_s);
+        tint = ms > 0.f ? V(sigma_s.x / ms, sigma_s.y / ms, sigma_s.z / ms) : tint;
+        hitAlbedo = reduce_max(sigma_s) / sigma_t;
+      }
+      emission = principledEmission(s, scalar);
+    }
     vec3f albedo;
-    if (s.phaseMode == 0) albedo = .7f * ray.hitColor;
-    else albedo = s.scatteringAlbedo * ray.hitColor;
+    if (s.phaseMode == 0) albedo = .7f * tint;
+    else albedo = hitAlbedo * tint;
+    // emission of an HGPhase hit (shadeRays.cu:613-617): this generation's fragment
+    if (s.phaseMode == 1 && reduce_max(emission) > 0.f) {
+      if (depth == 0) out.frag0 = tp * emission;
+      else out.add(tp * emission);
+    }
     // shadow ray (:640-746)
     Ray shadow;
     vec3f shadowTp = V(0.f);
@@ -868,6 +991,13 @@ void orc_rng_derived(uint64_t parentState, uint64_t h, int n, uint32_t *out, uin
 uint64_t orc_hash3(uint32_t a, uint32_t b, uint32_t c) { return hash3(a, b, c); }
 float orc_fastlog(float f) { return fastLog(f); }
 uint16_t orc_f2h(float f) { return f2h(f); }
+void orc_expp(int n, const float *x, float *out) {
+  for (int i = 0; i < n; i++) out[i] = expPortable(x[i]);
+}
+void orc_blackbody(float kelvin, float *rgb) {
+  vec3f c = principledBlackbodyColor(kelvin);
+  rgb[0] = c.x; rgb[1] = c.y; rgb[2] = c.z;
+}
 void orc_logp(int n, const float *x, float *out) {
   for (int i = 0; i < n; i++) out[i] = logPortable(x[i]);
 }
@@ -895,7 +1025,7 @@ void orc_build_ranges(const OrcScene *s, float *out) {
 }
 void orc_map_majorants(const OrcScene *s, const float *ranges, int64_t n, float *out) {
   for (int64_t i = 0; i < n; i++) {
-    float m = tfMajorant(*s, ranges[2 * i], ranges[2 * i + 1]);
+    float m = mapMajorant(*s, ranges[2 * i], ranges[2 * i + 1]);
     if (s->majorantRoundUp && m > 0.f) m = nextafterf(m, INF);
     out[i] = m;
   }
@@ -909,7 +1039,8 @@ void orc_sample_points(const OrcScene *s, int n, const float *P, float *outScala
   for (int i = 0; i < n; i++) {
     vec3f p = V(P[3 * i], P[3 * i + 1], P[3 * i + 2]);
     outScalar[i] = sampleField(sc, p);
-    vec4f m = sampleAndMap(sc, p);
+    float scalar;
+    vec4f m = sampleAndMap(sc, p, scalar);
     outRGBA[4 * i + 0] = m.x; outRGBA[4 * i + 1] = m.y; outRGBA[4 * i + 2] = m.z; outRGBA[4 * i + 3] = m.w;
   }
 }

@@ -30,6 +30,11 @@ typedef struct {
   int majorantRoundUp;    // 1: majorant bumped one ulp up (precision forms)
   int compensatedAccum;   // 1: Neumaier-compensated accumulation across waves (precision forms)
   int maxVolumeBounces;   // with phaseMode 1: up to this many volume bounces (multi-scatter build)
+  // principled volume coefficients (PrincipledVolume.h), enabled by `principled`
+  int principled;
+  float pDensity, pDensityThreshold, pDensityScale, pValueRange[2];
+  float pEmissionStrength, pBlackbodyIntensity, pTemperature;
+  float pScatterColor[3], pAbsorptionColor[3], pEmissionColor[3], pBlackbodyTint[3];
   int width, height;
 } OrcScene;
 }

@@ -36,6 +36,13 @@ def scenes():
                                        synth.DEFAULT_CAMERA, ambient=1.0)
     out["blobs_ea"] = synth.scene(blob, "f32", 24, 16, synth.tf_linear_ramp(128), 50.0, synth.DEFAULT_CAMERA,
                                   ambient=0.0, emission_absorption=True, bg_color=(0.1, 0.2, 0.3, 1.0))
+    # the multi-scatter build: HG sampling with up to 3 volume bounces; and a
+    # principled volume with absorption, emission and blackbody, 2 bounces
+    out["noise_multiscatter"] = dict(out["noise_f32"], anisotropy=0.6, max_volume_bounces=3)
+    out["noise_principled"] = dict(out["noise_f32"], anisotropy=-0.3, max_volume_bounces=2, principled={
+        "enabled": 1, "absorption_color": (0.2, 0.1, 0.05), "emission_strength": 1.5,
+        "blackbody_intensity": 0.5, "temperature": 4500.0, "density_threshold": 0.2})
+    out["noise_exact_log"] = dict(out["noise_u8"], exact_log=True)
     return out
 
 
@@ -57,12 +64,15 @@ def compute(name, d):
     return res
 
 
-def main():
+def main(names=None):
+    """(Re)writes the named fixtures, or all of them."""
     for name, d in scenes().items():
+        if names and name not in names:
+            continue
         res = compute(name, d)
         np.savez_compressed(os.path.join(HERE, f"{name}.npz"), **res)
         print(name, {k: v.shape for k, v in res.items()})
 
 
 if __name__ == "__main__":
-    main()
+    main(sys.argv[1:])

@@ -9,7 +9,8 @@ import oracle
 from tests.helpers import assert_bitexact
 
 HERE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
-NAMES = ["noise_f32", "noise_u8", "noise_f16", "blobs_ambient", "blobs_ea"]
+NAMES = ["noise_f32", "noise_u8", "noise_f16", "blobs_ambient", "blobs_ea", "noise_multiscatter",
+         "noise_principled", "noise_exact_log"]
 
 
 def _scene(name):

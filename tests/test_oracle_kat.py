@@ -344,3 +344,45 @@ def test_portable_log_within_two_ulp_on_free_flight_inputs():
     assert oracle.logp(np.array([1.0], np.float32))[0] == 0.0
     p2 = np.float32(2.0) ** -np.arange(1, 24, dtype=np.float32)
     assert np.allclose(oracle.logp(p2), np.log(p2.astype(np.float64)), rtol=2 ** -23, atol=0)
+
+
+def test_portable_exp_within_two_ulp():
+    x = np.linspace(-20, 20, 200001, dtype=np.float32)
+    v = oracle.expp(x).astype(np.float64)
+    t = np.exp(x.astype(np.float64))
+    assert (np.abs(v - t) <= 2 * np.spacing(t.astype(np.float32))).all()
+    assert oracle.expp(np.array([0.0], np.float32))[0] == 1.0
+
+
+@pytest.mark.parametrize("kelvin", [500.0, 1500.0, 1900.0, 3000.0, 6500.0, 6700.0, 8000.0, 20000.0, 50000.0])
+def test_blackbody_colour_matches_the_reference_formula(kelvin):
+    # PrincipledVolume.h:64-82, evaluated here in float64
+    k = min(max(kelvin, 1000.0), 40000.0)
+    t = k / 100.0
+    cl = lambda v: min(max(v, 0.0), 1.0)
+    if t <= 66.0:
+        r, g = 1.0, cl(0.390081578 * np.log(t) - 0.631841444)
+    else:
+        r = cl(1.292936186 * (t - 60.0) ** -0.1332047592)
+        g = cl(1.129890860 * (t - 60.0) ** -0.0755148492)
+    b = 1.0 if t >= 66.0 else (0.0 if t <= 19.0 else cl(0.543206789 * np.log(t - 10.0) - 1.196254089))
+    assert np.allclose(oracle.blackbody(kelvin), [r, g, b], rtol=0, atol=2e-6)
+
+
+def test_principled_volume_emission_adds_light():
+    from tests.helpers import small_noise_scene
+    d = small_noise_scene(w=24, h=16, phase="hg", anisotropy=0.4)
+    means = []
+    for pv in ({"enabled": 1}, {"enabled": 1, "emission_strength": 2.0},
+               {"enabled": 1, "emission_strength": 2.0, "blackbody_intensity": 1.0, "temperature": 5000.0}):
+        acc = np.zeros((16, 24, 4), np.float32)
+        oracle.render(oracle.Scene(dict(d, principled=pv)), 0, 16, accum=acc)
+        means.append(float(oracle.resolve(acc, 16)[..., :3].mean()))
+    assert means[0] < means[1] < means[2]
+    # the default build (SimplePhase) has no emission
+    s = small_noise_scene(w=24, h=16, phase="simple")
+    a = np.zeros((16, 24, 4), np.float32)
+    b = np.zeros_like(a)
+    oracle.render(oracle.Scene(dict(s, principled={"enabled": 1})), 0, 4, accum=a)
+    oracle.render(oracle.Scene(dict(s, principled={"enabled": 1, "emission_strength": 5.0})), 0, 4, accum=b)
+    assert np.array_equal(a, b)
