@@ -15,8 +15,9 @@ enum ErrorBits : unsigned { ERR_ITER_CAP = 1u, ERR_ABORTED = 2u };
 constexpr int kMaxDirLights = 16;
 constexpr int kMaxTF = 4096;
 constexpr int kCellsPerMC = 8;  // StructuredData.cu:26
-constexpr int kRenderMaxThreads = 128;  // __launch_bounds__ of the render kernel:
-constexpr int kRenderMinBlocks = 5;     // 5 x 128 threads per SM (at most 102 registers)
+constexpr int kRenderMaxThreads = 128;  // __launch_bounds__ of the render kernels:
+constexpr int kRenderMinBlocks = 6;     // plain: 6 x 128 threads per SM (at most 85 registers)
+constexpr int kRenderMinBlocksExt = 5;  // extended (multi-scatter, principled): 5 x 128 (102)
 
 // Principled volume coefficients evaluated from the field value
 // (PrincipledVolumeParams::DD, PrincipledVolume.h:33-46).

@@ -348,7 +348,7 @@ struct TraceState {
   float nextCellBegin;
   float3 tNext, tStep;
   int cx, cy, cz;
-  int bits;             // 1/2/4: DDA direction > 0 on x/y/z
+  int bits;             // 1/2/4: DDA direction > 0 on x/y/z; 8/16/32: component fixed up from 0
   uint64_t rng;         // Random rng of isProg
   float t, tUpper, maj; // current Woodcock range
 };
@@ -369,6 +369,7 @@ DEV bool boxTest(float3 org, float3 dir, float &t0, float &t1, float3 lo, float3
 // Returns false if the ray has no cell to visit.  raySeed is advanced when
 // the box test passes (Random rng(ray.rngSeed, ...), MCAccelerator.h:592).
 DEV bool traceBegin(const VolumeDD &v, TraceState &ts, float3 org, float3 dir, float tMax, uint64_t &raySeed) {
+  const int fixed = (dir.x == 0.f ? 8 : 0) | (dir.y == 0.f ? 16 : 0) | (dir.z == 0.f ? 32 : 0);
   if (dir.x == 0.f) dir.x = 1e-6f;
   if (dir.y == 0.f) dir.y = 1e-6f;
   if (dir.z == 0.f) dir.z = 1e-6f;
@@ -402,7 +403,9 @@ DEV bool traceBegin(const VolumeDD &v, TraceState &ts, float3 org, float3 dir, f
   ts.tStep = f3(fabsf(rcpd.x), fabsf(rcpd.y), fabsf(rcpd.z));
   ts.tNext = f3(d.x == 0.f ? kInf : fabsf(fe.x - oi.x) * ts.tStep.x, d.y == 0.f ? kInf : fabsf(fe.y - oi.y) * ts.tStep.y,
                 d.z == 0.f ? kInf : fabsf(fe.z - oi.z) * ts.tStep.z);
-  ts.bits = (d.x > 0.f ? 1 : 0) | (d.y > 0.f ? 2 : 0) | (d.z > 0.f ? 4 : 0);
+  // bits 0-2: DDA direction > 0 on x/y/z; bits 3-5: that component of the
+  // ray direction was exactly 0 and was replaced by 1e-6 above
+  ts.bits = (d.x > 0.f ? 1 : 0) | (d.y > 0.f ? 2 : 0) | (d.z > 0.f ? 4 : 0) | fixed;
   ts.cx = (int)fc.x;
   ts.cy = (int)fc.y;
   ts.cz = (int)fc.z;
@@ -661,7 +664,8 @@ DEV void renderLoop(const JobDD *jobs, const int *chunkStart, int numJobs, int n
   const unsigned FULL = 0xffffffffu;
   const int lane = threadIdx.x & 31;
 
-  unsigned long long nSamples = 0, nVisits = 0, nRays = 0;
+  // lane work counters, 32-bit, flushed to the launch counters (below)
+  unsigned nSamples = 0, nVisits = 0, nRays = 0;
   unsigned errBits = 0;
 
   // warp-uniform work chunk
@@ -677,7 +681,6 @@ DEV void renderLoop(const JobDD *jobs, const int *chunkStart, int numJobs, int n
   TraceState ts;
   uint64_t raySeed = 0;
   float3 primDir = f3(0.f, 0.f, 0.f);
-  float4 bg = make_float4(0.f, 0.f, 0.f, 0.f);
   float3 shadowTp = f3(0.f, 0.f, 0.f);
   float3 hitRGB = f3(0.f, 0.f, 0.f);
   float misWeight = 0.f;
@@ -700,6 +703,14 @@ DEV void renderLoop(const JobDD *jobs, const int *chunkStart, int numJobs, int n
   // then (B) a tight loop that only steps macrocells and Woodcock ranges
   // until at least sd.serviceBatch lanes (or every busy lane) need service.
   while (true) {
+    // between two service passes a lane traces at most one ray (< 2^24
+    // counter increments), so 32-bit lane counters flushed from 2^31 on never wrap
+    if ((nSamples | nVisits | nRays) >= 0x80000000u) {
+      atomicAdd(&ctr->samples, (unsigned long long)nSamples);
+      atomicAdd(&ctr->mcVisits, (unsigned long long)nVisits);
+      atomicAdd(&ctr->rays, (unsigned long long)nRays);
+      nSamples = nVisits = nRays = 0;
+    }
     {
       const JobDD &J = jobs[BATCH ? job : 0];
       const VolumeDD &v = J.v;
@@ -765,7 +776,11 @@ DEV void renderLoop(const JobDD *jobs, const int *chunkStart, int numJobs, int n
           } else {
             // bounce() volume-hit branch, shadeRays.cu:608-746
             uint64_t random = rngDerive(raySeed, (uint64_t)__float_as_uint(tHit));
-            const float3 won = normalize3(primDir);
+            // the ray's own direction: the plain kernels undo the zero fix-up
+            // of traceBegin instead of keeping a copy in registers
+            const float3 won = normalize3(EXT ? primDir
+                                              : f3((ts.bits & 8) ? 0.f : ts.dir.x, (ts.bits & 16) ? 0.f : ts.dir.y,
+                                                   (ts.bits & 32) ? 0.f : ts.dir.z));
             const float3 woN = f3(-won.x, -won.y, -won.z);  // dg.wo
             const float offsetEpsilon = fmax_(1e-4f, 1e-6f * fmax_(fmax_(fabsf(P.x), fabsf(P.y)), fabsf(P.z)));
             LightSample ls;
@@ -891,6 +906,14 @@ DEV void renderLoop(const JobDD *jobs, const int *chunkStart, int numJobs, int n
         const float clampMax = 10.f * (1 + accumID);
         const bool cmp = fr.comp != nullptr;
         if (!shadowRay && (!EXT || depth == 0)) {
+          // the primary ray's miss colour (generateRays.cu:217-227), computed here
+          // rather than kept in registers for the whole wave
+          float4 bg = fr.bgColor;
+          if (!(fr.bgColor.w >= 0.f)) {
+            const float t = (iy + .5f) / float(fr.height);
+            bg = make_float4((1.0f - t) * 0.9f + t * 0.15f, (1.0f - t) * 0.9f + t * 0.25f, (1.0f - t) * 0.9f + t * .8f,
+                             (1.0f - t) * 1.f + t * 1.f);
+          }
           const float f0x = fmin_(bg.x, clampMax), f0y = fmin_(bg.y, clampMax), f0z = fmin_(bg.z, clampMax);
           if (accumID == 0) {
             acc = make_float4(f0x, f0y, f0z, bg.w);
@@ -1027,13 +1050,7 @@ DEV void renderLoop(const JobDD *jobs, const int *chunkStart, int numJobs, int n
             } else tMax = 0.f;
           }
         }
-        if (fr.bgColor.w >= 0.f) bg = fr.bgColor;
-        else {
-          const float t = (iy + .5f) / float(H);
-          bg = make_float4((1.0f - t) * 0.9f + t * 0.15f, (1.0f - t) * 0.9f + t * 0.25f, (1.0f - t) * 0.9f + t * .8f,
-                           (1.0f - t) * 1.f + t * 1.f);
-        }
-        primDir = d;
+        if (EXT) primDir = d;
         shadowRay = false;
         if (EXT) {
           pathTp = f3(1.f, 1.f, 1.f);
@@ -1141,23 +1158,24 @@ DEV void renderLoop(const JobDD *jobs, const int *chunkStart, int numJobs, int n
     }
   }
 
-  // counters: warp reduction, one atomic per warp
+  // counters: warp reduction in 64 bits, one atomic per warp
+  unsigned long long wSamples = nSamples, wVisits = nVisits, wRays = nRays;
   for (int o = 16; o > 0; o >>= 1) {
-    nSamples += __shfl_down_sync(FULL, nSamples, o);
-    nVisits += __shfl_down_sync(FULL, nVisits, o);
-    nRays += __shfl_down_sync(FULL, nRays, o);
+    wSamples += __shfl_down_sync(FULL, wSamples, o);
+    wVisits += __shfl_down_sync(FULL, wVisits, o);
+    wRays += __shfl_down_sync(FULL, wRays, o);
     errBits |= __shfl_down_sync(FULL, errBits, o);
   }
   if (lane == 0) {
-    atomicAdd(&ctr->samples, nSamples);
-    atomicAdd(&ctr->mcVisits, nVisits);
-    atomicAdd(&ctr->rays, nRays);
+    atomicAdd(&ctr->samples, wSamples);
+    atomicAdd(&ctr->mcVisits, wVisits);
+    atomicAdd(&ctr->rays, wRays);
     if (errBits) atomicOr(&ctr->errorFlags, (unsigned long long)errBits);
   }
 }
 
 template <int T, int LOG, bool EXT>
-__global__ void __launch_bounds__(kRenderMaxThreads, kRenderMinBlocks)
+__global__ void __launch_bounds__(kRenderMaxThreads, EXT ? kRenderMinBlocksExt : kRenderMinBlocks)
     renderKernel(const __grid_constant__ JobDD job, const __grid_constant__ SchedDD sd, LaunchCounters *ctr) {
   extern __shared__ float4 sTF[];
   __shared__ float u8lut[256];
@@ -1169,7 +1187,7 @@ __global__ void __launch_bounds__(kRenderMaxThreads, kRenderMinBlocks)
 }
 
 template <bool EXT>
-__global__ void __launch_bounds__(kRenderMaxThreads, kRenderMinBlocks)
+__global__ void __launch_bounds__(kRenderMaxThreads, EXT ? kRenderMinBlocksExt : kRenderMinBlocks)
     renderBatchKernel(const JobDD *jobs, const int *chunkStart, int numJobs, const __grid_constant__ SchedDD sd,
                       LaunchCounters *ctr) {
   __shared__ float u8lut[256];

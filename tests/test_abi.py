@@ -68,15 +68,16 @@ def test_kernels_compiled_for_sm100a():
     log = open(os.path.join(ROOT, "barney_b200", "csrc", "ptxas.log")).read()
     assert "for 'sm_100a'" in log
     assert "renderKernel" in log
-    # The render megakernels are capped at 5 blocks of 128 threads per SM
-    # (at most 102 registers); the few spill bytes that costs are a measured
-    # trade for the fifth block.  A large spill would mean a regression.
+    # The plain render kernels are capped at 6 blocks of 128 threads per SM
+    # (80 registers), the extended ones at 5 (96); the spill bytes that costs
+    # are a measured trade for the extra blocks.  A large spill would mean a
+    # regression.
     blocks = log.split("Function properties for ")
     render = [b for b in blocks[1:] if b.split()[0].startswith(("_ZN3bnb12renderKernel", "_ZN3bnb17renderBatch"))]
     assert len(render) >= 2
     for b in render:
         m = re.search(r"(\d+) bytes spill stores", b)
-        assert m and int(m.group(1)) <= 256, b.splitlines()[1]
+        assert m and int(m.group(1)) <= 320, b.splitlines()[1]
 
 
 def test_header_compiles_as_c_and_shim_as_cpp(tmp_path):
