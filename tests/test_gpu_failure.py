@@ -55,3 +55,35 @@ def test_batch_deadline_aborts_and_context_recovers():
         for r in big + [small]:
             r.close()
         ctx.close()
+
+
+def test_iteration_cap_ends_runaway_rays_and_sets_the_error_bit():
+    # A majorant far above every sample the rays meet: the TF is opaque only
+    # at its last entry, which the field reaches at one voxel in the centre,
+    # so the centre macrocell's majorant is 1e9 times the density rays see
+    # and a ray crossing it would take ~1e8 Woodcock steps.  Each ray stops
+    # at 2^22 steps, as if it left the grid, with error bit 1; the context
+    # then renders normally.
+    import barney_b200 as bn
+    from barney_b200 import synth
+    vol = (0.5 * synth.value_noise(24, 3)).astype(np.float32)
+    vol[12, 12, 12] = 1.0
+    tf = np.zeros((256, 4), np.float32)
+    tf[:, :3] = 0.5
+    tf[:, 3] = 1e-9
+    tf[-1, 3] = 1.0
+    d = synth.scene(vol, "f32", 4, 4, tf, 1e9, synth.DEFAULT_CAMERA)
+    r = bn.VolumeRenderer(d, color_format="float4")
+    try:
+        r.set_spp(1)
+        r.render()
+        st = r.stats()
+        assert st["error_flags"] & 1
+        assert np.isfinite(r.read()).all()
+    finally:
+        r.close()
+    ok = small_noise_scene(w=16, h=12)
+    img, st = gpu_render(ok, 2)
+    ref, _, _ = oracle_render(ok, 2)
+    assert_bitexact(img, ref, "after capped rays")
+    assert st["error_flags"] == 0
