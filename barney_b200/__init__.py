@@ -49,7 +49,8 @@ EXPORTS = [
     "bnxSetLaunchConfig", "bnxFrameBufferDevicePointer", "bnxVolumeGetMacrocells",
     "bnxRenderStructuredNoAlloc", "bnxSetScheduling", "bnxRenderBatch", "bnxSetBatchGraphs", "bnxAutotuneBatch",
     "bnxServerCreate", "bnxServerDestroy", "bnxServerSubmit", "bnxServerWait", "bnxServerGetStats",
-    "bnxServerResetStats", "bnxServerReserve", "bnxSetRenderTimeout", "bnxAnariTransferFunction1D", "bnxAnariDensityScale",
+    "bnxServerResetStats", "bnxServerReserve", "bnxSetRenderTimeout", "bnxSetPixelPartition",
+    "bnxPixelPartitionOwners", "bnxAnariTransferFunction1D", "bnxAnariDensityScale",
     "bnxAnariStructuredRegular",
 ]
 
@@ -163,6 +164,7 @@ def lib(build_if_missing=True):
         "bnxServerGetStats": ([P, P], None), "bnxServerResetStats": ([P], None),
         "bnxServerReserve": ([P, ctypes.c_size_t], None),
         "bnxSetRenderTimeout": ([P, I], None),
+        "bnxSetPixelPartition": ([P, I, I], None), "bnxPixelPartitionOwners": ([I, I, I, P], None),
         "bnxAnariTransferFunction1D": ([P, I, I, P, I, bn_float4, F, P], I),
         "bnxAnariDensityScale": ([F], F),
         "bnxAnariStructuredRegular": ([P, I, I, P, I, I, I, bn_float3, bn_float3], P),
@@ -436,6 +438,11 @@ class VolumeRenderer:
         self.L.bnxSetScheduling(self.ctx, service_batch)
         check()
 
+    def set_partition(self, rank, count):
+        """Render only this rank's pixel tiles (bnxSetPixelPartition)."""
+        self.L.bnxSetPixelPartition(self.ctx, int(rank), int(count))
+        check()
+
     def set_timeout(self, milliseconds):
         self.L.bnxSetRenderTimeout(self.ctx, int(milliseconds))
         check()
@@ -458,6 +465,26 @@ class VolumeRenderer:
             self.close()
         except Exception:
             pass
+
+
+def partition_owners(width, height, count):
+    """(height, width) int32 map: the rank that renders each pixel of a frame
+    partitioned over `count` ranks (bnxPixelPartitionOwners)."""
+    owners = np.zeros((height, width), np.int32)
+    L = lib()
+    L.bnxPixelPartitionOwners(int(width), int(height), int(count), owners.ctypes.data)
+    check()
+    return owners
+
+
+def merge_partitions(frames, owners):
+    """Assemble a frame from per-rank frames (stacked on axis 0; numpy or
+    torch) by the owner map: pixel (y, x) is taken from frame owners[y, x]."""
+    out = frames[0].clone() if hasattr(frames[0], "clone") else frames[0].copy()
+    for r in range(1, len(frames)):
+        sel = owners == r
+        out[sel] = frames[r][sel]
+    return out
 
 
 class Server:

@@ -53,9 +53,21 @@ def _stale():
 
 
 def build(force=False, verbose=False):
-    """Compile every source for sm_100a into barney_b200/libbarney_b200.so."""
+    """Compile every source for sm_100a into barney_b200/libbarney_b200.so.
+    Processes that find the library stale at the same time (ranks of one job)
+    build it once: the build holds an exclusive lock, and whoever gets the
+    lock next sees the fresh library."""
     if not force and not _stale():
         return LIB
+    import fcntl
+    with open(LIB + ".lock", "w") as lock:
+        fcntl.flock(lock, fcntl.LOCK_EX)
+        if not force and not _stale():
+            return LIB
+        return _build_locked(verbose)
+
+
+def _build_locked(verbose):
     objs = []
     logs = []
     for src in SOURCES:

@@ -148,6 +148,8 @@ JobDD buildJob(Context *ctx, Renderer &r, Model &m, Camera &cam, FrameBuffer &fb
   // default build treats a volume scatter as the end of the path
   // (shadeRays.cu:23-25,774-796), so there it has no effect, as in Barney
   fr.maxVolumeBounces = (p.hgPhase && p.maxVolumeBounces > 0) ? p.maxVolumeBounces : 0;
+  fr.partRank = ctx->partRank;
+  fr.partCount = ctx->partCount;
   fr.accum = (float4 *)fb.accum.ptr;
   fr.comp = nullptr;
   if (p.compensatedAccum) {
@@ -192,9 +194,12 @@ static LaunchCounters *pinnedCounters(Context *ctx) {
   return ctx->hostCounters;
 }
 
-static bool waitWithDeadline(Context *ctx, cudaEvent_t done) {
+// The deadline counts from `start`, taken before the frame's first launch: a
+// launch can block the calling thread (a kernel's code is loaded on its first
+// launch in a process), and that time belongs to the frame too.
+static bool waitWithDeadline(Context *ctx, cudaEvent_t done, std::chrono::steady_clock::time_point start) {
   if (ctx->timeoutMs <= 0) return false;
-  const auto deadline = std::chrono::steady_clock::now() + std::chrono::milliseconds(ctx->timeoutMs);
+  const auto deadline = start + std::chrono::milliseconds(ctx->timeoutMs);
   while (true) {
     cudaError_t q = cudaEventQuery(done);
     if (q == cudaSuccess) return false;
@@ -210,6 +215,7 @@ static bool waitWithDeadline(Context *ctx, cudaEvent_t done) {
 }
 
 static void render(Context *ctx, Renderer &r, Model &m, Camera &cam, FrameBuffer &fb) {
+  const auto start = std::chrono::steady_clock::now();
   JobDD job = buildJob(ctx, r, m, cam, fb);
   if (job.fr.spp <= 0) return;
   ck(cudaMemsetAsync(ctx->dCounters, 0, sizeof(LaunchCounters), ctx->stream), "counter reset");
@@ -226,7 +232,7 @@ static void render(Context *ctx, Renderer &r, Model &m, Camera &cam, FrameBuffer
   // until the render finished, before the deadline could be checked.
   ck(cudaMemcpyAsync(pinnedCounters(ctx), ctx->dCounters, sizeof(LaunchCounters), cudaMemcpyDeviceToHost, ctx->stream),
      "counter read");
-  waitWithDeadline(ctx, ctx->ev[1]);
+  waitWithDeadline(ctx, ctx->ev[1], start);
   ck(cudaStreamSynchronize(ctx->stream), "render");
   const LaunchCounters hc = *ctx->hostCounters;
   readStats(ctx, hc, (unsigned long long)fb.width * fb.height * job.fr.spp);
@@ -261,8 +267,10 @@ void reserveBatch(Context *ctx, int n) {
 // replayed; per-frame values (cameras, accumIDs) travel in the pinned job
 // table the graph copies from.  Results equal one bnRender per job.
 void renderBatch(Context *ctx, const std::vector<BatchEntry> &entries) {
+  const auto start = std::chrono::steady_clock::now();
   const int n = (int)entries.size();
   if (n == 0) return;
+  if (ctx->partCount > 1) throw Error(E_UNSUPPORTED, "a pixel partition applies to bnRender only, not to batches");
   reserveBatch(ctx, n);
   std::vector<const void *> key;
   long long chunks = 0;
@@ -328,7 +336,7 @@ void renderBatch(Context *ctx, const std::vector<BatchEntry> &entries) {
   } else {
     enqueue(ctx->stream, true);
   }
-  waitWithDeadline(ctx, ctx->ev[2]);
+  waitWithDeadline(ctx, ctx->ev[2], start);
   ck(cudaStreamSynchronize(ctx->stream), "batch render");
   const bool aborted = ctx->hostCounters->errorFlags & ERR_ABORTED;
   for (int i = 0; i < n; i++) entries[i].fb->accumID = aborted ? 0 : entries[i].fb->accumID + ctx->hostJobs[i].fr.spp;
@@ -859,6 +867,31 @@ BN_API void bnxRenderBatch(BNContext context, const BNXRenderJob *jobs, int numJ
   Context *c = getContext(context);
   c->activate();
   renderBatch(c, batchEntries(jobs, numJobs));
+  BN_CATCH()
+}
+
+BN_API void bnxSetPixelPartition(BNContext context, int rank, int count) {
+  BN_TRY
+  Context *c = getContext(context);
+  if (count < 1 || rank < 0 || rank >= count) throw Error(E_INVALID_ARG, "need 0 <= rank < count");
+  c->partRank = rank;
+  c->partCount = count;
+  BN_CATCH()
+}
+
+BN_API void bnxPixelPartitionOwners(int width, int height, int count, int *owners) {
+  BN_TRY
+  if (width <= 0 || height <= 0 || count < 1 || !owners) throw Error(E_INVALID_ARG, "bad partition query");
+  // pixel order of the render kernel: 4-row bands, column-major inside a
+  // band, 32 pixels per chunk, kPartTileChunks chunks per tile
+  for (int iy = 0; iy < height; iy++) {
+    const int band = iy / 4;
+    const int rows = std::min(4, height - 4 * band);
+    for (int ix = 0; ix < width; ix++) {
+      const long long w = (long long)band * 4 * width + (long long)ix * rows + (iy - 4 * band);
+      owners[(size_t)iy * width + ix] = (int)((w / 32 / kPartTileChunks) % count);
+    }
+  }
   BN_CATCH()
 }
 

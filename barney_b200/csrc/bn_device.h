@@ -15,6 +15,7 @@ enum ErrorBits : unsigned { ERR_ITER_CAP = 1u, ERR_ABORTED = 2u };
 constexpr int kMaxDirLights = 16;
 constexpr int kMaxTF = 4096;
 constexpr int kCellsPerMC = 8;  // StructuredData.cu:26
+constexpr int kPartTileChunks = 32;    // pixel-tile partition: 32 chunks of 32 pixels per tile
 constexpr int kRenderMaxThreads = 128;  // __launch_bounds__ of the render kernels:
 constexpr int kRenderMinBlocks = 6;     // plain: 6 x 128 threads per SM (at most 85 registers)
 constexpr int kRenderMinBlocksExt = 5;  // extended (multi-scatter, principled): 5 x 128 (102)
@@ -72,6 +73,7 @@ struct FrameDD {
   int emissionAbsorption;
   int exactLog;
   int maxVolumeBounces;  // > 0: multi-scatter build (HG phase), scattered rays up to this many volume bounces
+  int partRank, partCount;  // pixel-tile partition: render the tiles t with t % partCount == partRank
   float4 *accum;        // width*height, linear
   float4 *comp;         // width*height Neumaier compensation terms, or null (plain sums)
   int accumID0;         // accumID of the first wave of this launch

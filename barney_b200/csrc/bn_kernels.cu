@@ -984,6 +984,9 @@ DEV void renderLoop(const JobDD *jobs, const int *chunkStart, int numJobs, int n
         }
         const int first = BATCH ? __ldg(chunkStart + j) : 0;
         const int npix = jobs[j].fr.width * jobs[j].fr.height;
+        if (!BATCH && jobs[j].fr.partCount > 1)  // this rank's k-th chunk -> the frame's chunk
+          c = (c / kPartTileChunks * jobs[j].fr.partCount + jobs[j].fr.partRank) * kPartTileChunks +
+              c % kPartTileChunks;
         chunkJob = j;
         chunkBase = (c - first) * kChunk;
         chunkLeft = min(kChunk, npix - chunkBase);
@@ -1174,6 +1177,16 @@ DEV void renderLoop(const JobDD *jobs, const int *chunkStart, int numJobs, int n
   }
 }
 
+// Chunks of a frame of numChunks chunks that partition rank `rank` of
+// `count` renders: whole tiles of kPartTileChunks chunks, t % count == rank.
+__host__ __device__ inline int partitionChunks(int numChunks, int rank, int count) {
+  const int tiles = (numChunks + kPartTileChunks - 1) / kPartTileChunks;
+  if (rank >= tiles) return 0;
+  const int mine = (tiles - 1 - rank) / count + 1;
+  const int last = rank + (mine - 1) * count;
+  return (mine - 1) * kPartTileChunks + min(kPartTileChunks, numChunks - last * kPartTileChunks);
+}
+
 template <int T, int LOG, bool EXT>
 __global__ void __launch_bounds__(kRenderMaxThreads, EXT ? kRenderMinBlocksExt : kRenderMinBlocks)
     renderKernel(const __grid_constant__ JobDD job, const __grid_constant__ SchedDD sd, LaunchCounters *ctr) {
@@ -1182,7 +1195,8 @@ __global__ void __launch_bounds__(kRenderMaxThreads, EXT ? kRenderMinBlocksExt :
   for (int i = threadIdx.x; i < job.v.tfN; i += blockDim.x) sTF[i] = job.v.tf[i];
   for (int i = threadIdx.x; i < 256; i += blockDim.x) u8lut[i] = (float)i * 1.f / 255.f;
   __syncthreads();
-  const int numChunks = (job.fr.width * job.fr.height + kChunk - 1) / kChunk;
+  int numChunks = (job.fr.width * job.fr.height + kChunk - 1) / kChunk;
+  if (job.fr.partCount > 1) numChunks = partitionChunks(numChunks, job.fr.partRank, job.fr.partCount);
   renderLoop<T, false, LOG, EXT>(&job, nullptr, 1, numChunks, sd, ctr, sTF, u8lut);
 }
 

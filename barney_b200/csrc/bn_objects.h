@@ -345,6 +345,7 @@ struct Context {
   int hostCapacity = 0;
   bool useGraphs = true;
   int timeoutMs = 0;                 // render deadline (0: none)
+  int partRank = 0, partCount = 1;   // pixel-tile partition (bnxSetPixelPartition)
   cudaStream_t abortStream = nullptr;
   cudaGraphExec_t graphExec = nullptr;
   std::vector<const void *> graphKey;

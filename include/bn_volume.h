@@ -228,11 +228,23 @@ BN_API void bnxGetStats(BNContext context, BNXStats *stats);
    selects the context's own stream. */
 BN_API void bnxSetStream(BNContext context, void *cudaStream);
 BN_API void *bnxGetStream(BNContext context);
-/* Deadline of bnRender (0: none).  When a frame exceeds it, the render
-   kernel is told to stop (every warp quits at its next pixel chunk), the
-   frame buffer's accumulation is reset and bnRender records error 8
-   (timeout); the context stays usable. */
+/* Deadline of bnRender and bnxRenderBatch (0: none), counted from the call.
+   When a frame is still running at the deadline, the render kernel is told
+   to stop (every warp quits at its next pixel chunk), the frame buffer's
+   accumulation is reset and the call records error 8 (timeout); the context
+   stays usable.  A frame that has finished by the time the deadline is
+   checked is kept. */
 BN_API void bnxSetRenderTimeout(BNContext context, int milliseconds);
+/* Pixel-tile data parallelism (the reference deals tiles round-robin across
+   GPUs, TiledFB.cu:230-261): bnRender on this context renders only the tiles
+   of 1024 pixels whose index modulo `count` is `rank` (count 1: all).  The
+   other pixels of the frame buffer are left as they were; a frame is
+   assembled from each rank's owned pixels, which bnxPixelPartitionOwners
+   lists.  Per-pixel results equal an unpartitioned render.  Batches reject a
+   partition. */
+BN_API void bnxSetPixelPartition(BNContext context, int rank, int count);
+/* owners[y * width + x] = the rank that renders pixel (x, y) */
+BN_API void bnxPixelPartitionOwners(int width, int height, int count, int *owners);
 /* Launch parameters of the render kernel (0 = automatic). */
 BN_API void bnxSetLaunchConfig(BNContext context, int blocksPerSM, int threadsPerBlock);
 /* Warp scheduling of the render kernel: a warp keeps stepping macrocells and

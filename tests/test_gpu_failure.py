@@ -12,9 +12,12 @@ pytestmark = pytest.mark.gpu
 def test_render_deadline_aborts_and_context_recovers():
     import barney_b200 as bn
     from barney_b200 import synth
-    big = synth.config2(n=96, width=1920, height=1080, spp=256)  # a frame of ~100 ms
+    big = synth.config2(n=96, width=1920, height=1080, spp=256)  # a frame of ~50 ms
     r = bn.VolumeRenderer(big, color_format="rgba8")
     try:
+        r.set_spp(1)
+        r.render()  # the kernels' code is loaded on the first launch of a process
+        r.set_spp(256)
         r.set_timeout(1)
         with pytest.raises(bn.BarneyError) as e:
             r.render()
@@ -59,15 +62,15 @@ def test_batch_deadline_aborts_and_context_recovers():
 
 def test_iteration_cap_ends_runaway_rays_and_sets_the_error_bit():
     # A majorant far above every sample the rays meet: the TF is opaque only
-    # at its last entry, which the field reaches at one voxel in the centre,
-    # so the centre macrocell's majorant is 1e9 times the density rays see
-    # and a ray crossing it would take ~1e8 Woodcock steps.  Each ray stops
+    # at its last entry, which the field reaches at one voxel per macrocell,
+    # so every macrocell's majorant is 1e9 times the density rays see and a
+    # ray crossing one would take ~1e8 Woodcock steps.  Each ray stops
     # at 2^22 steps, as if it left the grid, with error bit 1; the context
     # then renders normally.
     import barney_b200 as bn
     from barney_b200 import synth
     vol = (0.5 * synth.value_noise(24, 3)).astype(np.float32)
-    vol[12, 12, 12] = 1.0
+    vol[4::8, 4::8, 4::8] = 1.0  # one spike in every macrocell
     tf = np.zeros((256, 4), np.float32)
     tf[:, :3] = 0.5
     tf[:, 3] = 1e-9
