@@ -276,12 +276,14 @@ void renderBatch(Context *ctx, const std::vector<BatchEntry> &entries) {
   long long chunks = 0;
   unsigned long long pixelSamples = 0;
   bool extended = false;  // multi-scatter or principled: the extended kernel
+  int voxelType = -2;     // the type every job shares, else -1
   ctx->hostChunks[0] = 0;
   for (int i = 0; i < n; i++) {
     const BatchEntry &e = entries[i];
     JobDD job = buildJob(ctx, *e.r, *e.m, *e.c, *e.fb);
     if (job.fr.spp <= 0) throw Error(E_INVALID_ARG, "every batch job needs pathsPerPixel >= 1");
     extended = extended || job.fr.maxVolumeBounces > 0 || job.v.pv.enabled;
+    voxelType = voxelType == -2 || voxelType == job.v.type ? job.v.type : -1;
     ctx->hostJobs[i] = job;
     chunks += ((long long)job.fr.width * job.fr.height + 31) / 32;
     if (chunks > 0x7fffffffLL) throw Error(E_INVALID_ARG, "batch too large");
@@ -296,6 +298,7 @@ void renderBatch(Context *ctx, const std::vector<BatchEntry> &entries) {
   key.push_back((const void *)(intptr_t)ctx->sched.serviceBatch);
   key.push_back((const void *)(intptr_t)n);
   key.push_back((const void *)(intptr_t)(extended ? 1 : 0));
+  key.push_back((const void *)(intptr_t)voxelType);
   auto enqueue = [&](cudaStream_t s, bool timed) {
     ck(cudaMemcpyAsync(ctx->batchJobs.ptr, ctx->hostJobs, n * sizeof(JobDD), cudaMemcpyHostToDevice, s), "job table");
     ck(cudaMemcpyAsync(ctx->batchChunks.ptr, ctx->hostChunks, (n + 1) * sizeof(int), cudaMemcpyHostToDevice, s),
@@ -303,7 +306,7 @@ void renderBatch(Context *ctx, const std::vector<BatchEntry> &entries) {
     ck(cudaMemsetAsync(ctx->dCounters, 0, sizeof(LaunchCounters), s), "counter reset");
     if (timed) ck(cudaEventRecord(ctx->ev[0], s), "event");
     ck(launchRenderBatch((const JobDD *)ctx->batchJobs.ptr, (const int *)ctx->batchChunks.ptr, n, ctx->dCounters,
-                         ctx->blocksPerSM, ctx->threadsPerBlock, s, ctx->sched, extended),
+                         ctx->blocksPerSM, ctx->threadsPerBlock, s, ctx->sched, extended, voxelType),
        "batch render kernel");
     if (timed) ck(cudaEventRecord(ctx->ev[1], s), "event");
     ck(launchResolveBatch((const JobDD *)ctx->batchJobs.ptr, (const int *)ctx->batchChunks.ptr, n, (int)chunks, s),

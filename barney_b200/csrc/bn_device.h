@@ -115,10 +115,11 @@ cudaError_t launchRender(const VolumeDD &vol, const FrameDD &frame, LaunchCounte
 // jobs / chunkStart: device arrays; chunkStart has numJobs+1 entries, the
 // prefix sum of each job's ceil(width*height/32) pixel chunks.
 // extended: some job has fr.maxVolumeBounces > 0 or a principled volume
-// (selects the kernel instantiation that implements them)
+// (selects the kernel instantiation that implements them); voxelType: the
+// VoxelType all jobs share (a kernel compiled for it) or -1 (mixed)
 cudaError_t launchRenderBatch(const JobDD *jobs, const int *chunkStart, int numJobs, LaunchCounters *counters,
                               int blocksPerSM, int threadsPerBlock, cudaStream_t s, const SchedDD &sd = SchedDD(),
-                              bool extended = false);
+                              bool extended = false, int voxelType = -1);
 cudaError_t launchResolve(const float4 *accum, int numPixels, int accumID, int fmt, void *out, cudaStream_t s,
                           const float4 *comp = nullptr);
 // resolves every job of a batch table into its fr.color after its waves

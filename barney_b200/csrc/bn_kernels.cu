@@ -1200,14 +1200,15 @@ __global__ void __launch_bounds__(kRenderMaxThreads, EXT ? kRenderMinBlocksExt :
   renderLoop<T, false, LOG, EXT>(&job, nullptr, 1, numChunks, sd, ctr, sTF, u8lut);
 }
 
-template <bool EXT>
+// T: the voxel type every job of the batch has, or -1 (mixed: a switch per sample)
+template <int T, bool EXT>
 __global__ void __launch_bounds__(kRenderMaxThreads, EXT ? kRenderMinBlocksExt : kRenderMinBlocks)
     renderBatchKernel(const JobDD *jobs, const int *chunkStart, int numJobs, const __grid_constant__ SchedDD sd,
                       LaunchCounters *ctr) {
   __shared__ float u8lut[256];
   for (int i = threadIdx.x; i < 256; i += blockDim.x) u8lut[i] = (float)i * 1.f / 255.f;
   __syncthreads();
-  renderLoop<-1, true, 2, EXT>(jobs, chunkStart, numJobs, __ldg(chunkStart + numJobs), sd, ctr, nullptr, u8lut);
+  renderLoop<T, true, 2, EXT>(jobs, chunkStart, numJobs, __ldg(chunkStart + numJobs), sd, ctr, nullptr, u8lut);
 }
 
 // ---------------------------------------------------------------------------
@@ -1368,10 +1369,22 @@ cudaError_t launchRender(const VolumeDD &v, const FrameDD &fr, LaunchCounters *c
   }
 }
 
+template <bool EXT>
+static auto batchKernelFor(int voxelType) {
+  switch (voxelType) {
+  case VOX_F32: return renderBatchKernel<VOX_F32, EXT>;
+  case VOX_U8: return renderBatchKernel<VOX_U8, EXT>;
+  case VOX_F16: return renderBatchKernel<VOX_F16, EXT>;
+  case VOX_U16: return renderBatchKernel<VOX_U16, EXT>;
+  case VOX_BF16: return renderBatchKernel<VOX_BF16, EXT>;
+  default: return renderBatchKernel<-1, EXT>;
+  }
+}
+
 cudaError_t launchRenderBatch(const JobDD *jobs, const int *chunkStart, int numJobs, LaunchCounters *ctr, int bps,
-                              int tpb, cudaStream_t s, const SchedDD &sd, bool extended) {
+                              int tpb, cudaStream_t s, const SchedDD &sd, bool extended, int voxelType) {
   if (tpb <= 0) tpb = 128;
-  auto kern = extended ? renderBatchKernel<true> : renderBatchKernel<false>;
+  auto kern = extended ? batchKernelFor<true>(voxelType) : batchKernelFor<false>(voxelType);
   if (bps <= 0) {
     int occ = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, tpb, 0) != cudaSuccess)

@@ -49,6 +49,9 @@ def parse():
     p.add_argument("--rates", default="50,200,500,1000,2000", help="config 5: arrival rates (req/s)")
     p.add_argument("--dtype", default=None, help="storage type for config 3 (f32, f16, u8, bf16)")
     p.add_argument("--spp", type=int, default=None)
+    p.add_argument("--phase", default="hg", choices=["hg", "simple"],
+                   help="configs 2/3: hg = the multi-scatter build's HGPhase (albedo 0.8); "
+                        "simple = Barney's default build, SimplePhase (0.7 x TF colour)")
     p.add_argument("--max-volume-bounces", type=int, default=0,
                    help="configs 2/3: multi-scatter build with up to this many volume bounces")
     p.add_argument("--e2e-steps", type=int, default=None)
@@ -80,11 +83,15 @@ def workload(args, xp, device):
     vol = synth.to_storage(synth.value_noise(n, 0, xp=xp, device=device), dtype)
     d = synth.config2(vol=vol, dtype=dtype, spp=args.spp or (64 if args.config == "2" else 256))
     scatter = "HG single scatter"
+    if args.phase == "simple":
+        d["phase"] = "simple"
+        scatter = "SimplePhase single scatter (default build)"
     if args.max_volume_bounces > 0:
         d["max_volume_bounces"] = args.max_volume_bounces
         scatter = f"HG multi-scatter (up to {args.max_volume_bounces} volume bounces)"
     desc = {"workload": f"{n}^3 {dtype} 6-octave value noise (seed 0), 8^3 macrocells, 1920x1080, {d['spp']} spp, "
-                        f"256-entry knot TF (seed 1) density 50, {scatter} albedo 0.8, "
+                        f"256-entry knot TF (seed 1) density 50, {scatter}"
+                        f"{'' if args.phase == 'simple' else ' albedo 0.8'}, "
                         "dir light + ambient 0.25",
             "volume": f"{n}^3 {dtype}", "image": [1920, 1080], "spp": d["spp"]}
     return d, desc

@@ -269,3 +269,21 @@ def test_anari_structured_regular_field_renders_like_native_calls():
         ctx.close()
     ref, _ = gpu_render(dict(d, density=dens), 2)
     assert_bitexact(img, ref, "ANARI-mapped field vs native calls")
+
+
+@pytest.mark.parametrize("w,h", [(1, 1), (1, 37), (37, 1), (5, 9), (33, 7)])
+def test_degenerate_frame_shapes(w, h):
+    # single pixels, single rows / columns and heights that end in a partial
+    # 4-row band exercise the chunk and band arithmetic of the pixel order
+    d = small_noise_scene(w=w, h=h)
+    img, st = gpu_render(d, 3)
+    ref, _, ost = oracle_render(d, 3)
+    assert_bitexact(img, ref, f"{w}x{h}")
+    assert st["rays"] == ost["rays"]
+
+
+def test_long_accumulation_in_a_thin_frame():
+    d = small_blob_scene(w=3, h=11, bg_color=(0, 0, 0, -1))
+    img, _ = gpu_render(d, 7, renders=3)  # accumIDs 0..20
+    ref, _, _ = oracle_render(d, 21)
+    assert_bitexact(img, ref, "3 x 7 waves")
