@@ -275,14 +275,14 @@ void renderBatch(Context *ctx, const std::vector<BatchEntry> &entries) {
   std::vector<const void *> key;
   long long chunks = 0;
   unsigned long long pixelSamples = 0;
-  bool extended = false;  // multi-scatter or principled: the extended kernel
+  bool extended = false;  // multi-scatter, principled or exact log: the extended kernel
   int voxelType = -2;     // the type every job shares, else -1
   ctx->hostChunks[0] = 0;
   for (int i = 0; i < n; i++) {
     const BatchEntry &e = entries[i];
     JobDD job = buildJob(ctx, *e.r, *e.m, *e.c, *e.fb);
     if (job.fr.spp <= 0) throw Error(E_INVALID_ARG, "every batch job needs pathsPerPixel >= 1");
-    extended = extended || job.fr.maxVolumeBounces > 0 || job.v.pv.enabled;
+    extended = extended || job.fr.maxVolumeBounces > 0 || job.v.pv.enabled || job.fr.exactLog;
     voxelType = voxelType == -2 || voxelType == job.v.type ? job.v.type : -1;
     ctx->hostJobs[i] = job;
     chunks += ((long long)job.fr.width * job.fr.height + 31) / 32;

@@ -114,8 +114,9 @@ cudaError_t launchRender(const VolumeDD &vol, const FrameDD &frame, LaunchCounte
                          int threadsPerBlock, cudaStream_t s, const SchedDD &sd = SchedDD());
 // jobs / chunkStart: device arrays; chunkStart has numJobs+1 entries, the
 // prefix sum of each job's ceil(width*height/32) pixel chunks.
-// extended: some job has fr.maxVolumeBounces > 0 or a principled volume
-// (selects the kernel instantiation that implements them); voxelType: the
+// extended: some job has fr.maxVolumeBounces > 0, a principled volume or
+// exact-log free flight (selects the kernel instantiation that implements
+// them); voxelType: the
 // VoxelType all jobs share (a kernel compiled for it) or -1 (mixed)
 cudaError_t launchRenderBatch(const JobDD *jobs, const int *chunkStart, int numJobs, LaunchCounters *counters,
                               int blocksPerSM, int threadsPerBlock, cudaStream_t s, const SchedDD &sd = SchedDD(),

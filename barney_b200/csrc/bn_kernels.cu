@@ -659,7 +659,7 @@ __device__ __noinline__ void principledAtHit(const VolumeDD &v, float3 P, const 
 constexpr int kMaxPathDepth = 10;
 
 template <int T, bool BATCH, int LOG, bool EXT>
-DEV void renderLoop(const JobDD *jobs, const int *chunkStart, int numJobs, int numChunks, const SchedDD &sd,
+DEV void renderLoop(const JobDD *__restrict__ jobs, const int *__restrict__ chunkStart, int numJobs, int numChunks, const SchedDD &sd,
                     LaunchCounters *ctr, const float4 *sTF, const float *u8lut) {
   const unsigned FULL = 0xffffffffu;
   const int lane = threadIdx.x & 31;
@@ -1203,12 +1203,15 @@ __global__ void __launch_bounds__(kRenderMaxThreads, EXT ? kRenderMinBlocksExt :
 // T: the voxel type every job of the batch has, or -1 (mixed: a switch per sample)
 template <int T, bool EXT>
 __global__ void __launch_bounds__(kRenderMaxThreads, EXT ? kRenderMinBlocksExt : kRenderMinBlocks)
-    renderBatchKernel(const JobDD *jobs, const int *chunkStart, int numJobs, const __grid_constant__ SchedDD sd,
+    renderBatchKernel(const JobDD *__restrict__ jobs, const int *__restrict__ chunkStart, int numJobs, const __grid_constant__ SchedDD sd,
                       LaunchCounters *ctr) {
   __shared__ float u8lut[256];
   for (int i = threadIdx.x; i < 256; i += blockDim.x) u8lut[i] = (float)i * 1.f / 255.f;
   __syncthreads();
-  renderLoop<T, true, 2, EXT>(jobs, chunkStart, numJobs, __ldg(chunkStart + numJobs), sd, ctr, nullptr, u8lut);
+  // plain batch kernels draw free-flight distances with fastLog only; batches
+  // with an exact-log job run the extended kernel, which chooses per job
+  renderLoop<T, true, EXT ? 2 : 0, EXT>(jobs, chunkStart, numJobs, __ldg(chunkStart + numJobs), sd, ctr, nullptr,
+                                        u8lut);
 }
 
 // ---------------------------------------------------------------------------
