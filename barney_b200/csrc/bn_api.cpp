@@ -654,6 +654,8 @@ BN_API void bnFrameBufferResize(BNFrameBuffer fbh, BNDataType fmt, int sx, int s
   default: throw Error(E_UNSUPPORTED, "unsupported frame buffer colour format");
   }
   if (sx <= 0 || sy <= 0) throw Error(E_INVALID_ARG, "frame buffer size must be positive");
+  if ((long long)sx * sy > kMaxFramePixels)  // the kernels index pixels and chunks with 32-bit ints
+    throw Error(E_INVALID_ARG, "frame buffer larger than 2^31 - 1 pixels");
   if (!(channels & BN_FB_COLOR)) throw Error(E_UNSUPPORTED, "the colour channel is required");
   fb->width = sx;
   fb->height = sy;
@@ -775,6 +777,8 @@ BN_API int bnxRenderStructuredNoAlloc(const BNXNoAllocFrame *f, void *stream) {
   if (f->numTFValues < 2 || f->numTFValues > kMaxTF) throw Error(E_INVALID_ARG, "numTFValues must be in [2, 4096]");
   if (f->width <= 0 || f->height <= 0 || f->pathsPerPixel <= 0 || f->accumID < 0)
     throw Error(E_INVALID_ARG, "width, height and pathsPerPixel must be positive, accumID >= 0");
+  if ((long long)f->width * f->height > kMaxFramePixels)
+    throw Error(E_INVALID_ARG, "frame larger than 2^31 - 1 pixels");
   if (f->numDirLights < 0 || f->numDirLights > kMaxDirLights || (f->numDirLights && !f->dirLights))
     throw Error(E_INVALID_ARG, "numDirLights must be in [0, 16] with a host array of lights");
   int mc[3];

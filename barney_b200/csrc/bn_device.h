@@ -15,6 +15,7 @@ enum ErrorBits : unsigned { ERR_ITER_CAP = 1u, ERR_ABORTED = 2u };
 constexpr int kMaxDirLights = 16;
 constexpr int kMaxTF = 4096;
 constexpr int kCellsPerMC = 8;  // StructuredData.cu:26
+constexpr long long kMaxFramePixels = 0x7fffffffLL;  // pixels of one frame (32-bit pixel / chunk indices)
 constexpr int kPartTileChunks = 32;    // pixel-tile partition: 32 chunks of 32 pixels per tile
 constexpr int kRenderMaxThreads = 128;  // __launch_bounds__ of the render kernels:
 constexpr int kRenderMinBlocks = 6;     // plain: 6 x 128 threads per SM (at most 85 registers)

@@ -432,6 +432,7 @@ BN_API long long bnxServerSubmit(BNXServer server, const BNXRequest *q) {
   cam->commit();
   r->camera = cam;
   if (q->width <= 0 || q->height <= 0 || q->spp <= 0) throw Error(E_INVALID_ARG, "width, height, spp must be > 0");
+  if ((long long)q->width * q->height > kMaxFramePixels) throw Error(E_INVALID_ARG, "frame larger than 2^31 - 1 pixels");
   const int fmt = q->colorFormat == BN_FLOAT4 ? FMT_FLOAT4 : q->colorFormat == BN_UFIXED8_RGBA ? FMT_RGBA8
                 : q->colorFormat == BN_UFIXED8_RGBA_SRGB ? FMT_RGBA8_SRGB : -1;
   if (fmt < 0) throw Error(E_UNSUPPORTED, "unsupported colour format");

@@ -5,6 +5,7 @@ import os
 import re
 import subprocess
 
+import numpy as np
 import pytest
 
 import barney_b200 as bn
@@ -95,3 +96,27 @@ def test_header_compiles_as_c_and_shim_as_cpp(tmp_path):
     subprocess.run(["g++", "-std=c++17", "-I", os.path.join(ROOT, "include"), str(cpp_src), "-L", lib_dir,
                     "-lbarney_b200", "-Wl,-rpath," + lib_dir, "-o", str(tmp_path / "client")], check=True)
     subprocess.run([str(tmp_path / "client")], check=True)
+
+
+def test_frame_sizes_beyond_32_bit_pixel_indices_are_rejected_without_a_gpu():
+    # the no-allocation entry point validates its frame description before any
+    # device work: a frame of more than 2^31 - 1 pixels is an argument error
+    from tests.test_zz_no_alloc import BNXNoAllocFrame
+    L = bn.lib()
+    L.bnClearLastError()
+    f = BNXNoAllocFrame()
+    f.voxelType = bn.BN_FLOAT32
+    # non-null stand-ins: validation rejects the frame before any pointer is used
+    f.voxels = f.transferFunction = f.accum = f.color = 256
+    f.dims[:] = (8, 8, 8)
+    f.numTFValues = 2
+    f.width, f.height, f.pathsPerPixel = 65536, 65536, 1
+    f.colorFormat = bn.BN_FLOAT4
+    rc = L.bnxRenderStructuredNoAlloc(ctypes.byref(f), None)
+    assert rc == 2 and L.bnGetLastError() == 2
+    assert b"2^31" in L.bnGetLastErrorString()
+    L.bnClearLastError()
+    owners = np.zeros(1, np.int32)
+    L.bnxPixelPartitionOwners(0, 5, 1, owners.ctypes.data)  # empty frame
+    assert L.bnGetLastError() == 2
+    L.bnClearLastError()
