@@ -1027,8 +1027,10 @@ DEV void renderLoop(const JobDD *__restrict__ jobs, const int *__restrict__ chun
       if (phase == LP_NEWSAMPLE) {
         const int W = fr.width, H = fr.height;
         const int accumID = fr.accumID0 + k;
-        uint64_t rnd = rngSeed2(unsigned(ix + W * accumID), unsigned(iy + H * accumID));
-        raySeed = rngSeed2((uint32_t)(ix + accumID * W), (uint32_t)iy);
+        // 32-bit wrap-around arithmetic, as the reference's ints do on the GPU
+        const unsigned uAcc = (unsigned)accumID;
+        uint64_t rnd = rngSeed2((unsigned)ix + (unsigned)W * uAcc, (unsigned)iy + (unsigned)H * uAcc);
+        raySeed = rngSeed2((unsigned)ix + uAcc * (unsigned)W, (uint32_t)iy);
         const float pixel_u = (accumID == 0) ? .5f : rngFloat(rnd);
         const float pixel_v = (accumID == 0) ? .5f : rngFloat(rnd);
         const float image_u = ((ix + pixel_u) / float(W));

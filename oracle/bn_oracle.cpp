@@ -765,8 +765,10 @@ static PixelSample renderPixelSample(const Scene &sc, int ix, int iy, int accumI
   const int W = s.width, H = s.height;
   PixelSample out{};
   Ray ray;
-  Random2 rand(unsigned(ix + W * accumID), unsigned(iy + H * accumID));
-  ray.rngSeed.seed(ix + accumID * W, iy);
+  // 32-bit wrap-around arithmetic, as the reference's ints do on the GPU
+  const unsigned uAcc = (unsigned)accumID;
+  Random2 rand((unsigned)ix + (unsigned)W * uAcc, (unsigned)iy + (unsigned)H * uAcc);
+  ray.rngSeed.seed((unsigned)ix + uAcc * (unsigned)W, (unsigned)iy);
   float pixel_u = ((accumID == 0) ? .5f : rand());
   float pixel_v = ((accumID == 0) ? .5f : rand());
   float image_u = ((ix + pixel_u) / float(W));
@@ -1072,8 +1074,10 @@ void orc_trace_primary(const OrcScene *s, int ix, int iy, int accumID, int *hit,
   LocalStats st;
   const int W = s->width, H = s->height;
   Ray ray;
-  Random2 rand(unsigned(ix + W * accumID), unsigned(iy + H * accumID));
-  ray.rngSeed.seed(ix + accumID * W, iy);
+  // 32-bit wrap-around arithmetic, as the reference's ints do on the GPU
+  const unsigned uAcc = (unsigned)accumID;
+  Random2 rand((unsigned)ix + (unsigned)W * uAcc, (unsigned)iy + (unsigned)H * uAcc);
+  ray.rngSeed.seed((unsigned)ix + uAcc * (unsigned)W, (unsigned)iy);
   float pixel_u = ((accumID == 0) ? .5f : rand());
   float pixel_v = ((accumID == 0) ? .5f : rand());
   float image_u = ((ix + pixel_u) / float(W));
