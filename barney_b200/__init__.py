@@ -42,7 +42,7 @@ EXPORTS = [
     "bnContextCreate", "bnContextDestroy", "bnPhysicalDeviceCount", "bnRelease", "bnAddReference", "bnCommit",
     "bnSet1i", "bnSet2i", "bnSet3i", "bnSet4i", "bnSet1f", "bnSet2f", "bnSet3f", "bnSet4f", "bnSetObject",
     "bnSetData", "bnDataCreate", "bnTextureData3DCreate", "bnScalarFieldCreate", "bnVolumeCreate",
-    "bnVolumeSetXF", "bnLightCreate", "bnGroupCreate", "bnGroupBuild", "bnModelCreate", "bnSetInstances",
+    "bnVolumeSetXF", "bnLightCreate", "bnGeometryCreate", "bnMaterialCreate", "bnGroupCreate", "bnGroupBuild", "bnModelCreate", "bnSetInstances",
     "bnBuild", "bnCameraCreate", "bnRendererCreate", "bnFrameBufferCreate", "bnFrameBufferResize",
     "bnFrameBufferRead", "bnFrameBufferGetSize", "bnAccumReset", "bnRender", "bnGetLastError",
     "bnGetLastErrorString", "bnClearLastError", "bnxGetStats", "bnxSetStream", "bnxGetStream",
@@ -146,7 +146,8 @@ def lib(build_if_missing=True):
         "bnDataCreate": ([P, I, I, ctypes.c_size_t, P], P),
         "bnTextureData3DCreate": ([P, I, I, I, I, I, P], P), "bnScalarFieldCreate": ([P, I, S], P),
         "bnVolumeCreate": ([P, I, P], P), "bnVolumeSetXF": ([P, bn_float2, P, I, F], None),
-        "bnLightCreate": ([P, I, S], P), "bnGroupCreate": ([P, I, P, I, P, I], P), "bnGroupBuild": ([P], None),
+        "bnLightCreate": ([P, I, S], P), "bnGeometryCreate": ([P, I, S], P), "bnMaterialCreate": ([P, I, S], P),
+        "bnGroupCreate": ([P, I, P, I, P, I], P), "bnGroupBuild": ([P], None),
         "bnModelCreate": ([P], P), "bnSetInstances": ([P, I, P, P, I], None), "bnBuild": ([P, I], None),
         "bnCameraCreate": ([P, S], P), "bnRendererCreate": ([P, S], P), "bnFrameBufferCreate": ([P, I], P),
         "bnFrameBufferResize": ([P, I, I, I, ctypes.c_uint32], None),
@@ -317,8 +318,20 @@ class VolumeRenderer:
                     L.bnSet3f(self.vol, name, *map(float, pv[key]))
         L.bnCommit(self.vol)
         check()
-        vols = (ctypes.c_void_p * 1)(self.vol)
-        self.group = self._keep(L.bnGroupCreate(self.ctx, 0, None, 0, vols, 1))
+        # an isoSurface geometry with a matte material on the same field; with
+        # desc["volume"] False the group holds the isosurface alone
+        geoms, n_geoms = None, 0
+        self.iso = self.material = None
+        if desc.get("iso"):
+            self.material = self._keep(L.bnMaterialCreate(self.ctx, 0, b"matte"))
+            self.iso = self._keep(L.bnGeometryCreate(self.ctx, 0, b"isoSurface"))
+            check()
+            L.bnSetObject(self.iso, b"scalarField", sf)
+            self.set_iso(**desc["iso"])
+            geoms, n_geoms = (ctypes.c_void_p * 1)(self.iso), 1
+        with_vol = desc.get("volume", True)
+        vols = (ctypes.c_void_p * 1)(self.vol) if with_vol else None
+        self.group = self._keep(L.bnGroupCreate(self.ctx, 0, geoms, n_geoms, vols, 1 if with_vol else 0))
         check()
         lights = desc.get("dir_lights", [])
         if lights:
@@ -352,6 +365,22 @@ class VolumeRenderer:
     def _keep(self, h):
         self._objects.append(h)
         return h
+
+    def set_iso(self, value=None, color=None, opacity=None):
+        """Isosurface parameters: iso value; the matte material's "color" (rgb or
+        rgba) and "opacity"."""
+        L = self.L
+        if color is not None:
+            c = tuple(float(x) for x in color)
+            (L.bnSet3f if len(c) == 3 else L.bnSet4f)(self.material, b"color", *c)
+        if opacity is not None:
+            L.bnSet1f(self.material, b"opacity", float(opacity))
+        L.bnCommit(self.material)
+        if value is not None:
+            L.bnSet1f(self.iso, b"isoValue", float(value))
+        L.bnSetObject(self.iso, b"material", self.material)
+        L.bnCommit(self.iso)
+        check()
 
     def set_transfer_function(self, tf, domain, density):
         tf = np.ascontiguousarray(tf, np.float32).reshape(-1, 4)

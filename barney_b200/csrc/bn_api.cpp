@@ -36,23 +36,45 @@ ObjectSP getObject(BNObject h) {
 // ---------------------------------------------------------------------------
 // volume: TF upload, macrocell build (MCVolumeAccel::build, MCAccelerator.h:156-195)
 // ---------------------------------------------------------------------------
-VolumeDD Volume::dd() const {
+// The field part of the device data: voxels, grid and macrocell grid
+// (StructuredData::getDD, buildMCs).
+static VolumeDD fieldDD(const StructuredField &f, const int mcDims[3]) {
   VolumeDD v{};
-  const TextureData &td = *sf->scalars;
+  const TextureData &td = *f.scalars;
   v.voxels = td.buf.ptr;
   v.type = td.type;
   v.numScalars = make_int3(td.dims[0], td.dims[1], td.dims[2]);
-  v.numCells = make_int3(sf->numCells[0], sf->numCells[1], sf->numCells[2]);
-  v.gridOrigin = F3(sf->gridOrigin);
-  v.rcpSpacing = make_float3(1.f / sf->gridSpacing.x, 1.f / sf->gridSpacing.y, 1.f / sf->gridSpacing.z);
-  v.boundsLo = F3(sf->boundsLo);
-  v.boundsHi = F3(sf->boundsHi);
+  v.numCells = make_int3(f.numCells[0], f.numCells[1], f.numCells[2]);
+  v.gridOrigin = F3(f.gridOrigin);
+  v.rcpSpacing = make_float3(1.f / f.gridSpacing.x, 1.f / f.gridSpacing.y, 1.f / f.gridSpacing.z);
+  v.boundsLo = F3(f.boundsLo);
+  v.boundsHi = F3(f.boundsHi);
+  v.mcDims = make_int3(mcDims[0], mcDims[1], mcDims[2]);
+  v.mcOrigin = F3(f.boundsLo);                          // StructuredData.cu:76
+  const v3 mcs = {8.f * f.gridSpacing.x, 8.f * f.gridSpacing.y, 8.f * f.gridSpacing.z};  // :77
+  v.rcpMcSpacing = make_float3(1.f / mcs.x, 1.f / mcs.y, 1.f / mcs.z);
+  return v;
+}
+
+// Checks a field against its texture data; returns its macrocell grid dims
+// (StructuredData.cu:74) and count.
+static size_t macrocellDims(const StructuredField &f, int d[3]) {
+  if (!f.scalars) throw Error(E_STATE, "scalar field has no textureData");
+  const TextureData &td = *f.scalars;
+  for (int a = 0; a < 3; a++)
+    if (f.numScalars[a] != td.dims[a] || f.numScalars[a] < 2)
+      throw Error(E_INVALID_ARG, "structured field 'dims' must match the texture data and be >= 2");
+  for (int a = 0; a < 3; a++) d[a] = (f.numCells[a] + kCellsPerMC - 1) / kCellsPerMC;
+  const size_t n = (size_t)d[0] * d[1] * d[2];
+  if (n > 0x7fffffffull) throw Error(E_INVALID_ARG, "number of macrocells cannot be expressed in 32 bits");
+  return n;
+}
+
+VolumeDD Volume::dd() const {
+  VolumeDD v = fieldDD(*sf, mcDims);
+  v.hasVolume = 1;
   v.majorants = (const float *)majorants.ptr;
   v.mcOccupied = (const unsigned *)occupied.ptr;
-  v.mcDims = make_int3(mcDims[0], mcDims[1], mcDims[2]);
-  v.mcOrigin = F3(sf->boundsLo);                          // StructuredData.cu:76
-  const v3 mcs = {8.f * sf->gridSpacing.x, 8.f * sf->gridSpacing.y, 8.f * sf->gridSpacing.z};  // :77
-  v.rcpMcSpacing = make_float3(1.f / mcs.x, 1.f / mcs.y, 1.f / mcs.z);
   v.tf = (const float4 *)tfBuf.ptr;
   v.tfN = (int)tfValues.size();
   v.domLo = domain[0];
@@ -72,15 +94,9 @@ void Volume::uploadTF() {
 
 void Volume::build() {
   if (!sf || !sf->scalars) throw Error(E_STATE, "volume's scalar field has no textureData");
-  const TextureData &td = *sf->scalars;
-  for (int a = 0; a < 3; a++)
-    if (sf->numScalars[a] != td.dims[a] || sf->numScalars[a] < 2)
-      throw Error(E_INVALID_ARG, "structured field 'dims' must match the texture data and be >= 2");
   if (!built) {
     int d[3];
-    for (int a = 0; a < 3; a++) d[a] = (sf->numCells[a] + kCellsPerMC - 1) / kCellsPerMC;  // StructuredData.cu:74
-    const size_t n = (size_t)d[0] * d[1] * d[2];
-    if (n > 0x7fffffffull) throw Error(E_INVALID_ARG, "number of macrocells cannot be expressed in 32 bits");
+    const size_t n = macrocellDims(*sf, d);
     memcpy(mcDims, d, sizeof d);
     ranges.resize(n * sizeof(float2));
     majorants.resize(n * sizeof(float));
@@ -108,21 +124,80 @@ void Volume::commit() {  // Volume.cpp:26-35
   if (built && needsMajorantRebuild) remapMajorants();
 }
 
+// MCIsoSurfaceAccel::build (MCAccelerator.h:200-230): the field's macrocell
+// scalar ranges, when no volume of the group has built them
+void IsoSurface::buildRanges() {
+  if (!sf) throw Error(E_STATE, "isoSurface has no scalarField");
+  if (rangesOf == sf.get() && rangesTex == sf->scalars.get() && ranges.ptr) return;
+  int d[3];
+  const size_t n = macrocellDims(*sf, d);
+  memcpy(mcDims, d, sizeof d);
+  ranges.resize(n * sizeof(float2));
+  ck(launchBuildMacrocells(fieldDD(*sf, mcDims), (float2 *)ranges.ptr, nullptr, nullptr, 0, ctx->stream),
+     "macrocell range build");
+  rangesOf = sf.get();
+  rangesTex = sf->scalars.get();
+}
+
+// The isosurface part of a job (MCIsoSurfaceAccel::DD with the AnariMatte
+// material's device data): constant parameters read as
+// PossiblyMappedParameter::DD::eval does (HostMaterial.h:98-115), Lambertian
+// albedo .85 * color / pi, alpha color.w * opacity (AnariMatte.h:49-71), the
+// normal's step |bounds size| * .1 / (sum of macrocell dims) (MCAccelerator.h:445-447).
+static IsoDD isoDD(const IsoSurface &g, const float2 *ranges, const int mcDims[3]) {
+  if (!g.material) throw Error(E_STATE, "isoSurface has no material");
+  if (!g.material->committed) throw Error(E_STATE, "isoSurface material has not been committed");
+  IsoDD d{};
+  d.enabled = 1;
+  d.isoValue = g.isoValue;
+  d.ranges = ranges;
+  const Material &m = *g.material;
+  float c[4] = {m.color[0], m.color[1], m.color[2], m.color[3]};
+  if (std::isnan(c[0])) { c[0] = c[1] = c[2] = 0.f; c[3] = 1.f; }
+  const float opacity = std::isnan(m.opacity) ? 0.f : m.opacity;
+  const float reflectance = .85f, oneOverPi = 1.f / (float)M_PI;
+  d.albedo = make_float3(reflectance * c[0] * oneOverPi, reflectance * c[1] * oneOverPi, reflectance * c[2] * oneOverPi);
+  d.alpha = c[3] * opacity;
+  const StructuredField &f = *g.sf;
+  const v3 size = {f.boundsHi.x - f.boundsLo.x, f.boundsHi.y - f.boundsLo.y, f.boundsHi.z - f.boundsLo.z};
+  d.normalDelta = sqrtf(size.x * size.x + size.y * size.y + size.z * size.z) * .1f /
+                  float(mcDims[0] + mcDims[1] + mcDims[2]);
+  return d;
+}
+
 // ---------------------------------------------------------------------------
 // render (Context::renderTiles, Context.cpp:139-182, + finalizeFrame)
 // ---------------------------------------------------------------------------
 // The device job of one (renderer, model, camera, frame buffer) tuple,
 // validated; fr.spp waves starting at the frame buffer's accumID.
 JobDD buildJob(Context *ctx, Renderer &r, Model &m, Camera &cam, FrameBuffer &fb) {
-  if (!m.built || !m.group || !m.group->volume) throw Error(E_STATE, "model has no built volume instance");
+  if (!m.built || !m.group || (!m.group->volume && !m.group->iso))
+    throw Error(E_STATE, "model has no built volume or isosurface instance");
   if (fb.width <= 0 || fb.height <= 0) throw Error(E_STATE, "frame buffer has not been resized");
   if (cam.apertureRadius > 0.f) throw Error(E_UNSUPPORTED, "depth-of-field cameras are not supported");
   const Renderer::Params &p = r.p;
-  Volume &vol = *m.group->volume;
-  vol.build();  // no-op unless the TF changed
   JobDD job{};
   VolumeDD &v = job.v;
-  v = vol.dd();
+  Volume *vol = m.group->volume.get();
+  IsoSurface *iso = m.group->iso.get();
+  if (vol) {
+    vol->build();  // no-op unless the TF changed
+    v = vol->dd();
+  }
+  if (iso) {
+    if (!iso->sf) throw Error(E_STATE, "isoSurface has no scalarField");
+    if (p.emissionAbsorption) throw Error(E_UNSUPPORTED, "isosurfaces do not render in emission-absorption mode");
+    if (vol) {
+      if (iso->sf != vol->sf)
+        throw Error(E_UNSUPPORTED, "an isosurface and a volume of one group must share their scalar field");
+      v.iso = isoDD(*iso, (const float2 *)vol->ranges.ptr, vol->mcDims);
+    } else {
+      iso->buildRanges();
+      v = fieldDD(*iso->sf, iso->mcDims);
+      v.hasVolume = 0;
+      v.iso = isoDD(*iso, (const float2 *)iso->ranges.ptr, iso->mcDims);
+    }
+  }
   v.phase = p.hgPhase ? PHASE_HG : PHASE_SIMPLE;
   FrameDD &fr = job.fr;
   fr.dir00 = F3(cam.dir00);
@@ -275,14 +350,15 @@ void renderBatch(Context *ctx, const std::vector<BatchEntry> &entries) {
   std::vector<const void *> key;
   long long chunks = 0;
   unsigned long long pixelSamples = 0;
-  bool extended = false;  // multi-scatter, principled or exact log: the extended kernel
+  int extended = 0;  // 1: multi-scatter, principled or exact log; 2: isosurfaces (the extended kernels)
   int voxelType = -2;     // the type every job shares, else -1
   ctx->hostChunks[0] = 0;
   for (int i = 0; i < n; i++) {
     const BatchEntry &e = entries[i];
     JobDD job = buildJob(ctx, *e.r, *e.m, *e.c, *e.fb);
     if (job.fr.spp <= 0) throw Error(E_INVALID_ARG, "every batch job needs pathsPerPixel >= 1");
-    extended = extended || job.fr.maxVolumeBounces > 0 || job.v.pv.enabled || job.fr.exactLog;
+    extended = std::max(extended, job.v.iso.enabled ? 2
+                                  : (job.fr.maxVolumeBounces > 0 || job.v.pv.enabled || job.fr.exactLog) ? 1 : 0);
     voxelType = voxelType == -2 || voxelType == job.v.type ? job.v.type : -1;
     ctx->hostJobs[i] = job;
     chunks += ((long long)job.fr.width * job.fr.height + 31) / 32;
@@ -297,7 +373,7 @@ void renderBatch(Context *ctx, const std::vector<BatchEntry> &entries) {
   key.push_back((const void *)(intptr_t)(ctx->blocksPerSM * 4096 + ctx->threadsPerBlock));
   key.push_back((const void *)(intptr_t)ctx->sched.serviceBatch);
   key.push_back((const void *)(intptr_t)n);
-  key.push_back((const void *)(intptr_t)(extended ? 1 : 0));
+  key.push_back((const void *)(intptr_t)extended);
   key.push_back((const void *)(intptr_t)voxelType);
   auto enqueue = [&](cudaStream_t s, bool timed) {
     ck(cudaMemcpyAsync(ctx->batchJobs.ptr, ctx->hostJobs, n * sizeof(JobDD), cudaMemcpyHostToDevice, s), "job table");
@@ -566,22 +642,51 @@ BN_API BNLight bnLightCreate(BNContext context, int, const char *type) {
   BN_CATCH(nullptr)
 }
 
-BN_API BNGroup bnGroupCreate(BNContext context, int, BNGeom *, int numGeoms, BNVolume *volumes, int numVolumes) {
+BN_API BNGeom bnGeometryCreate(BNContext context, int, const char *type) {
   BN_TRY
   Context *c = getContext(context);
-  if (numGeoms != 0) throw Error(E_UNSUPPORTED, "surface geometry is not supported");
-  if (numVolumes != 1 || !volumes) throw Error(E_UNSUPPORTED, "exactly one volume per group is supported");
+  if (!type || std::string(type) != "isoSurface")
+    throw Error(E_UNSUPPORTED, std::string("unsupported geometry type '") + (type ? type : "(null)") +
+                                   "' (only 'isoSurface')");
+  return c->add(std::make_shared<IsoSurface>(c));
+  BN_CATCH(nullptr)
+}
+
+BN_API BNMaterial bnMaterialCreate(BNContext context, int, const char *type) {
+  BN_TRY
+  Context *c = getContext(context);
+  const std::string t = type ? type : "";
+  if (t != "matte" && t != "AnariMatte")  // HostMaterial.cpp:82-95
+    throw Error(E_UNSUPPORTED, "unsupported material type '" + t + "' (only 'matte' / 'AnariMatte')");
+  return c->add(std::make_shared<Material>(c));
+  BN_CATCH(nullptr)
+}
+
+BN_API BNGroup bnGroupCreate(BNContext context, int, BNGeom *geoms, int numGeoms, BNVolume *volumes, int numVolumes) {
+  BN_TRY
+  Context *c = getContext(context);
+  if (numGeoms < 0 || numGeoms > 1 || (numGeoms == 1 && !geoms))
+    throw Error(E_UNSUPPORTED, "at most one (isoSurface) geometry per group is supported");
+  if (numVolumes < 0 || numVolumes > 1 || (numVolumes == 1 && !volumes))
+    throw Error(E_UNSUPPORTED, "at most one volume per group is supported");
+  if (numGeoms + numVolumes == 0) throw Error(E_UNSUPPORTED, "a group needs a volume or an isoSurface");
   auto g = std::make_shared<Group>(c);
-  g->volume = getAs<Volume>(volumes[0], Object::K_VOLUME, "BNVolume");
+  if (numVolumes == 1) g->volume = getAs<Volume>(volumes[0], Object::K_VOLUME, "BNVolume");
+  if (numGeoms == 1) g->iso = getAs<IsoSurface>(geoms[0], Object::K_GEOM, "BNGeom");
   return c->add(g);
   BN_CATCH(nullptr)
+}
+
+static void buildGroup(Group &g) {
+  if (g.volume) g.volume->build();
+  if (g.iso && !(g.volume && g.iso->sf == g.volume->sf)) g.iso->buildRanges();
 }
 
 BN_API void bnGroupBuild(BNGroup group) {
   BN_TRY
   auto g = getAs<Group>(group, Object::K_GROUP, "BNGroup");
   g->ctx->activate();
-  g->volume->build();
+  buildGroup(*g);
   ck(cudaStreamSynchronize(g->ctx->stream), "group build");
   BN_CATCH()
 }
@@ -613,7 +718,7 @@ BN_API void bnBuild(BNModel model, int) {
   BN_TRY
   auto m = getAs<Model>(model, Object::K_MODEL, "BNModel");
   m->ctx->activate();
-  if (m->group && m->group->volume) m->group->volume->build();
+  if (m->group) buildGroup(*m->group);
   ck(cudaStreamSynchronize(m->ctx->stream), "model build");
   m->built = true;
   BN_CATCH()
@@ -789,6 +894,7 @@ BN_API int bnxRenderStructuredNoAlloc(const BNXNoAllocFrame *f, void *stream) {
                                    " macrocells; the no-allocation entry point holds at most " +
                                    std::to_string((long long)kNoAllocMaxMacrocells) + " (a 513^3 grid)");
   VolumeDD v{};
+  v.hasVolume = 1;
   const v3 org = {f->gridOrigin.x, f->gridOrigin.y, f->gridOrigin.z};
   const v3 spc = {f->gridSpacing.x, f->gridSpacing.y, f->gridSpacing.z};
   v.voxels = f->voxels;

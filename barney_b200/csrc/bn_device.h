@@ -20,6 +20,7 @@ constexpr int kPartTileChunks = 32;    // pixel-tile partition: 32 chunks of 32 
 constexpr int kRenderMaxThreads = 128;  // __launch_bounds__ of the render kernels:
 constexpr int kRenderMinBlocks = 6;     // plain: 6 x 128 threads per SM (at most 85 registers)
 constexpr int kRenderMinBlocksExt = 5;  // extended (multi-scatter, principled): 5 x 128 (102)
+constexpr int kRenderMinBlocksIso = 4;  // extended with isosurfaces: 4 x 128 (128)
 
 // Principled volume coefficients evaluated from the field value
 // (PrincipledVolumeParams::DD, PrincipledVolume.h:33-46).
@@ -28,6 +29,18 @@ struct PrincipledDD {
   float density, densityThreshold, densityScale, valueLo, valueHi;
   float emissionStrength, blackbodyIntensity, temperature;
   float3 scatterColor, absorptionColor, emissionColor, blackbodyTint;
+};
+
+// isoSurface geometry on the field (MCIsoSurfaceAccel::DD,
+// MCAccelerator.h:75-123) with an AnariMatte material of constant colour and
+// opacity (AnariMatte.h:49-71).
+struct IsoDD {
+  int enabled;
+  float isoValue;
+  const float2 *ranges;  // macrocell scalar ranges (lo, hi) of the field, mcDims cells
+  float3 albedo;         // Lambertian albedo: .85 * color * (1/pi)
+  float alpha;           // color.w * opacity: below 1 a ray passes the surface with probability 1 - alpha
+  float normalDelta;     // central-difference step of the normal: |bounds size| * .1 / (mcDims.x + .y + .z)
 };
 
 // Structured field + macrocell majorant grid + transfer function
@@ -53,6 +66,8 @@ struct VolumeDD {
   float anisotropy;
   float scatteringAlbedo;
   PrincipledDD pv;
+  int hasVolume;        // 0: the group holds an isosurface on this field and no volume
+  IsoDD iso;
 };
 
 struct DirLightDD {
@@ -106,7 +121,8 @@ struct LaunchCounters {
 };
 
 // launchers (bn_kernels.cu).  Both majorant launchers also write the
-// occupancy bitmap of the new majorants, ceil(n/32) words.
+// occupancy bitmap of the new majorants, ceil(n/32) words; with majorants
+// null, launchBuildMacrocells writes the scalar ranges only.
 cudaError_t launchBuildMacrocells(const VolumeDD &vol, float2 *ranges, float *majorants, unsigned *occupied,
                                   int roundUp, cudaStream_t s);
 cudaError_t launchMapMajorants(const VolumeDD &vol, const float2 *ranges, float *majorants, unsigned *occupied,
@@ -115,13 +131,13 @@ cudaError_t launchRender(const VolumeDD &vol, const FrameDD &frame, LaunchCounte
                          int threadsPerBlock, cudaStream_t s, const SchedDD &sd = SchedDD());
 // jobs / chunkStart: device arrays; chunkStart has numJobs+1 entries, the
 // prefix sum of each job's ceil(width*height/32) pixel chunks.
-// extended: some job has fr.maxVolumeBounces > 0, a principled volume or
-// exact-log free flight (selects the kernel instantiation that implements
-// them); voxelType: the
+// extended: 2 if some job has an isosurface, else 1 if some job has
+// fr.maxVolumeBounces > 0, a principled volume or exact-log free flight,
+// else 0 (selects the kernel instantiation that implements them); voxelType: the
 // VoxelType all jobs share (a kernel compiled for it) or -1 (mixed)
 cudaError_t launchRenderBatch(const JobDD *jobs, const int *chunkStart, int numJobs, LaunchCounters *counters,
                               int blocksPerSM, int threadsPerBlock, cudaStream_t s, const SchedDD &sd = SchedDD(),
-                              bool extended = false, int voxelType = -1);
+                              int extended = 0, int voxelType = -1);
 cudaError_t launchResolve(const float4 *accum, int numPixels, int accumID, int fmt, void *out, cudaStream_t s,
                           const float4 *comp = nullptr);
 // resolves every job of a batch table into its fr.color after its waves

@@ -323,7 +323,7 @@ __global__ void __launch_bounds__(128) mcBuildKernel(VolumeDD v, float2 *ranges,
         }
       }
     ranges[tid] = make_float2(lo, hi);
-    majorants[tid] = roundUpMajorant(mapMajorant(v, lo, hi), roundUp);
+    if (majorants) majorants[tid] = roundUpMajorant(mapMajorant(v, lo, hi), roundUp);
   }
 }
 
@@ -508,14 +508,19 @@ DEV float3 hgSampleDirection(float3 wi_in, float g, uint64_t &random) {
 }
 
 // shadeRays.cu:294-402 restricted to the constant environment and
-// directional lights, N = 0 (volume hit).  Returns false if no light
-// sample; sets lightNeedsMIS / lightIsDirLight.
-DEV bool sampleLights(const FrameDD &fr, uint64_t &random, LightSample &ls, bool &needsMIS, bool &isDir) {
+// directional lights.  N = 0 for a volume hit; SURF instantiations take the
+// front-facing normal N of a surface hit.  Returns false if no light sample;
+// sets lightNeedsMIS / lightIsDirLight.
+template <bool SURF = false>
+DEV bool sampleLights(const FrameDD &fr, uint64_t &random, LightSample &ls, bool &needsMIS, bool &isDir,
+                      float3 N = make_float3(0.f, 0.f, 0.f)) {
   needsMIS = false;
   isDir = false;
-  // sampleEnvLight
-  const float3 eDir = randomDirection(random);
-  const float eRad = kFourPi * fr.ambientRadiance;
+  const bool nZero = !SURF || (N.x == 0.f && N.y == 0.f && N.z == 0.f);
+  // sampleEnvLight: the sphere for N = 0, else the hemisphere about N
+  float3 eDir = randomDirection(random);
+  if (!nZero && dot3(eDir, N) < 0.f) eDir = f3(-eDir.x, -eDir.y, -eDir.z);
+  const float eRad = (nZero ? kFourPi : 2.f * ONE_PI_F) * fr.ambientRadiance;
   float elsWeight = eRad;  // reduce_max of a grey radiance
   float dlsWeight = 0.f;
   float3 dDir = f3(0.f, 0.f, 0.f), dRad = f3(0.f, 0.f, 0.f);
@@ -528,7 +533,8 @@ DEV bool sampleLights(const FrameDD &fr, uint64_t &random, LightSample &ls, bool
       w[i] = 0.f;
       const DirLightDD &L = fr.dirLights[lID[i]];
       float3 rad = f3(L.color.x * L.radiance, L.color.y * L.radiance, L.color.z * L.radiance);
-      float weight = 1.f;
+      float weight = nZero ? 1.f : dot3(L.toLight, N);
+      if (!nZero && weight <= 1e-3f) continue;
       weight *= fmax_(fmax_(rad.x, rad.y), rad.z);
       if (weight <= 1e-3f) continue;
       w[i] = weight;
@@ -560,7 +566,7 @@ DEV bool sampleLights(const FrameDD &fr, uint64_t &random, LightSample &ls, bool
     const float s = 1.f / elsWeight;
     ls.dir = eDir;
     ls.radiance = f3(eRad * s, eRad * s, eRad * s);
-    ls.pdf = kOneOverFourPi;
+    ls.pdf = nZero ? kOneOverFourPi : 1.f / (2.f * ONE_PI_F);
     needsMIS = true;
     return true;
   }
@@ -601,6 +607,150 @@ DEV float sampleJob(const VolumeDD &v, float3 P, const float *u8lut) {
   }
 }
 
+// ---------------------------------------------------------------------------
+// isoSurface geometry (MCIsoSurfaceAccel::isProg, MCAccelerator.h:325-548)
+// ---------------------------------------------------------------------------
+static constexpr float kTwoPi = 2.f * ONE_PI_F;
+static constexpr float kOneOverPi = 1.f / ONE_PI_F;
+static constexpr float kOneOverTwoPi = 1.f / kTwoPi;
+
+// The isosurface's intersection program for one ray: box test, its own RNG
+// derived from the ray's seed (which this advances), a DDA over the
+// macrocell scalar ranges and, in every macrocell whose range holds the iso
+// value, ten linear steps from the cell's entry to its exit, intersecting the
+// first segment whose end values bracket the iso value.  The program reports
+// no intersection to the traversal; it lowers only the ray's own tMax.
+// dir: the ray direction after the zero fix-up; tMax: the ray's tMax.
+// Returns tHit < tMax on a hit, else tMax; *seed is the ray's RNG seed,
+// advanced when the box test passes.
+template <int T>
+DEV float isoIntersect(const VolumeDD &v, float3 org, float3 dir, float tMax, uint64_t *seed,
+                                           const float *u8lut) {
+  float t0 = 0.f, t1 = tMax;
+  if (!boxTest(org, dir, t0, t1, v.boundsLo, v.boundsHi)) return tMax;
+  uint64_t raySeed = *seed;
+  float tHit;
+  const float3 o = f3((org.x - v.mcOrigin.x) * v.rcpMcSpacing.x, (org.y - v.mcOrigin.y) * v.rcpMcSpacing.y,
+                      (org.z - v.mcOrigin.z) * v.rcpMcSpacing.z);
+  const float3 d = f3(dir.x * v.rcpMcSpacing.x, dir.y * v.rcpMcSpacing.y, dir.z * v.rcpMcSpacing.z);
+  uint64_t rng = rngDerive(raySeed, kHash000);  // hash(instance 0, geometry 0, primitive 0)
+  *seed = raySeed;
+  const float iso = v.iso.isoValue;
+  tHit = tMax;
+  // dda3 (DDA.h:61-201), tMax = the box test's t1
+  const float3 rcpd = f3(1.f / d.x, 1.f / d.y, 1.f / d.z);
+  const float3 fs = f3((float)v.mcDims.x, (float)v.mcDims.y, (float)v.mcDims.z);
+  float lx = (0.f - o.x) * rcpd.x, ly = (0.f - o.y) * rcpd.y, lz = (0.f - o.z) * rcpd.z;
+  float hx = (fs.x - o.x) * rcpd.x, hy = (fs.y - o.y) * rcpd.y, hz = (fs.z - o.z) * rcpd.z;
+  float nx = fmin_(lx, hx), ny = fmin_(ly, hy), nz = fmin_(lz, hz);
+  float fx = fmax_(lx, hx), fy = fmax_(ly, hy), fz = fmax_(lz, hz);
+  if (d.x == 0.f) { if (o.x < 0.f || o.x > fs.x) return tMax; nx = -kInf; fx = kInf; }
+  if (d.y == 0.f) { if (o.y < 0.f || o.y > fs.y) return tMax; ny = -kInf; fy = kInf; }
+  if (d.z == 0.f) { if (o.z < 0.f || o.z > fs.z) return tMax; nz = -kInf; fz = kInf; }
+  const float ray_t0 = fmax_(0.f, fmax_(fmax_(nx, ny), nz));
+  const float ray_t1 = fmin_(t1, fmin_(fmin_(fx, fy), fz));
+  if (ray_t0 > ray_t1) return tMax;
+  const float3 oi = f3(o.x + ray_t0 * d.x, o.y + ray_t0 * d.y, o.z + ray_t0 * d.z);
+  const float3 fc = f3(fmax_(0.f, fmin_(fs.x - 1.f, floorf(oi.x))), fmax_(0.f, fmin_(fs.y - 1.f, floorf(oi.y))),
+                       fmax_(0.f, fmin_(fs.z - 1.f, floorf(oi.z))));
+  const float3 fe = f3(d.x > 0.f ? fc.x + 1.f : fc.x, d.y > 0.f ? fc.y + 1.f : fc.y, d.z > 0.f ? fc.z + 1.f : fc.z);
+  const float3 tStep = f3(fabsf(rcpd.x), fabsf(rcpd.y), fabsf(rcpd.z));
+  float3 tNext = f3(d.x == 0.f ? kInf : fabsf(fe.x - oi.x) * tStep.x, d.y == 0.f ? kInf : fabsf(fe.y - oi.y) * tStep.y,
+                    d.z == 0.f ? kInf : fabsf(fe.z - oi.z) * tStep.z);
+  int cx = (int)fc.x, cy = (int)fc.y, cz = (int)fc.z;
+  const int sx = d.x > 0.f ? 1 : -1, sy = d.y > 0.f ? 1 : -1, sz = d.z > 0.f ? 1 : -1;
+  const int ex = d.x > 0.f ? v.mcDims.x : -1, ey = d.y > 0.f ? v.mcDims.y : -1, ez = d.z > 0.f ? v.mcDims.z : -1;
+  float nextCellBegin = 0.f;
+  // every iteration leaves one cell and the grid has < 2^31 cells, so the
+  // loop ends; the bound only guards against a non-finite step
+  for (int iter = 0; iter < (1 << 24); iter++) {
+    const float tClosest = fmin_(fmin_(tNext.x, tNext.y), tNext.z);
+    const float ct0 = ray_t0 + nextCellBegin;
+    const float ct1 = ray_t0 + fmin_(tClosest, t1);
+    // the macrocell callback
+    const float upper = fmin_(ct1, tMax);
+    if (ct0 < upper) {
+      const float2 rg = __ldg(v.iso.ranges + (cx + v.mcDims.x * (cy + v.mcDims.y * cz)));
+      if (iso >= rg.x && iso <= rg.y) {
+        float tt1 = ct0;
+        float ff1 = sampleJob<T>(v, f3(org.x + tt1 * dir.x, org.y + tt1 * dir.y, org.z + tt1 * dir.z), u8lut);
+        bool done = false;
+        for (int i = 1; i <= 10; i++) {
+          const float tt0 = tt1;
+          const float ff0 = ff1;
+          const float fi = (float)i / 10.f;
+          tt1 = (1.f - fi) * ct0 + fi * ct1;
+          ff1 = sampleJob<T>(v, f3(org.x + tt1 * dir.x, org.y + tt1 * dir.y, org.z + tt1 * dir.z), u8lut);
+          if (isnan(ff0) || isnan(ff1)) continue;
+          if (iso >= fmin_(ff0, ff1) && iso <= fmax_(ff0, ff1)) {
+            float t = (iso - ff0) / (ff1 - ff0);
+            t = (1.f - t) * tt0 + t * tt1;
+            tHit = (t < tHit) ? t : tHit;  // a 0/0 segment (NaN) keeps tHit
+            if (tHit < tMax) { done = true; break; }
+          }
+        }
+        if (done) break;
+      }
+    }
+    nextCellBegin = tClosest;
+    if (tNext.x == tClosest) { tNext.x += tStep.x; cx += sx; if (cx == ex) break; }
+    if (tNext.y == tClosest) { tNext.y += tStep.y; cy += sy; if (cy == ey) break; }
+    if (tNext.z == tClosest) { tNext.z += tStep.z; cz += sz; if (cz == ez) break; }
+  }
+  if (!(tHit < tMax)) return tMax;
+  if (v.iso.alpha < 1.f && rngFloat(rng) > v.iso.alpha) return tMax;  // Lambertian::getOpacity
+  return tHit;
+}
+
+// The hit normal (MCAccelerator.h:444-478): central differences over
+// +-normalDelta, one-sided where a neighbour lies outside the field, and
+// -normalize(dir) for a zero gradient; returned normalized and rounded to
+// binary16, as Ray::packNormal stores it.
+template <int T>
+__device__ __noinline__ float3 isoNormal(const VolumeDD &v, float3 P, float3 dir, const float *u8lut) {
+  const float dl = v.iso.normalDelta;
+  const float fP = sampleJob<T>(v, P, u8lut);
+  float fx0 = sampleJob<T>(v, f3(P.x + -dl, P.y + 0.f, P.z + 0.f), u8lut);
+  float fx1 = sampleJob<T>(v, f3(P.x + dl, P.y + 0.f, P.z + 0.f), u8lut);
+  float fy0 = sampleJob<T>(v, f3(P.x + 0.f, P.y + -dl, P.z + 0.f), u8lut);
+  float fy1 = sampleJob<T>(v, f3(P.x + 0.f, P.y + dl, P.z + 0.f), u8lut);
+  float fz0 = sampleJob<T>(v, f3(P.x + 0.f, P.y + 0.f, P.z + -dl), u8lut);
+  float fz1 = sampleJob<T>(v, f3(P.x + 0.f, P.y + 0.f, P.z + dl), u8lut);
+  float dx = 2.f, dy = 2.f, dz = 2.f;
+  if (isnan(fx0)) { dx -= 1.f; fx0 = fP; }
+  if (isnan(fx1)) { dx -= 1.f; fx1 = fP; }
+  if (isnan(fy0)) { dy -= 1.f; fy0 = fP; }
+  if (isnan(fy1)) { dy -= 1.f; fy1 = fP; }
+  if (isnan(fz0)) { dz -= 1.f; fz0 = fP; }
+  if (isnan(fz1)) { dz -= 1.f; fz1 = fP; }
+  float3 n = f3(dx == 0.f ? 0.f : (fx1 - fx0) / dx, dy == 0.f ? 0.f : (fy1 - fy0) / dy, dz == 0.f ? 0.f : (fz1 - fz0) / dz);
+  if (n.x == 0.f && n.y == 0.f && n.z == 0.f) {
+    const float3 dn = normalize3(dir);
+    n = f3(-dn.x, -dn.y, -dn.z);
+  }
+  n = normalize3(n);
+  return f3(roundHalf(n.x), roundHalf(n.y), roundHalf(n.z));
+}
+
+// owl::common::frame(N) (embree's LinearSpace3 frame(): dx from the larger
+// of (0, N.z, -N.y) and (-N.z, 0, N.x), dy = normalize(cross(N, dx))) applied
+// to v: dx * v.x + dy * v.y + N * v.z
+DEV float3 frameXfm(float3 N, float3 v) {
+  const float3 dx0 = f3(0.f, N.z, -N.y);
+  const float3 dx1 = f3(-N.z, 0.f, N.x);
+  const float3 dx = normalize3(dot3(dx0, dx0) > dot3(dx1, dx1) ? dx0 : dx1);
+  const float3 dy = normalize3(cross3(N, dx));
+  return f3(dx.x * v.x + dy.x * v.y + N.x * v.z, dx.y * v.x + dy.y * v.y + N.y * v.z,
+            dx.z * v.x + dy.z * v.y + N.z * v.z);
+}
+
+// Lambertian::pdf (Lambertian.h:45-54): cosine pdf about the normal turned toward wi
+DEV float lambertPdf(float3 Ng, float3 wi) {
+  float3 N = Ng;
+  if (dot3(wi, N) < 0.f) N = f3(-N.x, -N.y, -N.z);
+  return fmax_(dot3(wi, N), 0.f) * kOneOverPi;
+}
+
 // Lane phases of the render loop.
 enum LanePhase : int {
   LP_IDLE = 0,      // no pixel
@@ -614,10 +764,6 @@ enum LanePhase : int {
 
 constexpr int kChunk = 32;  // pixels a warp takes at a time (one 8x4 tile)
 
-// The render loop shared by the single-frame kernel (one job, read from a
-// __grid_constant__ parameter, TF staged in shared memory) and the batch
-// kernel (a job table in global memory, chunks of all jobs in one counter).
-// LOG: 0 fastLog (Volume.h:154-164), 1 -logf (bnx.exactLog), 2 per job (batch)
 // A principled volume's hit in the multi-scatter build (MCAccelerator.h:621-659):
 // tint, scattering albedo and emission from the field value at P (sampled
 // again: it is the collision's value).  Not inlined, so that the render loop
@@ -658,11 +804,121 @@ __device__ __noinline__ void principledAtHit(const VolumeDD &v, float3 P, const 
 // shadeRays.cu:17-41 (MAX_PATH_DEPTH)
 constexpr int kMaxPathDepth = 10;
 
-template <int T, bool BATCH, int LOG, bool EXT>
+// bounce() for a hit on the isosurface (shadeRays.cu:540-878) with the
+// Lambertian BSDF of its AnariMatte material (Lambertian.h:45-86): a shadow
+// ray toward a light sample, weighted by f_r and the surface's cosine, then,
+// within the path depth and the one diffuse bounce allowed
+// (MAX_DIFFUSE_BOUNCES), a cosine-sampled scattered ray.  A sample of pdf 0
+// sends the ray out again unchanged from its own origin (the reference keeps
+// the cleared ray, :757-768).  cosineSampleHemisphere (DG.h:162-168) draws
+// its two numbers in argument order; its sincosf is sincosPortable.  Not
+// inlined, so that the render loop keeps its registers.
+struct SurfaceBounce {
+  uint64_t shadowSeed;  // the shadow ray's RNG seed (the ray's, after its bounce RNG was derived)
+  uint64_t seed;        // the ray's RNG seed after the bounce
+  float3 shadowOrg, shadowTp;
+  float3 lightDir;
+  float shadowMis;
+  float3 scatOrg, scatDir, pathTp;
+  float pathMis;
+  int flags;            // 1 shadow ray, 2 scattered ray, 4 it re-traces the incoming ray, 8 a diffuse bounce
+};
+template <int T>
+__device__ __noinline__ SurfaceBounce surfaceBounce(const VolumeDD &v, const FrameDD &fr, float3 P, float tHit,
+                                                    float3 dirFixed, float3 inOrg, float3 dir, float3 pathTp,
+                                                    uint64_t raySeed, int depth, int nDifB, const float *u8lut) {
+  SurfaceBounce out;
+  out.flags = 0;
+  out.shadowMis = 1.f;
+  out.pathTp = pathTp;
+  out.pathMis = 1.f;
+  uint64_t random = rngDerive(raySeed, (uint64_t)__float_as_uint(tHit));
+  out.shadowSeed = raySeed;
+  const float3 Ng = normalize3(isoNormal<T>(v, P, dirFixed, u8lut));
+  const bool hitWasOnFront = dot3(dir, Ng) < 0.f;
+  const float3 Ngff = hitWasOnFront ? Ng : f3(-Ng.x, -Ng.y, -Ng.z);
+  const float3 won = normalize3(dir);
+  const float3 woN = f3(-won.x, -won.y, -won.z);  // dg.wo
+  const float offsetEpsilon = fmax_(1e-4f, 1e-6f * fmax_(fmax_(fabsf(P.x), fabsf(P.y)), fabsf(P.z)));
+  const float3 alb = v.iso.albedo;
+  LightSample ls;
+  bool needsMIS, isDir;
+  if (sampleLights<true>(fr, random, ls, needsMIS, isDir, Ngff)) {
+    // Lambertian::eval: the cosine against the shading normal, not turned
+    const float cosThetaI = fmax_(dot3(ls.dir, Ng), 0.f);
+    const float fpdf = cosThetaI * kOneOverPi;
+    float3 fv = f3(alb.x * kOneOverPi * cosThetaI, alb.y * kOneOverPi * cosThetaI, alb.z * kOneOverPi * cosThetaI);
+    if (fpdf > 0.f && !(fmax_(fmax_(fv.x, fv.y), fv.z) < 1e-4f)) {
+      fv = f3(fmin_(fv.x, 13.f), fmin_(fv.y, 13.f), fmin_(fv.z, 13.f));
+      const float ip = isinf(ls.pdf) ? 1.f : (1.f / ls.pdf);
+      const float cl = kOneOverPi * fabsf(dot3(Ng, ls.dir));
+      const float3 tp = f3(pathTp.x * ip * fv.x * ls.radiance.x * cl, pathTp.y * ip * fv.y * ls.radiance.y * cl,
+                           pathTp.z * ip * fv.z * ls.radiance.z * cl);
+      // shadowRay.rngSeed = ray.rngSeed; ray.rngSeed.next(tMax)
+      raySeed = (raySeed ^ ((uint64_t)__float_as_uint(tHit) << 1)) * kRngMul;
+      bool alive = true;
+      if (!isDir && needsMIS) {
+        const float pl = kOneOverFourPi;
+        const float ps = lambertPdf(Ng, ls.dir);
+        out.shadowMis = pl / (pl + ps + 1e-10f);
+        if (out.shadowMis < 1e-5f) alive = false;
+      }
+      if (alive && kInf * (1.f - 2.f * offsetEpsilon) > 0.f) {
+        out.shadowTp = f3(roundHalf(tp.x), roundHalf(tp.y), roundHalf(tp.z));
+        out.shadowOrg = f3(P.x + offsetEpsilon * Ngff.x, P.y + offsetEpsilon * Ngff.y, P.z + offsetEpsilon * Ngff.z);
+        out.lightDir = ls.dir;
+        out.flags |= 1;
+      }
+    }
+  }
+  out.seed = raySeed;
+  if (depth >= kMaxPathDepth) return out;
+  // Lambertian::scatter
+  float3 N = Ng;
+  if (dot3(woN, N) < 0.f) N = f3(-N.x, -N.y, -N.z);
+  const float su = rngFloat(random);
+  const float sv = rngFloat(random);
+  const float cosTheta = sqrtf(sv);
+  const float sinTheta = sqrtf(1.0f - sv);
+  float sinPhi, cosPhi;
+  sincosPortable(kTwoPi * su, sinPhi, cosPhi);
+  const float3 local = f3(cosPhi * sinTheta, sinPhi * sinTheta, cosTheta);
+  const float pdf = local.z * kOneOverPi;
+  if (!(pdf > 0.f) || pdf <= 1e-6f) {  // the same ray again, tMax infinite
+    out.scatOrg = inOrg;
+    out.scatDir = dir;
+    out.flags |= 2 | 4;
+    return out;
+  }
+  if (nDifB >= 1) return out;
+  out.scatDir = normalize3(frameXfm(N, local));
+  const float c = fabsf(dot3(Ng, normalize3(out.scatDir)));
+  const float denom = isinf(pdf) ? 1.f : (pdf + 1e-10f);
+  out.pathTp = f3(roundHalf(pathTp.x * fmin_((alb.x * c) / denom, 2.5f)),
+                  roundHalf(pathTp.y * fmin_((alb.y * c) / denom, 2.5f)),
+                  roundHalf(pathTp.z * fmin_((alb.z * c) / denom, 2.5f)));
+  if (needsMIS && !isinf(pdf)) {
+    const float ps = lambertPdf(Ng, out.scatDir);
+    out.pathMis = ps / (ps + kOneOverFourPi);
+  }
+  out.scatOrg = f3(P.x + (1.f * offsetEpsilon) * Ngff.x, P.y + (1.f * offsetEpsilon) * Ngff.y,
+                   P.z + (1.f * offsetEpsilon) * Ngff.z);
+  out.flags |= 2 | 8;
+  return out;
+}
+
+// The render loop shared by the single-frame kernel (one job, read from a
+// __grid_constant__ parameter, TF staged in shared memory) and the batch
+// kernel (a job table in global memory, chunks of all jobs in one counter).
+// LOG: 0 fastLog (Volume.h:154-164), 1 -logf (bnx.exactLog), 2 per job (batch)
+// EXT: 0 the plain kernels; 1 multi-scatter paths and principled volumes;
+// 2 also isosurfaces (ISO)
+template <int T, bool BATCH, int LOG, int EXT>
 DEV void renderLoop(const JobDD *__restrict__ jobs, const int *__restrict__ chunkStart, int numJobs, int numChunks, const SchedDD &sd,
                     LaunchCounters *ctr, const float4 *sTF, const float *u8lut) {
   const unsigned FULL = 0xffffffffu;
   const int lane = threadIdx.x & 31;
+  constexpr bool ISO = EXT >= 2;
 
   // lane work counters, 32-bit, flushed to the launch counters (below)
   unsigned nSamples = 0, nVisits = 0, nRays = 0;
@@ -689,13 +945,15 @@ DEV void renderLoop(const JobDD *__restrict__ jobs, const int *__restrict__ chun
   // EXT (the instantiation for multi-scatter paths and principled volumes;
   // the plain kernels compile neither): the path's throughput, rounded to binary16 like
   // PathState::throughput (Ray.h:17-23); the MIS weight of the path ray; its
-  // generation; the volume bounces taken; and a scattered ray that waits
-  // while its generation's shadow ray is traced (it starts where the shadow
-  // ray starts, in direction primDir, with RNG seed pendSeed)
+  // generation; the volume and diffuse bounces taken; and a scattered ray
+  // that waits while its generation's shadow ray is traced (pend 1: it
+  // starts where the shadow ray starts; pend 2: at the origin kept in hitRGB;
+  // in direction primDir, with RNG seed pendSeed).  A ray that hits the
+  // isosurface carries bit 64 of ts.bits, its hit distance in ts.rayTMax.
   float3 pathTp = f3(1.f, 1.f, 1.f);
   float pathMis = 1.f;
-  int depth = 0, nVolB = 0;
-  bool pend = false;
+  int depth = 0, nVolB = 0, nDifB = 0;
+  int pend = 0;
   uint64_t pendSeed = 0;
 
   // Each round: (A) one service pass over the lanes whose ray needs host
@@ -715,6 +973,11 @@ DEV void renderLoop(const JobDD *__restrict__ jobs, const int *__restrict__ chun
       const JobDD &J = jobs[BATCH ? job : 0];
       const VolumeDD &v = J.v;
       const FrameDD &fr = J.fr;
+      // a ray that left the volume behind its isosurface hit has hit the surface
+      if (ISO && phase == LP_ENDED && (ts.bits & 64)) {
+        ts.t = ts.rayTMax;
+        phase = LP_HIT;
+      }
       // ------------------------------------------------------------------
       // A1. collisions: shading and shadow-ray spawn (shadeRays.cu:608-746)
       // ------------------------------------------------------------------
@@ -722,6 +985,7 @@ DEV void renderLoop(const JobDD *__restrict__ jobs, const int *__restrict__ chun
         const int accumID = fr.accumID0 + k;
         const float clampMax = 10.f * (1 + accumID);
         const bool cmp = fr.comp != nullptr;
+        const bool surf = ISO && (ts.bits & 64);  // the hit is on the isosurface
         bool spawned = false;
         if (!shadowRay) {
           if (!EXT) {  // primary hit: generation-0 accumulation (fragment 0, alpha 1)
@@ -742,7 +1006,7 @@ DEV void renderLoop(const JobDD *__restrict__ jobs, const int *__restrict__ chun
           float hitAlb = v.scatteringAlbedo;
           if (EXT) {
             float3 frag = f3(0.f, 0.f, 0.f);
-            if (v.phase == PHASE_HG && v.pv.enabled && !fr.emissionAbsorption) {
+            if (v.phase == PHASE_HG && v.pv.enabled && !fr.emissionAbsorption && !surf) {
               float3 e;
               principledAtHit<T>(v, P, BATCH ? v.tf : sTF, u8lut, tint, hitAlb, e);
               // emission of the HGPhase hit: incomingThroughput * emission (shadeRays.cu:613-617)
@@ -772,6 +1036,45 @@ DEV void renderLoop(const JobDD *__restrict__ jobs, const int *__restrict__ chun
               if (ex > 0.f) accAdd(acc.x, comp.x, ex, cmp);
               if (ey > 0.f) accAdd(acc.y, comp.y, ey, cmp);
               if (ez > 0.f) accAdd(acc.z, comp.z, ez, cmp);
+            }
+          } else if (ISO && surf) {
+            const SurfaceBounce sb = surfaceBounce<T>(v, fr, P, tHit, ts.dir, ts.org, primDir, pathTp, raySeed, depth,
+                                                      nDifB, u8lut);
+            raySeed = (sb.flags & 1) ? sb.shadowSeed : sb.seed;
+            if (sb.flags & 1) {  // makeShadowRay (Ray.h:147-157)
+              misWeight = sb.shadowMis;
+              shadowTp = sb.shadowTp;
+              ts.org = sb.shadowOrg;
+              ts.dir = sb.lightDir;
+              ts.rayTMax = kInf;
+              shadowRay = true;
+              spawned = true;
+              nRays++;
+              steps = 0;
+              phase = LP_BEGIN;
+            }
+            if (sb.flags & 2) {
+              if (sb.flags & 8) {
+                nDifB++;
+                pathTp = sb.pathTp;
+                pathMis = sb.pathMis;
+              }
+              depth++;
+              primDir = sb.scatDir;
+              if (spawned) {  // after the shadow ray: from its origin, or from the one kept in hitRGB
+                pend = (sb.flags & 4) ? 2 : 1;
+                if (sb.flags & 4) hitRGB = sb.scatOrg;
+                pendSeed = sb.seed;
+              } else {
+                ts.org = sb.scatOrg;
+                ts.dir = primDir;
+                ts.rayTMax = kInf;
+                shadowRay = false;
+                spawned = true;
+                nRays++;
+                steps = 0;
+                phase = LP_BEGIN;
+              }
             }
           } else {
             // bounce() volume-hit branch, shadeRays.cu:608-746
@@ -859,7 +1162,7 @@ DEV void renderLoop(const JobDD *__restrict__ jobs, const int *__restrict__ chun
                   pathMis = 1.f;
                 }
                 if (spawned) {  // after the shadow ray, from the shadow ray's origin
-                  pend = true;
+                  pend = 1;
                   pendSeed = scatSeed;
                 } else {
                   ts.org = f3(P.x + (1.f * offsetEpsilon) * woN.x, P.y + (1.f * offsetEpsilon) * woN.y,
@@ -879,10 +1182,11 @@ DEV void renderLoop(const JobDD *__restrict__ jobs, const int *__restrict__ chun
         }
         if (!spawned) {
           if (EXT && pend) {  // the shadow ray was occluded: the scattered ray goes next
+            if (pend == 2) ts.org = hitRGB;
             ts.dir = primDir;
             ts.rayTMax = kInf;
             raySeed = pendSeed;
-            pend = false;
+            pend = 0;
             shadowRay = false;
             nRays++;
             steps = 0;
@@ -940,10 +1244,11 @@ DEV void renderLoop(const JobDD *__restrict__ jobs, const int *__restrict__ chun
           if (f1z > 0.f) accAdd(acc.z, comp.z, f1z, cmp);
         }
         if (EXT && shadowRay && pend) {  // the scattered ray goes next, from the shadow ray's origin
+          if (pend == 2) ts.org = hitRGB;
           ts.dir = primDir;
           ts.rayTMax = kInf;
           raySeed = pendSeed;
-          pend = false;
+          pend = 0;
           shadowRay = false;
           nRays++;
           steps = 0;
@@ -1062,7 +1367,8 @@ DEV void renderLoop(const JobDD *__restrict__ jobs, const int *__restrict__ chun
           pathMis = 1.f;
           depth = 0;
           nVolB = 0;
-          pend = false;
+          nDifB = 0;
+          pend = 0;
         }
         nRays++;
         steps = 0;
@@ -1075,7 +1381,32 @@ DEV void renderLoop(const JobDD *__restrict__ jobs, const int *__restrict__ chun
       // ------------------------------------------------------------------
       // A5. ray set-up, primary and shadow rays together
       // ------------------------------------------------------------------
-      if (phase == LP_BEGIN) phase = traceBegin(v, ts, ts.org, ts.dir, ts.rayTMax, raySeed) ? LP_CELL : LP_ENDED;
+      if (phase == LP_BEGIN) {
+        if (ISO && v.iso.enabled) {
+          // the traversal calls the isosurface first; its hit lowers only the
+          // ray's own tMax, so the volume's box test and DDA run to the
+          // traversal's tMax while its Woodcock ranges stop at the surface.  A
+          // shadow ray that hits the surface is occluded.
+          const float3 dF = f3(ts.dir.x == 0.f ? 1e-6f : ts.dir.x, ts.dir.y == 0.f ? 1e-6f : ts.dir.y,
+                               ts.dir.z == 0.f ? 1e-6f : ts.dir.z);
+          const float tIso = isoIntersect<T>(v, ts.org, dF, ts.rayTMax, &raySeed, u8lut);
+          const bool isoHit = tIso < ts.rayTMax;
+          if (isoHit && shadowRay) {
+            phase = LP_HIT;
+          } else {
+            const bool inVol = v.hasVolume && traceBegin(v, ts, ts.org, ts.dir, ts.rayTMax, raySeed);
+            ts.dir = dF;
+            ts.bits = isoHit ? (ts.bits | 64) : (ts.bits & ~64);
+            if (isoHit) ts.rayTMax = tIso;
+            if (inVol) phase = LP_CELL;
+            else if (isoHit) { ts.t = tIso; phase = LP_HIT; }
+            else phase = LP_ENDED;
+          }
+        } else {
+          phase = traceBegin(v, ts, ts.org, ts.dir, ts.rayTMax, raySeed) ? LP_CELL : LP_ENDED;
+          if (ISO) ts.bits &= ~64;
+        }
+      }
 
     }
     {
@@ -1098,6 +1429,8 @@ DEV void renderLoop(const JobDD *__restrict__ jobs, const int *__restrict__ chun
               if (!ddaStep(v, ts, tClosest)) { phase = LP_ENDED; break; }
               if (++steps > (1u << 22)) { errBits |= ERR_ITER_CAP; phase = LP_ENDED; break; }
             } else {
+              // no collision can precede a surface hit at or before this cell's start
+              if (ISO && (ts.bits & 64) && ts.rayT0 + ts.nextCellBegin >= ts.rayTMax) { phase = LP_ENDED; break; }
               ts.maj = __ldg(v.majorants + ci);
               ts.t = ts.rayT0 + ts.nextCellBegin;
               ts.tUpper = fmin_(ts.rayT0 + fmin_(tClosest, ts.ddaTMax), ts.rayTMax);
@@ -1139,8 +1472,10 @@ DEV void renderLoop(const JobDD *__restrict__ jobs, const int *__restrict__ chun
               }
             }
             if (w >= rngFloat(ts.rng) * ts.maj) {
-              hitRGB = f3(0.f, 0.f, 0.f);
-              if (!isnan(s) && !((EXT && v.pv.enabled) && tfw <= 0.f)) {
+              if (ISO) ts.bits &= ~64;  // a volume collision before the surface
+              // (with isosurfaces a shadow ray keeps hitRGB: it may hold a waiting ray's origin)
+              if (!(ISO && shadowRay)) hitRGB = f3(0.f, 0.f, 0.f);
+              if (!(ISO && shadowRay) && !isnan(s) && !((EXT && v.pv.enabled) && tfw <= 0.f)) {
                 const float4 a = BATCH ? __ldg(&v.tf[idx]) : sTF[idx];
                 const float4 b = BATCH ? __ldg(&v.tf[idx + 1]) : sTF[idx + 1];
                 hitRGB = f3((1.f - f) * a.x + f * b.x, (1.f - f) * a.y + f * b.y, (1.f - f) * a.z + f * b.z);
@@ -1189,8 +1524,8 @@ __host__ __device__ inline int partitionChunks(int numChunks, int rank, int coun
   return (mine - 1) * kPartTileChunks + min(kPartTileChunks, numChunks - last * kPartTileChunks);
 }
 
-template <int T, int LOG, bool EXT>
-__global__ void __launch_bounds__(kRenderMaxThreads, EXT ? kRenderMinBlocksExt : kRenderMinBlocks)
+template <int T, int LOG, int EXT>
+__global__ void __launch_bounds__(kRenderMaxThreads, EXT >= 2 ? kRenderMinBlocksIso : EXT ? kRenderMinBlocksExt : kRenderMinBlocks)
     renderKernel(const __grid_constant__ JobDD job, const __grid_constant__ SchedDD sd, LaunchCounters *ctr) {
   extern __shared__ float4 sTF[];
   __shared__ float u8lut[256];
@@ -1203,8 +1538,8 @@ __global__ void __launch_bounds__(kRenderMaxThreads, EXT ? kRenderMinBlocksExt :
 }
 
 // T: the voxel type every job of the batch has, or -1 (mixed: a switch per sample)
-template <int T, bool EXT>
-__global__ void __launch_bounds__(kRenderMaxThreads, EXT ? kRenderMinBlocksExt : kRenderMinBlocks)
+template <int T, int EXT>
+__global__ void __launch_bounds__(kRenderMaxThreads, EXT >= 2 ? kRenderMinBlocksIso : EXT ? kRenderMinBlocksExt : kRenderMinBlocks)
     renderBatchKernel(const JobDD *__restrict__ jobs, const int *__restrict__ chunkStart, int numJobs, const __grid_constant__ SchedDD sd,
                       LaunchCounters *ctr) {
   __shared__ float u8lut[256];
@@ -1328,7 +1663,8 @@ cudaError_t launchBuildMacrocells(const VolumeDD &v, float2 *ranges, float *majo
   default: mcBuildKernel<VOX_BF16><<<blocks, 128, 0, s>>>(v, ranges, majorants, roundUp); break;
   }
   cudaError_t e = cudaGetLastError();
-  return e != cudaSuccess ? e : launchOccupancy(majorants, n, occupied, s);
+  if (e != cudaSuccess || !majorants) return e;
+  return launchOccupancy(majorants, n, occupied, s);
 }
 
 cudaError_t launchMapMajorants(const VolumeDD &v, const float2 *ranges, float *majorants, unsigned *occupied,
@@ -1344,9 +1680,10 @@ template <int T>
 static cudaError_t launchRenderT(const VolumeDD &v, const FrameDD &fr, const SchedDD &sd, LaunchCounters *ctr,
                                  int bps, int tpb, cudaStream_t s) {
   const size_t smem = (size_t)v.tfN * sizeof(float4);
-  const bool ext = fr.maxVolumeBounces > 0 || v.pv.enabled;
-  auto kern = ext ? (fr.exactLog ? renderKernel<T, 1, true> : renderKernel<T, 0, true>)
-                  : (fr.exactLog ? renderKernel<T, 1, false> : renderKernel<T, 0, false>);
+  const int ext = v.iso.enabled ? 2 : (fr.maxVolumeBounces > 0 || v.pv.enabled) ? 1 : 0;
+  auto kern = ext == 2   ? (fr.exactLog ? renderKernel<T, 1, 2> : renderKernel<T, 0, 2>)
+              : ext == 1 ? (fr.exactLog ? renderKernel<T, 1, 1> : renderKernel<T, 0, 1>)
+                         : (fr.exactLog ? renderKernel<T, 1, 0> : renderKernel<T, 0, 0>);
   if (smem > 48 * 1024 &&
       cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
     return cudaGetLastError();
@@ -1374,7 +1711,7 @@ cudaError_t launchRender(const VolumeDD &v, const FrameDD &fr, LaunchCounters *c
   }
 }
 
-template <bool EXT>
+template <int EXT>
 static auto batchKernelFor(int voxelType) {
   switch (voxelType) {
   case VOX_F32: return renderBatchKernel<VOX_F32, EXT>;
@@ -1387,9 +1724,11 @@ static auto batchKernelFor(int voxelType) {
 }
 
 cudaError_t launchRenderBatch(const JobDD *jobs, const int *chunkStart, int numJobs, LaunchCounters *ctr, int bps,
-                              int tpb, cudaStream_t s, const SchedDD &sd, bool extended, int voxelType) {
+                              int tpb, cudaStream_t s, const SchedDD &sd, int extended, int voxelType) {
   if (tpb <= 0) tpb = 128;
-  auto kern = extended ? batchKernelFor<true>(voxelType) : batchKernelFor<false>(voxelType);
+  auto kern = extended >= 2 ? batchKernelFor<2>(voxelType)
+              : extended    ? batchKernelFor<1>(voxelType)
+                            : batchKernelFor<0>(voxelType);
   if (bps <= 0) {
     int occ = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, tpb, 0) != cudaSuccess)
@@ -1416,7 +1755,7 @@ cudaError_t launchResolve(const float4 *accum, int n, int accumID, int fmt, void
 
 int renderKernelMaxBlocksPerSM(int tpb) {
   int occ = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, renderKernel<VOX_F32, 0, false>, tpb, 256 * sizeof(float4)) !=
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, renderKernel<VOX_F32, 0, 0>, tpb, 256 * sizeof(float4)) !=
       cudaSuccess) {
     cudaGetLastError();
     return 1;

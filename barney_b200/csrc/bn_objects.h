@@ -86,7 +86,8 @@ struct Context;
 // objects (Object.h:42-56 set/commit interface)
 // ---------------------------------------------------------------------------
 struct Object : std::enable_shared_from_this<Object> {
-  enum Kind { K_DATA, K_TEXDATA, K_FIELD, K_VOLUME, K_GROUP, K_MODEL, K_LIGHT, K_CAMERA, K_RENDERER, K_FB };
+  enum Kind { K_DATA, K_TEXDATA, K_FIELD, K_VOLUME, K_GROUP, K_MODEL, K_LIGHT, K_CAMERA, K_RENDERER, K_FB, K_GEOM,
+              K_MATERIAL };
   Context *ctx;
   Kind kind;
   Object(Context *c, Kind k) : ctx(c), kind(k) {}
@@ -204,6 +205,63 @@ struct Volume : Object {
   void commit() override;
 };
 
+// AnariMatte (AnariMatte.h:15-46, AnariMatte.cpp:40-90) with constant
+// parameters: "color" (float3 gives alpha 1, float4) and "opacity" (float).
+// Sampler- and attribute-mapped parameters are not supported.
+struct Material : Object {
+  float color[4] = {.8f, .8f, .8f, 1.f};
+  float opacity = 1.f;
+  bool committed = false;  // HostMaterial::hasBeenCommittedAtLeastOnce
+  explicit Material(Context *c) : Object(c, K_MATERIAL) {}
+  bool set1f(const std::string &m, float v) override {
+    if (m == "opacity") { opacity = v; return true; }
+    return false;
+  }
+  bool set3f(const std::string &m, float x, float y, float z) override {
+    if (m == "color") { color[0] = x; color[1] = y; color[2] = z; color[3] = 1.f; return true; }
+    return false;
+  }
+  bool set4f(const std::string &m, float x, float y, float z, float w) override {
+    if (m == "color") { color[0] = x; color[1] = y; color[2] = z; color[3] = w; return true; }
+    return false;
+  }
+  void commit() override { committed = true; }
+};
+
+// isoSurface geometry (IsoSurface.h:27-80, IsoSurface.cpp:36-90): an iso
+// value on a structured scalar field, drawn with a material.
+struct IsoSurface : Object {
+  float isoValue = NAN;
+  std::shared_ptr<StructuredField> sf;
+  std::shared_ptr<Material> material;
+  // macrocell scalar ranges of the field, built when no volume of the group
+  // provides them (StructuredData::buildMCs, StructuredData.cu:71-96)
+  DeviceBuffer ranges;
+  int mcDims[3] = {0, 0, 0};
+  const StructuredField *rangesOf = nullptr;  // the field (and its texture) the ranges were built for
+  const TextureData *rangesTex = nullptr;
+  explicit IsoSurface(Context *c) : Object(c, K_GEOM) {}
+  bool set1i(const std::string &m, int) override { return m == "userID"; }
+  bool set1f(const std::string &m, float v) override {
+    if (m == "isoValue") { isoValue = v; return true; }
+    return false;
+  }
+  bool setObject(const std::string &m, const ObjectSP &v) override {
+    if (m == "scalarField") {
+      if (!v || v->kind != K_FIELD) throw Error(E_INVALID_ARG, "'scalarField' value set on 'isoSurface' is not a scalar field");
+      sf = std::static_pointer_cast<StructuredField>(v);
+      return true;
+    }
+    if (m == "material") {
+      if (v && v->kind != K_MATERIAL) throw Error(E_INVALID_ARG, "invalid material in geometry::set(\"material\")");
+      material = v ? std::static_pointer_cast<Material>(v) : nullptr;
+      return true;
+    }
+    return false;
+  }
+  void buildRanges();
+};
+
 struct DirLight : Object {
   v3 direction{0.f, 0.f, -1.f};  // DirLight.h:37
   float irradiance = NAN;
@@ -241,7 +299,8 @@ struct DirLight : Object {
 };
 
 struct Group : Object {
-  std::shared_ptr<Volume> volume;
+  std::shared_ptr<Volume> volume;     // at most one volume
+  std::shared_ptr<IsoSurface> iso;    // at most one isosurface geometry
   std::shared_ptr<Data> lights;
   explicit Group(Context *c) : Object(c, K_GROUP) {}
 };

@@ -58,6 +58,8 @@ class OrcScene(ctypes.Structure):
         ("pTemperature", ctypes.c_float),
         ("pScatterColor", ctypes.c_float * 3), ("pAbsorptionColor", ctypes.c_float * 3),
         ("pEmissionColor", ctypes.c_float * 3), ("pBlackbodyTint", ctypes.c_float * 3),
+        ("iso", ctypes.c_int), ("isoValue", ctypes.c_float), ("isoColor", ctypes.c_float * 4),
+        ("isoOpacity", ctypes.c_float), ("noVolume", ctypes.c_int),
         ("width", ctypes.c_int),
         ("height", ctypes.c_int),
     ]
@@ -109,6 +111,8 @@ def lib():
         L.orc_expp.argtypes = [I, P, P]
         L.orc_blackbody.argtypes = [F, P]
         L.orc_hg_sample.argtypes = [P, F, U64, I, P]
+        L.orc_iso_trace.argtypes = [P, P, P, F, U64, P, P, P]
+        L.orc_frame_xfm.argtypes = [P, P, P]
         _lib = L
     return _lib
 
@@ -131,6 +135,17 @@ def principled_params(p):
                     ("emission_color", (1.0, 1.0, 1.0)), ("blackbody_tint", (1.0, 1.0, 1.0))):
         out[k] = tuple(max(float(x), 0.0) for x in p.get(k, dflt))
     return out
+
+
+def iso_params(p):
+    """Isosurface parameters: iso value and the AnariMatte material's constant
+    color (rgb gives alpha 1) and opacity (AnariMatte.h:44-45 defaults .8 / 1)."""
+    if not p:
+        return {"enabled": 0, "value": 0.0, "color": (0.8, 0.8, 0.8, 1.0), "opacity": 1.0}
+    c = tuple(float(x) for x in p.get("color", (0.8, 0.8, 0.8)))
+    if len(c) == 3:
+        c = c + (1.0,)
+    return {"enabled": 1, "value": float(p["value"]), "color": c, "opacity": float(p.get("opacity", 1.0))}
 
 
 def _ptr(a):
@@ -185,6 +200,12 @@ class Scene:
         s.pTemperature = pv["temperature"]
         s.pScatterColor[:], s.pAbsorptionColor[:] = pv["scatter_color"], pv["absorption_color"]
         s.pEmissionColor[:], s.pBlackbodyTint[:] = pv["emission_color"], pv["blackbody_tint"]
+        iso = iso_params(desc.get("iso"))
+        s.iso = iso["enabled"]
+        s.isoValue = iso["value"]
+        s.isoColor[:] = iso["color"]
+        s.isoOpacity = iso["opacity"]
+        s.noVolume = 0 if desc.get("volume", True) else 1
         s.width, s.height = desc["width"], desc["height"]
         self.s = s
 
@@ -259,6 +280,25 @@ def hg_sample(wi, g, seed_state, n):
     wi = np.ascontiguousarray(wi, np.float32)
     out = np.empty((n, 3), np.float32)
     lib().orc_hg_sample(_ptr(wi), g, seed_state, n, _ptr(out))
+    return out
+
+
+def iso_trace(sc, org, dir, tmax=1e30, seed_state=0xcafef00dd15ea5e5):
+    """One ray against the scene's isosurface: (hit, t, stored normal)."""
+    org = np.ascontiguousarray(org, np.float32)
+    dir = np.ascontiguousarray(dir, np.float32)
+    hit, t = ctypes.c_int(0), ctypes.c_float(0.0)
+    n = np.zeros(3, np.float32)
+    lib().orc_iso_trace(sc.ref, _ptr(org), _ptr(dir), tmax, seed_state, ctypes.byref(hit), ctypes.byref(t), _ptr(n))
+    return bool(hit.value), t.value, n
+
+
+def frame_xfm(N, v):
+    """owl::common::frame(N) applied to v (the Lambertian's local-to-world map)."""
+    N = np.ascontiguousarray(N, np.float32)
+    v = np.ascontiguousarray(v, np.float32)
+    out = np.zeros(3, np.float32)
+    lib().orc_frame_xfm(_ptr(N), _ptr(v), _ptr(out))
     return out
 
 

@@ -241,6 +241,8 @@ struct Scene {
   vec3f gridOrigin, gridSpacing, mcOrigin, mcSpacing;
   vec3f boundsLo, boundsHi;
   std::vector<float> majorants;
+  std::vector<float> ranges;  // per macrocell lo, hi (MCGrid scalar ranges)
+  float isoDelta = 0.f;       // central-difference step of the isosurface normal
   // camera DD, Camera.cu:82-100
   vec3f dir00, dirdu, dirdv, lens00;
   explicit Scene(const OrcScene &s) : s(s) {}
@@ -464,8 +466,12 @@ static void setupScene(Scene &sc) {
   sc.mcOrigin = sc.boundsLo;                                          // :76
   sc.mcSpacing = V(8.f) * sc.gridSpacing;                             // :77
   int64_t n = (int64_t)sc.mcDims.x * sc.mcDims.y * sc.mcDims.z;
-  std::vector<float> ranges(2 * n);
+  std::vector<float> &ranges = sc.ranges;
+  ranges.resize(2 * n);
   buildRanges(s, sc.mcDims, ranges.data());
+  // MCAccelerator.h:445-447: length(bounds.size()) * .1 / (sum of macrocell dims)
+  const vec3f bsize = sc.boundsHi - sc.boundsLo;
+  sc.isoDelta = sqrtf(dot(bsize, bsize)) * .1f / float(sc.mcDims.x + sc.mcDims.y + sc.mcDims.z);
   sc.majorants.resize(n);
   for (int64_t i = 0; i < n; i++) {                                   // MCGrid.cu:97-113
     float m = mapMajorant(s, ranges[2 * i], ranges[2 * i + 1]);
@@ -539,6 +545,8 @@ struct Ray {
   float tMax;
   RNGSeed rngSeed;
   bool hadHit = false;
+  bool surf = false;   // the hit is on the isosurface (else a volume collision)
+  vec3f N;             // isosurface hit: normal as stored in the ray (vec3h, Ray.h:61-62)
   vec3f P;
   vec3f hitColor;  // mapped rgb at the collision (phase tint)
   float hitScalar; // field value at the collision (principled volumes)
@@ -562,16 +570,130 @@ static bool woodcock(vec4f &sample, float &scalar, const Scene &sc, vec3f org, v
   }
 }
 
-// TraceRays::run (traceRays.dev.cu:26-52) + MCVolumeAccel::isProg
-// (MCAccelerator.h:552-689) for one identity-instanced structured volume.
-static void traceRay(const Scene &sc, Ray &ray, LocalStats &st) {
+// ---------------------------------------------------------------------------
+// isoSurface geometry on the field: MCIsoSurfaceAccel::isProg
+// (MCAccelerator.h:325-548) with an AnariMatte material (AnariMatte.h:49-71)
+// ---------------------------------------------------------------------------
+// The constant material parameters (HostMaterial.h:98-115: a NaN value reads
+// as (0,0,0,1)); Lambertian albedo = .85 * color * (1/pi), alpha = color.w * opacity.x
+static const float ONE_OVER_PI = 1.f / ONE_PI;
+static inline vec4f isoColor(const OrcScene &s) {
+  if (std::isnan(s.isoColor[0])) return {0.f, 0.f, 0.f, 1.f};
+  return {s.isoColor[0], s.isoColor[1], s.isoColor[2], s.isoColor[3]};
+}
+static inline float isoOpacity(const OrcScene &s) { return std::isnan(s.isoOpacity) ? 0.f : s.isoOpacity; }
+static inline vec3f isoAlbedo(const OrcScene &s) {
+  const vec4f c = isoColor(s);
+  const float reflectance = .85f;
+  return V(reflectance * c.x * ONE_OVER_PI, reflectance * c.y * ONE_OVER_PI, reflectance * c.z * ONE_OVER_PI);
+}
+static inline float isoAlpha(const OrcScene &s) { return isoColor(s).w * isoOpacity(s); }
+
+// The isosurface's intersection program for one ray: box test, its own RNG
+// (derived from the ray's seed, which this advances), a DDA over the
+// macrocell ranges and, in every macrocell whose range holds the iso value,
+// ten linear steps between the cell's entry and exit, intersecting the
+// segment whose end values bracket the iso value.  The program reports no
+// intersection to the traversal: it only lowers the ray's own tMax.
+// tMax: the traversal's ray tMax.  Returns true with tHit < ray.tMax on a hit.
+static bool isoIntersect(const Scene &sc, Ray &ray, vec3f obj_org, vec3f obj_dir, float tMax, float &tHit) {
+  float t0 = 0.f, t1 = tMax;
+  if (!boxTest(obj_org, obj_dir, t0, t1, sc.boundsLo, sc.boundsHi)) return false;
+  const vec3f dda_org = (obj_org - sc.mcOrigin) * rcp(sc.mcSpacing);
+  const vec3f dda_dir = obj_dir * rcp(sc.mcSpacing);
+  // Random rng(ray.rngSeed, hash(instance 0, geometry 0, primitive 0))
+  Random2 rng(ray.rngSeed, hash3(0, 0, 0));
+  const float iso = sc.s.isoValue;
+  const float prdTMax = ray.tMax;
+  tHit = prdTMax;
+  dda3(dda_org, dda_dir, t1, sc.mcDims, [&](const vec3i &c, float ct0, float ct1) -> bool {
+    const float lower = ct0, upper = fmin_(ct1, prdTMax);
+    if (lower >= upper) return true;
+    const int64_t idx = (int64_t)c.x + (int64_t)sc.mcDims.x * ((int64_t)c.y + (int64_t)sc.mcDims.y * c.z);
+    const float rlo = sc.ranges[2 * idx], rhi = sc.ranges[2 * idx + 1];
+    if (!(iso >= rlo && iso <= rhi)) return true;
+    float tt1 = ct0;
+    float ff1 = sampleField(sc, obj_org + tt1 * obj_dir);
+    const int numSteps = 10;
+    for (int i = 1; i <= numSteps; i++) {
+      const float tt0 = tt1;
+      const float ff0 = ff1;
+      tt1 = lerp_l(i / float(numSteps), ct0, ct1);
+      ff1 = sampleField(sc, obj_org + tt1 * obj_dir);
+      if (std::isnan(ff0) || std::isnan(ff1)) continue;
+      const float vlo = fmin_(ff0, ff1), vhi = fmax_(ff0, ff1);
+      if (iso >= vlo && iso <= vhi) {
+        float t = (iso - ff0) / (ff1 - ff0);
+        t = lerp_l(t, tt0, tt1);
+        tHit = (t < tHit) ? t : tHit;  // min(tHit, t); a 0/0 segment (NaN) keeps tHit
+        if (tHit < prdTMax) return false;
+      }
+    }
+    return true;
+  });
+  if (!(tHit < prdTMax)) return false;
+  const float opacity = isoAlpha(sc.s);  // Lambertian::getOpacity
+  if (opacity < 1.f && rng() > opacity) return false;
+  return true;
+}
+
+// The hit normal (MCAccelerator.h:444-478): central differences of the field
+// over +-delta, one-sided where a neighbour is outside; a zero gradient
+// falls back to -normalize(dir).  Returned as Ray::packNormal stores it
+// (normalized, rounded to binary16).
+static vec3f isoNormal(const Scene &sc, vec3f osP, vec3f obj_dir) {
+  const float delta = sc.isoDelta;
+  const float fP = sampleField(sc, osP);
+  float fPx0 = sampleField(sc, osP + V(-delta, 0.f, 0.f));
+  float fPx1 = sampleField(sc, osP + V(+delta, 0.f, 0.f));
+  float fPy0 = sampleField(sc, osP + V(0.f, -delta, 0.f));
+  float fPy1 = sampleField(sc, osP + V(0.f, +delta, 0.f));
+  float fPz0 = sampleField(sc, osP + V(0.f, 0.f, -delta));
+  float fPz1 = sampleField(sc, osP + V(0.f, 0.f, +delta));
+  float dx = 2.f, dy = 2.f, dz = 2.f;
+  if (std::isnan(fPx0)) { dx -= 1.f; fPx0 = fP; }
+  if (std::isnan(fPx1)) { dx -= 1.f; fPx1 = fP; }
+  if (std::isnan(fPy0)) { dy -= 1.f; fPy0 = fP; }
+  if (std::isnan(fPy1)) { dy -= 1.f; fPy1 = fP; }
+  if (std::isnan(fPz0)) { dz -= 1.f; fPz0 = fP; }
+  if (std::isnan(fPz1)) { dz -= 1.f; fPz1 = fP; }
+  vec3f osN = V(dx == 0.f ? 0.f : (fPx1 - fPx0) / dx, dy == 0.f ? 0.f : (fPy1 - fPy0) / dy,
+                dz == 0.f ? 0.f : (fPz1 - fPz0) / dz);
+  if (isZero(osN)) osN = -normalize(obj_dir);
+  return halfRound(normalize(osN));
+}
+
+// TraceRays::run (traceRays.dev.cu:26-52) over the group's isosurface, then
+// its volume (MCVolumeAccel::isProg, MCAccelerator.h:552-689), for one
+// identity instance.  The traversal calls the isosurface first: its hit
+// lowers only the ray's own tMax, so the volume's box test and DDA still run
+// to the traversal's tMax while its Woodcock ranges stop at the surface.  A
+// shadow ray that hits the surface is occluded and skips the volume, and the
+// volume's DDA stops at the first occupied macrocell that starts at or
+// beyond a surface hit; neither can change the outcome.
+static void traceRay(const Scene &sc, Ray &ray, LocalStats &st, bool shadowRay = false) {
   st.rays++;
   vec3f dir = ray.dir;
   if (dir.x == 0.f) dir.x = 1e-6f;
   if (dir.y == 0.f) dir.y = 1e-6f;
   if (dir.z == 0.f) dir.z = 1e-6f;
   const vec3f obj_org = ray.org, obj_dir = dir;
-  float t0 = 0.f, t1 = ray.tMax;
+  const float tMax = ray.tMax;  // the traversal's tMax
+  bool isoHit = false;
+  if (sc.s.iso) {
+    float tHit;
+    if (isoIntersect(sc, ray, obj_org, obj_dir, tMax, tHit)) {
+      isoHit = true;
+      ray.hadHit = true;  // AnariMatte setHit -> Ray::setHit (Ray.h:88-99)
+      ray.surf = true;
+      ray.tMax = tHit;
+      ray.P = obj_org + tHit * obj_dir;
+      ray.N = isoNormal(sc, ray.P, obj_dir);
+      if (shadowRay) return;
+    }
+  }
+  if (sc.s.noVolume) return;
+  float t0 = 0.f, t1 = tMax;
   if (!boxTest(obj_org, obj_dir, t0, t1, sc.boundsLo, sc.boundsHi)) return;
   vec3f dda_org = (obj_org - sc.mcOrigin) * rcp(sc.mcSpacing);
   vec3f dda_dir = obj_dir * rcp(sc.mcSpacing);
@@ -580,12 +702,14 @@ static void traceRay(const Scene &sc, Ray &ray, LocalStats &st) {
     const float majorant = sc.majorants[(int64_t)c.x + (int64_t)sc.mcDims.x * ((int64_t)c.y + (int64_t)sc.mcDims.y * c.z)];
     st.mcVisits++;
     if (majorant == 0.f) return true;
+    if (isoHit && ct0 >= ray.tMax) return false;
     vec4f sample = {0, 0, 0, 0};
     float scalar = 0.f;
     float upper = fmin_(ct1, ray.tMax);
     if (!woodcock(sample, scalar, sc, obj_org, obj_dir, ct0, upper, majorant, rng, st)) return true;
     vec3f P = obj_org + upper * obj_dir;
     ray.hadHit = true;           // Ray::setVolumeHit -> setHit (Ray.h:101-144)
+    ray.surf = false;
     ray.P = P;
     ray.tMax = upper;
     ray.hitColor = V(sample.x, sample.y, sample.z);
@@ -677,17 +801,25 @@ static vec3f hgSampleDirection(vec3f wi_in, float g, Random2 &random) {
 
 // shadeRays.cu:294-402 for the lights this path has: the constant
 // environment (renderer.ambientRadiance, no env-map texture) and
-// directional lights.  N is the zero vector for volume hits.
+// directional lights.  N is the zero vector for volume hits and the
+// front-facing normal for surface hits.
+static const float ONE_OVER_TWO_PI = 1.f / TWO_PI;
 static bool sampleLights(const Scene &sc, LightSample &ls, Random2 &random, bool &lightNeedsMIS,
-                         bool &lightIsDirLight) {
+                         bool &lightIsDirLight, vec3f N = V(0.f)) {
   const OrcScene &s = sc.s;
   lightNeedsMIS = false;
-  // sampleEnvLight :266-291 (N == 0 branch)
+  // sampleEnvLight :266-291
   LightSample els;
   els.direction = randomDirection(random);
   els.distance = INF;
-  els.radiance = V(FOUR_PI * s.ambientRadiance);
-  els.pdf = ONE_OVER_FOUR_PI;
+  if (!isZero(N)) {
+    els.radiance = V(TWO_PI * s.ambientRadiance);
+    if (dot(els.direction, N) < 0.f) els.direction = -els.direction;
+    els.pdf = ONE_OVER_TWO_PI;
+  } else {
+    els.radiance = V(FOUR_PI * s.ambientRadiance);
+    els.pdf = ONE_OVER_FOUR_PI;
+  }
   float elsWeight = reduce_max(els.radiance);
   // sampleAreaLights: none on this path -> false, no random numbers
   float alsWeight = 0.f;
@@ -705,7 +837,8 @@ static bool sampleLights(const Scene &sc, LightSample &ls, Random2 &random, bool
       weights[i] = 0.f;
       const float *L = s.dirLights + 7 * lID[i];
       vec3f rad = V(L[4], L[5], L[6]) * L[3];
-      float weight = 1.f;  // N == 0
+      const vec3f lightDir = -normalize(V(L[0], L[1], L[2]));
+      float weight = isZero(N) ? 1.f : dot(lightDir, N);
       if (weight <= 1e-3f) continue;
       weight *= reduce_max(rad);
       if (weight <= 1e-3f) continue;
@@ -755,6 +888,112 @@ static bool sampleLights(const Scene &sc, LightSample &ls, Random2 &random, bool
   }
   if (std::isnan(ls.pdf) || (ls.pdf <= 0.f)) return false;
   return true;
+}
+
+// ---------------------------------------------------------------------------
+// surface hits: bounce() with a Lambertian BSDF (shadeRays.cu:540-878,
+// packedBSDF/Lambertian.h:45-86, DG.h:162-193)
+// ---------------------------------------------------------------------------
+// owl::common::frame(N) (the owl submodule, absent here): the orthonormal
+// basis of embree's LinearSpace3 frame() -- dx from the larger of
+// (0, N.z, -N.y) and (-N.z, 0, N.x), dy = normalize(cross(N, dx)), dz = N --
+// and xfmVector(frame, v) = dx * v.x + dy * v.y + dz * v.z.
+static vec3f frameXfm(vec3f N, vec3f v) {
+  const vec3f dx0 = V(0.f, N.z, -N.y);
+  const vec3f dx1 = V(-N.z, 0.f, N.x);
+  const vec3f dx = normalize(dot(dx0, dx0) > dot(dx1, dx1) ? dx0 : dx1);
+  const vec3f dy = normalize(cross(N, dx));
+  return dx * v.x + dy * v.y + N * v.z;
+}
+// Lambertian::pdf: the cosine pdf about the normal turned toward wi
+static inline float lambertPdf(vec3f Ng, vec3f wi) {
+  vec3f N = Ng;
+  if (dot(wi, N) < 0.f) N = -N;
+  const float cosThetaI = fmax_(dot(wi, N), 0.f);
+  return cosThetaI * ONE_OVER_PI;
+}
+
+// bounce() for a hit on the isosurface: shadow ray toward a light sample
+// with the Lambertian's f_r and the surface's cosine, then (path depth and
+// the one diffuse bounce allowed, MAX_DIFFUSE_BOUNCES) a cosine-sampled
+// scattered ray.  cosineSampleHemisphere draws its two numbers in argument
+// order (u for the azimuth first); its sincosf is sincosPortable.
+static void surfaceBounce(const Scene &sc, Ray &ray, int depth, Random2 &random, vec3f P, vec3f wo,
+                          float offsetEpsilon, vec3f &tp, float &pathMis, int &numDiffuseBounces, Ray &shadow,
+                          vec3f &shadowTp, float &shadowMis, bool &haveShadow, bool &haveScatter) {
+  const vec3f albedo = isoAlbedo(sc.s);
+  const vec3f Ng = normalize(ray.N);
+  const bool hitWasOnFront = dot(ray.dir, Ng) < 0.f;
+  const vec3f Ngff = hitWasOnFront ? Ng : -Ng;
+  LightSample ls;
+  bool lightNeedsMIS = false, lightIsDirLight = false;
+  if (sampleLights(sc, ls, random, lightNeedsMIS, lightIsDirLight, Ngff)) {
+    // Lambertian::eval: cosine against the shading normal (dg.Ns = Ng, not turned)
+    const float cosThetaI = fmax_(dot(ls.direction, Ng), 0.f);
+    const float fpdf = cosThetaI * ONE_OVER_PI;
+    vec3f fval = albedo * ONE_OVER_PI * cosThetaI;
+    if ((fpdf > 0.f) && !(reduce_max(fval) < 1e-4f)) {
+      fval = vmin(fval, V(13.f));
+      const float cosL = ONE_OVER_PI * fabsf(dot(Ng, ls.direction));
+      vec3f tp_sr = tp * (std::isinf(ls.pdf) ? 1.f : (1.f / ls.pdf)) * fval * ls.radiance * cosL;
+      shadow.org = P + offsetEpsilon * Ngff;
+      shadow.dir = ls.direction;
+      shadow.tMax = ls.distance * (1.f - 2.f * offsetEpsilon);
+      shadowTp = halfRound(tp_sr);
+      shadow.rngSeed = ray.rngSeed;
+      ray.rngSeed.nextHashed((uint64_t)floatBits(ray.tMax));
+      haveShadow = true;
+      if (!lightIsDirLight && lightNeedsMIS) {
+        const float pdf_light = ONE_OVER_FOUR_PI;
+        const float pdf_scatter = lambertPdf(Ng, ls.direction);
+        shadowMis = pdf_light / (pdf_light + pdf_scatter + 1e-10f);
+        if (shadowMis < 1e-5f) haveShadow = false;
+      }
+      if (!(shadow.tMax > 0.f)) haveShadow = false;
+    }
+  }
+  if (depth >= MAX_PATH_DEPTH) return;
+  // Lambertian::scatter
+  vec3f N = Ng;
+  if (dot(wo, N) < 0.f) N = -N;
+  const float su = random();
+  const float sv = random();
+  const float phi = TWO_PI * su;
+  const float cosTheta = sqrtf(sv);
+  const float sinTheta = sqrtf(1.0f - sv);
+  float sinPhi, cosPhi;
+  sincosPortable(phi, sinPhi, cosPhi);
+  const vec3f localDir = V(cosPhi * sinTheta, sinPhi * sinTheta, cosTheta);
+  const vec3f sdir = frameXfm(N, localDir);
+  const float pdf = localDir.z * ONE_OVER_PI;
+  if (!(pdf > 0.f) || pdf <= 1e-6f) {
+    // no valid sample: the ray, cleared, goes out again unchanged (:757-768)
+    ray.tMax = INF;
+    ray.hadHit = false;
+    ray.surf = false;
+    haveScatter = true;
+    return;
+  }
+  if (numDiffuseBounces >= 1) return;  // MAX_DIFFUSE_BOUNCES
+  numDiffuseBounces++;
+  ray.org = P + (1.f * offsetEpsilon) * Ngff;
+  ray.dir = normalize(sdir);
+  const float c = fabsf(dot(Ng, normalize(ray.dir)));
+  const float denom = std::isinf(pdf) ? 1.f : (pdf + 1e-10f);
+  vec3f scatterFactor = V((albedo.x * c) / denom, (albedo.y * c) / denom, (albedo.z * c) / denom);
+  scatterFactor = vmin(scatterFactor, V(2.5f));
+  tp = halfRound(tp * scatterFactor);
+  if (lightNeedsMIS && !std::isinf(pdf)) {
+    const float ps = lambertPdf(Ng, ray.dir);
+    const float pl = ONE_OVER_FOUR_PI;
+    pathMis = ps / (ps + pl);
+  } else {
+    pathMis = 1.f;
+  }
+  ray.tMax = INF;
+  ray.hadHit = false;
+  ray.surf = false;
+  haveScatter = true;
 }
 
 // one wave for one pixel: generateRays.cu:43-244, trace, bounce()
@@ -812,13 +1051,22 @@ static PixelSample renderPixelSample(const Scene &sc, int ix, int iy, int accumI
   // path state: throughput (vec3h), MIS weight of the path ray, bounces
   vec3f tp = V(1.f);
   float pathMis = 1.f;
-  int numVolumeBounces = 0;
+  int numVolumeBounces = 0, numDiffuseBounces = 0;
   for (int depth = 0;; depth++) {
-    // ---- bounce() on a volume hit of generation `depth` (shadeRays.cu:608-878)
+    // ---- bounce() on a hit of generation `depth` (shadeRays.cu:608-878)
     Random2 random(ray.rngSeed, (uint64_t)floatBits(ray.tMax));
     const vec3f P = ray.P;
     const vec3f wo = -normalize(ray.dir);
     const float offsetEpsilon = fmax_(1e-4f, 1e-6f * reduce_max(vabs(P)));  // safe_eps
+    Ray shadow;
+    vec3f shadowTp = V(0.f);
+    float shadowMis = 1.f;
+    bool haveShadow = false;
+    bool haveScatter = false;
+    if (ray.surf) {
+      surfaceBounce(sc, ray, depth, random, P, wo, offsetEpsilon, tp, pathMis, numDiffuseBounces, shadow, shadowTp,
+                    shadowMis, haveShadow, haveScatter);
+    } else {
     // bsdf at the collision (Phase.h): SimplePhase(0.7) or HGPhase.  The
     // multi-scatter build re-derives a principled volume's tint, albedo and
     // emission from the field value at the hit (MCAccelerator.h:621-659).
@@ -855,10 +1103,6 @@ static PixelSample renderPixelSample(const Scene &sc, int ix, int iy, int accumI
       else out.add(tp * emission);
     }
     // shadow ray (:640-746)
-    Ray shadow;
-    vec3f shadowTp = V(0.f);
-    float shadowMis = 1.f;
-    bool haveShadow = false;
     LightSample ls;
     bool lightNeedsMIS = false, lightIsDirLight = false;
     if (sampleLights(sc, ls, random, lightNeedsMIS, lightIsDirLight)) {
@@ -892,7 +1136,6 @@ static PixelSample renderPixelSample(const Scene &sc, int ix, int iy, int accumI
     // the volume-bounce budget.  A sample with pdf <= 1e-6 would end the path
     // here (the reference re-traces the old ray); with anisotropy clamped to
     // [-0.99, 0.99] (Volume.cpp:55-57) the HG pdf stays above 2e-4.
-    bool haveScatter = false;
     if (s.phaseMode == 1 && s.maxVolumeBounces > 0 && depth < MAX_PATH_DEPTH) {
       const vec3f wi_in = normalize(-wo);
       const vec3f sdir = hgSampleDirection(wi_in, s.anisotropy, random);
@@ -918,9 +1161,10 @@ static PixelSample renderPixelSample(const Scene &sc, int ix, int iy, int accumI
         haveScatter = true;
       }
     }
+    }
     // ---- generation depth+1: the shadow ray, then the scattered ray
     if (haveShadow) {
-      traceRay(sc, shadow, st);
+      traceRay(sc, shadow, st, true);
       out.add(shadow.hadHit ? V(0.f) : (shadowMis * shadowTp));
     }
     if (!haveScatter) return out;
@@ -929,7 +1173,7 @@ static PixelSample renderPixelSample(const Scene &sc, int ix, int iy, int accumI
       out.add(tp * V(s.ambientRadiance) * pathMis);
       return out;
     }
-    // a secondary volume hit: no emission without principled volumes
+    // a secondary hit: emission of principled volumes only
   }
 }
 
@@ -1015,6 +1259,29 @@ void orc_hg_sample(const float *wi, float g, uint64_t seedState, int n, float *o
   }
 }
 float orc_h2f(uint16_t h) { return h2f(h); }
+
+// One ray against the scene's isosurface: *hit, the hit distance and the
+// stored normal; the ray's RNG state starts at seedState.
+void orc_iso_trace(const OrcScene *s, const float *org, const float *dir, float tMax, uint64_t seedState, int *hit,
+                   float *tOut, float *nOut) {
+  Scene sc(*s);
+  setupScene(sc);
+  Ray ray;
+  ray.org = V(org[0], org[1], org[2]);
+  ray.dir = V(dir[0], dir[1], dir[2]);
+  ray.tMax = tMax;
+  ray.rngSeed.state = seedState;
+  float tHit = tMax;
+  *hit = isoIntersect(sc, ray, ray.org, ray.dir, tMax, tHit) ? 1 : 0;
+  *tOut = tHit;
+  const vec3f n = *hit ? isoNormal(sc, ray.org + tHit * ray.dir, ray.dir) : V(0.f);
+  nOut[0] = n.x; nOut[1] = n.y; nOut[2] = n.z;
+}
+// owl::common::frame(N) applied to v
+void orc_frame_xfm(const float *N, const float *v, float *out) {
+  const vec3f r = frameXfm(V(N[0], N[1], N[2]), V(v[0], v[1], v[2]));
+  out[0] = r.x; out[1] = r.y; out[2] = r.z;
+}
 
 void orc_mc_dims(const OrcScene *s, int *out3) {
   out3[0] = (s->dims[0] - 1 + 7) / 8;

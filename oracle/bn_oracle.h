@@ -35,6 +35,13 @@ typedef struct {
   float pDensity, pDensityThreshold, pDensityScale, pValueRange[2];
   float pEmissionStrength, pBlackbodyIntensity, pTemperature;
   float pScatterColor[3], pAbsorptionColor[3], pEmissionColor[3], pBlackbodyTint[3];
+  // isoSurface geometry on the same field (MCIsoSurfaceAccel) with an
+  // AnariMatte material of constant color and opacity, enabled by `iso`
+  int iso;
+  float isoValue;
+  float isoColor[4];      // AnariMatte "color" (rgba; a float3 set gives alpha 1)
+  float isoOpacity;       // AnariMatte "opacity"
+  int noVolume;           // 1: the group holds the isosurface alone (no volume)
   int width, height;
 } OrcScene;
 }

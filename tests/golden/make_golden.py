@@ -43,6 +43,14 @@ def scenes():
         "enabled": 1, "absorption_color": (0.2, 0.1, 0.05), "emission_strength": 1.5,
         "blackbody_intensity": 0.5, "temperature": 4500.0, "density_threshold": 0.2})
     out["noise_exact_log"] = dict(out["noise_u8"], exact_log=True)
+    # isosurfaces with a matte material: alone on the blobs (directional light
+    # + ambient), inside the noise volume, and semi-opaque in the multi-scatter build
+    out["blobs_iso"] = synth.scene(blob, "f32", 24, 16, synth.tf_linear_ramp(128), 50.0, synth.DEFAULT_CAMERA,
+                                   ambient=0.3, dir_lights=synth.CONFIG2_LIGHTS, volume=False,
+                                   iso={"value": 0.3, "color": (0.9, 0.5, 0.2)})
+    out["noise_iso"] = dict(out["noise_f32"], iso={"value": 0.55, "color": (0.3, 0.6, 0.9)})
+    out["noise_iso_multiscatter"] = dict(out["noise_f32"], anisotropy=0.4, max_volume_bounces=2,
+                                         iso={"value": 0.5, "color": (0.8, 0.8, 0.3, 0.9), "opacity": 0.7})
     return out
 
 

@@ -386,3 +386,85 @@ def test_principled_volume_emission_adds_light():
     oracle.render(oracle.Scene(dict(s, principled={"enabled": 1})), 0, 4, accum=a)
     oracle.render(oracle.Scene(dict(s, principled={"enabled": 1, "emission_strength": 5.0})), 0, 4, accum=b)
     assert np.array_equal(a, b)
+
+
+# ---------------------------------------------------------------------------
+# isosurfaces (MCIsoSurfaceAccel::isProg) with a matte (Lambertian) material
+# ---------------------------------------------------------------------------
+def ramp_scene(iso=0.37, nx=17, ny=9, nz=9, **kw):
+    """Field f(x, y, z) = x on [0,1]^3: an x-ramp whose isosurface is the plane
+    x = iso with normal +x.  Values i/16 are exact in binary32."""
+    from barney_b200 import synth
+    x = (np.arange(nx, dtype=np.float32) / f32(nx - 1))
+    vol = np.broadcast_to(x[None, None, :], (nz, ny, nx)).astype(np.float32).copy()
+    d = synth.scene(vol, "f32", 16, 16, synth.tf_linear_ramp(2), 1.0,
+                    {"position": (2.0, 0.5, 0.5), "direction": (-1.0, 0.0, 0.0), "up": (0.0, 1.0, 0.0), "fovy": 10.0},
+                    volume=False, iso={"value": iso, "color": (0.9, 0.6, 0.3)})
+    d.update(kw)
+    return d
+
+
+def test_iso_ramp_plane_hit_distance_and_normal():
+    sc = oracle.Scene(ramp_scene(0.37))
+    # from the -x side and from the +x side: the plane x = 0.37; linear
+    # interpolation of a linear field finds it to rounding
+    hit, t, n = oracle.iso_trace(sc, (-0.5, 0.5, 0.5), (1.0, 0.0, 0.0))
+    assert hit and abs(t - 0.87) < 2e-6
+    assert n.tolist() == [1.0, 0.0, 0.0]  # gradient +x, normalized, binary16
+    hit, t, n = oracle.iso_trace(sc, (1.5, 0.5, 0.5), (-1.0, 0.0, 0.0))
+    assert hit and abs(t - 1.13) < 2e-6
+    assert n.tolist() == [1.0, 0.0, 0.0]  # the stored normal does not face the ray
+    # an oblique ray: t where 0.2 + t * 0.6 = 0.37 (direction normalized)
+    d = np.array([0.6, 0.48, 0.64], np.float32)
+    hit, t, _ = oracle.iso_trace(sc, (0.2, 0.1, 0.1), d)
+    assert hit and abs(t - (0.17 / 0.6)) < 2e-6
+    # short of the plane, or an iso value outside the field's range: no hit
+    assert not oracle.iso_trace(sc, (-0.5, 0.5, 0.5), (1.0, 0.0, 0.0), tmax=0.8)[0]
+    assert not oracle.iso_trace(oracle.Scene(ramp_scene(1.5)), (-0.5, 0.5, 0.5), (1.0, 0.0, 0.0))[0]
+
+
+def test_frame_is_orthonormal_and_maps_z_to_the_normal():
+    rng = np.random.default_rng(5)
+    for _ in range(64):
+        N = rng.normal(size=3).astype(np.float32)
+        N = (N / np.linalg.norm(N)).astype(np.float32)
+        assert np.array_equal(oracle.frame_xfm(N, (0.0, 0.0, 1.0)), N)
+        ex, ey = oracle.frame_xfm(N, (1.0, 0.0, 0.0)), oracle.frame_xfm(N, (0.0, 1.0, 0.0))
+        for a, b in ((ex, ey), (ex, N), (ey, N)):
+            assert abs(float(np.dot(a, b))) < 1e-6
+        assert abs(float(np.linalg.norm(ex)) - 1) < 1e-6 and abs(float(np.linalg.norm(ey)) - 1) < 1e-6
+        # right-handed: dy = N x dx
+        assert np.allclose(np.cross(N, ex), ey, atol=1e-6)
+
+
+def test_iso_plane_facing_a_directional_light_radiance():
+    """Every sample of the plane x = 0.37 seen along -x, lit head-on by one
+    directional light with no ambient: the shadow ray's fragment is
+    halfRound(tp) with tp = (.85 c / pi) / pi * cos * (1/pi * |cos|) -- the
+    Lambertian's albedo carries 1/pi, its eval another, the surface cosine a
+    third (shadeRays.cu:686-691) -- and the diffuse bounce escapes into a black
+    environment."""
+    d = ramp_scene(0.37, ambient=0.0, dir_lights=[{"direction": (-1.0, 0.0, 0.0), "radiance": 1.0}])
+    spp = 8
+    acc, _, st = oracle.render(oracle.Scene(d), 0, spp)
+    one_over_pi = f32(1.0) / f32(math.pi)
+    expect = []
+    for c in (0.9, 0.6, 0.3):
+        albedo = f32(0.85) * f32(c) * one_over_pi
+        fval = albedo * one_over_pi * f32(1.0)
+        tp = f32(1.0) * f32(1.0) * fval * f32(1.0) * (one_over_pi * f32(1.0))
+        expect.append(float(np.float16(tp)))
+    img = acc / spp
+    assert np.array_equal(img[..., :3], np.broadcast_to(np.array(expect, np.float32), img[..., :3].shape))
+    assert np.all(img[..., 3] == 1.0)
+    # per sample: the primary ray, its shadow ray and the diffuse bounce
+    assert st["rays"] == 3 * 16 * 16 * spp and st["samples"] == 0
+
+
+def test_iso_opacity_zero_passes_every_ray_and_one_blocks():
+    d = ramp_scene(0.37, bg_color=(0.25, 0.5, 0.75, 1.0))
+    acc, _, st = oracle.render(oracle.Scene(dict(d, iso={"value": 0.37, "opacity": 0.0})), 0, 2)
+    assert np.array_equal(acc / 2, np.broadcast_to(np.array([0.25, 0.5, 0.75, 1.0], np.float32), acc.shape))
+    assert st["rays"] == 16 * 16 * 2
+    acc1, _, _ = oracle.render(oracle.Scene(d), 0, 2)
+    assert not np.array_equal(acc1, acc)
