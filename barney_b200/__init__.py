@@ -318,13 +318,13 @@ class VolumeRenderer:
                     L.bnSet3f(self.vol, name, *map(float, pv[key]))
         L.bnCommit(self.vol)
         check()
-        # an isoSurface geometry with a matte material on the same field; with
+        # an iso_surface geometry with a matte material on the same field; with
         # desc["volume"] False the group holds the isosurface alone
         geoms, n_geoms = None, 0
         self.iso = self.material = None
         if desc.get("iso"):
             self.material = self._keep(L.bnMaterialCreate(self.ctx, 0, b"matte"))
-            self.iso = self._keep(L.bnGeometryCreate(self.ctx, 0, b"isoSurface"))
+            self.iso = self._keep(L.bnGeometryCreate(self.ctx, 0, b"iso_surface"))
             check()
             L.bnSetObject(self.iso, b"scalarField", sf)
             self.set_iso(**desc["iso"])

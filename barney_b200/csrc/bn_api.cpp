@@ -559,6 +559,11 @@ BN_API void bnSetData(BNObject t, const char *n, BNData v) {
     g->lights = v ? getAs<Data>(v, Object::K_DATA, "BNData") : nullptr;
     return;
   }
+  if (o->kind == Object::K_GEOM && name == "isoValues") {  // IsoSurface.cpp:60-68
+    // kept, and unused: the intersection program reads isoValue only (MCAccelerator.h:325-548)
+    std::static_pointer_cast<IsoSurface>(o)->isoValues = v ? getObject(v) : nullptr;
+    return;
+  }
   warnUnsupported(n);
   BN_CATCH()
 }
@@ -645,9 +650,9 @@ BN_API BNLight bnLightCreate(BNContext context, int, const char *type) {
 BN_API BNGeom bnGeometryCreate(BNContext context, int, const char *type) {
   BN_TRY
   Context *c = getContext(context);
-  if (!type || std::string(type) != "isoSurface")
-    throw Error(E_UNSUPPORTED, std::string("unsupported geometry type '") + (type ? type : "(null)") +
-                                   "' (only 'isoSurface')");
+  const std::string t = type ? type : "";
+  if (t != "iso_surface" && t != "isoSurface")  // Geometry.cpp:33
+    throw Error(E_UNSUPPORTED, "unsupported geometry type '" + t + "' (only 'iso_surface')");
   return c->add(std::make_shared<IsoSurface>(c));
   BN_CATCH(nullptr)
 }

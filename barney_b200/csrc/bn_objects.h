@@ -228,10 +228,11 @@ struct Material : Object {
   void commit() override { committed = true; }
 };
 
-// isoSurface geometry (IsoSurface.h:27-80, IsoSurface.cpp:36-90): an iso
+// "iso_surface" geometry (IsoSurface.h:27-80, IsoSurface.cpp:36-90): an iso
 // value on a structured scalar field, drawn with a material.
 struct IsoSurface : Object {
   float isoValue = NAN;
+  ObjectSP isoValues;  // bnSetData "isoValues"
   std::shared_ptr<StructuredField> sf;
   std::shared_ptr<Material> material;
   // macrocell scalar ranges of the field, built when no volume of the group
@@ -248,7 +249,7 @@ struct IsoSurface : Object {
   }
   bool setObject(const std::string &m, const ObjectSP &v) override {
     if (m == "scalarField") {
-      if (!v || v->kind != K_FIELD) throw Error(E_INVALID_ARG, "'scalarField' value set on 'isoSurface' is not a scalar field");
+      if (!v || v->kind != K_FIELD) throw Error(E_INVALID_ARG, "'scalarField' value set on 'iso_surface' is not a scalar field");
       sf = std::static_pointer_cast<StructuredField>(v);
       return true;
     }

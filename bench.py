@@ -54,6 +54,8 @@ def parse():
                         "simple = Barney's default build, SimplePhase (0.7 x TF colour)")
     p.add_argument("--max-volume-bounces", type=int, default=0,
                    help="configs 2/3: multi-scatter build with up to this many volume bounces")
+    p.add_argument("--iso", type=float, default=None,
+                   help="configs 2/3: add an iso_surface at this value (matte, colour .8) on the volume's field")
     p.add_argument("--e2e-steps", type=int, default=None)
     p.add_argument("--cpu-seconds", type=float, default=12.0)
     p.add_argument("--no-cpu-baseline", action="store_true")
@@ -89,6 +91,9 @@ def workload(args, xp, device):
     if args.max_volume_bounces > 0:
         d["max_volume_bounces"] = args.max_volume_bounces
         scatter = f"HG multi-scatter (up to {args.max_volume_bounces} volume bounces)"
+    if args.iso is not None:
+        d["iso"] = {"value": args.iso}
+        scatter += f", matte isosurface at {args.iso:g} (one diffuse bounce)"
     desc = {"workload": f"{n}^3 {dtype} 6-octave value noise (seed 0), 8^3 macrocells, 1920x1080, {d['spp']} spp, "
                         f"256-entry knot TF (seed 1) density 50, {scatter}"
                         f"{'' if args.phase == 'simple' else ' albedo 0.8'}, "

@@ -157,16 +157,18 @@ BN_API void bnVolumeSetXF(BNVolume volume, bn_float2 domain, const bn_float4 *co
                           int numColorMapValues, float densityAt1);
 /* replaces barney.cu bnLightCreate; type "directional" */
 BN_API BNLight bnLightCreate(BNContext context, int whichSlot, const char *type);
-/* replaces barney.cu:394 bnGeometryCreate (Geometry::create); type "isoSurface" only
-   (IsoSurface.cpp): bnSet1f "isoValue", bnSetObject "scalarField" (a structured
-   field) and "material" (a committed material).  With a volume in the same
-   group the isosurface must lie on the volume's field. */
+/* replaces barney.cu:394 bnGeometryCreate (Geometry::create, Geometry.cpp:33);
+   type "iso_surface" only (IsoSurface.cpp): bnSet1f "isoValue", bnSetObject
+   "scalarField" (a structured field) and "material" (a committed material),
+   bnSetData "isoValues" (kept, unused, as by the reference's intersection
+   program).  With a volume in the same group the isosurface must lie on the
+   volume's field. */
 BN_API BNGeom bnGeometryCreate(BNContext context, int whichSlot, const char *type);
 /* replaces barney.cu:405 bnMaterialCreate (HostMaterial::create); type "matte" /
    "AnariMatte" with constant parameters: bnSet3f / bnSet4f "color" (default
    .8,.8,.8), bnSet1f "opacity" (default 1) */
 BN_API BNMaterial bnMaterialCreate(BNContext context, int whichSlot, const char *type);
-/* replaces barney.cu:510 bnGroupCreate; at most one isoSurface geometry and at
+/* replaces barney.cu:510 bnGroupCreate; at most one iso_surface geometry and at
    most one volume, at least one of the two */
 BN_API BNGroup bnGroupCreate(BNContext context, int whichSlot, BNGeom *geoms, int numGeoms,
                              BNVolume *volumes, int numVolumes);

@@ -100,6 +100,8 @@ def test_iso_api_errors():
         L.bnSetObject(r.iso, b"scalarField", r.vol)  # not a scalar field
         assert L.bnGetLastError() == 2
         L.bnClearLastError()
+        L.bnSetData(r.iso, b"isoValues", None)  # as the ANARI device sets it; unused
+        assert L.bnGetLastError() == 0
         # a material that was never committed
         m = L.bnMaterialCreate(r.ctx, 0, b"AnariMatte")
         L.bnSetObject(r.iso, b"material", m)
