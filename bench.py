@@ -355,7 +355,13 @@ def run_ours(args):
     kms = [s["render_ms"] for s in stats]
     achieved = statistics.mean(a / (k * 1e-3) for a, k in zip(alg, kms)) / 1e9
     peak, peak_kind = measured_peak()
-    traffic = profiled_traffic(f"config{args.config}_{d['dtype']}")
+    # the committed capture applies to the same workload only: same config,
+    # storage, spp, phase, bounces and isosurface
+    tkey = f"config{args.config}_{d['dtype']}_spp{d['spp']}"
+    tkey += ("_simple" if d.get("phase") == "simple" else "") + \
+        (f"_msc{d['max_volume_bounces']}" if d.get("max_volume_bounces") else "") + \
+        (f"_iso{d['iso']['value']:g}" if d.get("iso") else "")
+    traffic = profiled_traffic(tkey)
 
     # end to end through the C ABI with host buffers: per step the camera is
     # set from host memory (kernel parameters) and the rgba8 frame is read
