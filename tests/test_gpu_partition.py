@@ -59,3 +59,17 @@ def test_partition_is_rejected_for_batches():
     finally:
         r.close()
         ctx.close()
+
+
+def test_isosurface_partitions_merge_into_the_full_frame():
+    import barney_b200 as bn
+    d = small_noise_scene(w=67, h=45, iso={"value": 0.5, "opacity": 0.8}, max_volume_bounces=2)
+    full, fst = _render(d, 2, 0, 1)
+    parts, rays = [], 0
+    for rank in range(3):
+        img, st = _render(d, 2, rank, 3)
+        parts.append(img)
+        rays += st["rays"]
+    owners = bn.partition_owners(d["width"], d["height"], 3)
+    assert_bitexact(bn.merge_partitions(np.stack(parts), owners), full, "3 isosurface partitions")
+    assert rays == fst["rays"]

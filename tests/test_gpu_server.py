@@ -114,20 +114,22 @@ def test_reserved_buffers_serve_identical_frames():
 
 
 def test_extended_requests_in_the_server_equal_the_oracle():
-    # multi-scatter, principled and exact-log requests run the extended batch
-    # kernel beside plain ones; each frame still equals the oracle's
+    # multi-scatter, principled, exact-log and isosurface requests run the
+    # extended batch kernels beside plain ones; each frame still equals the oracle's
     import barney_b200 as bn
     ctx = bn.Context()
     scenes = [small_noise_scene(n=24, w=24, h=16, anisotropy=0.6, max_volume_bounces=3),
               small_noise_scene(n=24, w=20, h=18, principled={"enabled": 1, "emission_strength": 1.0}),
               small_noise_scene(n=24, w=16, h=16, dtype="u8", exact_log=True),
-              small_blob_scene(n=20, w=24, h=20)]
+              small_blob_scene(n=20, w=24, h=20),
+              small_noise_scene(n=24, w=20, h=16, iso={"value": 0.5}),
+              small_blob_scene(n=20, w=16, h=20, volume=False, iso={"value": 0.3, "opacity": 0.7})]
     rs = [bn.VolumeRenderer(d, context=ctx, color_format="float4") for d in scenes]
     server = bn.Server(ctx, hbm_budget_bytes=1 << 30, max_slots=8, slice_waves=2)
     try:
         rng = np.random.default_rng(17)
         reqs = []
-        for i in range(12):
+        for i in range(18):
             k = i % len(scenes)
             cam = synth.orbit_camera(rng)
             w, h, spp = scenes[k]["width"], scenes[k]["height"], 1 + i % 4
