@@ -128,7 +128,9 @@ void Volume::commit() {  // Volume.cpp:26-35
 // scalar ranges, when no volume of the group has built them
 void IsoSurface::buildRanges() {
   if (!sf) throw Error(E_STATE, "isoSurface has no scalarField");
-  if (rangesOf == sf.get() && rangesTex == sf->scalars.get() && ranges.ptr) return;
+  if (rangesOf == sf.get() && rangesTex == sf->scalars.get() && ranges.ptr &&
+      !memcmp(rangesDims, sf->numScalars, sizeof rangesDims))
+    return;
   int d[3];
   const size_t n = macrocellDims(*sf, d);
   memcpy(mcDims, d, sizeof d);
@@ -137,6 +139,7 @@ void IsoSurface::buildRanges() {
      "macrocell range build");
   rangesOf = sf.get();
   rangesTex = sf->scalars.get();
+  memcpy(rangesDims, sf->numScalars, sizeof rangesDims);
 }
 
 // The isosurface part of a job (MCIsoSurfaceAccel::DD with the AnariMatte

@@ -239,8 +239,9 @@ struct IsoSurface : Object {
   // provides them (StructuredData::buildMCs, StructuredData.cu:71-96)
   DeviceBuffer ranges;
   int mcDims[3] = {0, 0, 0};
-  const StructuredField *rangesOf = nullptr;  // the field (and its texture) the ranges were built for
+  const StructuredField *rangesOf = nullptr;  // the field, texture and dims the ranges were built for
   const TextureData *rangesTex = nullptr;
+  int rangesDims[3] = {0, 0, 0};
   explicit IsoSurface(Context *c) : Object(c, K_GEOM) {}
   bool set1i(const std::string &m, int) override { return m == "userID"; }
   bool set1f(const std::string &m, float v) override {
