@@ -33,7 +33,21 @@ ISO_SCENES = {
                                                     cut_plane=(0.0, 1.0, 0.0, -0.5)),
     "noise_f16_alone_exact_log": lambda: small_noise_scene(dtype="f16", volume=False, exact_log=True,
                                                            iso={"value": 0.6}),
+    # edge cases: an iso value never set (NaN: no macrocell qualifies, the
+    # walk still derives its RNG), an iso value on voxel values exactly, and
+    # plateaus at the iso value (0/0 segments) on a clamped ramp
+    "nan_iso_value": lambda: small_noise_scene(iso={"value": float("nan")}),
+    "iso_on_voxel_values": lambda: ramp_scene(0.5, ambient=0.6),
+    "iso_plateau": lambda: _plateau_scene(),
 }
+
+
+def _plateau_scene():
+    d = ramp_scene(0.25, ambient=0.6, dir_lights=[{"direction": (-1.0, -0.2, 0.1), "radiance": 1.0}])
+    d["voxels"] = np.clip(d["voxels"], np.float32(0.25), np.float32(0.75))
+    d["camera"] = {"position": (1.8, 1.4, 1.6), "direction": (-1.3, -0.9, -1.1), "up": (0.0, 1.0, 0.0),
+                   "fovy": 40.0}
+    return d
 
 
 @pytest.mark.parametrize("name", sorted(ISO_SCENES))
