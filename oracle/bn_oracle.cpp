@@ -34,7 +34,12 @@
 //   barney/native/volume/MCGrid.cu:97-141         mapMCs
 //   barney/native/kernels/shadeRays.cu:17-402,475-1042 light sampling, bounce, accumulate
 //   barney/native/packedBSDF/Phase.h:14-176       HGPhase, SimplePhase
-//   barney/native/render/DG.h:183-193             randomDirection
+//   barney/native/render/DG.h:162-193             cosineSampleHemisphere, randomDirection
+//   barney/native/volume/MCAccelerator.h:325-548  MCIsoSurfaceAccel::isProg (isosurface hit, normal)
+//   barney/native/geometry/IsoSurface.cpp:36-90   isoSurface parameters
+//   barney/native/material/AnariMatte.h:49-71     matte material -> Lambertian
+//   barney/native/material/HostMaterial.h:98-115  constant material parameters
+//   barney/native/packedBSDF/Lambertian.h:45-86   Lambertian pdf, eval, scatter
 //   barney/native/light/EnvMap.h:136-151          constant-env pdf
 //   barney/native/light/DirLight.cu:11-20         directional light device data
 //   barney/native/fb/TiledFB.cu:13-52, LocalFB.cpp:61-71 resolve / tonemap
