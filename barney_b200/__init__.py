@@ -41,8 +41,10 @@ COLOR_FORMATS = {"float4": BN_FLOAT4, "rgba8": BN_UFIXED8_RGBA, "rgba8_srgb": BN
 EXPORTS = [
     "bnContextCreate", "bnContextDestroy", "bnPhysicalDeviceCount", "bnRelease", "bnAddReference", "bnCommit",
     "bnSet1i", "bnSet2i", "bnSet3i", "bnSet4i", "bnSet1f", "bnSet2f", "bnSet3f", "bnSet4f", "bnSetObject",
-    "bnSetData", "bnDataCreate", "bnTextureData3DCreate", "bnScalarFieldCreate", "bnVolumeCreate",
+    "bnSetData", "bnSetString", "bnSet4x3fv", "bnSet4x4fv", "bnDataCreate", "bnDataSet",
+    "bnTextureData2DCreate", "bnTexture2DCreate", "bnTexture3DCreate", "bnSamplerCreate", "bnTextureData3DCreate", "bnScalarFieldCreate", "bnVolumeCreate",
     "bnVolumeSetXF", "bnLightCreate", "bnGeometryCreate", "bnMaterialCreate", "bnGroupCreate", "bnGroupBuild", "bnModelCreate", "bnSetInstances",
+    "bnUpdateInstanceTransforms", "bnSetInstanceAttributes",
     "bnBuild", "bnCameraCreate", "bnRendererCreate", "bnFrameBufferCreate", "bnFrameBufferResize",
     "bnFrameBufferRead", "bnFrameBufferGetSize", "bnAccumReset", "bnRender", "bnGetLastError",
     "bnGetLastErrorString", "bnClearLastError", "bnxGetStats", "bnxSetStream", "bnxGetStream",
@@ -142,7 +144,14 @@ def lib(build_if_missing=True):
         "bnSet1i": ([P, S, I], None), "bnSet2i": ([P, S, I, I], None), "bnSet3i": ([P, S, I, I, I], None),
         "bnSet4i": ([P, S, I, I, I, I], None), "bnSet1f": ([P, S, F], None), "bnSet2f": ([P, S, F, F], None),
         "bnSet3f": ([P, S, F, F, F], None), "bnSet4f": ([P, S, F, F, F, F], None),
-        "bnSetObject": ([P, S, P], None), "bnSetData": ([P, S, P], None),
+        "bnSetObject": ([P, S, P], None), "bnSetData": ([P, S, P], None), "bnSetString": ([P, S, S], None),
+        "bnSet4x3fv": ([P, S, P], None), "bnSet4x4fv": ([P, S, P], None),
+        "bnDataSet": ([P, ctypes.c_size_t, P], None),
+        "bnTextureData2DCreate": ([P, I, I, I, I, P], P),
+        "bnTexture2DCreate": ([P, I, I, ctypes.c_uint32, ctypes.c_uint32, P, I, I, I, I], P),
+        "bnTexture3DCreate": ([P, I, I, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, P, I, I], P),
+        "bnSamplerCreate": ([P, I, S], P),
+        "bnUpdateInstanceTransforms": ([P, I, P, I], None), "bnSetInstanceAttributes": ([P, I, S, P], None),
         "bnDataCreate": ([P, I, I, ctypes.c_size_t, P], P),
         "bnTextureData3DCreate": ([P, I, I, I, I, I, P], P), "bnScalarFieldCreate": ([P, I, S], P),
         "bnVolumeCreate": ([P, I, P], P), "bnVolumeSetXF": ([P, bn_float2, P, I, F], None),

@@ -553,6 +553,24 @@ BN_API void bnSetObject(BNObject t, const char *n, BNObject v) {
   if (!getObject(t)->setObject(n ? n : "", val)) warnUnsupported(n);
   BN_CATCH()
 }
+BN_API void bnSetString(BNObject t, const char *n, const char *) {
+  BN_TRY
+  getObject(t);
+  warnUnsupported(n);
+  BN_CATCH()
+}
+BN_API void bnSet4x3fv(BNObject t, const char *n, const BNTransform *) {
+  BN_TRY
+  getObject(t);
+  warnUnsupported(n);
+  BN_CATCH()
+}
+BN_API void bnSet4x4fv(BNObject t, const char *n, const bn_float4 *) {
+  BN_TRY
+  getObject(t);
+  warnUnsupported(n);
+  BN_CATCH()
+}
 BN_API void bnSetData(BNObject t, const char *n, BNData v) {
   BN_TRY
   ObjectSP o = getObject(t);
@@ -569,6 +587,44 @@ BN_API void bnSetData(BNObject t, const char *n, BNData v) {
   }
   warnUnsupported(n);
   BN_CATCH()
+}
+
+BN_API void bnDataSet(BNData data, size_t n, const void *items) {  // Data::set
+  BN_TRY
+  auto d = getAs<Data>(data, Object::K_DATA, "BNData");
+  const BNObject *objs = (const BNObject *)items;
+  std::vector<ObjectSP> next;
+  for (size_t i = 0; i < n; i++) next.push_back(objs && objs[i] ? getObject(objs[i]) : nullptr);
+  d->items.swap(next);
+  BN_CATCH()
+}
+
+static void *unsupportedObject(BNContext context, const char *what) {
+  getContext(context);
+  throw Error(E_UNSUPPORTED, std::string(what) + " is not supported (surface materials are not mapped)");
+}
+BN_API BNTextureData bnTextureData2DCreate(BNContext context, int, BNDataType, int, int, const void *) {
+  BN_TRY
+  return (BNTextureData)unsupportedObject(context, "bnTextureData2DCreate");
+  BN_CATCH(nullptr)
+}
+BN_API BNTexture2D bnTexture2DCreate(BNContext context, int, BNDataType, uint32_t, uint32_t, const void *,
+                                     BNTextureFilterMode, BNTextureAddressMode, BNTextureAddressMode,
+                                     BNTextureColorSpace) {
+  BN_TRY
+  return (BNTexture2D)unsupportedObject(context, "bnTexture2DCreate");
+  BN_CATCH(nullptr)
+}
+BN_API BNTexture3D bnTexture3DCreate(BNContext context, int, BNDataType, uint32_t, uint32_t, uint32_t, const void *,
+                                     BNTextureFilterMode, BNTextureAddressMode) {
+  BN_TRY
+  return (BNTexture3D)unsupportedObject(context, "bnTexture3DCreate");
+  BN_CATCH(nullptr)
+}
+BN_API BNSampler bnSamplerCreate(BNContext context, int, const char *) {
+  BN_TRY
+  return (BNSampler)unsupportedObject(context, "bnSamplerCreate");
+  BN_CATCH(nullptr)
 }
 
 BN_API BNData bnDataCreate(BNContext context, int, BNDataType type, size_t n, const void *items) {
@@ -706,19 +762,35 @@ BN_API BNModel bnModelCreate(BNContext context) {
   BN_CATCH(nullptr)
 }
 
+static bool isIdentity(const BNTransform &x) {
+  return x.l.vx.x == 1 && x.l.vx.y == 0 && x.l.vx.z == 0 && x.l.vy.x == 0 && x.l.vy.y == 1 && x.l.vy.z == 0 &&
+         x.l.vz.x == 0 && x.l.vz.y == 0 && x.l.vz.z == 1 && x.p.x == 0 && x.p.y == 0 && x.p.z == 0;
+}
+
 BN_API void bnSetInstances(BNModel model, int, BNGroup *groups, BNTransform *xfms, int n) {
   BN_TRY
   auto m = getAs<Model>(model, Object::K_MODEL, "BNModel");
   if (n > 1) throw Error(E_UNSUPPORTED, "only one instance is supported");
-  if (n == 1 && xfms) {
-    const BNTransform &x = xfms[0];
-    bool identity = x.l.vx.x == 1 && x.l.vx.y == 0 && x.l.vx.z == 0 && x.l.vy.x == 0 && x.l.vy.y == 1 &&
-                    x.l.vy.z == 0 && x.l.vz.x == 0 && x.l.vz.y == 0 && x.l.vz.z == 1 && x.p.x == 0 && x.p.y == 0 &&
-                    x.p.z == 0;
-    if (!identity) throw Error(E_UNSUPPORTED, "only identity instance transforms are supported");
-  }
+  if (n == 1 && xfms && !isIdentity(xfms[0]))
+    throw Error(E_UNSUPPORTED, "only identity instance transforms are supported");
   m->group = (n == 1 && groups) ? getAs<Group>(groups[0], Object::K_GROUP, "BNGroup") : nullptr;
   m->built = false;
+  BN_CATCH()
+}
+
+BN_API void bnUpdateInstanceTransforms(BNModel model, int, BNTransform *xfms, int n) {
+  BN_TRY
+  auto m = getAs<Model>(model, Object::K_MODEL, "BNModel");
+  if (n != (m->group ? 1 : 0)) throw Error(E_INVALID_ARG, "instance count differs from bnSetInstances");
+  if (n == 1 && xfms && !isIdentity(xfms[0]))
+    throw Error(E_UNSUPPORTED, "only identity instance transforms are supported");
+  BN_CATCH()
+}
+
+BN_API void bnSetInstanceAttributes(BNModel model, int, const char *name, BNData data) {
+  BN_TRY
+  getAs<Model>(model, Object::K_MODEL, "BNModel");
+  if (data) warnUnsupported(name);
   BN_CATCH()
 }
 

@@ -6,8 +6,9 @@
 // default arguments.  Code written against that header can be rebuilt
 // against barney_b200 by including this file instead: it re-exports the
 // extern "C" symbols of bn_volume.h inside the same namespace, with the
-// reference's default arguments.  Only the structured-volume subset that
-// bn_volume.h implements is available.
+// reference's default arguments.  Every bn* entry point of barney.h is
+// declared; outside the structured-volume and isosurface path they record
+// an "unsupported" error instead of rendering.
 #pragma once
 #include "bn_volume.h"
 
@@ -24,6 +25,13 @@ using ::BNFrameBuffer;
 using ::BNFrameBufferChannel;
 using ::BNGeom;
 using ::BNGroup;
+using ::BNMaterial;
+using ::BNSampler;
+using ::BNTexture2D;
+using ::BNTexture3D;
+using ::BNTextureAddressMode;
+using ::BNTextureColorSpace;
+using ::BNTextureFilterMode;
 using ::BNLight;
 using ::BNModel;
 using ::BNObject;
@@ -44,6 +52,16 @@ using ::bnCommit;
 using ::bnContextCreate;
 using ::bnContextDestroy;
 using ::bnDataCreate;
+using ::bnDataSet;
+using ::bnGeometryCreate;
+using ::bnMaterialCreate;
+using ::bnSamplerCreate;
+using ::bnSet4x3fv;
+using ::bnSet4x4fv;
+using ::bnSetInstanceAttributes;
+using ::bnSetString;
+using ::bnTextureData2DCreate;
+using ::bnUpdateInstanceTransforms;
 using ::bnFrameBufferGetSize;
 using ::bnFrameBufferRead;
 using ::bnGroupBuild;
@@ -75,6 +93,18 @@ inline BNRenderer bnRendererCreate(BNContext c, const char *type = "default") { 
 inline void bnFrameBufferResize(BNFrameBuffer fb, BNDataType fmt, int sx, int sy,
                                 uint32_t channels = BN_FB_COLOR) {
   ::bnFrameBufferResize(fb, fmt, sx, sy, channels);
+}
+inline BNTexture2D bnTexture2DCreate(BNContext c, int slot, BNDataType fmt, uint32_t sx, uint32_t sy,
+                                     const void *texels, BNTextureFilterMode filter = BN_TEXTURE_LINEAR,
+                                     BNTextureAddressMode ax = BN_TEXTURE_WRAP,
+                                     BNTextureAddressMode ay = BN_TEXTURE_WRAP,
+                                     BNTextureColorSpace cs = BN_COLOR_SPACE_LINEAR) {
+  return ::bnTexture2DCreate(c, slot, fmt, sx, sy, texels, filter, ax, ay, cs);
+}
+inline BNTexture3D bnTexture3DCreate(BNContext c, int slot, BNDataType fmt, uint32_t sx, uint32_t sy, uint32_t sz,
+                                     const void *texels, BNTextureFilterMode filter = BN_TEXTURE_LINEAR,
+                                     BNTextureAddressMode a = BN_TEXTURE_CLAMP) {
+  return ::bnTexture3DCreate(c, slot, fmt, sx, sy, sz, texels, filter, a);
 }
 // barney.h polymorphic setters
 inline void bnSet(BNObject o, const char *n, bn_float2 v) { ::bnSet2f(o, n, v.x, v.y); }

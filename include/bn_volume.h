@@ -46,6 +46,9 @@ typedef BNObject BNTextureData;
 typedef BNObject BNScalarField;
 typedef BNObject BNGeom;
 typedef BNObject BNMaterial;
+typedef BNObject BNSampler;
+typedef BNObject BNTexture2D;
+typedef BNObject BNTexture3D;
 typedef BNObject BNVolume;
 typedef BNObject BNGroup;
 typedef BNObject BNModel;
@@ -128,6 +131,13 @@ BN_API void bnSet4f(BNObject target, const char *paramName, float x, float y, fl
 BN_API void bnSetObject(BNObject target, const char *paramName, BNObject value);
 /* replaces barney.cu bnSetData (Group "lights", Group.cpp:50-51) */
 BN_API void bnSetData(BNObject target, const char *paramName, BNData value);
+/* replace barney.cu:559 bnSetString, :654 bnSet4x3fv, :662 bnSet4x4fv: no
+   object of this path has string or matrix parameters (sampler- or
+   attribute-mapped material inputs are not supported); each records
+   "unsupported parameter" */
+BN_API void bnSetString(BNObject target, const char *paramName, const char *value);
+BN_API void bnSet4x3fv(BNObject target, const char *paramName, const BNTransform *affineMatrix);
+BN_API void bnSet4x4fv(BNObject target, const char *paramName, const bn_float4 *xfm);
 
 /* ---------------------------------------------------------------------- */
 /* scene content                                                           */
@@ -135,6 +145,25 @@ BN_API void bnSetData(BNObject target, const char *paramName, BNData value);
 /* replaces barney.cu bnDataCreate (BN_OBJECT arrays of lights) */
 BN_API BNData bnDataCreate(BNContext context, int whichSlot, BNDataType dataType, size_t numItems,
                            const void *items);
+/* replaces barney.cu:498 bnDataSet: new contents of a BN_OBJECT array */
+BN_API void bnDataSet(BNData data, size_t numItems, const void *items);
+/* barney.h texture and sampler objects (barney.h:203-223 enums; barney.cu:205
+   bnTextureData2DCreate, :242 bnTexture2DCreate, :272 bnTexture3DCreate, :417
+   bnSamplerCreate) feed surface materials, which this path does not map:
+   each returns NULL and records "unsupported" */
+typedef enum { BN_TEXTURE_NEAREST, BN_TEXTURE_LINEAR } BNTextureFilterMode;
+typedef enum { BN_TEXTURE_WRAP, BN_TEXTURE_CLAMP, BN_TEXTURE_BORDER, BN_TEXTURE_MIRROR } BNTextureAddressMode;
+typedef enum { BN_COLOR_SPACE_LINEAR, BN_COLOR_SPACE_SRGB } BNTextureColorSpace;
+BN_API BNTextureData bnTextureData2DCreate(BNContext context, int whichSlot, BNDataType texelFormat, int width,
+                                           int height, const void *items);
+BN_API BNTexture2D bnTexture2DCreate(BNContext context, int whichSlot, BNDataType texelFormat, uint32_t sizeX,
+                                     uint32_t sizeY, const void *texels, BNTextureFilterMode filterMode,
+                                     BNTextureAddressMode addressModeX, BNTextureAddressMode addressModeY,
+                                     BNTextureColorSpace colorSpace);
+BN_API BNTexture3D bnTexture3DCreate(BNContext context, int whichSlot, BNDataType texelFormat, uint32_t sizeX,
+                                     uint32_t sizeY, uint32_t sizeZ, const void *texels,
+                                     BNTextureFilterMode filterMode, BNTextureAddressMode addressMode);
+BN_API BNSampler bnSamplerCreate(BNContext context, int whichSlot, const char *type);
 /* replaces barney.cu:223 bnTextureData3DCreate. texelFormat: BN_FLOAT32,
    BN_UFIXED8 / BN_UINT8 (unorm, x/255), BN_UFIXED16 (unorm, x/65535),
    BNX_FLOAT16, BNX_BFLOAT16. texels may be host or device memory; it is
@@ -180,6 +209,14 @@ BN_API BNModel bnModelCreate(BNContext ctx);
 /* replaces barney.cu bnSetInstances; one group, transform NULL or identity */
 BN_API void bnSetInstances(BNModel model, int whichSlot, BNGroup *groups, BNTransform *xfms,
                            int numInstances);
+/* replaces barney.cu:352 bnUpdateInstanceTransforms: the transforms of the
+   instances bnSetInstances set, which must stay identity */
+BN_API void bnUpdateInstanceTransforms(BNModel model, int whichSlot, BNTransform *instanceTransforms,
+                                       int numInstances);
+/* replaces barney.cu:323 bnSetInstanceAttributes: instance attributes are not
+   read by this path; a NULL array is accepted, any other records
+   "unsupported" */
+BN_API void bnSetInstanceAttributes(BNModel model, int whichSlot, const char *attributeName, BNData data);
 /* replaces barney.cu:542 bnBuild */
 BN_API void bnBuild(BNModel model, int whichSlot);
 

@@ -94,7 +94,16 @@ def test_header_compiles_as_c_and_shim_as_cpp(tmp_path):
     cpp_src.write_text('#include "barney_shim.hpp"\nint main(){ using namespace barney_cuda;\n'
                        ' BNContext c = bnContextCreate(1, nullptr, 0, nullptr);\n'
                        ' BNFrameBuffer fb = bnFrameBufferCreate(c); bnFrameBufferResize(fb, BN_UFIXED8_RGBA, 4, 4);\n'
-                       ' bn_float3 v{1,2,3}; bnSet(fb, "x", v); return 0; }\n')
+                       ' bn_float3 v{1,2,3}; bnSet(fb, "x", v);\n'
+                       # the call forms the ANARI device uses for isosurfaces and materials
+                       ' BNMaterial m = bnMaterialCreate(c, 0, "AnariMatte"); bnSetString(m, "color", "attribute0");\n'
+                       ' BNGeom g = bnGeometryCreate(c, 0, "iso_surface"); bnSetData(g, "isoValues", (BNData)nullptr);\n'
+                       ' BNSampler smp = bnSamplerCreate(c, 0, "texture2D"); bnSetObject(m, "color", smp);\n'
+                       ' BNTexture2D t = bnTexture2DCreate(c, 0, BN_FLOAT4, 2, 2, nullptr); (void)t;\n'
+                       ' BNTexture3D t3 = bnTexture3DCreate(c, 0, BN_FLOAT32, 2, 2, 2, nullptr); (void)t3;\n'
+                       ' BNModel md = bnModelCreate(c); bnUpdateInstanceTransforms(md, 0, nullptr, 0);\n'
+                       ' bnSetInstanceAttributes(md, 0, "color", nullptr); bnDataSet(nullptr, 0, nullptr);\n'
+                       ' return 0; }\n')
     lib_dir = os.path.dirname(bn.LIB_PATH)
     subprocess.run(["g++", "-std=c++17", "-I", os.path.join(ROOT, "include"), str(cpp_src), "-L", lib_dir,
                     "-lbarney_b200", "-Wl,-rpath," + lib_dir, "-o", str(tmp_path / "client")], check=True)
