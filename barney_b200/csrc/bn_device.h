@@ -110,7 +110,7 @@ struct JobDD {
 // busy lanes) need service -- shading, accumulation, a new ray -- and then
 // serves them together.
 struct SchedDD {
-  int serviceBatch = 24;
+  int serviceBatch = 22;
 };
 
 // Device counters of one launch (samples, mcVisits, rays, errorFlags)

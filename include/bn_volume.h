@@ -300,7 +300,7 @@ BN_API void bnxSetLaunchConfig(BNContext context, int blocksPerSM, int threadsPe
 /* Warp scheduling of the render kernel: a warp keeps stepping macrocells and
    Woodcock ranges until at least serviceBatch of its lanes (or all of its
    busy lanes) need service -- shading, accumulation, a new ray -- and then
-   serves them together (1..32, default 24). */
+   serves them together (1..32, default 22). */
 BN_API void bnxSetScheduling(BNContext context, int serviceBatch);
 /* Render several jobs in one persistent launch (each job: renderer, model,
    camera, frame buffer of this context; distinct frame buffers).  Same
