@@ -472,7 +472,7 @@ class VolumeRenderer:
         check()
         return ranges, maj
 
-    def set_scheduling(self, service_batch=16):
+    def set_scheduling(self, service_batch=22):
         self.L.bnxSetScheduling(self.ctx, service_batch)
         check()
 
