@@ -343,6 +343,7 @@ class VolumeRenderer:
         self.group = self._keep(L.bnGroupCreate(self.ctx, 0, geoms, n_geoms, vols, 1 if with_vol else 0))
         check()
         lights = desc.get("dir_lights", [])
+        self.lights_data = None
         if lights:
             hs = []
             for l in lights:
@@ -355,6 +356,7 @@ class VolumeRenderer:
                 hs.append(h)
             arr = (ctypes.c_void_p * len(hs))(*hs)
             data = self._keep(L.bnDataCreate(self.ctx, 0, BN_OBJECT, len(hs), arr))
+            self.lights_data = data
             L.bnSetData(self.group, b"lights", data)
         L.bnGroupBuild(self.group)
         check()

@@ -287,3 +287,38 @@ def test_long_accumulation_in_a_thin_frame():
     img, _ = gpu_render(d, 7, renders=3)  # accumIDs 0..20
     ref, _, _ = oracle_render(d, 21)
     assert_bitexact(img, ref, "3 x 7 waves")
+
+
+def test_data_set_and_instance_transform_updates():
+    """bnDataSet replaces the group's light list in place; bnUpdateInstanceTransforms
+    accepts the identity for the one instance and rejects anything else."""
+    import ctypes
+    bn = _bn()
+    d = small_noise_scene()
+    r = bn.VolumeRenderer(d)
+    L = r.L
+    try:
+        L.bnClearLastError()
+        L.bnDataSet(r.lights_data, 0, None)  # no directional lights any more
+        assert L.bnGetLastError() == 0
+        r.set_spp(2)
+        r.render()
+        ref, _, _ = oracle_render(dict(d, dir_lights=[]), 2)
+        assert_bitexact(r.read(), ref, "lights removed by bnDataSet")
+
+        class BNTransform(ctypes.Structure):
+            _fields_ = [("m", ctypes.c_float * 12)]
+        ident = BNTransform()
+        ident.m[:] = (1, 0, 0, 0, 1, 0, 0, 0, 1, 0, 0, 0)
+        L.bnUpdateInstanceTransforms(r.model, 0, ctypes.byref(ident), 1)
+        assert L.bnGetLastError() == 0
+        moved = BNTransform()
+        moved.m[:] = (1, 0, 0, 0, 1, 0, 0, 0, 1, 0.5, 0, 0)
+        L.bnUpdateInstanceTransforms(r.model, 0, ctypes.byref(moved), 1)
+        assert L.bnGetLastError() == 3
+        L.bnClearLastError()
+        L.bnUpdateInstanceTransforms(r.model, 0, ctypes.byref(ident), 2)
+        assert L.bnGetLastError() == 2
+        L.bnClearLastError()
+    finally:
+        r.close()
