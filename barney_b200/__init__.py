@@ -18,7 +18,9 @@ import numpy as np
 from . import build as _build
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = _build.LIB
+# BARNEY_B200_LIBRARY selects another build of the library, e.g. the
+# bounds-checked libbarney_b200_bc.so; it is loaded as it is, never rebuilt
+LIB_PATH = os.environ.get("BARNEY_B200_LIBRARY") or _build.LIB
 _lib = None
 
 # BNDataType values (include/bn_volume.h)
@@ -49,7 +51,7 @@ EXPORTS = [
     "bnFrameBufferRead", "bnFrameBufferGetSize", "bnAccumReset", "bnRender", "bnGetLastError",
     "bnGetLastErrorString", "bnClearLastError", "bnxGetStats", "bnxSetStream", "bnxGetStream",
     "bnxSetLaunchConfig", "bnxFrameBufferDevicePointer", "bnxVolumeGetMacrocells",
-    "bnxRenderStructuredNoAlloc", "bnxSetScheduling", "bnxRenderBatch", "bnxSetBatchGraphs", "bnxAutotuneBatch",
+    "bnxRenderStructuredNoAlloc", "bnxSetScheduling", "bnxBoundsViolations", "bnxRenderBatch", "bnxSetBatchGraphs", "bnxAutotuneBatch",
     "bnxServerCreate", "bnxServerDestroy", "bnxServerSubmit", "bnxServerWait", "bnxServerGetStats",
     "bnxServerResetStats", "bnxServerReserve", "bnxSetRenderTimeout", "bnxSetPixelPartition",
     "bnxPixelPartitionOwners", "bnxAnariTransferFunction1D", "bnxAnariDensityScale",
@@ -132,7 +134,7 @@ def lib(build_if_missing=True):
     global _lib
     if _lib is not None:
         return _lib
-    if build_if_missing and _build._stale():
+    if build_if_missing and LIB_PATH == _build.LIB and _build._stale():
         _build.build()
     if not os.path.exists(LIB_PATH):
         raise BarneyError("libbarney_b200.so is missing; run barney_b200.build.build()")
@@ -167,7 +169,8 @@ def lib(build_if_missing=True):
         "bnxSetLaunchConfig": ([P, I, I], None), "bnxFrameBufferDevicePointer": ([P], P),
         "bnxVolumeGetMacrocells": ([P, P, P, P], None),
         "bnxRenderStructuredNoAlloc": ([P, P], I),
-        "bnxSetScheduling": ([P, I], None), "bnxRenderBatch": ([P, P, I], None),
+        "bnxSetScheduling": ([P, I], None), "bnxBoundsViolations": ([P], ctypes.c_longlong),
+        "bnxRenderBatch": ([P, P, I], None),
         "bnxSetBatchGraphs": ([P, I], None), "bnxAutotuneBatch": ([P, P, I, P], None),
         "bnxServerCreate": ([P, P], P), "bnxServerDestroy": ([P], None),
         "bnxServerSubmit": ([P, P], ctypes.c_longlong), "bnxServerWait": ([P, ctypes.c_longlong, I, P], I),

@@ -1,6 +1,7 @@
 """Build recipe for libbarney_b200.so (in-tree, sm_100a only).
 
     python -m barney_b200.build          # or barney_b200.build.build()
+    python -m barney_b200.build --bounds-check   # libbarney_b200_bc.so, every access checked
 
 Device code: --fmad=false with IEEE division and square root, so the kernels
 evaluate every FP32 expression exactly as written (bit-identical to the CPU
@@ -14,6 +15,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libbarney_b200.so")
+LIB_BC = os.path.join(HERE, "libbarney_b200_bc.so")  # bounds-checked build (-DBNB_BOUNDS_CHECK)
 SOURCES = ["bn_kernels.cu", "bn_api.cpp", "bn_server.cpp"]
 HEADERS = ["bn_device.h", "bn_objects.h", os.path.join("..", "..", "include", "bn_volume.h")]
 
@@ -33,70 +35,76 @@ def nvcc():
     return "nvcc"
 
 
-def _digest():
+def _digest(bounds_check=False):
     """Content hash of every input of the build (sources, headers, flags)."""
     import hashlib
-    h = hashlib.sha1(" ".join(NVCC_FLAGS).encode())
+    h = hashlib.sha1((" ".join(NVCC_FLAGS) + (" -DBNB_BOUNDS_CHECK" if bounds_check else "")).encode())
     for s in SOURCES + HEADERS:
         with open(os.path.join(CSRC, s), "rb") as f:
             h.update(f.read())
     return h.hexdigest()
 
 
-def _stale():
-    """True unless libbarney_b200.so was built from the current sources
-    (content hash, so copies that reset file times do not force a rebuild)."""
-    if not os.path.exists(LIB) or not os.path.exists(LIB + ".sha1"):
+def _stale(bounds_check=False):
+    """True unless the library was built from the current sources (content
+    hash, so copies that reset file times do not force a rebuild)."""
+    lib = LIB_BC if bounds_check else LIB
+    if not os.path.exists(lib) or not os.path.exists(lib + ".sha1"):
         return True
-    with open(LIB + ".sha1") as f:
-        return f.read().strip() != _digest()
+    with open(lib + ".sha1") as f:
+        return f.read().strip() != _digest(bounds_check)
 
 
-def build(force=False, verbose=False):
-    """Compile every source for sm_100a into barney_b200/libbarney_b200.so.
+def build(force=False, verbose=False, bounds_check=False):
+    """Compile every source for sm_100a into barney_b200/libbarney_b200.so
+    (bounds_check: libbarney_b200_bc.so with -DBNB_BOUNDS_CHECK).
     Processes that find the library stale at the same time (ranks of one job)
     build it once: the build holds an exclusive lock, and whoever gets the
     lock next sees the fresh library."""
-    if not force and not _stale():
-        return LIB
+    lib = LIB_BC if bounds_check else LIB
+    if not force and not _stale(bounds_check):
+        return lib
     import fcntl
-    with open(LIB + ".lock", "w") as lock:
+    with open(lib + ".lock", "w") as lock:
         fcntl.flock(lock, fcntl.LOCK_EX)
-        if not force and not _stale():
-            return LIB
-        return _build_locked(verbose)
+        if not force and not _stale(bounds_check):
+            return lib
+        return _build_locked(verbose, bounds_check)
 
 
-def _build_locked(verbose):
+def _build_locked(verbose, bounds_check=False):
+    LIB_OUT = LIB_BC if bounds_check else LIB
+    flags = NVCC_FLAGS + (["-DBNB_BOUNDS_CHECK"] if bounds_check else [])
     objs = []
     logs = []
     for src in SOURCES:
-        obj = os.path.join(CSRC, os.path.splitext(src)[0] + ".o")
-        cmd = [nvcc(), *NVCC_FLAGS, "-c", os.path.join(CSRC, src), "-o", obj]
+        obj = os.path.join(CSRC, os.path.splitext(src)[0] + ("_bc.o" if bounds_check else ".o"))
+        cmd = [nvcc(), *flags, "-c", os.path.join(CSRC, src), "-o", obj]
         r = subprocess.run(cmd, capture_output=True, text=True)
         logs.append(r.stdout + r.stderr)
         if r.returncode != 0:
             sys.stderr.write(r.stdout + r.stderr)
             raise RuntimeError("nvcc failed on " + src)
         objs.append(obj)
-    tmp = LIB + ".tmp"
+    tmp = LIB_OUT + ".tmp"
     cmd = [nvcc(), "-gencode", "arch=compute_100a,code=sm_100a", "-shared", "-o", tmp, *objs,
            "-Xcompiler", "-fPIC"]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         sys.stderr.write(r.stdout + r.stderr)
         raise RuntimeError("link failed")
-    os.replace(tmp, LIB)
-    with open(LIB + ".sha1", "w") as f:
-        f.write(_digest())
+    os.replace(tmp, LIB_OUT)
+    with open(LIB_OUT + ".sha1", "w") as f:
+        f.write(_digest(bounds_check))
     for o in objs:
         os.remove(o)
-    with open(os.path.join(CSRC, "ptxas.log"), "w") as f:
-        f.write("\n".join(logs))
+    if not bounds_check:
+        with open(os.path.join(CSRC, "ptxas.log"), "w") as f:
+            f.write("\n".join(logs))
     if verbose:
         print("\n".join(logs))
-    return LIB
+    return LIB_OUT
 
 
 if __name__ == "__main__":
-    print(build(force="--force" in sys.argv, verbose=True))
+    print(build(force="--force" in sys.argv, verbose=True, bounds_check="--bounds-check" in sys.argv))

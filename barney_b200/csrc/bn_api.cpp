@@ -1031,6 +1031,14 @@ BN_API int bnxRenderStructuredNoAlloc(const BNXNoAllocFrame *f, void *stream) {
   BN_CATCH(g_lastError)
 }
 
+BN_API long long bnxBoundsViolations(BNContext context) {
+  BN_TRY
+  if (!boundsCheckedBuild()) return -1;  // the normal build has no checks
+  getContext(context)->activate();
+  return readBoundsViolations();
+  BN_CATCH(-2)
+}
+
 BN_API void bnxSetScheduling(BNContext context, int serviceBatch) {
   BN_TRY
   Context *c = getContext(context);

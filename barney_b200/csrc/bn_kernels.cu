@@ -33,6 +33,22 @@ namespace bnb {
 
 #define DEV __device__ __forceinline__
 
+// Bounds-checked build (-DBNB_BOUNDS_CHECK, libbarney_b200_bc.so): every
+// indexed access of the render and macrocell kernels is checked first; an
+// index outside its array is counted in g_boundsViolations and the access is
+// skipped.  In the normal build BNB_IN is true and the checks compile away.
+#ifdef BNB_BOUNDS_CHECK
+__device__ unsigned long long g_boundsViolations;
+__device__ __forceinline__ bool bnbIn(long long i, long long n) {
+  if (i >= 0 && i < n) return true;
+  atomicAdd(&g_boundsViolations, 1ull);
+  return false;
+}
+#define BNB_IN(i, n) bnbIn((long long)(i), (long long)(n))
+#else
+#define BNB_IN(i, n) true
+#endif
+
 #define kInf __int_as_float(0x7f800000)
 // math.h:13-18
 #define ONE_PI_F 3.14159265358979323846f
@@ -181,6 +197,8 @@ DEV float sampleField(const VolumeDD &v, float3 P, const float *u8lut) {
   const int64_t nx = v.numScalars.x, nxy = (int64_t)v.numScalars.x * v.numScalars.y;
   const int64_t b = (int64_t)x0 + nx * y0 + nxy * z0;
   const int64_t oy = dy ? nx : 0, oz = dz ? nxy : 0;
+  if (!BNB_IN(b, nxy * v.numScalars.z) || !BNB_IN(b + oz + oy + dx, nxy * v.numScalars.z))
+    return __int_as_float(0x7fc00000);
   float v000 = loadVoxel<T>(v.voxels, b, u8lut);
   float v001 = loadVoxel<T>(v.voxels, b + dx, u8lut);
   float v010 = loadVoxel<T>(v.voxels, b + oy, u8lut);
@@ -313,6 +331,7 @@ __global__ void __launch_bounds__(128) mcBuildKernel(VolumeDD v, float2 *ranges,
     const int z1 = min(z0 + kCellsPerMC, v.numScalars.z - 1);
     float lo = kInf, hi = -kInf;
     const int64_t nx = v.numScalars.x, nxy = (int64_t)v.numScalars.x * v.numScalars.y;
+    if (!BNB_IN(x1 + nx * y1 + nxy * z1, nxy * v.numScalars.z)) continue;
     for (int z = z0; z <= z1; z++)
       for (int y = y0; y <= y1; y++) {
         const int64_t row = nx * y + nxy * z;
@@ -670,7 +689,10 @@ DEV float isoIntersect(const VolumeDD &v, float3 org, float3 dir, float tMax, ui
     // the macrocell callback
     const float upper = fmin_(ct1, tMax);
     if (ct0 < upper) {
-      const float2 rg = __ldg(v.iso.ranges + (cx + v.mcDims.x * (cy + v.mcDims.y * cz)));
+      const int rci = cx + v.mcDims.x * (cy + v.mcDims.y * cz);
+      const float2 rg = BNB_IN(rci, (long long)v.mcDims.x * v.mcDims.y * v.mcDims.z)
+                            ? __ldg(v.iso.ranges + rci)
+                            : make_float2(1.f, 0.f);  // (bounds-checked build: an empty range)
       if (iso >= rg.x && iso <= rg.y) {
         float tt1 = ct0;
         float ff1 = sampleJob<T>(v, f3(org.x + tt1 * dir.x, org.y + tt1 * dir.y, org.z + tt1 * dir.z), u8lut);
@@ -1192,8 +1214,10 @@ DEV void renderLoop(const JobDD *__restrict__ jobs, const int *__restrict__ chun
             steps = 0;
             phase = LP_BEGIN;
           } else if (++k == fr.spp) {  // no ray left: the wave is done
-            fr.accum[pix] = acc;
-            if (cmp) fr.comp[pix] = comp;
+            if (BNB_IN(pix, (long long)fr.width * fr.height)) {
+              fr.accum[pix] = acc;
+              if (cmp) fr.comp[pix] = comp;
+            }
             phase = LP_IDLE;
           } else {
             phase = LP_NEWSAMPLE;
@@ -1254,8 +1278,10 @@ DEV void renderLoop(const JobDD *__restrict__ jobs, const int *__restrict__ chun
           steps = 0;
           phase = LP_BEGIN;
         } else if (++k == fr.spp) {
-          fr.accum[pix] = acc;
-          if (cmp) fr.comp[pix] = comp;
+          if (BNB_IN(pix, (long long)fr.width * fr.height)) {
+            fr.accum[pix] = acc;
+            if (cmp) fr.comp[pix] = comp;
+          }
           phase = LP_IDLE;
         } else {
           phase = LP_NEWSAMPLE;
@@ -1312,8 +1338,9 @@ DEV void renderLoop(const JobDD *__restrict__ jobs, const int *__restrict__ chun
         iy = 4 * band + within % rows;
         pix = (int64_t)iy * W + ix;
         k = 0;
-        acc = fr.accumID0 > 0 ? fr.accum[pix] : make_float4(0.f, 0.f, 0.f, 0.f);
-        comp = (fr.accumID0 > 0 && fr.comp) ? fr.comp[pix] : make_float4(0.f, 0.f, 0.f, 0.f);
+        const bool pixIn = BNB_IN(pix, (long long)fr.width * fr.height);
+        acc = (fr.accumID0 > 0 && pixIn) ? fr.accum[pix] : make_float4(0.f, 0.f, 0.f, 0.f);
+        comp = (fr.accumID0 > 0 && fr.comp && pixIn) ? fr.comp[pix] : make_float4(0.f, 0.f, 0.f, 0.f);
         phase = LP_NEWSAMPLE;
       }
       for (int i = 0; i < take; i++) need &= need - 1u;
@@ -1423,7 +1450,8 @@ DEV void renderLoop(const JobDD *__restrict__ jobs, const int *__restrict__ chun
             const float tClosest = fmin_(fmin_(ts.tNext.x, ts.tNext.y), ts.tNext.z);
             // cell indices are inside the grid here and the grid has < 2^31 cells
             const int ci = ts.cx + v.mcDims.x * (ts.cy + v.mcDims.y * ts.cz);
-            const bool occupied = (__ldg(v.mcOccupied + (ci >> 5)) >> (ci & 31)) & 1u;
+            const bool occupied = BNB_IN(ci, (long long)v.mcDims.x * v.mcDims.y * v.mcDims.z) &&
+                                  ((__ldg(v.mcOccupied + (ci >> 5)) >> (ci & 31)) & 1u);
             nVisits++;
             if (!occupied) {  // majorant == 0
               if (!ddaStep(v, ts, tClosest)) { phase = LP_ENDED; break; }
@@ -1463,6 +1491,7 @@ DEV void renderLoop(const JobDD *__restrict__ jobs, const int *__restrict__ chun
               f *= (float)(v.tfN - 1);
               idx = min(v.tfN - 2, max(0, (int)f));
               f -= (float)idx;
+              if (!BNB_IN(idx, v.tfN - 1)) idx = 0;
               const float w0 = BATCH ? __ldg(&v.tf[idx].w) : sTF[idx].w;
               const float w1 = BATCH ? __ldg(&v.tf[idx + 1].w) : sTF[idx + 1].w;
               w = ((1.f - f) * w0 + f * w1) * v.baseDensity;
@@ -1753,6 +1782,27 @@ cudaError_t launchResolve(const float4 *accum, int n, int accumID, int fmt, void
   return cudaGetLastError();
 }
 
+bool boundsCheckedBuild() {
+#ifdef BNB_BOUNDS_CHECK
+  return true;
+#else
+  return false;
+#endif
+}
+
+// Out-of-range accesses the bounds-checked build has counted (and resets
+// the count); -1 in the normal build.
+long long readBoundsViolations() {
+#ifdef BNB_BOUNDS_CHECK
+  unsigned long long n = 0, zero = 0;
+  if (cudaMemcpyFromSymbol(&n, g_boundsViolations, sizeof n) != cudaSuccess) return -2;
+  if (cudaMemcpyToSymbol(g_boundsViolations, &zero, sizeof zero) != cudaSuccess) return -2;
+  return (long long)n;
+#else
+  return -1;
+#endif
+}
+
 int renderKernelMaxBlocksPerSM(int tpb) {
   int occ = 0;
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, renderKernel<VOX_F32, 0, 0>, tpb, 256 * sizeof(float4)) !=
@@ -1798,6 +1848,7 @@ __global__ void __launch_bounds__(128) mcMajorantScratchKernel(VolumeDD v, int r
     const int z1 = min(z0 + kCellsPerMC, v.numScalars.z - 1);
     float lo = kInf, hi = -kInf;
     const int64_t nx = v.numScalars.x, nxy = (int64_t)v.numScalars.x * v.numScalars.y;
+    if (!BNB_IN(x1 + nx * y1 + nxy * z1, nxy * v.numScalars.z)) continue;
     for (int z = z0; z <= z1; z++)
       for (int y = y0; y <= y1; y++) {
         const int64_t row = nx * y + nxy * z;

@@ -302,6 +302,12 @@ BN_API void bnxSetLaunchConfig(BNContext context, int blocksPerSM, int threadsPe
    busy lanes) need service -- shading, accumulation, a new ray -- and then
    serves them together (1..32, default 22). */
 BN_API void bnxSetScheduling(BNContext context, int serviceBatch);
+/* Bounds-checked build (libbarney_b200_bc.so, python -m barney_b200.build
+   --bounds-check): every indexed access of the render and macrocell kernels
+   is checked; an out-of-range index is counted and the access skipped.
+   Returns the count since the last call on this context's device (and resets
+   it), -1 in the normal build, -2 on error. */
+BN_API long long bnxBoundsViolations(BNContext context);
 /* Render several jobs in one persistent launch (each job: renderer, model,
    camera, frame buffer of this context; distinct frame buffers).  Same
    result as one bnRender per job, bit for bit.  The launch sequence is

@@ -132,3 +132,11 @@ def test_frame_sizes_beyond_32_bit_pixel_indices_are_rejected_without_a_gpu():
     L.bnxPixelPartitionOwners(0, 5, 1, owners.ctypes.data)  # empty frame
     assert L.bnGetLastError() == 2
     L.bnClearLastError()
+
+
+def test_normal_build_reports_no_bounds_checking():
+    # bnxBoundsViolations is -1 in the normal build, before it needs a context
+    L = bn.lib()
+    L.bnClearLastError()
+    assert L.bnxBoundsViolations(None) == -1
+    assert L.bnGetLastError() == 0
