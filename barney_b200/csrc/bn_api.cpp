@@ -93,6 +93,7 @@ void Volume::uploadTF() {
 }
 
 void Volume::build() {
+  NvtxRange range("volume build");
   if (!sf || !sf->scalars) throw Error(E_STATE, "volume's scalar field has no textureData");
   if (!built) {
     int d[3];
@@ -127,6 +128,7 @@ void Volume::commit() {  // Volume.cpp:26-35
 // MCIsoSurfaceAccel::build (MCAccelerator.h:200-230): the field's macrocell
 // scalar ranges, when no volume of the group has built them
 void IsoSurface::buildRanges() {
+  NvtxRange range("isosurface ranges");
   if (!sf) throw Error(E_STATE, "isoSurface has no scalarField");
   if (rangesOf == sf.get() && rangesTex == sf->scalars.get() && ranges.ptr &&
       !memcmp(rangesDims, sf->numScalars, sizeof rangesDims))
@@ -293,6 +295,7 @@ static bool waitWithDeadline(Context *ctx, cudaEvent_t done, std::chrono::steady
 }
 
 static void render(Context *ctx, Renderer &r, Model &m, Camera &cam, FrameBuffer &fb) {
+  NvtxRange range("bnRender");
   const auto start = std::chrono::steady_clock::now();
   JobDD job = buildJob(ctx, r, m, cam, fb);
   if (job.fr.spp <= 0) return;
@@ -345,6 +348,7 @@ void reserveBatch(Context *ctx, int n) {
 // replayed; per-frame values (cameras, accumIDs) travel in the pinned job
 // table the graph copies from.  Results equal one bnRender per job.
 void renderBatch(Context *ctx, const std::vector<BatchEntry> &entries) {
+  NvtxRange range("bnxRenderBatch");
   const auto start = std::chrono::steady_clock::now();
   const int n = (int)entries.size();
   if (n == 0) return;
@@ -862,6 +866,7 @@ BN_API void bnFrameBufferGetSize(BNFrameBuffer fbh, int *sx, int *sy) {
 }
 
 BN_API void bnFrameBufferRead(BNFrameBuffer fbh, BNFrameBufferChannel ch, void *ptr, BNDataType fmt) {
+  NvtxRange range("bnFrameBufferRead");
   BN_TRY
   auto fb = getAs<FrameBuffer>(fbh, Object::K_FB, "BNFrameBuffer");
   if (!ptr) return;  // FrameBuffer.cu:319

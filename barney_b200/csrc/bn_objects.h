@@ -16,6 +16,7 @@
 #include "bn_device.h"
 
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include <algorithm>
 #include <cmath>
@@ -81,6 +82,17 @@ struct DeviceBuffer {
 };
 
 struct Context;
+
+// NVTX range for the length of a scope: the host stages of a frame (render,
+// batch, server slice, macrocell build, read-back) show up as named ranges
+// in NVTX-aware tools (ncu --nvtx); without a tool attached a push/pop is a
+// check of one pointer.
+struct NvtxRange {
+  explicit NvtxRange(const char *name) { nvtxRangePushA(name); }
+  ~NvtxRange() { nvtxRangePop(); }
+  NvtxRange(const NvtxRange &) = delete;
+  NvtxRange &operator=(const NvtxRange &) = delete;
+};
 
 // ---------------------------------------------------------------------------
 // objects (Object.h:42-56 set/commit interface)

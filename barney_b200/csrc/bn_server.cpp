@@ -309,6 +309,7 @@ struct Server {
         entries.push_back({r->renderer.get(), r->model.get(), r->camera.get(), r->fb.get()});
       }
       const auto t0 = Clock::now();
+      NvtxRange range("server slice");
       std::string err;
       const bool graphs = ctx->useGraphs;
       ctx->useGraphs = false;  // the batch changes every slice: plain launches
