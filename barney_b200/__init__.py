@@ -51,7 +51,8 @@ EXPORTS = [
     "bnFrameBufferRead", "bnFrameBufferGetSize", "bnAccumReset", "bnRender", "bnGetLastError",
     "bnGetLastErrorString", "bnClearLastError", "bnxGetStats", "bnxSetStream", "bnxGetStream",
     "bnxSetLaunchConfig", "bnxFrameBufferDevicePointer", "bnxVolumeGetMacrocells",
-    "bnxRenderStructuredNoAlloc", "bnxSetScheduling", "bnxBoundsViolations", "bnxRenderBatch", "bnxSetBatchGraphs", "bnxAutotuneBatch",
+    "bnxRenderStructuredNoAlloc", "bnxSetScheduling", "bnxBoundsViolations", "bnxFrameBufferCheckpointSize",
+    "bnxFrameBufferCheckpoint", "bnxFrameBufferRestore", "bnxRenderBatch", "bnxSetBatchGraphs", "bnxAutotuneBatch",
     "bnxServerCreate", "bnxServerDestroy", "bnxServerSubmit", "bnxServerWait", "bnxServerGetStats",
     "bnxServerResetStats", "bnxServerReserve", "bnxSetRenderTimeout", "bnxSetPixelPartition",
     "bnxPixelPartitionOwners", "bnxAnariTransferFunction1D", "bnxAnariDensityScale",
@@ -170,6 +171,8 @@ def lib(build_if_missing=True):
         "bnxVolumeGetMacrocells": ([P, P, P, P], None),
         "bnxRenderStructuredNoAlloc": ([P, P], I),
         "bnxSetScheduling": ([P, I], None), "bnxBoundsViolations": ([P], ctypes.c_longlong),
+        "bnxFrameBufferCheckpointSize": ([P], ctypes.c_size_t), "bnxFrameBufferCheckpoint": ([P, P], None),
+        "bnxFrameBufferRestore": ([P, P, ctypes.c_size_t], None),
         "bnxRenderBatch": ([P, P, I], None),
         "bnxSetBatchGraphs": ([P, I], None), "bnxAutotuneBatch": ([P, P, I, P], None),
         "bnxServerCreate": ([P, P], P), "bnxServerDestroy": ([P], None),
@@ -444,6 +447,20 @@ class VolumeRenderer:
 
     def accum_reset(self):
         self.L.bnAccumReset(self.fb)
+        check()
+
+    def checkpoint(self):
+        """The frame buffer's progressive state (bnxFrameBufferCheckpoint) as bytes."""
+        n = self.L.bnxFrameBufferCheckpointSize(self.fb)
+        check()
+        buf = ctypes.create_string_buffer(n)
+        self.L.bnxFrameBufferCheckpoint(self.fb, buf)
+        check()
+        return buf.raw
+
+    def restore(self, data):
+        """Continue from a checkpoint of a frame buffer of the same size."""
+        self.L.bnxFrameBufferRestore(self.fb, data, len(data))
         check()
 
     def read(self, out=None):

@@ -880,6 +880,71 @@ BN_API void bnFrameBufferRead(BNFrameBuffer fbh, BNFrameBufferChannel ch, void *
   BN_CATCH()
 }
 
+// checkpoint header of bnxFrameBufferCheckpoint
+struct CheckpointHeader {
+  uint32_t magic, version;
+  int32_t width, height;
+  uint32_t accumID, hasComp, reserved[2];
+};
+static_assert(sizeof(CheckpointHeader) == 32, "checkpoint header is 32 bytes");
+static constexpr uint32_t kCheckpointMagic = 0x43584E42u;  // "BNXC"
+
+BN_API size_t bnxFrameBufferCheckpointSize(BNFrameBuffer fbh) {
+  BN_TRY
+  auto fb = getAs<FrameBuffer>(fbh, Object::K_FB, "BNFrameBuffer");
+  if (fb->width <= 0 || fb->height <= 0) throw Error(E_STATE, "frame buffer has not been resized");
+  const size_t px = (size_t)fb->width * fb->height * sizeof(float4);
+  return sizeof(CheckpointHeader) + px + (fb->comp.ptr ? px : 0);
+  BN_CATCH(0)
+}
+
+BN_API void bnxFrameBufferCheckpoint(BNFrameBuffer fbh, void *out) {
+  BN_TRY
+  auto fb = getAs<FrameBuffer>(fbh, Object::K_FB, "BNFrameBuffer");
+  if (!out) throw Error(E_INVALID_ARG, "null checkpoint destination");
+  if (fb->width <= 0 || fb->height <= 0) throw Error(E_STATE, "frame buffer has not been resized");
+  Context *ctx = fb->ctx;
+  ctx->activate();
+  CheckpointHeader h{kCheckpointMagic, 1u, fb->width, fb->height, fb->accumID, fb->comp.ptr ? 1u : 0u, {0u, 0u}};
+  memcpy(out, &h, sizeof h);
+  const size_t px = (size_t)fb->width * fb->height * sizeof(float4);
+  char *dst = (char *)out + sizeof h;
+  ck(cudaMemcpyAsync(dst, fb->accum.ptr, px, cudaMemcpyDeviceToHost, ctx->stream), "checkpoint");
+  if (fb->comp.ptr) ck(cudaMemcpyAsync(dst + px, fb->comp.ptr, px, cudaMemcpyDeviceToHost, ctx->stream), "checkpoint");
+  ck(cudaStreamSynchronize(ctx->stream), "checkpoint");
+  BN_CATCH()
+}
+
+BN_API void bnxFrameBufferRestore(BNFrameBuffer fbh, const void *in, size_t bytes) {
+  BN_TRY
+  auto fb = getAs<FrameBuffer>(fbh, Object::K_FB, "BNFrameBuffer");
+  if (!in || bytes < sizeof(CheckpointHeader)) throw Error(E_INVALID_ARG, "checkpoint too short");
+  CheckpointHeader h;
+  memcpy(&h, in, sizeof h);
+  if (h.magic != kCheckpointMagic || h.version != 1u) throw Error(E_INVALID_ARG, "not a frame buffer checkpoint");
+  if (h.width != fb->width || h.height != fb->height)
+    throw Error(E_INVALID_ARG, "checkpoint size differs from the frame buffer's");
+  const size_t px = (size_t)fb->width * fb->height * sizeof(float4);
+  if (bytes != sizeof h + px + (h.hasComp ? px : 0)) throw Error(E_INVALID_ARG, "checkpoint length is wrong");
+  Context *ctx = fb->ctx;
+  ctx->activate();
+  const char *src = (const char *)in + sizeof h;
+  ck(cudaMemcpyAsync(fb->accum.ptr, src, px, cudaMemcpyHostToDevice, ctx->stream), "restore");
+  if (h.hasComp) {
+    if (!fb->comp.ptr) fb->comp.resize(px);
+    ck(cudaMemcpyAsync(fb->comp.ptr, src + px, px, cudaMemcpyHostToDevice, ctx->stream), "restore");
+  } else if (fb->comp.ptr) {
+    ck(cudaMemsetAsync(fb->comp.ptr, 0, px, ctx->stream), "restore");
+  }
+  fb->accumID = h.accumID;
+  if (h.accumID > 0)
+    ck(launchResolve((const float4 *)fb->accum.ptr, fb->width * fb->height, (int)fb->accumID, fb->colorFormat,
+                     fb->color.ptr, ctx->stream, h.hasComp ? (const float4 *)fb->comp.ptr : nullptr),
+       "resolve kernel");
+  ck(cudaStreamSynchronize(ctx->stream), "restore");
+  BN_CATCH()
+}
+
 BN_API void bnAccumReset(BNFrameBuffer fbh) {
   BN_TRY
   getAs<FrameBuffer>(fbh, Object::K_FB, "BNFrameBuffer")->accumID = 0;

@@ -308,6 +308,20 @@ BN_API void bnxSetScheduling(BNContext context, int serviceBatch);
    Returns the count since the last call on this context's device (and resets
    it), -1 in the normal build, -2 on error. */
 BN_API long long bnxBoundsViolations(BNContext context);
+
+/* Checkpoint / resume of a frame buffer's progressive state (the reference's
+   only resumable state: the accumulation tiles and accumID, FrameBuffer.h:147).
+   Layout: a 32-byte header (uint32 magic 0x43584E42 "BNXC", version 1, width,
+   height, accumID, compensation flag, 2 reserved), the width*height float4
+   accumulation buffer and, with the flag set, its float4 compensation terms. */
+BN_API size_t bnxFrameBufferCheckpointSize(BNFrameBuffer fb);
+/* writes bnxFrameBufferCheckpointSize(fb) bytes to host memory */
+BN_API void bnxFrameBufferCheckpoint(BNFrameBuffer fb, void *hostOut);
+/* fb must be resized to the checkpoint's width and height; restores accumID
+   and the buffers and resolves the colour buffer again, so that reads return
+   the checkpointed frame and the next bnRender continues its accumulation
+   exactly as if it had never stopped */
+BN_API void bnxFrameBufferRestore(BNFrameBuffer fb, const void *hostIn, size_t bytes);
 /* Render several jobs in one persistent launch (each job: renderer, model,
    camera, frame buffer of this context; distinct frame buffers).  Same
    result as one bnRender per job, bit for bit.  The launch sequence is
