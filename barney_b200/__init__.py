@@ -51,7 +51,7 @@ EXPORTS = [
     "bnFrameBufferRead", "bnFrameBufferGetSize", "bnAccumReset", "bnRender", "bnGetLastError",
     "bnGetLastErrorString", "bnClearLastError", "bnxGetStats", "bnxSetStream", "bnxGetStream",
     "bnxSetLaunchConfig", "bnxFrameBufferDevicePointer", "bnxVolumeGetMacrocells",
-    "bnxRenderStructuredNoAlloc", "bnxSetScheduling", "bnxBoundsViolations", "bnxFrameBufferCheckpointSize",
+    "bnxRenderStructuredNoAlloc", "bnxSetScheduling", "bnxBoundsViolations", "bnxInjectAllocationFailure", "bnxFrameBufferCheckpointSize",
     "bnxFrameBufferCheckpoint", "bnxFrameBufferRestore", "bnxRenderBatch", "bnxSetBatchGraphs", "bnxAutotuneBatch",
     "bnxServerCreate", "bnxServerDestroy", "bnxServerSubmit", "bnxServerWait", "bnxServerGetStats",
     "bnxServerResetStats", "bnxServerReserve", "bnxSetRenderTimeout", "bnxSetPixelPartition",
@@ -171,6 +171,7 @@ def lib(build_if_missing=True):
         "bnxVolumeGetMacrocells": ([P, P, P, P], None),
         "bnxRenderStructuredNoAlloc": ([P, P], I),
         "bnxSetScheduling": ([P, I], None), "bnxBoundsViolations": ([P], ctypes.c_longlong),
+        "bnxInjectAllocationFailure": ([I], None),
         "bnxFrameBufferCheckpointSize": ([P], ctypes.c_size_t), "bnxFrameBufferCheckpoint": ([P, P], None),
         "bnxFrameBufferRestore": ([P, P, ctypes.c_size_t], None),
         "bnxRenderBatch": ([P, P, I], None),

@@ -846,13 +846,16 @@ BN_API void bnFrameBufferResize(BNFrameBuffer fbh, BNDataType fmt, int sx, int s
   if ((long long)sx * sy > kMaxFramePixels)  // the kernels index pixels and chunks with 32-bit ints
     throw Error(E_INVALID_ARG, "frame buffer larger than 2^31 - 1 pixels");
   if (!(channels & BN_FB_COLOR)) throw Error(E_UNSUPPORTED, "the colour channel is required");
+  // unusable until both buffers exist: a failed allocation leaves a frame
+  // buffer that every render and read rejects as not resized
+  fb->width = fb->height = 0;
+  fb->comp.release();
+  fb->accumID = 0;
+  fb->accum.resize((size_t)sx * sy * sizeof(float4));
+  fb->color.resize((size_t)sx * sy * (f == FMT_FLOAT4 ? 16 : 4));
   fb->width = sx;
   fb->height = sy;
   fb->colorFormat = f;
-  fb->accum.resize((size_t)sx * sy * sizeof(float4));
-  fb->color.resize((size_t)sx * sy * (f == FMT_FLOAT4 ? 16 : 4));
-  fb->comp.release();
-  fb->accumID = 0;
   BN_CATCH()
 }
 
@@ -874,6 +877,7 @@ BN_API void bnFrameBufferRead(BNFrameBuffer fbh, BNFrameBufferChannel ch, void *
   int f = fmt == BN_FLOAT4 ? FMT_FLOAT4 : fmt == BN_UFIXED8_RGBA ? FMT_RGBA8
         : fmt == BN_UFIXED8_RGBA_SRGB ? FMT_RGBA8_SRGB : -1;
   if (f != fb->colorFormat) throw Error(E_INVALID_ARG, "requested format differs from the frame buffer's format");
+  if (fb->width <= 0 || fb->height <= 0) throw Error(E_STATE, "frame buffer has not been resized");
   fb->ctx->activate();
   ck(cudaMemcpyAsync(ptr, fb->color.ptr, fb->color.bytes, cudaMemcpyDefault, fb->ctx->stream), "frame read");
   ck(cudaStreamSynchronize(fb->ctx->stream), "frame read");
@@ -1099,6 +1103,10 @@ BN_API int bnxRenderStructuredNoAlloc(const BNXNoAllocFrame *f, void *stream) {
   ck(launchRenderNoAlloc(v, fr, fmt, f->color, 0, (cudaStream_t)stream), "no-allocation render");
   return 0;
   BN_CATCH(g_lastError)
+}
+
+BN_API void bnxInjectAllocationFailure(int afterAllocations) {
+  allocFailCountdown().store(afterAllocations < 0 ? -1 : afterAllocations);
 }
 
 BN_API long long bnxBoundsViolations(BNContext context) {

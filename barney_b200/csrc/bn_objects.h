@@ -19,6 +19,7 @@
 #include <nvtx3/nvToolsExt.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstring>
 #include <memory>
@@ -41,6 +42,25 @@ enum : int { E_OK = 0, E_INVALID_HANDLE = 1, E_INVALID_ARG = 2, E_UNSUPPORTED = 
              E_OOM = 6, E_INTERNAL = 7, E_TIMEOUT = 8 };
 extern thread_local int g_lastError;
 extern thread_local std::string g_lastErrorString;
+
+// Host-side fault injection (bnxInjectAllocationFailure): after a countdown
+// of device allocations, one fails as if the device were out of memory.  The
+// failure is made on the host; no CUDA call fails and no device state changes.
+inline std::atomic<int> &allocFailCountdown() {
+  static std::atomic<int> c{-1};
+  return c;
+}
+// cudaMalloc, or the injected failure
+inline cudaError_t deviceMalloc(void **p, size_t n) {
+  int c = allocFailCountdown().load();
+  while (c >= 0) {
+    if (allocFailCountdown().compare_exchange_weak(c, c - 1)) {
+      if (c == 0) return cudaErrorMemoryAllocation;
+      break;
+    }
+  }
+  return cudaMalloc(p, n);
+}
 
 inline void ck(cudaError_t e, const char *what) {
   if (e != cudaSuccess) {
@@ -76,7 +96,7 @@ struct DeviceBuffer {
   void resize(size_t n) {
     if (n == bytes && ptr) return;
     release();
-    if (n) ck(cudaMalloc(&ptr, n), "cudaMalloc");
+    if (n) ck(deviceMalloc(&ptr, n), "cudaMalloc");
     bytes = n;
   }
 };
@@ -429,7 +449,7 @@ struct Context {
     ck(cudaSetDevice(dev), "cudaSetDevice");
     ck(cudaStreamCreateWithFlags(&ownStream, cudaStreamNonBlocking), "cudaStreamCreate");
     stream = ownStream;
-    ck(cudaMalloc(&dCounters, sizeof(LaunchCounters)), "cudaMalloc counters");
+    ck(deviceMalloc((void **)&dCounters, sizeof(LaunchCounters)), "cudaMalloc counters");
     ck(cudaMemset(dCounters, 0, sizeof(LaunchCounters)), "cudaMemset");
     for (auto &e : ev) ck(cudaEventCreate(&e), "cudaEventCreate");
   }

@@ -85,7 +85,7 @@ struct BufferPool {
     // a new chunk, not under the lock: cudaMalloc can take milliseconds
     const size_t size = std::max(kChunkBytes, need);
     void *base = nullptr;
-    ck(cudaMalloc(&base, size), "server buffer chunk");
+    ck(deviceMalloc(&base, size), "server buffer chunk");
     std::lock_guard<std::mutex> l(m);
     chunks.push_back({(unsigned char *)base, size, need});
     deviceBytesHeld += size;
@@ -104,7 +104,7 @@ struct BufferPool {
         if (deviceBytesHeld >= bytes) return;
       }
       void *base = nullptr;
-      ck(cudaMalloc(&base, kChunkBytes), "server buffer chunk");
+      ck(deviceMalloc(&base, kChunkBytes), "server buffer chunk");
       std::lock_guard<std::mutex> l(m);
       chunks.push_back({(unsigned char *)base, kChunkBytes, 0});
       deviceBytesHeld += kChunkBytes;

@@ -308,6 +308,11 @@ BN_API void bnxSetScheduling(BNContext context, int serviceBatch);
    Returns the count since the last call on this context's device (and resets
    it), -1 in the normal build, -2 on error. */
 BN_API long long bnxBoundsViolations(BNContext context);
+/* Host-side fault injection for tests: after afterAllocations more device
+   allocations (frame buffers, textures, macrocell grids, server buffers), the
+   next one fails once with error 6 (out of memory), made on the host; no CUDA
+   call fails.  A negative count disables it. */
+BN_API void bnxInjectAllocationFailure(int afterAllocations);
 
 /* Checkpoint / resume of a frame buffer's progressive state (the reference's
    only resumable state: the accumulation tiles and accumID, FrameBuffer.h:147).

@@ -90,3 +90,51 @@ def test_iteration_cap_ends_runaway_rays_and_sets_the_error_bit():
     ref, _, _ = oracle_render(ok, 2)
     assert_bitexact(img, ref, "after capped rays")
     assert st["error_flags"] == 0
+
+
+def test_injected_allocation_failures_leave_the_context_usable():
+    """Host-side fault injection: a device allocation that fails as if the
+    device were out of memory (error 6) leaves the object unusable but safe
+    (renders and reads of a frame buffer whose resize failed are rejected),
+    and the context keeps working."""
+    import barney_b200 as bn
+    from tests.helpers import assert_bitexact, oracle_render, small_noise_scene
+    d = small_noise_scene(w=24, h=16)
+    r = bn.VolumeRenderer(d)
+    L = r.L
+    try:
+        L.bnClearLastError()
+        L.bnxInjectAllocationFailure(0)  # the next allocation fails
+        L.bnFrameBufferResize(r.fb, bn.BN_FLOAT4, 25, 16, 1)
+        assert L.bnGetLastError() == 6
+        L.bnClearLastError()
+        L.bnRender(r.renderer, r.model, r.camera, r.fb)  # not resized: rejected, nothing launched
+        assert L.bnGetLastError() == 5
+        L.bnClearLastError()
+        L.bnxInjectAllocationFailure(1)  # the accumulation buffer succeeds, the colour buffer fails
+        L.bnFrameBufferResize(r.fb, bn.BN_FLOAT4, 26, 16, 1)
+        assert L.bnGetLastError() == 6
+        L.bnClearLastError()
+        out = np.zeros((16, 24, 4), np.float32)
+        L.bnFrameBufferRead(r.fb, 1, out.ctypes.data, bn.BN_FLOAT4)
+        assert L.bnGetLastError() == 5
+        L.bnClearLastError()
+        L.bnFrameBufferResize(r.fb, bn.BN_FLOAT4, 24, 16, 1)  # no injection left: works
+        assert L.bnGetLastError() == 0
+        r.set_spp(2)
+        r.render()
+        ref, _, _ = oracle_render(d, 2)
+        assert_bitexact(r.read(), ref, "after failed resizes")
+        # a texture that cannot be allocated: NULL and error 6
+        L.bnxInjectAllocationFailure(0)
+        vox = np.ascontiguousarray(d["voxels"])
+        nz, ny, nx = vox.shape
+        assert not L.bnTextureData3DCreate(r.ctx, 0, bn.BN_FLOAT32, nx, ny, nz, vox.ctypes.data)
+        assert L.bnGetLastError() == 6
+        L.bnClearLastError()
+        r.accum_reset()
+        r.render()
+        assert_bitexact(r.read(), ref, "after a failed texture")
+    finally:
+        L.bnxInjectAllocationFailure(-1)
+        r.close()
