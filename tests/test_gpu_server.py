@@ -143,3 +143,41 @@ def test_extended_requests_in_the_server_equal_the_oracle():
         for r in rs:
             r.close()
         ctx.close()
+
+
+def test_malformed_dropped_and_failed_requests_leave_the_server_serving():
+    """Serving-queue stress on the host side: malformed requests are refused at
+    submit, requests never waited for are dropped with the server, and a request
+    whose buffers cannot be allocated (injected failure) fails alone; every
+    other request still returns the oracle's frame."""
+    bn, ctx, scenes, rs, server = _setup(1 << 30, 8, 2)
+    L = ctx.L
+    try:
+        cam = synth.DEFAULT_CAMERA
+        for bad in ((0, 16, 1, "float4"), (16, 16, 0, "float4"), (70000, 70000, 1, "float4")):
+            with pytest.raises(bn.BarneyError):
+                server.submit(rs[0], cam, *bad)
+        L.bnClearLastError()
+        # the next device allocation (this request's buffers) fails as out of memory
+        L.bnxInjectAllocationFailure(0)
+        failing = server.submit(rs[1], cam, 40, 36, 2, "float4")
+        with pytest.raises(bn.BarneyError):
+            server.wait(failing, np.zeros((36, 40, 4), np.float32), timeout_ms=60000)
+        L.bnxInjectAllocationFailure(-1)
+        rng = np.random.default_rng(5)
+        reqs = []
+        for i in range(12):
+            k = i % len(scenes)
+            c = synth.orbit_camera(rng)
+            w, h, spp = scenes[k]["width"], scenes[k]["height"], 1 + i % 3
+            reqs.append((server.submit(rs[k], c, w, h, spp, "float4"), k, c, w, h, spp))
+        for rid, k, c, w, h, spp in reqs[::2]:  # every other request is never waited for
+            out = np.zeros((h, w, 4), np.float32)
+            assert server.wait(rid, out, timeout_ms=60000)
+            assert_bitexact(out, _expected(scenes[k], c, w, h, spp), f"request {rid}")
+    finally:
+        L.bnxInjectAllocationFailure(-1)
+        server.close()  # drops the requests nobody waited for
+        for r in rs:
+            r.close()
+        ctx.close()
