@@ -343,6 +343,9 @@ def run_ours(args):
             e1.record(stream)
             torch.cuda.synchronize()
             ms += e0.elapsed_time(e1)
+    torch.cuda.synchronize()
+    if world > 1:  # the timed region is bracketed by a barrier on both sides
+        dist.barrier()
     clocks = sampler.stop() if sampler else None
     samples = sum(s["samples"] for s in stats)
     rays = sum(s["rays"] for s in stats)
