@@ -382,7 +382,27 @@ void renderBatch(Context *ctx, const std::vector<BatchEntry> &entries) {
   key.push_back((const void *)(intptr_t)n);
   key.push_back((const void *)(intptr_t)extended);
   key.push_back((const void *)(intptr_t)voxelType);
+  // one job without a graph (a server slice with one request, say): the
+  // single-frame kernel, which takes the job as a kernel parameter and keeps
+  // the TF in shared memory, and a plain resolve -- the same frame as the
+  // batch kernel's, faster
+  const bool solo = n == 1 && !ctx->useGraphs;
   auto enqueue = [&](cudaStream_t s, bool timed) {
+    if (solo) {
+      const JobDD &job = ctx->hostJobs[0];
+      ck(cudaMemsetAsync(ctx->dCounters, 0, sizeof(LaunchCounters), s), "counter reset");
+      if (timed) ck(cudaEventRecord(ctx->ev[0], s), "event");
+      ck(launchRender(job.v, job.fr, ctx->dCounters, ctx->blocksPerSM, ctx->threadsPerBlock, s, ctx->sched),
+         "render kernel");
+      if (timed) ck(cudaEventRecord(ctx->ev[1], s), "event");
+      ck(launchResolve(job.fr.accum, job.fr.width * job.fr.height, job.fr.accumID0 + job.fr.spp, job.fr.colorFormat,
+                       job.fr.color, s, job.fr.comp),
+         "resolve kernel");
+      if (timed) ck(cudaEventRecord(ctx->ev[2], s), "event");
+      ck(cudaMemcpyAsync(ctx->hostCounters, ctx->dCounters, sizeof(LaunchCounters), cudaMemcpyDeviceToHost, s),
+         "counter read");
+      return;
+    }
     ck(cudaMemcpyAsync(ctx->batchJobs.ptr, ctx->hostJobs, n * sizeof(JobDD), cudaMemcpyHostToDevice, s), "job table");
     ck(cudaMemcpyAsync(ctx->batchChunks.ptr, ctx->hostChunks, (n + 1) * sizeof(int), cudaMemcpyHostToDevice, s),
        "chunk table");

@@ -322,3 +322,23 @@ def test_data_set_and_instance_transform_updates():
         L.bnClearLastError()
     finally:
         r.close()
+
+
+@pytest.mark.parametrize("graphs", [False, True])
+def test_one_job_batch_equals_bnrender(graphs):
+    # without a graph a one-job batch runs the single-frame kernel; with one,
+    # the batch kernel: the same frame either way
+    bn = _bn()
+    d = small_noise_scene(w=37, h=23, iso={"value": 0.5})
+    ctx = bn.Context()
+    r = bn.VolumeRenderer(d, context=ctx)
+    try:
+        ctx.set_graphs(graphs)
+        r.set_spp(2)
+        ctx.render_batch([r])
+        ctx.render_batch([r])  # accumulates: 4 waves
+        ref, _, _ = oracle_render(d, 4)
+        assert_bitexact(r.read(), ref, f"one-job batch, graphs={graphs}")
+    finally:
+        r.close()
+        ctx.close()
