@@ -6,9 +6,16 @@ imports this package; only ``tests/``, ``__graft_entry__.smoke()`` and the
 CPU-baseline / reference legs of ``bench.py`` use it, and only as the checker
 or the timed CPU baseline.
 
-Parity unpinned: the reference cannot be built here and ships no golden
-vectors for this path; the restatement is pinned by hand-derived known
-answers (tests/test_oracle_kat.py) and committed fixtures (tests/golden/).
+Pinned to the reference's own code: tests/test_ref_golden.py checks this
+restatement bit for bit against golden vectors that the reference's own
+sources produce (its RNG, hash, fastLog, DDA, trilinear texture sampler,
+transfer function, Woodcock tracking and principled-volume functions,
+compiled from where they lie by oracle/Makefile target `ref`;
+tests/golden/make_ref_golden.py).  The shading, light sampling and
+accumulation steps, which the reference cannot run outside its full
+renderer, are pinned by hand-derived known answers
+(tests/test_oracle_kat.py) and by frames rendered through the same compiled
+traversal.
 """
 import ctypes
 import os
@@ -102,6 +109,9 @@ def lib():
         L.orc_dda_cells.argtypes = [P, P, F, P, I, P, P]
         L.orc_dda_cells.restype = I
         L.orc_trace_primary.argtypes = [P, I, I, I, P, P, P]
+        L.orc_tex3d.argtypes = [P, I, P, P]
+        L.orc_trace_ray.argtypes = [P, P, P, F, U64, P, P, P, P]
+        L.orc_principled.argtypes = [P, I, P, P, P]
         L.orc_render.argtypes = [P, I, I, P, P, I, I, I, I, I, P]
         L.orc_render.restype = D
         L.orc_resolve.argtypes = [P, P, ctypes.c_int64, I, I, P]
@@ -335,6 +345,44 @@ def tf_map(sc, v):
     rgba = np.zeros((v.size, 4), np.float32)
     lib().orc_tf_map(sc.ref, v.size, _ptr(v), _ptr(rgba))
     return rgba
+
+
+def tex3d(sc, tc):
+    """LINEAR tex3D of the scene's field at unnormalized texel coordinates."""
+    tc = np.ascontiguousarray(tc, np.float32).reshape(-1, 3)
+    out = np.zeros(tc.shape[0], np.float32)
+    lib().orc_tex3d(sc.ref, tc.shape[0], _ptr(tc), _ptr(out))
+    return out
+
+
+def trace_ray(sc, org, dir, tmax, seed_state):
+    """One ray with an explicit RNG seed state through the volume: (hit, t,
+    rgb at the collision, [samples, macrocell visits])."""
+    org = np.ascontiguousarray(org, np.float32)
+    dir = np.ascontiguousarray(dir, np.float32)
+    hit, t = ctypes.c_int(0), ctypes.c_float(0.0)
+    rgb = np.zeros(3, np.float32)
+    counts = np.zeros(2, np.int32)
+    lib().orc_trace_ray(sc.ref, _ptr(org), _ptr(dir), tmax, seed_state, ctypes.byref(hit), ctypes.byref(t),
+                        _ptr(rgb), _ptr(counts))
+    return bool(hit.value), t.value, rgb, counts
+
+
+def trace_primary(sc, ix, iy, accum_id):
+    """The primary ray of pixel (ix, iy) at accum_id: (hit, t, rgb)."""
+    hit, t = ctypes.c_int(0), ctypes.c_float(0.0)
+    rgb = np.zeros(3, np.float32)
+    lib().orc_trace_primary(sc.ref, ix, iy, accum_id, ctypes.byref(hit), ctypes.byref(t), _ptr(rgb))
+    return bool(hit.value), t.value, rgb
+
+
+def principled(sc, v):
+    """The principled volume's sampleMap (tint rgb, sigma_t) and emission."""
+    v = np.ascontiguousarray(v, np.float32).reshape(-1)
+    m = np.zeros((v.size, 4), np.float32)
+    e = np.zeros((v.size, 3), np.float32)
+    lib().orc_principled(sc.ref, v.size, _ptr(v), _ptr(m), _ptr(e))
+    return m, e
 
 
 def dda_cells(org, dir, tmax, grid, max_cells=4096):

@@ -440,9 +440,8 @@ static inline vec4f sampleAndMap(const Scene &sc, vec3f P, float &scalar) {
 }
 
 // StructuredData.cu:31-62, cellsPerMC = 8, NEAREST fetch at integer coords
-static void buildRanges(const OrcScene &s, vec3i mcDims, float *out) {
-  const int64_t n = (int64_t)mcDims.x * mcDims.y * mcDims.z;
-  for (int64_t tid = 0; tid < n; tid++) {
+static void buildRangesSpan(const OrcScene &s, vec3i mcDims, float *out, int64_t begin, int64_t end) {
+  for (int64_t tid = begin; tid < end; tid++) {
     vec3i mc = {(int)(tid % mcDims.x), (int)((tid / mcDims.x) % mcDims.y), (int)(tid / ((int64_t)mcDims.x * mcDims.y))};
     float lo = INF, hi = -INF;  // owl interval<float> default = empty
     for (int iiz = 0; iiz <= 8; iiz++)
@@ -457,6 +456,16 @@ static void buildRanges(const OrcScene &s, vec3i mcDims, float *out) {
     out[2 * tid + 0] = lo;
     out[2 * tid + 1] = hi;
   }
+}
+// every macrocell is independent: large grids are split over the host's threads
+static void buildRanges(const OrcScene &s, vec3i mcDims, float *out) {
+  const int64_t n = (int64_t)mcDims.x * mcDims.y * mcDims.z;
+  const int64_t nt = n < 4096 ? 1 : std::max(1u, std::thread::hardware_concurrency());
+  if (nt == 1) return buildRangesSpan(s, mcDims, out, 0, n);
+  std::vector<std::thread> pool;
+  for (int64_t t = 0; t < nt; t++)
+    pool.emplace_back(buildRangesSpan, std::cref(s), mcDims, out, n * t / nt, n * (t + 1) / nt);
+  for (auto &th : pool) th.join();
 }
 
 static void setupScene(Scene &sc) {
@@ -1362,6 +1371,43 @@ void orc_trace_primary(const OrcScene *s, int ix, int iy, int accumID, int *hit,
   *hit = ray.hadHit;
   *t = ray.tMax;
   rgb[0] = ray.hitColor.x; rgb[1] = ray.hitColor.y; rgb[2] = ray.hitColor.z;
+}
+
+// LINEAR tex3D at unnormalized texel coordinates (Texture.cpp:339-411)
+void orc_tex3d(const OrcScene *s, int n, const float *tc, float *out) {
+  for (int i = 0; i < n; i++) out[i] = tex3DLinear(*s, tc[3 * i], tc[3 * i + 1], tc[3 * i + 2]);
+}
+
+// One ray with an explicit RNG seed state through the volume's isProg:
+// hit flag, t, rgb at the collision, and the samples / macrocell visits taken.
+void orc_trace_ray(const OrcScene *s, const float *org, const float *dir, float tMax, uint64_t seedState, int *hit,
+                   float *t, float *rgb, int *counts) {
+  Scene sc(*s);
+  setupScene(sc);
+  LocalStats st;
+  Ray ray;
+  ray.org = V(org[0], org[1], org[2]);
+  ray.dir = V(dir[0], dir[1], dir[2]);
+  ray.tMax = tMax;
+  ray.rngSeed.state = seedState;
+  traceRay(sc, ray, st);
+  *hit = ray.hadHit;
+  *t = ray.hadHit ? ray.tMax : 0.f;
+  rgb[0] = ray.hadHit ? ray.hitColor.x : 0.f;
+  rgb[1] = ray.hadHit ? ray.hitColor.y : 0.f;
+  rgb[2] = ray.hadHit ? ray.hitColor.z : 0.f;
+  counts[0] = (int)st.samples;
+  counts[1] = (int)st.mcVisits;
+}
+
+// The principled volume's sampleMap (tint rgb, sigma_t) and emission at scalars
+void orc_principled(const OrcScene *s, int n, const float *v, float *outMap, float *outEmission) {
+  for (int i = 0; i < n; i++) {
+    const vec4f m = principledSampleMap(*s, v[i]);
+    const vec3f e = principledEmission(*s, v[i]);
+    outMap[4 * i] = m.x; outMap[4 * i + 1] = m.y; outMap[4 * i + 2] = m.z; outMap[4 * i + 3] = m.w;
+    outEmission[3 * i] = e.x; outEmission[3 * i + 1] = e.y; outEmission[3 * i + 2] = e.z;
+  }
 }
 
 // Render waves accumID0 .. accumID0+spp-1 over the pixel rectangle
