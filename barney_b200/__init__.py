@@ -272,8 +272,8 @@ class Context:
 
 
 class VolumeRenderer:
-    """One structured volume rendered through the bn* API (the call sequence
-    of SURVEY section 3.2/3.3: texture data -> structured field -> volume +
+    """One structured volume rendered through the bn* API, in the call order
+    of Barney's own clients (texture data -> structured field -> volume +
     transfer function -> group -> model -> build; camera, renderer, frame
     buffer -> bnRender -> bnFrameBufferRead).
 

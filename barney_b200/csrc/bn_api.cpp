@@ -5,6 +5,7 @@
 #include "bn_objects.h"
 
 #include <chrono>
+#include <climits>
 #include <thread>
 
 namespace bnb {
@@ -950,12 +951,19 @@ BN_API void bnxFrameBufferRestore(BNFrameBuffer fbh, const void *in, size_t byte
     throw Error(E_INVALID_ARG, "checkpoint size differs from the frame buffer's");
   const size_t px = (size_t)fb->width * fb->height * sizeof(float4);
   if (bytes != sizeof h + px + (h.hasComp ? px : 0)) throw Error(E_INVALID_ARG, "checkpoint length is wrong");
+  // the render loop and the resolve count waves in an int
+  if (h.accumID > (uint32_t)INT_MAX) throw Error(E_INVALID_ARG, "checkpoint accumID is out of range");
   Context *ctx = fb->ctx;
   ctx->activate();
+  // allocate before anything is copied, so that a failed allocation leaves
+  // the frame buffer as it was
+  if (h.hasComp && !fb->comp.ptr) fb->comp.resize(px);
+  // from here on a failed copy leaves an empty frame buffer (accumID 0: the
+  // next render writes its first wave instead of adding to the buffer)
+  fb->accumID = 0;
   const char *src = (const char *)in + sizeof h;
   ck(cudaMemcpyAsync(fb->accum.ptr, src, px, cudaMemcpyHostToDevice, ctx->stream), "restore");
   if (h.hasComp) {
-    if (!fb->comp.ptr) fb->comp.resize(px);
     ck(cudaMemcpyAsync(fb->comp.ptr, src + px, px, cudaMemcpyHostToDevice, ctx->stream), "restore");
   } else if (fb->comp.ptr) {
     ck(cudaMemsetAsync(fb->comp.ptr, 0, px, ctx->stream), "restore");

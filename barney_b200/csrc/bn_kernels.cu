@@ -331,7 +331,13 @@ __global__ void __launch_bounds__(128) mcBuildKernel(VolumeDD v, float2 *ranges,
     const int z1 = min(z0 + kCellsPerMC, v.numScalars.z - 1);
     float lo = kInf, hi = -kInf;
     const int64_t nx = v.numScalars.x, nxy = (int64_t)v.numScalars.x * v.numScalars.y;
-    if (!BNB_IN(x1 + nx * y1 + nxy * z1, nxy * v.numScalars.z)) continue;
+    if (!BNB_IN(x1 + nx * y1 + nxy * z1, nxy * v.numScalars.z)) {
+      // (bounds-checked build) a counted violation: an empty range and a
+      // zero majorant, so the macrocell reads as empty
+      ranges[tid] = make_float2(kInf, -kInf);
+      if (majorants) majorants[tid] = 0.f;
+      continue;
+    }
     for (int z = z0; z <= z1; z++)
       for (int y = y0; y <= y1; y++) {
         const int64_t row = nx * y + nxy * z;
@@ -1848,7 +1854,12 @@ __global__ void __launch_bounds__(128) mcMajorantScratchKernel(VolumeDD v, int r
     const int z1 = min(z0 + kCellsPerMC, v.numScalars.z - 1);
     float lo = kInf, hi = -kInf;
     const int64_t nx = v.numScalars.x, nxy = (int64_t)v.numScalars.x * v.numScalars.y;
-    if (!BNB_IN(x1 + nx * y1 + nxy * z1, nxy * v.numScalars.z)) continue;
+    if (!BNB_IN(x1 + nx * y1 + nxy * z1, nxy * v.numScalars.z)) {
+      // (bounds-checked build) a counted violation: a zero majorant, not the
+      // previous call's value left in the shared scratch
+      majorants[tid] = 0.f;
+      continue;
+    }
     for (int z = z0; z <= z1; z++)
       for (int y = y0; y <= y1; y++) {
         const int64_t row = nx * y + nxy * z;
@@ -1862,18 +1873,24 @@ __global__ void __launch_bounds__(128) mcMajorantScratchKernel(VolumeDD v, int r
   }
 }
 
-// Device address of g_noAllocScratch on the current device, looked up once
-// per device with cudaGetSymbolAddress (the host-side name of the array is
-// only a stand-in, never a device address).
-static void *noAllocScratchAddress(cudaError_t *err) {
+// Device address of g_noAllocScratch on the current device (the host-side
+// name of the array is only a stand-in, never a device address).  Looked up
+// with cudaGetSymbolAddress on every call made while stream s is not
+// capturing, so that a device reset, after which the module and its array
+// are loaded anew, is picked up; a call on a capturing stream uses the
+// address its device's last such call found.
+static void *noAllocScratchAddress(cudaStream_t s, cudaError_t *err) {
   static std::mutex m;
   static void *addr[64] = {nullptr};
   int dev = 0;
   *err = cudaGetDevice(&dev);
   if (*err != cudaSuccess) return nullptr;
   if (dev < 0 || dev >= 64) { *err = cudaErrorInvalidDevice; return nullptr; }
+  cudaStreamCaptureStatus capture = cudaStreamCaptureStatusNone;
+  *err = cudaStreamIsCapturing(s, &capture);
+  if (*err != cudaSuccess) return nullptr;
   std::lock_guard<std::mutex> l(m);
-  if (!addr[dev]) {
+  if (capture == cudaStreamCaptureStatusNone || !addr[dev]) {
     void *p = nullptr;
     *err = cudaGetSymbolAddress(&p, g_noAllocScratch);
     if (*err != cudaSuccess) return nullptr;
@@ -1886,7 +1903,7 @@ cudaError_t launchRenderNoAlloc(VolumeDD v, FrameDD fr, int fmt, void *color, in
   const int64_t n = (int64_t)v.mcDims.x * v.mcDims.y * v.mcDims.z;
   if (n <= 0 || n > kNoAllocMaxMacrocells) return cudaErrorInvalidValue;
   cudaError_t e = cudaSuccess;
-  unsigned char *base = (unsigned char *)noAllocScratchAddress(&e);
+  unsigned char *base = (unsigned char *)noAllocScratchAddress(s, &e);
   if (!base) return e;
   LaunchCounters *ctr = (LaunchCounters *)base;
   float *majorants = (float *)(base + kNoAllocCountersBytes);

@@ -369,9 +369,13 @@ BN_API void bnxVolumeGetMacrocells(BNVolume volume, int *dims3, float *rangesHos
    library until exit).
    Larger volumes are rejected with error 2 and a message.  All calls share
    that array, so calls whose work overlaps on the GPU (other streams, other
-   host threads) race; serialise them.  The first call on each device looks
-   up the array's device address (cudaGetSymbolAddress); make that first call
-   outside any stream capture.  Returns 0 or the error code also recorded for
+   host threads) race; serialise them.  Every call made while its stream is
+   not capturing looks up the array's device address (cudaGetSymbolAddress,
+   which allocates nothing); a call on a capturing stream reuses the address
+   found by its device's last such call.  So make the first call on each
+   device outside any stream capture, and again the first call after a
+   cudaDeviceReset: a reset unloads the array, and the address remembered
+   from before it is stale.  Returns 0 or the error code also recorded for
    bnGetLastError. */
 #define BNX_NOALLOC_MAX_MACROCELLS (64 * 64 * 64)
 typedef struct {

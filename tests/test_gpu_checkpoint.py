@@ -56,3 +56,54 @@ def test_restore_rejects_a_checkpoint_of_another_size():
     finally:
         a.close()
         b.close()
+
+
+def test_restore_rejects_an_accum_id_beyond_int_max():
+    import struct
+    import barney_b200 as bn
+    a = bn.VolumeRenderer(small_noise_scene(w=16, h=16))
+    try:
+        bad = struct.pack("<8I", 0x43584E42, 1, 16, 16, 2 ** 31, 0, 0, 0) + bytes(16 * 16 * 16)
+        with pytest.raises(bn.BarneyError):
+            a.restore(bad)
+        ok = struct.pack("<8I", 0x43584E42, 1, 16, 16, 2 ** 31 - 1, 0, 0, 0) + bytes(16 * 16 * 16)
+        a.restore(ok)
+    finally:
+        a.close()
+
+
+def test_failed_restore_allocation_leaves_the_frame_buffer_as_it_was():
+    """A compensated checkpoint restored into an uncompensated frame buffer
+    needs a compensation buffer; when that allocation fails, nothing of the
+    checkpoint is applied and the frame continues as if there had been no
+    restore."""
+    import barney_b200 as bn
+    L = bn.lib()
+    dc = small_noise_scene(w=24, h=16, compensated_accum=True)
+    a = bn.VolumeRenderer(dc)
+    try:
+        a.set_spp(2)
+        a.render()
+        ck = a.checkpoint()
+    finally:
+        a.close()
+    d = small_noise_scene(w=24, h=16)
+    b = bn.VolumeRenderer(d)
+    try:
+        b.set_spp(3)
+        b.render()
+        L.bnxInjectAllocationFailure(0)
+        try:
+            with pytest.raises(bn.BarneyError):
+                b.restore(ck)
+        finally:
+            L.bnxInjectAllocationFailure(-1)
+            L.bnClearLastError()
+        b.render()
+        resumed = b.read().copy()
+    finally:
+        b.close()
+    sc = oracle.Scene(d)
+    acc = np.zeros((16, 24, 4), np.float32)
+    oracle.render(sc, 0, 6, accum=acc)
+    assert_bitexact(resumed, oracle.resolve(acc, 6), "3 + 3 waves around a failed restore")

@@ -5,7 +5,10 @@ must not stall on cudaMalloc's implicit synchronisation).
 
 Through the C ABI it must give the same frames as the regular bnRender path
 (bit-exact, the bar every parity test here uses), on two calls in a row that
-reuse its static scratch, and reject volumes beyond its fixed scratch size.
+reuse its static scratch, for every voxel type and colour format; allocate
+nothing (an allocation made to fail succeeds it no harm, and the device's
+free memory does not move); accept exactly the largest grid its scratch
+holds (513^3 scalars, 64^3 macrocells) and reject the next larger one.
 This file is named so pytest collects it last.
 """
 import ctypes
@@ -37,14 +40,19 @@ class BNXNoAllocFrame(ctypes.Structure):
 class NoAllocCall:
     """Device buffers owned by the caller (this test), one frame description."""
 
-    def __init__(self, d):
+    def __init__(self, d, color_format="float4"):
         import torch
         import barney_b200 as bn
         self.bn = bn
-        self.vox = torch.from_numpy(np.ascontiguousarray(d["voxels"])).cuda()
+        v = d["voxels"]
+        self.vox = v if isinstance(v, torch.Tensor) else torch.from_numpy(np.ascontiguousarray(v)).cuda()
         self.tf = torch.from_numpy(np.ascontiguousarray(d["tf"], np.float32)).cuda()
         self.accum = torch.zeros((d["height"], d["width"], 4), dtype=torch.float32, device="cuda")
-        self.color = torch.zeros((d["height"], d["width"], 4), dtype=torch.float32, device="cuda")
+        if color_format == "float4":
+            self.color = torch.zeros((d["height"], d["width"], 4), dtype=torch.float32, device="cuda")
+        else:  # 8-bit RGBA packed in 32 bits
+            self.color = torch.zeros((d["height"], d["width"]), dtype=torch.int32, device="cuda")
+        self.color_format = color_format
         lights = d.get("dir_lights", [])
         self.lights = np.array([[*l["direction"], l.get("radiance", 1.0), *l.get("color", (1, 1, 1))]
                                 for l in lights], np.float32).reshape(-1, 7)
@@ -72,7 +80,7 @@ class NoAllocCall:
         f.anisotropy = d.get("anisotropy", 0.6)
         f.scatteringAlbedo = d.get("scattering_albedo", 0.9)
         f.width, f.height = d["width"], d["height"]
-        f.colorFormat = bn.BN_FLOAT4
+        f.colorFormat = bn.COLOR_FORMATS[color_format]
         f.accum = self.accum.data_ptr()
         f.color = self.color.data_ptr()
         self.f = f
@@ -85,12 +93,13 @@ class NoAllocCall:
         rc = L.bnxRenderStructuredNoAlloc(ctypes.byref(self.f), ctypes.c_void_p(torch.cuda.current_stream().cuda_stream))
         torch.cuda.synchronize()
         assert rc == 0, L.bnGetLastErrorString()
-        return self.color.cpu().numpy()
+        out = self.color.cpu().numpy()
+        return out if self.color_format == "float4" else out.view(np.uint32)
 
 
-def regular_path(d, spp, renders):
+def regular_path(d, spp, renders, color_format="float4"):
     import barney_b200 as bn
-    r = bn.VolumeRenderer(d, color_format="float4")
+    r = bn.VolumeRenderer(d, color_format=color_format)
     try:
         r.set_spp(spp)
         out = []
@@ -124,5 +133,65 @@ def test_no_alloc_rejects_volume_beyond_scratch():
     L.bnClearLastError()
     rc = L.bnxRenderStructuredNoAlloc(ctypes.byref(call.f), None)
     assert rc == 2
+    assert b"macrocells" in L.bnGetLastErrorString()
+    L.bnClearLastError()
+
+
+@pytest.mark.parametrize("dtype,color_format", [("u8", "rgba8"), ("f16", "float4"), ("f32", "rgba8_srgb")])
+def test_no_alloc_voxel_types_and_colour_formats(dtype, color_format):
+    d = small_noise_scene(n=33, w=40, h=24, dtype=dtype)
+    expect = regular_path(d, 2, renders=2, color_format=color_format)
+    call = NoAllocCall(d, color_format)
+    assert_bitexact(call.render(0, 2), expect[0], f"{dtype} {color_format}: first call")
+    assert_bitexact(call.render(2, 2), expect[1], f"{dtype} {color_format}: second call")
+
+
+def test_no_alloc_allocates_nothing():
+    """The library's own device allocations go through one wrapper; armed to
+    fail the next one, a no-allocation call still succeeds (and leaves the
+    failure armed for the next allocation).  The device's free memory is the
+    same before and after a call."""
+    import torch
+    import barney_b200 as bn
+    L = bn.lib()
+    d = small_noise_scene(n=40, w=48, h=32)
+    expect = regular_path(d, 3, renders=1)
+    call = NoAllocCall(d)
+    call.render(0, 3)  # warm-up: loads the kernels and looks the scratch up
+    free0, _ = torch.cuda.mem_get_info()
+    L.bnxInjectAllocationFailure(0)
+    try:
+        frame = call.render(0, 3)
+        free1, _ = torch.cuda.mem_get_info()
+        # the armed failure is still pending: the next library allocation fails
+        with pytest.raises(bn.BarneyError):
+            bn.VolumeRenderer(d)
+    finally:
+        L.bnxInjectAllocationFailure(-1)
+        L.bnClearLastError()
+    assert_bitexact(frame, expect[0], "frame with an allocation made to fail")
+    assert free1 == free0, (free0, free1)
+
+
+def test_no_alloc_accepts_its_largest_grid_and_rejects_the_next():
+    """513^3 scalars are exactly 64^3 macrocells: accepted, and equal to
+    bnRender; one more scalar along x needs 65 x 64 x 64: rejected."""
+    import torch
+    import barney_b200 as bn
+    g = torch.Generator(device="cuda")
+    g.manual_seed(1)
+    vol = torch.randint(0, 256, (513, 513, 513), dtype=torch.uint8, device="cuda", generator=g)
+    d = synth.scene(vol, "u8", 24, 16, synth.tf_knots(256, 1), 20.0, synth.DEFAULT_CAMERA)
+    expect = regular_path(d, 1, renders=1)
+    call = NoAllocCall(d)
+    assert_bitexact(call.render(0, 1), expect[0], "513^3 grid")
+    del call
+    big = synth.scene(torch.zeros((513, 513, 514), dtype=torch.uint8, device="cuda"), "u8", 8, 8,
+                      synth.tf_knots(256, 1), 20.0, synth.DEFAULT_CAMERA)
+    call = NoAllocCall(big)
+    call.f.accumID, call.f.pathsPerPixel = 0, 1
+    L = bn.lib()
+    L.bnClearLastError()
+    assert L.bnxRenderStructuredNoAlloc(ctypes.byref(call.f), None) == 2
     assert b"macrocells" in L.bnGetLastErrorString()
     L.bnClearLastError()
