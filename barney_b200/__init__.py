@@ -50,7 +50,7 @@ EXPORTS = [
     "bnBuild", "bnCameraCreate", "bnRendererCreate", "bnFrameBufferCreate", "bnFrameBufferResize",
     "bnFrameBufferRead", "bnFrameBufferGetSize", "bnAccumReset", "bnRender", "bnGetLastError",
     "bnGetLastErrorString", "bnClearLastError", "bnxGetStats", "bnxSetStream", "bnxGetStream",
-    "bnxSetLaunchConfig", "bnxFrameBufferDevicePointer", "bnxVolumeGetMacrocells",
+    "bnxSetLaunchConfig", "bnxFrameBufferDevicePointer", "bnxVolumeGetMacrocells", "bnxVolumeSample",
     "bnxRenderStructuredNoAlloc", "bnxSetScheduling", "bnxBoundsViolations", "bnxInjectAllocationFailure", "bnxFrameBufferCheckpointSize",
     "bnxFrameBufferCheckpoint", "bnxFrameBufferRestore", "bnxRenderBatch", "bnxSetBatchGraphs", "bnxAutotuneBatch",
     "bnxServerCreate", "bnxServerDestroy", "bnxServerSubmit", "bnxServerWait", "bnxServerGetStats",
@@ -168,7 +168,7 @@ def lib(build_if_missing=True):
         "bnGetLastErrorString": ([], S), "bnClearLastError": ([], None),
         "bnxGetStats": ([P, P], None), "bnxSetStream": ([P, P], None), "bnxGetStream": ([P], P),
         "bnxSetLaunchConfig": ([P, I, I], None), "bnxFrameBufferDevicePointer": ([P], P),
-        "bnxVolumeGetMacrocells": ([P, P, P, P], None),
+        "bnxVolumeGetMacrocells": ([P, P, P, P], None), "bnxVolumeSample": ([P, P, I, P, P, I], None),
         "bnxRenderStructuredNoAlloc": ([P, P], I),
         "bnxSetScheduling": ([P, I], None), "bnxBoundsViolations": ([P], ctypes.c_longlong),
         "bnxInjectAllocationFailure": ([I], None),
@@ -427,6 +427,7 @@ class VolumeRenderer:
         L.bnSet1i(self.renderer, b"bnx.emissionAbsorption", int(desc.get("emission_absorption", False)))
         L.bnSet1i(self.renderer, b"bnx.exactLog", int(desc.get("exact_log", False)))
         L.bnSet1i(self.renderer, b"bnx.compensatedAccum", int(desc.get("compensated_accum", False)))
+        L.bnSet1i(self.renderer, b"bnx.fastMath", int(desc.get("fast_math", False)))
         L.bnCommit(self.renderer)
         check()
 
@@ -494,6 +495,17 @@ class VolumeRenderer:
         self.L.bnxVolumeGetMacrocells(self.vol, None, ranges.ctypes.data, maj.ctypes.data)
         check()
         return ranges, maj
+
+    def sample(self, points, fast_math=False):
+        """The field (NaN outside) and sampleAndMap's rgba at world points,
+        evaluated on the device by the render kernels' code (bnxVolumeSample)."""
+        P = np.ascontiguousarray(points, np.float32).reshape(-1, 3)
+        scal = np.zeros(P.shape[0], np.float32)
+        rgba = np.zeros((P.shape[0], 4), np.float32)
+        self.L.bnxVolumeSample(self.vol, P.ctypes.data, P.shape[0], scal.ctypes.data, rgba.ctypes.data,
+                               1 if fast_math else 0)
+        check()
+        return scal, rgba
 
     def set_scheduling(self, service_batch=22):
         self.L.bnxSetScheduling(self.ctx, service_batch)

@@ -5,7 +5,9 @@
 
 Device code: --fmad=false with IEEE division and square root, so the kernels
 evaluate every FP32 expression exactly as written (bit-identical to the CPU
-restatement in oracle/).  Host code: -ffp-contract=off for the same reason
+restatement in oracle/); bn_kernels.cu is compiled a second time with
+-DBNB_FAST_MATH, FMA contraction and approximate division and square root into
+the fast-math object (the renderer parameter bnx.fastMath).  Host code: -ffp-contract=off for the same reason
 (camera set-up).
 """
 import os
@@ -17,6 +19,10 @@ CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libbarney_b200.so")
 LIB_BC = os.path.join(HERE, "libbarney_b200_bc.so")  # bounds-checked build (-DBNB_BOUNDS_CHECK)
 SOURCES = ["bn_kernels.cu", "bn_api.cpp", "bn_server.cpp"]
+# the fast-math object (renderer parameter bnx.fastMath): bn_kernels.cu again,
+# with FMA contraction and approximate division and square root
+FAST_SOURCE = "bn_kernels.cu"
+FAST_FLAGS = ["-DBNB_FAST_MATH", "--fmad=true", "-prec-div=false", "-prec-sqrt=false"]
 HEADERS = ["bn_device.h", "bn_objects.h", os.path.join("..", "..", "include", "bn_volume.h")]
 
 NVCC_FLAGS = [
@@ -38,7 +44,7 @@ def nvcc():
 def _digest(bounds_check=False):
     """Content hash of every input of the build (sources, headers, flags)."""
     import hashlib
-    h = hashlib.sha1((" ".join(NVCC_FLAGS) + (" -DBNB_BOUNDS_CHECK" if bounds_check else "")).encode())
+    h = hashlib.sha1((" ".join(NVCC_FLAGS + FAST_FLAGS) + (" -DBNB_BOUNDS_CHECK" if bounds_check else "")).encode())
     for s in SOURCES + HEADERS:
         with open(os.path.join(CSRC, s), "rb") as f:
             h.update(f.read())
@@ -77,13 +83,20 @@ def _build_locked(verbose, bounds_check=False):
     flags = NVCC_FLAGS + (["-DBNB_BOUNDS_CHECK"] if bounds_check else [])
     objs = []
     logs = []
-    for src in SOURCES:
-        obj = os.path.join(CSRC, os.path.splitext(src)[0] + ("_bc.o" if bounds_check else ".o"))
-        cmd = [nvcc(), *flags, "-c", os.path.join(CSRC, src), "-o", obj]
-        r = subprocess.run(cmd, capture_output=True, text=True)
-        logs.append(r.stdout + r.stderr)
-        if r.returncode != 0:
-            sys.stderr.write(r.stdout + r.stderr)
+    units = [(src, os.path.splitext(src)[0], flags) for src in SOURCES]
+    exact = {"--fmad=false", "-prec-div=true", "-prec-sqrt=true"}
+    units.append((FAST_SOURCE, "bn_kernels_fast", [f for f in flags if f not in exact] + FAST_FLAGS))
+    # the objects compile in parallel (the two kernel objects dominate)
+    procs = []
+    for src, stem, fl in units:
+        obj = os.path.join(CSRC, stem + ("_bc.o" if bounds_check else ".o"))
+        cmd = [nvcc(), *fl, "-c", os.path.join(CSRC, src), "-o", obj]
+        procs.append((src, obj, subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True)))
+    for src, obj, p in procs:
+        out, _ = p.communicate()
+        logs.append(f"== {os.path.basename(obj)}\n" + out)
+        if p.returncode != 0:
+            sys.stderr.write(out)
             raise RuntimeError("nvcc failed on " + src)
         objs.append(obj)
     tmp = LIB_OUT + ".tmp"

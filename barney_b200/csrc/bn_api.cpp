@@ -225,6 +225,7 @@ JobDD buildJob(Context *ctx, Renderer &r, Model &m, Camera &cam, FrameBuffer &fb
   }
   fr.emissionAbsorption = p.emissionAbsorption;
   fr.exactLog = p.exactLog;
+  fr.fastMath = p.fastMath;
   // maxVolumeBounces acts in the multi-scatter build only (bnx.hgPhase); the
   // default build treats a volume scatter as the end of the path
   // (shadeRays.cu:23-25,774-796), so there it has no effect, as in Barney
@@ -295,6 +296,18 @@ static bool waitWithDeadline(Context *ctx, cudaEvent_t done, std::chrono::steady
   return true;
 }
 
+// A job that needs none of the extended kernels' features (isosurface,
+// multi-scatter, principled volume) runs the fast-math kernels when its
+// renderer asks for them (bnx.fastMath); every other job the exact ones.
+static bool plainJob(const JobDD &job) {
+  return !job.v.iso.enabled && job.fr.maxVolumeBounces <= 0 && !job.v.pv.enabled;
+}
+static cudaError_t launchRenderJob(Context *ctx, const JobDD &job, cudaStream_t s) {
+  if (job.fr.fastMath && plainJob(job))
+    return fastmath::launchRender(job.v, job.fr, ctx->dCounters, ctx->blocksPerSM, ctx->threadsPerBlock, s, ctx->sched);
+  return launchRender(job.v, job.fr, ctx->dCounters, ctx->blocksPerSM, ctx->threadsPerBlock, s, ctx->sched);
+}
+
 static void render(Context *ctx, Renderer &r, Model &m, Camera &cam, FrameBuffer &fb) {
   NvtxRange range("bnRender");
   const auto start = std::chrono::steady_clock::now();
@@ -302,8 +315,7 @@ static void render(Context *ctx, Renderer &r, Model &m, Camera &cam, FrameBuffer
   if (job.fr.spp <= 0) return;
   ck(cudaMemsetAsync(ctx->dCounters, 0, sizeof(LaunchCounters), ctx->stream), "counter reset");
   ck(cudaEventRecord(ctx->ev[0], ctx->stream), "event");
-  ck(launchRender(job.v, job.fr, ctx->dCounters, ctx->blocksPerSM, ctx->threadsPerBlock, ctx->stream, ctx->sched),
-     "render kernel");
+  ck(launchRenderJob(ctx, job, ctx->stream), "render kernel");
   ck(cudaEventRecord(ctx->ev[1], ctx->stream), "event");
   fb.accumID += job.fr.spp;
   ck(launchResolve((const float4 *)fb.accum.ptr, fb.width * fb.height, (int)fb.accumID, fb.colorFormat, fb.color.ptr,
@@ -360,6 +372,7 @@ void renderBatch(Context *ctx, const std::vector<BatchEntry> &entries) {
   unsigned long long pixelSamples = 0;
   int extended = 0;  // 1: multi-scatter, principled or exact log; 2: isosurfaces (the extended kernels)
   int voxelType = -2;     // the type every job shares, else -1
+  bool fast = true;       // every job asks for the fast-math kernels
   ctx->hostChunks[0] = 0;
   for (int i = 0; i < n; i++) {
     const BatchEntry &e = entries[i];
@@ -368,6 +381,7 @@ void renderBatch(Context *ctx, const std::vector<BatchEntry> &entries) {
     extended = std::max(extended, job.v.iso.enabled ? 2
                                   : (job.fr.maxVolumeBounces > 0 || job.v.pv.enabled || job.fr.exactLog) ? 1 : 0);
     voxelType = voxelType == -2 || voxelType == job.v.type ? job.v.type : -1;
+    fast = fast && job.fr.fastMath;
     ctx->hostJobs[i] = job;
     chunks += ((long long)job.fr.width * job.fr.height + 31) / 32;
     if (chunks > 0x7fffffffLL) throw Error(E_INVALID_ARG, "batch too large");
@@ -383,6 +397,8 @@ void renderBatch(Context *ctx, const std::vector<BatchEntry> &entries) {
   key.push_back((const void *)(intptr_t)n);
   key.push_back((const void *)(intptr_t)extended);
   key.push_back((const void *)(intptr_t)voxelType);
+  fast = fast && extended == 0;  // the fast-math object holds the plain kernels only
+  key.push_back((const void *)(intptr_t)(fast ? 1 : 0));
   // one job without a graph (a server slice with one request, say): the
   // single-frame kernel, which takes the job as a kernel parameter and keeps
   // the TF in shared memory, and a plain resolve -- the same frame as the
@@ -393,8 +409,7 @@ void renderBatch(Context *ctx, const std::vector<BatchEntry> &entries) {
       const JobDD &job = ctx->hostJobs[0];
       ck(cudaMemsetAsync(ctx->dCounters, 0, sizeof(LaunchCounters), s), "counter reset");
       if (timed) ck(cudaEventRecord(ctx->ev[0], s), "event");
-      ck(launchRender(job.v, job.fr, ctx->dCounters, ctx->blocksPerSM, ctx->threadsPerBlock, s, ctx->sched),
-         "render kernel");
+      ck(launchRenderJob(ctx, job, s), "render kernel");
       if (timed) ck(cudaEventRecord(ctx->ev[1], s), "event");
       ck(launchResolve(job.fr.accum, job.fr.width * job.fr.height, job.fr.accumID0 + job.fr.spp, job.fr.colorFormat,
                        job.fr.color, s, job.fr.comp),
@@ -409,8 +424,10 @@ void renderBatch(Context *ctx, const std::vector<BatchEntry> &entries) {
        "chunk table");
     ck(cudaMemsetAsync(ctx->dCounters, 0, sizeof(LaunchCounters), s), "counter reset");
     if (timed) ck(cudaEventRecord(ctx->ev[0], s), "event");
-    ck(launchRenderBatch((const JobDD *)ctx->batchJobs.ptr, (const int *)ctx->batchChunks.ptr, n, ctx->dCounters,
-                         ctx->blocksPerSM, ctx->threadsPerBlock, s, ctx->sched, extended, voxelType),
+    ck((fast ? fastmath::launchRenderBatch : launchRenderBatch)((const JobDD *)ctx->batchJobs.ptr,
+                                                                (const int *)ctx->batchChunks.ptr, n, ctx->dCounters,
+                                                                ctx->blocksPerSM, ctx->threadsPerBlock, s, ctx->sched,
+                                                                extended, voxelType),
        "batch render kernel");
     if (timed) ck(cudaEventRecord(ctx->ev[1], s), "event");
     ck(launchResolveBatch((const JobDD *)ctx->batchJobs.ptr, (const int *)ctx->batchChunks.ptr, n, (int)chunks, s),
@@ -1038,6 +1055,35 @@ BN_API void bnxVolumeGetMacrocells(BNVolume vh, int *dims3, float *rangesOut, fl
   if (rangesOut) ck(cudaMemcpyAsync(rangesOut, v->ranges.ptr, v->ranges.bytes, cudaMemcpyDefault, v->ctx->stream), "copy");
   if (majOut) ck(cudaMemcpyAsync(majOut, v->majorants.ptr, v->majorants.bytes, cudaMemcpyDefault, v->ctx->stream), "copy");
   ck(cudaStreamSynchronize(v->ctx->stream), "copy");
+  BN_CATCH()
+}
+
+BN_API void bnxVolumeSample(BNVolume vh, const float *points, int n, float *scalarsOut, float *rgbaOut,
+                            int fastMath) {
+  BN_TRY
+  auto v = getAs<Volume>(vh, Object::K_VOLUME, "BNVolume");
+  if (n < 0 || (n > 0 && (!points || !scalarsOut || !rgbaOut)))
+    throw Error(E_INVALID_ARG, "bnxVolumeSample needs n >= 0 and, for n > 0, points and both outputs");
+  if (!v->built) throw Error(E_STATE, "volume has not been built");
+  if (n == 0) return;
+  v->ctx->activate();
+  v->build();  // no-op unless the TF changed
+  const VolumeDD dd = v->dd();
+  const size_t un = (size_t)n;
+  DeviceBuffer dP, dS, dR;
+  dP.resize(un * sizeof(float3));
+  dS.resize(un * sizeof(float));
+  dR.resize(un * sizeof(float4));
+  cudaStream_t s = v->ctx->stream;
+  ck(cudaMemcpyAsync(dP.ptr, points, un * sizeof(float3), cudaMemcpyDefault, s), "sample points");
+  // principled volumes render with the exact kernels only, so they sample with them here too
+  const bool fast = fastMath && !dd.pv.enabled;
+  ck((fast ? fastmath::launchSampleProbe : launchSampleProbe)(dd, (const float3 *)dP.ptr, n, (float *)dS.ptr,
+                                                              (float4 *)dR.ptr, s),
+     "sample kernel");
+  ck(cudaMemcpyAsync(scalarsOut, dS.ptr, un * sizeof(float), cudaMemcpyDefault, s), "sample read");
+  ck(cudaMemcpyAsync(rgbaOut, dR.ptr, un * sizeof(float4), cudaMemcpyDefault, s), "sample read");
+  ck(cudaStreamSynchronize(s), "sample");
   BN_CATCH()
 }
 

@@ -88,6 +88,7 @@ struct FrameDD {
   DirLightDD dirLights[kMaxDirLights];
   int emissionAbsorption;
   int exactLog;
+  int fastMath;          // the job asks for the fast-math kernels (host-side choice; kernels ignore it)
   int maxVolumeBounces;  // > 0: multi-scatter build (HG phase), scattered rays up to this many volume bounces
   int partRank, partCount;  // pixel-tile partition: render the tiles t with t % partCount == partRank
   float4 *accum;        // width*height, linear
@@ -153,5 +154,26 @@ bool boundsCheckedBuild();
 // bn_kernels.cu).
 constexpr int64_t kNoAllocMaxMacrocells = 64 * 64 * 64;
 cudaError_t launchRenderNoAlloc(VolumeDD v, FrameDD fr, int fmt, void *color, int roundUp, cudaStream_t s);
+
+// Field samples and TF lookups (sampleAndMap) at n device points P into
+// device arrays scalar (NaN outside the field) and rgba.
+cudaError_t launchSampleProbe(const VolumeDD &vol, const float3 *P, int n, float *scalar, float4 *rgba, cudaStream_t s);
+
+// The fast-math form (renderer parameter bnx.fastMath): the plain kernels
+// (no isosurface, multi-scatter or principled volume) compiled with FMA
+// contraction and approximate division and square root, except where a
+// sample's texel coordinate and TF coordinate are formed (explicitly
+// rounded there).  Same launch semantics as the exact launchers; a job that
+// needs an extended kernel returns cudaErrorInvalidValue.
+namespace fastmath {
+cudaError_t launchRender(const VolumeDD &vol, const FrameDD &frame, LaunchCounters *counters, int blocksPerSM,
+                         int threadsPerBlock, cudaStream_t s, const SchedDD &sd = SchedDD());
+cudaError_t launchRenderBatch(const JobDD *jobs, const int *chunkStart, int numJobs, LaunchCounters *counters,
+                              int blocksPerSM, int threadsPerBlock, cudaStream_t s, const SchedDD &sd = SchedDD(),
+                              int extended = 0, int voxelType = -1);
+cudaError_t launchSampleProbe(const VolumeDD &vol, const float3 *P, int n, float *scalar, float4 *rgba, cudaStream_t s);
+long long readBoundsViolationsHere();  // bounds-checked build only
+}  // namespace fastmath
+long long readBoundsViolationsHere();  // bounds-checked build only
 
 }  // namespace bnb

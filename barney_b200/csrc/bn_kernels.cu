@@ -30,6 +30,13 @@
 #include <mutex>
 
 namespace bnb {
+// The fast-math object (-DBNB_FAST_MATH, compiled with FMA contraction and
+// approximate division and square root) holds the plain render kernels and
+// their launchers in bnb::fastmath; macrocell builds, resolves and the
+// no-allocation path exist only in the exact object.
+#ifdef BNB_FAST_MATH
+namespace fastmath {
+#endif
 
 #define DEV __device__ __forceinline__
 
@@ -161,9 +168,9 @@ DEV float loadVoxel(const void *p, int64_t i, const float *u8lut) {
     // evaluated unfused, equals the correctly rounded quotient for every
     // 16-bit x (checked exhaustively in tests/test_oracle_kat.py)
     const float x = (float)__ldg((const unsigned short *)p + i);
-    const float r = 1.f / 65535.f;
-    const float q = x * r;
-    return q + (x - q * 65535.f) * r;
+    const float r = __fdiv_rn(1.f, 65535.f);
+    const float q = __fmul_rn(x, r);
+    return __fadd_rn(q, __fmul_rn(__fsub_rn(x, __fmul_rn(q, 65535.f)), r));
   }
   return __uint_as_float((uint32_t)__ldg((const unsigned short *)p + i) << 16);
 }
@@ -178,14 +185,21 @@ DEV void lerpCoords(int &i0, int &d, float &f, int N, float tc) {
   i0 = iu;
   d = 1;
 }
-DEV float lerp_l(float f, float a, float b) { return (1.f - f) * a + f * b; }
+// (1 - f) a + f b with each operation rounded (never fused): the trilinear
+// and TF interpolations keep the reference's evaluation in the fast-math
+// build too, so samples and TF lookups stay within the bar set for them
+DEV float lerp_l(float f, float a, float b) { return __fadd_rn(__fmul_rn(1.f - f, a), __fmul_rn(f, b)); }
 
 // StructuredDataSampler::DD::sample + CPU LINEAR tex3D; returns NaN outside
+// The cell-space position is rounded explicitly (__fmul_rn is never fused
+// into the following +.5): in the fast-math build a fused form would move the
+// texel coordinate, and so the interpolation weights, by far more than the
+// 2 ulp allowed for a sample.  In the exact build it is the same product.
 template <int T>
 DEV float sampleField(const VolumeDD &v, float3 P, const float *u8lut) {
-  float rx = (P.x - v.gridOrigin.x) * v.rcpSpacing.x;
-  float ry = (P.y - v.gridOrigin.y) * v.rcpSpacing.y;
-  float rz = (P.z - v.gridOrigin.z) * v.rcpSpacing.z;
+  float rx = __fmul_rn(P.x - v.gridOrigin.x, v.rcpSpacing.x);
+  float ry = __fmul_rn(P.y - v.gridOrigin.y, v.rcpSpacing.y);
+  float rz = __fmul_rn(P.z - v.gridOrigin.z, v.rcpSpacing.z);
   if (rx < 0.f || ry < 0.f || rz < 0.f) return __int_as_float(0x7fc00000);
   if (rx >= (float)v.numCells.x || ry >= (float)v.numCells.y || rz >= (float)v.numCells.z)
     return __int_as_float(0x7fc00000);
@@ -315,10 +329,11 @@ DEV float roundUpMajorant(float m, int roundUp) {
   return (roundUp && m > 0.f) ? __int_as_float(__float_as_int(m) + 1) : m;
 }
 
+#ifndef BNB_FAST_MATH
 template <int T>
 __global__ void __launch_bounds__(128) mcBuildKernel(VolumeDD v, float2 *ranges, float *majorants, int roundUp) {
   __shared__ float u8lut[256];
-  for (int i = threadIdx.x; i < 256; i += blockDim.x) u8lut[i] = (float)i * 1.f / 255.f;
+  for (int i = threadIdx.x; i < 256; i += blockDim.x) u8lut[i] = __fdiv_rn((float)i * 1.f, 255.f);
   __syncthreads();
   const int64_t n = (int64_t)v.mcDims.x * v.mcDims.y * v.mcDims.z;
   for (int64_t tid = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; tid < n; tid += (int64_t)gridDim.x * blockDim.x) {
@@ -359,6 +374,7 @@ __global__ void mcMapKernel(VolumeDD v, const float2 *ranges, float *majorants, 
     majorants[i] = roundUpMajorant(mapMajorant(v, r.x, r.y), roundUp);
   }
 }
+#endif  // !BNB_FAST_MATH
 
 // ---------------------------------------------------------------------------
 // render megakernel
@@ -617,6 +633,20 @@ DEV void neumaier(float &sum, float &c, float x) {
 DEV void accAdd(float &sum, float &c, float x, bool comp) {
   if (comp) neumaier(sum, c, x);
   else sum += x;
+}
+
+// TransferFunction::DD::map's table coordinate of a non-NaN scalar
+// (TransferFunction.h:74-83): entry idx and fraction f.  The division and the
+// scaling are rounded explicitly, as in sampleField: in the fast-math build an
+// approximate quotient or a fused scale would move f by up to 2^-16 over a
+// 256-entry table.  x/1 == x exactly, so a unit domain skips the division.
+DEV void tfLocate(const VolumeDD &v, float s, int &idx, float &f) {
+  const float span = v.domHi - v.domLo;
+  f = span == 1.f ? (s - v.domLo) : __fdiv_rn(s - v.domLo, span);
+  f = fmin_(1.f, fmax_(0.f, f));
+  f = __fmul_rn(f, (float)(v.tfN - 1));
+  idx = min(v.tfN - 2, max(0, (int)f));
+  f -= (float)idx;
 }
 
 // Field sample of a job: compile-time voxel type, or (T < 0) the job's type.
@@ -1491,16 +1521,11 @@ DEV void renderLoop(const JobDD *__restrict__ jobs, const int *__restrict__ chun
             float w = 0.f, f = 0.f, tfw = 0.f;
             int idx = 0;
             if (!isnan(s)) {
-              const float span = v.domHi - v.domLo;
-              f = span == 1.f ? (s - v.domLo) : (s - v.domLo) / span;  // x/1 == x exactly
-              f = fmin_(1.f, fmax_(0.f, f));
-              f *= (float)(v.tfN - 1);
-              idx = min(v.tfN - 2, max(0, (int)f));
-              f -= (float)idx;
+              tfLocate(v, s, idx, f);
               if (!BNB_IN(idx, v.tfN - 1)) idx = 0;
               const float w0 = BATCH ? __ldg(&v.tf[idx].w) : sTF[idx].w;
               const float w1 = BATCH ? __ldg(&v.tf[idx + 1].w) : sTF[idx + 1].w;
-              w = ((1.f - f) * w0 + f * w1) * v.baseDensity;
+              w = __fmul_rn(lerp_l(f, w0, w1), v.baseDensity);
               if (EXT) {  // principled volume (Volume.h:66-72): density sigma_t times the TF's
                 tfw = w;
                 if (v.pv.enabled) w = tfw <= 0.f ? 0.f : principledSigmaT(v.pv, s) * tfw;
@@ -1513,7 +1538,7 @@ DEV void renderLoop(const JobDD *__restrict__ jobs, const int *__restrict__ chun
               if (!(ISO && shadowRay) && !isnan(s) && !((EXT && v.pv.enabled) && tfw <= 0.f)) {
                 const float4 a = BATCH ? __ldg(&v.tf[idx]) : sTF[idx];
                 const float4 b = BATCH ? __ldg(&v.tf[idx + 1]) : sTF[idx + 1];
-                hitRGB = f3((1.f - f) * a.x + f * b.x, (1.f - f) * a.y + f * b.y, (1.f - f) * a.z + f * b.z);
+                hitRGB = f3(lerp_l(f, a.x, b.x), lerp_l(f, a.y, b.y), lerp_l(f, a.z, b.z));
                 if ((EXT && v.pv.enabled)) hitRGB = principledTintTimes(v.pv, s, hitRGB);
               }
               phase = LP_HIT;
@@ -1565,7 +1590,7 @@ __global__ void __launch_bounds__(kRenderMaxThreads, EXT >= 2 ? kRenderMinBlocks
   extern __shared__ float4 sTF[];
   __shared__ float u8lut[256];
   for (int i = threadIdx.x; i < job.v.tfN; i += blockDim.x) sTF[i] = job.v.tf[i];
-  for (int i = threadIdx.x; i < 256; i += blockDim.x) u8lut[i] = (float)i * 1.f / 255.f;
+  for (int i = threadIdx.x; i < 256; i += blockDim.x) u8lut[i] = __fdiv_rn((float)i * 1.f, 255.f);
   __syncthreads();
   int numChunks = (job.fr.width * job.fr.height + kChunk - 1) / kChunk;
   if (job.fr.partCount > 1) numChunks = partitionChunks(numChunks, job.fr.partRank, job.fr.partCount);
@@ -1578,7 +1603,7 @@ __global__ void __launch_bounds__(kRenderMaxThreads, EXT >= 2 ? kRenderMinBlocks
     renderBatchKernel(const JobDD *__restrict__ jobs, const int *__restrict__ chunkStart, int numJobs, const __grid_constant__ SchedDD sd,
                       LaunchCounters *ctr) {
   __shared__ float u8lut[256];
-  for (int i = threadIdx.x; i < 256; i += blockDim.x) u8lut[i] = (float)i * 1.f / 255.f;
+  for (int i = threadIdx.x; i < 256; i += blockDim.x) u8lut[i] = __fdiv_rn((float)i * 1.f, 255.f);
   __syncthreads();
   // plain batch kernels draw free-flight distances with fastLog only; batches
   // with an exact-log job run the extended kernel, which chooses per job
@@ -1586,6 +1611,41 @@ __global__ void __launch_bounds__(kRenderMaxThreads, EXT >= 2 ? kRenderMinBlocks
                                         u8lut);
 }
 
+// Field samples and transfer-function lookups at given points
+// (bnxVolumeSample): the structured sampler (NaN outside) and sampleAndMap
+// (Volume.h:62-74), with the expressions of the render loop's Woodcock step.
+template <int T>
+__global__ void sampleProbeKernel(VolumeDD v, const float3 *P, int n, float *scalar, float4 *rgba) {
+  __shared__ float u8lut[256];
+  for (int i = threadIdx.x; i < 256; i += blockDim.x) u8lut[i] = __fdiv_rn((float)i * 1.f, 255.f);
+  __syncthreads();
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const float s = sampleField<T>(v, P[i], u8lut);
+    float4 m = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (!isnan(s)) {
+      int idx;
+      float f;
+      tfLocate(v, s, idx, f);
+      const float4 a = v.tf[idx], b = v.tf[idx + 1];
+      float3 rgb = f3(lerp_l(f, a.x, b.x), lerp_l(f, a.y, b.y), lerp_l(f, a.z, b.z));
+      float w = __fmul_rn(lerp_l(f, a.w, b.w), v.baseDensity);
+      if (v.pv.enabled) {  // principled: TF density 0 maps to 0, else sigma_t and tint times the TF's
+        if (w <= 0.f) {
+          rgb = f3(0.f, 0.f, 0.f);
+          w = 0.f;
+        } else {
+          rgb = principledTintTimes(v.pv, s, rgb);
+          w = principledSigmaT(v.pv, s) * w;
+        }
+      }
+      m = make_float4(rgb.x, rgb.y, rgb.z, w);
+    }
+    scalar[i] = s;
+    rgba[i] = m;
+  }
+}
+
+#ifndef BNB_FAST_MATH
 // ---------------------------------------------------------------------------
 // resolve (TiledFB.cu:13-52, math.h:61-125)
 // ---------------------------------------------------------------------------
@@ -1647,6 +1707,8 @@ __global__ void resolveBatchKernel(const JobDD *jobs, const int *chunkStart, int
   }
 }
 
+#endif  // !BNB_FAST_MATH
+
 // ---------------------------------------------------------------------------
 // launchers
 // ---------------------------------------------------------------------------
@@ -1663,6 +1725,7 @@ static int smCount() {
   return n;
 }
 
+#ifndef BNB_FAST_MATH
 // Occupancy bitmap of a majorant grid: one ballot per warp packs the
 // "majorant != 0" flags of 32 consecutive macrocells into one word.  The
 // render loop tests these bits (32 KB for a 64^3 grid, resident in L1)
@@ -1710,15 +1773,21 @@ cudaError_t launchMapMajorants(const VolumeDD &v, const float2 *ranges, float *m
   cudaError_t e = cudaGetLastError();
   return e != cudaSuccess ? e : launchOccupancy(majorants, n, occupied, s);
 }
+#endif  // !BNB_FAST_MATH
 
 template <int T>
 static cudaError_t launchRenderT(const VolumeDD &v, const FrameDD &fr, const SchedDD &sd, LaunchCounters *ctr,
                                  int bps, int tpb, cudaStream_t s) {
   const size_t smem = (size_t)v.tfN * sizeof(float4);
   const int ext = v.iso.enabled ? 2 : (fr.maxVolumeBounces > 0 || v.pv.enabled) ? 1 : 0;
+#ifdef BNB_FAST_MATH
+  if (ext) return cudaErrorInvalidValue;  // the fast-math object holds the plain kernels only
+  auto kern = fr.exactLog ? renderKernel<T, 1, 0> : renderKernel<T, 0, 0>;
+#else
   auto kern = ext == 2   ? (fr.exactLog ? renderKernel<T, 1, 2> : renderKernel<T, 0, 2>)
               : ext == 1 ? (fr.exactLog ? renderKernel<T, 1, 1> : renderKernel<T, 0, 1>)
                          : (fr.exactLog ? renderKernel<T, 1, 0> : renderKernel<T, 0, 0>);
+#endif
   if (smem > 48 * 1024 &&
       cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
     return cudaGetLastError();
@@ -1761,9 +1830,14 @@ static auto batchKernelFor(int voxelType) {
 cudaError_t launchRenderBatch(const JobDD *jobs, const int *chunkStart, int numJobs, LaunchCounters *ctr, int bps,
                               int tpb, cudaStream_t s, const SchedDD &sd, int extended, int voxelType) {
   if (tpb <= 0) tpb = 128;
+#ifdef BNB_FAST_MATH
+  if (extended) return cudaErrorInvalidValue;  // the fast-math object holds the plain kernels only
+  auto kern = batchKernelFor<0>(voxelType);
+#else
   auto kern = extended >= 2 ? batchKernelFor<2>(voxelType)
               : extended    ? batchKernelFor<1>(voxelType)
                             : batchKernelFor<0>(voxelType);
+#endif
   if (bps <= 0) {
     int occ = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, tpb, 0) != cudaSuccess)
@@ -1774,6 +1848,30 @@ cudaError_t launchRenderBatch(const JobDD *jobs, const int *chunkStart, int numJ
   return cudaGetLastError();
 }
 
+cudaError_t launchSampleProbe(const VolumeDD &v, const float3 *P, int n, float *scalar, float4 *rgba, cudaStream_t s) {
+  if (n <= 0) return cudaSuccess;
+  const int blocks = std::max(1, std::min((n + 255) / 256, smCount() * 8));
+  switch (v.type) {
+  case VOX_F32: sampleProbeKernel<VOX_F32><<<blocks, 256, 0, s>>>(v, P, n, scalar, rgba); break;
+  case VOX_U8: sampleProbeKernel<VOX_U8><<<blocks, 256, 0, s>>>(v, P, n, scalar, rgba); break;
+  case VOX_F16: sampleProbeKernel<VOX_F16><<<blocks, 256, 0, s>>>(v, P, n, scalar, rgba); break;
+  case VOX_U16: sampleProbeKernel<VOX_U16><<<blocks, 256, 0, s>>>(v, P, n, scalar, rgba); break;
+  default: sampleProbeKernel<VOX_BF16><<<blocks, 256, 0, s>>>(v, P, n, scalar, rgba); break;
+  }
+  return cudaGetLastError();
+}
+
+#ifdef BNB_BOUNDS_CHECK
+// out-of-range accesses counted by this object's kernels since the last call
+long long readBoundsViolationsHere() {
+  unsigned long long n = 0, zero = 0;
+  if (cudaMemcpyFromSymbol(&n, g_boundsViolations, sizeof n) != cudaSuccess) return -2;
+  if (cudaMemcpyToSymbol(g_boundsViolations, &zero, sizeof zero) != cudaSuccess) return -2;
+  return (long long)n;
+}
+#endif
+
+#ifndef BNB_FAST_MATH
 cudaError_t launchResolveBatch(const JobDD *jobs, const int *chunkStart, int numJobs, int numChunks, cudaStream_t s) {
   const int blocks = std::max(1, std::min((numChunks + 7) / 8, smCount() * 8));
   resolveBatchKernel<<<blocks, 256, 0, s>>>(jobs, chunkStart, numJobs, numChunks);
@@ -1800,10 +1898,8 @@ bool boundsCheckedBuild() {
 // the count); -1 in the normal build.
 long long readBoundsViolations() {
 #ifdef BNB_BOUNDS_CHECK
-  unsigned long long n = 0, zero = 0;
-  if (cudaMemcpyFromSymbol(&n, g_boundsViolations, sizeof n) != cudaSuccess) return -2;
-  if (cudaMemcpyToSymbol(g_boundsViolations, &zero, sizeof zero) != cudaSuccess) return -2;
-  return (long long)n;
+  const long long a = readBoundsViolationsHere(), b = fastmath::readBoundsViolationsHere();
+  return (a < 0 || b < 0) ? -2 : a + b;
 #else
   return -1;
 #endif
@@ -1840,7 +1936,7 @@ static __device__ __align__(256) unsigned char
 template <int T>
 __global__ void __launch_bounds__(128) mcMajorantScratchKernel(VolumeDD v, int roundUp) {
   __shared__ float u8lut[256];
-  for (int i = threadIdx.x; i < 256; i += blockDim.x) u8lut[i] = (float)i * 1.f / 255.f;
+  for (int i = threadIdx.x; i < 256; i += blockDim.x) u8lut[i] = __fdiv_rn((float)i * 1.f, 255.f);
   __syncthreads();
   float *majorants = (float *)(g_noAllocScratch + kNoAllocCountersBytes);
   const int64_t n = (int64_t)v.mcDims.x * v.mcDims.y * v.mcDims.z;
@@ -1928,5 +2024,9 @@ cudaError_t launchRenderNoAlloc(VolumeDD v, FrameDD fr, int fmt, void *color, in
   if (e != cudaSuccess) return e;
   return launchResolve(fr.accum, fr.width * fr.height, fr.accumID0 + fr.spp, fmt, color, s);
 }
+#endif  // !BNB_FAST_MATH
 
+#ifdef BNB_FAST_MATH
+}  // namespace fastmath
+#endif
 }  // namespace bnb

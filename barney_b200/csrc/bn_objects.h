@@ -385,6 +385,7 @@ struct Renderer : Object {
     int emissionAbsorption = 0;   // bnx
     int exactLog = 0;             // bnx
     int compensatedAccum = 0;     // bnx: Neumaier-compensated accumulation (precision forms)
+    int fastMath = 0;             // bnx: the fast-math kernels (FMA contraction, approximate division)
   } staged, p;
   explicit Renderer(Context *c) : Object(c, K_RENDERER) {}
   bool set1i(const std::string &m, int v) override {
@@ -395,6 +396,7 @@ struct Renderer : Object {
     if (m == "bnx.emissionAbsorption") { staged.emissionAbsorption = v ? 1 : 0; return true; }
     if (m == "bnx.exactLog") { staged.exactLog = v ? 1 : 0; return true; }
     if (m == "bnx.compensatedAccum") { staged.compensatedAccum = v ? 1 : 0; return true; }
+    if (m == "bnx.fastMath") { staged.fastMath = v ? 1 : 0; return true; }
     return false;
   }
   bool set1f(const std::string &m, float v) override {

@@ -395,6 +395,50 @@ def run_ours(args):
     h2d = 3 * 3 * 4 + 4 + 8  # position, direction, up, fovy, accumID/spp words
     d2h = d["width"] * d["height"] * 4
 
+    # the fast-math form (bnx.fastMath: FMA contraction, approximate division;
+    # within 2 ulp per sample and 3 standard errors per pixel of the exact
+    # path) on the same workload, timed the same way
+    fast = None
+    plain_kernels = not d.get("max_volume_bounces") and not d.get("iso")
+    if plain_kernels and not tile_dp:
+        r.L.bnSet1i(r.renderer, b"bnx.fastMath", 1)
+        r.L.bnCommit(r.renderer)
+        bn.check()
+        for _ in range(args.warmup):
+            frame()
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        fstats, fms = [], 0.0
+        if flush is None:
+            e0.record(stream)
+            for _ in range(args.steps):
+                fstats.append(frame())
+            e1.record(stream)
+            torch.cuda.synchronize()
+            fms = e0.elapsed_time(e1)
+        else:
+            for _ in range(args.steps):
+                flush.add_(1)
+                e0.record(stream)
+                fstats.append(frame())
+                e1.record(stream)
+                torch.cuda.synchronize()
+                fms += e0.elapsed_time(e1)
+        if world > 1:
+            dist.barrier()
+        fms_max, fsamples_all, _ = reduce_over_ranks(fms, sum(s["samples"] for s in fstats), 0, device="cuda")
+        falg = [8 * es * s["samples"] + 4 * s["mc_visits"] + 16 * s["pixel_samples"] for s in fstats]
+        fkms = [s["render_ms"] for s in fstats]
+        fach = statistics.mean(a / (k * 1e-3) for a, k in zip(falg, fkms)) / 1e9
+        fast = {"value": fsamples_all / (fms_max / 1e3) / 1e6, "unit": "Msamples/s",
+                "ms_per_step": fms_max / args.steps, "frames_per_s": world * args.steps / (fms_max / 1e3),
+                "kernel_ms": statistics.mean(fkms), "roofline_frac": fach / peak,
+                "form": "bnx.fastMath: FMA contraction, approximate division and square root outside the "
+                        "texel and TF coordinates"}
+        r.L.bnSet1i(r.renderer, b"bnx.fastMath", 0)
+        r.L.bnCommit(r.renderer)
+
     cpu = None
     if world == 1 and not args.no_cpu_baseline:
         dh = dict(d)
@@ -428,6 +472,9 @@ def run_ours(args):
                     "frames_per_s": (1 if tile_dp else world) * e2e_steps / (e2e_ms_max / 1e3)},
             "cpu_baseline": cpu,
         }
+        if fast is not None:
+            line["fast_math"] = fast
+            line["gpu_launches"] += 2 * args.steps
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.barrier()
@@ -676,7 +723,10 @@ def run_rmse(args):
     forms = [("plain f32 (fastLog)", "f32", {}), ("f32 exact -log", "f32", {"exact_log": True}),
              ("f16 storage", "f16", {"majorant_round_up": True, "compensated_accum": True}),
              ("bf16 storage", "bf16", {"majorant_round_up": True, "compensated_accum": True}),
-             ("u8 storage", "u8", {"majorant_round_up": True, "compensated_accum": True})]
+             ("u8 storage", "u8", {"majorant_round_up": True, "compensated_accum": True}),
+             ("f32 fast math", "f32", {"fast_math": True}),
+             ("f16 storage, fast math", "f16", {"majorant_round_up": True, "compensated_accum": True,
+                                               "fast_math": True})]
     out = []
     for name, dtype, kw in forms:
         d = dict(base, voxels=synth.to_storage(f32, dtype), dtype=dtype, **kw)

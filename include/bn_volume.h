@@ -354,6 +354,18 @@ BN_API void *bnxFrameBufferDevicePointer(BNFrameBuffer fb);
    ranges (2 floats per cell) and majorants (1 float per cell), x fastest. */
 BN_API void bnxVolumeGetMacrocells(BNVolume volume, int *dims3, float *rangesHostOut,
                                    float *majorantsHostOut);
+/* The volume's field and transfer function evaluated on the device at n
+   world-space points (3 floats each, host or device memory): scalarsOut[i]
+   is the trilinear field value (NaN outside the field, as
+   StructuredDataSampler::DD::sample, StructuredData.h:101-112, returns) and
+   rgbaOut[4i..4i+3] the mapped colour and density of Volume::DD::sampleAndMap
+   (Volume.h:62-74), computed by the same device code as the render kernels'
+   Woodcock step -- the fast-math kernels' with fastMath != 0 (principled
+   volumes, which render with the exact kernels only, sample with those
+   too).  A diagnostic
+   with no reference counterpart; allocates temporary device memory. */
+BN_API void bnxVolumeSample(BNVolume volume, const float *points, int n, float *scalarsOut, float *rgbaOut,
+                            int fastMath);
 
 /* No-allocation render (no reference counterpart).  For callers that cannot
    allocate device memory while rendering -- an application that reserves

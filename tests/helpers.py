@@ -54,3 +54,27 @@ def assert_bitexact(a, b, what=""):
     bad = np.argwhere(av != bv)
     assert bad.size == 0, f"{what}: {len(bad)} mismatches, first at {bad[:5].tolist()}: " \
                           f"{a[tuple(bad[0])] if bad.size else ''} vs {b[tuple(bad[0])] if bad.size else ''}"
+
+
+def empty_checkpoint(width, height, accum_id):
+    """A checkpoint of an empty frame buffer at accum_id (bnxFrameBufferRestore
+    header: magic, version, width, height, accumID, hasComp, 2 reserved words),
+    so that a render continues with the wave accum_id onto an empty buffer."""
+    import struct
+    return struct.pack("<8I", 0x43584E42, 1, width, height, accum_id, 0, 0, 0) + bytes(width * height * 16)
+
+
+def render_batches(r, width, height, batches, per_batch):
+    """Per-batch mean frames (batches, H, W, 4) of a VolumeRenderer: batch b
+    renders waves b*per_batch .. (b+1)*per_batch-1 onto an empty buffer."""
+    out = []
+    r.set_spp(per_batch)
+    for b in range(batches):
+        r.accum_reset()
+        if b:
+            r.restore(empty_checkpoint(width, height, b * per_batch))
+        r.render()
+        ck = r.checkpoint()
+        acc = np.frombuffer(ck[32:32 + width * height * 16], np.float32).reshape(height, width, 4)
+        out.append(acc.astype(np.float64) / per_batch)
+    return np.stack(out)

@@ -16,13 +16,11 @@ reference's sources compiled here).
 
 All comparisons are bit-exact.
 """
-import os
-import struct
-
 import numpy as np
 import pytest
 
 from test_ref_golden import FIELD_NAMES, TRACE_NAMES, assert_same, field_scene, load, trace_scene
+from tests.helpers import empty_checkpoint
 
 pytestmark = pytest.mark.gpu
 
@@ -41,10 +39,21 @@ def test_macrocells(name):
     assert_same(maj, z[name + "__majorants"], f"{name}: majorants")
 
 
-def empty_checkpoint(width, height, accum_id):
-    """A checkpoint of an empty frame buffer at accum_id (header: magic,
-    version, width, height, accumID, hasComp, 2 reserved words)."""
-    return struct.pack("<8I", 0x43584E42, 1, width, height, accum_id, 0, 0, 0) + bytes(width * height * 16)
+@pytest.mark.parametrize("name", FIELD_NAMES)
+def test_field_samples(name):
+    """The render kernels' sampler and sampleAndMap on the device
+    (bnxVolumeSample) at the fixture's world points: the reference's CPU
+    LINEAR tex3D behind StructuredDataSampler, and its TF map (principled
+    sampleAndMap for the principled scene)."""
+    import barney_b200 as bn
+    z = load("ref_field.npz")
+    r = bn.VolumeRenderer(field_scene(z, name))
+    try:
+        scal, rgba = r.sample(z[name + "__P"])
+    finally:
+        r.close()
+    assert_same(scal, z[name + "__sample"], f"{name}: structured sampler")
+    assert_same(rgba, z[name + "__sample_rgba"], f"{name}: sampleAndMap")
 
 
 def expected_wave(hit, rgb, accum_id, bg=(0.0, 0.0, 0.0, 1.0)):
