@@ -50,7 +50,7 @@ EXPORTS = [
     "bnBuild", "bnCameraCreate", "bnRendererCreate", "bnFrameBufferCreate", "bnFrameBufferResize",
     "bnFrameBufferRead", "bnFrameBufferGetSize", "bnAccumReset", "bnRender", "bnGetLastError",
     "bnGetLastErrorString", "bnClearLastError", "bnxGetStats", "bnxSetStream", "bnxGetStream",
-    "bnxSetLaunchConfig", "bnxFrameBufferDevicePointer", "bnxVolumeGetMacrocells", "bnxVolumeSample",
+    "bnxSetLaunchConfig", "bnxFrameBufferDevicePointer", "bnxVolumeGetMacrocells", "bnxVolumeSample", "bnxSetRegrouping",
     "bnxRenderStructuredNoAlloc", "bnxSetScheduling", "bnxBoundsViolations", "bnxInjectAllocationFailure", "bnxFrameBufferCheckpointSize",
     "bnxFrameBufferCheckpoint", "bnxFrameBufferRestore", "bnxRenderBatch", "bnxSetBatchGraphs", "bnxAutotuneBatch",
     "bnxServerCreate", "bnxServerDestroy", "bnxServerSubmit", "bnxServerWait", "bnxServerGetStats",
@@ -170,7 +170,7 @@ def lib(build_if_missing=True):
         "bnxSetLaunchConfig": ([P, I, I], None), "bnxFrameBufferDevicePointer": ([P], P),
         "bnxVolumeGetMacrocells": ([P, P, P, P], None), "bnxVolumeSample": ([P, P, I, P, P, I], None),
         "bnxRenderStructuredNoAlloc": ([P, P], I),
-        "bnxSetScheduling": ([P, I], None), "bnxBoundsViolations": ([P], ctypes.c_longlong),
+        "bnxSetScheduling": ([P, I], None), "bnxSetRegrouping": ([P, I], None), "bnxBoundsViolations": ([P], ctypes.c_longlong),
         "bnxInjectAllocationFailure": ([I], None),
         "bnxFrameBufferCheckpointSize": ([P], ctypes.c_size_t), "bnxFrameBufferCheckpoint": ([P, P], None),
         "bnxFrameBufferRestore": ([P, P, ctypes.c_size_t], None),
@@ -506,6 +506,11 @@ class VolumeRenderer:
                                1 if fast_math else 0)
         check()
         return scal, rgba
+
+    def set_regrouping(self, enable=True):
+        """Regrouped kernel for plain jobs, or the per-lane kernel (default)."""
+        self.L.bnxSetRegrouping(self.ctx, 1 if enable else 0)
+        check()
 
     def set_scheduling(self, service_batch=22):
         self.L.bnxSetScheduling(self.ctx, service_batch)

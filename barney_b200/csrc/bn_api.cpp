@@ -302,8 +302,14 @@ static bool waitWithDeadline(Context *ctx, cudaEvent_t done, std::chrono::steady
 static bool plainJob(const JobDD &job) {
   return !job.v.iso.enabled && job.fr.maxVolumeBounces <= 0 && !job.v.pv.enabled;
 }
+// Plain jobs run the regrouped kernel unless the context turned it off
+// (bnxSetRegrouping); the per-lane kernel is the same frame.
 static cudaError_t launchRenderJob(Context *ctx, const JobDD &job, cudaStream_t s) {
-  if (job.fr.fastMath && plainJob(job))
+  const bool plain = plainJob(job);
+  if (plain && ctx->sched.regrouped)
+    return job.fr.fastMath ? fastmath::launchRenderRegrouped(job.v, job.fr, ctx->dCounters, s)
+                           : launchRenderRegrouped(job.v, job.fr, ctx->dCounters, s);
+  if (job.fr.fastMath && plain)
     return fastmath::launchRender(job.v, job.fr, ctx->dCounters, ctx->blocksPerSM, ctx->threadsPerBlock, s, ctx->sched);
   return launchRender(job.v, job.fr, ctx->dCounters, ctx->blocksPerSM, ctx->threadsPerBlock, s, ctx->sched);
 }
@@ -1189,6 +1195,12 @@ BN_API long long bnxBoundsViolations(BNContext context) {
   getContext(context)->activate();
   return readBoundsViolations();
   BN_CATCH(-2)
+}
+
+BN_API void bnxSetRegrouping(BNContext context, int enable) {
+  BN_TRY
+  getContext(context)->sched.regrouped = enable ? 1 : 0;
+  BN_CATCH()
 }
 
 BN_API void bnxSetScheduling(BNContext context, int serviceBatch) {

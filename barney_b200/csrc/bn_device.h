@@ -112,6 +112,7 @@ struct JobDD {
 // serves them together.
 struct SchedDD {
   int serviceBatch = 22;
+  int regrouped = 0;  // plain single-frame jobs: the regrouped kernel (launchRenderRegrouped) instead of renderLoop's
 };
 
 // Device counters of one launch (samples, mcVisits, rays, errorFlags)
@@ -155,6 +156,12 @@ bool boundsCheckedBuild();
 constexpr int64_t kNoAllocMaxMacrocells = 64 * 64 * 64;
 cudaError_t launchRenderNoAlloc(VolumeDD v, FrameDD fr, int fmt, void *color, int roundUp, cudaStream_t s);
 
+// The regrouped render kernel for a plain single-frame job (no isosurface,
+// multi-scatter or principled volume; cudaErrorInvalidValue otherwise): the
+// same frame and counters as launchRender, pixel slots advanced by
+// phase-compacted lists in shared memory.  Launch shape from the occupancy.
+cudaError_t launchRenderRegrouped(const VolumeDD &vol, const FrameDD &frame, LaunchCounters *counters, cudaStream_t s);
+
 // Field samples and TF lookups (sampleAndMap) at n device points P into
 // device arrays scalar (NaN outside the field) and rgba.
 cudaError_t launchSampleProbe(const VolumeDD &vol, const float3 *P, int n, float *scalar, float4 *rgba, cudaStream_t s);
@@ -172,6 +179,7 @@ cudaError_t launchRenderBatch(const JobDD *jobs, const int *chunkStart, int numJ
                               int blocksPerSM, int threadsPerBlock, cudaStream_t s, const SchedDD &sd = SchedDD(),
                               int extended = 0, int voxelType = -1);
 cudaError_t launchSampleProbe(const VolumeDD &vol, const float3 *P, int n, float *scalar, float4 *rgba, cudaStream_t s);
+cudaError_t launchRenderRegrouped(const VolumeDD &vol, const FrameDD &frame, LaunchCounters *counters, cudaStream_t s);
 long long readBoundsViolationsHere();  // bounds-checked build only
 }  // namespace fastmath
 long long readBoundsViolationsHere();  // bounds-checked build only

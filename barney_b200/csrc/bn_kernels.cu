@@ -1597,6 +1597,608 @@ __global__ void __launch_bounds__(kRenderMaxThreads, EXT >= 2 ? kRenderMinBlocks
   renderLoop<T, false, LOG, EXT>(&job, nullptr, 1, numChunks, sd, ctr, sTF, u8lut);
 }
 
+// ---------------------------------------------------------------------------
+// Regrouped render kernel (plain single-frame jobs)
+// ---------------------------------------------------------------------------
+// A CTA owns kWFSlots pixel slots.  A slot's whole state -- its pixel and
+// wave, the accumulator and the ray in flight -- lives in shared memory, so
+// any thread of the CTA can advance any slot.  The CTA works in rounds of
+// four phases; each phase first compacts the slots that need it into a list
+// (warp ballots), then all threads work through that list:
+//   service  collisions (shading, shadow-ray spawn) and ended rays
+//            (accumulation) -- renderLoop's A1 and A2;
+//   fetch    new pixels for idle slots (one chunk range per round) -- A3;
+//   prepare  primary-ray generation and ray set-up -- A4 and A5;
+//   trace    macrocell walk and Woodcock steps -- B1 and B2.  A lane whose
+//            ray needs service stores it and takes the next slot of the
+//            list; the phase ends after kWFTraceIters steps of the warp or
+//            when the list is used up, and rays still in flight carry over
+//            to the next round.
+// Each slot runs exactly the state machine of a renderLoop lane (plain
+// kernels: no isosurface, multi-scatter or principled volume), in the same
+// order per pixel, so frames and work counters are the same bit for bit;
+// only which thread executes a step changes.
+// 384 slots for 256 threads, 3 CTAs per SM; a trace phase may end early
+// below 16 busy lanes of 32 after 4 steps (the fastest of the settings
+// measured on the 512^3 workload; all are slower than the per-lane kernel)
+constexpr int kWFThreads = 256;
+constexpr int kWFSlots = 384;
+constexpr int kWFMinBlocks = 3;
+constexpr int kWFTraceIters = 64;
+constexpr int kWFMinActive = 16;
+constexpr int kWFMinIters = 4;
+constexpr unsigned kWFMaxRounds = 1u << 22;
+
+struct WFSlots {
+  float4 acc[kWFSlots];
+  float ox[kWFSlots], oy[kWFSlots], oz[kWFSlots];     // ray origin
+  float dx[kWFSlots], dy[kWFSlots], dz[kWFSlots];     // ray direction (zero components fixed up by the set-up)
+  float rayTMax[kWFSlots];
+  unsigned seedLo[kWFSlots], seedHi[kWFSlots];       // the ray's RNG seed
+  int meta[kWFSlots];                                 // bits 0-3 LanePhase, bit 4 shadow ray, bits 8-13 TraceState::bits
+  int ix[kWFSlots], iy[kWFSlots], k[kWFSlots];        // pixel and wave of the launch
+  float stx[kWFSlots], sty[kWFSlots], stz[kWFSlots];  // shadow-ray throughput
+  float mis[kWFSlots];                                // shadow-ray MIS weight
+  float hx[kWFSlots], hy[kWFSlots], hz[kWFSlots];     // TF colour at the collision
+  float ddaTMax[kWFSlots], rayT0[kWFSlots], ncb[kWFSlots];
+  float tnx[kWFSlots], tny[kWFSlots], tnz[kWFSlots];
+  float tsx[kWFSlots], tsy[kWFSlots], tsz[kWFSlots];
+  int cx[kWFSlots], cy[kWFSlots], cz[kWFSlots];
+  unsigned rngLo[kWFSlots], rngHi[kWFSlots];          // the Woodcock RNG
+  float t[kWFSlots], tUpper[kWFSlots], maj[kWFSlots];
+  unsigned steps[kWFSlots];
+  int list[kWFSlots];
+  int listCount, listHead, live;
+  int curChunk, curBase, curLeft, newChunk0, newChunks, exhausted, aborted;
+};
+
+DEV uint64_t wfJoin(unsigned lo, unsigned hi) { return (uint64_t)lo | ((uint64_t)hi << 32); }
+DEV int wfPhase(int meta) { return meta & 15; }
+
+// The slots whose phase satisfies pred, in sh.list[0 .. sh.listCount).
+// Called by every thread of the CTA; sh.listCount must be 0 on entry, and the
+// list is complete after the caller's next __syncthreads.
+template <typename Pred>
+DEV void wfCompact(WFSlots &sh, Pred pred) {
+  const int lane = threadIdx.x & 31;
+  for (int s0 = 0; s0 < kWFSlots; s0 += kWFThreads) {
+    const int s = s0 + threadIdx.x;
+    const bool in = s < kWFSlots && pred(wfPhase(sh.meta[s]));
+    const unsigned m = __ballot_sync(0xffffffffu, in);
+    int base = 0;
+    if (lane == 0 && m) base = atomicAdd(&sh.listCount, __popc(m));
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if (in) sh.list[base + __popc(m & ((1u << lane) - 1u))] = s;
+  }
+}
+
+DEV void wfLoadTrace(const WFSlots &sh, int s, TraceState &ts) {
+  ts.org = f3(sh.ox[s], sh.oy[s], sh.oz[s]);
+  ts.dir = f3(sh.dx[s], sh.dy[s], sh.dz[s]);
+  ts.rayTMax = sh.rayTMax[s];
+  ts.ddaTMax = sh.ddaTMax[s];
+  ts.rayT0 = sh.rayT0[s];
+  ts.nextCellBegin = sh.ncb[s];
+  ts.tNext = f3(sh.tnx[s], sh.tny[s], sh.tnz[s]);
+  ts.tStep = f3(sh.tsx[s], sh.tsy[s], sh.tsz[s]);
+  ts.cx = sh.cx[s];
+  ts.cy = sh.cy[s];
+  ts.cz = sh.cz[s];
+  ts.bits = (sh.meta[s] >> 8) & 63;
+  ts.rng = wfJoin(sh.rngLo[s], sh.rngHi[s]);
+  ts.t = sh.t[s];
+  ts.tUpper = sh.tUpper[s];
+  ts.maj = sh.maj[s];
+}
+
+// bytes of dynamic shared memory: the slots, then the TF table
+__host__ __device__ inline size_t wfSlotsBytes() { return (sizeof(WFSlots) + 15) & ~(size_t)15; }
+
+template <int T, int LOG>
+__global__ void __launch_bounds__(kWFThreads, kWFMinBlocks)
+    renderKernelWF(const __grid_constant__ JobDD job, LaunchCounters *ctr) {
+  extern __shared__ __align__(16) unsigned char wfSmem[];
+  __shared__ float u8lut[256];
+  WFSlots &sh = *reinterpret_cast<WFSlots *>(wfSmem);
+  float4 *sTF = reinterpret_cast<float4 *>(wfSmem + wfSlotsBytes());
+  const VolumeDD &v = job.v;
+  const FrameDD &fr = job.fr;
+  const int tid = threadIdx.x;
+  const unsigned FULL = 0xffffffffu;
+  for (int i = tid; i < v.tfN; i += blockDim.x) sTF[i] = v.tf[i];
+  for (int i = tid; i < 256; i += blockDim.x) u8lut[i] = __fdiv_rn((float)i * 1.f, 255.f);
+  for (int s = tid; s < kWFSlots; s += blockDim.x) sh.meta[s] = LP_IDLE;
+  if (tid == 0) {
+    sh.curChunk = 0;
+    sh.curBase = 0;
+    sh.curLeft = 0;
+    sh.exhausted = 0;
+    sh.aborted = 0;
+  }
+  const int W = fr.width, H = fr.height;
+  const int npix = W * H;
+  const int frameChunks = (npix + kChunk - 1) / kChunk;
+  const int numChunks = fr.partCount > 1 ? partitionChunks(frameChunks, fr.partRank, fr.partCount) : frameChunks;
+  const bool cmp = fr.comp != nullptr;
+  unsigned nSamples = 0, nVisits = 0, nRays = 0, errBits = 0;
+  // this rank's chunk c -> the frame's chunk, and the pixels it holds
+  auto frameChunk = [&](int c) {
+    return fr.partCount > 1 ? (c / kPartTileChunks * fr.partCount + fr.partRank) * kPartTileChunks + c % kPartTileChunks
+                            : c;
+  };
+  auto chunkPixels = [&](int c) { return c < numChunks ? min(kChunk, npix - frameChunk(c) * kChunk) : 0; };
+
+  // every round steps every ray in flight at least once, so a frame ends in
+  // far fewer rounds than this bound; reaching it ends the launch with the
+  // iteration-cap error instead of running on
+  for (unsigned round = 0;; round++) {
+    if (round >= kWFMaxRounds) {
+      errBits |= ERR_ITER_CAP;
+      break;
+    }
+    if ((nSamples | nVisits | nRays) >= 0x80000000u) {
+      atomicAdd(&ctr->samples, (unsigned long long)nSamples);
+      atomicAdd(&ctr->mcVisits, (unsigned long long)nVisits);
+      atomicAdd(&ctr->rays, (unsigned long long)nRays);
+      nSamples = nVisits = nRays = 0;
+    }
+    // ---------------------------------------------------------------- service
+    if (tid == 0) sh.listCount = 0;
+    __syncthreads();
+    // collisions first, then ended rays: each warp runs mostly one of the two branches
+    wfCompact(sh, [](int p) { return p == LP_HIT; });
+    __syncthreads();
+    wfCompact(sh, [](int p) { return p == LP_ENDED; });
+    __syncthreads();
+    for (int j = tid; j < sh.listCount; j += kWFThreads) {
+      const int s = sh.list[j];
+      int meta = sh.meta[s];
+      const int phase = wfPhase(meta);
+      const bool shadowRay = (meta >> 4) & 1;
+      int kk = sh.k[s];
+      float4 acc = sh.acc[s];
+      const int accumID = fr.accumID0 + kk;
+      const float clampMax = 10.f * (1 + accumID);
+      const int64_t pix = (int64_t)sh.iy[s] * W + sh.ix[s];
+      float4 comp = make_float4(0.f, 0.f, 0.f, 0.f);
+      if (cmp && BNB_IN(pix, (long long)npix)) comp = fr.comp[pix];  // the scratch copy of this pixel's terms
+      bool spawned = false;
+      if (phase == LP_HIT) {
+        // A1 (shadeRays.cu:608-746)
+        if (!shadowRay) {
+          if (accumID == 0) {
+            acc = make_float4(0.f, 0.f, 0.f, 1.f);
+            comp = make_float4(0.f, 0.f, 0.f, 0.f);
+          } else {
+            accAdd(acc.w, comp.w, 1.f, cmp);
+          }
+          const float tHit = sh.t[s];
+          const float3 org = f3(sh.ox[s], sh.oy[s], sh.oz[s]);
+          const float3 dir = f3(sh.dx[s], sh.dy[s], sh.dz[s]);
+          const float3 P = f3(org.x + tHit * dir.x, org.y + tHit * dir.y, org.z + tHit * dir.z);
+          const float3 hitRGB = f3(sh.hx[s], sh.hy[s], sh.hz[s]);
+          if (fr.emissionAbsorption) {
+            const float ex = fmin_(hitRGB.x, clampMax), ey = fmin_(hitRGB.y, clampMax), ez = fmin_(hitRGB.z, clampMax);
+            if (accumID == 0) acc = make_float4(ex, ey, ez, 1.f);
+            else {
+              if (ex > 0.f) accAdd(acc.x, comp.x, ex, cmp);
+              if (ey > 0.f) accAdd(acc.y, comp.y, ey, cmp);
+              if (ez > 0.f) accAdd(acc.z, comp.z, ez, cmp);
+            }
+          } else {
+            uint64_t raySeed = wfJoin(sh.seedLo[s], sh.seedHi[s]);
+            uint64_t random = rngDerive(raySeed, (uint64_t)__float_as_uint(tHit));
+            const int bits = (meta >> 8) & 63;
+            const float3 won = normalize3(f3((bits & 8) ? 0.f : dir.x, (bits & 16) ? 0.f : dir.y, (bits & 32) ? 0.f : dir.z));
+            const float3 woN = f3(-won.x, -won.y, -won.z);
+            const float offsetEpsilon = fmax_(1e-4f, 1e-6f * fmax_(fmax_(fabsf(P.x), fabsf(P.y)), fabsf(P.z)));
+            LightSample ls;
+            bool needsMIS, isDir;
+            if (sampleLights(fr, random, ls, needsMIS, isDir)) {
+              float3 alb;
+              float fpdf;
+              if (v.phase == PHASE_SIMPLE) {
+                alb = f3(.7f * hitRGB.x, .7f * hitRGB.y, .7f * hitRGB.z);
+                fpdf = kOneOverFourPi;
+              } else {
+                const float a = v.scatteringAlbedo;
+                alb = f3(a * hitRGB.x, a * hitRGB.y, a * hitRGB.z);
+                const float3 wi_in = normalize3(f3(-woN.x, -woN.y, -woN.z));
+                fpdf = hgPhase(v.anisotropy, dot3(wi_in, normalize3(ls.dir)));
+              }
+              float3 fv = f3(fpdf * alb.x, fpdf * alb.y, fpdf * alb.z);
+              if (fpdf > 0.f && !(fmax_(fmax_(fv.x, fv.y), fv.z) < 1e-4f)) {
+                fv = f3(fmin_(fv.x, 13.f), fmin_(fv.y, 13.f), fmin_(fv.z, 13.f));
+                const float ip = isinf(ls.pdf) ? 1.f : (1.f / ls.pdf);
+                const float3 tp = f3(1.f * ip * fv.x * ls.radiance.x * 1.f, 1.f * ip * fv.y * ls.radiance.y * 1.f,
+                                     1.f * ip * fv.z * ls.radiance.z * 1.f);
+                float misWeight = 1.f;
+                bool alive = true;
+                if (!isDir && needsMIS) {
+                  const float pl = kOneOverFourPi;
+                  float ps;
+                  if (v.phase == PHASE_SIMPLE) ps = kOneOverFourPi;
+                  else ps = hgPhase(v.anisotropy, dot3(normalize3(f3(-woN.x, -woN.y, -woN.z)), normalize3(ls.dir)));
+                  misWeight = pl / (pl + ps + 1e-10f);
+                  if (misWeight < 1e-5f) alive = false;
+                }
+                const float sTMax = kInf * (1.f - 2.f * offsetEpsilon);
+                if (alive && sTMax > 0.f) {
+                  sh.stx[s] = roundHalf(tp.x);
+                  sh.sty[s] = roundHalf(tp.y);
+                  sh.stz[s] = roundHalf(tp.z);
+                  sh.mis[s] = misWeight;
+                  sh.ox[s] = P.x + offsetEpsilon * woN.x;
+                  sh.oy[s] = P.y + offsetEpsilon * woN.y;
+                  sh.oz[s] = P.z + offsetEpsilon * woN.z;
+                  sh.dx[s] = ls.dir.x;
+                  sh.dy[s] = ls.dir.y;
+                  sh.dz[s] = ls.dir.z;
+                  sh.rayTMax[s] = sTMax;
+                  meta = (meta & ~31) | LP_BEGIN | 16;
+                  spawned = true;
+                  nRays++;
+                  sh.steps[s] = 0;
+                }
+              }
+            }
+            sh.seedLo[s] = (unsigned)raySeed;
+            sh.seedHi[s] = (unsigned)(raySeed >> 32);
+          }
+        }
+      } else {
+        // A2 (shadeRays.cu:507-600, 996-1040)
+        if (!shadowRay) {
+          float4 bg = fr.bgColor;
+          if (!(fr.bgColor.w >= 0.f)) {
+            const float tt = (sh.iy[s] + .5f) / float(H);
+            bg = make_float4((1.0f - tt) * 0.9f + tt * 0.15f, (1.0f - tt) * 0.9f + tt * 0.25f,
+                             (1.0f - tt) * 0.9f + tt * .8f, (1.0f - tt) * 1.f + tt * 1.f);
+          }
+          const float f0x = fmin_(bg.x, clampMax), f0y = fmin_(bg.y, clampMax), f0z = fmin_(bg.z, clampMax);
+          if (accumID == 0) {
+            acc = make_float4(f0x, f0y, f0z, bg.w);
+            comp = make_float4(0.f, 0.f, 0.f, 0.f);
+          } else {
+            if (bg.w > 0.f) accAdd(acc.w, comp.w, bg.w, cmp);
+            if (f0x > 0.f) accAdd(acc.x, comp.x, f0x, cmp);
+            if (f0y > 0.f) accAdd(acc.y, comp.y, f0y, cmp);
+            if (f0z > 0.f) accAdd(acc.z, comp.z, f0z, cmp);
+          }
+        } else {
+          const float mw = sh.mis[s];
+          const float f1x = fmin_(mw * sh.stx[s], clampMax);
+          const float f1y = fmin_(mw * sh.sty[s], clampMax);
+          const float f1z = fmin_(mw * sh.stz[s], clampMax);
+          if (f1x > 0.f) accAdd(acc.x, comp.x, f1x, cmp);
+          if (f1y > 0.f) accAdd(acc.y, comp.y, f1y, cmp);
+          if (f1z > 0.f) accAdd(acc.z, comp.z, f1z, cmp);
+        }
+      }
+      if (!spawned) {
+        if (++kk == fr.spp) {
+          if (BNB_IN(pix, (long long)npix)) fr.accum[pix] = acc;
+          meta = (meta & ~15) | LP_IDLE;
+        } else {
+          meta = (meta & ~15) | LP_NEWSAMPLE;
+        }
+      }
+      if (cmp && BNB_IN(pix, (long long)npix)) fr.comp[pix] = comp;
+      sh.acc[s] = acc;
+      sh.k[s] = kk;
+      sh.meta[s] = meta;
+    }
+    // ---------------------------------------------------------------- fetch
+    __syncthreads();
+    if (tid == 0) sh.listCount = 0;
+    __syncthreads();
+    wfCompact(sh, [](int p) { return p == LP_IDLE; });
+    __syncthreads();
+    if (tid == 0) {
+      const int n = sh.listCount;
+      int nNew = 0;
+      if (n > sh.curLeft && !sh.exhausted) {
+        nNew = (n - sh.curLeft + kChunk - 1) / kChunk;
+        sh.newChunk0 = (int)atomicAdd(&ctr->nextPixel, (unsigned)nNew);
+        if (*(volatile unsigned *)&ctr->abort) {
+          sh.aborted = 1;
+          sh.exhausted = 1;
+          nNew = 0;
+        }
+      }
+      sh.newChunks = nNew;
+    }
+    __syncthreads();
+    {
+      const int n = sh.listCount, left = sh.curLeft, nNew = sh.newChunks, c0 = sh.newChunk0;
+      const bool aborted = sh.aborted;
+      for (int j = tid; j < n; j += kWFThreads) {
+        int c = -1, w = 0;
+        if (j < left) {
+          c = sh.curChunk;
+          w = sh.curBase + j;
+        } else if (!aborted) {
+          const int jj = j - left, i = jj / kChunk, o = jj % kChunk;
+          if (i < nNew && o < chunkPixels(c0 + i)) {
+            c = c0 + i;
+            w = o;
+          }
+        }
+        if (c < 0) continue;  // no pixel for this slot this round
+        const int s = sh.list[j];
+        // pixel order: 4-row bands, column-major inside a band (8x4 tiles per 32 pixels)
+        const int wf = frameChunk(c) * kChunk + w;
+        const int band = wf / (4 * W);
+        const int rows = min(4, H - 4 * band);
+        const int within = wf - band * 4 * W;
+        const int px = within / rows, py = 4 * band + within % rows;
+        const int64_t pix = (int64_t)py * W + px;
+        const bool pixIn = BNB_IN(pix, (long long)npix);
+        sh.ix[s] = px;
+        sh.iy[s] = py;
+        sh.k[s] = 0;
+        sh.acc[s] = (fr.accumID0 > 0 && pixIn) ? fr.accum[pix] : make_float4(0.f, 0.f, 0.f, 0.f);
+        if (cmp && pixIn && fr.accumID0 == 0) fr.comp[pix] = make_float4(0.f, 0.f, 0.f, 0.f);
+        sh.meta[s] = LP_NEWSAMPLE;
+      }
+    }
+    __syncthreads();
+    if (tid == 0) {
+      const int n = sh.listCount;
+      if (sh.newChunks > 0) {
+        const int last = sh.newChunk0 + sh.newChunks - 1;
+        const int used = n - sh.curLeft - kChunk * (sh.newChunks - 1);
+        if (last < numChunks) {
+          sh.curChunk = last;
+          sh.curBase = used;
+          sh.curLeft = max(0, chunkPixels(last) - used);
+        } else {
+          sh.curLeft = 0;
+        }
+        if (sh.newChunk0 + sh.newChunks >= numChunks) sh.exhausted = 1;
+      } else if (!sh.aborted) {
+        const int took = min(n, sh.curLeft);
+        sh.curBase += took;
+        sh.curLeft -= took;
+      }
+      sh.listCount = 0;
+      sh.live = 0;
+    }
+    __syncthreads();
+    // ---------------------------------------------------------------- prepare
+    wfCompact(sh, [](int p) { return p == LP_NEWSAMPLE; });  // new primary rays first, then shadow rays
+    __syncthreads();
+    wfCompact(sh, [](int p) { return p == LP_BEGIN; });
+    __syncthreads();
+    for (int j = tid; j < sh.listCount; j += kWFThreads) {
+      const int s = sh.list[j];
+      int meta = sh.meta[s];
+      float3 org, dir;
+      float tMax;
+      uint64_t raySeed;
+      if (wfPhase(meta) == LP_NEWSAMPLE) {
+        // A4 (generateRays.cu:71-243)
+        const int px = sh.ix[s], py = sh.iy[s];
+        const int accumID = fr.accumID0 + sh.k[s];
+        const unsigned uAcc = (unsigned)accumID;
+        uint64_t rnd = rngSeed2((unsigned)px + (unsigned)W * uAcc, (unsigned)py + (unsigned)H * uAcc);
+        raySeed = rngSeed2((unsigned)px + uAcc * (unsigned)W, (uint32_t)py);
+        const float pixel_u = (accumID == 0) ? .5f : rngFloat(rnd);
+        const float pixel_v = (accumID == 0) ? .5f : rngFloat(rnd);
+        const float image_u = ((px + pixel_u) / float(W));
+        const float image_v = ((py + pixel_v) / float(H));
+        const float aspect = W / float(H);
+        const float su = 1.f * aspect * (image_u - .5f), sv = 1.f * (image_v - .5f);
+        float3 d = f3(fr.dir00.x + su * fr.dirdu.x + sv * fr.dirdv.x, fr.dir00.y + su * fr.dirdu.y + sv * fr.dirdv.y,
+                      fr.dir00.z + su * fr.dirdu.z + sv * fr.dirdv.z);
+        d = normalize3(d);
+        float3 o = fr.lens00;
+        tMax = 1e30f;
+        if (fr.cutPlane.w > -1e28f) {
+          const float3 N = f3(fr.cutPlane.x, fr.cutPlane.y, fr.cutPlane.z);
+          const float dist_org = dot3(N, o) + fr.cutPlane.w;
+          const float denom = dot3(N, d);
+          if (dist_org >= 0.f) {
+            if (denom < 0.f) tMax = fmin_(tMax, -dist_org / denom);
+          } else {
+            if (denom > 0.f) {
+              const float te = -dist_org / denom;
+              o = f3(o.x + te * d.x, o.y + te * d.y, o.z + te * d.z);
+            } else tMax = 0.f;
+          }
+        }
+        meta &= ~16;  // a primary ray
+        nRays++;
+        sh.steps[s] = 0;
+        org = o;
+        dir = d;
+      } else {
+        org = f3(sh.ox[s], sh.oy[s], sh.oz[s]);
+        dir = f3(sh.dx[s], sh.dy[s], sh.dz[s]);
+        tMax = sh.rayTMax[s];
+        raySeed = wfJoin(sh.seedLo[s], sh.seedHi[s]);
+      }
+      // A5: TraceRays::run fix-up, isProg prologue, dda3 set-up
+      TraceState ts;
+      const bool inside = traceBegin(v, ts, org, dir, tMax, raySeed);
+      sh.ox[s] = ts.org.x;
+      sh.oy[s] = ts.org.y;
+      sh.oz[s] = ts.org.z;
+      sh.dx[s] = ts.dir.x;
+      sh.dy[s] = ts.dir.y;
+      sh.dz[s] = ts.dir.z;
+      sh.rayTMax[s] = ts.rayTMax;
+      sh.seedLo[s] = (unsigned)raySeed;
+      sh.seedHi[s] = (unsigned)(raySeed >> 32);
+      if (inside) {
+        sh.ddaTMax[s] = ts.ddaTMax;
+        sh.rayT0[s] = ts.rayT0;
+        sh.ncb[s] = ts.nextCellBegin;
+        sh.tnx[s] = ts.tNext.x;
+        sh.tny[s] = ts.tNext.y;
+        sh.tnz[s] = ts.tNext.z;
+        sh.tsx[s] = ts.tStep.x;
+        sh.tsy[s] = ts.tStep.y;
+        sh.tsz[s] = ts.tStep.z;
+        sh.cx[s] = ts.cx;
+        sh.cy[s] = ts.cy;
+        sh.cz[s] = ts.cz;
+        sh.rngLo[s] = (unsigned)ts.rng;
+        sh.rngHi[s] = (unsigned)(ts.rng >> 32);
+        meta = (meta & ~(15 | (63 << 8))) | LP_CELL | (ts.bits << 8);
+      } else {
+        // rays that miss keep only their fix-up bits (none are read at a miss)
+        meta = (meta & ~15) | LP_ENDED;
+      }
+      sh.meta[s] = meta;
+    }
+    __syncthreads();
+    // ---------------------------------------------------------------- trace
+    if (tid == 0) {
+      sh.listCount = 0;
+      sh.listHead = 0;
+    }
+    __syncthreads();
+    wfCompact(sh, [](int p) { return p == LP_CELL || p == LP_WOODCOCK; });
+    __syncthreads();
+    {
+      const int lane = tid & 31;
+      const int n = sh.listCount;
+      int s = -1;
+      int phase = LP_IDLE, meta = 0;
+      unsigned steps = 0;
+      TraceState ts;
+      for (int it = 0; it < kWFTraceIters; it++) {
+        // lanes without a ray take the next slots of the list
+        const unsigned need = __ballot_sync(FULL, s < 0);
+        if (need) {
+          int base = 0;
+          if (lane == 0) base = atomicAdd(&sh.listHead, __popc(need));
+          base = __shfl_sync(FULL, base, 0);
+          const int r = base + __popc(need & ((1u << lane) - 1u));
+          if (s < 0 && r < n) {
+            s = sh.list[r];
+            meta = sh.meta[s];
+            phase = wfPhase(meta);
+            steps = sh.steps[s];
+            wfLoadTrace(sh, s, ts);
+          }
+        }
+        if (!__ballot_sync(FULL, s >= 0)) break;  // the list is used up
+        if (s >= 0) {
+          // B1 (DDA.h:172-200, MCAccelerator.h:596-612)
+          if (phase == LP_CELL) {
+            while (true) {
+              const float tClosest = fmin_(fmin_(ts.tNext.x, ts.tNext.y), ts.tNext.z);
+              const int ci = ts.cx + v.mcDims.x * (ts.cy + v.mcDims.y * ts.cz);
+              const bool occupied = BNB_IN(ci, (long long)v.mcDims.x * v.mcDims.y * v.mcDims.z) &&
+                                    ((__ldg(v.mcOccupied + (ci >> 5)) >> (ci & 31)) & 1u);
+              nVisits++;
+              if (!occupied) {
+                if (!ddaStep(v, ts, tClosest)) { phase = LP_ENDED; break; }
+                if (++steps > (1u << 22)) { errBits |= ERR_ITER_CAP; phase = LP_ENDED; break; }
+              } else {
+                ts.maj = __ldg(v.majorants + ci);
+                ts.t = ts.rayT0 + ts.nextCellBegin;
+                ts.tUpper = fmin_(ts.rayT0 + fmin_(tClosest, ts.ddaTMax), ts.rayTMax);
+                phase = LP_WOODCOCK;
+                break;
+              }
+            }
+          }
+          // B2 (Volume.h:180-201)
+          if (phase == LP_WOODCOCK) {
+            const float r = rngFloat(ts.rng);
+            const float dt = LOG == 1 ? (-logPortable(1.f - r) / ts.maj) : (-fastLog(1.f - r) / ts.maj);
+            ts.t += dt;
+            if (ts.t >= ts.tUpper) {
+              const float tClosest = fmin_(fmin_(ts.tNext.x, ts.tNext.y), ts.tNext.z);
+              phase = ddaStep(v, ts, tClosest) ? LP_CELL : LP_ENDED;
+            } else {
+              const float3 P = f3(ts.org.x + ts.t * ts.dir.x, ts.org.y + ts.t * ts.dir.y, ts.org.z + ts.t * ts.dir.z);
+              const float smp = sampleField<T>(v, P, u8lut);
+              nSamples++;
+              float w = 0.f, f = 0.f;
+              int idx = 0;
+              if (!isnan(smp)) {
+                tfLocate(v, smp, idx, f);
+                if (!BNB_IN(idx, v.tfN - 1)) idx = 0;
+                w = __fmul_rn(lerp_l(f, sTF[idx].w, sTF[idx + 1].w), v.baseDensity);
+              }
+              if (w >= rngFloat(ts.rng) * ts.maj) {
+                float3 hit = f3(0.f, 0.f, 0.f);
+                if (!isnan(smp)) {
+                  const float4 a = sTF[idx], b = sTF[idx + 1];
+                  hit = f3(lerp_l(f, a.x, b.x), lerp_l(f, a.y, b.y), lerp_l(f, a.z, b.z));
+                }
+                sh.hx[s] = hit.x;
+                sh.hy[s] = hit.y;
+                sh.hz[s] = hit.z;
+                phase = LP_HIT;
+              }
+            }
+            if (++steps > (1u << 22)) {
+              errBits |= ERR_ITER_CAP;
+              phase = LP_ENDED;
+            }
+          }
+          if (phase != LP_CELL && phase != LP_WOODCOCK) {  // the ray needs service: store it, take another
+            sh.t[s] = ts.t;
+            sh.meta[s] = (meta & ~15) | phase;
+            sh.steps[s] = steps;
+            s = -1;
+          }
+        }
+        // after kWFMinIters steps of every ray it holds: once the list is used
+        // up and the warp runs under three quarters full, its rays carry over
+        // to the next round instead of holding the CTA at the barrier.  (Every
+        // slot of the list has been taken and stepped by then.)
+        if (it + 1 >= kWFMinIters && __popc(__ballot_sync(FULL, s >= 0)) < kWFMinActive &&
+            *(volatile int *)&sh.listHead >= n)
+          break;
+      }
+      if (s >= 0) {  // carries over to the next round
+        sh.ncb[s] = ts.nextCellBegin;
+        sh.tnx[s] = ts.tNext.x;
+        sh.tny[s] = ts.tNext.y;
+        sh.tnz[s] = ts.tNext.z;
+        sh.cx[s] = ts.cx;
+        sh.cy[s] = ts.cy;
+        sh.cz[s] = ts.cz;
+        sh.rngLo[s] = (unsigned)ts.rng;
+        sh.rngHi[s] = (unsigned)(ts.rng >> 32);
+        sh.t[s] = ts.t;
+        sh.tUpper[s] = ts.tUpper;
+        sh.maj[s] = ts.maj;
+        sh.steps[s] = steps;
+        sh.meta[s] = (meta & ~15) | phase;
+      }
+      // count live slots for the exit test (after the barrier below)
+      __syncthreads();
+      int liveHere = 0;
+      for (int s2 = tid; s2 < kWFSlots; s2 += kWFThreads) liveHere += wfPhase(sh.meta[s2]) != LP_IDLE;
+      liveHere = __reduce_add_sync(FULL, liveHere);
+      if (lane == 0 && liveHere) atomicAdd(&sh.live, liveHere);
+    }
+    __syncthreads();
+    if (sh.exhausted && sh.curLeft <= 0 && sh.live == 0) break;
+  }
+  if (sh.aborted && threadIdx.x == 0) errBits |= ERR_ABORTED;
+  unsigned long long wSamples = nSamples, wVisits = nVisits, wRays = nRays;
+  for (int o = 16; o > 0; o >>= 1) {
+    wSamples += __shfl_down_sync(FULL, wSamples, o);
+    wVisits += __shfl_down_sync(FULL, wVisits, o);
+    wRays += __shfl_down_sync(FULL, wRays, o);
+    errBits |= __shfl_down_sync(FULL, errBits, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomicAdd(&ctr->samples, wSamples);
+    atomicAdd(&ctr->mcVisits, wVisits);
+    atomicAdd(&ctr->rays, wRays);
+    if (errBits) atomicOr(&ctr->errorFlags, (unsigned long long)errBits);
+  }
+}
+
 // T: the voxel type every job of the batch has, or -1 (mixed: a switch per sample)
 template <int T, int EXT>
 __global__ void __launch_bounds__(kRenderMaxThreads, EXT >= 2 ? kRenderMinBlocksIso : EXT ? kRenderMinBlocksExt : kRenderMinBlocks)
@@ -1801,6 +2403,33 @@ static cudaError_t launchRenderT(const VolumeDD &v, const FrameDD &fr, const Sch
   job.fr = fr;
   kern<<<smCount() * bps, tpb, smem, s>>>(job, sd, ctr);
   return cudaGetLastError();
+}
+
+template <int T>
+static cudaError_t launchRenderWFT(const VolumeDD &v, const FrameDD &fr, LaunchCounters *ctr, cudaStream_t s) {
+  const size_t smem = wfSlotsBytes() + (size_t)v.tfN * sizeof(float4);
+  auto kern = fr.exactLog ? renderKernelWF<T, 1> : renderKernelWF<T, 0>;
+  if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+    return cudaGetLastError();
+  int occ = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kWFThreads, smem) != cudaSuccess)
+    return cudaGetLastError();
+  JobDD job;
+  job.v = v;
+  job.fr = fr;
+  kern<<<smCount() * (occ > 0 ? occ : 1), kWFThreads, smem, s>>>(job, ctr);
+  return cudaGetLastError();
+}
+
+cudaError_t launchRenderRegrouped(const VolumeDD &v, const FrameDD &fr, LaunchCounters *ctr, cudaStream_t s) {
+  if (v.iso.enabled || fr.maxVolumeBounces > 0 || v.pv.enabled) return cudaErrorInvalidValue;  // plain jobs only
+  switch (v.type) {
+  case VOX_F32: return launchRenderWFT<VOX_F32>(v, fr, ctr, s);
+  case VOX_U8: return launchRenderWFT<VOX_U8>(v, fr, ctr, s);
+  case VOX_F16: return launchRenderWFT<VOX_F16>(v, fr, ctr, s);
+  case VOX_U16: return launchRenderWFT<VOX_U16>(v, fr, ctr, s);
+  default: return launchRenderWFT<VOX_BF16>(v, fr, ctr, s);
+  }
 }
 
 cudaError_t launchRender(const VolumeDD &v, const FrameDD &fr, LaunchCounters *ctr, int bps, int tpb, cudaStream_t s,

@@ -62,6 +62,8 @@ def parse():
     p.add_argument("--tile-dp", action="store_true",
                    help="configs 1-3 on N GPUs: split each frame's pixel tiles across the ranks and gather "
                         "the frame over NCCL every step (strong scaling) instead of one frame per rank")
+    p.add_argument("--kernel", default="per-lane", choices=["per-lane", "regrouped"],
+                   help="render kernel of plain jobs: one pixel per lane (default) or regrouped pixel slots")
     p.add_argument("--rmse", action="store_true", help="image RMSE of every storage form vs the FP64 oracle")
     p.add_argument("--rmse-size", default="96x54", help="image size of the RMSE frames")
     p.add_argument("--rmse-spp", type=int, default=4096)
@@ -294,6 +296,7 @@ def run_ours(args):
 
     d, desc = workload(args, torch, "cuda")
     r = bn.VolumeRenderer(d, color_format="rgba8", gpu=local)
+    r.set_regrouping(args.kernel == "regrouped")
     stream = torch.cuda.current_stream()
     r.L.bnxSetStream(r.ctx, stream.cuda_stream)
     bn.check()
@@ -455,7 +458,8 @@ def run_ours(args):
             "higher_is_better": True, "scaling": "strong" if tile_dp else "weak", "vs_baseline": None,
             "dtype": d["dtype"],
             "data": "synthetic (seeded value noise / Gaussian blobs generated on device)",
-            "config": dict(desc, parallelism=(f"pixel tiles x{world}, NCCL all-gather per frame" if tile_dp
+            "config": dict(desc, kernel=args.kernel,
+                           parallelism=(f"pixel tiles x{world}, NCCL all-gather per frame" if tile_dp
                                               else f"replicas x{world}" if world > 1 else "single GPU"),
                            l2="inputs larger than L2" if flush is None
                            else "L2 flushed before every timed step (256 MB write, untimed)"),

@@ -297,6 +297,17 @@ BN_API void bnxSetPixelPartition(BNContext context, int rank, int count);
 BN_API void bnxPixelPartitionOwners(int width, int height, int count, int *owners);
 /* Launch parameters of the render kernel (0 = automatic). */
 BN_API void bnxSetLaunchConfig(BNContext context, int blocksPerSM, int threadsPerBlock);
+/* With enable != 0, plain jobs (no isosurface, multi-scatter or principled
+   volume) of bnRender, and single-job batches without a graph, render with
+   the regrouped kernel: pixel slots whose state lives in shared memory,
+   advanced phase by phase (shading and accumulation, new pixels, ray
+   generation and set-up, macrocell walk and Woodcock steps) over lists
+   compacted per phase, so that every phase runs with full warps.  The
+   default (0) is the per-lane kernel (one pixel per lane;
+   bnxSetLaunchConfig and bnxSetScheduling apply to it), which is faster on
+   the workloads measured.  Both give the same frames and counters.  No
+   reference counterpart. */
+BN_API void bnxSetRegrouping(BNContext context, int enable);
 /* Warp scheduling of the render kernel: a warp keeps stepping macrocells and
    Woodcock ranges until at least serviceBatch of its lanes (or all of its
    busy lanes) need service -- shading, accumulation, a new ray -- and then
