@@ -106,7 +106,8 @@ class BNXLaunchConfig(ctypes.Structure):
 
 
 class BNXServerConfig(ctypes.Structure):
-    _fields_ = [("hbmBudgetBytes", ctypes.c_size_t), ("maxSlots", ctypes.c_int), ("sliceWaves", ctypes.c_int)]
+    _fields_ = [("hbmBudgetBytes", ctypes.c_size_t), ("maxSlots", ctypes.c_int), ("sliceWaves", ctypes.c_int),
+                ("slicePixelWaves", ctypes.c_longlong)]
 
 
 _F3 = ctypes.c_float * 3
@@ -568,10 +569,10 @@ def merge_partitions(frames, owners):
 class Server:
     """Continuous-batching render server over resident volumes (bnxServer*)."""
 
-    def __init__(self, context, hbm_budget_bytes=150 << 30, max_slots=256, slice_waves=4):
+    def __init__(self, context, hbm_budget_bytes=150 << 30, max_slots=256, slice_waves=4, slice_pixel_waves=0):
         self.L = lib()
         self.context = context
-        cfg = BNXServerConfig(hbm_budget_bytes, max_slots, slice_waves)
+        cfg = BNXServerConfig(hbm_budget_bytes, max_slots, slice_waves, slice_pixel_waves)
         self.h = self.L.bnxServerCreate(context.ctx, ctypes.byref(cfg))
         check()
 

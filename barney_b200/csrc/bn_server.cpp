@@ -300,13 +300,23 @@ struct Server {
       std::vector<BatchEntry> entries;
       std::vector<int> waves;
       long long sliceWaves = 0, pixelWaves = 0;
-      for (auto &r : slice) {
-        const int n = std::min(cfg.sliceWaves, r->spp - r->wavesDone);
-        sliceWaves += n;
-        pixelWaves += (long long)n * r->fb->width * r->fb->height;
-        r->renderer->p.pathsPerPixel = n;
-        waves.push_back(n);
-        entries.push_back({r->renderer.get(), r->model.get(), r->camera.get(), r->fb.get()});
+      {
+        // oldest first (active is in admission order) while the slice's
+        // pixel-waves fit cfg.slicePixelWaves; the others wait for the next
+        // launch, so that no slice holds the GPU for long
+        std::vector<std::shared_ptr<ServerRequest>> inSlice;
+        for (auto &r : slice) {
+          const int n = std::min(cfg.sliceWaves, r->spp - r->wavesDone);
+          const long long pw = (long long)n * r->fb->width * r->fb->height;
+          if (!inSlice.empty() && cfg.slicePixelWaves > 0 && pixelWaves + pw > cfg.slicePixelWaves) continue;
+          sliceWaves += n;
+          pixelWaves += pw;
+          r->renderer->p.pathsPerPixel = n;
+          waves.push_back(n);
+          entries.push_back({r->renderer.get(), r->model.get(), r->camera.get(), r->fb.get()});
+          inSlice.push_back(r);
+        }
+        slice.swap(inSlice);
       }
       const auto t0 = Clock::now();
       NvtxRange range("server slice");
@@ -347,7 +357,21 @@ struct Server {
         }
         finished[r->id] = r;
       }
-      active.swap(still);
+      // requests left out of this slice stay active, in admission order
+      {
+        std::vector<std::shared_ptr<ServerRequest>> next;
+        size_t si = 0;
+        for (auto &r : active) {
+          if (si < slice.size() && slice[si] == r) {
+            si++;
+            if (!r->done) next.push_back(r);
+          } else {
+            next.push_back(r);
+          }
+        }
+        active.swap(next);
+      }
+      (void)still;
       if (trace) {
         std::fprintf(trace, "%.3f %.3f %.3f %.3f %zu %d %d %zu %lld %lld\n",
                      std::chrono::duration<double, std::milli>(t0 - created).count(),
@@ -384,6 +408,7 @@ BN_API BNXServer bnxServerCreate(BNContext context, const BNXServerConfig *confi
   BNXServerConfig cfg{(size_t)150 << 30, 256, 4};
   if (config) cfg = *config;
   if (cfg.maxSlots < 1 || cfg.sliceWaves < 1) throw Error(E_INVALID_ARG, "maxSlots and sliceWaves must be >= 1");
+  if (cfg.slicePixelWaves < 0) throw Error(E_INVALID_ARG, "slicePixelWaves must be >= 0");
   c->activate();
   auto s = std::make_unique<Server>(c, cfg);
   Server *raw = s.get();

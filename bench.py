@@ -59,6 +59,8 @@ def parse():
     p.add_argument("--e2e-steps", type=int, default=None)
     p.add_argument("--cpu-seconds", type=float, default=12.0)
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-serving", action="store_true",
+                   help="skip the served-vs-plain measurement that the default run adds")
     p.add_argument("--tile-dp", action="store_true",
                    help="configs 1-3 on N GPUs: split each frame's pixel tiles across the ranks and gather "
                         "the frame over NCCL every step (strong scaling) instead of one frame per rank")
@@ -450,6 +452,15 @@ def run_ours(args):
         cpu.pop("seconds", None)
     r.close()
 
+    serving = None
+    if world == 1 and args.config == "2" and not args.no_serving and d["spp"] == 64 and d["dtype"] == "f32" \
+            and not d.get("max_volume_bounces") and not d.get("iso") and d.get("phase") != "simple":
+        torch.cuda.empty_cache()
+        # the north star's comparison on one request stream, bounded for the
+        # default run (--config 5 runs it at 10 000 requests per rate)
+        serving = serving_arms(n_sat=400, rates=[200.0, 1000.0], n_rate=400)
+        serving["reduced"] = "400 requests at saturation and per rate (the full sweep: bench.py --config 5)"
+
     if rank == 0:
         n_frames = (1 if tile_dp else world) * args.steps
         line = {
@@ -479,6 +490,9 @@ def run_ours(args):
         if fast is not None:
             line["fast_math"] = fast
             line["gpu_launches"] += 2 * args.steps
+        if serving is not None:
+            line["serving"] = serving
+            line["served_over_plain"] = serving["served_over_plain"]
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.barrier()
@@ -546,35 +560,31 @@ def run_batch(args):
     return 0
 
 
-def serving_volumes(xp, device, storage=None):
-    """16 resident volumes, seeds 100-115: edge log-U[128, 1024], field and
-    storage type drawn per seed (storage forced to `storage` if given)."""
+def serving_volumes(xp, device):
+    """16 resident float32 volumes, seeds 100-115: edge log-U[128, 1024] and
+    the field (Gaussian blobs or value noise) drawn per seed."""
     import math
     import numpy as np
     from barney_b200 import synth
-    vols = []
+    out = []
     for seed in range(100, 116):
         rng = np.random.default_rng(seed)
         edge = int(round(math.exp(rng.uniform(math.log(128), math.log(1024)))))
         field = "blobs" if rng.integers(2) == 0 else "noise"
-        dtype = ["u8", "f16", "f32"][int(rng.integers(3))]
-        vols.append((seed, edge, field, storage or dtype))
-    out = []
-    for seed, edge, field, dtype in vols:
         f = synth.blobs(edge, seed, xp=xp, device=device) if field == "blobs" else \
             synth.value_noise(edge, seed, xp=xp, device=device)
-        vol = synth.to_storage(f, dtype)
         if field == "blobs":
-            d = synth.scene(vol, dtype, 256, 256, synth.tf_linear_ramp(128), 50.0, synth.DEFAULT_CAMERA, ambient=1.0)
+            d = synth.scene(f, "f32", 256, 256, synth.tf_linear_ramp(128), 50.0, synth.DEFAULT_CAMERA, ambient=1.0)
         else:
-            d = synth.config2(vol=vol, dtype=dtype, width=256, height=256)
+            d = synth.config2(vol=f, dtype="f32", width=256, height=256)
         d["seed"], d["edge"], d["field"] = seed, edge, field
         out.append(d)
-        del f
     return out
 
 
 def request_stream(n, seed=7):
+    """n requests: a volume of the 16, side {256, 512, 1024}, spp {1, 4, 16},
+    a camera on an orbit about the volume."""
     import numpy as np
     from barney_b200 import synth
     rng = np.random.default_rng(seed)
@@ -587,84 +597,53 @@ def request_stream(n, seed=7):
     return reqs
 
 
-def run_serving(args):
-    """Config 5: Poisson arrivals of render requests over 16 resident
-    volumes, served with continuous batching under a 150 GB HBM budget.
-    Served form: volumes stored as fp16 (majorants from the stored values,
-    rounded up), compensated accumulation.  Plain form: float32 volumes, one
-    bnRender per request, back to back."""
-    import threading
+def poisson_arrivals(n, rate, seed):
+    import numpy as np
+    return np.cumsum(np.random.default_rng(seed).exponential(1.0 / rate, n))
+
+
+def percentile(xs, q):
+    xs = sorted(xs)
+    return xs[min(len(xs) - 1, int(q * (len(xs) - 1) + 0.5))] if xs else None
+
+
+def serving_arms(n_sat, rates, n_rate, fast_math=True):
+    """Both forms of the serving workload on ONE request stream (seed 7):
+
+    served  f16 storage (majorants from the stored values, rounded up),
+            compensated accumulation (and the fast-math kernels if fast_math),
+            continuous batching by the render server under a 150 GB budget;
+    plain   the float32 volumes, exact kernels, one bnRender + read-back per
+            request, back to back.
+
+    Throughput: the first n_sat requests submitted at once (served) and
+    rendered back to back (plain).  Latency at each rate: the first n_rate
+    requests arriving as a Poisson process; the served arm is measured live,
+    the plain arm's latencies follow from its measured per-request service
+    times by the FIFO queue recursion (one request at a time, in arrival
+    order)."""
     import numpy as np
     import torch
     import barney_b200 as bn
+    from barney_b200 import synth
     torch.cuda.set_device(0)
-    rates = [float(x) for x in args.rates.split(",")]
-    ctx = bn.Context()
-    served = []
-    for d in serving_volumes(torch, "cuda", storage="f16"):
-        d["majorant_round_up"] = True
-        d["compensated_accum"] = True
-        served.append(bn.VolumeRenderer(d, context=ctx, color_format="rgba8"))
-    torch.cuda.empty_cache()
-    server = bn.Server(ctx, hbm_budget_bytes=150 << 30, max_slots=256, slice_waves=4)
-    server.reserve(8 << 30)  # request buffers taken before serving (peak use measured below 5 GB)
-    results = []
-    for rate in rates:
-        n = args.requests or max(200, min(10000, int(rate * 6)))
-        reqs = request_stream(n, seed=int(rate))
-        server.reset_stats()
-        ids = []
-        rng = np.random.default_rng(int(rate) + 1)
-
-        def producer():
-            t_next = time.perf_counter()
-            for v, side, spp, cam in reqs:
-                t_next += rng.exponential(1.0 / rate)
-                delay = t_next - time.perf_counter()
-                if delay > 0:
-                    time.sleep(delay)
-                ids.append(server.submit(served[v], cam, side, side, spp, "rgba8"))
-
-        th = threading.Thread(target=producer)
-        th.start()
-        th.join()
-        host = np.zeros((1024 * 1024,), np.uint32)
-        for rid in ids:
-            server.wait(rid, host)
-        st = server.stats()
-        results.append({"rate_req_s": rate, "requests": n, "frames_per_s": st["completed"] / st["wallSeconds"],
-                        "p50_ms": st["p50Ms"], "p99_ms": st["p99Ms"], "mean_ms": st["meanMs"],
-                        "queue_p99_ms": st["queueP99Ms"], "max_launch_ms": st["maxSliceMs"],
-                        "launches": st["launches"], "gpu_busy_frac": st["busySeconds"] / st["wallSeconds"],
-                        "Msamples_per_s": st["samples"] / st["wallSeconds"] / 1e6,
-                        "peak_request_bytes": st["peakBytes"]})
-        print(json.dumps({"partial": results[-1]}), flush=True)
-    server.close()
-    for r in served:
-        r.close()
-    ctx.close()
-    torch.cuda.empty_cache()
-    # plain FP32 path: the same kind of stream, one bnRender per request into a
-    # frame buffer of the request's size (allocated once per size and volume,
-    # as a plain-API client would), read back to host memory
-    import ctypes
+    n_all = max(n_sat, n_rate)
+    reqs = request_stream(n_all, seed=7)
+    vols = serving_volumes(torch, "cuda")
+    # plain arm first: float32 volumes, one frame buffer per (volume, size)
     ctx2 = bn.Context()
-    plain = [bn.VolumeRenderer(d, context=ctx2, color_format="rgba8") for d in serving_volumes(torch, "cuda", "f32")]
+    plain = [bn.VolumeRenderer(d, context=ctx2, color_format="rgba8") for d in vols]
     L = bn.lib()
     fbs = {}
-    for i, r in enumerate(plain):
+    for i in range(len(plain)):
         for side in (256, 512, 1024):
             fb = L.bnFrameBufferCreate(ctx2.ctx, 0)
             L.bnFrameBufferResize(fb, bn.BN_UFIXED8_RGBA, side, side, bn.BN_FB_COLOR)
             fbs[i, side] = fb
     bn.check()
-    reqs = request_stream(args.requests or 300, seed=99)
     host = np.zeros((1024 * 1024,), np.uint32)
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    service_ms = []
-    for v, side, spp, cam in reqs:
-        ts = time.perf_counter()
+
+    def plain_one(v, side, spp, cam):
         r = plain[v]
         r.set_camera(cam)
         r.set_spp(spp)
@@ -672,27 +651,106 @@ def run_serving(args):
         L.bnAccumReset(fb)
         L.bnRender(r.renderer, r.model, r.camera, fb)
         L.bnFrameBufferRead(fb, bn.BN_FB_COLOR, host.ctypes.data, bn.BN_UFIXED8_RGBA)
-        service_ms.append((time.perf_counter() - ts) * 1e3)
+        return r.stats()["samples"]
+
+    for q in reqs[:16]:  # warm-up: load the kernels
+        plain_one(*q)
+    torch.cuda.synchronize()
+    service, plain_samples = [], 0
+    t0 = time.perf_counter()
+    for q in reqs:
+        ts = time.perf_counter()
+        smp = plain_one(*q)
+        service.append(time.perf_counter() - ts)
+        if len(service) <= n_sat:
+            plain_samples += smp
+        if len(service) == n_sat:
+            plain_wall = time.perf_counter() - t0
     bn.check()
-    plain_fps = len(reqs) / (time.perf_counter() - t0)
-    service_ms.sort()
-    plain_service = {"p50_ms": service_ms[len(service_ms) // 2],
-                     "p99_ms": service_ms[min(len(service_ms) - 1, int(0.99 * (len(service_ms) - 1) + 0.5))],
-                     "max_ms": service_ms[-1]}
+    plain_fps = n_sat / plain_wall
     for r in plain:
         r.close()
     ctx2.close()
-    best = max(results, key=lambda x: x["frames_per_s"])
-    line = {"metric": METRIC, "value": best["frames_per_s"], "unit": "frames/s", "n_gpus": 1,
-            "steps": len(results), "warmup": 0, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
+    # served arm: f16 copies of the same volumes
+    ctx = bn.Context()
+    served = []
+    for d in vols:
+        ds = dict(d, voxels=synth.to_storage(d["voxels"], "f16"), dtype="f16", majorant_round_up=True,
+                  compensated_accum=True, fast_math=fast_math)
+        served.append(bn.VolumeRenderer(ds, context=ctx, color_format="rgba8"))
+    del vols
+    torch.cuda.empty_cache()
+    server = bn.Server(ctx, hbm_budget_bytes=150 << 30, max_slots=256, slice_waves=4,
+                       slice_pixel_waves=16 << 20)
+    server.reserve(8 << 30)
+
+    def serve(sub, arrivals):
+        server.reset_stats()
+        ids = []
+        t_start = time.perf_counter()
+        for (v, side, spp, cam), ta in zip(sub, arrivals):
+            delay = t_start + ta - time.perf_counter()
+            if delay > 0:
+                time.sleep(delay)
+            ids.append(server.submit(served[v], cam, side, side, spp, "rgba8"))
+        for rid in ids:
+            server.wait(rid, host)
+        return server.stats()
+
+    serve(reqs[:16], [0.0] * 16)  # warm-up
+    st = serve(reqs[:n_sat], [0.0] * n_sat)
+    sat = {"frames_per_s": st["completed"] / st["wallSeconds"],
+           "Msamples_per_s": st["samples"] / st["wallSeconds"] / 1e6, "requests": n_sat}
+    rate_rows = []
+    for rate in rates:
+        arr = poisson_arrivals(n_rate, rate, seed=int(rate) + 1)
+        st = serve(reqs[:n_rate], arr)
+        # the plain arm on the same arrivals: FIFO, its measured service times
+        free, lat = 0.0, []
+        for ta, sv in zip(arr, service[:n_rate]):
+            start = max(ta, free)
+            free = start + sv
+            lat.append((free - ta) * 1e3)
+        plain_span = max(free, float(arr[-1]))
+        rate_rows.append({"rate_req_s": rate, "requests": n_rate,
+                          "served": {"frames_per_s": st["completed"] / st["wallSeconds"],
+                                     "p50_ms": st["p50Ms"], "p99_ms": st["p99Ms"], "max_launch_ms": st["maxSliceMs"],
+                                     "gpu_busy_frac": st["busySeconds"] / st["wallSeconds"]},
+                          "plain": {"frames_per_s": n_rate / plain_span, "p50_ms": percentile(lat, 0.5),
+                                    "p99_ms": percentile(lat, 0.99)}})
+        print(json.dumps({"partial": rate_rows[-1]}), file=sys.stderr, flush=True)
+    server.close()
+    for r in served:
+        r.close()
+    ctx.close()
+    torch.cuda.empty_cache()
+    svc_ms = [x * 1e3 for x in service[:n_sat]]
+    return {"served_over_plain": sat["frames_per_s"] / plain_fps,
+            "served": sat,
+            "plain": {"frames_per_s": plain_fps, "Msamples_per_s": plain_samples / plain_wall / 1e6,
+                      "service_p50_ms": percentile(svc_ms, 0.5), "service_p99_ms": percentile(svc_ms, 0.99)},
+            "rates": rate_rows,
+            "stream": "one request stream (seed 7) for both arms: volume of 16, side {256,512,1024}, "
+                      "spp {1,4,16}, orbit camera",
+            "served_form": "f16 storage, majorants rounded up, compensated accumulation" +
+                           (", fast-math kernels" if fast_math else "") +
+                           ", continuous batching (4 waves and at most 16M pixel-waves per launch), 150 GB budget",
+            "plain_form": "f32 storage, exact kernels, one bnRender + read-back per request"}
+
+
+def run_serving(args):
+    """Config 5: the served and plain forms on one Poisson request stream over
+    16 resident volumes (10 000 requests per rate unless --requests)."""
+    rates = [float(x) for x in args.rates.split(",")]
+    n = args.requests or 10000
+    res = serving_arms(n_sat=min(n, 2000), rates=rates, n_rate=n)
+    line = {"metric": METRIC, "value": res["served"]["frames_per_s"], "unit": "frames/s", "n_gpus": 1,
+            "steps": len(rates), "warmup": 1, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f16 storage, f32 arithmetic", "data": "synthetic (16 seeded volumes)",
             "config": {"workload": "Poisson request stream over 16 resident volumes (seeds 100-115, edges "
                                    "log-U[128,1024]); side {256,512,1024}, spp {1,4,16}; HBM budget 150 GB",
-                       "served": "fp16 storage, majorants rounded up, compensated accumulation, continuous batching",
-                       "plain": "f32 storage, one bnRender per request"},
-            "rates": results, "plain_fp32_frames_per_s": plain_fps,
-            "plain_fp32_service_time": plain_service,
-            "served_over_plain": best["frames_per_s"] / plain_fps}
+                       "requests_per_rate": n, "rates": rates},
+            "serving": res, "served_over_plain": res["served_over_plain"]}
     print(json.dumps(line), flush=True)
     return 0
 

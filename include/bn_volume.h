@@ -442,6 +442,9 @@ typedef struct {
   size_t hbmBudgetBytes;  /* device memory for admitted requests' buffers */
   int maxSlots;           /* requests rendered together in one launch */
   int sliceWaves;         /* waves per request per launch */
+  long long slicePixelWaves; /* at most this many pixel-waves (pixels x waves) per launch,
+                                oldest requests first, others wait for the next launch; the
+                                oldest request always runs.  0: no limit */
 } BNXServerConfig;
 typedef struct {
   BNModel model;          /* a built model of the server's context */

@@ -13,14 +13,15 @@ from tests.helpers import assert_bitexact, oracle_render, small_blob_scene, smal
 pytestmark = pytest.mark.gpu
 
 
-def _setup(budget, slots, slice_waves):
+def _setup(budget, slots, slice_waves, slice_pixel_waves=0):
     import barney_b200 as bn
     ctx = bn.Context()
     scenes = [small_noise_scene(n=40, w=48, h=32), small_blob_scene(n=24, w=40, h=36),
               small_noise_scene(n=33, w=37, h=29, dtype="u8", phase="simple"),
               small_noise_scene(n=24, w=16, h=16, dtype="f16", compensated_accum=True)]
     rs = [bn.VolumeRenderer(d, context=ctx, color_format="float4") for d in scenes]
-    server = bn.Server(ctx, hbm_budget_bytes=budget, max_slots=slots, slice_waves=slice_waves)
+    server = bn.Server(ctx, hbm_budget_bytes=budget, max_slots=slots, slice_waves=slice_waves,
+                       slice_pixel_waves=slice_pixel_waves)
     return bn, ctx, scenes, rs, server
 
 
@@ -37,9 +38,12 @@ def _expected(scene, cam, w, h, spp):
     return oracle.resolve(acc, spp, comp=comp)
 
 
-@pytest.mark.parametrize("budget,slots,slice_waves", [(1 << 30, 8, 2), (60000, 4, 1), (1 << 30, 64, 16)])
-def test_mixed_requests_equal_solo_renders(budget, slots, slice_waves):
-    bn, ctx, scenes, rs, server = _setup(budget, slots, slice_waves)
+@pytest.mark.parametrize("budget,slots,slice_waves,slice_pixel_waves",
+                         [(1 << 30, 8, 2, 0), (60000, 4, 1, 0), (1 << 30, 64, 16, 0), (1 << 30, 64, 4, 3000)])
+def test_mixed_requests_equal_solo_renders(budget, slots, slice_waves, slice_pixel_waves):
+    """(the last setting caps a launch at 3000 pixel-waves: most requests wait
+    out some launches, and their frames are still exact)"""
+    bn, ctx, scenes, rs, server = _setup(budget, slots, slice_waves, slice_pixel_waves)
     try:
         rng = np.random.default_rng(5)
         reqs = []
