@@ -456,7 +456,7 @@ def run_ours(args):
     if world == 1 and args.config == "2" and not args.no_serving and d["spp"] == 64 and d["dtype"] == "f32" \
             and not d.get("max_volume_bounces") and not d.get("iso") and d.get("phase") != "simple":
         torch.cuda.empty_cache()
-        # the north star's comparison on one request stream, bounded for the
+        # served f16 vs plain f32 on one request stream, bounded for the
         # default run (--config 5 runs it at 10 000 requests per rate)
         serving = serving_arms(n_sat=400, rates=[200.0, 1000.0], n_rate=400)
         serving["reduced"] = "400 requests at saturation and per rate (the full sweep: bench.py --config 5)"
