@@ -1600,125 +1600,171 @@ __global__ void __launch_bounds__(kRenderMaxThreads, EXT >= 2 ? kRenderMinBlocks
 // ---------------------------------------------------------------------------
 // Regrouped render kernel (plain single-frame jobs)
 // ---------------------------------------------------------------------------
-// A CTA owns kWFSlots pixel slots.  A slot's whole state -- its pixel and
+// A CTA owns kAQSlots pixel slots.  A slot's whole state -- its pixel and
 // wave, the accumulator and the ray in flight -- lives in shared memory, so
-// any thread of the CTA can advance any slot.  The CTA works in rounds of
-// four phases; each phase first compacts the slots that need it into a list
-// (warp ballots), then all threads work through that list:
-//   service  collisions (shading, shadow-ray spawn) and ended rays
-//            (accumulation) -- renderLoop's A1 and A2;
-//   fetch    new pixels for idle slots (one chunk range per round) -- A3;
-//   prepare  primary-ray generation and ray set-up -- A4 and A5;
-//   trace    macrocell walk and Woodcock steps -- B1 and B2.  A lane whose
-//            ray needs service stores it and takes the next slot of the
-//            list; the phase ends after kWFTraceIters steps of the warp or
-//            when the list is used up, and rays still in flight carry over
-//            to the next round.
+// any thread of the CTA can advance any slot.  Every slot waits in one of
+// four ring queues in shared memory:
+//   idle   no pixel: the next pixels of the frame go to these slots;
+//   trace  a ray to be walked through the macrocells and Woodcock ranges;
+//   hit    a primary ray's collision, to be shaded;
+//   end    a primary ray that left the volume, or a shadow ray that reached
+//          the light or was occluded: accumulation.
+// Each warp runs on its own, with no barrier: it picks the queue with the
+// most work and takes up to 32 slots from it, one per lane.
+//   fetch, hit and end passes: the slots' service (renderLoop's A1-A3), then
+//          primary-ray generation (A4) and ray set-up (A5) where needed; each
+//          slot then joins the queue of its next step;
+//   trace pass: lanes step their rays (B1, B2); a lane whose ray needs
+//          service hands the slot to the hit or end queue and takes the next
+//          ray of the trace queue, until that queue is empty and fewer than
+//          kAQMinHeld lanes still hold rays while service work waits.
 // Each slot runs exactly the state machine of a renderLoop lane (plain
 // kernels: no isosurface, multi-scatter or principled volume), in the same
 // order per pixel, so frames and work counters are the same bit for bit;
 // only which thread executes a step changes.
-// 384 slots for 256 threads, 3 CTAs per SM; a trace phase may end early
-// below 16 busy lanes of 32 after 4 steps (the fastest of the settings
-// measured on the 512^3 workload; all are slower than the per-lane kernel)
-constexpr int kWFThreads = 256;
-constexpr int kWFSlots = 384;
-constexpr int kWFMinBlocks = 3;
-constexpr int kWFTraceIters = 64;
-constexpr int kWFMinActive = 16;
-constexpr int kWFMinIters = 4;
-constexpr unsigned kWFMaxRounds = 1u << 22;
+//
+// Queues: kAQRing cells per queue and two counters.  A producer reserves
+// cells with atomicAdd on tail and fills each with a compare-and-swap once
+// the cell is empty; a consumer reserves cells with a compare-and-swap on
+// head (never past tail) and empties each with an exchange once it is
+// filled.  A slot is in at most one queue, so a queue never holds more than
+// kAQSlots entries.  Every wait for a cell is bounded (kAQSpinCap); running
+// past the bound ends the launch with the iteration-cap error.
+constexpr int kAQThreads = 256;
+constexpr int kAQSlots = 384;
+constexpr int kAQRing = 512;  // cells per queue: a power of two >= kAQSlots
+constexpr int kAQMinBlocks = 3;
+constexpr int kAQMinHeld = 16;
+constexpr int kAQServeMin = 16;
+constexpr unsigned kAQSpinCap = 1u << 20;
+constexpr unsigned kAQIdleCap = 1u << 24;
+enum AQQueue : int { AQ_IDLE = 0, AQ_TRACE = 1, AQ_HIT = 2, AQ_END = 3 };
+constexpr int kAQDrop = 15;  // a slot left out of every queue (the frame's pixels are all taken)
 
-struct WFSlots {
-  float4 acc[kWFSlots];
-  float ox[kWFSlots], oy[kWFSlots], oz[kWFSlots];     // ray origin
-  float dx[kWFSlots], dy[kWFSlots], dz[kWFSlots];     // ray direction (zero components fixed up by the set-up)
-  float rayTMax[kWFSlots];
-  unsigned seedLo[kWFSlots], seedHi[kWFSlots];       // the ray's RNG seed
-  int meta[kWFSlots];                                 // bits 0-3 LanePhase, bit 4 shadow ray, bits 8-13 TraceState::bits
-  int ix[kWFSlots], iy[kWFSlots], k[kWFSlots];        // pixel and wave of the launch
-  float stx[kWFSlots], sty[kWFSlots], stz[kWFSlots];  // shadow-ray throughput
-  float mis[kWFSlots];                                // shadow-ray MIS weight
-  float hx[kWFSlots], hy[kWFSlots], hz[kWFSlots];     // TF colour at the collision
-  float ddaTMax[kWFSlots], rayT0[kWFSlots], ncb[kWFSlots];
-  float tnx[kWFSlots], tny[kWFSlots], tnz[kWFSlots];
-  float tsx[kWFSlots], tsy[kWFSlots], tsz[kWFSlots];
-  int cx[kWFSlots], cy[kWFSlots], cz[kWFSlots];
-  unsigned rngLo[kWFSlots], rngHi[kWFSlots];          // the Woodcock RNG
-  float t[kWFSlots], tUpper[kWFSlots], maj[kWFSlots];
-  unsigned steps[kWFSlots];
-  int list[kWFSlots];
-  int listCount, listHead, live;
-  int curChunk, curBase, curLeft, newChunk0, newChunks, exhausted, aborted;
+struct AQShared {
+  float4 acc[kAQSlots];
+  float ox[kAQSlots], oy[kAQSlots], oz[kAQSlots];   // ray origin
+  float dx[kAQSlots], dy[kAQSlots], dz[kAQSlots];   // ray direction (zero components fixed up by the set-up)
+  float rayTMax[kAQSlots];
+  unsigned seedLo[kAQSlots], seedHi[kAQSlots];      // the ray's RNG seed
+  int meta[kAQSlots];  // bits 0-3 LanePhase at the hand-off, bit 4 shadow ray, bits 8-13 TraceState::bits
+  int ix[kAQSlots], iy[kAQSlots], k[kAQSlots];       // pixel and wave of the launch
+  float fx[kAQSlots], fy[kAQSlots], fz[kAQSlots];    // TF colour at a primary hit; a shadow ray's fragment
+  float ddaTMax[kAQSlots], rayT0[kAQSlots], ncb[kAQSlots];
+  float tnx[kAQSlots], tny[kAQSlots], tnz[kAQSlots];
+  float tsx[kAQSlots], tsy[kAQSlots], tsz[kAQSlots];
+  int cx[kAQSlots], cy[kAQSlots], cz[kAQSlots];
+  unsigned rngLo[kAQSlots], rngHi[kAQSlots];         // the Woodcock RNG
+  float t[kAQSlots], tUpper[kAQSlots], maj[kAQSlots];
+  unsigned steps[kAQSlots];
+  unsigned cell[4][kAQRing];  // slot + 1, or 0 when empty
+  unsigned head[4], tail[4];
+  int live;       // slots holding a pixel
+  int exhausted;  // no pixel of the frame is left to take
+  int aborted;
+  int failed;     // a bounded wait ran out: every warp leaves
 };
 
 DEV uint64_t wfJoin(unsigned lo, unsigned hi) { return (uint64_t)lo | ((uint64_t)hi << 32); }
-DEV int wfPhase(int meta) { return meta & 15; }
+DEV unsigned aqLoad(const unsigned *p) { return *(const volatile unsigned *)p; }
+DEV int aqLoadI(const int *p) { return *(const volatile int *)p; }
 
-// The slots whose phase satisfies pred, in sh.list[0 .. sh.listCount).
-// Called by every thread of the CTA; sh.listCount must be 0 on entry, and the
-// list is complete after the caller's next __syncthreads.
-template <typename Pred>
-DEV void wfCompact(WFSlots &sh, Pred pred) {
+// Slot s joins queue q for every lane with put.  Called by all lanes of the
+// warp.  False (that lane) when the wait for an empty cell ran out.
+DEV bool aqPush(AQShared &sh, int q, bool put, int s) {
+  const unsigned FULL = 0xffffffffu;
   const int lane = threadIdx.x & 31;
-  for (int s0 = 0; s0 < kWFSlots; s0 += kWFThreads) {
-    const int s = s0 + threadIdx.x;
-    const bool in = s < kWFSlots && pred(wfPhase(sh.meta[s]));
-    const unsigned m = __ballot_sync(0xffffffffu, in);
-    int base = 0;
-    if (lane == 0 && m) base = atomicAdd(&sh.listCount, __popc(m));
-    base = __shfl_sync(0xffffffffu, base, 0);
-    if (in) sh.list[base + __popc(m & ((1u << lane) - 1u))] = s;
+  const unsigned m = __ballot_sync(FULL, put);
+  if (!m) return true;
+  const int leader = __ffs(m) - 1;
+  unsigned base = 0;
+  if (lane == leader) base = atomicAdd(&sh.tail[q], (unsigned)__popc(m));
+  base = __shfl_sync(FULL, base, leader);
+  if (!put) return true;
+  const unsigned c = (base + (unsigned)__popc(m & ((1u << lane) - 1u))) & (kAQRing - 1);
+  __threadfence_block();  // the slot's state is visible before its cell
+  for (unsigned spins = 0; atomicCAS(&sh.cell[q][c], 0u, (unsigned)s + 1u) != 0u;)
+    if (++spins > kAQSpinCap) return false;
+  return true;
+}
+
+// Lanes with want take one slot each from queue q, as many as it holds;
+// -1 for the others.  Called by all lanes of the warp.  ok turns false when
+// the wait for a filled cell ran out.
+DEV int aqPop(AQShared &sh, int q, bool want, bool &ok) {
+  const unsigned FULL = 0xffffffffu;
+  const int lane = threadIdx.x & 31;
+  const unsigned m = __ballot_sync(FULL, want);
+  if (!m) return -1;
+  int got = 0;
+  unsigned base = 0;
+  if (lane == 0) {
+    const int n = __popc(m);
+    unsigned h = aqLoad(&sh.head[q]);
+    for (int tries = 0; tries < 1024; tries++) {
+      const int avail = (int)(aqLoad(&sh.tail[q]) - h);
+      const int take = min(n, avail);
+      if (take <= 0) break;
+      const unsigned old = atomicCAS(&sh.head[q], h, h + (unsigned)take);
+      if (old == h) {
+        got = take;
+        base = h;
+        break;
+      }
+      h = old;
+    }
   }
+  got = __shfl_sync(FULL, got, 0);
+  base = __shfl_sync(FULL, base, 0);
+  const int r = __popc(m & ((1u << lane) - 1u));
+  if (!want || r >= got) return -1;
+  const unsigned c = (base + (unsigned)r) & (kAQRing - 1);
+  unsigned v = 0;
+  for (unsigned spins = 0; (v = atomicExch(&sh.cell[q][c], 0u)) == 0u;)
+    if (++spins > kAQSpinCap) {
+      ok = false;
+      return -1;
+    }
+  __threadfence_block();  // the slot's state is read after its cell
+  return (int)v - 1;
 }
 
-DEV void wfLoadTrace(const WFSlots &sh, int s, TraceState &ts) {
-  ts.org = f3(sh.ox[s], sh.oy[s], sh.oz[s]);
-  ts.dir = f3(sh.dx[s], sh.dy[s], sh.dz[s]);
-  ts.rayTMax = sh.rayTMax[s];
-  ts.ddaTMax = sh.ddaTMax[s];
-  ts.rayT0 = sh.rayT0[s];
-  ts.nextCellBegin = sh.ncb[s];
-  ts.tNext = f3(sh.tnx[s], sh.tny[s], sh.tnz[s]);
-  ts.tStep = f3(sh.tsx[s], sh.tsy[s], sh.tsz[s]);
-  ts.cx = sh.cx[s];
-  ts.cy = sh.cy[s];
-  ts.cz = sh.cz[s];
-  ts.bits = (sh.meta[s] >> 8) & 63;
-  ts.rng = wfJoin(sh.rngLo[s], sh.rngHi[s]);
-  ts.t = sh.t[s];
-  ts.tUpper = sh.tUpper[s];
-  ts.maj = sh.maj[s];
-}
-
-// bytes of dynamic shared memory: the slots, then the TF table
-__host__ __device__ inline size_t wfSlotsBytes() { return (sizeof(WFSlots) + 15) & ~(size_t)15; }
+// bytes of dynamic shared memory: the slots and queues, then the TF table
+__host__ __device__ inline size_t wfSlotsBytes() { return (sizeof(AQShared) + 15) & ~(size_t)15; }
 
 template <int T, int LOG>
-__global__ void __launch_bounds__(kWFThreads, kWFMinBlocks)
+__global__ void __launch_bounds__(kAQThreads, kAQMinBlocks)
     renderKernelWF(const __grid_constant__ JobDD job, LaunchCounters *ctr) {
   extern __shared__ __align__(16) unsigned char wfSmem[];
   __shared__ float u8lut[256];
-  WFSlots &sh = *reinterpret_cast<WFSlots *>(wfSmem);
+  AQShared &sh = *reinterpret_cast<AQShared *>(wfSmem);
   float4 *sTF = reinterpret_cast<float4 *>(wfSmem + wfSlotsBytes());
   const VolumeDD &v = job.v;
   const FrameDD &fr = job.fr;
   const int tid = threadIdx.x;
+  const int lane = tid & 31;
   const unsigned FULL = 0xffffffffu;
   for (int i = tid; i < v.tfN; i += blockDim.x) sTF[i] = v.tf[i];
   for (int i = tid; i < 256; i += blockDim.x) u8lut[i] = __fdiv_rn((float)i * 1.f, 255.f);
-  for (int s = tid; s < kWFSlots; s += blockDim.x) sh.meta[s] = LP_IDLE;
+  for (int i = tid; i < 4 * kAQRing; i += blockDim.x) (&sh.cell[0][0])[i] = 0u;
+  __syncthreads();
+  for (int s = tid; s < kAQSlots; s += blockDim.x) sh.cell[AQ_IDLE][s] = (unsigned)s + 1u;
+  if (tid < 4) {
+    sh.head[tid] = 0u;
+    sh.tail[tid] = tid == AQ_IDLE ? (unsigned)kAQSlots : 0u;
+  }
   if (tid == 0) {
-    sh.curChunk = 0;
-    sh.curBase = 0;
-    sh.curLeft = 0;
+    sh.live = 0;
     sh.exhausted = 0;
     sh.aborted = 0;
+    sh.failed = 0;
   }
+  __syncthreads();
   const int W = fr.width, H = fr.height;
   const int npix = W * H;
   const int frameChunks = (npix + kChunk - 1) / kChunk;
   const int numChunks = fr.partCount > 1 ? partitionChunks(frameChunks, fr.partRank, fr.partCount) : frameChunks;
+  const unsigned totalPix = (unsigned)numChunks * (unsigned)kChunk;  // pixel indices of this rank's chunks
   const bool cmp = fr.comp != nullptr;
   unsigned nSamples = 0, nVisits = 0, nRays = 0, errBits = 0;
   // this rank's chunk c -> the frame's chunk, and the pixels it holds
@@ -1726,365 +1772,91 @@ __global__ void __launch_bounds__(kWFThreads, kWFMinBlocks)
     return fr.partCount > 1 ? (c / kPartTileChunks * fr.partCount + fr.partRank) * kPartTileChunks + c % kPartTileChunks
                             : c;
   };
-  auto chunkPixels = [&](int c) { return c < numChunks ? min(kChunk, npix - frameChunk(c) * kChunk) : 0; };
+  auto chunkPixels = [&](int c) { return min(kChunk, npix - frameChunk(c) * kChunk); };
+  bool ok = true;
+  unsigned idlePolls = 0;
 
-  // every round steps every ray in flight at least once, so a frame ends in
-  // far fewer rounds than this bound; reaching it ends the launch with the
-  // iteration-cap error instead of running on
-  for (unsigned round = 0;; round++) {
-    if (round >= kWFMaxRounds) {
-      errBits |= ERR_ITER_CAP;
-      break;
-    }
+  while (true) {
     if ((nSamples | nVisits | nRays) >= 0x80000000u) {
       atomicAdd(&ctr->samples, (unsigned long long)nSamples);
       atomicAdd(&ctr->mcVisits, (unsigned long long)nVisits);
       atomicAdd(&ctr->rays, (unsigned long long)nRays);
       nSamples = nVisits = nRays = 0;
     }
-    // ---------------------------------------------------------------- service
-    if (tid == 0) sh.listCount = 0;
-    __syncthreads();
-    // collisions first, then ended rays: each warp runs mostly one of the two branches
-    wfCompact(sh, [](int p) { return p == LP_HIT; });
-    __syncthreads();
-    wfCompact(sh, [](int p) { return p == LP_ENDED; });
-    __syncthreads();
-    for (int j = tid; j < sh.listCount; j += kWFThreads) {
-      const int s = sh.list[j];
-      int meta = sh.meta[s];
-      const int phase = wfPhase(meta);
-      const bool shadowRay = (meta >> 4) & 1;
-      int kk = sh.k[s];
-      float4 acc = sh.acc[s];
-      const int accumID = fr.accumID0 + kk;
-      const float clampMax = 10.f * (1 + accumID);
-      const int64_t pix = (int64_t)sh.iy[s] * W + sh.ix[s];
-      float4 comp = make_float4(0.f, 0.f, 0.f, 0.f);
-      if (cmp && BNB_IN(pix, (long long)npix)) comp = fr.comp[pix];  // the scratch copy of this pixel's terms
-      bool spawned = false;
-      if (phase == LP_HIT) {
-        // A1 (shadeRays.cu:608-746)
-        if (!shadowRay) {
-          if (accumID == 0) {
-            acc = make_float4(0.f, 0.f, 0.f, 1.f);
-            comp = make_float4(0.f, 0.f, 0.f, 0.f);
-          } else {
-            accAdd(acc.w, comp.w, 1.f, cmp);
-          }
-          const float tHit = sh.t[s];
-          const float3 org = f3(sh.ox[s], sh.oy[s], sh.oz[s]);
-          const float3 dir = f3(sh.dx[s], sh.dy[s], sh.dz[s]);
-          const float3 P = f3(org.x + tHit * dir.x, org.y + tHit * dir.y, org.z + tHit * dir.z);
-          const float3 hitRGB = f3(sh.hx[s], sh.hy[s], sh.hz[s]);
-          if (fr.emissionAbsorption) {
-            const float ex = fmin_(hitRGB.x, clampMax), ey = fmin_(hitRGB.y, clampMax), ez = fmin_(hitRGB.z, clampMax);
-            if (accumID == 0) acc = make_float4(ex, ey, ez, 1.f);
-            else {
-              if (ex > 0.f) accAdd(acc.x, comp.x, ex, cmp);
-              if (ey > 0.f) accAdd(acc.y, comp.y, ey, cmp);
-              if (ez > 0.f) accAdd(acc.z, comp.z, ez, cmp);
-            }
-          } else {
-            uint64_t raySeed = wfJoin(sh.seedLo[s], sh.seedHi[s]);
-            uint64_t random = rngDerive(raySeed, (uint64_t)__float_as_uint(tHit));
-            const int bits = (meta >> 8) & 63;
-            const float3 won = normalize3(f3((bits & 8) ? 0.f : dir.x, (bits & 16) ? 0.f : dir.y, (bits & 32) ? 0.f : dir.z));
-            const float3 woN = f3(-won.x, -won.y, -won.z);
-            const float offsetEpsilon = fmax_(1e-4f, 1e-6f * fmax_(fmax_(fabsf(P.x), fabsf(P.y)), fabsf(P.z)));
-            LightSample ls;
-            bool needsMIS, isDir;
-            if (sampleLights(fr, random, ls, needsMIS, isDir)) {
-              float3 alb;
-              float fpdf;
-              if (v.phase == PHASE_SIMPLE) {
-                alb = f3(.7f * hitRGB.x, .7f * hitRGB.y, .7f * hitRGB.z);
-                fpdf = kOneOverFourPi;
-              } else {
-                const float a = v.scatteringAlbedo;
-                alb = f3(a * hitRGB.x, a * hitRGB.y, a * hitRGB.z);
-                const float3 wi_in = normalize3(f3(-woN.x, -woN.y, -woN.z));
-                fpdf = hgPhase(v.anisotropy, dot3(wi_in, normalize3(ls.dir)));
-              }
-              float3 fv = f3(fpdf * alb.x, fpdf * alb.y, fpdf * alb.z);
-              if (fpdf > 0.f && !(fmax_(fmax_(fv.x, fv.y), fv.z) < 1e-4f)) {
-                fv = f3(fmin_(fv.x, 13.f), fmin_(fv.y, 13.f), fmin_(fv.z, 13.f));
-                const float ip = isinf(ls.pdf) ? 1.f : (1.f / ls.pdf);
-                const float3 tp = f3(1.f * ip * fv.x * ls.radiance.x * 1.f, 1.f * ip * fv.y * ls.radiance.y * 1.f,
-                                     1.f * ip * fv.z * ls.radiance.z * 1.f);
-                float misWeight = 1.f;
-                bool alive = true;
-                if (!isDir && needsMIS) {
-                  const float pl = kOneOverFourPi;
-                  float ps;
-                  if (v.phase == PHASE_SIMPLE) ps = kOneOverFourPi;
-                  else ps = hgPhase(v.anisotropy, dot3(normalize3(f3(-woN.x, -woN.y, -woN.z)), normalize3(ls.dir)));
-                  misWeight = pl / (pl + ps + 1e-10f);
-                  if (misWeight < 1e-5f) alive = false;
-                }
-                const float sTMax = kInf * (1.f - 2.f * offsetEpsilon);
-                if (alive && sTMax > 0.f) {
-                  sh.stx[s] = roundHalf(tp.x);
-                  sh.sty[s] = roundHalf(tp.y);
-                  sh.stz[s] = roundHalf(tp.z);
-                  sh.mis[s] = misWeight;
-                  sh.ox[s] = P.x + offsetEpsilon * woN.x;
-                  sh.oy[s] = P.y + offsetEpsilon * woN.y;
-                  sh.oz[s] = P.z + offsetEpsilon * woN.z;
-                  sh.dx[s] = ls.dir.x;
-                  sh.dy[s] = ls.dir.y;
-                  sh.dz[s] = ls.dir.z;
-                  sh.rayTMax[s] = sTMax;
-                  meta = (meta & ~31) | LP_BEGIN | 16;
-                  spawned = true;
-                  nRays++;
-                  sh.steps[s] = 0;
-                }
-              }
-            }
-            sh.seedLo[s] = (unsigned)raySeed;
-            sh.seedHi[s] = (unsigned)(raySeed >> 32);
-          }
-        }
-      } else {
-        // A2 (shadeRays.cu:507-600, 996-1040)
-        if (!shadowRay) {
-          float4 bg = fr.bgColor;
-          if (!(fr.bgColor.w >= 0.f)) {
-            const float tt = (sh.iy[s] + .5f) / float(H);
-            bg = make_float4((1.0f - tt) * 0.9f + tt * 0.15f, (1.0f - tt) * 0.9f + tt * 0.25f,
-                             (1.0f - tt) * 0.9f + tt * .8f, (1.0f - tt) * 1.f + tt * 1.f);
-          }
-          const float f0x = fmin_(bg.x, clampMax), f0y = fmin_(bg.y, clampMax), f0z = fmin_(bg.z, clampMax);
-          if (accumID == 0) {
-            acc = make_float4(f0x, f0y, f0z, bg.w);
-            comp = make_float4(0.f, 0.f, 0.f, 0.f);
-          } else {
-            if (bg.w > 0.f) accAdd(acc.w, comp.w, bg.w, cmp);
-            if (f0x > 0.f) accAdd(acc.x, comp.x, f0x, cmp);
-            if (f0y > 0.f) accAdd(acc.y, comp.y, f0y, cmp);
-            if (f0z > 0.f) accAdd(acc.z, comp.z, f0z, cmp);
-          }
-        } else {
-          const float mw = sh.mis[s];
-          const float f1x = fmin_(mw * sh.stx[s], clampMax);
-          const float f1y = fmin_(mw * sh.sty[s], clampMax);
-          const float f1z = fmin_(mw * sh.stz[s], clampMax);
-          if (f1x > 0.f) accAdd(acc.x, comp.x, f1x, cmp);
-          if (f1y > 0.f) accAdd(acc.y, comp.y, f1y, cmp);
-          if (f1z > 0.f) accAdd(acc.z, comp.z, f1z, cmp);
-        }
-      }
-      if (!spawned) {
-        if (++kk == fr.spp) {
-          if (BNB_IN(pix, (long long)npix)) fr.accum[pix] = acc;
-          meta = (meta & ~15) | LP_IDLE;
-        } else {
-          meta = (meta & ~15) | LP_NEWSAMPLE;
-        }
-      }
-      if (cmp && BNB_IN(pix, (long long)npix)) fr.comp[pix] = comp;
-      sh.acc[s] = acc;
-      sh.k[s] = kk;
-      sh.meta[s] = meta;
+    // the queue to work on: a full warp of service work first, then rays
+    int pend[4] = {0, 0, 0, 0};
+    int exhausted = 0, live = 0, failed = 0;
+    if (lane == 0) {
+      for (int q = 0; q < 4; q++) pend[q] = (int)(aqLoad(&sh.tail[q]) - aqLoad(&sh.head[q]));
+      exhausted = aqLoadI(&sh.exhausted);
+      __threadfence_block();
+      live = aqLoadI(&sh.live);
+      failed = aqLoadI(&sh.failed);
     }
-    // ---------------------------------------------------------------- fetch
-    __syncthreads();
-    if (tid == 0) sh.listCount = 0;
-    __syncthreads();
-    wfCompact(sh, [](int p) { return p == LP_IDLE; });
-    __syncthreads();
-    if (tid == 0) {
-      const int n = sh.listCount;
-      int nNew = 0;
-      if (n > sh.curLeft && !sh.exhausted) {
-        nNew = (n - sh.curLeft + kChunk - 1) / kChunk;
-        sh.newChunk0 = (int)atomicAdd(&ctr->nextPixel, (unsigned)nNew);
-        if (*(volatile unsigned *)&ctr->abort) {
-          sh.aborted = 1;
-          sh.exhausted = 1;
-          nNew = 0;
-        }
+    for (int q = 0; q < 4; q++) pend[q] = __shfl_sync(FULL, pend[q], 0);
+    exhausted = __shfl_sync(FULL, exhausted, 0);
+    live = __shfl_sync(FULL, live, 0);
+    failed = __shfl_sync(FULL, failed, 0);
+    if (failed) break;
+    if (exhausted) pend[AQ_IDLE] = 0;
+    // a full warp of service work first, then rays
+    int q = -1;
+    if (pend[AQ_HIT] >= 32) q = AQ_HIT;
+    else if (pend[AQ_END] >= 32) q = AQ_END;
+    else if (pend[AQ_IDLE] >= 32) q = AQ_IDLE;
+    else if (pend[AQ_TRACE] > 0) q = AQ_TRACE;
+    else if (pend[AQ_HIT] > 0) q = AQ_HIT;
+    else if (pend[AQ_END] > 0) q = AQ_END;
+    else if (pend[AQ_IDLE] > 0) q = AQ_IDLE;
+    if (q < 0) {
+      if (exhausted && live == 0) break;  // the frame is done
+      if (++idlePolls > kAQIdleCap) {
+        errBits |= ERR_ITER_CAP;
+        if (lane == 0) atomicExch(&sh.failed, 1);
+        break;
       }
-      sh.newChunks = nNew;
+      __nanosleep(128);
+      continue;
     }
-    __syncthreads();
-    {
-      const int n = sh.listCount, left = sh.curLeft, nNew = sh.newChunks, c0 = sh.newChunk0;
-      const bool aborted = sh.aborted;
-      for (int j = tid; j < n; j += kWFThreads) {
-        int c = -1, w = 0;
-        if (j < left) {
-          c = sh.curChunk;
-          w = sh.curBase + j;
-        } else if (!aborted) {
-          const int jj = j - left, i = jj / kChunk, o = jj % kChunk;
-          if (i < nNew && o < chunkPixels(c0 + i)) {
-            c = c0 + i;
-            w = o;
-          }
-        }
-        if (c < 0) continue;  // no pixel for this slot this round
-        const int s = sh.list[j];
-        // pixel order: 4-row bands, column-major inside a band (8x4 tiles per 32 pixels)
-        const int wf = frameChunk(c) * kChunk + w;
-        const int band = wf / (4 * W);
-        const int rows = min(4, H - 4 * band);
-        const int within = wf - band * 4 * W;
-        const int px = within / rows, py = 4 * band + within % rows;
-        const int64_t pix = (int64_t)py * W + px;
-        const bool pixIn = BNB_IN(pix, (long long)npix);
-        sh.ix[s] = px;
-        sh.iy[s] = py;
-        sh.k[s] = 0;
-        sh.acc[s] = (fr.accumID0 > 0 && pixIn) ? fr.accum[pix] : make_float4(0.f, 0.f, 0.f, 0.f);
-        if (cmp && pixIn && fr.accumID0 == 0) fr.comp[pix] = make_float4(0.f, 0.f, 0.f, 0.f);
-        sh.meta[s] = LP_NEWSAMPLE;
-      }
-    }
-    __syncthreads();
-    if (tid == 0) {
-      const int n = sh.listCount;
-      if (sh.newChunks > 0) {
-        const int last = sh.newChunk0 + sh.newChunks - 1;
-        const int used = n - sh.curLeft - kChunk * (sh.newChunks - 1);
-        if (last < numChunks) {
-          sh.curChunk = last;
-          sh.curBase = used;
-          sh.curLeft = max(0, chunkPixels(last) - used);
-        } else {
-          sh.curLeft = 0;
-        }
-        if (sh.newChunk0 + sh.newChunks >= numChunks) sh.exhausted = 1;
-      } else if (!sh.aborted) {
-        const int took = min(n, sh.curLeft);
-        sh.curBase += took;
-        sh.curLeft -= took;
-      }
-      sh.listCount = 0;
-      sh.live = 0;
-    }
-    __syncthreads();
-    // ---------------------------------------------------------------- prepare
-    wfCompact(sh, [](int p) { return p == LP_NEWSAMPLE; });  // new primary rays first, then shadow rays
-    __syncthreads();
-    wfCompact(sh, [](int p) { return p == LP_BEGIN; });
-    __syncthreads();
-    for (int j = tid; j < sh.listCount; j += kWFThreads) {
-      const int s = sh.list[j];
-      int meta = sh.meta[s];
-      float3 org, dir;
-      float tMax;
-      uint64_t raySeed;
-      if (wfPhase(meta) == LP_NEWSAMPLE) {
-        // A4 (generateRays.cu:71-243)
-        const int px = sh.ix[s], py = sh.iy[s];
-        const int accumID = fr.accumID0 + sh.k[s];
-        const unsigned uAcc = (unsigned)accumID;
-        uint64_t rnd = rngSeed2((unsigned)px + (unsigned)W * uAcc, (unsigned)py + (unsigned)H * uAcc);
-        raySeed = rngSeed2((unsigned)px + uAcc * (unsigned)W, (uint32_t)py);
-        const float pixel_u = (accumID == 0) ? .5f : rngFloat(rnd);
-        const float pixel_v = (accumID == 0) ? .5f : rngFloat(rnd);
-        const float image_u = ((px + pixel_u) / float(W));
-        const float image_v = ((py + pixel_v) / float(H));
-        const float aspect = W / float(H);
-        const float su = 1.f * aspect * (image_u - .5f), sv = 1.f * (image_v - .5f);
-        float3 d = f3(fr.dir00.x + su * fr.dirdu.x + sv * fr.dirdv.x, fr.dir00.y + su * fr.dirdu.y + sv * fr.dirdv.y,
-                      fr.dir00.z + su * fr.dirdu.z + sv * fr.dirdv.z);
-        d = normalize3(d);
-        float3 o = fr.lens00;
-        tMax = 1e30f;
-        if (fr.cutPlane.w > -1e28f) {
-          const float3 N = f3(fr.cutPlane.x, fr.cutPlane.y, fr.cutPlane.z);
-          const float dist_org = dot3(N, o) + fr.cutPlane.w;
-          const float denom = dot3(N, d);
-          if (dist_org >= 0.f) {
-            if (denom < 0.f) tMax = fmin_(tMax, -dist_org / denom);
-          } else {
-            if (denom > 0.f) {
-              const float te = -dist_org / denom;
-              o = f3(o.x + te * d.x, o.y + te * d.y, o.z + te * d.z);
-            } else tMax = 0.f;
-          }
-        }
-        meta &= ~16;  // a primary ray
-        nRays++;
-        sh.steps[s] = 0;
-        org = o;
-        dir = d;
-      } else {
-        org = f3(sh.ox[s], sh.oy[s], sh.oz[s]);
-        dir = f3(sh.dx[s], sh.dy[s], sh.dz[s]);
-        tMax = sh.rayTMax[s];
-        raySeed = wfJoin(sh.seedLo[s], sh.seedHi[s]);
-      }
-      // A5: TraceRays::run fix-up, isProg prologue, dda3 set-up
-      TraceState ts;
-      const bool inside = traceBegin(v, ts, org, dir, tMax, raySeed);
-      sh.ox[s] = ts.org.x;
-      sh.oy[s] = ts.org.y;
-      sh.oz[s] = ts.org.z;
-      sh.dx[s] = ts.dir.x;
-      sh.dy[s] = ts.dir.y;
-      sh.dz[s] = ts.dir.z;
-      sh.rayTMax[s] = ts.rayTMax;
-      sh.seedLo[s] = (unsigned)raySeed;
-      sh.seedHi[s] = (unsigned)(raySeed >> 32);
-      if (inside) {
-        sh.ddaTMax[s] = ts.ddaTMax;
-        sh.rayT0[s] = ts.rayT0;
-        sh.ncb[s] = ts.nextCellBegin;
-        sh.tnx[s] = ts.tNext.x;
-        sh.tny[s] = ts.tNext.y;
-        sh.tnz[s] = ts.tNext.z;
-        sh.tsx[s] = ts.tStep.x;
-        sh.tsy[s] = ts.tStep.y;
-        sh.tsz[s] = ts.tStep.z;
-        sh.cx[s] = ts.cx;
-        sh.cy[s] = ts.cy;
-        sh.cz[s] = ts.cz;
-        sh.rngLo[s] = (unsigned)ts.rng;
-        sh.rngHi[s] = (unsigned)(ts.rng >> 32);
-        meta = (meta & ~(15 | (63 << 8))) | LP_CELL | (ts.bits << 8);
-      } else {
-        // rays that miss keep only their fix-up bits (none are read at a miss)
-        meta = (meta & ~15) | LP_ENDED;
-      }
-      sh.meta[s] = meta;
-    }
-    __syncthreads();
-    // ---------------------------------------------------------------- trace
-    if (tid == 0) {
-      sh.listCount = 0;
-      sh.listHead = 0;
-    }
-    __syncthreads();
-    wfCompact(sh, [](int p) { return p == LP_CELL || p == LP_WOODCOCK; });
-    __syncthreads();
-    {
-      const int lane = tid & 31;
-      const int n = sh.listCount;
-      int s = -1;
-      int phase = LP_IDLE, meta = 0;
+    idlePolls = 0;
+
+    if (q == AQ_TRACE) {
+      // ---------------------------------------------------------------- trace
+      int s = -1, phase = LP_IDLE, meta = 0;
       unsigned steps = 0;
       TraceState ts;
-      for (int it = 0; it < kWFTraceIters; it++) {
-        // lanes without a ray take the next slots of the list
-        const unsigned need = __ballot_sync(FULL, s < 0);
-        if (need) {
-          int base = 0;
-          if (lane == 0) base = atomicAdd(&sh.listHead, __popc(need));
-          base = __shfl_sync(FULL, base, 0);
-          const int r = base + __popc(need & ((1u << lane) - 1u));
-          if (s < 0 && r < n) {
-            s = sh.list[r];
-            meta = sh.meta[s];
-            phase = wfPhase(meta);
-            steps = sh.steps[s];
-            wfLoadTrace(sh, s, ts);
+      while (true) {
+        const bool need = s < 0;
+        if (__any_sync(FULL, need)) {
+          int avail = 0;
+          if (lane == 0) avail = (int)(aqLoad(&sh.tail[AQ_TRACE]) - aqLoad(&sh.head[AQ_TRACE]));
+          if (__shfl_sync(FULL, avail, 0) > 0) {
+            const int ns = aqPop(sh, AQ_TRACE, need, ok);
+            if (ns >= 0) {
+              s = ns;
+              meta = sh.meta[s];
+              phase = meta & 15;
+              steps = sh.steps[s];
+              ts.org = f3(sh.ox[s], sh.oy[s], sh.oz[s]);
+              ts.dir = f3(sh.dx[s], sh.dy[s], sh.dz[s]);
+              ts.rayTMax = sh.rayTMax[s];
+              ts.ddaTMax = sh.ddaTMax[s];
+              ts.rayT0 = sh.rayT0[s];
+              ts.nextCellBegin = sh.ncb[s];
+              ts.tNext = f3(sh.tnx[s], sh.tny[s], sh.tnz[s]);
+              ts.tStep = f3(sh.tsx[s], sh.tsy[s], sh.tsz[s]);
+              ts.cx = sh.cx[s];
+              ts.cy = sh.cy[s];
+              ts.cz = sh.cz[s];
+              ts.bits = (meta >> 8) & 63;
+              ts.rng = wfJoin(sh.rngLo[s], sh.rngHi[s]);
+              ts.t = sh.t[s];
+              ts.tUpper = sh.tUpper[s];
+              ts.maj = sh.maj[s];
+            }
           }
         }
-        if (!__ballot_sync(FULL, s >= 0)) break;  // the list is used up
+        if (!__any_sync(FULL, s >= 0)) break;
         if (s >= 0) {
           // B1 (DDA.h:172-200, MCAccelerator.h:596-612)
           if (phase == LP_CELL) {
@@ -2126,14 +1898,16 @@ __global__ void __launch_bounds__(kWFThreads, kWFMinBlocks)
                 w = __fmul_rn(lerp_l(f, sTF[idx].w, sTF[idx + 1].w), v.baseDensity);
               }
               if (w >= rngFloat(ts.rng) * ts.maj) {
-                float3 hit = f3(0.f, 0.f, 0.f);
-                if (!isnan(smp)) {
-                  const float4 a = sTF[idx], b = sTF[idx + 1];
-                  hit = f3(lerp_l(f, a.x, b.x), lerp_l(f, a.y, b.y), lerp_l(f, a.z, b.z));
+                if (!(meta & 16)) {  // a primary ray's collision keeps its TF colour for the shading
+                  float3 hit = f3(0.f, 0.f, 0.f);
+                  if (!isnan(smp)) {
+                    const float4 a = sTF[idx], b = sTF[idx + 1];
+                    hit = f3(lerp_l(f, a.x, b.x), lerp_l(f, a.y, b.y), lerp_l(f, a.z, b.z));
+                  }
+                  sh.fx[s] = hit.x;
+                  sh.fy[s] = hit.y;
+                  sh.fz[s] = hit.z;
                 }
-                sh.hx[s] = hit.x;
-                sh.hy[s] = hit.y;
-                sh.hz[s] = hit.z;
                 phase = LP_HIT;
               }
             }
@@ -2142,48 +1916,336 @@ __global__ void __launch_bounds__(kWFThreads, kWFMinBlocks)
               phase = LP_ENDED;
             }
           }
-          if (phase != LP_CELL && phase != LP_WOODCOCK) {  // the ray needs service: store it, take another
-            sh.t[s] = ts.t;
-            sh.meta[s] = (meta & ~15) | phase;
-            sh.steps[s] = steps;
-            s = -1;
+        }
+        // rays that need service go to the hit (a primary ray's collision)
+        // or end queue (everything else)
+        const bool fin = s >= 0 && phase != LP_CELL && phase != LP_WOODCOCK;
+        const bool toHit = fin && phase == LP_HIT && !(meta & 16);
+        if (fin) {
+          sh.t[s] = ts.t;
+          sh.meta[s] = (meta & ~15) | phase;
+        }
+        ok &= aqPush(sh, AQ_HIT, toHit, s);
+        ok &= aqPush(sh, AQ_END, fin && !toHit, s);
+        if (fin) s = -1;
+        // under kAQMinHeld busy lanes with the trace queue empty and service
+        // work waiting, the rays in hand go back to the trace queue
+        const int held = __popc(__ballot_sync(FULL, s >= 0));
+        if (held == 0 || held >= kAQMinHeld) continue;
+        int tAvail = 0, sAvail = 0;
+        if (lane == 0) {
+          tAvail = (int)(aqLoad(&sh.tail[AQ_TRACE]) - aqLoad(&sh.head[AQ_TRACE]));
+          sAvail = (int)(aqLoad(&sh.tail[AQ_HIT]) - aqLoad(&sh.head[AQ_HIT])) +
+                   (int)(aqLoad(&sh.tail[AQ_END]) - aqLoad(&sh.head[AQ_END]));
+          if (!aqLoadI(&sh.exhausted)) sAvail += (int)(aqLoad(&sh.tail[AQ_IDLE]) - aqLoad(&sh.head[AQ_IDLE]));
+        }
+        tAvail = __shfl_sync(FULL, tAvail, 0);
+        sAvail = __shfl_sync(FULL, sAvail, 0);
+        if (tAvail > 0 || sAvail < kAQServeMin) continue;
+        if (s >= 0) {
+          sh.ncb[s] = ts.nextCellBegin;
+          sh.tnx[s] = ts.tNext.x;
+          sh.tny[s] = ts.tNext.y;
+          sh.tnz[s] = ts.tNext.z;
+          sh.cx[s] = ts.cx;
+          sh.cy[s] = ts.cy;
+          sh.cz[s] = ts.cz;
+          sh.rngLo[s] = (unsigned)ts.rng;
+          sh.rngHi[s] = (unsigned)(ts.rng >> 32);
+          sh.t[s] = ts.t;
+          sh.tUpper[s] = ts.tUpper;
+          sh.maj[s] = ts.maj;
+          sh.steps[s] = steps;
+          sh.meta[s] = (meta & ~15) | phase;
+        }
+        ok &= aqPush(sh, AQ_TRACE, s >= 0, s);
+        break;
+      }
+    } else {
+      // ---------------------------------------------------------- fetch / hit / end
+      int s = aqPop(sh, q, true, ok);
+      int phase = kAQDrop;  // where the slot goes after this pass
+      int meta = 0, kk = 0, px = 0, py = 0;
+      float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
+      float4 comp = make_float4(0.f, 0.f, 0.f, 0.f);
+      int64_t pix = 0;
+      uint64_t raySeed = 0;
+      float3 org = f3(0.f, 0.f, 0.f), dir = f3(0.f, 0.f, 0.f);
+      float tMax = 0.f;
+      bool dirty = false;  // acc / k changed
+      if (q == AQ_IDLE) {
+        // A3: the next pixels of this rank's chunks, in chunk order
+        // the slots count as live before they take pixels, so that no warp
+        // sees the frame exhausted with none live while these are assigned
+        const unsigned m = __ballot_sync(FULL, s >= 0);
+        unsigned base = 0;
+        int ab = 0;
+        if (lane == 0 && m) {
+          atomicAdd(&sh.live, __popc(m));
+          __threadfence_block();
+          base = atomicAdd(&ctr->nextPixel, (unsigned)__popc(m));
+          ab = (int)*(volatile unsigned *)&ctr->abort;
+        }
+        base = __shfl_sync(FULL, base, 0);
+        ab = __shfl_sync(FULL, ab, 0);
+        bool ends = false;
+        if (s >= 0) {
+          const unsigned p = base + (unsigned)__popc(m & ((1u << lane) - 1u));
+          if (ab || p >= totalPix) {
+            ends = true;  // nothing left for this slot: it stays out of every queue
+          } else {
+            const int c = (int)(p / kChunk), o = (int)(p % kChunk);
+            if (o >= chunkPixels(c)) {
+              phase = LP_IDLE;  // past the frame's last pixel: back to the idle queue
+            } else {
+              // pixel order: 4-row bands, column-major inside a band (8x4 tiles per 32 pixels)
+              const int wf = frameChunk(c) * kChunk + o;
+              const int band = wf / (4 * W);
+              const int rows = min(4, H - 4 * band);
+              const int within = wf - band * 4 * W;
+              px = within / rows;
+              py = 4 * band + within % rows;
+              pix = (int64_t)py * W + px;
+              const bool pixIn = BNB_IN(pix, (long long)npix);
+              kk = 0;
+              acc = (fr.accumID0 > 0 && pixIn) ? fr.accum[pix] : make_float4(0.f, 0.f, 0.f, 0.f);
+              if (cmp && pixIn && fr.accumID0 == 0) fr.comp[pix] = make_float4(0.f, 0.f, 0.f, 0.f);
+              sh.ix[s] = px;
+              sh.iy[s] = py;
+              dirty = true;
+              phase = LP_NEWSAMPLE;
+            }
           }
         }
-        // after kWFMinIters steps of every ray it holds: once the list is used
-        // up and the warp runs under three quarters full, its rays carry over
-        // to the next round instead of holding the CTA at the barrier.  (Every
-        // slot of the list has been taken and stepped by then.)
-        if (it + 1 >= kWFMinIters && __popc(__ballot_sync(FULL, s >= 0)) < kWFMinActive &&
-            *(volatile int *)&sh.listHead >= n)
-          break;
+        const unsigned noPix = __ballot_sync(FULL, s >= 0 && phase != LP_NEWSAMPLE);
+        const unsigned ended = __ballot_sync(FULL, ends);
+        if (lane == 0) {
+          if (ab) atomicExch(&sh.aborted, 1);
+          if (ended) atomicExch(&sh.exhausted, 1);
+          __threadfence_block();
+          if (noPix) atomicSub(&sh.live, __popc(noPix));
+        }
+      } else if (s >= 0) {
+        meta = sh.meta[s];
+        kk = sh.k[s];
+        acc = sh.acc[s];
+        px = sh.ix[s];
+        py = sh.iy[s];
+        pix = (int64_t)py * W + px;
+        if (cmp && BNB_IN(pix, (long long)npix)) comp = fr.comp[pix];
+        const bool shadowRay = (meta >> 4) & 1;
+        const int accumID = fr.accumID0 + kk;
+        const float clampMax = 10.f * (1 + accumID);
+        dirty = true;
+        bool spawned = false;
+        if (q == AQ_HIT) {
+          // A1 (shadeRays.cu:608-746): a primary ray's collision
+          if (accumID == 0) {
+            acc = make_float4(0.f, 0.f, 0.f, 1.f);
+            comp = make_float4(0.f, 0.f, 0.f, 0.f);
+          } else {
+            accAdd(acc.w, comp.w, 1.f, cmp);
+          }
+          const float tHit = sh.t[s];
+          const float3 o0 = f3(sh.ox[s], sh.oy[s], sh.oz[s]);
+          const float3 d0 = f3(sh.dx[s], sh.dy[s], sh.dz[s]);
+          const float3 P = f3(o0.x + tHit * d0.x, o0.y + tHit * d0.y, o0.z + tHit * d0.z);
+          const float3 hitRGB = f3(sh.fx[s], sh.fy[s], sh.fz[s]);
+          raySeed = wfJoin(sh.seedLo[s], sh.seedHi[s]);
+          if (fr.emissionAbsorption) {
+            const float ex = fmin_(hitRGB.x, clampMax), ey = fmin_(hitRGB.y, clampMax), ez = fmin_(hitRGB.z, clampMax);
+            if (accumID == 0) acc = make_float4(ex, ey, ez, 1.f);
+            else {
+              if (ex > 0.f) accAdd(acc.x, comp.x, ex, cmp);
+              if (ey > 0.f) accAdd(acc.y, comp.y, ey, cmp);
+              if (ez > 0.f) accAdd(acc.z, comp.z, ez, cmp);
+            }
+          } else {
+            uint64_t random = rngDerive(raySeed, (uint64_t)__float_as_uint(tHit));
+            const int bits = (meta >> 8) & 63;
+            const float3 won = normalize3(f3((bits & 8) ? 0.f : d0.x, (bits & 16) ? 0.f : d0.y, (bits & 32) ? 0.f : d0.z));
+            const float3 woN = f3(-won.x, -won.y, -won.z);
+            const float offsetEpsilon = fmax_(1e-4f, 1e-6f * fmax_(fmax_(fabsf(P.x), fabsf(P.y)), fabsf(P.z)));
+            LightSample ls;
+            bool needsMIS, isDir;
+            if (sampleLights(fr, random, ls, needsMIS, isDir)) {
+              float3 alb;
+              float fpdf;
+              if (v.phase == PHASE_SIMPLE) {
+                alb = f3(.7f * hitRGB.x, .7f * hitRGB.y, .7f * hitRGB.z);
+                fpdf = kOneOverFourPi;
+              } else {
+                const float a = v.scatteringAlbedo;
+                alb = f3(a * hitRGB.x, a * hitRGB.y, a * hitRGB.z);
+                const float3 wi_in = normalize3(f3(-woN.x, -woN.y, -woN.z));
+                fpdf = hgPhase(v.anisotropy, dot3(wi_in, normalize3(ls.dir)));
+              }
+              float3 fv = f3(fpdf * alb.x, fpdf * alb.y, fpdf * alb.z);
+              if (fpdf > 0.f && !(fmax_(fmax_(fv.x, fv.y), fv.z) < 1e-4f)) {
+                fv = f3(fmin_(fv.x, 13.f), fmin_(fv.y, 13.f), fmin_(fv.z, 13.f));
+                const float ip = isinf(ls.pdf) ? 1.f : (1.f / ls.pdf);
+                const float3 tp = f3(1.f * ip * fv.x * ls.radiance.x * 1.f, 1.f * ip * fv.y * ls.radiance.y * 1.f,
+                                     1.f * ip * fv.z * ls.radiance.z * 1.f);
+                float misWeight = 1.f;
+                bool alive = true;
+                if (!isDir && needsMIS) {
+                  // the light sample's phase pdf is fpdf (the same expression)
+                  misWeight = kOneOverFourPi / (kOneOverFourPi + fpdf + 1e-10f);
+                  if (misWeight < 1e-5f) alive = false;
+                }
+                const float sTMax = kInf * (1.f - 2.f * offsetEpsilon);
+                if (alive && sTMax > 0.f) {
+                  // the fragment the shadow ray adds if it reaches the light
+                  sh.fx[s] = fmin_(misWeight * roundHalf(tp.x), clampMax);
+                  sh.fy[s] = fmin_(misWeight * roundHalf(tp.y), clampMax);
+                  sh.fz[s] = fmin_(misWeight * roundHalf(tp.z), clampMax);
+                  // makeShadowRay (Ray.h:147-157)
+                  org = f3(P.x + offsetEpsilon * woN.x, P.y + offsetEpsilon * woN.y, P.z + offsetEpsilon * woN.z);
+                  dir = ls.dir;
+                  tMax = sTMax;
+                  meta |= 16;
+                  spawned = true;
+                  nRays++;
+                  phase = LP_BEGIN;
+                }
+              }
+            }
+          }
+        } else {
+          // A2 (shadeRays.cu:507-600, 996-1040): a ray that ended
+          const int endPhase = meta & 15;
+          if (!shadowRay) {
+            float4 bg = fr.bgColor;
+            if (!(fr.bgColor.w >= 0.f)) {
+              const float tt = (py + .5f) / float(H);
+              bg = make_float4((1.0f - tt) * 0.9f + tt * 0.15f, (1.0f - tt) * 0.9f + tt * 0.25f,
+                               (1.0f - tt) * 0.9f + tt * .8f, (1.0f - tt) * 1.f + tt * 1.f);
+            }
+            const float f0x = fmin_(bg.x, clampMax), f0y = fmin_(bg.y, clampMax), f0z = fmin_(bg.z, clampMax);
+            if (accumID == 0) {
+              acc = make_float4(f0x, f0y, f0z, bg.w);
+              comp = make_float4(0.f, 0.f, 0.f, 0.f);
+            } else {
+              if (bg.w > 0.f) accAdd(acc.w, comp.w, bg.w, cmp);
+              if (f0x > 0.f) accAdd(acc.x, comp.x, f0x, cmp);
+              if (f0y > 0.f) accAdd(acc.y, comp.y, f0y, cmp);
+              if (f0z > 0.f) accAdd(acc.z, comp.z, f0z, cmp);
+            }
+          } else if (endPhase == LP_ENDED) {  // the shadow ray reached the light
+            const float f1x = sh.fx[s], f1y = sh.fy[s], f1z = sh.fz[s];
+            if (f1x > 0.f) accAdd(acc.x, comp.x, f1x, cmp);
+            if (f1y > 0.f) accAdd(acc.y, comp.y, f1y, cmp);
+            if (f1z > 0.f) accAdd(acc.z, comp.z, f1z, cmp);
+          }
+          // an occluded shadow ray adds nothing
+        }
+        if (!spawned) {
+          if (++kk == fr.spp) {  // the pixel's last wave
+            if (BNB_IN(pix, (long long)npix)) {
+              fr.accum[pix] = acc;
+              if (cmp) fr.comp[pix] = comp;
+            }
+            phase = LP_IDLE;
+          } else {
+            phase = LP_NEWSAMPLE;
+          }
+        }
+        if (cmp && phase != LP_IDLE && BNB_IN(pix, (long long)npix)) fr.comp[pix] = comp;
       }
-      if (s >= 0) {  // carries over to the next round
-        sh.ncb[s] = ts.nextCellBegin;
-        sh.tnx[s] = ts.tNext.x;
-        sh.tny[s] = ts.tNext.y;
-        sh.tnz[s] = ts.tNext.z;
-        sh.cx[s] = ts.cx;
-        sh.cy[s] = ts.cy;
-        sh.cz[s] = ts.cz;
-        sh.rngLo[s] = (unsigned)ts.rng;
-        sh.rngHi[s] = (unsigned)(ts.rng >> 32);
-        sh.t[s] = ts.t;
-        sh.tUpper[s] = ts.tUpper;
-        sh.maj[s] = ts.maj;
-        sh.steps[s] = steps;
-        sh.meta[s] = (meta & ~15) | phase;
+      const unsigned doneNow = __ballot_sync(FULL, q != AQ_IDLE && s >= 0 && phase == LP_IDLE);
+      if (lane == 0 && doneNow) atomicSub(&sh.live, __popc(doneNow));
+      // A4: primary rays (generateRays.cu:71-243)
+      if (phase == LP_NEWSAMPLE) {
+        const int accumID = fr.accumID0 + kk;
+        const unsigned uAcc = (unsigned)accumID;
+        uint64_t rnd = rngSeed2((unsigned)px + (unsigned)W * uAcc, (unsigned)py + (unsigned)H * uAcc);
+        raySeed = rngSeed2((unsigned)px + uAcc * (unsigned)W, (uint32_t)py);
+        const float pixel_u = (accumID == 0) ? .5f : rngFloat(rnd);
+        const float pixel_v = (accumID == 0) ? .5f : rngFloat(rnd);
+        const float image_u = ((px + pixel_u) / float(W));
+        const float image_v = ((py + pixel_v) / float(H));
+        const float aspect = W / float(H);
+        const float su = 1.f * aspect * (image_u - .5f), sv = 1.f * (image_v - .5f);
+        float3 d = f3(fr.dir00.x + su * fr.dirdu.x + sv * fr.dirdv.x, fr.dir00.y + su * fr.dirdu.y + sv * fr.dirdv.y,
+                      fr.dir00.z + su * fr.dirdu.z + sv * fr.dirdv.z);
+        d = normalize3(d);
+        float3 o = fr.lens00;
+        tMax = 1e30f;
+        if (fr.cutPlane.w > -1e28f) {
+          const float3 N = f3(fr.cutPlane.x, fr.cutPlane.y, fr.cutPlane.z);
+          const float dist_org = dot3(N, o) + fr.cutPlane.w;
+          const float denom = dot3(N, d);
+          if (dist_org >= 0.f) {
+            if (denom < 0.f) tMax = fmin_(tMax, -dist_org / denom);
+          } else {
+            if (denom > 0.f) {
+              const float te = -dist_org / denom;
+              o = f3(o.x + te * d.x, o.y + te * d.y, o.z + te * d.z);
+            } else tMax = 0.f;
+          }
+        }
+        meta &= ~16;  // a primary ray
+        nRays++;
+        org = o;
+        dir = d;
+        phase = LP_BEGIN;
       }
-      // count live slots for the exit test (after the barrier below)
-      __syncthreads();
-      int liveHere = 0;
-      for (int s2 = tid; s2 < kWFSlots; s2 += kWFThreads) liveHere += wfPhase(sh.meta[s2]) != LP_IDLE;
-      liveHere = __reduce_add_sync(FULL, liveHere);
-      if (lane == 0 && liveHere) atomicAdd(&sh.live, liveHere);
+      // A5: TraceRays::run fix-up, isProg prologue, dda3 set-up
+      if (phase == LP_BEGIN) {
+        TraceState ts;
+        const bool inside = traceBegin(v, ts, org, dir, tMax, raySeed);
+        sh.ox[s] = ts.org.x;
+        sh.oy[s] = ts.org.y;
+        sh.oz[s] = ts.org.z;
+        sh.dx[s] = ts.dir.x;
+        sh.dy[s] = ts.dir.y;
+        sh.dz[s] = ts.dir.z;
+        sh.rayTMax[s] = ts.rayTMax;
+        sh.seedLo[s] = (unsigned)raySeed;
+        sh.seedHi[s] = (unsigned)(raySeed >> 32);
+        if (inside) {
+          sh.ddaTMax[s] = ts.ddaTMax;
+          sh.rayT0[s] = ts.rayT0;
+          sh.ncb[s] = ts.nextCellBegin;
+          sh.tnx[s] = ts.tNext.x;
+          sh.tny[s] = ts.tNext.y;
+          sh.tnz[s] = ts.tNext.z;
+          sh.tsx[s] = ts.tStep.x;
+          sh.tsy[s] = ts.tStep.y;
+          sh.tsz[s] = ts.tStep.z;
+          sh.cx[s] = ts.cx;
+          sh.cy[s] = ts.cy;
+          sh.cz[s] = ts.cz;
+          sh.rngLo[s] = (unsigned)ts.rng;
+          sh.rngHi[s] = (unsigned)(ts.rng >> 32);
+          sh.steps[s] = 0;
+          meta = (meta & ~(15 | (63 << 8))) | LP_CELL | (ts.bits << 8);
+          phase = LP_CELL;
+        } else {
+          // rays that miss keep only their fix-up bits (none are read at a miss)
+          meta = (meta & ~15) | LP_ENDED;
+          phase = LP_ENDED;
+        }
+      }
+      if (s >= 0 && phase != kAQDrop) {
+        if (dirty) {
+          sh.acc[s] = acc;
+          sh.k[s] = kk;
+        }
+        if (phase != LP_IDLE) sh.meta[s] = meta;
+      }
+      const bool keep = s >= 0 && phase != kAQDrop;
+      ok &= aqPush(sh, AQ_TRACE, keep && phase == LP_CELL, s);
+      ok &= aqPush(sh, AQ_END, keep && phase == LP_ENDED, s);
+      ok &= aqPush(sh, AQ_IDLE, keep && phase == LP_IDLE, s);
     }
-    __syncthreads();
-    if (sh.exhausted && sh.curLeft <= 0 && sh.live == 0) break;
+    if (!__all_sync(FULL, ok)) {
+      errBits |= ERR_ITER_CAP;
+      if (lane == 0) atomicExch(&sh.failed, 1);
+      break;
+    }
   }
-  if (sh.aborted && threadIdx.x == 0) errBits |= ERR_ABORTED;
+  if (threadIdx.x == 0 && aqLoadI(&sh.aborted)) errBits |= ERR_ABORTED;
   unsigned long long wSamples = nSamples, wVisits = nVisits, wRays = nRays;
   for (int o = 16; o > 0; o >>= 1) {
     wSamples += __shfl_down_sync(FULL, wSamples, o);
@@ -2412,12 +2474,12 @@ static cudaError_t launchRenderWFT(const VolumeDD &v, const FrameDD &fr, LaunchC
   if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
     return cudaGetLastError();
   int occ = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kWFThreads, smem) != cudaSuccess)
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kAQThreads, smem) != cudaSuccess)
     return cudaGetLastError();
   JobDD job;
   job.v = v;
   job.fr = fr;
-  kern<<<smCount() * (occ > 0 ? occ : 1), kWFThreads, smem, s>>>(job, ctr);
+  kern<<<smCount() * (occ > 0 ? occ : 1), kAQThreads, smem, s>>>(job, ctr);
   return cudaGetLastError();
 }
 

@@ -299,11 +299,11 @@ BN_API void bnxPixelPartitionOwners(int width, int height, int count, int *owner
 BN_API void bnxSetLaunchConfig(BNContext context, int blocksPerSM, int threadsPerBlock);
 /* With enable != 0, plain jobs (no isosurface, multi-scatter or principled
    volume) of bnRender, and single-job batches without a graph, render with
-   the regrouped kernel: pixel slots whose state lives in shared memory,
-   advanced phase by phase (shading and accumulation, new pixels, ray
-   generation and set-up, macrocell walk and Woodcock steps) over lists
-   compacted per phase, so that every phase runs with full warps.  The
-   default (0) is the per-lane kernel (one pixel per lane;
+   the regrouped kernel: pixel slots whose state lives in shared memory and
+   which wait in ring queues there (new pixels, rays to trace, collisions to
+   shade, rays that ended); each warp takes up to 32 slots from one queue at
+   a time, with no block-wide barrier, so that every step runs with full
+   warps.  The default (0) is the per-lane kernel (one pixel per lane;
    bnxSetLaunchConfig and bnxSetScheduling apply to it), which is faster on
    the workloads measured.  Both give the same frames and counters.  No
    reference counterpart. */

@@ -1,5 +1,6 @@
 """The regrouped render kernel (bnxSetRegrouping): pixel slots in shared
-memory advanced phase by phase over compacted lists.  It must give the
+memory, taken by warps from ring queues (new pixels, rays to trace,
+collisions to shade, rays that ended).  It must give the
 per-lane kernel's frames and work counters bit for bit (both are checked
 against the CPU oracle here), over every plain scene of the parity tests,
 accumulation across renders and compensated accumulation, pixel partitions,
