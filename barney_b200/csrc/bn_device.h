@@ -136,10 +136,11 @@ cudaError_t launchRender(const VolumeDD &vol, const FrameDD &frame, LaunchCounte
 // extended: 2 if some job has an isosurface, else 1 if some job has
 // fr.maxVolumeBounces > 0, a principled volume or exact-log free flight,
 // else 0 (selects the kernel instantiation that implements them); voxelType: the
-// VoxelType all jobs share (a kernel compiled for it) or -1 (mixed)
+// VoxelType all jobs share (a kernel compiled for it) or -1 (mixed);
+// compensated: some job carries compensation terms (fr.comp)
 cudaError_t launchRenderBatch(const JobDD *jobs, const int *chunkStart, int numJobs, LaunchCounters *counters,
                               int blocksPerSM, int threadsPerBlock, cudaStream_t s, const SchedDD &sd = SchedDD(),
-                              int extended = 0, int voxelType = -1);
+                              int extended = 0, int voxelType = -1, bool compensated = true);
 cudaError_t launchResolve(const float4 *accum, int numPixels, int accumID, int fmt, void *out, cudaStream_t s,
                           const float4 *comp = nullptr);
 // resolves every job of a batch table into its fr.color after its waves
@@ -177,7 +178,7 @@ cudaError_t launchRender(const VolumeDD &vol, const FrameDD &frame, LaunchCounte
                          int threadsPerBlock, cudaStream_t s, const SchedDD &sd = SchedDD());
 cudaError_t launchRenderBatch(const JobDD *jobs, const int *chunkStart, int numJobs, LaunchCounters *counters,
                               int blocksPerSM, int threadsPerBlock, cudaStream_t s, const SchedDD &sd = SchedDD(),
-                              int extended = 0, int voxelType = -1);
+                              int extended = 0, int voxelType = -1, bool compensated = true);
 cudaError_t launchSampleProbe(const VolumeDD &vol, const float3 *P, int n, float *scalar, float4 *rgba, cudaStream_t s);
 cudaError_t launchRenderRegrouped(const VolumeDD &vol, const FrameDD &frame, LaunchCounters *counters, cudaStream_t s);
 long long readBoundsViolationsHere();  // bounds-checked build only

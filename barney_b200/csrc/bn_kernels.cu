@@ -971,7 +971,9 @@ __device__ __noinline__ SurfaceBounce surfaceBounce(const VolumeDD &v, const Fra
 // LOG: 0 fastLog (Volume.h:154-164), 1 -logf (bnx.exactLog), 2 per job (batch)
 // EXT: 0 the plain kernels; 1 multi-scatter paths and principled volumes;
 // 2 also isosurfaces (ISO)
-template <int T, bool BATCH, int LOG, int EXT>
+// CMP: jobs may carry compensation terms (fr.comp); false compiles the
+// compensated sums out
+template <int T, bool BATCH, int LOG, int EXT, bool CMP>
 DEV void renderLoop(const JobDD *__restrict__ jobs, const int *__restrict__ chunkStart, int numJobs, int numChunks, const SchedDD &sd,
                     LaunchCounters *ctr, const float4 *sTF, const float *u8lut) {
   const unsigned FULL = 0xffffffffu;
@@ -995,9 +997,14 @@ DEV void renderLoop(const JobDD *__restrict__ jobs, const int *__restrict__ chun
   TraceState ts;
   uint64_t raySeed = 0;
   float3 primDir = f3(0.f, 0.f, 0.f);
-  float3 shadowTp = f3(0.f, 0.f, 0.f);
+  // shadowFrag: the fragment a shadow ray adds when it reaches the light
+  // (min(MIS weight x throughput, clamp)), formed when the ray is spawned.
+  // The plain kernels keep it in hitRGB's registers: a primary ray's TF
+  // colour is dead once its collision is shaded, and a shadow ray's own
+  // collision colour is never read.
   float3 hitRGB = f3(0.f, 0.f, 0.f);
-  float misWeight = 0.f;
+  float3 shadowFragStore = f3(0.f, 0.f, 0.f);
+  float3 &shadowFrag = EXT ? shadowFragStore : hitRGB;
   bool shadowRay = false;
   unsigned steps = 0;
   // EXT (the instantiation for multi-scatter paths and principled volumes;
@@ -1042,7 +1049,7 @@ DEV void renderLoop(const JobDD *__restrict__ jobs, const int *__restrict__ chun
       if (phase == LP_HIT) {
         const int accumID = fr.accumID0 + k;
         const float clampMax = 10.f * (1 + accumID);
-        const bool cmp = fr.comp != nullptr;
+        const bool cmp = CMP && fr.comp != nullptr;
         const bool surf = ISO && (ts.bits & 64);  // the hit is on the isosurface
         bool spawned = false;
         if (!shadowRay) {
@@ -1100,8 +1107,8 @@ DEV void renderLoop(const JobDD *__restrict__ jobs, const int *__restrict__ chun
                                                       nDifB, u8lut);
             raySeed = (sb.flags & 1) ? sb.shadowSeed : sb.seed;
             if (sb.flags & 1) {  // makeShadowRay (Ray.h:147-157)
-              misWeight = sb.shadowMis;
-              shadowTp = sb.shadowTp;
+              shadowFrag = f3(fmin_(sb.shadowMis * sb.shadowTp.x, clampMax), fmin_(sb.shadowMis * sb.shadowTp.y, clampMax),
+                              fmin_(sb.shadowMis * sb.shadowTp.z, clampMax));
               ts.org = sb.shadowOrg;
               ts.dir = sb.lightDir;
               ts.rayTMax = kInf;
@@ -1168,19 +1175,18 @@ DEV void renderLoop(const JobDD *__restrict__ jobs, const int *__restrict__ chun
                                      tin.z * ip * fv.z * ls.radiance.z * 1.f);
                 // shadowRay.rngSeed = ray.rngSeed; ray.rngSeed.next(tMax)
                 if (EXT) scatSeed = (raySeed ^ ((uint64_t)__float_as_uint(tHit) << 1)) * kRngMul;
-                misWeight = 1.f;
+                float misWeight = 1.f;
                 bool alive = true;
                 if (!isDir && needsMIS) {
-                  const float pl = kOneOverFourPi;
-                  float ps;
-                  if (v.phase == PHASE_SIMPLE) ps = kOneOverFourPi;
-                  else ps = hgPhase(v.anisotropy, dot3(normalize3(f3(-woN.x, -woN.y, -woN.z)), normalize3(ls.dir)));
-                  misWeight = pl / (pl + ps + 1e-10f);
+                  // the phase pdf of the light sample's direction is fpdf
+                  // (the same expression: 1/4pi, or hgPhase of the same vectors)
+                  misWeight = kOneOverFourPi / (kOneOverFourPi + fpdf + 1e-10f);
                   if (misWeight < 1e-5f) alive = false;
                 }
                 const float sTMax = kInf * (1.f - 2.f * offsetEpsilon);
                 if (alive && sTMax > 0.f) {
-                  shadowTp = f3(roundHalf(tp.x), roundHalf(tp.y), roundHalf(tp.z));
+                  shadowFrag = f3(fmin_(misWeight * roundHalf(tp.x), clampMax), fmin_(misWeight * roundHalf(tp.y), clampMax),
+                                  fmin_(misWeight * roundHalf(tp.z), clampMax));
                   // makeShadowRay (Ray.h:147-157); its RNG seed is the primary's,
                   // which is not used again by this wave
                   ts.org = f3(P.x + offsetEpsilon * woN.x, P.y + offsetEpsilon * woN.y, P.z + offsetEpsilon * woN.z);
@@ -1268,7 +1274,7 @@ DEV void renderLoop(const JobDD *__restrict__ jobs, const int *__restrict__ chun
       if (phase == LP_ENDED) {
         const int accumID = fr.accumID0 + k;
         const float clampMax = 10.f * (1 + accumID);
-        const bool cmp = fr.comp != nullptr;
+        const bool cmp = CMP && fr.comp != nullptr;
         if (!shadowRay && (!EXT || depth == 0)) {
           // the primary ray's miss colour (generateRays.cu:217-227), computed here
           // rather than kept in registers for the whole wave
@@ -1296,9 +1302,7 @@ DEV void renderLoop(const JobDD *__restrict__ jobs, const int *__restrict__ chun
           if (fy > 0.f) accAdd(acc.y, comp.y, fy, cmp);
           if (fz > 0.f) accAdd(acc.z, comp.z, fz, cmp);
         } else {  // the shadow ray reached the light
-          const float f1x = fmin_(misWeight * shadowTp.x, clampMax);
-          const float f1y = fmin_(misWeight * shadowTp.y, clampMax);
-          const float f1z = fmin_(misWeight * shadowTp.z, clampMax);
+          const float f1x = shadowFrag.x, f1y = shadowFrag.y, f1z = shadowFrag.z;
           if (f1x > 0.f) accAdd(acc.x, comp.x, f1x, cmp);
           if (f1y > 0.f) accAdd(acc.y, comp.y, f1y, cmp);
           if (f1z > 0.f) accAdd(acc.z, comp.z, f1z, cmp);
@@ -1376,7 +1380,7 @@ DEV void renderLoop(const JobDD *__restrict__ jobs, const int *__restrict__ chun
         k = 0;
         const bool pixIn = BNB_IN(pix, (long long)fr.width * fr.height);
         acc = (fr.accumID0 > 0 && pixIn) ? fr.accum[pix] : make_float4(0.f, 0.f, 0.f, 0.f);
-        comp = (fr.accumID0 > 0 && fr.comp && pixIn) ? fr.comp[pix] : make_float4(0.f, 0.f, 0.f, 0.f);
+        comp = (CMP && fr.accumID0 > 0 && fr.comp && pixIn) ? fr.comp[pix] : make_float4(0.f, 0.f, 0.f, 0.f);
         phase = LP_NEWSAMPLE;
       }
       for (int i = 0; i < take; i++) need &= need - 1u;
@@ -1584,7 +1588,7 @@ __host__ __device__ inline int partitionChunks(int numChunks, int rank, int coun
   return (mine - 1) * kPartTileChunks + min(kPartTileChunks, numChunks - last * kPartTileChunks);
 }
 
-template <int T, int LOG, int EXT>
+template <int T, int LOG, int EXT, bool CMP>
 __global__ void __launch_bounds__(kRenderMaxThreads, EXT >= 2 ? kRenderMinBlocksIso : EXT ? kRenderMinBlocksExt : kRenderMinBlocks)
     renderKernel(const __grid_constant__ JobDD job, const __grid_constant__ SchedDD sd, LaunchCounters *ctr) {
   extern __shared__ float4 sTF[];
@@ -1594,7 +1598,7 @@ __global__ void __launch_bounds__(kRenderMaxThreads, EXT >= 2 ? kRenderMinBlocks
   __syncthreads();
   int numChunks = (job.fr.width * job.fr.height + kChunk - 1) / kChunk;
   if (job.fr.partCount > 1) numChunks = partitionChunks(numChunks, job.fr.partRank, job.fr.partCount);
-  renderLoop<T, false, LOG, EXT>(&job, nullptr, 1, numChunks, sd, ctr, sTF, u8lut);
+  renderLoop<T, false, LOG, EXT, CMP>(&job, nullptr, 1, numChunks, sd, ctr, sTF, u8lut);
 }
 
 // ---------------------------------------------------------------------------
@@ -2262,7 +2266,7 @@ __global__ void __launch_bounds__(kAQThreads, kAQMinBlocks)
 }
 
 // T: the voxel type every job of the batch has, or -1 (mixed: a switch per sample)
-template <int T, int EXT>
+template <int T, int EXT, bool CMP>
 __global__ void __launch_bounds__(kRenderMaxThreads, EXT >= 2 ? kRenderMinBlocksIso : EXT ? kRenderMinBlocksExt : kRenderMinBlocks)
     renderBatchKernel(const JobDD *__restrict__ jobs, const int *__restrict__ chunkStart, int numJobs, const __grid_constant__ SchedDD sd,
                       LaunchCounters *ctr) {
@@ -2271,8 +2275,8 @@ __global__ void __launch_bounds__(kRenderMaxThreads, EXT >= 2 ? kRenderMinBlocks
   __syncthreads();
   // plain batch kernels draw free-flight distances with fastLog only; batches
   // with an exact-log job run the extended kernel, which chooses per job
-  renderLoop<T, true, EXT ? 2 : 0, EXT>(jobs, chunkStart, numJobs, __ldg(chunkStart + numJobs), sd, ctr, nullptr,
-                                        u8lut);
+  renderLoop<T, true, EXT ? 2 : 0, EXT, CMP>(jobs, chunkStart, numJobs, __ldg(chunkStart + numJobs), sd, ctr, nullptr,
+                                             u8lut);
 }
 
 // Field samples and transfer-function lookups at given points
@@ -2444,13 +2448,18 @@ static cudaError_t launchRenderT(const VolumeDD &v, const FrameDD &fr, const Sch
                                  int bps, int tpb, cudaStream_t s) {
   const size_t smem = (size_t)v.tfN * sizeof(float4);
   const int ext = v.iso.enabled ? 2 : (fr.maxVolumeBounces > 0 || v.pv.enabled) ? 1 : 0;
+  // plain kernels with and without compensated sums; the extended kernels
+  // decide per job
+  const bool cmp = fr.comp != nullptr;
 #ifdef BNB_FAST_MATH
   if (ext) return cudaErrorInvalidValue;  // the fast-math object holds the plain kernels only
-  auto kern = fr.exactLog ? renderKernel<T, 1, 0> : renderKernel<T, 0, 0>;
+  auto kern = cmp ? (fr.exactLog ? renderKernel<T, 1, 0, true> : renderKernel<T, 0, 0, true>)
+                  : (fr.exactLog ? renderKernel<T, 1, 0, false> : renderKernel<T, 0, 0, false>);
 #else
-  auto kern = ext == 2   ? (fr.exactLog ? renderKernel<T, 1, 2> : renderKernel<T, 0, 2>)
-              : ext == 1 ? (fr.exactLog ? renderKernel<T, 1, 1> : renderKernel<T, 0, 1>)
-                         : (fr.exactLog ? renderKernel<T, 1, 0> : renderKernel<T, 0, 0>);
+  auto kern = ext == 2   ? (fr.exactLog ? renderKernel<T, 1, 2, true> : renderKernel<T, 0, 2, true>)
+              : ext == 1 ? (fr.exactLog ? renderKernel<T, 1, 1, true> : renderKernel<T, 0, 1, true>)
+              : cmp      ? (fr.exactLog ? renderKernel<T, 1, 0, true> : renderKernel<T, 0, 0, true>)
+                         : (fr.exactLog ? renderKernel<T, 1, 0, false> : renderKernel<T, 0, 0, false>);
 #endif
   if (smem > 48 * 1024 &&
       cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
@@ -2506,28 +2515,30 @@ cudaError_t launchRender(const VolumeDD &v, const FrameDD &fr, LaunchCounters *c
   }
 }
 
-template <int EXT>
+template <int EXT, bool CMP>
 static auto batchKernelFor(int voxelType) {
   switch (voxelType) {
-  case VOX_F32: return renderBatchKernel<VOX_F32, EXT>;
-  case VOX_U8: return renderBatchKernel<VOX_U8, EXT>;
-  case VOX_F16: return renderBatchKernel<VOX_F16, EXT>;
-  case VOX_U16: return renderBatchKernel<VOX_U16, EXT>;
-  case VOX_BF16: return renderBatchKernel<VOX_BF16, EXT>;
-  default: return renderBatchKernel<-1, EXT>;
+  case VOX_F32: return renderBatchKernel<VOX_F32, EXT, CMP>;
+  case VOX_U8: return renderBatchKernel<VOX_U8, EXT, CMP>;
+  case VOX_F16: return renderBatchKernel<VOX_F16, EXT, CMP>;
+  case VOX_U16: return renderBatchKernel<VOX_U16, EXT, CMP>;
+  case VOX_BF16: return renderBatchKernel<VOX_BF16, EXT, CMP>;
+  default: return renderBatchKernel<-1, EXT, CMP>;
   }
 }
 
 cudaError_t launchRenderBatch(const JobDD *jobs, const int *chunkStart, int numJobs, LaunchCounters *ctr, int bps,
-                              int tpb, cudaStream_t s, const SchedDD &sd, int extended, int voxelType) {
+                              int tpb, cudaStream_t s, const SchedDD &sd, int extended, int voxelType,
+                              bool compensated) {
   if (tpb <= 0) tpb = 128;
 #ifdef BNB_FAST_MATH
   if (extended) return cudaErrorInvalidValue;  // the fast-math object holds the plain kernels only
-  auto kern = batchKernelFor<0>(voxelType);
+  auto kern = compensated ? batchKernelFor<0, true>(voxelType) : batchKernelFor<0, false>(voxelType);
 #else
-  auto kern = extended >= 2 ? batchKernelFor<2>(voxelType)
-              : extended    ? batchKernelFor<1>(voxelType)
-                            : batchKernelFor<0>(voxelType);
+  auto kern = extended >= 2 ? batchKernelFor<2, true>(voxelType)
+              : extended    ? batchKernelFor<1, true>(voxelType)
+              : compensated ? batchKernelFor<0, true>(voxelType)
+                            : batchKernelFor<0, false>(voxelType);
 #endif
   if (bps <= 0) {
     int occ = 0;
@@ -2598,7 +2609,7 @@ long long readBoundsViolations() {
 
 int renderKernelMaxBlocksPerSM(int tpb) {
   int occ = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, renderKernel<VOX_F32, 0, 0>, tpb, 256 * sizeof(float4)) !=
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, renderKernel<VOX_F32, 0, 0, false>, tpb, 256 * sizeof(float4)) !=
       cudaSuccess) {
     cudaGetLastError();
     return 1;
