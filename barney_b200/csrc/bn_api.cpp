@@ -379,7 +379,7 @@ void renderBatch(Context *ctx, const std::vector<BatchEntry> &entries) {
   int extended = 0;  // 1: multi-scatter, principled or exact log; 2: isosurfaces (the extended kernels)
   int voxelType = -2;     // the type every job shares, else -1
   bool fast = true;       // every job asks for the fast-math kernels
-  bool compensated = false;  // some job keeps compensation terms
+  int compJobs = 0;  // jobs that keep compensation terms
   ctx->hostChunks[0] = 0;
   for (int i = 0; i < n; i++) {
     const BatchEntry &e = entries[i];
@@ -389,7 +389,7 @@ void renderBatch(Context *ctx, const std::vector<BatchEntry> &entries) {
                                   : (job.fr.maxVolumeBounces > 0 || job.v.pv.enabled || job.fr.exactLog) ? 1 : 0);
     voxelType = voxelType == -2 || voxelType == job.v.type ? job.v.type : -1;
     fast = fast && job.fr.fastMath;
-    compensated = compensated || job.fr.comp != nullptr;
+    compJobs += job.fr.comp != nullptr;
     ctx->hostJobs[i] = job;
     chunks += ((long long)job.fr.width * job.fr.height + 31) / 32;
     if (chunks > 0x7fffffffLL) throw Error(E_INVALID_ARG, "batch too large");
@@ -435,7 +435,8 @@ void renderBatch(Context *ctx, const std::vector<BatchEntry> &entries) {
     ck((fast ? fastmath::launchRenderBatch : launchRenderBatch)((const JobDD *)ctx->batchJobs.ptr,
                                                                 (const int *)ctx->batchChunks.ptr, n, ctx->dCounters,
                                                                 ctx->blocksPerSM, ctx->threadsPerBlock, s, ctx->sched,
-                                                                extended, voxelType, compensated),
+                                                                extended, voxelType,
+                                                                compJobs == 0 ? 0 : compJobs == n ? 2 : 1),
        "batch render kernel");
     if (timed) ck(cudaEventRecord(ctx->ev[1], s), "event");
     ck(launchResolveBatch((const JobDD *)ctx->batchJobs.ptr, (const int *)ctx->batchChunks.ptr, n, (int)chunks, s),

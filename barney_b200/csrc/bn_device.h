@@ -18,7 +18,9 @@ constexpr int kCellsPerMC = 8;  // StructuredData.cu:26
 constexpr long long kMaxFramePixels = 0x7fffffffLL;  // pixels of one frame (32-bit pixel / chunk indices)
 constexpr int kPartTileChunks = 32;    // pixel-tile partition: 32 chunks of 32 pixels per tile
 constexpr int kRenderMaxThreads = 128;  // __launch_bounds__ of the render kernels:
-constexpr int kRenderMinBlocks = 6;     // plain: 6 x 128 threads per SM (at most 85 registers)
+constexpr int kRenderMinBlocks = 7;     // plain single-frame: 7 x 128 threads per SM (at most 73 registers)
+constexpr int kRenderMinBlocksBatch = 6;  // plain batch and compensated single-frame: 6 x 128 (85; at 7 the
+                                          // compensated kernels spill 140-364 B)
 constexpr int kRenderMinBlocksExt = 5;  // extended (multi-scatter, principled): 5 x 128 (102)
 constexpr int kRenderMinBlocksIso = 5;  // extended with isosurfaces: 5 x 128 (102; 3 % faster than 4 x 128)
 
@@ -137,10 +139,11 @@ cudaError_t launchRender(const VolumeDD &vol, const FrameDD &frame, LaunchCounte
 // fr.maxVolumeBounces > 0, a principled volume or exact-log free flight,
 // else 0 (selects the kernel instantiation that implements them); voxelType: the
 // VoxelType all jobs share (a kernel compiled for it) or -1 (mixed);
-// compensated: some job carries compensation terms (fr.comp)
+// compensated: how many jobs carry compensation terms (fr.comp): 0 none,
+// 1 some, 2 all
 cudaError_t launchRenderBatch(const JobDD *jobs, const int *chunkStart, int numJobs, LaunchCounters *counters,
                               int blocksPerSM, int threadsPerBlock, cudaStream_t s, const SchedDD &sd = SchedDD(),
-                              int extended = 0, int voxelType = -1, bool compensated = true);
+                              int extended = 0, int voxelType = -1, int compensated = 1);
 cudaError_t launchResolve(const float4 *accum, int numPixels, int accumID, int fmt, void *out, cudaStream_t s,
                           const float4 *comp = nullptr);
 // resolves every job of a batch table into its fr.color after its waves
@@ -178,7 +181,7 @@ cudaError_t launchRender(const VolumeDD &vol, const FrameDD &frame, LaunchCounte
                          int threadsPerBlock, cudaStream_t s, const SchedDD &sd = SchedDD());
 cudaError_t launchRenderBatch(const JobDD *jobs, const int *chunkStart, int numJobs, LaunchCounters *counters,
                               int blocksPerSM, int threadsPerBlock, cudaStream_t s, const SchedDD &sd = SchedDD(),
-                              int extended = 0, int voxelType = -1, bool compensated = true);
+                              int extended = 0, int voxelType = -1, int compensated = 1);
 cudaError_t launchSampleProbe(const VolumeDD &vol, const float3 *P, int n, float *scalar, float4 *rgba, cudaStream_t s);
 cudaError_t launchRenderRegrouped(const VolumeDD &vol, const FrameDD &frame, LaunchCounters *counters, cudaStream_t s);
 long long readBoundsViolationsHere();  // bounds-checked build only

@@ -626,8 +626,7 @@ DEV float roundHalf(float x) { return __half2float(__float2half_rn(x)); }
 // Neumaier-compensated sum (precision forms): sum += x, error kept in c.
 DEV void neumaier(float &sum, float &c, float x) {
   const float t = sum + x;
-  if (fabsf(sum) >= fabsf(x)) c += (sum - t) + x;
-  else c += (x - t) + sum;
+  c += fabsf(sum) >= fabsf(x) ? (sum - t) + x : (x - t) + sum;
   sum = t;
 }
 DEV void accAdd(float &sum, float &c, float x, bool comp) {
@@ -971,9 +970,9 @@ __device__ __noinline__ SurfaceBounce surfaceBounce(const VolumeDD &v, const Fra
 // LOG: 0 fastLog (Volume.h:154-164), 1 -logf (bnx.exactLog), 2 per job (batch)
 // EXT: 0 the plain kernels; 1 multi-scatter paths and principled volumes;
 // 2 also isosurfaces (ISO)
-// CMP: jobs may carry compensation terms (fr.comp); false compiles the
-// compensated sums out
-template <int T, bool BATCH, int LOG, int EXT, bool CMP>
+// CMP: compensated sums (fr.comp) in no job (0: compiled out), in the jobs
+// that carry terms (1: a test per sum), or in every job (2)
+template <int T, bool BATCH, int LOG, int EXT, int CMP>
 DEV void renderLoop(const JobDD *__restrict__ jobs, const int *__restrict__ chunkStart, int numJobs, int numChunks, const SchedDD &sd,
                     LaunchCounters *ctr, const float4 *sTF, const float *u8lut) {
   const unsigned FULL = 0xffffffffu;
@@ -990,8 +989,7 @@ DEV void renderLoop(const JobDD *__restrict__ jobs, const int *__restrict__ chun
 
   // lane state
   int phase = LP_IDLE;
-  int job = 0, ix = 0, iy = 0, k = 0;
-  int64_t pix = 0;
+  int job = 0, ix = 0, iy = 0, k = 0;  // the pixel's index iy * width + ix is formed where it is used
   float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
   float4 comp = make_float4(0.f, 0.f, 0.f, 0.f);
   TraceState ts;
@@ -1049,7 +1047,7 @@ DEV void renderLoop(const JobDD *__restrict__ jobs, const int *__restrict__ chun
       if (phase == LP_HIT) {
         const int accumID = fr.accumID0 + k;
         const float clampMax = 10.f * (1 + accumID);
-        const bool cmp = CMP && fr.comp != nullptr;
+        const bool cmp = CMP == 2 || (CMP == 1 && fr.comp != nullptr);
         const bool surf = ISO && (ts.bits & 64);  // the hit is on the isosurface
         bool spawned = false;
         if (!shadowRay) {
@@ -1256,6 +1254,7 @@ DEV void renderLoop(const JobDD *__restrict__ jobs, const int *__restrict__ chun
             steps = 0;
             phase = LP_BEGIN;
           } else if (++k == fr.spp) {  // no ray left: the wave is done
+            const int64_t pix = (int64_t)iy * fr.width + ix;
             if (BNB_IN(pix, (long long)fr.width * fr.height)) {
               fr.accum[pix] = acc;
               if (cmp) fr.comp[pix] = comp;
@@ -1274,7 +1273,7 @@ DEV void renderLoop(const JobDD *__restrict__ jobs, const int *__restrict__ chun
       if (phase == LP_ENDED) {
         const int accumID = fr.accumID0 + k;
         const float clampMax = 10.f * (1 + accumID);
-        const bool cmp = CMP && fr.comp != nullptr;
+        const bool cmp = CMP == 2 || (CMP == 1 && fr.comp != nullptr);
         if (!shadowRay && (!EXT || depth == 0)) {
           // the primary ray's miss colour (generateRays.cu:217-227), computed here
           // rather than kept in registers for the whole wave
@@ -1318,6 +1317,7 @@ DEV void renderLoop(const JobDD *__restrict__ jobs, const int *__restrict__ chun
           steps = 0;
           phase = LP_BEGIN;
         } else if (++k == fr.spp) {
+          const int64_t pix = (int64_t)iy * fr.width + ix;
           if (BNB_IN(pix, (long long)fr.width * fr.height)) {
             fr.accum[pix] = acc;
             if (cmp) fr.comp[pix] = comp;
@@ -1376,11 +1376,11 @@ DEV void renderLoop(const JobDD *__restrict__ jobs, const int *__restrict__ chun
         job = chunkJob;
         ix = within / rows;
         iy = 4 * band + within % rows;
-        pix = (int64_t)iy * W + ix;
+        const int64_t pix = (int64_t)iy * W + ix;
         k = 0;
         const bool pixIn = BNB_IN(pix, (long long)fr.width * fr.height);
         acc = (fr.accumID0 > 0 && pixIn) ? fr.accum[pix] : make_float4(0.f, 0.f, 0.f, 0.f);
-        comp = (CMP && fr.accumID0 > 0 && fr.comp && pixIn) ? fr.comp[pix] : make_float4(0.f, 0.f, 0.f, 0.f);
+        comp = (CMP && fr.accumID0 > 0 && (CMP == 2 || fr.comp) && pixIn) ? fr.comp[pix] : make_float4(0.f, 0.f, 0.f, 0.f);
         phase = LP_NEWSAMPLE;
       }
       for (int i = 0; i < take; i++) need &= need - 1u;
@@ -1588,8 +1588,11 @@ __host__ __device__ inline int partitionChunks(int numChunks, int rank, int coun
   return (mine - 1) * kPartTileChunks + min(kPartTileChunks, numChunks - last * kPartTileChunks);
 }
 
-template <int T, int LOG, int EXT, bool CMP>
-__global__ void __launch_bounds__(kRenderMaxThreads, EXT >= 2 ? kRenderMinBlocksIso : EXT ? kRenderMinBlocksExt : kRenderMinBlocks)
+template <int T, int LOG, int EXT, int CMP>
+__global__ void __launch_bounds__(kRenderMaxThreads, EXT >= 2 ? kRenderMinBlocksIso
+                                                     : EXT    ? kRenderMinBlocksExt
+                                                     : CMP    ? kRenderMinBlocksBatch
+                                                              : kRenderMinBlocks)
     renderKernel(const __grid_constant__ JobDD job, const __grid_constant__ SchedDD sd, LaunchCounters *ctr) {
   extern __shared__ float4 sTF[];
   __shared__ float u8lut[256];
@@ -2266,8 +2269,8 @@ __global__ void __launch_bounds__(kAQThreads, kAQMinBlocks)
 }
 
 // T: the voxel type every job of the batch has, or -1 (mixed: a switch per sample)
-template <int T, int EXT, bool CMP>
-__global__ void __launch_bounds__(kRenderMaxThreads, EXT >= 2 ? kRenderMinBlocksIso : EXT ? kRenderMinBlocksExt : kRenderMinBlocks)
+template <int T, int EXT, int CMP>
+__global__ void __launch_bounds__(kRenderMaxThreads, EXT >= 2 ? kRenderMinBlocksIso : EXT ? kRenderMinBlocksExt : kRenderMinBlocksBatch)
     renderBatchKernel(const JobDD *__restrict__ jobs, const int *__restrict__ chunkStart, int numJobs, const __grid_constant__ SchedDD sd,
                       LaunchCounters *ctr) {
   __shared__ float u8lut[256];
@@ -2453,13 +2456,13 @@ static cudaError_t launchRenderT(const VolumeDD &v, const FrameDD &fr, const Sch
   const bool cmp = fr.comp != nullptr;
 #ifdef BNB_FAST_MATH
   if (ext) return cudaErrorInvalidValue;  // the fast-math object holds the plain kernels only
-  auto kern = cmp ? (fr.exactLog ? renderKernel<T, 1, 0, true> : renderKernel<T, 0, 0, true>)
-                  : (fr.exactLog ? renderKernel<T, 1, 0, false> : renderKernel<T, 0, 0, false>);
+  auto kern = cmp ? (fr.exactLog ? renderKernel<T, 1, 0, 2> : renderKernel<T, 0, 0, 2>)
+                  : (fr.exactLog ? renderKernel<T, 1, 0, 0> : renderKernel<T, 0, 0, 0>);
 #else
-  auto kern = ext == 2   ? (fr.exactLog ? renderKernel<T, 1, 2, true> : renderKernel<T, 0, 2, true>)
-              : ext == 1 ? (fr.exactLog ? renderKernel<T, 1, 1, true> : renderKernel<T, 0, 1, true>)
-              : cmp      ? (fr.exactLog ? renderKernel<T, 1, 0, true> : renderKernel<T, 0, 0, true>)
-                         : (fr.exactLog ? renderKernel<T, 1, 0, false> : renderKernel<T, 0, 0, false>);
+  auto kern = ext == 2   ? (fr.exactLog ? renderKernel<T, 1, 2, 1> : renderKernel<T, 0, 2, 1>)
+              : ext == 1 ? (fr.exactLog ? renderKernel<T, 1, 1, 1> : renderKernel<T, 0, 1, 1>)
+              : cmp      ? (fr.exactLog ? renderKernel<T, 1, 0, 2> : renderKernel<T, 0, 0, 2>)
+                         : (fr.exactLog ? renderKernel<T, 1, 0, 0> : renderKernel<T, 0, 0, 0>);
 #endif
   if (smem > 48 * 1024 &&
       cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
@@ -2515,7 +2518,7 @@ cudaError_t launchRender(const VolumeDD &v, const FrameDD &fr, LaunchCounters *c
   }
 }
 
-template <int EXT, bool CMP>
+template <int EXT, int CMP>
 static auto batchKernelFor(int voxelType) {
   switch (voxelType) {
   case VOX_F32: return renderBatchKernel<VOX_F32, EXT, CMP>;
@@ -2529,16 +2532,19 @@ static auto batchKernelFor(int voxelType) {
 
 cudaError_t launchRenderBatch(const JobDD *jobs, const int *chunkStart, int numJobs, LaunchCounters *ctr, int bps,
                               int tpb, cudaStream_t s, const SchedDD &sd, int extended, int voxelType,
-                              bool compensated) {
+                              int compensated) {
   if (tpb <= 0) tpb = 128;
 #ifdef BNB_FAST_MATH
   if (extended) return cudaErrorInvalidValue;  // the fast-math object holds the plain kernels only
-  auto kern = compensated ? batchKernelFor<0, true>(voxelType) : batchKernelFor<0, false>(voxelType);
+  auto kern = compensated == 2   ? batchKernelFor<0, 2>(voxelType)
+              : compensated == 1 ? batchKernelFor<0, 1>(voxelType)
+                                 : batchKernelFor<0, 0>(voxelType);
 #else
-  auto kern = extended >= 2 ? batchKernelFor<2, true>(voxelType)
-              : extended    ? batchKernelFor<1, true>(voxelType)
-              : compensated ? batchKernelFor<0, true>(voxelType)
-                            : batchKernelFor<0, false>(voxelType);
+  auto kern = extended >= 2      ? batchKernelFor<2, 1>(voxelType)
+              : extended         ? batchKernelFor<1, 1>(voxelType)
+              : compensated == 2 ? batchKernelFor<0, 2>(voxelType)
+              : compensated == 1 ? batchKernelFor<0, 1>(voxelType)
+                                 : batchKernelFor<0, 0>(voxelType);
 #endif
   if (bps <= 0) {
     int occ = 0;
@@ -2609,7 +2615,7 @@ long long readBoundsViolations() {
 
 int renderKernelMaxBlocksPerSM(int tpb) {
   int occ = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, renderKernel<VOX_F32, 0, 0, false>, tpb, 256 * sizeof(float4)) !=
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, renderKernel<VOX_F32, 0, 0, 0>, tpb, 256 * sizeof(float4)) !=
       cudaSuccess) {
     cudaGetLastError();
     return 1;
