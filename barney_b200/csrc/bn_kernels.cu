@@ -2451,18 +2451,19 @@ static cudaError_t launchRenderT(const VolumeDD &v, const FrameDD &fr, const Sch
                                  int bps, int tpb, cudaStream_t s) {
   const size_t smem = (size_t)v.tfN * sizeof(float4);
   const int ext = v.iso.enabled ? 2 : (fr.maxVolumeBounces > 0 || v.pv.enabled) ? 1 : 0;
-  // plain kernels with and without compensated sums; the extended kernels
-  // decide per job
+  // kernels with and without compensated sums
   const bool cmp = fr.comp != nullptr;
 #ifdef BNB_FAST_MATH
   if (ext) return cudaErrorInvalidValue;  // the fast-math object holds the plain kernels only
   auto kern = cmp ? (fr.exactLog ? renderKernel<T, 1, 0, 2> : renderKernel<T, 0, 0, 2>)
                   : (fr.exactLog ? renderKernel<T, 1, 0, 0> : renderKernel<T, 0, 0, 0>);
 #else
-  auto kern = ext == 2   ? (fr.exactLog ? renderKernel<T, 1, 2, 1> : renderKernel<T, 0, 2, 1>)
-              : ext == 1 ? (fr.exactLog ? renderKernel<T, 1, 1, 1> : renderKernel<T, 0, 1, 1>)
-              : cmp      ? (fr.exactLog ? renderKernel<T, 1, 0, 2> : renderKernel<T, 0, 0, 2>)
-                         : (fr.exactLog ? renderKernel<T, 1, 0, 0> : renderKernel<T, 0, 0, 0>);
+  auto kern = ext == 2 ? (cmp ? (fr.exactLog ? renderKernel<T, 1, 2, 2> : renderKernel<T, 0, 2, 2>)
+                              : (fr.exactLog ? renderKernel<T, 1, 2, 0> : renderKernel<T, 0, 2, 0>))
+              : ext == 1 ? (cmp ? (fr.exactLog ? renderKernel<T, 1, 1, 2> : renderKernel<T, 0, 1, 2>)
+                                : (fr.exactLog ? renderKernel<T, 1, 1, 0> : renderKernel<T, 0, 1, 0>))
+              : cmp ? (fr.exactLog ? renderKernel<T, 1, 0, 2> : renderKernel<T, 0, 0, 2>)
+                    : (fr.exactLog ? renderKernel<T, 1, 0, 0> : renderKernel<T, 0, 0, 0>);
 #endif
   if (smem > 48 * 1024 &&
       cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
@@ -2540,8 +2541,8 @@ cudaError_t launchRenderBatch(const JobDD *jobs, const int *chunkStart, int numJ
               : compensated == 1 ? batchKernelFor<0, 1>(voxelType)
                                  : batchKernelFor<0, 0>(voxelType);
 #else
-  auto kern = extended >= 2      ? batchKernelFor<2, 1>(voxelType)
-              : extended         ? batchKernelFor<1, 1>(voxelType)
+  auto kern = extended >= 2      ? (compensated ? batchKernelFor<2, 1>(voxelType) : batchKernelFor<2, 0>(voxelType))
+              : extended         ? (compensated ? batchKernelFor<1, 1>(voxelType) : batchKernelFor<1, 0>(voxelType))
               : compensated == 2 ? batchKernelFor<0, 2>(voxelType)
               : compensated == 1 ? batchKernelFor<0, 1>(voxelType)
                                  : batchKernelFor<0, 0>(voxelType);
