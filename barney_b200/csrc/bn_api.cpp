@@ -1283,12 +1283,12 @@ BN_API void bnxAutotuneBatch(BNContext context, const BNXRenderJob *jobs, int nu
   std::vector<BatchEntry> e = batchEntries(jobs, numJobs);
   std::vector<uint32_t> saved;
   for (auto &x : e) saved.push_back(x.fb->accumID);
-  const int maxBps = std::max(1, renderKernelMaxBlocksPerSM(128));
+  // blocks per SM: 0, the occupancy of the kernel the batch runs
   struct Cand { int tpb, bps, service; };
   std::vector<Cand> cands;
   for (int tpb : {64, 128})
     for (int service : {4, 8, 12, 16, 20, 24, 28})
-      cands.push_back({tpb, tpb == 64 ? 2 * maxBps : maxBps, service});
+      cands.push_back({tpb, 0, service});
   Cand bestC{c->threadsPerBlock, c->blocksPerSM, c->sched.serviceBatch};
   float bestMs = 1e30f;
   for (const Cand &k : cands) {

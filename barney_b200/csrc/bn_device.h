@@ -148,7 +148,6 @@ cudaError_t launchResolve(const float4 *accum, int numPixels, int accumID, int f
                           const float4 *comp = nullptr);
 // resolves every job of a batch table into its fr.color after its waves
 cudaError_t launchResolveBatch(const JobDD *jobs, const int *chunkStart, int numJobs, int numChunks, cudaStream_t s);
-int renderKernelMaxBlocksPerSM(int threadsPerBlock);
 // out-of-range accesses counted by the bounds-checked build since the last
 // call (then reset); -1 in the normal build, -2 on a CUDA error
 long long readBoundsViolations();

@@ -2614,16 +2614,6 @@ long long readBoundsViolations() {
 #endif
 }
 
-int renderKernelMaxBlocksPerSM(int tpb) {
-  int occ = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, renderKernel<VOX_F32, 0, 0, 0>, tpb, 256 * sizeof(float4)) !=
-      cudaSuccess) {
-    cudaGetLastError();
-    return 1;
-  }
-  return occ;
-}
-
 // ---------------------------------------------------------------------------
 // No-allocation render (bnxRenderStructuredNoAlloc)
 //

@@ -352,7 +352,8 @@ typedef struct {
 BN_API void bnxRenderBatch(BNContext context, const BNXRenderJob *jobs, int numJobs);
 BN_API void bnxSetBatchGraphs(BNContext context, int enable);
 /* Times candidate launch shapes and scheduling thresholds on this batch,
-   keeps the fastest for the context and reports it.  The tuning frames are
+   keeps the fastest for the context and reports it (blocksPerSM 0: as many
+   blocks per SM as the batch's kernel fits).  The tuning frames are
    rendered into the jobs' frame buffers and discarded (accumulation reset). */
 typedef struct {
   int threadsPerBlock, blocksPerSM, serviceBatch;
