@@ -56,7 +56,7 @@ EXPORTS = [
     "bnxServerCreate", "bnxServerDestroy", "bnxServerSubmit", "bnxServerWait", "bnxServerGetStats",
     "bnxServerResetStats", "bnxServerReserve", "bnxSetRenderTimeout", "bnxSetPixelPartition",
     "bnxPixelPartitionOwners", "bnxAnariTransferFunction1D", "bnxAnariDensityScale",
-    "bnxAnariStructuredRegular",
+    "bnxAnariStructuredRegular", "bnxAnariRendererParams", "bnxAnariRendererCommit", "bnxAnariRenderFrame",
 ]
 
 
@@ -87,6 +87,41 @@ def anari_transfer_function_1d(colors=None, opacities=None, uniform_color=(1.0, 
     L.bnxAnariTransferFunction1D(_void_p(c), nc, ch, _void_p(o), no, uc, uniform_opacity, out.ctypes.data)
     check()
     return out
+
+
+# ANARI renderer parameters (BNXAnariRenderer; barney/anari/Renderer.cpp:22-37)
+BNX_ANARI_BITS = {"pixelSamples": 0x1, "ambientRadiance": 0x2, "background": 0x4, "cutPlane": 0x8,
+                  "maxVolumeBounces": 0x10, "crosshairs": 0x20}
+
+
+class BNXAnariRenderer(ctypes.Structure):
+    _fields_ = [("set", ctypes.c_uint), ("pixelSamples", ctypes.c_int), ("ambientRadiance", ctypes.c_float),
+                ("background", bn_float4), ("cutPlane", bn_float4), ("maxVolumeBounces", ctypes.c_int),
+                ("crosshairs", ctypes.c_int)]
+
+
+def anari_renderer(**params):
+    """A BNXAnariRenderer with the given ANARI renderer parameters set (the
+    others take the ANARI device's defaults when it is committed)."""
+    p = BNXAnariRenderer()
+    for k, val in params.items():
+        if k not in BNX_ANARI_BITS:
+            raise ValueError(f"unknown ANARI renderer parameter {k!r}")
+        p.set |= BNX_ANARI_BITS[k]
+        setattr(p, k, bn_float4(*val) if k in ("background", "cutPlane") else val)
+    return p
+
+
+def anari_renderer_params(**params):
+    """The parameters an ANARI renderer commit uses: the given ones, the
+    defaults for the rest (bnxAnariRendererParams)."""
+    out = BNXAnariRenderer()
+    lib().bnxAnariRendererParams(ctypes.byref(anari_renderer(**params)), ctypes.byref(out))
+    check()
+    return {"set": out.set, "pixelSamples": out.pixelSamples, "ambientRadiance": out.ambientRadiance,
+            "background": (out.background.x, out.background.y, out.background.z, out.background.w),
+            "cutPlane": (out.cutPlane.x, out.cutPlane.y, out.cutPlane.z, out.cutPlane.w),
+            "maxVolumeBounces": out.maxVolumeBounces, "crosshairs": out.crosshairs}
 
 
 class BNXStats(ctypes.Structure):
@@ -186,6 +221,8 @@ def lib(build_if_missing=True):
         "bnxAnariTransferFunction1D": ([P, I, I, P, I, bn_float4, F, P], I),
         "bnxAnariDensityScale": ([F], F),
         "bnxAnariStructuredRegular": ([P, I, I, P, I, I, I, bn_float3, bn_float3], P),
+        "bnxAnariRendererParams": ([P, P], None), "bnxAnariRendererCommit": ([P, P], None),
+        "bnxAnariRenderFrame": ([P, P, P, P], None),
     }
     for name, (args, res) in sig.items():
         fn = getattr(L, name)
@@ -507,6 +544,17 @@ class VolumeRenderer:
                                1 if fast_math else 0)
         check()
         return scal, rgba
+
+    def anari_commit_renderer(self, **params):
+        """The ANARI renderer's commit (bnxAnariRendererCommit) on this renderer."""
+        self.L.bnxAnariRendererCommit(self.renderer, ctypes.byref(anari_renderer(**params)))
+        check()
+
+    def anari_render_frame(self):
+        """anariRenderFrame (bnxAnariRenderFrame): accumulation starts over
+        after any commit or build of the context since the last frame."""
+        self.L.bnxAnariRenderFrame(self.renderer, self.model, self.camera, self.fb)
+        check()
 
     def set_regrouping(self, enable=True):
         """Regrouped kernel for plain jobs, or the per-lane kernel (default)."""

@@ -548,6 +548,7 @@ BN_API void bnCommit(BNObject target) {
   ObjectSP o = getObject(target);
   o->ctx->activate();
   o->commit();
+  o->ctx->commitEpoch++;
   BN_CATCH()
 }
 
@@ -746,6 +747,7 @@ BN_API void bnVolumeSetXF(BNVolume volume, bn_float2 domain, const bn_float4 *va
   memcpy(v->tfValues.data(), values, n * sizeof(bn_float4));
   v->baseDensity = densityAt1;
   v->needsMajorantRebuild = true;
+  v->ctx->commitEpoch++;
   BN_CATCH()
 }
 
@@ -803,6 +805,7 @@ BN_API void bnGroupBuild(BNGroup group) {
   g->ctx->activate();
   buildGroup(*g);
   ck(cudaStreamSynchronize(g->ctx->stream), "group build");
+  g->ctx->commitEpoch++;
   BN_CATCH()
 }
 
@@ -826,6 +829,7 @@ BN_API void bnSetInstances(BNModel model, int, BNGroup *groups, BNTransform *xfm
     throw Error(E_UNSUPPORTED, "only identity instance transforms are supported");
   m->group = (n == 1 && groups) ? getAs<Group>(groups[0], Object::K_GROUP, "BNGroup") : nullptr;
   m->built = false;
+  m->ctx->commitEpoch++;
   BN_CATCH()
 }
 
@@ -852,6 +856,7 @@ BN_API void bnBuild(BNModel model, int) {
   if (m->group) buildGroup(*m->group);
   ck(cudaStreamSynchronize(m->ctx->stream), "model build");
   m->built = true;
+  m->ctx->commitEpoch++;
   BN_CATCH()
 }
 
@@ -1383,6 +1388,58 @@ BN_API BNScalarField bnxAnariStructuredRegular(BNContext context, int slot, BNDa
   if (g_lastError) return nullptr;
   return sf;
   BN_CATCH(nullptr)
+}
+
+// Renderer::commitParameters, barney/anari/Renderer.cpp:22-37: each
+// parameter the application did not set takes the ANARI device's default.
+BN_API void bnxAnariRendererParams(const BNXAnariRenderer *in, BNXAnariRenderer *out) {
+  BN_TRY
+  if (!out) throw Error(E_INVALID_ARG, "bnxAnariRendererParams: out is NULL");
+  BNXAnariRenderer d{};
+  const unsigned set = in ? in->set : 0u;
+  d.pixelSamples = (set & BNX_ANARI_PIXEL_SAMPLES) ? in->pixelSamples : 1;
+  d.ambientRadiance = (set & BNX_ANARI_AMBIENT_RADIANCE) ? in->ambientRadiance : 1.f;
+  d.background = (set & BNX_ANARI_BACKGROUND) ? in->background : bn_float4{0.f, 0.f, 0.f, 1.f};
+  d.cutPlane = (set & BNX_ANARI_CUT_PLANE) ? in->cutPlane : bn_float4{0.f, 0.f, 0.f, 0.f};
+  d.maxVolumeBounces = (set & BNX_ANARI_MAX_VOLUME_BOUNCES) ? in->maxVolumeBounces : 0;
+  d.crosshairs = (set & BNX_ANARI_CROSSHAIRS) ? (in->crosshairs ? 1 : 0) : 0;
+  d.set = BNX_ANARI_PIXEL_SAMPLES | BNX_ANARI_AMBIENT_RADIANCE | BNX_ANARI_BACKGROUND | BNX_ANARI_CUT_PLANE |
+          BNX_ANARI_MAX_VOLUME_BOUNCES | BNX_ANARI_CROSSHAIRS;
+  *out = d;
+  BN_CATCH()
+}
+
+// Renderer::finalize, barney/anari/Renderer.cpp:40-51 (the background image
+// and the denoiser flags are not mapped: textures and the denoiser are not
+// built)
+BN_API void bnxAnariRendererCommit(BNRenderer renderer, const BNXAnariRenderer *params) {
+  BN_TRY
+  getAs<Renderer>(renderer, Object::K_RENDERER, "BNRenderer");
+  BNXAnariRenderer p;
+  bnxAnariRendererParams(params, &p);
+  bnSet4f(renderer, "bgColor", p.background.x, p.background.y, p.background.z, p.background.w);
+  bnSet1i(renderer, "crosshairs", p.crosshairs);
+  bnSet1i(renderer, "pathsPerPixel", p.pixelSamples);
+  bnSet1f(renderer, "ambientRadiance", p.ambientRadiance);
+  bnSet1i(renderer, "maxVolumeBounces", p.maxVolumeBounces);
+  bnSet4f(renderer, "cutPlane", p.cutPlane.x, p.cutPlane.y, p.cutPlane.z, p.cutPlane.w);
+  if (g_lastError) return;
+  bnCommit(renderer);
+  BN_CATCH()
+}
+
+// Frame::renderFrame, barney/anari/Frame.cpp:172-178 and 226-261: a frame
+// after any object finalization (here: any commit or build of the context)
+// starts its accumulation over
+BN_API void bnxAnariRenderFrame(BNRenderer renderer, BNModel model, BNCamera camera, BNFrameBuffer frameBuffer) {
+  BN_TRY
+  auto fb = getAs<FrameBuffer>(frameBuffer, Object::K_FB, "BNFrameBuffer");
+  if (fb->anariFrameEpoch != fb->ctx->commitEpoch) {
+    fb->accumID = 0;
+    fb->anariFrameEpoch = fb->ctx->commitEpoch;
+  }
+  bnRender(renderer, model, camera, frameBuffer);
+  BN_CATCH()
 }
 
 }  // extern "C"

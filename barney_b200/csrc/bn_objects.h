@@ -415,6 +415,7 @@ struct FrameBuffer : Object {
   int width = 0, height = 0;
   int colorFormat = FMT_RGBA8;
   uint32_t accumID = 0;
+  uint64_t anariFrameEpoch = ~0ull;  // the context's commitEpoch at this buffer's last bnxAnariRenderFrame
   DeviceBuffer accum, color, comp;
   explicit FrameBuffer(Context *c) : Object(c, K_FB) {}
 };
@@ -440,6 +441,7 @@ struct Context {
   int hostCapacity = 0;
   bool useGraphs = true;
   int timeoutMs = 0;                 // render deadline (0: none)
+  uint64_t commitEpoch = 0;          // commits and builds so far (bnxAnariRenderFrame)
   int partRank = 0, partCount = 1;   // pixel-tile partition (bnxSetPixelPartition)
   cudaStream_t abortStream = nullptr;
   cudaGraphExec_t graphExec = nullptr;

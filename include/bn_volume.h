@@ -507,6 +507,39 @@ BN_API BNScalarField bnxAnariStructuredRegular(BNContext context, int slot, BNDa
                                                const void *data, int nx, int ny, int nz, bn_float3 origin,
                                                bn_float3 spacing);
 
+/* ANARI "renderer" parameters (Renderer.cpp:22-37).  set: the BNX_ANARI_*
+   bits of the parameters the application set; the others take the ANARI
+   device's defaults. */
+#define BNX_ANARI_PIXEL_SAMPLES 0x1u
+#define BNX_ANARI_AMBIENT_RADIANCE 0x2u
+#define BNX_ANARI_BACKGROUND 0x4u
+#define BNX_ANARI_CUT_PLANE 0x8u
+#define BNX_ANARI_MAX_VOLUME_BOUNCES 0x10u
+#define BNX_ANARI_CROSSHAIRS 0x20u
+typedef struct {
+  unsigned set;
+  int pixelSamples;       /* default 1 */
+  float ambientRadiance;  /* default 1 */
+  bn_float4 background;   /* default (0, 0, 0, 1) */
+  bn_float4 cutPlane;     /* default (0, 0, 0, 0): a zero normal clips nothing */
+  int maxVolumeBounces;   /* default 0 */
+  int crosshairs;         /* default 0 (accepted; the debug overlay is not built) */
+} BNXAnariRenderer;
+/* Fills the parameters in that are not set with the defaults
+   (Renderer::commitParameters); out->set has every bit. */
+BN_API void bnxAnariRendererParams(const BNXAnariRenderer *in, BNXAnariRenderer *out);
+/* What the ANARI renderer's commit does to the Barney renderer
+   (Renderer::finalize, Renderer.cpp:40-51): the parameters, with their
+   defaults, as bgColor, crosshairs, pathsPerPixel, ambientRadiance,
+   maxVolumeBounces and cutPlane, then bnCommit. */
+BN_API void bnxAnariRendererCommit(BNRenderer renderer, const BNXAnariRenderer *params);
+/* anariRenderFrame (Frame::renderFrame, Frame.cpp:165-262): if any object of
+   the context was committed or built (bnCommit, bnGroupBuild, bnBuild,
+   bnSetInstances, bnVolumeSetXF) since this frame buffer's last frame --
+   or this is its first frame -- its accumulation starts over
+   (bnAccumReset); then bnRender. */
+BN_API void bnxAnariRenderFrame(BNRenderer renderer, BNModel model, BNCamera camera, BNFrameBuffer frameBuffer);
+
 #ifdef __cplusplus
 }
 #endif

@@ -53,3 +53,35 @@ def test_density_scale():
     assert L.bnxAnariDensityScale(0.5) == 2.0
     assert L.bnxAnariDensityScale(0.0) == 1.0
     assert L.bnxAnariDensityScale(-3.0) == 1.0
+
+
+# Renderer::commitParameters (barney/anari/Renderer.cpp:22-37): the value of
+# each parameter the application did not set
+ANARI_RENDERER_DEFAULTS = {"pixelSamples": 1, "ambientRadiance": 1.0, "background": (0.0, 0.0, 0.0, 1.0),
+                           "cutPlane": (0.0, 0.0, 0.0, 0.0), "maxVolumeBounces": 0, "crosshairs": 0}
+
+
+def test_renderer_defaults():
+    got = bn.anari_renderer_params()
+    assert got.pop("set") == 0x3F
+    assert got == ANARI_RENDERER_DEFAULTS
+
+
+@pytest.mark.parametrize("mask", range(64))
+def test_renderer_parameters_set_and_default(mask):
+    rng = np.random.default_rng(mask)
+    values = {"pixelSamples": int(rng.integers(1, 64)), "ambientRadiance": float(f32(rng.random())),
+              "background": tuple(float(x) for x in rng.random(4).astype(np.float32)),
+              "cutPlane": tuple(float(x) for x in (rng.random(4) - 0.5).astype(np.float32)),
+              "maxVolumeBounces": int(rng.integers(0, 9)), "crosshairs": 1}
+    names = list(ANARI_RENDERER_DEFAULTS)
+    given = {k: values[k] for i, k in enumerate(names) if mask >> i & 1}
+    got = bn.anari_renderer_params(**given)
+    assert got.pop("set") == 0x3F
+    want = dict(ANARI_RENDERER_DEFAULTS, **given)
+    assert got == want
+
+
+def test_renderer_unknown_parameter_is_refused():
+    with pytest.raises(ValueError):
+        bn.anari_renderer(denoise=True)
