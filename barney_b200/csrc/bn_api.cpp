@@ -377,6 +377,7 @@ void renderBatch(Context *ctx, const std::vector<BatchEntry> &entries) {
   long long chunks = 0;
   unsigned long long pixelSamples = 0;
   int extended = 0;  // 1: multi-scatter, principled or exact log; 2: isosurfaces (the extended kernels)
+  bool anyIso = false, anyPvms = false;
   int voxelType = -2;     // the type every job shares, else -1
   bool fast = true;       // every job asks for the fast-math kernels
   int compJobs = 0;  // jobs that keep compensation terms
@@ -387,6 +388,8 @@ void renderBatch(Context *ctx, const std::vector<BatchEntry> &entries) {
     if (job.fr.spp <= 0) throw Error(E_INVALID_ARG, "every batch job needs pathsPerPixel >= 1");
     extended = std::max(extended, job.v.iso.enabled ? 2
                                   : (job.fr.maxVolumeBounces > 0 || job.v.pv.enabled || job.fr.exactLog) ? 1 : 0);
+    anyIso = anyIso || job.v.iso.enabled;
+    anyPvms = anyPvms || job.fr.maxVolumeBounces > 0 || job.v.pv.enabled;
     voxelType = voxelType == -2 || voxelType == job.v.type ? job.v.type : -1;
     fast = fast && job.fr.fastMath;
     compJobs += job.fr.comp != nullptr;
@@ -403,6 +406,8 @@ void renderBatch(Context *ctx, const std::vector<BatchEntry> &entries) {
   key.push_back((const void *)(intptr_t)(ctx->blocksPerSM * 4096 + ctx->threadsPerBlock));
   key.push_back((const void *)(intptr_t)ctx->sched.serviceBatch);
   key.push_back((const void *)(intptr_t)n);
+  // isosurfaces without volume bounces or principled volumes: the smaller kernel
+  if (anyIso && !anyPvms) extended = 3;
   key.push_back((const void *)(intptr_t)extended);
   key.push_back((const void *)(intptr_t)voxelType);
   fast = fast && extended == 0;  // the fast-math object holds the plain kernels only

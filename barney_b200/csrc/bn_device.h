@@ -135,9 +135,11 @@ cudaError_t launchRender(const VolumeDD &vol, const FrameDD &frame, LaunchCounte
                          int threadsPerBlock, cudaStream_t s, const SchedDD &sd = SchedDD());
 // jobs / chunkStart: device arrays; chunkStart has numJobs+1 entries, the
 // prefix sum of each job's ceil(width*height/32) pixel chunks.
-// extended: 2 if some job has an isosurface, else 1 if some job has
-// fr.maxVolumeBounces > 0, a principled volume or exact-log free flight,
-// else 0 (selects the kernel instantiation that implements them); voxelType: the
+// extended: 2 if some job has an isosurface and some job volume bounces
+// (fr.maxVolumeBounces > 0) or a principled volume, 3 if some job has an
+// isosurface and none has either, else 1 if some job has volume bounces, a
+// principled volume or exact-log free flight, else 0 (selects the kernel
+// instantiation that implements them); voxelType: the
 // VoxelType all jobs share (a kernel compiled for it) or -1 (mixed);
 // compensated: how many jobs carry compensation terms (fr.comp): 0 none,
 // 1 some, 2 all

@@ -668,6 +668,10 @@ static constexpr float kTwoPi = 2.f * ONE_PI_F;
 static constexpr float kOneOverPi = 1.f / ONE_PI_F;
 static constexpr float kOneOverTwoPi = 1.f / kTwoPi;
 
+// (float)i / 10.f for i = 0..10, each the correctly rounded quotient (the
+// literals below are those quotients)
+__constant__ float kIsoTenths[11] = {0.f, .1f, .2f, .3f, .4f, .5f, .6f, .7f, .8f, .9f, 1.f};
+
 // The isosurface's intersection program for one ray: box test, its own RNG
 // derived from the ray's seed (which this advances), a DDA over the
 // macrocell scalar ranges and, in every macrocell whose range holds the iso
@@ -732,10 +736,13 @@ DEV float isoIntersect(const VolumeDD &v, float3 org, float3 dir, float tMax, ui
         float tt1 = ct0;
         float ff1 = sampleJob<T>(v, f3(org.x + tt1 * dir.x, org.y + tt1 * dir.y, org.z + tt1 * dir.z), u8lut);
         bool done = false;
+        // one copy of the sampler for the ten steps (not unrolled: the
+        // unrolled scan held ten, a large share of this kernel's code)
+#pragma unroll 1
         for (int i = 1; i <= 10; i++) {
           const float tt0 = tt1;
           const float ff0 = ff1;
-          const float fi = (float)i / 10.f;
+          const float fi = kIsoTenths[i];  // (float)i / 10.f
           tt1 = (1.f - fi) * ct0 + fi * ct1;
           ff1 = sampleJob<T>(v, f3(org.x + tt1 * dir.x, org.y + tt1 * dir.y, org.z + tt1 * dir.z), u8lut);
           if (isnan(ff0) || isnan(ff1)) continue;
@@ -767,20 +774,29 @@ template <int T>
 __device__ __noinline__ float3 isoNormal(const VolumeDD &v, float3 P, float3 dir, const float *u8lut) {
   const float dl = v.iso.normalDelta;
   const float fP = sampleJob<T>(v, P, u8lut);
-  float fx0 = sampleJob<T>(v, f3(P.x + -dl, P.y + 0.f, P.z + 0.f), u8lut);
-  float fx1 = sampleJob<T>(v, f3(P.x + dl, P.y + 0.f, P.z + 0.f), u8lut);
-  float fy0 = sampleJob<T>(v, f3(P.x + 0.f, P.y + -dl, P.z + 0.f), u8lut);
-  float fy1 = sampleJob<T>(v, f3(P.x + 0.f, P.y + dl, P.z + 0.f), u8lut);
-  float fz0 = sampleJob<T>(v, f3(P.x + 0.f, P.y + 0.f, P.z + -dl), u8lut);
-  float fz1 = sampleJob<T>(v, f3(P.x + 0.f, P.y + 0.f, P.z + dl), u8lut);
-  float dx = 2.f, dy = 2.f, dz = 2.f;
-  if (isnan(fx0)) { dx -= 1.f; fx0 = fP; }
-  if (isnan(fx1)) { dx -= 1.f; fx1 = fP; }
-  if (isnan(fy0)) { dy -= 1.f; fy0 = fP; }
-  if (isnan(fy1)) { dy -= 1.f; fy1 = fP; }
-  if (isnan(fz0)) { dz -= 1.f; fz0 = fP; }
-  if (isnan(fz1)) { dz -= 1.f; fz1 = fP; }
-  float3 n = f3(dx == 0.f ? 0.f : (fx1 - fx0) / dx, dy == 0.f ? 0.f : (fy1 - fy0) / dy, dz == 0.f ? 0.f : (fz1 - fz0) / dz);
+  // central differences: samples at P -/+ dl along x, then y, then z (one
+  // copy of the sampler in a loop); an axis whose sample is NaN (outside the
+  // field) uses fP instead and halves its step count
+  float3 n = f3(0.f, 0.f, 0.f);
+  float fLo = 0.f;
+#pragma unroll 1
+  for (int i = 0; i < 6; i++) {
+    const int axis = i >> 1;
+    const float o = (i & 1) ? dl : -dl;
+    const float fv = sampleJob<T>(v, f3(P.x + (axis == 0 ? o : 0.f), P.y + (axis == 1 ? o : 0.f),
+                                        P.z + (axis == 2 ? o : 0.f)), u8lut);
+    if (!(i & 1)) {
+      fLo = fv;
+      continue;
+    }
+    float f0 = fLo, f1 = fv, d = 2.f;
+    if (isnan(f0)) { d -= 1.f; f0 = fP; }
+    if (isnan(f1)) { d -= 1.f; f1 = fP; }
+    const float c = d == 0.f ? 0.f : (f1 - f0) / d;
+    if (axis == 0) n.x = c;
+    else if (axis == 1) n.y = c;
+    else n.z = c;
+  }
   if (n.x == 0.f && n.y == 0.f && n.z == 0.f) {
     const float3 dn = normalize3(dir);
     n = f3(-dn.x, -dn.y, -dn.z);
@@ -969,7 +985,8 @@ __device__ __noinline__ SurfaceBounce surfaceBounce(const VolumeDD &v, const Fra
 // kernel (a job table in global memory, chunks of all jobs in one counter).
 // LOG: 0 fastLog (Volume.h:154-164), 1 -logf (bnx.exactLog), 2 per job (batch)
 // EXT: 0 the plain kernels; 1 multi-scatter paths and principled volumes;
-// 2 also isosurfaces (ISO)
+// 2 also isosurfaces (ISO); 3 isosurfaces (with their diffuse bounce)
+// without volume bounces or principled volumes
 // CMP: compensated sums (fr.comp) in no job (0: compiled out), in the jobs
 // that carry terms (1: a test per sum), or in every job (2)
 template <int T, bool BATCH, int LOG, int EXT, int CMP>
@@ -978,6 +995,7 @@ DEV void renderLoop(const JobDD *__restrict__ jobs, const int *__restrict__ chun
   const unsigned FULL = 0xffffffffu;
   const int lane = threadIdx.x & 31;
   constexpr bool ISO = EXT >= 2;
+  constexpr bool PVMS = EXT == 1 || EXT == 2;  // principled volumes and volume bounces compiled in
 
   // lane work counters, 32-bit, flushed to the launch counters (below)
   unsigned nSamples = 0, nVisits = 0, nRays = 0;
@@ -1069,7 +1087,7 @@ DEV void renderLoop(const JobDD *__restrict__ jobs, const int *__restrict__ chun
           float hitAlb = v.scatteringAlbedo;
           if (EXT) {
             float3 frag = f3(0.f, 0.f, 0.f);
-            if (v.phase == PHASE_HG && v.pv.enabled && !fr.emissionAbsorption && !surf) {
+            if (PVMS && v.phase == PHASE_HG && v.pv.enabled && !fr.emissionAbsorption && !surf) {
               float3 e;
               principledAtHit<T>(v, P, BATCH ? v.tf : sTF, u8lut, tint, hitAlb, e);
               // emission of the HGPhase hit: incomingThroughput * emission (shadeRays.cu:613-617)
@@ -1203,7 +1221,7 @@ DEV void renderLoop(const JobDD *__restrict__ jobs, const int *__restrict__ chun
             // end the path here (the reference re-traces the old ray); with
             // anisotropy clamped to [-0.99, 0.99] (Volume.cpp:55-57) the HG
             // pdf stays above 2e-4, so neither can happen.
-            if (EXT && fr.maxVolumeBounces > 0 && depth < kMaxPathDepth) {
+            if (PVMS && fr.maxVolumeBounces > 0 && depth < kMaxPathDepth) {
               const float3 wi_in = normalize3(f3(-woN.x, -woN.y, -woN.z));
               const float3 sdir = hgSampleDirection(wi_in, v.anisotropy, random);
               const float pdf = hgPhase(v.anisotropy, dot3(wi_in, sdir));
@@ -1530,7 +1548,7 @@ DEV void renderLoop(const JobDD *__restrict__ jobs, const int *__restrict__ chun
               const float w0 = BATCH ? __ldg(&v.tf[idx].w) : sTF[idx].w;
               const float w1 = BATCH ? __ldg(&v.tf[idx + 1].w) : sTF[idx + 1].w;
               w = __fmul_rn(lerp_l(f, w0, w1), v.baseDensity);
-              if (EXT) {  // principled volume (Volume.h:66-72): density sigma_t times the TF's
+              if (PVMS) {  // principled volume (Volume.h:66-72): density sigma_t times the TF's
                 tfw = w;
                 if (v.pv.enabled) w = tfw <= 0.f ? 0.f : principledSigmaT(v.pv, s) * tfw;
               }
@@ -1539,11 +1557,11 @@ DEV void renderLoop(const JobDD *__restrict__ jobs, const int *__restrict__ chun
               if (ISO) ts.bits &= ~64;  // a volume collision before the surface
               // (with isosurfaces a shadow ray keeps hitRGB: it may hold a waiting ray's origin)
               if (!(ISO && shadowRay)) hitRGB = f3(0.f, 0.f, 0.f);
-              if (!(ISO && shadowRay) && !isnan(s) && !((EXT && v.pv.enabled) && tfw <= 0.f)) {
+              if (!(ISO && shadowRay) && !isnan(s) && !((PVMS && v.pv.enabled) && tfw <= 0.f)) {
                 const float4 a = BATCH ? __ldg(&v.tf[idx]) : sTF[idx];
                 const float4 b = BATCH ? __ldg(&v.tf[idx + 1]) : sTF[idx + 1];
                 hitRGB = f3(lerp_l(f, a.x, b.x), lerp_l(f, a.y, b.y), lerp_l(f, a.z, b.z));
-                if ((EXT && v.pv.enabled)) hitRGB = principledTintTimes(v.pv, s, hitRGB);
+                if ((PVMS && v.pv.enabled)) hitRGB = principledTintTimes(v.pv, s, hitRGB);
               }
               phase = LP_HIT;
             }
@@ -2450,7 +2468,8 @@ template <int T>
 static cudaError_t launchRenderT(const VolumeDD &v, const FrameDD &fr, const SchedDD &sd, LaunchCounters *ctr,
                                  int bps, int tpb, cudaStream_t s) {
   const size_t smem = (size_t)v.tfN * sizeof(float4);
-  const int ext = v.iso.enabled ? 2 : (fr.maxVolumeBounces > 0 || v.pv.enabled) ? 1 : 0;
+  const bool pvms = fr.maxVolumeBounces > 0 || v.pv.enabled;
+  const int ext = v.iso.enabled ? (pvms ? 2 : 3) : pvms ? 1 : 0;
   // kernels with and without compensated sums
   const bool cmp = fr.comp != nullptr;
 #ifdef BNB_FAST_MATH
@@ -2458,8 +2477,11 @@ static cudaError_t launchRenderT(const VolumeDD &v, const FrameDD &fr, const Sch
   auto kern = cmp ? (fr.exactLog ? renderKernel<T, 1, 0, 2> : renderKernel<T, 0, 0, 2>)
                   : (fr.exactLog ? renderKernel<T, 1, 0, 0> : renderKernel<T, 0, 0, 0>);
 #else
-  auto kern = ext == 2 ? (cmp ? (fr.exactLog ? renderKernel<T, 1, 2, 2> : renderKernel<T, 0, 2, 2>)
-                              : (fr.exactLog ? renderKernel<T, 1, 2, 0> : renderKernel<T, 0, 2, 0>))
+  // isosurfaces without volume bounces or principled volumes: the smaller
+  // EXT 3 kernel unless the job keeps compensated sums
+  auto kern = ext == 3 && !cmp ? (fr.exactLog ? renderKernel<T, 1, 3, 0> : renderKernel<T, 0, 3, 0>)
+              : ext >= 2 ? (cmp ? (fr.exactLog ? renderKernel<T, 1, 2, 2> : renderKernel<T, 0, 2, 2>)
+                                : (fr.exactLog ? renderKernel<T, 1, 2, 0> : renderKernel<T, 0, 2, 0>))
               : ext == 1 ? (cmp ? (fr.exactLog ? renderKernel<T, 1, 1, 2> : renderKernel<T, 0, 1, 2>)
                                 : (fr.exactLog ? renderKernel<T, 1, 1, 0> : renderKernel<T, 0, 1, 0>))
               : cmp ? (fr.exactLog ? renderKernel<T, 1, 0, 2> : renderKernel<T, 0, 0, 2>)
@@ -2541,7 +2563,8 @@ cudaError_t launchRenderBatch(const JobDD *jobs, const int *chunkStart, int numJ
               : compensated == 1 ? batchKernelFor<0, 1>(voxelType)
                                  : batchKernelFor<0, 0>(voxelType);
 #else
-  auto kern = extended >= 2      ? (compensated ? batchKernelFor<2, 1>(voxelType) : batchKernelFor<2, 0>(voxelType))
+  auto kern = extended == 3 && !compensated ? batchKernelFor<3, 0>(voxelType)
+              : extended >= 2    ? (compensated ? batchKernelFor<2, 1>(voxelType) : batchKernelFor<2, 0>(voxelType))
               : extended         ? (compensated ? batchKernelFor<1, 1>(voxelType) : batchKernelFor<1, 0>(voxelType))
               : compensated == 2 ? batchKernelFor<0, 2>(voxelType)
               : compensated == 1 ? batchKernelFor<0, 1>(voxelType)

@@ -72,7 +72,7 @@ def test_kernels_compiled_for_sm100a():
     # The plain single-frame render kernels are capped at 7 blocks of 128
     # threads per SM (72 registers), the plain batch and compensated ones at 6
     # (80), the extended ones at 5 (96); the spill bytes that costs are a
-    # measured trade for the extra blocks (the isosurface kernels, EXT 2,
+    # measured trade for the extra blocks (the isosurface kernels, EXT 2 and 3,
     # spill most and still run 3 % faster at 5 blocks than at 4).  A large
     # spill would mean a regression.
     blocks = log.split("Function properties for ")
@@ -84,7 +84,7 @@ def test_kernels_compiled_for_sm100a():
         # template arguments: renderKernel<T, LOG, EXT, CMP>, renderBatchKernel<T, EXT, CMP>
         args = re.findall(r"Li(n?\d+)E", name.split("EEEv")[0])
         ext = int(args[2] if "renderKernel" in name.split("I")[0] else args[1])
-        assert m and int(m.group(1)) <= (700 if ext == 2 else 320), b.splitlines()[1]
+        assert m and int(m.group(1)) <= (700 if ext >= 2 else 320), b.splitlines()[1]
 
 
 def test_header_compiles_as_c_and_shim_as_cpp(tmp_path):
