@@ -212,6 +212,7 @@ JobDD buildJob(Context *ctx, Renderer &r, Model &m, Camera &cam, FrameBuffer &fb
   fr.lens00 = F3(cam.lens00);
   fr.width = fb.width;
   fr.height = fb.height;
+  fr.aspect = (float)fr.width / (float)fr.height;  // generateRays.cu: W / float(H)
   fr.bgColor = p.bgColor;
   fr.ambientRadiance = p.ambientRadiance;
   fr.cutPlane = p.cutPlane;
@@ -223,6 +224,7 @@ JobDD buildJob(Context *ctx, Renderer &r, Model &m, Camera &cam, FrameBuffer &fb
       fr.dirLights[fr.numDirLights++] = std::static_pointer_cast<DirLight>(o)->dd();
     }
   }
+  fr.dirLightPick = fr.numDirLights > 0 ? 2.f / (float)fr.numDirLights : 0.f;
   fr.emissionAbsorption = p.emissionAbsorption;
   fr.exactLog = p.exactLog;
   fr.fastMath = p.fastMath;
@@ -1178,6 +1180,7 @@ BN_API int bnxRenderStructuredNoAlloc(const BNXNoAllocFrame *f, void *stream) {
   fr.lens00 = F3(cam.lens00);
   fr.width = f->width;
   fr.height = f->height;
+  fr.aspect = (float)fr.width / (float)fr.height;
   fr.bgColor = make_float4(f->bgColor.x, f->bgColor.y, f->bgColor.z, f->bgColor.w);
   fr.ambientRadiance = f->ambientRadiance;
   fr.cutPlane = make_float4(0.f, 0.f, 0.f, -1e30f);
@@ -1190,6 +1193,7 @@ BN_API int bnxRenderStructuredNoAlloc(const BNXNoAllocFrame *f, void *stream) {
     l.set3f("color", L[4], L[5], L[6]);
     fr.dirLights[i] = l.dd();
   }
+  fr.dirLightPick = fr.numDirLights > 0 ? 2.f / (float)fr.numDirLights : 0.f;
   fr.accum = (float4 *)f->accum;
   fr.accumID0 = f->accumID;
   fr.spp = f->pathsPerPixel;

@@ -83,10 +83,12 @@ struct DirLightDD {
 struct FrameDD {
   float3 dir00, dirdu, dirdv, lens00;   // PerspectiveCamera::commit, Camera.cu:82-100
   int width, height;
+  float aspect;          // width / (float)height, the one IEEE quotient _generateRays forms per ray
   float4 bgColor;
   float ambientRadiance;
   float4 cutPlane;
   int numDirLights;
+  float dirLightPick;    // 2.f / float(numDirLights) (shadeRays.cu's reservoir of two), 0 without lights
   DirLightDD dirLights[kMaxDirLights];
   int emissionAbsorption;
   int exactLog;

@@ -588,7 +588,7 @@ DEV bool sampleLights(const FrameDD &fr, uint64_t &random, LightSample &ls, bool
       if (i < 2) {
         const DirLightDD &L = fr.dirLights[lID[i]];
         dDir = L.toLight;
-        const float den = w[i] / sumW * (2.f / float(fr.numDirLights));
+        const float den = w[i] / sumW * fr.dirLightPick;  // (2.f / float(numDirLights)), formed on the host
         dRad = f3(L.color.x * L.radiance * 1.f / den, L.color.y * L.radiance * 1.f / den,
                   L.color.z * L.radiance * 1.f / den);
         if (w[i] != 0.f) dlsWeight = fmax_(fmax_(dRad.x, dRad.y), dRad.z);
@@ -1179,8 +1179,14 @@ DEV void renderLoop(const JobDD *__restrict__ jobs, const int *__restrict__ chun
               } else {
                 const float a = EXT ? hitAlb : v.scatteringAlbedo;  // plain kernels read it here, not earlier
                 alb = f3(a * tint.x, a * tint.y, a * tint.z);
-                const float3 wi_in = normalize3(f3(-woN.x, -woN.y, -woN.z));
-                fpdf = hgPhase(v.anisotropy, dot3(wi_in, normalize3(ls.dir)));
+                // HGPhase::pdf (Phase.h:51-58) is 1/4pi for |g| < 1e-3 whatever the
+                // angle: the directions are normalised only when it is not
+                if (fabsf(v.anisotropy) < 1e-3f) {
+                  fpdf = kOneOverFourPi;
+                } else {
+                  const float3 wi_in = normalize3(f3(-woN.x, -woN.y, -woN.z));
+                  fpdf = hgPhase(v.anisotropy, dot3(wi_in, normalize3(ls.dir)));
+                }
               }
               float3 fv = f3(fpdf * alb.x, fpdf * alb.y, fpdf * alb.z);
               if (fpdf > 0.f && !(fmax_(fmax_(fv.x, fv.y), fv.z) < 1e-4f)) {
@@ -1425,7 +1431,7 @@ DEV void renderLoop(const JobDD *__restrict__ jobs, const int *__restrict__ chun
         const float pixel_v = (accumID == 0) ? .5f : rngFloat(rnd);
         const float image_u = ((ix + pixel_u) / float(W));
         const float image_v = ((iy + pixel_v) / float(H));
-        const float aspect = W / float(H);
+        const float aspect = fr.aspect;  // W / float(H), formed on the host
         const float su = 1.f * aspect * (image_u - .5f), sv = 1.f * (image_v - .5f);
         float3 d = f3(fr.dir00.x + su * fr.dirdu.x + sv * fr.dirdv.x, fr.dir00.y + su * fr.dirdu.y + sv * fr.dirdv.y,
                       fr.dir00.z + su * fr.dirdu.z + sv * fr.dirdv.z);
@@ -2102,8 +2108,14 @@ __global__ void __launch_bounds__(kAQThreads, kAQMinBlocks)
               } else {
                 const float a = v.scatteringAlbedo;
                 alb = f3(a * hitRGB.x, a * hitRGB.y, a * hitRGB.z);
-                const float3 wi_in = normalize3(f3(-woN.x, -woN.y, -woN.z));
-                fpdf = hgPhase(v.anisotropy, dot3(wi_in, normalize3(ls.dir)));
+                // HGPhase::pdf (Phase.h:51-58) is 1/4pi for |g| < 1e-3 whatever the
+                // angle: the directions are normalised only when it is not
+                if (fabsf(v.anisotropy) < 1e-3f) {
+                  fpdf = kOneOverFourPi;
+                } else {
+                  const float3 wi_in = normalize3(f3(-woN.x, -woN.y, -woN.z));
+                  fpdf = hgPhase(v.anisotropy, dot3(wi_in, normalize3(ls.dir)));
+                }
               }
               float3 fv = f3(fpdf * alb.x, fpdf * alb.y, fpdf * alb.z);
               if (fpdf > 0.f && !(fmax_(fmax_(fv.x, fv.y), fv.z) < 1e-4f)) {
@@ -2189,7 +2201,7 @@ __global__ void __launch_bounds__(kAQThreads, kAQMinBlocks)
         const float pixel_v = (accumID == 0) ? .5f : rngFloat(rnd);
         const float image_u = ((px + pixel_u) / float(W));
         const float image_v = ((py + pixel_v) / float(H));
-        const float aspect = W / float(H);
+        const float aspect = fr.aspect;  // W / float(H), formed on the host
         const float su = 1.f * aspect * (image_u - .5f), sv = 1.f * (image_v - .5f);
         float3 d = f3(fr.dir00.x + su * fr.dirdu.x + sv * fr.dirdv.x, fr.dir00.y + su * fr.dirdu.y + sv * fr.dirdv.y,
                       fr.dir00.z + su * fr.dirdu.z + sv * fr.dirdv.z);
