@@ -439,6 +439,13 @@ void renderBatch(Context *ctx, const std::vector<BatchEntry> &entries) {
        "chunk table");
     ck(cudaMemsetAsync(ctx->dCounters, 0, sizeof(LaunchCounters), s), "counter reset");
     if (timed) ck(cudaEventRecord(ctx->ev[0], s), "event");
+    const int compMode = compJobs == 0 ? 0 : compJobs == n ? 2 : 1;
+    if (!ctx->useGraphs && extended == 0 && n <= kParamJobs)  // the jobs as one kernel parameter
+      ck((fast ? fastmath::launchRenderBatchParams : launchRenderBatchParams)(
+             ctx->hostJobs, ctx->hostChunks, n, ctx->dCounters, ctx->blocksPerSM, ctx->threadsPerBlock, s, ctx->sched,
+             voxelType, compMode),
+         "batch render kernel");
+    else
     ck((fast ? fastmath::launchRenderBatch : launchRenderBatch)((const JobDD *)ctx->batchJobs.ptr,
                                                                 (const int *)ctx->batchChunks.ptr, n, ctx->dCounters,
                                                                 ctx->blocksPerSM, ctx->threadsPerBlock, s, ctx->sched,

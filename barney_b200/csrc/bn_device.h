@@ -18,9 +18,9 @@ constexpr int kCellsPerMC = 8;  // StructuredData.cu:26
 constexpr long long kMaxFramePixels = 0x7fffffffLL;  // pixels of one frame (32-bit pixel / chunk indices)
 constexpr int kPartTileChunks = 32;    // pixel-tile partition: 32 chunks of 32 pixels per tile
 constexpr int kRenderMaxThreads = 128;  // __launch_bounds__ of the render kernels:
-constexpr int kRenderMinBlocks = 7;     // plain single-frame: 7 x 128 threads per SM (at most 73 registers)
-constexpr int kRenderMinBlocksBatch = 6;  // plain batch and compensated single-frame: 6 x 128 (85; at 7 the
-                                          // compensated kernels spill 140-364 B)
+constexpr int kRenderMinBlocks = 7;     // plain: 7 x 128 threads per SM (at most 73 registers)
+constexpr int kRenderMinBlocksMixedComp = 6;  // plain, compensated sums tested per job (mixed batches):
+                                              // 6 x 128 (85; at 7 they spill up to 348 B)
 constexpr int kRenderMinBlocksExt = 5;  // extended (multi-scatter, principled): 5 x 128 (102)
 constexpr int kRenderMinBlocksIso = 5;  // extended with isosurfaces: 5 x 128 (102; 3 % faster than 4 x 128)
 
@@ -148,6 +148,13 @@ cudaError_t launchRender(const VolumeDD &vol, const FrameDD &frame, LaunchCounte
 cudaError_t launchRenderBatch(const JobDD *jobs, const int *chunkStart, int numJobs, LaunchCounters *counters,
                               int blocksPerSM, int threadsPerBlock, cudaStream_t s, const SchedDD &sd = SchedDD(),
                               int extended = 0, int voxelType = -1, int compensated = 1);
+// The same for at most kParamJobs plain jobs (extended 0) whose table and
+// chunk prefix are in host memory: passed as one kernel parameter.  Not for
+// stream capture (the parameter would be frozen into the graph).
+constexpr int kParamJobs = 32;
+cudaError_t launchRenderBatchParams(const JobDD *hostJobs, const int *hostChunkStart, int numJobs,
+                                    LaunchCounters *counters, int blocksPerSM, int threadsPerBlock, cudaStream_t s,
+                                    const SchedDD &sd, int voxelType, int compensated);
 cudaError_t launchResolve(const float4 *accum, int numPixels, int accumID, int fmt, void *out, cudaStream_t s,
                           const float4 *comp = nullptr);
 // resolves every job of a batch table into its fr.color after its waves
@@ -185,6 +192,9 @@ cudaError_t launchRender(const VolumeDD &vol, const FrameDD &frame, LaunchCounte
 cudaError_t launchRenderBatch(const JobDD *jobs, const int *chunkStart, int numJobs, LaunchCounters *counters,
                               int blocksPerSM, int threadsPerBlock, cudaStream_t s, const SchedDD &sd = SchedDD(),
                               int extended = 0, int voxelType = -1, int compensated = 1);
+cudaError_t launchRenderBatchParams(const JobDD *hostJobs, const int *hostChunkStart, int numJobs,
+                                    LaunchCounters *counters, int blocksPerSM, int threadsPerBlock, cudaStream_t s,
+                                    const SchedDD &sd, int voxelType, int compensated);
 cudaError_t launchSampleProbe(const VolumeDD &vol, const float3 *P, int n, float *scalar, float4 *rgba, cudaStream_t s);
 cudaError_t launchRenderRegrouped(const VolumeDD &vol, const FrameDD &frame, LaunchCounters *counters, cudaStream_t s);
 long long readBoundsViolationsHere();  // bounds-checked build only

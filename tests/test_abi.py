@@ -69,9 +69,9 @@ def test_kernels_compiled_for_sm100a():
     log = open(os.path.join(ROOT, "barney_b200", "csrc", "ptxas.log")).read()
     assert "for 'sm_100a'" in log
     assert "renderKernel" in log
-    # The plain single-frame render kernels are capped at 7 blocks of 128
-    # threads per SM (72 registers), the plain batch and compensated ones at 6
-    # (80), the extended ones at 5 (96); the spill bytes that costs are a
+    # The plain render kernels are capped at 7 blocks of 128 threads per SM
+    # (72 registers), those that test compensation per job at 6 (80), the
+    # extended ones at 5 (96); the spill bytes that costs are a
     # measured trade for the extra blocks (the isosurface kernels, EXT 2 and 3,
     # spill most and still run 3 % faster at 5 blocks than at 4).  A large
     # spill would mean a regression.
@@ -82,7 +82,7 @@ def test_kernels_compiled_for_sm100a():
         name = b.split()[0]
         m = re.search(r"(\d+) bytes spill stores", b)
         # template arguments: renderKernel<T, LOG, EXT, CMP>, renderBatchKernel<T, EXT, CMP>
-        args = re.findall(r"Li(n?\d+)E", name.split("EEEv")[0])
+        args = re.findall(r"Li(n?\d+)E", name.split("EEv")[0])
         ext = int(args[2] if "renderKernel" in name.split("I")[0] else args[1])
         assert m and int(m.group(1)) <= (700 if ext >= 2 else 320), b.splitlines()[1]
 
