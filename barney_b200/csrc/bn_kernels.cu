@@ -681,85 +681,150 @@ __constant__ float kIsoTenths[11] = {0.f, .1f, .2f, .3f, .4f, .5f, .6f, .7f, .8f
 // dir: the ray direction after the zero fix-up; tMax: the ray's tMax.
 // Returns tHit < tMax on a hit, else tMax; *seed is the ray's RNG seed,
 // advanced when the box test passes.
-template <int T>
-DEV float isoIntersect(const VolumeDD &v, float3 org, float3 dir, float tMax, uint64_t *seed,
-                                           const float *u8lut) {
-  float t0 = 0.f, t1 = tMax;
-  if (!boxTest(org, dir, t0, t1, v.boundsLo, v.boundsHi)) return tMax;
-  uint64_t raySeed = *seed;
-  float tHit;
-  const float3 o = f3((org.x - v.mcOrigin.x) * v.rcpMcSpacing.x, (org.y - v.mcOrigin.y) * v.rcpMcSpacing.y,
-                      (org.z - v.mcOrigin.z) * v.rcpMcSpacing.z);
-  const float3 d = f3(dir.x * v.rcpMcSpacing.x, dir.y * v.rcpMcSpacing.y, dir.z * v.rcpMcSpacing.z);
-  uint64_t rng = rngDerive(raySeed, kHash000);  // hash(instance 0, geometry 0, primitive 0)
-  *seed = raySeed;
+//
+// Warp-cooperative: the lanes that call it together walk their own
+// macrocells, but the eleven field samples of every lane's current
+// candidate macrocell are spread over all those lanes (a lane whose ray is
+// done keeps sampling for the others), each taking the owner's ray through
+// shuffles, into the warp's slice of isoBuf (32 x 11 floats).  Each owner
+// then runs the reference's segment test over its eleven values in order.
+// A sample has no side effects, so taking all eleven where the reference may
+// stop early gives the same hit.  jobs/job: the ray's job (batch kernels
+// sample the owner's volume).
+constexpr int kIsoBufPerWarp = 32 * 11;
+template <int T, bool BATCH>
+DEV float isoIntersect(const JobDD *jobs, int job, const VolumeDD &v, float3 org, float3 dir, float tMax,
+                       uint64_t *seed, const float *u8lut, float *isoBuf) {
+  const unsigned mask = __activemask();
+  const int lane = threadIdx.x & 31;
+  float tHit = tMax;
+  bool walking = false;  // the ray still has macrocells to walk
+  uint64_t rng = 0;
+  float t1 = tMax, ray_t0 = 0.f, nextCellBegin = 0.f;
+  float3 tNext = f3(0.f, 0.f, 0.f), tStep = f3(0.f, 0.f, 0.f);
+  int cx = 0, cy = 0, cz = 0, sx = 0, sy = 0, sz = 0, ex = 0, ey = 0, ez = 0;
   const float iso = v.iso.isoValue;
-  tHit = tMax;
-  // dda3 (DDA.h:61-201), tMax = the box test's t1
-  const float3 rcpd = f3(1.f / d.x, 1.f / d.y, 1.f / d.z);
-  const float3 fs = f3((float)v.mcDims.x, (float)v.mcDims.y, (float)v.mcDims.z);
-  float lx = (0.f - o.x) * rcpd.x, ly = (0.f - o.y) * rcpd.y, lz = (0.f - o.z) * rcpd.z;
-  float hx = (fs.x - o.x) * rcpd.x, hy = (fs.y - o.y) * rcpd.y, hz = (fs.z - o.z) * rcpd.z;
-  float nx = fmin_(lx, hx), ny = fmin_(ly, hy), nz = fmin_(lz, hz);
-  float fx = fmax_(lx, hx), fy = fmax_(ly, hy), fz = fmax_(lz, hz);
-  if (d.x == 0.f) { if (o.x < 0.f || o.x > fs.x) return tMax; nx = -kInf; fx = kInf; }
-  if (d.y == 0.f) { if (o.y < 0.f || o.y > fs.y) return tMax; ny = -kInf; fy = kInf; }
-  if (d.z == 0.f) { if (o.z < 0.f || o.z > fs.z) return tMax; nz = -kInf; fz = kInf; }
-  const float ray_t0 = fmax_(0.f, fmax_(fmax_(nx, ny), nz));
-  const float ray_t1 = fmin_(t1, fmin_(fmin_(fx, fy), fz));
-  if (ray_t0 > ray_t1) return tMax;
-  const float3 oi = f3(o.x + ray_t0 * d.x, o.y + ray_t0 * d.y, o.z + ray_t0 * d.z);
-  const float3 fc = f3(fmax_(0.f, fmin_(fs.x - 1.f, floorf(oi.x))), fmax_(0.f, fmin_(fs.y - 1.f, floorf(oi.y))),
-                       fmax_(0.f, fmin_(fs.z - 1.f, floorf(oi.z))));
-  const float3 fe = f3(d.x > 0.f ? fc.x + 1.f : fc.x, d.y > 0.f ? fc.y + 1.f : fc.y, d.z > 0.f ? fc.z + 1.f : fc.z);
-  const float3 tStep = f3(fabsf(rcpd.x), fabsf(rcpd.y), fabsf(rcpd.z));
-  float3 tNext = f3(d.x == 0.f ? kInf : fabsf(fe.x - oi.x) * tStep.x, d.y == 0.f ? kInf : fabsf(fe.y - oi.y) * tStep.y,
-                    d.z == 0.f ? kInf : fabsf(fe.z - oi.z) * tStep.z);
-  int cx = (int)fc.x, cy = (int)fc.y, cz = (int)fc.z;
-  const int sx = d.x > 0.f ? 1 : -1, sy = d.y > 0.f ? 1 : -1, sz = d.z > 0.f ? 1 : -1;
-  const int ex = d.x > 0.f ? v.mcDims.x : -1, ey = d.y > 0.f ? v.mcDims.y : -1, ez = d.z > 0.f ? v.mcDims.z : -1;
-  float nextCellBegin = 0.f;
-  // every iteration leaves one cell and the grid has < 2^31 cells, so the
-  // loop ends; the bound only guards against a non-finite step
-  for (int iter = 0; iter < (1 << 24); iter++) {
-    const float tClosest = fmin_(fmin_(tNext.x, tNext.y), tNext.z);
-    const float ct0 = ray_t0 + nextCellBegin;
-    const float ct1 = ray_t0 + fmin_(tClosest, t1);
-    // the macrocell callback
-    const float upper = fmin_(ct1, tMax);
-    if (ct0 < upper) {
-      const int rci = cx + v.mcDims.x * (cy + v.mcDims.y * cz);
-      const float2 rg = BNB_IN(rci, (long long)v.mcDims.x * v.mcDims.y * v.mcDims.z)
-                            ? __ldg(v.iso.ranges + rci)
-                            : make_float2(1.f, 0.f);  // (bounds-checked build: an empty range)
-      if (iso >= rg.x && iso <= rg.y) {
-        float tt1 = ct0;
-        float ff1 = sampleJob<T>(v, f3(org.x + tt1 * dir.x, org.y + tt1 * dir.y, org.z + tt1 * dir.z), u8lut);
-        bool done = false;
-        // one copy of the sampler for the ten steps (not unrolled: the
-        // unrolled scan held ten, a large share of this kernel's code)
-#pragma unroll 1
-        for (int i = 1; i <= 10; i++) {
-          const float tt0 = tt1;
-          const float ff0 = ff1;
-          const float fi = kIsoTenths[i];  // (float)i / 10.f
-          tt1 = (1.f - fi) * ct0 + fi * ct1;
-          ff1 = sampleJob<T>(v, f3(org.x + tt1 * dir.x, org.y + tt1 * dir.y, org.z + tt1 * dir.z), u8lut);
-          if (isnan(ff0) || isnan(ff1)) continue;
-          if (iso >= fmin_(ff0, ff1) && iso <= fmax_(ff0, ff1)) {
-            float t = (iso - ff0) / (ff1 - ff0);
-            t = (1.f - t) * tt0 + t * tt1;
-            tHit = (t < tHit) ? t : tHit;  // a 0/0 segment (NaN) keeps tHit
-            if (tHit < tMax) { done = true; break; }
-          }
+  {
+    float t0 = 0.f;
+    if (boxTest(org, dir, t0, t1, v.boundsLo, v.boundsHi)) {
+      uint64_t raySeed = *seed;
+      const float3 o = f3((org.x - v.mcOrigin.x) * v.rcpMcSpacing.x, (org.y - v.mcOrigin.y) * v.rcpMcSpacing.y,
+                          (org.z - v.mcOrigin.z) * v.rcpMcSpacing.z);
+      const float3 d = f3(dir.x * v.rcpMcSpacing.x, dir.y * v.rcpMcSpacing.y, dir.z * v.rcpMcSpacing.z);
+      rng = rngDerive(raySeed, kHash000);  // hash(instance 0, geometry 0, primitive 0)
+      *seed = raySeed;
+      // dda3 (DDA.h:61-201), tMax = the box test's t1
+      const float3 rcpd = f3(1.f / d.x, 1.f / d.y, 1.f / d.z);
+      const float3 fs = f3((float)v.mcDims.x, (float)v.mcDims.y, (float)v.mcDims.z);
+      float lx = (0.f - o.x) * rcpd.x, ly = (0.f - o.y) * rcpd.y, lz = (0.f - o.z) * rcpd.z;
+      float hx = (fs.x - o.x) * rcpd.x, hy = (fs.y - o.y) * rcpd.y, hz = (fs.z - o.z) * rcpd.z;
+      float nx = fmin_(lx, hx), ny = fmin_(ly, hy), nz = fmin_(lz, hz);
+      float fx = fmax_(lx, hx), fy = fmax_(ly, hy), fz = fmax_(lz, hz);
+      walking = true;
+      if (d.x == 0.f) { if (o.x < 0.f || o.x > fs.x) walking = false; nx = -kInf; fx = kInf; }
+      if (d.y == 0.f) { if (o.y < 0.f || o.y > fs.y) walking = false; ny = -kInf; fy = kInf; }
+      if (d.z == 0.f) { if (o.z < 0.f || o.z > fs.z) walking = false; nz = -kInf; fz = kInf; }
+      ray_t0 = fmax_(0.f, fmax_(fmax_(nx, ny), nz));
+      const float ray_t1 = fmin_(t1, fmin_(fmin_(fx, fy), fz));
+      if (ray_t0 > ray_t1) walking = false;
+      const float3 oi = f3(o.x + ray_t0 * d.x, o.y + ray_t0 * d.y, o.z + ray_t0 * d.z);
+      const float3 fc = f3(fmax_(0.f, fmin_(fs.x - 1.f, floorf(oi.x))), fmax_(0.f, fmin_(fs.y - 1.f, floorf(oi.y))),
+                           fmax_(0.f, fmin_(fs.z - 1.f, floorf(oi.z))));
+      const float3 fe = f3(d.x > 0.f ? fc.x + 1.f : fc.x, d.y > 0.f ? fc.y + 1.f : fc.y, d.z > 0.f ? fc.z + 1.f : fc.z);
+      tStep = f3(fabsf(rcpd.x), fabsf(rcpd.y), fabsf(rcpd.z));
+      tNext = f3(d.x == 0.f ? kInf : fabsf(fe.x - oi.x) * tStep.x, d.y == 0.f ? kInf : fabsf(fe.y - oi.y) * tStep.y,
+                 d.z == 0.f ? kInf : fabsf(fe.z - oi.z) * tStep.z);
+      cx = (int)fc.x; cy = (int)fc.y; cz = (int)fc.z;
+      sx = d.x > 0.f ? 1 : -1; sy = d.y > 0.f ? 1 : -1; sz = d.z > 0.f ? 1 : -1;
+      ex = d.x > 0.f ? v.mcDims.x : -1; ey = d.y > 0.f ? v.mcDims.y : -1; ez = d.z > 0.f ? v.mcDims.z : -1;
+    }
+  }
+  // every step leaves one cell and the grid has < 2^31 cells, so each walk
+  // ends; the bound only guards against a non-finite step
+  int iter = 0;
+  // leave the current cell (DDA.h:184-199); false when the grid is left
+  auto stepCell = [&](float tClosest) -> bool {
+    nextCellBegin = tClosest;
+    if (tNext.x == tClosest) { tNext.x += tStep.x; cx += sx; if (cx == ex) return false; }
+    if (tNext.y == tClosest) { tNext.y += tStep.y; cy += sy; if (cy == ey) return false; }
+    if (tNext.z == tClosest) { tNext.z += tStep.z; cz += sz; if (cz == ez) return false; }
+    return true;
+  };
+  const int workers = __popc(mask);
+  const int wrank = __popc(mask & ((1u << lane) - 1u));
+  float *buf = isoBuf;
+  while (true) {
+    // 1. each walking ray moves to its next candidate macrocell (range holds
+    //    the iso value) or leaves the grid
+    bool cand = false;
+    float ct0 = 0.f, ct1 = 0.f, tClosest = 0.f;
+    while (walking) {
+      tClosest = fmin_(fmin_(tNext.x, tNext.y), tNext.z);
+      ct0 = ray_t0 + nextCellBegin;
+      ct1 = ray_t0 + fmin_(tClosest, t1);
+      // the macrocell callback
+      const float upper = fmin_(ct1, tMax);
+      if (ct0 < upper) {
+        const int rci = cx + v.mcDims.x * (cy + v.mcDims.y * cz);
+        const float2 rg = BNB_IN(rci, (long long)v.mcDims.x * v.mcDims.y * v.mcDims.z)
+                              ? __ldg(v.iso.ranges + rci)
+                              : make_float2(1.f, 0.f);  // (bounds-checked build: an empty range)
+        if (iso >= rg.x && iso <= rg.y) {
+          cand = true;
+          break;
         }
-        if (done) break;
+      }
+      if (++iter >= (1 << 24) || !stepCell(tClosest)) walking = false;
+    }
+    const unsigned cmask = __ballot_sync(mask, cand);
+    if (!cmask) break;
+    // 2. the eleven samples of every candidate, spread over the warp: sample
+    //    point i is the entry for i = 0, else (1 - i/10) ct0 + (i/10) ct1
+    const int tasks = 11 * __popc(cmask);
+    for (int k0 = 0; k0 < tasks; k0 += workers) {
+      const int k = k0 + wrank;
+      const int r = k < tasks ? k / 11 : 0;
+      const int i = k < tasks ? k - 11 * r : 0;
+      const int owner = __fns(cmask, 0, r + 1);
+      const float ox = __shfl_sync(mask, org.x, owner), oy = __shfl_sync(mask, org.y, owner);
+      const float oz = __shfl_sync(mask, org.z, owner);
+      const float dx = __shfl_sync(mask, dir.x, owner), dy = __shfl_sync(mask, dir.y, owner);
+      const float dz = __shfl_sync(mask, dir.z, owner);
+      const float c0 = __shfl_sync(mask, ct0, owner), c1 = __shfl_sync(mask, ct1, owner);
+      const int oj = BATCH ? __shfl_sync(mask, job, owner) : 0;
+      if (k < tasks) {
+        const float fi = kIsoTenths[i];
+        const float tt = i == 0 ? c0 : (1.f - fi) * c0 + fi * c1;
+        const VolumeDD &vo = BATCH ? jobs[oj].v : v;
+        buf[owner * 11 + i] = sampleJob<T>(vo, f3(ox + tt * dx, oy + tt * dy, oz + tt * dz), u8lut);
       }
     }
-    nextCellBegin = tClosest;
-    if (tNext.x == tClosest) { tNext.x += tStep.x; cx += sx; if (cx == ex) break; }
-    if (tNext.y == tClosest) { tNext.y += tStep.y; cy += sy; if (cy == ey) break; }
-    if (tNext.z == tClosest) { tNext.z += tStep.z; cz += sz; if (cz == ez) break; }
+    __syncwarp(mask);
+    // 3. each candidate's segments in order (MCAccelerator.h:325-548): the
+    //    first that brackets the iso value and lies below tMax is the hit
+    if (cand) {
+      float tt1 = ct0;
+      float ff1 = buf[lane * 11];
+      bool done = false;
+#pragma unroll 1
+      for (int i = 1; i <= 10; i++) {
+        const float tt0 = tt1;
+        const float ff0 = ff1;
+        const float fi = kIsoTenths[i];  // (float)i / 10.f
+        tt1 = (1.f - fi) * ct0 + fi * ct1;
+        ff1 = buf[lane * 11 + i];
+        if (isnan(ff0) || isnan(ff1)) continue;
+        if (iso >= fmin_(ff0, ff1) && iso <= fmax_(ff0, ff1)) {
+          float t = (iso - ff0) / (ff1 - ff0);
+          t = (1.f - t) * tt0 + t * tt1;
+          tHit = (t < tHit) ? t : tHit;  // a 0/0 segment (NaN) keeps tHit
+          if (tHit < tMax) { done = true; break; }
+        }
+      }
+      // a hit ends the walk; otherwise on to the next macrocell
+      if (done || ++iter >= (1 << 24) || !stepCell(tClosest)) walking = false;
+    }
+    __syncwarp(mask);  // the buffer is read before the next round writes it
   }
   if (!(tHit < tMax)) return tMax;
   if (v.iso.alpha < 1.f && rngFloat(rng) > v.iso.alpha) return tMax;  // Lambertian::getOpacity
@@ -990,8 +1055,10 @@ __device__ __noinline__ SurfaceBounce surfaceBounce(const VolumeDD &v, const Fra
 // CMP: compensated sums (fr.comp) in no job (0: compiled out), in the jobs
 // that carry terms (1: a test per sum), or in every job (2)
 template <int T, bool BATCH, int LOG, int EXT, int CMP>
+// isoBuf: the warp's isosurface sample buffer (kIsoBufPerWarp floats in
+// shared memory; isosurface kernels only)
 DEV void renderLoop(const JobDD *__restrict__ jobs, const int *__restrict__ chunkStart, int numJobs, int numChunks, const SchedDD &sd,
-                    LaunchCounters *ctr, const float4 *sTF, const float *u8lut) {
+                    LaunchCounters *ctr, const float4 *sTF, const float *u8lut, float *isoBuf) {
   const unsigned FULL = 0xffffffffu;
   const int lane = threadIdx.x & 31;
   constexpr bool ISO = EXT >= 2;
@@ -1480,7 +1547,7 @@ DEV void renderLoop(const JobDD *__restrict__ jobs, const int *__restrict__ chun
           // shadow ray that hits the surface is occluded.
           const float3 dF = f3(ts.dir.x == 0.f ? 1e-6f : ts.dir.x, ts.dir.y == 0.f ? 1e-6f : ts.dir.y,
                                ts.dir.z == 0.f ? 1e-6f : ts.dir.z);
-          const float tIso = isoIntersect<T>(v, ts.org, dF, ts.rayTMax, &raySeed, u8lut);
+          const float tIso = isoIntersect<T, BATCH>(jobs, job, v, ts.org, dF, ts.rayTMax, &raySeed, u8lut, isoBuf);
           const bool isoHit = tIso < ts.rayTMax;
           if (isoHit && shadowRay) {
             phase = LP_HIT;
@@ -1620,12 +1687,14 @@ __global__ void __launch_bounds__(kRenderMaxThreads, EXT >= 2     ? kRenderMinBl
     renderKernel(const __grid_constant__ JobDD job, const __grid_constant__ SchedDD sd, LaunchCounters *ctr) {
   extern __shared__ float4 sTF[];
   __shared__ float u8lut[256];
+  __shared__ float sIsoBuf[EXT >= 2 ? kRenderMaxThreads / 32 * kIsoBufPerWarp : 1];
   for (int i = threadIdx.x; i < job.v.tfN; i += blockDim.x) sTF[i] = job.v.tf[i];
   for (int i = threadIdx.x; i < 256; i += blockDim.x) u8lut[i] = __fdiv_rn((float)i * 1.f, 255.f);
   __syncthreads();
   int numChunks = (job.fr.width * job.fr.height + kChunk - 1) / kChunk;
   if (job.fr.partCount > 1) numChunks = partitionChunks(numChunks, job.fr.partRank, job.fr.partCount);
-  renderLoop<T, false, LOG, EXT, CMP>(&job, nullptr, 1, numChunks, sd, ctr, sTF, u8lut);
+  renderLoop<T, false, LOG, EXT, CMP>(&job, nullptr, 1, numChunks, sd, ctr, sTF, u8lut,
+                                      EXT >= 2 ? sIsoBuf + (threadIdx.x >> 5) * kIsoBufPerWarp : nullptr);
 }
 
 // ---------------------------------------------------------------------------
@@ -2307,12 +2376,13 @@ __global__ void __launch_bounds__(kRenderMaxThreads, EXT >= 2     ? kRenderMinBl
     renderBatchKernel(const JobDD *__restrict__ jobs, const int *__restrict__ chunkStart, int numJobs, const __grid_constant__ SchedDD sd,
                       LaunchCounters *ctr) {
   __shared__ float u8lut[256];
+  __shared__ float sIsoBuf[EXT >= 2 ? kRenderMaxThreads / 32 * kIsoBufPerWarp : 1];
   for (int i = threadIdx.x; i < 256; i += blockDim.x) u8lut[i] = __fdiv_rn((float)i * 1.f, 255.f);
   __syncthreads();
   // plain batch kernels draw free-flight distances with fastLog only; batches
   // with an exact-log job run the extended kernel, which chooses per job
   renderLoop<T, true, EXT ? 2 : 0, EXT, CMP>(jobs, chunkStart, numJobs, __ldg(chunkStart + numJobs), sd, ctr, nullptr,
-                                             u8lut);
+                                             u8lut, EXT >= 2 ? sIsoBuf + (threadIdx.x >> 5) * kIsoBufPerWarp : nullptr);
 }
 
 // Field samples and transfer-function lookups at given points
@@ -2584,7 +2654,8 @@ __global__ void __launch_bounds__(kRenderMaxThreads, CMP == 1 ? kRenderMinBlocks
   __shared__ float u8lut[256];
   for (int i = threadIdx.x; i < 256; i += blockDim.x) u8lut[i] = __fdiv_rn((float)i * 1.f, 255.f);
   __syncthreads();
-  renderLoop<T, true, 0, 0, CMP>(tab.jobs, tab.chunkStart, numJobs, tab.chunkStart[numJobs], sd, ctr, nullptr, u8lut);
+  renderLoop<T, true, 0, 0, CMP>(tab.jobs, tab.chunkStart, numJobs, tab.chunkStart[numJobs], sd, ctr, nullptr, u8lut,
+                                 nullptr);
 }
 template <int CMP>
 static auto batchParamKernelFor(int voxelType) {
