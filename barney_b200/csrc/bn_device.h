@@ -22,7 +22,8 @@ constexpr int kRenderMinBlocks = 7;     // plain: 7 x 128 threads per SM (at mos
 constexpr int kRenderMinBlocksMixedComp = 6;  // plain, compensated sums tested per job (mixed batches):
                                               // 6 x 128 (85; at 7 they spill up to 348 B)
 constexpr int kRenderMinBlocksExt = 5;  // extended (multi-scatter, principled): 5 x 128 (102)
-constexpr int kRenderMinBlocksIso = 5;  // extended with isosurfaces: 5 x 128 (102; 3 % faster than 4 x 128)
+constexpr int kRenderMinBlocksIso = 4;  // extended with isosurfaces: 4 x 128 (128; with the warp-cooperative
+                                        // iso scan 3 % faster than 5 x 128, which spilled up to 820 B)
 
 // Principled volume coefficients evaluated from the field value
 // (PrincipledVolumeParams::DD, PrincipledVolume.h:33-46).

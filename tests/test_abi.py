@@ -71,11 +71,9 @@ def test_kernels_compiled_for_sm100a():
     assert "renderKernel" in log
     # The plain render kernels are capped at 7 blocks of 128 threads per SM
     # (72 registers), those that test compensation per job at 6 (80), the
-    # extended ones at 5 (96); the spill bytes that costs are a
-    # measured trade for the extra blocks (the isosurface kernels, EXT 2 and 3,
-    # spill most -- up to about 820 B with the warp-cooperative iso scan, which
-    # made the isosurface frame 25 % faster -- and still run 3 % faster at 5
-    # blocks than at 4).  A large spill would mean a regression.
+    # multi-scatter ones at 5 (96) and the isosurface ones (EXT 2 and 3) at 4
+    # (128); the spill bytes that costs are a measured trade for the extra
+    # blocks.  A large spill would mean a regression.
     blocks = log.split("Function properties for ")
     render = [b for b in blocks[1:] if b.split()[0].startswith(("_ZN3bnb12renderKernel", "_ZN3bnb17renderBatch"))]
     assert len(render) >= 2
@@ -85,7 +83,7 @@ def test_kernels_compiled_for_sm100a():
         # template arguments: renderKernel<T, LOG, EXT, CMP>, renderBatchKernel<T, EXT, CMP>
         args = re.findall(r"Li(n?\d+)E", name.split("EEv")[0])
         ext = int(args[2] if "renderKernel" in name.split("I")[0] else args[1])
-        assert m and int(m.group(1)) <= (900 if ext >= 2 else 320), b.splitlines()[1]
+        assert m and int(m.group(1)) <= 320, (ext, b.splitlines()[1])
 
 
 def test_header_compiles_as_c_and_shim_as_cpp(tmp_path):
