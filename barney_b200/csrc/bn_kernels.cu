@@ -835,10 +835,13 @@ DEV float isoIntersect(const JobDD *jobs, int job, const VolumeDD &v, float3 org
 // +-normalDelta, one-sided where a neighbour lies outside the field, and
 // -normalize(dir) for a zero gradient; returned normalized and rounded to
 // binary16, as Ray::packNormal stores it.
+// pre: the seven field values at P and P -/+ normalDelta along x, y, z
+// (isoNormalSamples, taken by the whole warp), or null to sample here
 template <int T>
-__device__ __noinline__ float3 isoNormal(const VolumeDD &v, float3 P, float3 dir, const float *u8lut) {
+__device__ __noinline__ float3 isoNormal(const VolumeDD &v, float3 P, float3 dir, const float *u8lut,
+                                         const float *pre) {
   const float dl = v.iso.normalDelta;
-  const float fP = sampleJob<T>(v, P, u8lut);
+  const float fP = pre ? pre[0] : sampleJob<T>(v, P, u8lut);
   // central differences: samples at P -/+ dl along x, then y, then z (one
   // copy of the sampler in a loop); an axis whose sample is NaN (outside the
   // field) uses fP instead and halves its step count
@@ -848,8 +851,9 @@ __device__ __noinline__ float3 isoNormal(const VolumeDD &v, float3 P, float3 dir
   for (int i = 0; i < 6; i++) {
     const int axis = i >> 1;
     const float o = (i & 1) ? dl : -dl;
-    const float fv = sampleJob<T>(v, f3(P.x + (axis == 0 ? o : 0.f), P.y + (axis == 1 ? o : 0.f),
-                                        P.z + (axis == 2 ? o : 0.f)), u8lut);
+    const float fv = pre ? pre[1 + i]
+                         : sampleJob<T>(v, f3(P.x + (axis == 0 ? o : 0.f), P.y + (axis == 1 ? o : 0.f),
+                                              P.z + (axis == 2 ? o : 0.f)), u8lut);
     if (!(i & 1)) {
       fLo = fv;
       continue;
@@ -964,7 +968,8 @@ struct SurfaceBounce {
 template <int T>
 __device__ __noinline__ SurfaceBounce surfaceBounce(const VolumeDD &v, const FrameDD &fr, float3 P, float tHit,
                                                     float3 dirFixed, float3 inOrg, float3 dir, float3 pathTp,
-                                                    uint64_t raySeed, int depth, int nDifB, const float *u8lut) {
+                                                    uint64_t raySeed, int depth, int nDifB, const float *u8lut,
+                                                    const float *normalSamples) {
   SurfaceBounce out;
   out.flags = 0;
   out.shadowMis = 1.f;
@@ -972,7 +977,7 @@ __device__ __noinline__ SurfaceBounce surfaceBounce(const VolumeDD &v, const Fra
   out.pathMis = 1.f;
   uint64_t random = rngDerive(raySeed, (uint64_t)__float_as_uint(tHit));
   out.shadowSeed = raySeed;
-  const float3 Ng = normalize3(isoNormal<T>(v, P, dirFixed, u8lut));
+  const float3 Ng = normalize3(isoNormal<T>(v, P, dirFixed, u8lut, normalSamples));
   const bool hitWasOnFront = dot3(dir, Ng) < 0.f;
   const float3 Ngff = hitWasOnFront ? Ng : f3(-Ng.x, -Ng.y, -Ng.z);
   const float3 won = normalize3(dir);
@@ -1043,6 +1048,42 @@ __device__ __noinline__ SurfaceBounce surfaceBounce(const VolumeDD &v, const Fra
                    P.z + (1.f * offsetEpsilon) * Ngff.z);
   out.flags |= 2 | 8;
   return out;
+}
+
+// The seven field samples of the normal (isoNormal) of every lane with
+// need, spread over all 32 lanes of the warp: for lane L, buf[7 L] at P and
+// buf[7 L + 1 + i] at P -/+ normalDelta along axis i / 2 (the points
+// isoNormal samples, formed by the same expressions).  Called by the whole
+// warp; P: the lane's hit point (ignored without need).
+template <int T, bool BATCH>
+DEV void isoNormalSamples(const JobDD *jobs, int job, const VolumeDD &v, float3 P, bool need, const float *u8lut,
+                          float *buf) {
+  const unsigned FULL = 0xffffffffu;
+  const int lane = threadIdx.x & 31;
+  const unsigned nmask = __ballot_sync(FULL, need);
+  if (!nmask) return;
+  const int tasks = 7 * __popc(nmask);
+  for (int k0 = 0; k0 < tasks; k0 += 32) {
+    const int k = k0 + lane;
+    const int r = k < tasks ? k / 7 : 0;
+    const int i = k < tasks ? k - 7 * r : 0;
+    const int owner = __fns(nmask, 0, r + 1);
+    const float px = __shfl_sync(FULL, P.x, owner), py = __shfl_sync(FULL, P.y, owner);
+    const float pz = __shfl_sync(FULL, P.z, owner);
+    const int oj = BATCH ? __shfl_sync(FULL, job, owner) : 0;
+    if (k < tasks) {
+      const VolumeDD &vo = BATCH ? jobs[oj].v : v;
+      float3 Q = f3(px, py, pz);
+      if (i > 0) {
+        const int axis = (i - 1) >> 1;
+        const float dl = vo.iso.normalDelta;
+        const float o = ((i - 1) & 1) ? dl : -dl;
+        Q = f3(px + (axis == 0 ? o : 0.f), py + (axis == 1 ? o : 0.f), pz + (axis == 2 ? o : 0.f));
+      }
+      buf[owner * 7 + i] = sampleJob<T>(vo, Q, u8lut);
+    }
+  }
+  __syncwarp();
 }
 
 // The render loop shared by the single-frame kernel (one job, read from a
@@ -1126,6 +1167,13 @@ DEV void renderLoop(const JobDD *__restrict__ jobs, const int *__restrict__ chun
         ts.t = ts.rayTMax;
         phase = LP_HIT;
       }
+      // the field samples of this pass's surface normals, taken by the whole
+      // warp (the lanes that shade a surface hit would take them one by one)
+      if (ISO)
+        isoNormalSamples<T, BATCH>(jobs, job, v,
+                                   f3(ts.org.x + ts.t * ts.dir.x, ts.org.y + ts.t * ts.dir.y, ts.org.z + ts.t * ts.dir.z),
+                                   phase == LP_HIT && !shadowRay && (ts.bits & 64) && !fr.emissionAbsorption, u8lut,
+                                   isoBuf);
       // ------------------------------------------------------------------
       // A1. collisions: shading and shadow-ray spawn (shadeRays.cu:608-746)
       // ------------------------------------------------------------------
@@ -1187,7 +1235,7 @@ DEV void renderLoop(const JobDD *__restrict__ jobs, const int *__restrict__ chun
             }
           } else if (ISO && surf) {
             const SurfaceBounce sb = surfaceBounce<T>(v, fr, P, tHit, ts.dir, ts.org, primDir, pathTp, raySeed, depth,
-                                                      nDifB, u8lut);
+                                                      nDifB, u8lut, isoBuf + lane * 7);
             raySeed = (sb.flags & 1) ? sb.shadowSeed : sb.seed;
             if (sb.flags & 1) {  // makeShadowRay (Ray.h:147-157)
               shadowFrag = f3(fmin_(sb.shadowMis * sb.shadowTp.x, clampMax), fmin_(sb.shadowMis * sb.shadowTp.y, clampMax),
