@@ -1118,7 +1118,7 @@ DEV void renderLoop(const JobDD *__restrict__ jobs, const int *__restrict__ chun
   int job = 0, ix = 0, iy = 0, k = 0;  // the pixel's index iy * width + ix is formed where it is used
   float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
   float4 comp = make_float4(0.f, 0.f, 0.f, 0.f);
-  TraceState ts;
+  TraceState ts{};  // defined in every lane: the warp-wide passes read idle lanes' too
   uint64_t raySeed = 0;
   float3 primDir = f3(0.f, 0.f, 0.f);
   // shadowFrag: the fragment a shadow ray adds when it reaches the light
@@ -1922,7 +1922,8 @@ __global__ void __launch_bounds__(kAQThreads, kAQMinBlocks)
   };
   auto chunkPixels = [&](int c) { return min(kChunk, npix - frameChunk(c) * kChunk); };
   bool ok = true;
-  unsigned idlePolls = 0;
+  unsigned idlePolls = 0;  // polls without work since the live-slot count last changed
+  int lastLive = -1;
 
   while (true) {
     if ((nSamples | nVisits | nRays) >= 0x80000000u) {
@@ -1958,6 +1959,10 @@ __global__ void __launch_bounds__(kAQThreads, kAQMinBlocks)
     else if (pend[AQ_IDLE] > 0) q = AQ_IDLE;
     if (q < 0) {
       if (exhausted && live == 0) break;  // the frame is done
+      if (live != lastLive) {  // other warps are finishing pixels: still progress
+        lastLive = live;
+        idlePolls = 0;
+      }
       if (++idlePolls > kAQIdleCap) {
         errBits |= ERR_ITER_CAP;
         if (lane == 0) atomicExch(&sh.failed, 1);
