@@ -468,3 +468,18 @@ def test_iso_opacity_zero_passes_every_ray_and_one_blocks():
     assert st["rays"] == 16 * 16 * 2
     acc1, _, _ = oracle.render(oracle.Scene(d), 0, 2)
     assert not np.array_equal(acc1, acc)
+
+
+def test_iso_scan_step_table_is_the_correctly_rounded_quotient():
+    # The isosurface scan's step fractions (MCAccelerator.h: (float)i / 10.f)
+    # come from a table in the kernels; every entry must be that quotient,
+    # rounded once to binary32, as the oracle evaluates it.
+    import os
+    import re
+    src = open(os.path.join(os.path.dirname(__file__), "..", "barney_b200", "csrc", "bn_kernels.cu")).read()
+    m = re.search(r"kIsoTenths\[11\]\s*=\s*\{([^}]*)\}", src)
+    assert m, "step table not found"
+    table = [np.float32(float(x.strip().rstrip("f"))) for x in m.group(1).split(",")]
+    assert len(table) == 11
+    for i, t in enumerate(table):
+        assert t.view(np.uint32) == (np.float32(i) / np.float32(10)).view(np.uint32), i
